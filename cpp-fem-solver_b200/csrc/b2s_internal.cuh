@@ -1,0 +1,402 @@
+// Internal definitions shared by the b2s CUDA sources (sm_100a only).
+//
+// Layout in HBM: every operator and factor is device resident for the life of
+// its handle.  CSR uses uint32 row_ptr / col_idx and FP64 values (plus an
+// optional FP32 copy for mixed-precision preconditioners); BAIJ stores blocks
+// row-major, contiguous per block.  Vectors are plain FP64 arrays.
+//
+// Numerics: the library is compiled with -fmad=false, so every a*b+c is a
+// rounded multiply followed by a rounded add, as in the reference compiled
+// with ISO C++17 (no contraction).  Per-row sums run in ascending column
+// order, so SpMV and triangular-solve rows equal the reference bit for bit.
+// Reductions (dots, norms) use a fixed-order two-level tree: block partials in
+// a fixed grid, combined by the last block to arrive; the result is identical
+// from run to run.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "b2s.h"
+
+namespace b2s {
+
+// ----------------------------------------------------------------- errors
+
+struct Error : std::runtime_error
+{
+    b2s_status status;
+    Error(b2s_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] inline void fail(b2s_status s, const std::string& m) { throw Error(s, m); }
+
+inline void cuda_check(cudaError_t e, const char* what)
+{
+    if (e != cudaSuccess)
+    {
+        if (e == cudaErrorMemoryAllocation)
+        {
+            cudaGetLastError();
+            fail(B2S_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
+        }
+        fail(B2S_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+#define B2S_CUDA(call) ::b2s::cuda_check((call), #call)
+
+// ------------------------------------------------------------ device buffer
+
+template <typename T>
+struct DBuf
+{
+    T* p = nullptr;
+    size_t n = 0;
+    DBuf() = default;
+    explicit DBuf(size_t count) { alloc(count); }
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf& operator=(DBuf&& o) noexcept
+    {
+        if (this != &o)
+        {
+            release();
+            p = o.p;
+            n = o.n;
+            o.p = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
+    ~DBuf() { release(); }
+    void alloc(size_t count)
+    {
+        release();
+        n = count;
+        if (count) B2S_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    }
+    // grows (never shrinks); contents are not preserved
+    void reserve(size_t count)
+    {
+        if (count > n) alloc(count);
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// --------------------------------------------------------------- constants
+
+constexpr int kThreads = 256;          // block size of streaming / reduction kernels
+constexpr int kMaxRedValues = 4;       // values reduced together by one kernel
+constexpr int kSpmvRowsPerCta = 256;   // staged SpMV: at most this many rows per CTA
+constexpr int kSpmvNnzPerCta = 3072;   // staged SpMV: nnz staged in shared memory per CTA
+
+// Device-side solver state: the scalars of one Krylov iteration.  Kernels read
+// it at entry, the last block of each reduction kernel updates it.
+struct KState
+{
+    double normb, tol;
+    double rz_old, pAp, alpha, beta, normr, omega, rho_old, rho_new;
+    double relres;
+    double aux[8];
+    int it;       // iteration index in progress
+    int it_end;   // the reference's returned count
+    int maxit;
+    int done;     // 1 once converged / failed / stopped
+    int status;   // b2s_status
+    int iters;    // iterations executed (SpMVs in the loop)
+    int pad[2];
+};
+
+}  // namespace b2s
+
+// ------------------------------------------------------------------ handles
+
+struct b2s_ctx
+{
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    uint64_t launches = 0;
+    // reduction scratch: partial sums (kMaxRedValues per block) + arrival counter
+    b2s::DBuf<double> partial;
+    b2s::DBuf<unsigned int> counter;
+    // general device scratch and pinned host staging
+    b2s::DBuf<b2s::KState> kstate;
+    b2s::DBuf<double> ws;             // Krylov workspace, grown on demand
+    b2s::DBuf<double> small;          // Hessenberg / Givens scratch
+    b2s::KState* h_kstate = nullptr;  // pinned mirror
+    double* h_scalar = nullptr;       // pinned, 64 doubles
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace b2s {
+
+struct CsrDev
+{
+    uint32_t n = 0, m = 0, nnz = 0;
+    DBuf<uint32_t> rp, ci;
+    DBuf<double> v;
+    DBuf<float> v32;            // FP32 copy, created on demand
+    DBuf<uint32_t> blk_row;     // staged-SpMV row partition (nblk+1)
+    uint32_t nblk = 0;
+    DBuf<double> diag;          // diagonal entries (0 where missing)
+    std::vector<uint32_t> h_rp, h_ci;  // host copies of the pattern (setup code)
+    std::vector<double> h_v;
+    void ensure_fp32(b2s_ctx* ctx);
+};
+
+struct BaijDev
+{
+    int bs = 3;
+    uint32_t nbr = 0, nbc = 0, nnzb = 0;
+    DBuf<uint32_t> rp, ci;
+    DBuf<double> v;
+    DBuf<uint32_t> diag_ptr;    // UINT32_MAX when missing
+    DBuf<uint32_t> blk_row;     // staged matvec row partition
+    uint32_t nblk = 0;
+    std::vector<uint32_t> h_rp, h_ci, h_diag;
+    std::vector<double> h_v;
+};
+
+// Preconditioner implementation.  apply() enqueues z = M^-1 r on ctx->stream
+// (device pointers).  `done` (device, may be null) lets the Krylov drivers
+// replay work after convergence: every kernel returns at once when *done != 0.
+struct PcImpl
+{
+    virtual ~PcImpl() = default;
+    virtual void apply(b2s_ctx* ctx, const double* r, double* z, const int* done) = 0;
+    // diagonal scaling that the PCG update kernel can fuse (null if none)
+    virtual const double* fused_diag() const { return nullptr; }
+    virtual bool is_identity() const { return false; }
+    virtual bool is_host() const { return false; }
+    virtual void export_data(b2s_ctx*, const std::string& what, uint64_t* sizes, uint32_t* rp, uint32_t* ci,
+                             double* v)
+    {
+        fail(B2S_UNSUPPORTED, "export '" + what + "' not available for this preconditioner");
+    }
+};
+
+}  // namespace b2s
+
+struct b2s_csr
+{
+    b2s_ctx* ctx = nullptr;
+    b2s::CsrDev d;
+};
+
+struct b2s_baij
+{
+    b2s_ctx* ctx = nullptr;
+    b2s::BaijDev d;
+};
+
+struct b2s_pc
+{
+    b2s_ctx* ctx = nullptr;
+    b2s_pc_kind kind = B2S_PC_NONE;
+    uint64_t n = 0;
+    double setup_ms = 0.0;
+    std::unique_ptr<b2s::PcImpl> impl;
+};
+
+namespace b2s {
+
+// ------------------------------------------------------------ API guarding
+
+template <typename F>
+b2s_status guarded(b2s_ctx* ctx, F&& f)
+{
+    try
+    {
+        f();
+        return B2S_OK;
+    }
+    catch (const Error& e)
+    {
+        if (ctx) ctx->err = e.what();
+        return e.status;
+    }
+    catch (const std::bad_alloc&)
+    {
+        if (ctx) ctx->err = "host allocation failed";
+        return B2S_OUT_OF_MEMORY;
+    }
+    catch (const std::exception& e)
+    {
+        if (ctx) ctx->err = e.what();
+        return B2S_CUDA_ERROR;
+    }
+}
+
+inline void need(bool cond, b2s_status s, const char* msg)
+{
+    if (!cond) fail(s, msg);
+}
+
+inline void note_launch(b2s_ctx* ctx, const char* what)
+{
+    ctx->launches++;
+#ifdef B2S_DEBUG_SYNC
+    B2S_CUDA(cudaStreamSynchronize(ctx->stream));
+#endif
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess) cuda_check(cudaGetLastError(), what);
+}
+
+#define B2S_LAUNCH(ctx, kernel, grid, block, smem, ...)                                    \
+    do                                                                                     \
+    {                                                                                      \
+        kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);                   \
+        ::b2s::note_launch((ctx), #kernel);                                                \
+    } while (0)
+
+inline unsigned stream_grid(const b2s_ctx* ctx, uint64_t n)
+{
+    uint64_t g = (n + kThreads - 1) / kThreads;
+    uint64_t cap = (uint64_t)ctx->sm_count * 8;
+    if (g > cap) g = cap;
+    return g ? (unsigned)g : 1u;
+}
+
+// reserve reduction scratch for `blocks` blocks
+inline void reserve_reduction(b2s_ctx* ctx, unsigned blocks)
+{
+    ctx->partial.reserve((size_t)blocks * kMaxRedValues);
+}
+
+// --------------------------------------------------- device-side reductions
+
+// Fixed-order block reduction of NV values (all threads receive the result).
+template <int NV>
+__device__ __forceinline__ void block_reduce(double (&v)[NV])
+{
+    __shared__ double sred[NV][kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+    {
+        double a = v[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+        if (lane == 0) sred[k][warp] = a;
+    }
+    __syncthreads();
+    if (warp == 0)
+    {
+#pragma unroll
+        for (int k = 0; k < NV; ++k)
+        {
+            double a = lane < (kThreads / 32) ? sred[k][lane] : 0.0;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
+            if (lane == 0) sred[k][0] = a;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] = sred[k][0];
+    __syncthreads();
+}
+
+// Grid-wide deterministic reduction: every block contributes v; returns true
+// in the last block to arrive, where v then holds the grid total (summed over
+// block partials in block order).  Must be called by all threads of every
+// block exactly once per kernel.
+template <int NV>
+__device__ __forceinline__ bool grid_reduce_last(double (&v)[NV], double* partial, unsigned int* counter)
+{
+    __shared__ bool s_last;
+    block_reduce<NV>(v);
+    if (threadIdx.x == 0)
+    {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) partial[(size_t)k * gridDim.x + blockIdx.x] = v[k];
+        __threadfence();
+        const unsigned t = atomicAdd(counter, 1u);
+        s_last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!s_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+    {
+        double a = 0.0;
+        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+            a += __ldcg(&partial[(size_t)k * gridDim.x + b]);
+        v[k] = a;
+    }
+    block_reduce<NV>(v);
+    if (threadIdx.x == 0) *counter = 0u;
+    return true;
+}
+
+// ---------------------------------------------------------- host helpers
+
+inline void h2d(b2s_ctx* ctx, void* dst, const void* src, size_t bytes)
+{
+    if (bytes) B2S_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+}
+inline void d2h(b2s_ctx* ctx, void* dst, const void* src, size_t bytes)
+{
+    if (bytes) B2S_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+}
+inline void d2d(b2s_ctx* ctx, void* dst, const void* src, size_t bytes)
+{
+    if (bytes) B2S_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+}
+inline void sync(b2s_ctx* ctx) { B2S_CUDA(cudaStreamSynchronize(ctx->stream)); }
+
+template <typename T>
+DBuf<T> upload(b2s_ctx* ctx, const T* src, size_t count)
+{
+    DBuf<T> b(count);
+    h2d(ctx, b.p, src, count * sizeof(T));
+    return b;
+}
+
+// ------------------------------------------- kernels shared across files
+
+// y = A x, staged CSR (csr.cu)
+void spmv(b2s_ctx* ctx, const CsrDev& A, const double* x, double* y, const int* done = nullptr);
+// dot product into *out (device), deterministic (blas1.cu)
+void dot_dev(b2s_ctx* ctx, uint64_t n, const double* a, const double* b, double* out, const int* done = nullptr);
+double dot_host(b2s_ctx* ctx, uint64_t n, const double* a, const double* b);
+void fill(b2s_ctx* ctx, double* x, double v, uint64_t n);
+void copy(b2s_ctx* ctx, double* dst, const double* src, uint64_t n, const int* done = nullptr);
+// BAIJ matvec (baij.cu)
+void baij_matvec(b2s_ctx* ctx, const BaijDev& A, const double* x, double* y, const int* done = nullptr);
+// row partition for staged kernels (csr.cu)
+void build_row_blocks(const uint32_t* rp, uint32_t nrows, uint32_t unit, uint32_t max_rows, uint32_t max_units,
+                      std::vector<uint32_t>& out);
+
+// preconditioner factories (one per file)
+std::unique_ptr<PcImpl> make_pc_diag(b2s_ctx* ctx, const CsrDev& A);
+std::unique_ptr<PcImpl> make_pc_identity(uint64_t n);
+std::unique_ptr<PcImpl> make_pc_ic0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);
+std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);
+std::unique_ptr<PcImpl> make_pc_ssor(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);
+std::unique_ptr<PcImpl> make_pc_amg_csr(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);
+std::unique_ptr<PcImpl> make_pc_amg_baij(b2s_ctx* ctx, const BaijDev& A, const b2s_pc_opts& o);
+std::unique_ptr<PcImpl> make_pc_bjacobi(b2s_ctx* ctx, const BaijDev& A);
+std::unique_ptr<PcImpl> make_pc_bilu0(b2s_ctx* ctx, const BaijDev& A, const b2s_pc_opts& o);
+std::unique_ptr<PcImpl> make_pc_learned_ic0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);
+std::unique_ptr<PcImpl> make_pc_host(uint64_t n, b2s_host_pc_fn fn, void* user);
+
+}  // namespace b2s

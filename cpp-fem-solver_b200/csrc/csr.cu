@@ -1,0 +1,155 @@
+// CSR handles and SpMV (SMatrix::spmv, array.cpp:3418-3442).
+#include "spmv_staged.cuh"
+
+#include <algorithm>
+
+namespace b2s {
+
+// Greedy row partition: a block closes when it holds max_rows rows or when
+// the next row would push it past max_units units (nnz or nonzero blocks); a
+// row that alone exceeds max_units gets a block of its own.
+void build_row_blocks(const uint32_t* rp, uint32_t nrows, uint32_t unit, uint32_t max_rows, uint32_t max_units,
+                      std::vector<uint32_t>& out)
+{
+    (void)unit;
+    out.clear();
+    out.push_back(0);
+    uint32_t start = 0;
+    while (start < nrows)
+    {
+        uint32_t r = start;
+        const uint32_t base = rp[start];
+        while (r < nrows && r - start < max_rows && rp[r + 1] - base <= max_units) ++r;
+        if (r == start) r = start + 1;  // a single oversized row
+        out.push_back(r);
+        start = r;
+    }
+}
+
+__global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+void CsrDev::ensure_fp32(b2s_ctx* ctx)
+{
+    if (v32.p || nnz == 0) return;
+    v32.alloc(nnz);
+    B2S_LAUNCH(ctx, k_to_f32, stream_grid(ctx, nnz), kThreads, 0, v.p, v32.p, (uint64_t)nnz);
+}
+
+__global__ void k_extract_diag(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                               const double* __restrict__ v, double* __restrict__ d)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        double di = 0.0;
+        for (uint32_t k = rp[i]; k < rp[i + 1]; ++k)
+            if (ci[k] == i)
+            {
+                di = v[k];
+                break;
+            }
+        d[i] = di;
+    }
+}
+
+void spmv(b2s_ctx* ctx, const CsrDev& A, const double* x, double* y, const int* done)
+{
+    if (A.n == 0) return;
+    launch_spmv(ctx, A, x, done, EpiStore{y});
+}
+
+}  // namespace b2s
+
+using namespace b2s;
+
+extern "C" {
+
+b2s_status b2s_csr_create(b2s_ctx* ctx, uint32_t n, uint32_t m, const uint32_t* row_ptr, const uint32_t* col_idx,
+                          const double* values, b2s_csr** out)
+{
+    if (!ctx || !out || !row_ptr) return B2S_INVALID_ARG;
+    *out = nullptr;
+    b2s_csr* A = new b2s_csr();
+    A->ctx = ctx;
+    b2s_status st = guarded(ctx, [&] {
+        B2S_CUDA(cudaSetDevice(ctx->device));
+        need(row_ptr[0] == 0, B2S_INVALID_ARG, "row_ptr[0] must be 0");
+        for (uint32_t i = 0; i < n; ++i) need(row_ptr[i + 1] >= row_ptr[i], B2S_INVALID_ARG, "row_ptr must be non-decreasing");
+        const uint32_t nnz = row_ptr[n];
+        need(nnz == 0 || (col_idx && values), B2S_INVALID_ARG, "null col_idx / values");
+        for (uint32_t i = 0; i < n; ++i)
+            for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+            {
+                need(col_idx[k] < m, B2S_INVALID_ARG, "column index out of range");
+                need(k == row_ptr[i] || col_idx[k] > col_idx[k - 1], B2S_INVALID_ARG,
+                     "columns must be strictly ascending within a row");
+            }
+        CsrDev& d = A->d;
+        d.n = n;
+        d.m = m;
+        d.nnz = nnz;
+        d.h_rp.assign(row_ptr, row_ptr + n + 1);
+        d.h_ci.assign(col_idx, col_idx + nnz);
+        d.h_v.assign(values, values + nnz);
+        d.rp = upload(ctx, row_ptr, (size_t)n + 1);
+        d.ci = upload(ctx, col_idx, nnz);
+        d.v = upload(ctx, values, nnz);
+        std::vector<uint32_t> blk;
+        build_row_blocks(row_ptr, n, 1, kSpmvRowsPerCta, kSpmvNnzPerCta, blk);
+        d.nblk = (uint32_t)blk.size() - 1;
+        d.blk_row = upload(ctx, blk.data(), blk.size());
+        if (n == m && n > 0)
+        {
+            d.diag.alloc(n);
+            B2S_LAUNCH(ctx, k_extract_diag, stream_grid(ctx, n), kThreads, 0, n, d.rp.p, d.ci.p, d.v.p, d.diag.p);
+        }
+        sync(ctx);
+    });
+    if (st != B2S_OK)
+    {
+        delete A;
+        return st;
+    }
+    *out = A;
+    return B2S_OK;
+}
+
+b2s_status b2s_csr_destroy(b2s_csr* A)
+{
+    if (!A) return B2S_INVALID_ARG;
+    cudaSetDevice(A->ctx->device);
+    delete A;
+    return B2S_OK;
+}
+
+b2s_status b2s_csr_info(const b2s_csr* A, uint32_t* n, uint32_t* m, uint32_t* nnz)
+{
+    if (!A) return B2S_INVALID_ARG;
+    if (n) *n = A->d.n;
+    if (m) *m = A->d.m;
+    if (nnz) *nnz = A->d.nnz;
+    return B2S_OK;
+}
+
+b2s_status b2s_spmv_device(b2s_ctx* ctx, const b2s_csr* A, const double* d_x, double* d_y)
+{
+    if (!ctx || !A) return B2S_INVALID_ARG;
+    return guarded(ctx, [&] { spmv(ctx, A->d, d_x, d_y); });
+}
+
+b2s_status b2s_spmv(b2s_ctx* ctx, const b2s_csr* A, const double* x, double* y)
+{
+    if (!ctx || !A || (!x && A->d.m) || (!y && A->d.n)) return B2S_INVALID_ARG;
+    return guarded(ctx, [&] {
+        DBuf<double> dx(A->d.m), dy(A->d.n);
+        h2d(ctx, dx.p, x, dx.bytes());
+        spmv(ctx, A->d, dx.p, dy.p);
+        d2h(ctx, y, dy.p, dy.bytes());
+        sync(ctx);
+    });
+}
+
+}  // extern "C"

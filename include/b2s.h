@@ -1,0 +1,279 @@
+/* b2s.h -- C ABI of the B200-native sparse iterative-solver library.
+ *
+ * This is the drop-in boundary for the sparse solver path of
+ * xuyinshen/cpp-FEM-solver: every solver and preconditioner that the
+ * reference exposes as a static member of sparse::SMatrix
+ * (ode-solver/include/math/array.hpp:266-373) or as a member / free function
+ * of block::BlockMatrix (ode-solver/include/math/blockMatrix.hpp:139-452)
+ * maps onto one entry point here.  The C++ drop-in headers
+ * include/b2s/math/array.hpp and include/b2s/math/blockMatrix.hpp re-expose
+ * the reference's own call surface on top of it.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Index arrays are uint32 (as in the
+ *     reference), values FP64.  Functions without a _device suffix take HOST
+ *     pointers and copy in/out; _device variants take device pointers already
+ *     resident on the context's GPU and enqueue on the context's stream.
+ *   - Every function returns b2s_status.  b2s_last_error(ctx) gives the
+ *     message of the last failure on that context.
+ *   - Handles belong to one context (one device, one CUDA stream).  Calls on
+ *     one context must be serialised by the caller; distinct contexts are
+ *     independent.
+ *   - Nothing here falls back to the CPU: without a usable GPU the context
+ *     cannot be created (B2S_NO_DEVICE) and no solver runs.
+ */
+#ifndef B2S_H
+#define B2S_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B2S_VERSION_MAJOR 0
+#define B2S_VERSION_MINOR 1
+
+typedef enum b2s_status
+{
+    B2S_OK = 0,
+    B2S_INVALID_ARG = 1,     /* std::invalid_argument in the reference */
+    B2S_SHAPE = 2,           /* std::invalid_argument (dimension mismatch) */
+    B2S_NOT_SPD = 3,         /* std::runtime_error: pAp <= 0, rz <= 0, IC(0) pivot <= 1e-14, diag <= 0 */
+    B2S_BREAKDOWN = 4,       /* std::runtime_error: Krylov breakdown below 1e-30 */
+    B2S_ZERO_PIVOT = 5,      /* std::runtime_error: ILU(0) |U_kk| < 1e-30, diag |d| < 1e-14 */
+    B2S_MISSING_DIAG = 6,    /* std::runtime_error: a row without diagonal entry */
+    B2S_SINGULAR_BLOCK = 7,  /* std::runtime_error: a singular diagonal block */
+    B2S_DIVERGED = 8,        /* NaN / Inf in a residual */
+    B2S_TIMEOUT = 9,         /* a bounded device-side wait gave up */
+    B2S_CUDA_ERROR = 10,
+    B2S_NO_DEVICE = 11,
+    B2S_OUT_OF_MEMORY = 12,
+    B2S_UNSUPPORTED = 13
+} b2s_status;
+
+typedef struct b2s_ctx b2s_ctx;
+typedef struct b2s_csr b2s_csr;
+typedef struct b2s_baij b2s_baij;
+typedef struct b2s_pc b2s_pc;
+
+/* ------------------------------------------------------------------ context */
+
+/* Creates a context on CUDA device `device` with its own non-blocking stream. */
+b2s_status b2s_ctx_create(int device, b2s_ctx** out);
+b2s_status b2s_ctx_destroy(b2s_ctx* ctx);
+/* Message of the last failure on ctx (static storage inside ctx). */
+const char* b2s_last_error(const b2s_ctx* ctx);
+/* Name of a status code. */
+const char* b2s_status_name(b2s_status st);
+/* The context's cudaStream_t, for callers that enqueue their own work. */
+void* b2s_ctx_stream(b2s_ctx* ctx);
+b2s_status b2s_ctx_synchronize(b2s_ctx* ctx);
+/* Number of this library's kernels launched on ctx since creation. */
+uint64_t b2s_ctx_kernel_launches(const b2s_ctx* ctx);
+
+/* ---------------------------------------------------------------- matrices */
+
+/* CSR matrix from host arrays (SMatrix CSR constructor, array.cpp:2183-2189).
+ * Columns must be sorted ascending within each row (the SMatrix COO
+ * constructor, array.cpp:2072-2182, guarantees this).  The arrays are copied
+ * to the device; the handle owns the copy. */
+b2s_status b2s_csr_create(b2s_ctx* ctx, uint32_t n, uint32_t m, const uint32_t* row_ptr, const uint32_t* col_idx,
+                          const double* values, b2s_csr** out);
+b2s_status b2s_csr_destroy(b2s_csr* A);
+b2s_status b2s_csr_info(const b2s_csr* A, uint32_t* n, uint32_t* m, uint32_t* nnz);
+
+/* Block-CSR (BAIJ) matrix, BlockMatrix<double,BS> constructor
+ * (blockMatrix.hpp:175-186).  bs in {1, 2, 3, 4}.  values holds
+ * nnzb*bs*bs doubles, row-major inside each block; vectors are node-major. */
+b2s_status b2s_baij_create(b2s_ctx* ctx, int bs, uint32_t nbr, uint32_t nbc, const uint32_t* row_ptr,
+                           const uint32_t* col_idx, const double* values, b2s_baij** out);
+b2s_status b2s_baij_destroy(b2s_baij* A);
+b2s_status b2s_baij_info(const b2s_baij* A, int* bs, uint32_t* nbr, uint32_t* nbc, uint32_t* nnzb);
+
+/* --------------------------------------------------------------- operators */
+
+/* y = A x.  SMatrix::spmv (array.cpp:3418-3442).  Each row is summed in
+ * ascending column order, so the result equals the reference bit for bit. */
+b2s_status b2s_spmv(b2s_ctx* ctx, const b2s_csr* A, const double* x, double* y);
+b2s_status b2s_spmv_device(b2s_ctx* ctx, const b2s_csr* A, const double* d_x, double* d_y);
+
+/* SMatrix::dot (array.cpp:3401-3416), deterministic fixed-order reduction. */
+b2s_status b2s_dot(b2s_ctx* ctx, uint64_t n, const double* a, const double* b, double* out);
+b2s_status b2s_dot_device(b2s_ctx* ctx, uint64_t n, const double* d_a, const double* d_b, double* out);
+
+/* BlockMatrix::matvec (blockMatrix.hpp:208-234); distributed_matvec
+ * (blockMatrix.hpp:351-442) on one device-resident matrix is the same call. */
+b2s_status b2s_baij_matvec(b2s_ctx* ctx, const b2s_baij* A, const double* x, double* y);
+b2s_status b2s_baij_matvec_device(b2s_ctx* ctx, const b2s_baij* A, const double* d_x, double* d_y);
+
+/* --------------------------------------------------------- preconditioners */
+
+typedef enum b2s_pc_kind
+{
+    B2S_PC_NONE = 0,        /* identity: "none", "identity", "noprecond", ("cg" for pcg) */
+    B2S_PC_DIAG = 1,        /* make_diag_preconditioner, array.cpp:2450-2508 */
+    B2S_PC_IC0 = 2,         /* make_ic0_preconditioner, array.cpp:2522-2732 */
+    B2S_PC_ILU0 = 3,        /* make_ilu0_preconditioner, array.cpp:2744-2934 */
+    B2S_PC_SSOR = 4,        /* make_ssor_preconditioner, array.cpp:3068-3164 */
+    B2S_PC_SA_AMG = 5,      /* smoothed aggregation: make_block_amg_preconditioner on the
+                               BS=1 condensed matrix, blockMatrix.hpp:1051-1179 */
+    B2S_PC_LEARNED_IC0 = 6, /* IC(0) pattern with values from the message-passing network */
+    B2S_PC_BJACOBI = 7,     /* BlockMatrix::gmres "blockjacobi", blockMatrix.hpp:714-733 */
+    B2S_PC_BILU0 = 8,       /* make_block_ilu0_preconditioner, blockMatrix.hpp:455-623 */
+    B2S_PC_BSA_AMG = 9      /* make_block_amg_preconditioner on a BAIJ matrix */
+} b2s_pc_kind;
+
+/* Storage / arithmetic precision of a preconditioner. */
+typedef enum b2s_precision
+{
+    B2S_FP64 = 0,
+    B2S_FP32 = 1, /* factors / hierarchy stored FP32, applied with FP32 accumulation */
+    B2S_BF16 = 2  /* AMG: BF16 fine-level operator storage, FP32 elsewhere */
+} b2s_precision;
+
+/* Triangular-solve schedule for IC(0)/ILU(0)/block ILU(0). */
+typedef enum b2s_trsv
+{
+    B2S_TRSV_AUTO = 0,
+    B2S_TRSV_LEVEL = 1,    /* one launch per level of the dependency DAG */
+    B2S_TRSV_SYNCFREE = 2  /* one launch; rows wait on bounded per-row ready flags */
+} b2s_trsv;
+
+typedef struct b2s_pc_opts
+{
+    double omega;        /* SSOR relaxation (reference default 1.2) */
+    int precision;       /* b2s_precision */
+    int trsv;            /* b2s_trsv */
+    int amg_ref_coarse;  /* 1: reproduce the reference's coarsest-level elimination
+                            (blockMatrix.hpp:958-1000) bit for bit; 0: correct pivoted LU */
+    int amg_max_levels;  /* 0: reference default 20 */
+    int amg_coarse_max;  /* 0: reference default 50 block rows */
+    const char* learned_weights; /* B2S_PC_LEARNED_IC0: path of a weight file, NULL = built-in init */
+} b2s_pc_opts;
+
+/* Fills opts with the reference's defaults. */
+void b2s_pc_opts_default(b2s_pc_opts* opts);
+
+b2s_status b2s_pc_create(b2s_ctx* ctx, const b2s_csr* A, b2s_pc_kind kind, const b2s_pc_opts* opts, b2s_pc** out);
+b2s_status b2s_pc_create_baij(b2s_ctx* ctx, const b2s_baij* A, b2s_pc_kind kind, const b2s_pc_opts* opts,
+                              b2s_pc** out);
+/* Preconditioner that calls back into host code (a user's std::function).
+ * The solver copies r to host, calls fn(user, r, z, n) and copies z back. */
+typedef int (*b2s_host_pc_fn)(void* user, const double* r, double* z, uint64_t n);
+b2s_status b2s_pc_create_host(b2s_ctx* ctx, uint64_t n, b2s_host_pc_fn fn, void* user, b2s_pc** out);
+b2s_status b2s_pc_destroy(b2s_pc* pc);
+/* z = M^-1 r (the functor returned by the reference factories). */
+b2s_status b2s_pc_apply(b2s_ctx* ctx, b2s_pc* pc, const double* r, double* z);
+b2s_status b2s_pc_apply_device(b2s_ctx* ctx, b2s_pc* pc, const double* d_r, double* d_z);
+/* Factor / hierarchy inspection (for parity tests).  what:
+ *   "ic0.L"  rp,ci,v of L incl. diagonal;   "ic0.diag"  diag (vals only)
+ *   "ilu0.L" strict L;  "ilu0.U" U incl. diagonal
+ *   "levels.L" / "levels.U": level of each row (ci holds levels, rp/v unused)
+ *   "ssor.colour": rp = color_ptr (ncolor+1), ci = new_id (n); v = diag2
+ *   "bilu0.L" / "bilu0.U" / "bilu0.inv": block factors (v = nnzb*bs*bs)
+ *   "amg.N.A", "amg.N.P": level N operator / prolongation; "amg.N.agg": aggregates in ci
+ * Query sizes with NULL arrays: sizes[0] = rows (+1 for rp), sizes[1] = nnz, sizes[2] = values. */
+b2s_status b2s_pc_export(b2s_ctx* ctx, b2s_pc* pc, const char* what, uint64_t* sizes, uint32_t* rp, uint32_t* ci,
+                         double* v);
+
+/* Maps a preconditioner name to a kind with the reference's alias tables:
+ * method B2S_PCG array.cpp:3482-3515, B2S_BICGSTAB 3637-3673, B2S_GMRES
+ * 4212-4242 (to_lower first); block GMRES blockMatrix.hpp:710-744 (exact
+ * match).  "amg" maps to B2S_PC_SA_AMG.  Unknown names: B2S_INVALID_ARG. */
+b2s_status b2s_pc_kind_from_name(int method, const char* name, b2s_pc_kind* kind);
+
+/* ----------------------------------------------------------------- solvers */
+
+typedef enum b2s_method
+{
+    B2S_PCG = 0,       /* SMatrix::pcg, array.cpp:3445-3601 */
+    B2S_BICGSTAB = 1,  /* SMatrix::bicgstab, array.cpp:3602-3842 */
+    B2S_GMRES = 2,     /* SMatrix::gmres, array.cpp:4190-4533; BlockMatrix::gmres */
+    B2S_FGMRES = 3,    /* flexible GMRES (Z stored), for variable / low-precision preconditioners */
+    B2S_BLOCK_GMRES = 4 /* name table of BlockMatrix::gmres for b2s_pc_kind_from_name only */
+} b2s_method;
+
+/* Gram-Schmidt variant for (F)GMRES. */
+typedef enum b2s_orth
+{
+    B2S_ORTH_MGS = 0, /* modified Gram-Schmidt, the reference's order */
+    B2S_ORTH_CGS2 = 1 /* classical Gram-Schmidt applied twice: two batched passes */
+} b2s_orth;
+
+typedef struct b2s_solve_opts
+{
+    double tol;      /* relative residual target (reference default 1e-10) */
+    int maxit;       /* reference default 2000 */
+    int restart;     /* GMRES restart length m */
+    int orth;        /* b2s_orth */
+    int ir_steps;    /* >0: iterative refinement sweeps around the solve (outer FP64 residual) */
+    double ir_inner_tol; /* relative tolerance of each refinement solve (0: 1e-4) */
+    int check_every; /* host polls convergence every this many iterations (0: auto) */
+    int use_graphs;  /* 1: replay iteration bodies as CUDA graphs */
+} b2s_solve_opts;
+
+void b2s_solve_opts_default(b2s_solve_opts* opts);
+
+typedef struct b2s_stats
+{
+    int it;               /* the reference's returned iteration count (its own convention) */
+    int iterations;       /* Krylov iterations executed (SpMVs in the loop) */
+    int spmvs;            /* operator applications incl. true-residual checks */
+    int pc_applies;       /* preconditioner applications */
+    int restarts;         /* GMRES restarts / refinement sweeps */
+    int status;           /* b2s_status of the solve */
+    double relres;        /* final recursive (or Givens) relative residual */
+    double relres_true;   /* ||b - A x|| / ||b|| recomputed in FP64 on exit */
+    double setup_ms;      /* preconditioner setup inside this call (0 when given one) */
+    double solve_ms;      /* iteration time, device events */
+} b2s_stats;
+
+/* Solves A x = b from x0 = 0.  pc may be NULL (identity).  Host pointers. */
+b2s_status b2s_solve(b2s_ctx* ctx, const b2s_csr* A, b2s_pc* pc, b2s_method method, const b2s_solve_opts* opts,
+                     const double* b, double* x, b2s_stats* stats);
+b2s_status b2s_solve_device(b2s_ctx* ctx, const b2s_csr* A, b2s_pc* pc, b2s_method method,
+                            const b2s_solve_opts* opts, const double* d_b, double* d_x, b2s_stats* stats);
+/* Same on a BAIJ operator (BlockMatrix::gmres; block PCG is an extension). */
+b2s_status b2s_solve_baij(b2s_ctx* ctx, const b2s_baij* A, b2s_pc* pc, b2s_method method, const b2s_solve_opts* opts,
+                          const double* b, double* x, b2s_stats* stats);
+b2s_status b2s_solve_baij_device(b2s_ctx* ctx, const b2s_baij* A, b2s_pc* pc, b2s_method method,
+                                 const b2s_solve_opts* opts, const double* d_b, double* d_x, b2s_stats* stats);
+
+/* ------------------------------------------------------------- generators
+ * Host-side problem generators for the benchmark configurations.  Two-step:
+ * call with NULL arrays to get n and nnz, then with arrays of that size.
+ * Output is CSR (sorted columns) or BAIJ. */
+
+/* 2-D 5-point Poisson on an N x N interior grid, Dirichlet by elimination
+ * (diagonal 4, off-diagonal -1; test_SMatrix_pcg.cpp:70-99). */
+b2s_status b2s_gen_poisson2d(uint32_t N, uint32_t* n, uint32_t* nnz, uint32_t* rp, uint32_t* ci, double* v);
+/* 3-D 7-point Poisson on N^3 (diagonal 6, off-diagonal -1). */
+b2s_status b2s_gen_poisson3d(uint32_t N, uint32_t* n, uint32_t* nnz, uint32_t* rp, uint32_t* ci, double* v);
+/* 3-D convection-diffusion, central diffusion + first-order upwind for a
+ * constant velocity (vx, vy, vz) >= 0: diagonal 6 + vx + vy + vz, upwind
+ * neighbours -1 - v_d, downwind -1. */
+b2s_status b2s_gen_convdiff3d(uint32_t N, double vx, double vy, double vz, uint32_t* n, uint32_t* nnz, uint32_t* rp,
+                              uint32_t* ci, double* v);
+/* Q1 hexahedral linear elasticity on an NE^3-element unit cube, E, nu,
+ * 2x2x2 Gauss quadrature, nodes on the x=0 face clamped (their block rows and
+ * columns eliminated).  BAIJ with bs=3, node-major. */
+b2s_status b2s_gen_elasticity_q1(uint32_t NE, double E, double nu, uint32_t* nbr, uint32_t* nnzb, uint32_t* rp,
+                                 uint32_t* ci, double* v);
+/* -div(k grad u) on an N x N grid, 5-point finite volume, harmonic-mean face
+ * coefficients, Dirichlet (zero) boundary; log k is a Gaussian random field
+ * with squared-exponential covariance (correlation length corr, variance var)
+ * sampled by FFT circulant embedding from `seed`.  kfield (N*N, optional)
+ * receives k. */
+b2s_status b2s_gen_grf_diffusion(uint32_t N, double corr, double var, uint64_t seed, uint32_t* n, uint32_t* nnz,
+                                 uint32_t* rp, uint32_t* ci, double* v, double* kfield);
+/* Uniform[-1,1] vector from a counter-based generator: element i is
+ * splitmix64(seed * 0x9E3779B97F4A7C15 + i) mapped to [-1, 1). */
+b2s_status b2s_gen_uniform(uint64_t seed, uint64_t n, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B2S_H */
