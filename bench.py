@@ -1,0 +1,356 @@
+"""Benchmark: time-to-tolerance of preconditioned CG on one B200.
+
+Workload (the configuration the headline metric is quoted on): -div(k grad u)
+= f on a 512 x 512 grid, 5-point finite volume, harmonic-mean face
+coefficients, log k a Gaussian random field (squared-exponential covariance,
+correlation length 0.05, variance uniform in [1, 4] drawn per seed), f
+uniform[-1, 1].  Systems are generated from held-out seeds (2000 + step on
+rank 0; ranks > 0 use their own seed range).  A step is one complete solve:
+preconditioner setup + PCG from x0 = 0 to relative residual 1e-8, verified by
+an FP64 true residual b - Ax.  Matrix generation and upload are outside the
+timed region; the right-hand side is already in HBM (`value`), or comes from
+pinned host memory together with the matrix (`e2e`).
+
+Arms
+  default            this library (C ABI, sm_100a kernels)
+  --impl reference   the reference library's own SMatrix::pcg(A, b, "ic")
+                     compiled from its sources (oracle/_ref/libref.so), on
+                     the host cores, same systems.
+
+Multi-GPU: the systems are independent, so N GPUs run N replicas on disjoint
+seeds ("scaling": "weak"); there is no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 512
+CORR = 0.05
+TOL = 1e-8
+MAXIT = 20000
+L2_FLUSH_BYTES = 512 << 20
+
+
+def load_b2s():
+    import __graft_entry__ as ge
+    return ge._load()
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{device}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            p = [s.strip() for s in line.split(",")]
+            if len(p) >= 9:
+                try:
+                    rows.append(p)
+                except Exception:
+                    pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def make_system(b2s, seed):
+    n, rp, ci, v = b2s.gen_grf_diffusion(N_GRID, seed, corr=CORR)
+    b = b2s.uniform(seed, n)
+    return n, rp, ci, v, b
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "of measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
+
+
+# ---------------------------------------------------------------- reference arm
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    b2s = load_b2s()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    try:
+        ref = oracle.Ref()
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference library not built: {e}"}))
+        return 0
+    cores = os.cpu_count() or 1
+    ref.set_threads(cores)
+    times, its = [], []
+    for k in range(args.warmup + args.steps):
+        n, rp, ci, v, b = make_system(b2s, 2000 + k)
+        A = ref.csr(n, n, rp, ci, v)
+        t0 = time.perf_counter()
+        x, it = ref.solve(A, 0, "ic", b, TOL, MAXIT)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt * 1e3)
+            its.append(it)
+    ms = float(np.mean(times))
+    line = {"metric": "time-to-rtol 1e-8 (PCG, 512^2 random-coefficient diffusion)", "value": ms, "unit": "ms",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded GRF diffusion, held-out seeds 2000+)", "impl": "reference",
+            "config": {"workload": "grf_diffusion_512 pcg rtol1e-8", "solver": "SMatrix::pcg(A,b,\"ic\")",
+                       "grid": N_GRID, "corr": CORR, "seeds": [2000 + args.warmup, 2000 + args.warmup + args.steps - 1]},
+            "iterations_mean": float(np.mean(its)),
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "reference",
+                             "sample": f"{args.steps} full solves (one system each)"},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b2s", choices=["b2s", "reference"])
+    ap.add_argument("--method", default="fp32_ic0", choices=["fp32_ic0", "fp64_ic0", "learned_ic0"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    rank, world, local = env_rank()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    b2s = load_b2s()
+    ctx = b2s.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    dev = torch.device("cuda", local)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    seeds = [2000 + rank * 100000 + k for k in range(args.warmup + args.steps)]
+    systems = [make_system(b2s, s) for s in seeds]
+
+    kinds = {"fp32_ic0": (b2s.PC_IC0, b2s.FP32), "fp64_ic0": (b2s.PC_IC0, b2s.FP64),
+             "learned_ic0": (b2s.PC_LEARNED_IC0, b2s.FP32)}
+
+    def timed_solve(n, rp, ci, v, b, method):
+        """Device-resident inputs; returns (ms, stats, relres_true)."""
+        A = b2s.CSR(ctx, n, n, rp, ci, v)
+        bt = torch.from_numpy(b).to(dev)
+        xt = torch.zeros(n, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        kind, prec = kinds[method]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.kernel_launches
+        e0.record(stream)
+        M = b2s.Precond(ctx, A, kind, precision=prec)
+        st = b2s.solve_device(ctx, A, bt.data_ptr(), xt.data_ptr(), b2s.PCG, M, tol=TOL, maxit=MAXIT)
+        e1.record(stream)
+        e1.synchronize()
+        launches = ctx.kernel_launches - l0
+        return e0.elapsed_time(e1), st, launches
+
+    def run(method, k_steps, warm):
+        ms, its, rel, launches = [], [], [], 0
+        for k in range(warm + k_steps):
+            n, rp, ci, v, b = systems[k % len(systems)]
+            t, st, nl = timed_solve(n, rp, ci, v, b, method)
+            if k >= warm:
+                ms.append(t)
+                its.append(st["iterations"])
+                rel.append(st["relres_true"])
+                launches += nl
+        return ms, its, rel, launches
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        head_ms, head_its, head_rel, launches = run(args.method, args.steps, args.warmup)
+    torch.cuda.synchronize()
+    clocks = clk.summary()
+    base_ms, base_its, base_rel, _ = run("fp64_ic0", args.steps, 1) if args.method != "fp64_ic0" else (
+        head_ms, head_its, head_rel, 0)
+
+    # e2e: host CSR + host b -> device, preconditioner, solve, x -> host (public C ABI, host pointers)
+    e2e_ms, h2d, d2h = [], 0, 0
+    kind, prec = kinds[args.method]
+    for k in range(args.steps):
+        n, rp, ci, v, b = systems[args.warmup + k]
+        torch.cuda.synchronize()
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        A = b2s.CSR(ctx, n, n, rp, ci, v)
+        M = b2s.Precond(ctx, A, kind, precision=prec)
+        x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=TOL, maxit=MAXIT)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        h2d = rp.nbytes + ci.nbytes + v.nbytes + b.nbytes
+        d2h = x.nbytes
+        del A, M
+
+    # roofline of the dominant kernel: the sync-free triangular solve of the
+    # preconditioner apply (forward L, backward L^T).  Algorithmic bytes of one
+    # triangle: factor values + column indices + row pointers + rhs + solution
+    # + diagonal, each read or written once.
+    n, rp, ci, v, b = systems[args.warmup]
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    M = b2s.Precond(ctx, A, kind, precision=prec)
+    r = torch.from_numpy(b).to(dev)
+    z = torch.empty_like(r)
+    nnz_l = (len(v) + n) // 2
+    vb = 4 if prec == b2s.FP32 else 8
+    tri_bytes = nnz_l * (vb + 4) + 4 * (n + 1) + 3 * vb * n
+    for _ in range(3):
+        b2s.lib().b2s_pc_apply_device(ctx.h, M.h, b2s.C.c_void_p(r.data_ptr()), b2s.C.c_void_p(z.data_ptr()))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 50
+    e0.record(stream)
+    for _ in range(reps):
+        b2s.lib().b2s_pc_apply_device(ctx.h, M.h, b2s.C.c_void_p(r.data_ptr()), b2s.C.c_void_p(z.data_ptr()))
+    e1.record(stream)
+    e1.synchronize()
+    tri_ms = e0.elapsed_time(e1) / reps / 2
+    pk, pk_kind = peaks()
+    achieved = tri_bytes / (tri_ms * 1e-3) / 1e9
+    roofline = {"kernel": "k_syncfree<TrsvOp> (IC(0) triangular solve)", "bound": "hbm",
+                "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+                "peak_kind": pk_kind, "traffic": None, "bytes_per_launch": tri_bytes, "ms_per_launch": tri_ms,
+                "note": "latency-bound: 1023 dependency levels per triangle on the 512^2 grid"}
+
+    # C2 (3-D Poisson 128^3) CSR SpMV against the HBM roofline (inputs > L2)
+    n3, rp3, ci3, v3 = b2s.gen_poisson3d(128)
+    A3 = b2s.CSR(ctx, n3, n3, rp3, ci3, v3)
+    x3 = torch.rand(n3, dtype=torch.float64, device=dev)
+    y3 = torch.empty_like(x3)
+    for _ in range(3):
+        A3.spmv_device(x3.data_ptr(), y3.data_ptr())
+    e0.record(stream)
+    for _ in range(20):
+        A3.spmv_device(x3.data_ptr(), y3.data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    spmv_ms = e0.elapsed_time(e1) / 20
+    spmv_bytes = 12 * len(v3) + 4 * (n3 + 1) + 16 * n3
+    spmv_gbs = spmv_bytes / (spmv_ms * 1e-3) / 1e9
+    spmv = {"kernel": "k_spmv_staged", "workload": "poisson3d_128 (n=2097152, nnz=14581760)",
+            "ms": spmv_ms, "achieved": spmv_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": spmv_gbs / pk["hbm_gbs"], "bytes_per_launch": spmv_bytes}
+
+    value = float(np.mean(head_ms))
+    if world > 1:
+        t = torch.tensor([value], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        value = float(t.item())
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle
+            ref = oracle.Ref()
+            cores = os.cpu_count() or 1
+            ref.set_threads(cores)
+            n, rp, ci, v, b = systems[args.warmup]
+            Ar = ref.csr(n, n, rp, ci, v)
+            t0 = time.perf_counter()
+            xr, itr = ref.solve(Ar, 0, "ic", b, TOL, MAXIT)
+            cms = (time.perf_counter() - t0) * 1e3
+            cpu = {"value": cms, "unit": "ms", "cores": cores, "kind": "reference", "iterations": itr,
+                   "sample": f"one full SMatrix::pcg(A,b,\"ic\") solve of seed {seeds[args.warmup]}"}
+        except Exception as e:
+            cpu = {"value": None, "unit": "ms", "cores": 0, "kind": "reference", "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": "time-to-rtol 1e-8 (PCG, 512^2 random-coefficient diffusion)",
+            "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 outer / f32 preconditioner" if prec == b2s.FP32 else "f64",
+            "data": "synthetic (seeded GRF diffusion, held-out seeds 2000+)",
+            "config": {"workload": "grf_diffusion_512 pcg rtol1e-8", "method": args.method, "grid": N_GRID,
+                       "corr": CORR, "parallelism": f"replicas x{world}", "l2": "flushed (512 MB write) before every step"},
+            "iterations_mean": float(np.mean(head_its)), "relres_true_max": float(np.max(head_rel)),
+            "fp64_ic0_pcg": {"ms": float(np.mean(base_ms)), "iterations_mean": float(np.mean(base_its)),
+                             "relres_true_max": float(np.max(base_rel))},
+            "speedup_vs_fp64_ic0": float(np.mean(base_ms)) / value,
+            "e2e": {"value": float(np.mean(e2e_ms)), "unit": "ms", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "spmv_c2": spmv,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,899 @@
+// Smoothed-aggregation AMG on BAIJ operators (make_block_amg_preconditioner,
+// blockMatrix.hpp:1051-1179; V-cycle blk_amg_vcycle, 946-1046).  The scalar
+// "amg" preconditioner runs the same code on the BS = 1 condensed matrix, as
+// test_BlockMatrix_schur3d.cpp:143-146 does with the reference.
+//
+// Setup, per level, all on the device:
+//   diag_inv   Gauss-Jordan inverse of each diagonal block (a failed inverse
+//              leaves zeros; the reference ignores the failure too)
+//   strength   off-diagonal blocks with Frobenius norm >= 0.25 * row maximum
+//   aggregates the reference's greedy rule -- rows in natural order, a row not
+//              yet aggregated opens an aggregate and pulls in up to 3 of its
+//              unaggregated strong neighbours in list order.  The rule is
+//              sequential by definition; one thread walks it with the strong
+//              lists streamed from HBM, which makes the aggregates identical
+//              to the reference's.
+//   P          (I - 2/3 D^-1 A) P_tent, one thread per row, blocks accumulated
+//              in the reference's order and emitted with ascending aggregate
+//   R = P^T    block transpose (rows sorted afterwards)
+//   A_c        R (A P): two-phase block SpGEMM -- candidate columns, segmented
+//              sort + unique for the pattern, then each output block summed in
+//              the reference's (pa, pb) order: bit-equal Galerkin operators
+//   coarsest   at most 50 block rows: dense elimination on one CTA, either the
+//              reference's own (amg_ref_coarse = 1: rows swapped in the matrix
+//              only, the V-cycle solve then repeats blockMatrix.hpp:958-1000
+//              exactly) or a correct partial-pivot LU (default).
+// Apply: one V(1,1) cycle with 2/3-damped block Jacobi; the pre-smoothing
+// step starts from zero so its residual is the right-hand side itself.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+
+#include "block_ops.cuh"
+#include "trisolve.cuh"
+
+namespace b2s {
+
+namespace {
+
+constexpr double kTheta = 0.25, kOmega = 2.0 / 3.0;
+
+// ------------------------------------------------------------ BAIJ helpers
+
+__global__ void k_find_diag(uint32_t nb, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                            uint32_t* __restrict__ dptr)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+    {
+        uint32_t d = 0xFFFFFFFFu;
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+            if (ci[p] == i)
+            {
+                d = p;
+                break;
+            }
+        dptr[i] = d;
+    }
+}
+
+// finalise a device-built BAIJ (diag pointers, staged-matvec partition)
+void finish_baij(b2s_ctx* ctx, BaijDev& M)
+{
+    M.diag_ptr.alloc(M.nbr ? M.nbr : 1);
+    if (M.nbr)
+        B2S_LAUNCH(ctx, k_find_diag, stream_grid(ctx, M.nbr), kThreads, 0, M.nbr, M.rp.p, M.ci.p, M.diag_ptr.p);
+    M.h_rp.resize(M.nbr + 1);
+    d2h(ctx, M.h_rp.data(), M.rp.p, (M.nbr + 1) * sizeof(uint32_t));
+    sync(ctx);
+    M.nnzb = M.h_rp[M.nbr];
+    const uint32_t cap = M.bs == 1 ? 3072 : M.bs == 2 ? 1024 : M.bs == 3 ? 512 : 256;
+    std::vector<uint32_t> blk;
+    build_row_blocks(M.h_rp.data(), M.nbr, 1, (uint32_t)(kThreads / M.bs), cap, blk);
+    M.nblk = (uint32_t)blk.size() - 1;
+    M.blk_row = upload(ctx, blk.data(), blk.size());
+}
+
+template <int BS>
+__global__ void k_diag_inv(uint32_t nb, const double* __restrict__ v, const uint32_t* __restrict__ dptr,
+                           double* __restrict__ dinv)
+{
+    constexpr int BV = BS * BS;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+    {
+        double M[BV], Mi[BV];
+        for (int k = 0; k < BV; ++k) Mi[k] = 0.0;
+        if (dptr[i] != 0xFFFFFFFFu)
+        {
+            for (int k = 0; k < BV; ++k) M[k] = v[(size_t)dptr[i] * BV + k];
+            double T[BV];
+            if (blk_inv<BS>(M, T))
+                for (int k = 0; k < BV; ++k) Mi[k] = T[k];
+        }
+        for (int k = 0; k < BV; ++k) dinv[(size_t)i * BV + k] = Mi[k];
+    }
+}
+
+// ------------------------------------------------------------ strength
+
+template <int BS>
+__device__ __forceinline__ double fro(const double* b)
+{
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < BS * BS; ++k) s += b[k] * b[k];
+    return sqrt(s);
+}
+
+template <int BS>
+__global__ void k_strength(uint32_t nb, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                           const double* __restrict__ v, const uint32_t* __restrict__ sp, uint32_t* __restrict__ cnt,
+                           uint32_t* __restrict__ sc)
+{
+    constexpr int BV = BS * BS;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+    {
+        double mx = 0.0;
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+            if (ci[p] != i)
+            {
+                const double f = fro<BS>(&v[(size_t)p * BV]);
+                mx = mx < f ? f : mx;
+            }
+        const double thr = kTheta * mx;
+        uint32_t c = 0, w = sp ? sp[i] : 0;
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+            if (ci[p] != i && fro<BS>(&v[(size_t)p * BV]) >= thr)
+            {
+                if (sc) sc[w++] = ci[p];
+                ++c;
+            }
+        if (cnt) cnt[i] = c;
+    }
+    if (cnt && blockIdx.x == 0 && threadIdx.x == 0) cnt[nb] = 0;
+}
+
+// ------------------------------------------------------------ aggregation
+
+// The greedy rule of blockMatrix.hpp:1101-1111, walked by one thread.
+__global__ void k_aggregate(uint32_t nb, const uint32_t* __restrict__ sp, const uint32_t* __restrict__ sc,
+                            int32_t* __restrict__ agg, uint32_t* __restrict__ nagg_out)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int32_t nagg = 0;
+    for (uint32_t i = 0; i < nb; ++i)
+    {
+        if (agg[i] != -1) continue;
+        agg[i] = nagg;
+        int sz = 1;
+        const uint32_t a = __ldg(&sp[i]), b = __ldg(&sp[i + 1]);
+        for (uint32_t p = a; p < b && sz < 4; ++p)
+        {
+            const uint32_t j = __ldg(&sc[p]);
+            if (agg[j] == -1)
+            {
+                agg[j] = nagg;
+                ++sz;
+            }
+        }
+        ++nagg;
+    }
+    *nagg_out = (uint32_t)nagg;
+}
+
+// ------------------------------------------------------------ prolongation
+
+// distinct aggregates among {agg[i]} U {agg[k] : k in row i}, ascending
+__device__ __forceinline__ uint32_t p_row_cols(uint32_t i, const uint32_t* rp, const uint32_t* ci, const int32_t* agg,
+                                               uint32_t* out)
+{
+    // count distinct; write ascending when out != null
+    uint32_t cnt = 0;
+    int32_t last = -1;
+    for (;;)
+    {
+        // smallest candidate greater than `last`
+        int32_t best = 0x7fffffff;
+        const int32_t gi = agg[i];
+        if (gi > last && gi < best) best = gi;
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+        {
+            const int32_t g = agg[ci[p]];
+            if (g > last && g < best) best = g;
+        }
+        if (best == 0x7fffffff) break;
+        if (out) out[cnt] = (uint32_t)best;
+        ++cnt;
+        last = best;
+    }
+    return cnt;
+}
+
+__global__ void k_p_count(uint32_t nb, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                          const int32_t* __restrict__ agg, uint32_t* __restrict__ cnt)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+        cnt[i] = p_row_cols(i, rp, ci, agg, nullptr);
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt[nb] = 0;
+}
+
+template <int BS>
+__global__ void k_p_fill(uint32_t nb, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                         const double* __restrict__ v, const double* __restrict__ dinv, const int32_t* __restrict__ agg,
+                         const uint32_t* __restrict__ prp, uint32_t* __restrict__ pci, double* __restrict__ pv)
+{
+    constexpr int BV = BS * BS;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+    {
+        const uint32_t base = prp[i];
+        const uint32_t cnt = p_row_cols(i, rp, ci, agg, pci + base);
+        for (uint32_t s = 0; s < cnt; ++s)
+            for (int k = 0; k < BV; ++k) pv[(size_t)(base + s) * BV + k] = 0.0;
+        auto slot = [&](uint32_t g) {
+            uint32_t lo = 0, hi = cnt;
+            while (lo < hi)
+            {
+                const uint32_t mid = (lo + hi) / 2;
+                if (pci[base + mid] < g)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            return base + lo;
+        };
+        {
+            double* I = &pv[(size_t)slot((uint32_t)agg[i]) * BV];
+            for (int r = 0; r < BS; ++r) I[r * BS + r] = 1.0;
+        }
+        const double* Di = &dinv[(size_t)i * BV];
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+        {
+            const double* ab = &v[(size_t)p * BV];
+            double* dst = &pv[(size_t)slot((uint32_t)agg[ci[p]]) * BV];
+            for (int r = 0; r < BS; ++r)
+                for (int c = 0; c < BS; ++c)
+                {
+                    double s = 0.0;
+                    for (int m = 0; m < BS; ++m) s += Di[r * BS + m] * ab[m * BS + c];
+                    dst[r * BS + c] -= kOmega * s;
+                }
+        }
+    }
+}
+
+// ------------------------------------------------------------ block transpose
+
+__global__ void k_bt_count(uint32_t nb, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                           uint32_t* __restrict__ cnt)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p) atomicAdd(&cnt[ci[p]], 1u);
+}
+
+template <int BS>
+__global__ void k_bt_fill(uint32_t nb, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                          const double* __restrict__ v, const uint32_t* __restrict__ trp, uint32_t* __restrict__ off,
+                          uint32_t* __restrict__ tci, double* __restrict__ tv)
+{
+    constexpr int BV = BS * BS;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+        {
+            const uint32_t j = ci[p];
+            const uint32_t d = trp[j] + atomicAdd(&off[j], 1u);
+            tci[d] = i;
+            for (int r = 0; r < BS; ++r)
+                for (int c = 0; c < BS; ++c) tv[(size_t)d * BV + r * BS + c] = v[(size_t)p * BV + c * BS + r];
+        }
+}
+
+template <int BS>
+__global__ void k_bt_sort(uint32_t nr, const uint32_t* __restrict__ rp, uint32_t* __restrict__ ci, double* __restrict__ v)
+{
+    constexpr int BV = BS * BS;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += gridDim.x * blockDim.x)
+    {
+        const uint32_t a = rp[i], b = rp[i + 1];
+        for (uint32_t p = a + 1; p < b; ++p)
+        {
+            const uint32_t c = ci[p];
+            double x[BV];
+            for (int k = 0; k < BV; ++k) x[k] = v[(size_t)p * BV + k];
+            uint32_t q = p;
+            while (q > a && ci[q - 1] > c)
+            {
+                ci[q] = ci[q - 1];
+                for (int k = 0; k < BV; ++k) v[(size_t)q * BV + k] = v[(size_t)(q - 1) * BV + k];
+                --q;
+            }
+            ci[q] = c;
+            for (int k = 0; k < BV; ++k) v[(size_t)q * BV + k] = x[k];
+        }
+    }
+}
+
+template <int BS>
+void block_transpose(b2s_ctx* ctx, const BaijDev& A, BaijDev& T)
+{
+    constexpr int BV = BS * BS;
+    T.bs = BS;
+    T.nbr = A.nbc;
+    T.nbc = A.nbr;
+    DBuf<uint32_t> cnt(T.nbr + 1);
+    B2S_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes(), ctx->stream));
+    if (A.nbr) B2S_LAUNCH(ctx, k_bt_count, stream_grid(ctx, A.nbr), kThreads, 0, A.nbr, A.rp.p, A.ci.p, cnt.p);
+    T.rp.alloc(T.nbr + 1);
+    const uint32_t nnz = exclusive_scan(ctx, cnt.p, T.rp.p, T.nbr);
+    T.ci.alloc(nnz ? nnz : 1);
+    T.v.alloc(nnz ? (size_t)nnz * BV : 1);
+    B2S_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes(), ctx->stream));
+    if (A.nbr)
+        B2S_LAUNCH(ctx, k_bt_fill<BS>, stream_grid(ctx, A.nbr), kThreads, 0, A.nbr, A.rp.p, A.ci.p, A.v.p, T.rp.p,
+                   cnt.p, T.ci.p, T.v.p);
+    if (T.nbr) B2S_LAUNCH(ctx, k_bt_sort<BS>, stream_grid(ctx, T.nbr), kThreads, 0, T.nbr, T.rp.p, T.ci.p, T.v.p);
+    finish_baij(ctx, T);
+}
+
+// ------------------------------------------------------------ block SpGEMM
+
+__global__ void k_mm_ub(uint32_t nr, const uint32_t* __restrict__ arp, const uint32_t* __restrict__ aci,
+                        const uint32_t* __restrict__ brp, uint32_t* __restrict__ cnt)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += gridDim.x * blockDim.x)
+    {
+        uint32_t c = 0;
+        for (uint32_t p = arp[i]; p < arp[i + 1]; ++p) c += brp[aci[p] + 1] - brp[aci[p]];
+        cnt[i] = c;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt[nr] = 0;
+}
+
+__global__ void k_mm_cand(uint32_t nr, const uint32_t* __restrict__ arp, const uint32_t* __restrict__ aci,
+                          const uint32_t* __restrict__ brp, const uint32_t* __restrict__ bci,
+                          const uint32_t* __restrict__ off, uint32_t* __restrict__ cand)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += gridDim.x * blockDim.x)
+    {
+        uint32_t w = off[i];
+        for (uint32_t p = arp[i]; p < arp[i + 1]; ++p)
+            for (uint32_t q = brp[aci[p]]; q < brp[aci[p] + 1]; ++q) cand[w++] = bci[q];
+    }
+}
+
+__global__ void k_mm_unique_count(uint32_t nr, const uint32_t* __restrict__ off, const uint32_t* __restrict__ cand,
+                                  uint32_t* __restrict__ cnt)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += gridDim.x * blockDim.x)
+    {
+        uint32_t c = 0;
+        for (uint32_t k = off[i]; k < off[i + 1]; ++k) c += (k == off[i] || cand[k] != cand[k - 1]);
+        cnt[i] = c;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt[nr] = 0;
+}
+
+__global__ void k_mm_unique_fill(uint32_t nr, const uint32_t* __restrict__ off, const uint32_t* __restrict__ cand,
+                                 const uint32_t* __restrict__ crp, uint32_t* __restrict__ cci)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += gridDim.x * blockDim.x)
+    {
+        uint32_t w = crp[i];
+        for (uint32_t k = off[i]; k < off[i + 1]; ++k)
+            if (k == off[i] || cand[k] != cand[k - 1]) cci[w++] = cand[k];
+    }
+}
+
+// C row i: every (pa, pb) product added into its column's block in the
+// reference's order (blk_matmul, blockMatrix.hpp:883-932)
+template <int BS>
+__global__ void k_mm_numeric(uint32_t nr, const uint32_t* __restrict__ arp, const uint32_t* __restrict__ aci,
+                             const double* __restrict__ av, const uint32_t* __restrict__ brp,
+                             const uint32_t* __restrict__ bci, const double* __restrict__ bv,
+                             const uint32_t* __restrict__ crp, const uint32_t* __restrict__ cci, double* __restrict__ cv)
+{
+    constexpr int BV = BS * BS;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += gridDim.x * blockDim.x)
+    {
+        const uint32_t c0 = crp[i], c1 = crp[i + 1];
+        for (uint32_t s = c0; s < c1; ++s)
+            for (int k = 0; k < BV; ++k) cv[(size_t)s * BV + k] = 0.0;
+        for (uint32_t pa = arp[i]; pa < arp[i + 1]; ++pa)
+        {
+            const uint32_t k = aci[pa];
+            const double* ab = &av[(size_t)pa * BV];
+            for (uint32_t pb = brp[k]; pb < brp[k + 1]; ++pb)
+            {
+                const uint32_t j = bci[pb];
+                uint32_t lo = c0, hi = c1;
+                while (lo < hi)
+                {
+                    const uint32_t mid = (lo + hi) / 2;
+                    if (cci[mid] < j)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                const double* bb = &bv[(size_t)pb * BV];
+                double* cb = &cv[(size_t)lo * BV];
+                for (int r = 0; r < BS; ++r)
+                    for (int c = 0; c < BS; ++c)
+                    {
+                        double s = 0.0;
+                        for (int m = 0; m < BS; ++m) s += ab[r * BS + m] * bb[m * BS + c];
+                        cb[r * BS + c] += s;
+                    }
+            }
+        }
+    }
+}
+
+template <int BS>
+void block_matmul(b2s_ctx* ctx, const BaijDev& A, const BaijDev& B, BaijDev& C)
+{
+    constexpr int BV = BS * BS;
+    const uint32_t nr = A.nbr;
+    C.bs = BS;
+    C.nbr = nr;
+    C.nbc = B.nbc;
+    DBuf<uint32_t> cnt(nr + 1), off(nr + 1);
+    if (nr) B2S_LAUNCH(ctx, k_mm_ub, stream_grid(ctx, nr), kThreads, 0, nr, A.rp.p, A.ci.p, B.rp.p, cnt.p);
+    const uint32_t total = exclusive_scan(ctx, cnt.p, off.p, nr);
+    DBuf<uint32_t> cand(total ? total : 1), sorted(total ? total : 1);
+    if (nr) B2S_LAUNCH(ctx, k_mm_cand, stream_grid(ctx, nr), kThreads, 0, nr, A.rp.p, A.ci.p, B.rp.p, B.ci.p, off.p, cand.p);
+    if (total)
+    {
+        size_t bytes = 0;
+        B2S_CUDA(cub::DeviceSegmentedSort::SortKeys(nullptr, bytes, cand.p, sorted.p, (int64_t)total, (int64_t)nr, off.p,
+                                                    off.p + 1, ctx->stream));
+        DBuf<uint8_t> tmp(bytes ? bytes : 1);
+        B2S_CUDA(cub::DeviceSegmentedSort::SortKeys(tmp.p, bytes, cand.p, sorted.p, (int64_t)total, (int64_t)nr, off.p,
+                                                    off.p + 1, ctx->stream));
+        ctx->launches += 1;
+    }
+    if (nr) B2S_LAUNCH(ctx, k_mm_unique_count, stream_grid(ctx, nr), kThreads, 0, nr, off.p, sorted.p, cnt.p);
+    C.rp.alloc(nr + 1);
+    const uint32_t nnz = exclusive_scan(ctx, cnt.p, C.rp.p, nr);
+    C.ci.alloc(nnz ? nnz : 1);
+    C.v.alloc(nnz ? (size_t)nnz * BV : 1);
+    if (nr)
+    {
+        B2S_LAUNCH(ctx, k_mm_unique_fill, stream_grid(ctx, nr), kThreads, 0, nr, off.p, sorted.p, C.rp.p, C.ci.p);
+        B2S_LAUNCH(ctx, k_mm_numeric<BS>, stream_grid(ctx, nr), kThreads, 0, nr, A.rp.p, A.ci.p, A.v.p, B.rp.p, B.ci.p,
+                   B.v.p, C.rp.p, C.ci.p, C.v.p);
+    }
+    finish_baij(ctx, C);
+}
+
+// ------------------------------------------------------------ coarsest level
+
+template <int BS>
+__global__ void k_dense_from_baij(uint32_t nb, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                                  const double* __restrict__ v, double* __restrict__ D, int sz)
+{
+    constexpr int BV = BS * BS;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+            for (int r = 0; r < BS; ++r)
+                for (int c = 0; c < BS; ++c)
+                    D[(size_t)(i * BS + r) * sz + ci[p] * BS + c] = v[(size_t)p * BV + r * BS + c];
+}
+
+// One CTA.  ref == 1: the reference's elimination (blockMatrix.hpp:962-981):
+// rows swapped, pivot clamped to +-1e-14, the multiplier column eliminated
+// along with the row (j from k).  ref == 0: LU with partial pivoting,
+// multipliers stored below the diagonal and the permutation kept in piv.
+__global__ void k_dense_factor(double* D, int sz, int ref, int* piv)
+{
+    __shared__ int s_pk;
+    __shared__ double s_red[kThreads];
+    __shared__ int s_idx[kThreads];
+    for (int i = threadIdx.x; i < sz; i += blockDim.x) piv[i] = i;
+    __syncthreads();
+    for (int k = 0; k < sz; ++k)
+    {
+        // first row with the largest |D[i][k]|, i >= k (strict > keeps the earliest)
+        double best = -1.0;
+        int bi = k;
+        for (int i = k + threadIdx.x; i < sz; i += blockDim.x)
+        {
+            const double a = fabs(D[(size_t)i * sz + k]);
+            if (a > best)
+            {
+                best = a;
+                bi = i;
+            }
+        }
+        s_red[threadIdx.x] = best;
+        s_idx[threadIdx.x] = bi;
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            // the earliest row attaining the maximum, as the sequential scan finds it
+            double b = -1.0;
+            int pk = k;
+            for (int t = 0; t < (int)blockDim.x; ++t)
+                if (s_red[t] > b || (s_red[t] == b && s_idx[t] < pk))
+                {
+                    b = s_red[t];
+                    pk = s_idx[t];
+                }
+            s_pk = pk;
+        }
+        __syncthreads();
+        const int pk = s_pk;
+        if (pk != k)
+        {
+            for (int j = threadIdx.x; j < sz; j += blockDim.x)
+            {
+                const double t = D[(size_t)k * sz + j];
+                D[(size_t)k * sz + j] = D[(size_t)pk * sz + j];
+                D[(size_t)pk * sz + j] = t;
+            }
+            if (threadIdx.x == 0 && !ref)
+            {
+                const int t = piv[k];
+                piv[k] = piv[pk];
+                piv[pk] = t;
+            }
+        }
+        __syncthreads();
+        double d = D[(size_t)k * sz + k];
+        if (ref)
+        {
+            if (fabs(d) < 1e-14) d = (d >= 0 ? 1e-14 : -1e-14);
+        }
+        else if (fabs(d) < 1e-300)
+        {
+            d = 1e-300;
+            if (threadIdx.x == 0) D[(size_t)k * sz + k] = d;
+        }
+        for (int i = k + 1 + threadIdx.x; i < sz; i += blockDim.x)
+        {
+            const double f = D[(size_t)i * sz + k] / d;
+            if (ref)
+                for (int j = k; j < sz; ++j) D[(size_t)i * sz + j] -= f * D[(size_t)k * sz + j];
+            else
+            {
+                D[(size_t)i * sz + k] = f;
+                for (int j = k + 1; j < sz; ++j) D[(size_t)i * sz + j] -= f * D[(size_t)k * sz + j];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// coarsest solve, one thread (the row sums are sequential in the reference)
+__global__ void k_dense_solve(const double* __restrict__ D, int sz, int ref, const int* __restrict__ piv,
+                              const double* __restrict__ rhs, double* __restrict__ x, const int* done)
+{
+    if (done && *done) return;
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (ref)
+    {
+        for (int i = 0; i < sz; ++i) x[i] = rhs[i];
+        for (int k = 0; k < sz; ++k)
+        {
+            double d = D[(size_t)k * sz + k];
+            if (fabs(d) < 1e-14) d = (d >= 0 ? 1e-14 : -1e-14);
+            for (int i = k + 1; i < sz; ++i) x[i] -= (D[(size_t)i * sz + k] / d) * x[k];
+        }
+        for (int i = sz - 1; i >= 0; --i)
+        {
+            for (int j = i + 1; j < sz; ++j) x[i] -= D[(size_t)i * sz + j] * x[j];
+            double d = D[(size_t)i * sz + i];
+            if (fabs(d) < 1e-14) d = (d >= 0 ? 1e-14 : -1e-14);
+            x[i] /= d;
+        }
+    }
+    else
+    {
+        for (int i = 0; i < sz; ++i) x[i] = rhs[piv[i]];
+        for (int i = 0; i < sz; ++i)
+            for (int j = 0; j < i; ++j) x[i] -= D[(size_t)i * sz + j] * x[j];
+        for (int i = sz - 1; i >= 0; --i)
+        {
+            for (int j = i + 1; j < sz; ++j) x[i] -= D[(size_t)i * sz + j] * x[j];
+            x[i] /= D[(size_t)i * sz + i];
+        }
+    }
+}
+
+// ------------------------------------------------------------ V-cycle kernels
+
+// pre-smoothing from zero: sol = omega * dinv * rhs   (A*0 = 0, so r = rhs)
+template <int BS, typename T>
+__global__ void k_smooth0(uint32_t nb, const T* __restrict__ dinv, const double* __restrict__ rhs,
+                          double* __restrict__ sol, const int* done)
+{
+    if (done && *done) return;
+    constexpr int BV = BS * BS;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+        for (int c = 0; c < BS; ++c)
+        {
+            double corr = 0.0;
+            for (int rr = 0; rr < BS; ++rr) corr += (double)dinv[(size_t)i * BV + c * BS + rr] * rhs[(size_t)i * BS + rr];
+            sol[(size_t)i * BS + c] = 0.0 + kOmega * corr;
+        }
+}
+
+// sol += omega * dinv * (rhs - Asol)
+template <int BS, typename T>
+__global__ void k_jacobi(uint32_t nb, const T* __restrict__ dinv, const double* __restrict__ rhs,
+                         const double* __restrict__ Asol, double* __restrict__ sol, const int* done)
+{
+    if (done && *done) return;
+    constexpr int BV = BS * BS;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+    {
+        double r[BS];
+        for (int c = 0; c < BS; ++c) r[c] = rhs[(size_t)i * BS + c] - Asol[(size_t)i * BS + c];
+        for (int c = 0; c < BS; ++c)
+        {
+            double corr = 0.0;
+            for (int rr = 0; rr < BS; ++rr) corr += (double)dinv[(size_t)i * BV + c * BS + rr] * r[rr];
+            sol[(size_t)i * BS + c] += kOmega * corr;
+        }
+    }
+}
+
+__global__ void k_sub(uint64_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ r,
+                      const int* done)
+{
+    if (done && *done) return;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        r[i] = a[i] - b[i];
+}
+
+__global__ void k_add(uint64_t n, const double* __restrict__ a, double* __restrict__ x, const int* done)
+{
+    if (done && *done) return;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        x[i] += a[i];
+}
+
+__global__ void k_zero(uint64_t n, double* __restrict__ x, const int* done)
+{
+    if (done && *done) return;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        x[i] = 0.0;
+}
+
+// ------------------------------------------------------------ hierarchy
+
+struct Level
+{
+    std::unique_ptr<BaijDev> own;  // operator (null on level 0 when borrowed)
+    const BaijDev* A = nullptr;
+    BaijDev P, R;
+    DBuf<double> dinv;
+    DBuf<int32_t> agg;
+    uint32_t nrows = 0;
+    bool has_p = false;
+    DBuf<double> tmp, r, rc, ec, sol;  // V-cycle work (rc / ec sized for the next level)
+};
+
+struct PcAMG final : PcImpl
+{
+    int bs = 1;
+    bool ref_coarse = false;
+    std::vector<std::unique_ptr<Level>> lv;
+    std::unique_ptr<BaijDev> fine_copy;  // BS=1 copy of a CSR operator
+    DBuf<double> dense;
+    DBuf<int> piv;
+    int sz = 0;
+
+    template <int BS>
+    void vcycle(b2s_ctx* ctx, int l, const double* rhs, double* sol, const int* done)
+    {
+        Level& L = *lv[l];
+        const uint64_t ndof = (uint64_t)L.nrows * BS;
+        const unsigned g = stream_grid(ctx, L.nrows), gd = stream_grid(ctx, ndof);
+        if (l == (int)lv.size() - 1)
+        {
+            B2S_LAUNCH(ctx, k_dense_solve, 1, 32, 0, dense.p, sz, ref_coarse ? 1 : 0, piv.p, rhs, sol, done);
+            return;
+        }
+        B2S_LAUNCH(ctx, (k_smooth0<BS, double>), g, kThreads, 0, L.nrows, L.dinv.p, rhs, sol, done);
+        baij_matvec(ctx, *L.A, sol, L.tmp.p, done);
+        B2S_LAUNCH(ctx, k_sub, gd, kThreads, 0, ndof, rhs, L.tmp.p, L.r.p, done);
+        baij_matvec(ctx, L.R, L.r.p, L.rc.p, done);
+        const uint64_t nc = (uint64_t)L.R.nbr * BS;
+        if (l + 1 < (int)lv.size() - 1)
+            vcycle<BS>(ctx, l + 1, L.rc.p, L.ec.p, done);
+        else
+        {
+            B2S_LAUNCH(ctx, k_zero, stream_grid(ctx, nc), kThreads, 0, nc, L.ec.p, done);
+            vcycle<BS>(ctx, l + 1, L.rc.p, L.ec.p, done);
+        }
+        baij_matvec(ctx, L.P, L.ec.p, L.tmp.p, done);
+        B2S_LAUNCH(ctx, k_add, gd, kThreads, 0, ndof, L.tmp.p, sol, done);
+        baij_matvec(ctx, *L.A, sol, L.tmp.p, done);
+        B2S_LAUNCH(ctx, (k_jacobi<BS, double>), g, kThreads, 0, L.nrows, L.dinv.p, rhs, L.tmp.p, sol, done);
+    }
+
+    void apply(b2s_ctx* ctx, const double* r, double* z, const int* done) override
+    {
+        switch (bs)
+        {
+            case 1: vcycle<1>(ctx, 0, r, z, done); break;
+            case 2: vcycle<2>(ctx, 0, r, z, done); break;
+            case 3: vcycle<3>(ctx, 0, r, z, done); break;
+            case 4: vcycle<4>(ctx, 0, r, z, done); break;
+        }
+    }
+
+    void export_baij(b2s_ctx* ctx, const BaijDev& M, uint64_t* sizes, uint32_t* rp, uint32_t* ci, double* v)
+    {
+        const size_t bv = (size_t)M.bs * M.bs;
+        sizes[0] = (uint64_t)M.nbr + 1;
+        sizes[1] = M.nnzb;
+        sizes[2] = (uint64_t)M.nnzb * bv;
+        if (rp) d2h(ctx, rp, M.rp.p, (M.nbr + 1) * sizeof(uint32_t));
+        if (ci) d2h(ctx, ci, M.ci.p, M.nnzb * sizeof(uint32_t));
+        if (v) d2h(ctx, v, M.v.p, M.nnzb * bv * sizeof(double));
+        sync(ctx);
+    }
+
+    void export_data(b2s_ctx* ctx, const std::string& what, uint64_t* sizes, uint32_t* rp, uint32_t* ci,
+                     double* v) override
+    {
+        if (what == "amg.levels")
+        {
+            sizes[0] = 0;
+            sizes[1] = lv.size();
+            sizes[2] = 0;
+            if (ci)
+                for (size_t k = 0; k < lv.size(); ++k) ci[k] = lv[k]->nrows;
+            return;
+        }
+        unsigned l = 0;
+        char tail[32] = {0};
+        if (std::sscanf(what.c_str(), "amg.%u.%31s", &l, tail) == 2 && l < lv.size())
+        {
+            Level& L = *lv[l];
+            const std::string t(tail);
+            if (t == "A") return export_baij(ctx, *L.A, sizes, rp, ci, v);
+            if (t == "P" && L.has_p) return export_baij(ctx, L.P, sizes, rp, ci, v);
+            if (t == "dinv")
+            {
+                sizes[0] = 0;
+                sizes[1] = 0;
+                sizes[2] = (uint64_t)L.nrows * bs * bs;
+                if (v) d2h(ctx, v, L.dinv.p, sizes[2] * sizeof(double));
+                sync(ctx);
+                return;
+            }
+            if (t == "agg" && L.has_p)
+            {
+                sizes[0] = 0;
+                sizes[1] = L.nrows;
+                sizes[2] = 0;
+                if (ci) d2h(ctx, ci, L.agg.p, L.nrows * sizeof(uint32_t));
+                sync(ctx);
+                return;
+            }
+        }
+        PcImpl::export_data(ctx, what, sizes, rp, ci, v);
+    }
+};
+
+template <int BS>
+void build_hierarchy(b2s_ctx* ctx, PcAMG& pc, const BaijDev& A0, int max_levels, uint32_t coarse_max)
+{
+    constexpr int BV = BS * BS;
+    const BaijDev* cur = &A0;
+    std::unique_ptr<BaijDev> cur_own;
+    for (int lvl = 0; lvl < max_levels; ++lvl)
+    {
+        auto L = std::make_unique<Level>();
+        const uint32_t n = cur->nbr;
+        L->nrows = n;
+        L->own = std::move(cur_own);
+        L->A = cur;
+        L->dinv.alloc((size_t)n * BV + 1);
+        if (n) B2S_LAUNCH(ctx, k_diag_inv<BS>, stream_grid(ctx, n), kThreads, 0, n, cur->v.p, cur->diag_ptr.p, L->dinv.p);
+        if (n <= coarse_max)
+        {
+            pc.lv.push_back(std::move(L));
+            cur = nullptr;
+            break;
+        }
+        // strength
+        DBuf<uint32_t> cnt(n + 1), sp(n + 1);
+        B2S_LAUNCH(ctx, k_strength<BS>, stream_grid(ctx, n), kThreads, 0, n, cur->rp.p, cur->ci.p, cur->v.p,
+                   (const uint32_t*)nullptr, cnt.p, (uint32_t*)nullptr);
+        const uint32_t ns = exclusive_scan(ctx, cnt.p, sp.p, n);
+        DBuf<uint32_t> sc(ns ? ns : 1);
+        B2S_LAUNCH(ctx, k_strength<BS>, stream_grid(ctx, n), kThreads, 0, n, cur->rp.p, cur->ci.p, cur->v.p, sp.p,
+                   (uint32_t*)nullptr, sc.p);
+        // aggregation
+        L->agg.alloc(n);
+        B2S_CUDA(cudaMemsetAsync(L->agg.p, 0xFF, (size_t)n * sizeof(int32_t), ctx->stream));
+        DBuf<uint32_t> nagg_d(1);
+        B2S_LAUNCH(ctx, k_aggregate, 1, 32, 0, n, sp.p, sc.p, L->agg.p, nagg_d.p);
+        uint32_t nagg = 0;
+        d2h(ctx, &nagg, nagg_d.p, sizeof(uint32_t));
+        sync(ctx);
+        // smoothed prolongation
+        L->P.bs = BS;
+        L->P.nbr = n;
+        L->P.nbc = nagg;
+        B2S_LAUNCH(ctx, k_p_count, stream_grid(ctx, n), kThreads, 0, n, cur->rp.p, cur->ci.p, L->agg.p, cnt.p);
+        L->P.rp.alloc(n + 1);
+        const uint32_t pn = exclusive_scan(ctx, cnt.p, L->P.rp.p, n);
+        L->P.ci.alloc(pn ? pn : 1);
+        L->P.v.alloc(pn ? (size_t)pn * BV : 1);
+        B2S_LAUNCH(ctx, k_p_fill<BS>, stream_grid(ctx, n), kThreads, 0, n, cur->rp.p, cur->ci.p, cur->v.p, L->dinv.p,
+                   L->agg.p, L->P.rp.p, L->P.ci.p, L->P.v.p);
+        finish_baij(ctx, L->P);
+        block_transpose<BS>(ctx, L->P, L->R);
+        L->has_p = true;
+        // Galerkin
+        BaijDev AP;
+        block_matmul<BS>(ctx, *cur, L->P, AP);
+        cur_own = std::make_unique<BaijDev>();
+        block_matmul<BS>(ctx, L->R, AP, *cur_own);
+        cur = cur_own.get();
+        pc.lv.push_back(std::move(L));
+    }
+    // work vectors
+    for (size_t k = 0; k < pc.lv.size(); ++k)
+    {
+        Level& L = *pc.lv[k];
+        const size_t nd = (size_t)L.nrows * BS + 1;
+        L.tmp.alloc(nd);
+        L.r.alloc(nd);
+        if (L.has_p)
+        {
+            const size_t nc = (size_t)L.R.nbr * BS + 1;
+            L.rc.alloc(nc);
+            L.ec.alloc(nc);
+        }
+    }
+    // coarsest dense operator (the last level; if max_levels was reached its P is unused)
+    Level& C = *pc.lv.back();
+    pc.sz = (int)(C.nrows * BS);
+    pc.dense.alloc((size_t)pc.sz * pc.sz + 1);
+    pc.piv.alloc(pc.sz + 1);
+    B2S_CUDA(cudaMemsetAsync(pc.dense.p, 0, pc.dense.bytes(), ctx->stream));
+    if (C.nrows)
+        B2S_LAUNCH(ctx, k_dense_from_baij<BS>, stream_grid(ctx, C.nrows), kThreads, 0, C.nrows, C.A->rp.p, C.A->ci.p,
+                   C.A->v.p, pc.dense.p, pc.sz);
+    B2S_LAUNCH(ctx, k_dense_factor, 1, kThreads, 0, pc.dense.p, pc.sz, pc.ref_coarse ? 1 : 0, pc.piv.p);
+    sync(ctx);
+}
+
+__global__ void k_copy_u32(const uint32_t* __restrict__ a, uint32_t* __restrict__ b, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        b[i] = a[i];
+}
+
+std::unique_ptr<PcImpl> build_amg(b2s_ctx* ctx, const BaijDev& A, const b2s_pc_opts& o,
+                                  std::unique_ptr<BaijDev> owned)
+{
+    need(A.nbr == A.nbc, B2S_SHAPE, "block AMG needs a square block matrix");
+    auto pc = std::make_unique<PcAMG>();
+    pc->bs = A.bs;
+    pc->ref_coarse = o.amg_ref_coarse != 0;
+    pc->fine_copy = std::move(owned);
+    const int max_levels = o.amg_max_levels > 0 ? o.amg_max_levels : 20;
+    const uint32_t coarse_max = o.amg_coarse_max > 0 ? (uint32_t)o.amg_coarse_max : 50u;
+    switch (A.bs)
+    {
+        case 1: build_hierarchy<1>(ctx, *pc, A, max_levels, coarse_max); break;
+        case 2: build_hierarchy<2>(ctx, *pc, A, max_levels, coarse_max); break;
+        case 3: build_hierarchy<3>(ctx, *pc, A, max_levels, coarse_max); break;
+        case 4: build_hierarchy<4>(ctx, *pc, A, max_levels, coarse_max); break;
+        default: fail(B2S_UNSUPPORTED, "block size must be 1..4");
+    }
+    return pc;
+}
+
+}  // namespace
+
+std::unique_ptr<PcImpl> make_pc_amg_baij(b2s_ctx* ctx, const BaijDev& A, const b2s_pc_opts& o)
+{
+    return build_amg(ctx, A, o, nullptr);
+}
+
+// scalar SA-AMG: BlockMatrix<double,1>::condense of the CSR operator, which
+// for a block size of 1 is the same pattern and values
+std::unique_ptr<PcImpl> make_pc_amg_csr(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o)
+{
+    need(A.n == A.m, B2S_SHAPE, "AMG needs a square matrix");
+    auto B = std::make_unique<BaijDev>();
+    B->bs = 1;
+    B->nbr = A.n;
+    B->nbc = A.m;
+    B->rp.alloc(A.n + 1);
+    B->ci.alloc(A.nnz ? A.nnz : 1);
+    B->v.alloc(A.nnz ? A.nnz : 1);
+    d2d(ctx, B->rp.p, A.rp.p, (A.n + 1) * sizeof(uint32_t));
+    d2d(ctx, B->ci.p, A.ci.p, A.nnz * sizeof(uint32_t));
+    d2d(ctx, B->v.p, A.v.p, A.nnz * sizeof(double));
+    finish_baij(ctx, *B);
+    const BaijDev& ref = *B;
+    return build_amg(ctx, ref, o, std::move(B));
+}
+
+}  // namespace b2s

@@ -1,0 +1,591 @@
+// IC(0) and ILU(0) preconditioners: factorisation and triangular solves on the
+// GPU.
+//   make_ic0_preconditioner  array.cpp:2522-2732
+//   make_ilu0_preconditioner array.cpp:2744-2934
+//
+// Setup (all on the device):
+//   1. split the pattern of A (L incl. diagonal for IC(0); strict L and U incl.
+//      diagonal for ILU(0)) with a count / scan / fill;
+//   2. level sets of the factor's dependency DAG: level[i] = 1 + max level of
+//      the rows row i reads, computed by one sync-free traversal, then rows
+//      sorted by (level, index) with a stable radix sort;
+//   3. the factorisation, one launch per level, one thread per row, each row
+//      computed with exactly the reference's loop (two-pointer merges, same
+//      order of operations) -- the factors equal the reference's bit for bit;
+//   4. IC(0): L^T (strict part) by a device transpose whose rows are then
+//      sorted, and the level sets of the upper solve.
+// Apply: forward and backward substitution, either one launch per level
+// (B2S_TRSV_LEVEL) or one sync-free launch per triangle (B2S_TRSV_SYNCFREE);
+// both evaluate every row in the reference's order, so the FP64 apply equals
+// the reference's bit for bit.  With B2S_FP32 the factor values and the
+// intermediate vectors are FP32 (FP32 accumulation); the factorisation itself
+// stays FP64.
+#include <algorithm>
+
+#include "trisolve.cuh"
+
+namespace b2s {
+
+// ------------------------------------------------------------ pattern split
+
+// mode 0: keep j <= i (IC(0) L); mode 1: j < i (ILU(0) L); mode 2: j >= i (ILU(0) U)
+__global__ void k_split_count(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci, int mode,
+                              uint32_t* __restrict__ cnt)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        uint32_t c = 0;
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+        {
+            const uint32_t j = ci[p];
+            c += mode == 0 ? (j <= i) : mode == 1 ? (j < i) : (j >= i);
+        }
+        cnt[i] = c;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) cnt[n] = 0;
+}
+
+__global__ void k_split_fill(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                             const double* __restrict__ v, int mode, const uint32_t* __restrict__ orp,
+                             uint32_t* __restrict__ oci, double* __restrict__ ov, uint32_t* __restrict__ dpos,
+                             unsigned long long* err)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        uint32_t d = orp[i];
+        bool has_diag = false;
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+        {
+            const uint32_t j = ci[p];
+            const bool keep = mode == 0 ? (j <= i) : mode == 1 ? (j < i) : (j >= i);
+            if (!keep) continue;
+            if (j == i)
+            {
+                has_diag = true;
+                if (dpos) dpos[i] = d;
+            }
+            oci[d] = j;
+            ov[d] = v[p];
+            ++d;
+        }
+        if (mode != 1 && !has_diag) atomicMin(err, ((unsigned long long)i << 8) | B2S_MISSING_DIAG);
+    }
+}
+
+struct Csr32
+{
+    uint32_t n = 0, nnz = 0;
+    DBuf<uint32_t> rp, ci;
+    DBuf<double> v;
+    DBuf<float> v32;
+    std::vector<uint32_t> h_rp;
+};
+
+static void split(b2s_ctx* ctx, const CsrDev& A, int mode, Csr32& out, uint32_t* dpos, unsigned long long* err)
+{
+    const uint32_t n = A.n;
+    DBuf<uint32_t> cnt(n + 1);
+    B2S_LAUNCH(ctx, k_split_count, stream_grid(ctx, n), kThreads, 0, n, A.rp.p, A.ci.p, mode, cnt.p);
+    out.n = n;
+    out.rp.alloc(n + 1);
+    out.nnz = exclusive_scan(ctx, cnt.p, out.rp.p, n);
+    out.ci.alloc(out.nnz ? out.nnz : 1);
+    out.v.alloc(out.nnz ? out.nnz : 1);
+    B2S_LAUNCH(ctx, k_split_fill, stream_grid(ctx, n), kThreads, 0, n, A.rp.p, A.ci.p, A.v.p, mode, out.rp.p,
+               out.ci.p, out.v.p, dpos, err);
+}
+
+static void check_err(b2s_ctx* ctx, DBuf<unsigned long long>& err, const char* what)
+{
+    unsigned long long e = 0;
+    d2h(ctx, &e, err.p, sizeof(e));
+    sync(ctx);
+    if (e != ~0ull)
+    {
+        const uint32_t row = (uint32_t)(e >> 8);
+        const b2s_status st = (b2s_status)(e & 0xff);
+        std::string msg = std::string(what) + ": ";
+        switch (st)
+        {
+            case B2S_MISSING_DIAG: msg += "missing diagonal entry"; break;
+            case B2S_NOT_SPD: msg += "matrix may not be SPD (pivot <= 1e-14)"; break;
+            case B2S_ZERO_PIVOT: msg += "breakdown: U_kk close to zero"; break;
+            default: msg += b2s_status_name(st);
+        }
+        fail(st, msg + " at row " + std::to_string(row));
+    }
+}
+
+// ------------------------------------------------------------ factorisation
+
+// IC(0) row, array.cpp:2577-2655
+__global__ void k_ic0_level(const uint32_t* __restrict__ rows, uint32_t count, const uint32_t* __restrict__ Lrp,
+                            const uint32_t* __restrict__ Lci, double* Lv, double* diag, unsigned long long* err)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint32_t i = rows[t];
+    const uint32_t rs = Lrp[i], re = Lrp[i + 1];
+    for (uint32_t p = rs; p < re; ++p)
+    {
+        const uint32_t j = Lci[p];
+        if (j >= i) break;
+        double sum = 0.0;
+        uint32_t pi = rs, pj = Lrp[j];
+        const uint32_t ej = Lrp[j + 1];
+        while (pi < p && pj < ej)
+        {
+            const uint32_t ki = Lci[pi], kj = Lci[pj];
+            if (ki == kj)
+            {
+                sum += Lv[pi] * Lv[pj];
+                ++pi;
+                ++pj;
+            }
+            else if (ki < kj)
+                ++pi;
+            else
+                ++pj;
+        }
+        Lv[p] = (Lv[p] - sum) / diag[j];
+    }
+    uint32_t dp = re;
+    for (uint32_t p = rs; p < re; ++p)
+        if (Lci[p] == i)
+        {
+            dp = p;
+            break;
+        }
+    if (dp == re)
+    {
+        atomicMin(err, ((unsigned long long)i << 8) | B2S_MISSING_DIAG);
+        diag[i] = 1.0;
+        return;
+    }
+    double sd = 0.0;
+    for (uint32_t p = rs; p < dp; ++p) sd += Lv[p] * Lv[p];
+    const double dv = Lv[dp] - sd;
+    if (!(dv > 1e-14))
+    {
+        atomicMin(err, ((unsigned long long)i << 8) | B2S_NOT_SPD);
+        diag[i] = 1.0;
+        return;
+    }
+    Lv[dp] = sqrt(dv);
+    diag[i] = Lv[dp];
+}
+
+// ILU(0) row, array.cpp:2840-2898 (IKJ; fill-in dropped)
+__global__ void k_ilu0_level(const uint32_t* __restrict__ rows, uint32_t count, const uint32_t* __restrict__ Lrp,
+                             const uint32_t* __restrict__ Lci, double* Lv, const uint32_t* __restrict__ Urp,
+                             const uint32_t* __restrict__ Uci, double* Uv, const uint32_t* __restrict__ dix,
+                             unsigned long long* err)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint32_t i = rows[t];
+    const uint32_t us = Urp[i], ue = Urp[i + 1];
+    for (uint32_t pl = Lrp[i]; pl < Lrp[i + 1]; ++pl)
+    {
+        const uint32_t k = Lci[pl];
+        const double ukk = Uv[dix[k]];
+        if (fabs(ukk) < 1e-30)
+        {
+            atomicMin(err, ((unsigned long long)i << 8) | B2S_ZERO_PIVOT);
+            return;
+        }
+        Lv[pl] /= ukk;
+        uint32_t pi = us, pk = Urp[k];
+        const uint32_t ek = Urp[k + 1];
+        while (pi < ue && pk < ek)
+        {
+            const uint32_t ji = Uci[pi], jk = Uci[pk];
+            if (ji == jk)
+            {
+                Uv[pi] -= Lv[pl] * Uv[pk];
+                ++pi;
+                ++pk;
+            }
+            else if (ji < jk)
+                ++pi;
+            else
+                ++pk;
+        }
+    }
+}
+
+// ------------------------------------------------------------ transpose
+
+__global__ void k_tr_count(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                           uint32_t* __restrict__ cnt)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+            if (ci[p] < i) atomicAdd(&cnt[ci[p]], 1u);
+}
+
+__global__ void k_tr_fill(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                          const double* __restrict__ v, const uint32_t* __restrict__ trp, uint32_t* __restrict__ off,
+                          uint32_t* __restrict__ tci, double* __restrict__ tv)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+        {
+            const uint32_t j = ci[p];
+            if (j < i)
+            {
+                const uint32_t d = trp[j] + atomicAdd(&off[j], 1u);
+                tci[d] = i;
+                tv[d] = v[p];
+            }
+        }
+}
+
+__global__ void k_row_sort(uint32_t n, const uint32_t* __restrict__ rp, uint32_t* __restrict__ ci, double* __restrict__ v)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const uint32_t a = rp[i], b = rp[i + 1];
+        for (uint32_t p = a + 1; p < b; ++p)
+        {
+            const uint32_t c = ci[p];
+            const double x = v[p];
+            uint32_t q = p;
+            while (q > a && ci[q - 1] > c)
+            {
+                ci[q] = ci[q - 1];
+                v[q] = v[q - 1];
+                --q;
+            }
+            ci[q] = c;
+            v[q] = x;
+        }
+    }
+}
+
+// strict lower part of L -> its transpose (strict upper) as sorted CSR
+static void transpose_strict(b2s_ctx* ctx, const Csr32& L, Csr32& T)
+{
+    const uint32_t n = L.n;
+    DBuf<uint32_t> cnt(n + 1);
+    B2S_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes(), ctx->stream));
+    B2S_LAUNCH(ctx, k_tr_count, stream_grid(ctx, n), kThreads, 0, n, L.rp.p, L.ci.p, cnt.p);
+    T.n = n;
+    T.rp.alloc(n + 1);
+    T.nnz = exclusive_scan(ctx, cnt.p, T.rp.p, n);
+    T.ci.alloc(T.nnz ? T.nnz : 1);
+    T.v.alloc(T.nnz ? T.nnz : 1);
+    B2S_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes(), ctx->stream));
+    B2S_LAUNCH(ctx, k_tr_fill, stream_grid(ctx, n), kThreads, 0, n, L.rp.p, L.ci.p, L.v.p, T.rp.p, cnt.p, T.ci.p,
+               T.v.p);
+    B2S_LAUNCH(ctx, k_row_sort, stream_grid(ctx, n), kThreads, 0, n, T.rp.p, T.ci.p, T.v.p);
+}
+
+// ------------------------------------------------------------ triangular solves
+
+template <typename T>
+__device__ __forceinline__ T ld_dep(const T* p)
+{
+    return __ldcg(p);
+}
+
+// One row of a triangular solve:  x_i = (rhs_i - sum_{deps j} V_ij x_j) [/ d_i]
+// in the row's column order.  VT: factor storage, XT: solution / accumulation
+// type, RT: right-hand-side type.  out64 (optional) receives x as FP64.
+template <bool LOWER, bool UNIT, typename VT, typename XT, typename RT>
+struct TrsvOp
+{
+    const uint32_t *rp, *ci;
+    const VT* v;
+    const VT* d;
+    const RT* rhs;
+    XT* x;
+    double* out64;
+    __device__ bool ready(uint32_t row, const uint32_t* flags, uint32_t epoch) const
+    {
+        return deps_ready<LOWER>(row, rp, ci, flags, epoch);
+    }
+    template <bool SYNCFREE>
+    __device__ __forceinline__ void row_compute(uint32_t row) const
+    {
+        XT sum = (XT)rhs[row];
+        const uint32_t a = __ldg(&rp[row]), b = __ldg(&rp[row + 1]);
+        for (uint32_t p = a; p < b; ++p)
+        {
+            const uint32_t j = __ldg(&ci[p]);
+            if (LOWER ? (j < row) : (j > row))
+            {
+                const XT xj = SYNCFREE ? ld_dep(&x[j]) : x[j];
+                sum -= (XT)__ldg(&v[p]) * xj;
+            }
+        }
+        const XT r = UNIT ? sum : sum / (XT)__ldg(&d[row]);
+        x[row] = r;
+        if (out64) out64[row] = (double)r;
+    }
+    __device__ void compute(uint32_t row) const { row_compute<true>(row); }
+};
+
+// A triangular factor ready for solves: CSR rows + divisor + schedule.
+struct Tri
+{
+    bool lower = true, unit = false;
+    uint32_t n = 0;
+    const Csr32* m = nullptr;
+    const double* d64 = nullptr;
+    const float* d32 = nullptr;
+    LevelSchedule sched;
+    SyncFree sf;
+
+    template <typename Op>
+    void run(b2s_ctx* ctx, int mode, const Op& op, const int* done)
+    {
+        run_schedule(ctx, mode, sched, sf, op, done);
+    }
+
+    // x = T^-1 rhs; precision per the type parameters
+    template <typename VT, typename XT, typename RT>
+    void solve(b2s_ctx* ctx, int mode, const VT* v, const VT* d, const RT* rhs, XT* x, double* out64, const int* done)
+    {
+        if (lower && unit)
+            run(ctx, mode, TrsvOp<true, true, VT, XT, RT>{m->rp.p, m->ci.p, v, d, rhs, x, out64}, done);
+        else if (lower)
+            run(ctx, mode, TrsvOp<true, false, VT, XT, RT>{m->rp.p, m->ci.p, v, d, rhs, x, out64}, done);
+        else if (unit)
+            run(ctx, mode, TrsvOp<false, true, VT, XT, RT>{m->rp.p, m->ci.p, v, d, rhs, x, out64}, done);
+        else
+            run(ctx, mode, TrsvOp<false, false, VT, XT, RT>{m->rp.p, m->ci.p, v, d, rhs, x, out64}, done);
+    }
+
+    void prepare(b2s_ctx* ctx, const Csr32& mat, bool lo, bool un)
+    {
+        m = &mat;
+        lower = lo;
+        unit = un;
+        n = mat.n;
+        sched.build(ctx, n, mat.rp.p, mat.ci.p, lo);
+        sf.init(ctx, n);
+    }
+};
+
+__global__ void k_f64_to_f32(const double* __restrict__ a, float* __restrict__ b, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+static void to_f32(b2s_ctx* ctx, const DBuf<double>& a, DBuf<float>& b, uint64_t n)
+{
+    b.alloc(n ? n : 1);
+    if (n) B2S_LAUNCH(ctx, k_f64_to_f32, stream_grid(ctx, n), kThreads, 0, a.p, b.p, n);
+}
+
+static int pick_trsv(const b2s_pc_opts& o) { return o.trsv == B2S_TRSV_LEVEL ? B2S_TRSV_LEVEL : B2S_TRSV_SYNCFREE; }
+
+static void export_csr(b2s_ctx* ctx, const Csr32& m, uint64_t* sizes, uint32_t* rp, uint32_t* ci, double* v)
+{
+    sizes[0] = (uint64_t)m.n + 1;
+    sizes[1] = m.nnz;
+    sizes[2] = m.nnz;
+    if (rp) d2h(ctx, rp, m.rp.p, (m.n + 1) * sizeof(uint32_t));
+    if (ci) d2h(ctx, ci, m.ci.p, m.nnz * sizeof(uint32_t));
+    if (v) d2h(ctx, v, m.v.p, m.nnz * sizeof(double));
+    sync(ctx);
+}
+
+static void export_levels(b2s_ctx* ctx, const LevelSchedule& s, uint64_t* sizes, uint32_t* ci)
+{
+    sizes[0] = 0;
+    sizes[1] = s.n;
+    sizes[2] = 0;
+    if (ci) d2h(ctx, ci, s.level.p, s.n * sizeof(uint32_t));
+    sync(ctx);
+}
+
+// ------------------------------------------------------------ IC(0)
+
+namespace {
+
+struct PcIC0 final : PcImpl
+{
+    uint32_t n = 0;
+    int mode = B2S_TRSV_SYNCFREE;
+    bool fp32 = false;
+    Csr32 L, LT;
+    DBuf<double> diag, y;
+    DBuf<float> diag32, y32, z32;
+    Tri fwd, bwd;
+
+    void apply(b2s_ctx* ctx, const double* r, double* z, const int* done) override
+    {
+        if (!fp32)
+        {
+            fwd.solve<double, double, double>(ctx, mode, L.v.p, diag.p, r, y.p, nullptr, done);
+            bwd.solve<double, double, double>(ctx, mode, LT.v.p, diag.p, y.p, z, nullptr, done);
+        }
+        else
+        {
+            fwd.solve<float, float, double>(ctx, mode, L.v32.p, diag32.p, r, y32.p, nullptr, done);
+            bwd.solve<float, float, float>(ctx, mode, LT.v32.p, diag32.p, y32.p, z32.p, z, done);
+        }
+    }
+
+    void export_data(b2s_ctx* ctx, const std::string& what, uint64_t* sizes, uint32_t* rp, uint32_t* ci,
+                     double* v) override
+    {
+        if (what == "ic0.L") return export_csr(ctx, L, sizes, rp, ci, v);
+        if (what == "ic0.LT") return export_csr(ctx, LT, sizes, rp, ci, v);
+        if (what == "ic0.diag")
+        {
+            sizes[0] = 0;
+            sizes[1] = 0;
+            sizes[2] = n;
+            if (v) d2h(ctx, v, diag.p, n * sizeof(double));
+            sync(ctx);
+            return;
+        }
+        if (what == "levels.L") return export_levels(ctx, fwd.sched, sizes, ci);
+        if (what == "levels.U") return export_levels(ctx, bwd.sched, sizes, ci);
+        PcImpl::export_data(ctx, what, sizes, rp, ci, v);
+    }
+};
+
+}  // namespace
+
+// factor IC(0) on the pattern of tril(A) with values Lv (already placed);
+// shared with the learned preconditioner, which factors corrected values.
+void ic0_factor_inplace(b2s_ctx* ctx, const LevelSchedule& s, const uint32_t* Lrp, const uint32_t* Lci, double* Lv,
+                        double* diag, const char* what)
+{
+    DBuf<unsigned long long> err(1);
+    const unsigned long long none = ~0ull;
+    h2d(ctx, err.p, &none, sizeof(none));
+    for (uint32_t l = 0; l < s.nlev; ++l)
+    {
+        const uint32_t a = s.h_ptr[l], cnt = s.h_ptr[l + 1] - a;
+        B2S_LAUNCH(ctx, k_ic0_level, (cnt + kThreads - 1) / kThreads, kThreads, 0, s.rows.p + a, cnt, Lrp, Lci, Lv,
+                   diag, err.p);
+    }
+    check_err(ctx, err, what);
+}
+
+std::unique_ptr<PcImpl> make_pc_ic0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o)
+{
+    need(A.n == A.m, B2S_SHAPE, "IC(0) needs a square matrix");
+    auto pc = std::make_unique<PcIC0>();
+    pc->n = A.n;
+    pc->mode = pick_trsv(o);
+    pc->fp32 = o.precision != B2S_FP64;
+    DBuf<unsigned long long> err(1);
+    const unsigned long long none = ~0ull;
+    h2d(ctx, err.p, &none, sizeof(none));
+    split(ctx, A, 0, pc->L, nullptr, err.p);
+    check_err(ctx, err, "IC(0) failed");
+    pc->diag.alloc(A.n ? A.n : 1);
+    pc->fwd.prepare(ctx, pc->L, true, false);
+    pc->fwd.d64 = pc->diag.p;
+    ic0_factor_inplace(ctx, pc->fwd.sched, pc->L.rp.p, pc->L.ci.p, pc->L.v.p, pc->diag.p, "IC(0) failed");
+    transpose_strict(ctx, pc->L, pc->LT);
+    pc->bwd.prepare(ctx, pc->LT, false, false);
+    pc->y.alloc(A.n ? A.n : 1);
+    if (pc->fp32)
+    {
+        to_f32(ctx, pc->L.v, pc->L.v32, pc->L.nnz);
+        to_f32(ctx, pc->LT.v, pc->LT.v32, pc->LT.nnz);
+        to_f32(ctx, pc->diag, pc->diag32, A.n);
+        pc->y32.alloc(A.n ? A.n : 1);
+        pc->z32.alloc(A.n ? A.n : 1);
+    }
+    sync(ctx);
+    return pc;
+}
+
+// ------------------------------------------------------------ ILU(0)
+
+namespace {
+
+struct PcILU0 final : PcImpl
+{
+    uint32_t n = 0;
+    int mode = B2S_TRSV_SYNCFREE;
+    bool fp32 = false;
+    Csr32 L, U;
+    DBuf<uint32_t> dix;
+    DBuf<double> udiag, y;
+    DBuf<float> udiag32, y32, z32;
+    Tri fwd, bwd;
+
+    void apply(b2s_ctx* ctx, const double* r, double* z, const int* done) override
+    {
+        if (!fp32)
+        {
+            fwd.solve<double, double, double>(ctx, mode, L.v.p, (const double*)nullptr, r, y.p, nullptr, done);
+            bwd.solve<double, double, double>(ctx, mode, U.v.p, udiag.p, y.p, z, nullptr, done);
+        }
+        else
+        {
+            fwd.solve<float, float, double>(ctx, mode, L.v32.p, (const float*)nullptr, r, y32.p, nullptr, done);
+            bwd.solve<float, float, float>(ctx, mode, U.v32.p, udiag32.p, y32.p, z32.p, z, done);
+        }
+    }
+
+    void export_data(b2s_ctx* ctx, const std::string& what, uint64_t* sizes, uint32_t* rp, uint32_t* ci,
+                     double* v) override
+    {
+        if (what == "ilu0.L") return export_csr(ctx, L, sizes, rp, ci, v);
+        if (what == "ilu0.U") return export_csr(ctx, U, sizes, rp, ci, v);
+        if (what == "levels.L") return export_levels(ctx, fwd.sched, sizes, ci);
+        if (what == "levels.U") return export_levels(ctx, bwd.sched, sizes, ci);
+        PcImpl::export_data(ctx, what, sizes, rp, ci, v);
+    }
+};
+
+__global__ void k_gather_diag(uint32_t n, const double* __restrict__ Uv, const uint32_t* __restrict__ dix,
+                              double* __restrict__ d)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) d[i] = Uv[dix[i]];
+}
+
+}  // namespace
+
+std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o)
+{
+    need(A.n == A.m, B2S_SHAPE, "ILU(0) needs a square matrix");
+    auto pc = std::make_unique<PcILU0>();
+    const uint32_t n = A.n;
+    pc->n = n;
+    pc->mode = pick_trsv(o);
+    pc->fp32 = o.precision != B2S_FP64;
+    DBuf<unsigned long long> err(1);
+    const unsigned long long none = ~0ull;
+    h2d(ctx, err.p, &none, sizeof(none));
+    pc->dix.alloc(n ? n : 1);
+    split(ctx, A, 1, pc->L, nullptr, err.p);
+    split(ctx, A, 2, pc->U, pc->dix.p, err.p);
+    check_err(ctx, err, "ILU(0) failed");
+    pc->fwd.prepare(ctx, pc->L, true, true);
+    // factor, level by level
+    for (uint32_t l = 0; l < pc->fwd.sched.nlev; ++l)
+    {
+        const uint32_t a = pc->fwd.sched.h_ptr[l], cnt = pc->fwd.sched.h_ptr[l + 1] - a;
+        B2S_LAUNCH(ctx, k_ilu0_level, (cnt + kThreads - 1) / kThreads, kThreads, 0, pc->fwd.sched.rows.p + a, cnt,
+                   pc->L.rp.p, pc->L.ci.p, pc->L.v.p, pc->U.rp.p, pc->U.ci.p, pc->U.v.p, pc->dix.p, err.p);
+    }
+    check_err(ctx, err, "ILU(0) failed");
+    pc->udiag.alloc(n ? n : 1);
+    if (n) B2S_LAUNCH(ctx, k_gather_diag, stream_grid(ctx, n), kThreads, 0, n, pc->U.v.p, pc->dix.p, pc->udiag.p);
+    pc->bwd.prepare(ctx, pc->U, false, false);
+    pc->y.alloc(n ? n : 1);
+    if (pc->fp32)
+    {
+        to_f32(ctx, pc->L.v, pc->L.v32, pc->L.nnz);
+        to_f32(ctx, pc->U.v, pc->U.v32, pc->U.nnz);
+        to_f32(ctx, pc->udiag, pc->udiag32, n);
+        pc->y32.alloc(n ? n : 1);
+        pc->z32.alloc(n ? n : 1);
+    }
+    sync(ctx);
+    return pc;
+}
+
+}  // namespace b2s

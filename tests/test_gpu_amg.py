@@ -1,0 +1,78 @@
+"""Smoothed-aggregation AMG on the GPU (blockMatrix.hpp:874-1179).
+
+With amg_ref_coarse=1 the whole hierarchy (aggregates, A, P, D^-1 on every
+level) and the V-cycle output equal the restatement bit for bit -- the
+restatement itself equals the compiled reference (tests/test_oracle_pin.py).
+The default coarse solve is a correct pivoted LU ("amg_exact" in the oracle),
+checked the same way; PCG with it converges where the reference's cannot."""
+import numpy as np
+import pytest
+
+import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+def hier_cases(b2s):
+    return {
+        "bs1_poisson2d": (1,) + P.poisson2d(40),
+        "bs3_mpi": (3,) + P.make_test_scalar(20, 3),
+        "bs1_poisson3d": (1,) + b2s.gen_poisson3d(14),
+    }
+
+
+@pytest.mark.parametrize("case", ["bs1_poisson2d", "bs3_mpi", "bs1_poisson3d"])
+@pytest.mark.parametrize("ref_coarse", [1, 0])
+def test_amg_hierarchy_and_vcycle(b2s, ctx, orc, case, ref_coarse):
+    bs, n, rp, ci, v = hier_cases(b2s)[case]
+    Ao = orc.csr(n, n, rp, ci, v)
+    Bo = orc.blk_condense(bs, Ao, n // bs, n // bs)
+    brp, bci, bv = Bo.export()
+    B = b2s.BAIJ(ctx, bs, n // bs, n // bs, brp, bci, bv)
+    M = b2s.Precond(ctx, B, b2s.PC_BSA_AMG, amg_ref_coarse=ref_coarse)
+    po = orc.blk_pc(Bo, "amg" if ref_coarse else "amg_exact")
+    levels = orc.amg_export(po, bs)
+    _, nrows, _ = M.export("amg.levels")
+    assert list(nrows) == [lv["nrows"] for lv in levels]
+    for k, lv in enumerate(levels):
+        Arp, Aci, Av = M.export(f"amg.{k}.A")
+        assert np.array_equal(Arp, lv["Arp"]) and np.array_equal(Aci, lv["Aci"]) and np.array_equal(Av, lv["Av"]), k
+        assert np.array_equal(M.export(f"amg.{k}.dinv")[2], lv["diag_inv"]), k
+        if "Prp" in lv:
+            Prp, Pci, Pv = M.export(f"amg.{k}.P")
+            assert np.array_equal(Prp, lv["Prp"]) and np.array_equal(Pci, lv["Pci"]) and np.array_equal(Pv, lv["Pv"])
+            agg = M.export(f"amg.{k}.agg")[1]
+            assert np.array_equal(agg.astype(np.int32), orc.amg_aggregates(po, k, lv["nrows"]))
+    r = P.drand(np.arange(n) + 5)
+    assert np.array_equal(M.apply(r), po.apply(r))
+
+
+def test_scalar_amg_string_is_sa(b2s, ctx, orc):
+    n, rp, ci, v = b2s.gen_poisson3d(16)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    M = b2s.Precond(ctx, A, b2s.pc_kind_from_name(b2s.PCG, "amg"))
+    po = orc.pc(orc.csr(n, n, rp, ci, v), "sa_amg_exact")
+    r = b2s.uniform(8, n)
+    assert np.array_equal(M.apply(r), po.apply(r))
+
+
+def test_amg_pcg_converges(b2s, ctx, orc):
+    n, rp, ci, v = b2s.gen_poisson3d(32)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(0, n)
+    M = b2s.Precond(ctx, A, b2s.PC_SA_AMG)
+    x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-10, maxit=500)
+    assert st["status"] == 0 and st["relres_true"] < 2e-10
+    xo, io = orc.solve_pc(orc.csr(n, n, rp, ci, v), 0, orc.pc(orc.csr(n, n, rp, ci, v), "sa_amg_exact"), b,
+                          1e-10, 500)
+    assert abs(st["it"] - io) <= 2
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-8
+
+
+def test_block_amg_elasticity_pcg(b2s, ctx):
+    nbr, rp, ci, v = b2s.gen_elasticity_q1(12)
+    B = b2s.BAIJ(ctx, 3, nbr, nbr, rp, ci, v)
+    b = b2s.uniform(1, 3 * nbr)
+    M = b2s.Precond(ctx, B, b2s.PC_BSA_AMG)
+    x, st = b2s.solve(ctx, B, b, b2s.PCG, M, tol=1e-8, maxit=2000)
+    assert st["status"] == 0 and st["relres_true"] < 2e-8
