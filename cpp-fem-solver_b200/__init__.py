@@ -109,7 +109,9 @@ EXPORTS = [
     "b2s_pc_create_baij", "b2s_pc_create_host", "b2s_pc_destroy", "b2s_pc_apply", "b2s_pc_apply_device",
     "b2s_pc_export", "b2s_pc_kind_from_name", "b2s_solve_opts_default", "b2s_solve", "b2s_solve_device",
     "b2s_solve_baij", "b2s_solve_baij_device", "b2s_gen_poisson2d", "b2s_gen_poisson3d", "b2s_gen_convdiff3d",
-    "b2s_gen_elasticity_q1", "b2s_gen_grf_diffusion", "b2s_gen_uniform",
+    "b2s_gen_elasticity_q1", "b2s_gen_grf_diffusion", "b2s_gen_uniform", "b2s_learner_create",
+    "b2s_learner_destroy", "b2s_learner_load", "b2s_learner_save", "b2s_learner_params", "b2s_learner_step",
+    "b2s_pc_create_learned",
 ]
 
 
@@ -174,6 +176,13 @@ def lib():
     f("b2s_gen_elasticity_q1", i32, u32, f64, f64, u32ptr, u32ptr, vp, vp, vp)
     f("b2s_gen_grf_diffusion", i32, u32, f64, f64, u64, u32ptr, u32ptr, vp, vp, vp, vp)
     f("b2s_gen_uniform", i32, u64, u64, _f64p)
+    f("b2s_learner_create", i32, vp, u64, pp)
+    f("b2s_learner_destroy", i32, vp)
+    f("b2s_learner_load", i32, vp, cp)
+    f("b2s_learner_save", i32, vp, cp)
+    f("b2s_learner_params", i32, vp, vp, C.POINTER(C.c_uint64), i32)
+    f("b2s_learner_step", i32, vp, vp, vp, i32, u64, vp, f64, i32, C.POINTER(C.c_double), vp)
+    f("b2s_pc_create_learned", i32, vp, vp, vp, C.POINTER(PcOpts), pp)
     _lib = L
     return L
 
@@ -368,6 +377,68 @@ class HostPrecond:
         try:
             if getattr(self, "h", None) and self.ctx.h:
                 lib().b2s_pc_destroy(self.h)
+        except Exception:
+            pass
+
+
+WEIGHTS = os.path.join(HERE, "weights", "learned_ic0.bin")
+
+
+class Learner:
+    """The learned-IC(0) message-passing network (b2s_learner)."""
+
+    def __init__(self, ctx: Context, seed: int = 0, weights: str | None = None):
+        self.ctx = ctx
+        h = C.c_void_p()
+        ctx.check(lib().b2s_learner_create(ctx.h, seed, C.byref(h)), "learner_create")
+        self.h = h
+        if weights:
+            self.load(weights)
+
+    @property
+    def nparams(self) -> int:
+        c = C.c_uint64()
+        lib().b2s_learner_params(self.h, None, C.byref(c), 0)
+        return c.value
+
+    def params(self) -> np.ndarray:
+        c = C.c_uint64(self.nparams)
+        out = np.zeros(c.value, np.float32)
+        self.ctx.check(lib().b2s_learner_params(self.h, _ptr(out), C.byref(c), 0), "learner_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        c = C.c_uint64(len(p))
+        self.ctx.check(lib().b2s_learner_params(self.h, _ptr(p), C.byref(c), 1), "learner_params")
+
+    def load(self, path: str):
+        self.ctx.check(lib().b2s_learner_load(self.h, path.encode()), "learner_load")
+
+    def save(self, path: str):
+        self.ctx.check(lib().b2s_learner_save(self.h, path.encode()), "learner_save")
+
+    def step(self, A: CSR, nprobes=4, seed=0, probes=None, lr=1e-3, update=True, want_grad=False):
+        loss = C.c_double()
+        grad = np.zeros(self.nparams, np.float32) if want_grad else None
+        pr = None if probes is None else np.ascontiguousarray(probes, np.float64)
+        self.ctx.check(lib().b2s_learner_step(self.ctx.h, self.h, A.h, int(nprobes), int(seed), _ptr(pr), float(lr),
+                                              1 if update else 0, C.byref(loss), _ptr(grad)), "learner_step")
+        return (loss.value, grad) if want_grad else loss.value
+
+    def precond(self, A: CSR, **opts) -> "Precond":
+        o = pc_opts(**opts)
+        P = Precond.__new__(Precond)
+        P.ctx, P.kind, P.n = self.ctx, PC_LEARNED_IC0, A.n
+        h = C.c_void_p()
+        self.ctx.check(lib().b2s_pc_create_learned(self.ctx.h, A.h, self.h, C.byref(o), C.byref(h)), "pc_learned")
+        P.h = h
+        return P
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.ctx.h:
+                lib().b2s_learner_destroy(self.h)
         except Exception:
             pass
 

@@ -386,6 +386,16 @@ void baij_matvec(b2s_ctx* ctx, const BaijDev& A, const double* x, double* y, con
 void build_row_blocks(const uint32_t* rp, uint32_t nrows, uint32_t unit, uint32_t max_rows, uint32_t max_units,
                       std::vector<uint32_t>& out);
 
+// Changes IC(0) factor values in place after the factorisation (the learned
+// preconditioner): L holds rows with the diagonal last, diag the diagonal.
+struct Ic0Correction
+{
+    virtual ~Ic0Correction() = default;
+    virtual void correct(b2s_ctx* ctx, const CsrDev& A, const uint32_t* Lrp, const uint32_t* Lci, uint32_t Lnnz,
+                         double* Lv, double* diag) = 0;
+};
+std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o, Ic0Correction* corr);
+
 // preconditioner factories (one per file)
 std::unique_ptr<PcImpl> make_pc_diag(b2s_ctx* ctx, const CsrDev& A);
 std::unique_ptr<PcImpl> make_pc_identity(uint64_t n);

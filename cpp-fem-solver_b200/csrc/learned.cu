@@ -1,0 +1,1134 @@
+// Learned IC(0): a message-passing network over the graph of A that corrects
+// the IC(0) factor values on the unchanged pattern (no counterpart in the
+// reference; its IC(0) is make_ic0_preconditioner, array.cpp:2522-2732).
+//
+// Network (26,502 parameters, FP32 master copy, BF16 copy used in the
+// forward pass, FP32 accumulation everywhere):
+//   node features f_i (8): scale-free statistics of row i -- mean / min / max
+//     of log(|a_ij| / a_ii) over the neighbours, log of the off-diagonal row
+//     sum over a_ii, degree / 4, and log(a_ii / mean_j a_jj)
+//   edge features e_ij (4): log(|a_ij|/a_ii), log(|a_ij|/a_jj),
+//     log(a_jj/a_ii), +1 for j < i / -1 for j > i
+//   h0 = relu(W_in f + b_in)                                   (64)
+//   3 layers:  [s | m] = h [W_s | W_m]^T ;  g_ij = sigmoid(W_g e_ij + b_g)
+//              h' = relu(s_i + b + (1/deg_i) sum_j g_ij * m_j) + h
+//   head:      c_ij = u.h_i + v.h_j + w.e_ij + b_o   (j < i)
+//              c_ii = d.h_i + b_d
+//   L~_ij = L_ij exp(0.5 tanh c_ij); the diagonal is kept >= 1e-3 sqrt(a_ii)
+//   (positive-pivot guard), so L~ L~^T stays SPD.
+// The output layer starts at zero: an untrained network returns IC(0).
+//
+// Training loss on probe vectors w (half standard normal, half smoothed by
+// ten 2/3-Jacobi sweeps, the modes IC(0) resolves worst):
+//   loss = mean_w ||(L~ L~^T - A) w||^2 / ||A w||^2
+// whose gradient in L~ needs only products with L~ and L~^T:
+//   dloss/dL~_ij = 2 (v_i u_j + w_i q_j) / ||Aw||^2,  u = L~^T w,
+//   v = L~ u - A w,  q = L~^T v.
+// All parameter gradients are reduced in a fixed order (per-CTA partials,
+// then one ordered sum), so training is deterministic.
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <dlfcn.h>
+
+#include <fstream>
+
+#include "b2s_internal.cuh"
+
+struct b2s_learner;
+
+namespace b2s {
+
+namespace {
+
+constexpr int H = 64, FIN = 8, FE = 4, NL = 3;
+constexpr float kScale = 0.5f;
+
+// parameter layout
+constexpr int OFF_WIN = 0, OFF_BIN = OFF_WIN + H * FIN;
+constexpr int LAYER0 = OFF_BIN + H;
+constexpr int L_WS = 0, L_WM = H * H, L_WG = 2 * H * H, L_BG = L_WG + H * FE, L_B = L_BG + H, L_SIZE = L_B + H;
+constexpr int OFF_OUT = LAYER0 + NL * L_SIZE;
+constexpr int O_U = 0, O_V = H, O_W = 2 * H, O_BO = 2 * H + FE, O_D = O_BO + 1, O_BD = O_D + H, O_SIZE = O_BD + 1;
+constexpr int NPARAM = OFF_OUT + O_SIZE;
+static_assert(NPARAM == 26502, "parameter count");
+
+__device__ __forceinline__ float sigm(float x) { return 1.0f / (1.0f + expf(-x)); }
+
+// ------------------------------------------------------------ graph setup
+
+// rev[p] = position of (j, i) in row j for the entry (i, j) at p; UINT32_MAX if absent
+__global__ void k_rev(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci, uint32_t* rev,
+                      int* nonsym)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+        {
+            const uint32_t j = ci[p];
+            uint32_t lo = rp[j], hi = rp[j + 1], f = 0xFFFFFFFFu;
+            while (lo < hi)
+            {
+                const uint32_t mid = (lo + hi) / 2;
+                if (ci[mid] == i)
+                {
+                    f = mid;
+                    break;
+                }
+                if (ci[mid] < i)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            rev[p] = f;
+            if (f == 0xFFFFFFFFu) atomicExch(nonsym, 1);
+        }
+}
+
+// node features F (n x 8), edge features EF (nnz x 4), inverse degree
+__global__ void k_features(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                           const double* __restrict__ v, const double* __restrict__ diag, double mean_logd,
+                           float* __restrict__ F, float* __restrict__ EF, float* __restrict__ invdeg)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const double aii = diag[i];
+        const double la = log(fabs(aii) + 1e-300);
+        double s = 0, mn = 1e300, mx = -1e300, off = 0;
+        int deg = 0;
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+        {
+            const uint32_t j = ci[p];
+            if (j == i) continue;
+            const double a = fabs(v[p]) + 1e-300;
+            const double t = log(a) - la;
+            s += t;
+            mn = fmin(mn, t);
+            mx = fmax(mx, t);
+            off += a;
+            ++deg;
+            const double lj = log(fabs(diag[j]) + 1e-300);
+            EF[(size_t)p * FE + 0] = (float)t;
+            EF[(size_t)p * FE + 1] = (float)(log(a) - lj);
+            EF[(size_t)p * FE + 2] = (float)(lj - la);
+            EF[(size_t)p * FE + 3] = j < i ? 1.0f : -1.0f;
+        }
+        float* f = F + (size_t)i * FIN;
+        f[0] = deg ? (float)(s / deg) : 0.f;
+        f[1] = deg ? (float)mn : 0.f;
+        f[2] = deg ? (float)mx : 0.f;
+        f[3] = (float)log(off / fabs(aii) + 1e-30);
+        f[4] = deg / 4.0f;
+        f[5] = (float)(la - mean_logd);
+        f[6] = 0.f;
+        f[7] = 0.f;
+        invdeg[i] = deg ? 1.0f / deg : 0.f;
+    }
+}
+
+__global__ void k_logdiag_sum(uint32_t n, const double* __restrict__ d, double* out, double* partial, unsigned* counter)
+{
+    double acc[1] = {0.0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        acc[0] += log(fabs(d[i]) + 1e-300);
+    if (grid_reduce_last<1>(acc, partial, counter))
+        if (threadIdx.x == 0) *out = acc[0] / (n ? n : 1);
+}
+
+// ------------------------------------------------------------ dense layers
+
+// Y (n x NO) = act(X (n x K) W^T + b), W (NO x K) in BF16, FP32 accumulation.
+// Optionally stores the pre-activation; RES adds X (K == NO) after the activation.
+constexpr int kFwdRows = 32, kBwdRows = 16;
+
+template <int K, int NO, bool RELU>
+__global__ void __launch_bounds__(256) k_linear(uint32_t n, const float* __restrict__ X,
+                                                const __nv_bfloat16* __restrict__ W, const float* __restrict__ bias,
+                                                float* __restrict__ Y, float* __restrict__ pre)
+{
+    constexpr int ROWS = kFwdRows, TPR = 256 / ROWS, CPT = NO / TPR;
+    __shared__ float Ws[K][NO + 1];
+    __shared__ float Xs[ROWS][K + 1];
+    for (int t = threadIdx.x; t < K * NO; t += blockDim.x)
+    {
+        const int o = t / K, k = t % K;
+        Ws[k][o] = __bfloat162float(W[t]);
+    }
+    const uint32_t r0 = blockIdx.x * ROWS;
+    for (int t = threadIdx.x; t < ROWS * K; t += blockDim.x)
+    {
+        const int r = t / K, k = t % K;
+        Xs[r][k] = (r0 + r < n) ? X[(size_t)(r0 + r) * K + k] : 0.f;
+    }
+    __syncthreads();
+    const int r = threadIdx.x / TPR, cg = threadIdx.x % TPR;
+    float acc[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) acc[c] = bias ? bias[cg + c * TPR] : 0.f;
+#pragma unroll 8
+    for (int k = 0; k < K; ++k)
+    {
+        const float x = Xs[r][k];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] += x * Ws[k][cg + c * TPR];
+    }
+    if (r0 + r < n)
+    {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c)
+        {
+            const int o = cg + c * TPR;
+            if (pre) pre[(size_t)(r0 + r) * NO + o] = acc[c];
+            Y[(size_t)(r0 + r) * NO + o] = RELU ? fmaxf(acc[c], 0.f) : acc[c];
+        }
+    }
+}
+
+// dX (n x K) [+]= dY (n x NO) W (NO x K)
+template <int K, int NO>
+__global__ void __launch_bounds__(256) k_linear_bwd_data(uint32_t n, const float* __restrict__ dY,
+                                                         const __nv_bfloat16* __restrict__ W, float* __restrict__ dX,
+                                                         int accumulate)
+{
+    constexpr int ROWS = kBwdRows, TPR = 256 / ROWS, CPT = K / TPR;
+    __shared__ float Ws[NO][K + 1];
+    __shared__ float Ds[ROWS][NO + 1];
+    for (int t = threadIdx.x; t < K * NO; t += blockDim.x)
+    {
+        const int o = t / K, k = t % K;
+        Ws[o][k] = __bfloat162float(W[t]);
+    }
+    const uint32_t r0 = blockIdx.x * ROWS;
+    for (int t = threadIdx.x; t < ROWS * NO; t += blockDim.x)
+    {
+        const int r = t / NO, o = t % NO;
+        Ds[r][o] = (r0 + r < n) ? dY[(size_t)(r0 + r) * NO + o] : 0.f;
+    }
+    __syncthreads();
+    const int r = threadIdx.x / TPR, cg = threadIdx.x % TPR;
+    float acc[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) acc[c] = 0.f;
+#pragma unroll 8
+    for (int o = 0; o < NO; ++o)
+    {
+        const float d = Ds[r][o];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] += d * Ws[o][cg + c * TPR];
+    }
+    if (r0 + r < n)
+#pragma unroll
+        for (int c = 0; c < CPT; ++c)
+        {
+            const size_t idx = (size_t)(r0 + r) * K + cg + c * TPR;
+            dX[idx] = accumulate ? dX[idx] + acc[c] : acc[c];
+        }
+}
+
+// per-CTA partial of dW (NO x K) = dY^T X and db = sum dY over a row chunk
+template <int K, int NO>
+__global__ void __launch_bounds__(256) k_linear_bwd_weight(uint32_t n, uint32_t rows_per_cta, const float* __restrict__ dY,
+                                                           const float* __restrict__ X, float* __restrict__ partial)
+{
+    constexpr int PAIRS = NO * K, PPT = (PAIRS + 255) / 256, TILE = 32;
+    __shared__ float Ds[TILE][NO];
+    __shared__ float Xs[TILE][K];
+    float acc[PPT];
+    float bacc = 0.f;
+#pragma unroll
+    for (int q = 0; q < PPT; ++q) acc[q] = 0.f;
+    const uint32_t r_begin = blockIdx.x * rows_per_cta;
+    const uint32_t r_end = min(n, r_begin + rows_per_cta);
+    for (uint32_t t0 = r_begin; t0 < r_end; t0 += TILE)
+    {
+        __syncthreads();
+        for (int t = threadIdx.x; t < TILE * NO; t += blockDim.x)
+        {
+            const int rr = t / NO, o = t % NO;
+            Ds[rr][o] = (t0 + rr < r_end) ? dY[(size_t)(t0 + rr) * NO + o] : 0.f;
+        }
+        for (int t = threadIdx.x; t < TILE * K; t += blockDim.x)
+        {
+            const int rr = t / K, k = t % K;
+            Xs[rr][k] = (t0 + rr < r_end) ? X[(size_t)(t0 + rr) * K + k] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < PPT; ++q)
+        {
+            const int pr = threadIdx.x + q * 256;
+            if (pr < PAIRS)
+            {
+                const int o = pr / K, k = pr % K;
+                float a = acc[q];
+                for (int rr = 0; rr < TILE; ++rr) a += Ds[rr][o] * Xs[rr][k];
+                acc[q] = a;
+            }
+        }
+        if (threadIdx.x < NO)
+            for (int rr = 0; rr < TILE; ++rr) bacc += Ds[rr][threadIdx.x];
+    }
+    float* out = partial + (size_t)blockIdx.x * (PAIRS + NO);
+#pragma unroll
+    for (int q = 0; q < PPT; ++q)
+    {
+        const int pr = threadIdx.x + q * 256;
+        if (pr < PAIRS) out[pr] = acc[q];
+    }
+    if (threadIdx.x < NO) out[PAIRS + threadIdx.x] = bacc;
+}
+
+// out[j] (+)= sum over b of partial[b * stride + j], in block order
+__global__ void k_reduce_partials(uint32_t nblocks, uint32_t stride, uint32_t count, const float* __restrict__ partial,
+                                  float* __restrict__ out, int accumulate)
+{
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < count; j += gridDim.x * blockDim.x)
+    {
+        float s = 0.f;
+        for (uint32_t b = 0; b < nblocks; ++b) s += partial[(size_t)b * stride + j];
+        out[j] = accumulate ? out[j] + s : s;
+    }
+}
+
+// ------------------------------------------------------------ message passing
+
+// SM = [s | m] (n x 128).  pre_i = s_i + b + invdeg_i sum_j g_ij m_j ;  Hn = relu(pre) + H
+__global__ void __launch_bounds__(256) k_aggregate(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                                                   const float* __restrict__ EF, const float* __restrict__ invdeg,
+                                                   const float* __restrict__ SM, const __nv_bfloat16* __restrict__ Wl,
+                                                   const float* __restrict__ Hin, float* __restrict__ pre,
+                                                   float* __restrict__ Hout)
+{
+    // one warp per node, 2 channels per lane
+    __shared__ float wg[H][FE], bg[H], bl[H];
+    for (int t = threadIdx.x; t < H * FE; t += blockDim.x) wg[t / FE][t % FE] = __bfloat162float(Wl[L_WG + t]);
+    for (int t = threadIdx.x; t < H; t += blockDim.x)
+    {
+        bg[t] = __bfloat162float(Wl[L_BG + t]);
+        bl[t] = __bfloat162float(Wl[L_B + t]);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint32_t i = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (i >= n) return;
+    float a0 = 0.f, a1 = 0.f;
+    const int c0 = lane, c1 = lane + 32;
+    for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+    {
+        const uint32_t j = ci[p];
+        if (j == i) continue;
+        const float* e = EF + (size_t)p * FE;
+        const float e0 = e[0], e1 = e[1], e2 = e[2], e3 = e[3];
+        const float g0 = sigm(bg[c0] + wg[c0][0] * e0 + wg[c0][1] * e1 + wg[c0][2] * e2 + wg[c0][3] * e3);
+        const float g1 = sigm(bg[c1] + wg[c1][0] * e0 + wg[c1][1] * e1 + wg[c1][2] * e2 + wg[c1][3] * e3);
+        a0 += g0 * SM[(size_t)j * 2 * H + H + c0];
+        a1 += g1 * SM[(size_t)j * 2 * H + H + c1];
+    }
+    const float id = invdeg[i];
+    const float p0 = SM[(size_t)i * 2 * H + c0] + bl[c0] + id * a0;
+    const float p1 = SM[(size_t)i * 2 * H + c1] + bl[c1] + id * a1;
+    pre[(size_t)i * H + c0] = p0;
+    pre[(size_t)i * H + c1] = p1;
+    Hout[(size_t)i * H + c0] = fmaxf(p0, 0.f) + Hin[(size_t)i * H + c0];
+    Hout[(size_t)i * H + c1] = fmaxf(p1, 0.f) + Hin[(size_t)i * H + c1];
+}
+
+// backward of k_aggregate for one layer.
+//   dpre = dHout * (pre > 0);  dHin = dHout (residual, written here);
+//   dSM[:, :64] = dpre;  dSM[j, 64:] = sum_{i in N(j)} invdeg_i g_ij dpre_i
+//   per-CTA partials of dW_g (64x4), db_g (64), db (64)
+__global__ void __launch_bounds__(256) k_aggregate_bwd(uint32_t n, const uint32_t* __restrict__ rp,
+                                                       const uint32_t* __restrict__ ci, const uint32_t* __restrict__ rev,
+                                                       const float* __restrict__ EF, const float* __restrict__ invdeg,
+                                                       const float* __restrict__ SM, const __nv_bfloat16* __restrict__ Wl,
+                                                       const float* __restrict__ pre, const float* __restrict__ dHout,
+                                                       float* __restrict__ dSM, float* __restrict__ dHin,
+                                                       float* __restrict__ partial)
+{
+    __shared__ float wg[H][FE], bg[H];
+    __shared__ float pw[8][H][FE + 2];  // per warp: dW_g (4), db_g, db
+    for (int t = threadIdx.x; t < H * FE; t += blockDim.x) wg[t / FE][t % FE] = __bfloat162float(Wl[L_WG + t]);
+    for (int t = threadIdx.x; t < H; t += blockDim.x) bg[t] = __bfloat162float(Wl[L_BG + t]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int t = lane; t < H * (FE + 2); t += 32) pw[warp][t / (FE + 2)][t % (FE + 2)] = 0.f;
+    __syncthreads();
+    const uint32_t j = blockIdx.x * 8 + warp;
+    if (j < n)
+    {
+        for (int h = 0; h < 2; ++h)
+        {
+            const int c = lane + 32 * h;
+            const float dp = pre[(size_t)j * H + c] > 0.f ? dHout[(size_t)j * H + c] : 0.f;
+            dSM[(size_t)j * 2 * H + c] = dp;
+            dHin[(size_t)j * H + c] = dHout[(size_t)j * H + c];
+            pw[warp][c][FE + 1] += dp;
+            // gather over neighbours i of j: edge (i, j) at rev[p] in row i
+            float dm = 0.f;
+            for (uint32_t p = rp[j]; p < rp[j + 1]; ++p)
+            {
+                const uint32_t i = ci[p];
+                if (i == j) continue;
+                const uint32_t q = rev[p];
+                const float* e = EF + (size_t)q * FE;
+                const float z = bg[c] + wg[c][0] * e[0] + wg[c][1] * e[1] + wg[c][2] * e[2] + wg[c][3] * e[3];
+                const float g = sigm(z);
+                const float dpi = pre[(size_t)i * H + c] > 0.f ? dHout[(size_t)i * H + c] : 0.f;
+                const float w = invdeg[i] * dpi;
+                dm += w * g;
+            }
+            dSM[(size_t)j * 2 * H + H + c] = dm;
+            // gate gradient for the edges (j, k) of row j (owned by node j)
+            const float dpj = dp * invdeg[j];
+            for (uint32_t p = rp[j]; p < rp[j + 1]; ++p)
+            {
+                const uint32_t k = ci[p];
+                if (k == j) continue;
+                const float* e = EF + (size_t)p * FE;
+                const float z = bg[c] + wg[c][0] * e[0] + wg[c][1] * e[1] + wg[c][2] * e[2] + wg[c][3] * e[3];
+                const float g = sigm(z);
+                const float dz = dpj * SM[(size_t)k * 2 * H + H + c] * g * (1.f - g);
+                pw[warp][c][0] += dz * e[0];
+                pw[warp][c][1] += dz * e[1];
+                pw[warp][c][2] += dz * e[2];
+                pw[warp][c][3] += dz * e[3];
+                pw[warp][c][FE] += dz;
+            }
+        }
+    }
+    __syncthreads();
+    // fixed-order sum over the 8 warps, then one partial per CTA
+    float* out = partial + (size_t)blockIdx.x * (H * (FE + 2));
+    for (int t = threadIdx.x; t < H * (FE + 2); t += blockDim.x)
+    {
+        float s = 0.f;
+        for (int w = 0; w < 8; ++w) s += pw[w][t / (FE + 2)][t % (FE + 2)];
+        out[t] = s;
+    }
+}
+
+// ------------------------------------------------------------ output head
+
+__device__ __forceinline__ float head_edge(const float* P, const float* hi, const float* hj, const float* e)
+{
+    float c = P[OFF_OUT + O_BO];
+    for (int k = 0; k < H; ++k) c += P[OFF_OUT + O_U + k] * hi[k] + P[OFF_OUT + O_V + k] * hj[k];
+    for (int k = 0; k < FE; ++k) c += P[OFF_OUT + O_W + k] * e[k];
+    return c;
+}
+
+// Lv <- L0 * exp(s tanh c) on the pattern of L (rows with diagonal last).  The
+// head uses FP32 parameters (Pf) rounded to BF16 by the caller.  C receives c.
+__global__ void k_head(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lci,
+                       const uint32_t* __restrict__ Arp, const double* __restrict__ Adiag, const float* __restrict__ EF,
+                       const float* __restrict__ Hf, const float* __restrict__ Pf, const double* __restrict__ L0,
+                       double* __restrict__ Lv, float* __restrict__ C, double* __restrict__ diag_out)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const float* hi = Hf + (size_t)i * H;
+        for (uint32_t q = Lrp[i]; q < Lrp[i + 1]; ++q)
+        {
+            const uint32_t j = Lci[q];
+            float c;
+            if (j == i)
+            {
+                c = Pf[OFF_OUT + O_BD];
+                for (int k = 0; k < H; ++k) c += Pf[OFF_OUT + O_D + k] * hi[k];
+            }
+            else
+            {
+                const uint32_t pA = Arp[i] + (q - Lrp[i]);  // L row i is a prefix of A row i
+                c = head_edge(Pf, hi, Hf + (size_t)j * H, EF + (size_t)pA * FE);
+            }
+            C[q] = c;
+            double val = L0[q] * exp((double)(kScale * tanhf(c)));
+            if (j == i)
+            {
+                const double lo = 1e-3 * sqrt(fabs(Adiag[i]));
+                if (val < lo) val = lo;
+                if (diag_out) diag_out[i] = val;
+            }
+            Lv[q] = val;
+        }
+    }
+}
+
+// dc from dL~ : dc = dL * L~ * s (1 - tanh^2 c), 0 where the guard clamped
+__global__ void k_head_dc(uint32_t nnz, const double* __restrict__ dL, const double* __restrict__ Lv,
+                          const double* __restrict__ L0, const float* __restrict__ C, float* __restrict__ dC)
+{
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += gridDim.x * blockDim.x)
+    {
+        const float t = tanhf(C[q]);
+        const double expected = L0[q] * exp((double)(kScale * t));
+        const bool clamped = fabs(Lv[q] - expected) > 1e-12 * fabs(expected);
+        dC[q] = clamped ? 0.f : (float)(dL[q] * Lv[q] * kScale * (1.f - t * t));
+    }
+}
+
+// head backward: dH_i += sum_row dc_q u (+ dc_ii d) ; dH_j += sum_{col j} dc_q v ;
+// per-CTA partials of du, dv, dw, dbo, dd, dbd
+__global__ void __launch_bounds__(256) k_head_bwd(uint32_t n, const uint32_t* __restrict__ Lrp,
+                                                  const uint32_t* __restrict__ Lci, const uint32_t* __restrict__ Trp,
+                                                  const uint32_t* __restrict__ Tpos, const uint32_t* __restrict__ Arp,
+                                                  const float* __restrict__ EF, const float* __restrict__ Hf,
+                                                  const float* __restrict__ Pf, const float* __restrict__ dC,
+                                                  float* __restrict__ dH, float* __restrict__ partial)
+{
+    __shared__ float pw[8][O_SIZE];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int t = lane; t < O_SIZE; t += 32) pw[warp][t] = 0.f;
+    __syncwarp();
+    const uint32_t i = blockIdx.x * 8 + warp;
+    if (i < n)
+    {
+        for (int h = 0; h < 2; ++h)
+        {
+            const int c = lane + 32 * h;
+            float dh = 0.f;
+            const float hic = Hf[(size_t)i * H + c];
+            for (uint32_t q = Lrp[i]; q < Lrp[i + 1]; ++q)
+            {
+                const uint32_t j = Lci[q];
+                const float d = dC[q];
+                if (j == i)
+                {
+                    dh += d * Pf[OFF_OUT + O_D + c];
+                    pw[warp][O_D + c] += d * hic;
+                    if (c == 0) pw[warp][O_BD] += d;
+                }
+                else
+                {
+                    dh += d * Pf[OFF_OUT + O_U + c];
+                    pw[warp][O_U + c] += d * hic;
+                    pw[warp][O_V + c] += d * Hf[(size_t)j * H + c];
+                    if (c < FE) pw[warp][O_W + c] += d * EF[(size_t)(Arp[i] + (q - Lrp[i])) * FE + c];
+                    if (c == 0) pw[warp][O_BO] += d;
+                }
+            }
+            // column part: entries (k, i) with k > i, listed in row i of L^T
+            for (uint32_t t = Trp[i]; t < Trp[i + 1]; ++t) dh += dC[Tpos[t]] * Pf[OFF_OUT + O_V + c];
+            dH[(size_t)i * H + c] = dh;
+        }
+    }
+    __syncthreads();
+    float* out = partial + (size_t)blockIdx.x * O_SIZE;
+    for (int t = threadIdx.x; t < O_SIZE; t += blockDim.x)
+    {
+        float s = 0.f;
+        for (int w = 0; w < 8; ++w) s += pw[w][t];
+        out[t] = s;
+    }
+}
+
+// ------------------------------------------------------------ loss
+
+// u = L~^T w : u_j = L~_jj w_j + sum_{i>j} L~_ij w_i  (via L^T rows: Trp / Tpos)
+__global__ void k_ltmul(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Trp,
+                        const uint32_t* __restrict__ Tci, const uint32_t* __restrict__ Tpos,
+                        const double* __restrict__ Lv, const double* __restrict__ w, double* __restrict__ u)
+{
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        double s = Lv[Lrp[j + 1] - 1] * w[j];
+        for (uint32_t t = Trp[j]; t < Trp[j + 1]; ++t) s += Lv[Tpos[t]] * w[Tci[t]];
+        u[j] = s;
+    }
+}
+
+// v = L~ u - Aw ; acc += v.v
+__global__ void k_lmul_res(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lci,
+                           const double* __restrict__ Lv, const double* __restrict__ u, const double* __restrict__ Aw,
+                           double* __restrict__ v, double* out, double* partial, unsigned* counter)
+{
+    double acc[1] = {0.0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        double s = 0.0;
+        for (uint32_t q = Lrp[i]; q < Lrp[i + 1]; ++q) s += Lv[q] * u[Lci[q]];
+        const double vi = s - Aw[i];
+        v[i] = vi;
+        acc[0] += vi * vi;
+    }
+    if (grid_reduce_last<1>(acc, partial, counter))
+        if (threadIdx.x == 0) *out = acc[0];
+}
+
+// dL_q += scale (v_i u_j + w_i q_j)
+__global__ void k_dL(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lci,
+                     const double* __restrict__ v, const double* __restrict__ u, const double* __restrict__ w,
+                     const double* __restrict__ qv, const double* __restrict__ scale, double* __restrict__ dL)
+{
+    const double s = *scale;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (uint32_t q = Lrp[i]; q < Lrp[i + 1]; ++q)
+        {
+            const uint32_t j = Lci[q];
+            dL[q] += s * (v[i] * u[j] + w[i] * qv[j]);
+        }
+}
+
+// scale = 2 / (P ||Aw||^2), loss += ||v||^2 / (P ||Aw||^2)
+__global__ void k_loss_scale(const double* vv, const double* aw2, int nprobes, double* scale, double* loss)
+{
+    const double d = (*aw2 > 0 ? *aw2 : 1.0) * nprobes;
+    *scale = 2.0 / d;
+    *loss += *vv / d;
+}
+
+// Jacobi smoothing of a probe: w <- w - (2/3) D^-1 (A w)
+__global__ void k_jacobi_probe(uint32_t n, const double* __restrict__ Aw, const double* __restrict__ d,
+                               double* __restrict__ w)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        w[i] -= (2.0 / 3.0) * Aw[i] / d[i];
+}
+
+__global__ void k_normal(uint64_t seed, uint32_t n, double* __restrict__ w)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        auto mix = [](uint64_t z) {
+            z += 0x9E3779B97F4A7C15ull;
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            return z ^ (z >> 31);
+        };
+        const double u1 = ((mix(seed * 0x9E3779B97F4A7C15ull + 2ull * i) >> 11) + 1.0) * (1.0 / 9007199254740993.0);
+        const double u2 = (mix(seed * 0x9E3779B97F4A7C15ull + 2ull * i + 1) >> 11) * (1.0 / 9007199254740992.0);
+        w[i] = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+    }
+}
+
+// ------------------------------------------------------------ optimiser
+
+__global__ void k_adam(uint32_t np, float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2,
+                       __nv_bfloat16* __restrict__ pb)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x)
+    {
+        const float gk = g[k];
+        const float mk = b1 * m[k] + (1.f - b1) * gk;
+        const float vk = b2 * v[k] + (1.f - b2) * gk * gk;
+        m[k] = mk;
+        v[k] = vk;
+        const float pk = p[k] - lr * (mk / c1) / (sqrtf(vk / c2) + eps);
+        p[k] = pk;
+        pb[k] = __float2bfloat16(pk);
+    }
+}
+
+__global__ void k_to_bf16(uint32_t np, const float* __restrict__ p, __nv_bfloat16* __restrict__ pb,
+                          float* __restrict__ pr)
+{
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x)
+    {
+        pb[k] = __float2bfloat16(p[k]);
+        pr[k] = __bfloat162float(pb[k]);
+    }
+}
+
+__global__ void k_lt_positions(uint32_t n, const uint32_t* __restrict__ Trp, const uint32_t* __restrict__ Tci,
+                               const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lci,
+                               uint32_t* __restrict__ Tpos)
+{
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+        for (uint32_t t = Trp[j]; t < Trp[j + 1]; ++t)
+        {
+            const uint32_t i = Tci[t];
+            uint32_t lo = Lrp[i], hi = Lrp[i + 1];
+            while (lo < hi)
+            {
+                const uint32_t mid = (lo + hi) / 2;
+                if (Lci[mid] < j)
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            Tpos[t] = lo;
+        }
+}
+
+// dpre0 = dH0 * (pre0 > 0)
+__global__ void k_relu_mask(uint64_t n, const float* __restrict__ pre, const float* __restrict__ dH, float* __restrict__ d)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        d[i] = pre[i] > 0.f ? dH[i] : 0.f;
+}
+
+// reduced gate partials [c][0..3 dW_g, 4 db_g, 5 db] -> layer gradient layout
+__global__ void k_gate_grads(const float* __restrict__ red, float* __restrict__ gl)
+{
+    for (int c = threadIdx.x; c < H; c += blockDim.x)
+    {
+        for (int e = 0; e < FE; ++e) gl[L_WG + c * FE + e] = red[c * (FE + 2) + e];
+        gl[L_BG + c] = red[c * (FE + 2) + FE];
+        gl[L_B + c] = red[c * (FE + 2) + FE + 1];
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ network state
+
+struct Gnn
+{
+    DBuf<float> p;                 // FP32 master parameters
+    DBuf<__nv_bfloat16> pb;        // BF16 copy (forward)
+    DBuf<float> pr;                // BF16-rounded values as FP32 (head)
+    DBuf<float> m, v, g;           // Adam moments, gradient
+    int step = 0;
+
+    void init(b2s_ctx* ctx, uint64_t seed)
+    {
+        p.alloc(NPARAM);
+        pb.alloc(NPARAM);
+        pr.alloc(NPARAM);
+        m.alloc(NPARAM);
+        v.alloc(NPARAM);
+        g.alloc(NPARAM);
+        std::vector<float> h(NPARAM, 0.f);
+        uint64_t s = seed * 0x9E3779B97F4A7C15ull + 12345;
+        auto rnd = [&]() {
+            s += 0x9E3779B97F4A7C15ull;
+            uint64_t z = s;
+            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+            z ^= z >> 31;
+            return (float)((z >> 11) * (1.0 / 9007199254740992.0)) * 2.f - 1.f;
+        };
+        const float sin_ = std::sqrt(6.f / (FIN + H)), sh = std::sqrt(6.f / (2 * H)), sg = std::sqrt(6.f / (FE + H));
+        for (int k = 0; k < H * FIN; ++k) h[OFF_WIN + k] = sin_ * rnd();
+        for (int l = 0; l < NL; ++l)
+        {
+            float* L = &h[LAYER0 + l * L_SIZE];
+            for (int k = 0; k < H * H; ++k) L[L_WS + k] = 0.5f * sh * rnd();
+            for (int k = 0; k < H * H; ++k) L[L_WM + k] = 0.5f * sh * rnd();
+            for (int k = 0; k < H * FE; ++k) L[L_WG + k] = sg * rnd();
+        }
+        // output head zero: the untrained network returns IC(0)
+        set(ctx, h.data());
+    }
+    void set(b2s_ctx* ctx, const float* host)
+    {
+        h2d(ctx, p.p, host, NPARAM * sizeof(float));
+        B2S_CUDA(cudaMemsetAsync(m.p, 0, m.bytes(), ctx->stream));
+        B2S_CUDA(cudaMemsetAsync(v.p, 0, v.bytes(), ctx->stream));
+        step = 0;
+        refresh(ctx);
+    }
+    void refresh(b2s_ctx* ctx)
+    {
+        B2S_LAUNCH(ctx, k_to_bf16, stream_grid(ctx, NPARAM), kThreads, 0, (uint32_t)NPARAM, p.p, pb.p, pr.p);
+    }
+};
+
+// graph-derived state of one matrix + the activations of one forward pass
+struct GnnGraph
+{
+    uint32_t n = 0, nnz = 0;
+    DBuf<uint32_t> rev;
+    DBuf<float> F, EF, invdeg;
+    DBuf<float> Hs[NL + 1], SM[NL], pre[NL], pre0;
+    DBuf<double> logd;
+
+    void build(b2s_ctx* ctx, const CsrDev& A)
+    {
+        n = A.n;
+        nnz = A.nnz;
+        rev.alloc(nnz ? nnz : 1);
+        DBuf<int> nonsym(1);
+        B2S_CUDA(cudaMemsetAsync(nonsym.p, 0, sizeof(int), ctx->stream));
+        B2S_LAUNCH(ctx, k_rev, stream_grid(ctx, n), kThreads, 0, n, A.rp.p, A.ci.p, rev.p, nonsym.p);
+        int h = 0;
+        d2h(ctx, &h, nonsym.p, sizeof(int));
+        sync(ctx);
+        if (h) fail(B2S_UNSUPPORTED, "learned IC(0) needs a structurally symmetric matrix");
+        F.alloc((size_t)n * FIN);
+        EF.alloc((size_t)nnz * FE);
+        B2S_CUDA(cudaMemsetAsync(EF.p, 0, EF.bytes(), ctx->stream));
+        invdeg.alloc(n);
+        logd.alloc(1);
+        reserve_reduction(ctx, stream_grid(ctx, n));
+        B2S_LAUNCH(ctx, k_logdiag_sum, stream_grid(ctx, n), kThreads, 0, n, A.diag.p, logd.p, ctx->partial.p,
+                   ctx->counter.p);
+        double mean = 0;
+        d2h(ctx, &mean, logd.p, sizeof(double));
+        sync(ctx);
+        B2S_LAUNCH(ctx, k_features, stream_grid(ctx, n), kThreads, 0, n, A.rp.p, A.ci.p, A.v.p, A.diag.p, mean, F.p,
+                   EF.p, invdeg.p);
+        for (int l = 0; l <= NL; ++l) Hs[l].alloc((size_t)n * H);
+        for (int l = 0; l < NL; ++l)
+        {
+            SM[l].alloc((size_t)n * 2 * H);
+            pre[l].alloc((size_t)n * H);
+        }
+        pre0.alloc((size_t)n * H);
+    }
+
+    void forward(b2s_ctx* ctx, const Gnn& net, const CsrDev& A)
+    {
+        const unsigned g64 = (n + kFwdRows - 1) / kFwdRows, gw = (n + 7) / 8;
+        B2S_LAUNCH(ctx, (k_linear<FIN, H, true>), g64, 256, 0, n, F.p, net.pb.p + OFF_WIN, net.pr.p + OFF_BIN, Hs[0].p,
+                   pre0.p);
+        for (int l = 0; l < NL; ++l)
+        {
+            const __nv_bfloat16* Wl = net.pb.p + LAYER0 + l * L_SIZE;
+            // [W_s ; W_m] are contiguous: one 128 x 64 weight
+            B2S_LAUNCH(ctx, (k_linear<H, 2 * H, false>), g64, 256, 0, n, Hs[l].p, Wl + L_WS, (const float*)nullptr,
+                       SM[l].p, (float*)nullptr);
+            B2S_LAUNCH(ctx, k_aggregate, gw, 256, 0, n, A.rp.p, A.ci.p, EF.p, invdeg.p, SM[l].p, Wl, Hs[l].p,
+                       pre[l].p, Hs[l + 1].p);
+        }
+    }
+};
+
+// IC(0) factor values -> corrected values (inference)
+struct LearnedCorrection final : Ic0Correction
+{
+    const Gnn* net;
+    explicit LearnedCorrection(const Gnn* g) : net(g) {}
+    void correct(b2s_ctx* ctx, const CsrDev& A, const uint32_t* Lrp, const uint32_t* Lci, uint32_t Lnnz, double* Lv,
+                 double* diag) override
+    {
+        GnnGraph G;
+        G.build(ctx, A);
+        G.forward(ctx, *net, A);
+        DBuf<double> L0(Lnnz ? Lnnz : 1);
+        d2d(ctx, L0.p, Lv, Lnnz * sizeof(double));
+        DBuf<float> C(Lnnz ? Lnnz : 1);
+        B2S_LAUNCH(ctx, k_head, stream_grid(ctx, A.n), kThreads, 0, A.n, Lrp, Lci, A.rp.p, A.diag.p, G.EF.p,
+                   G.Hs[NL].p, net->pr.p, L0.p, Lv, C.p, diag);
+        sync(ctx);
+    }
+};
+
+}  // namespace b2s
+
+// ------------------------------------------------------------ learner handle
+
+struct b2s_learner
+{
+    b2s_ctx* ctx = nullptr;
+    b2s::Gnn net;
+};
+
+namespace b2s {
+
+static const char kMagic[8] = {'B', '2', 'S', 'L', 'R', 'N', '0', '1'};
+
+static uint64_t fnv1a(const void* data, size_t bytes)
+{
+    const unsigned char* p = static_cast<const unsigned char*>(data);
+    uint64_t h = 1469598103934665603ull;
+    for (size_t i = 0; i < bytes; ++i)
+    {
+        h ^= p[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+static void load_weights(b2s_ctx* ctx, Gnn& net, const char* path)
+{
+    std::ifstream f(path, std::ios::binary);
+    if (!f) fail(B2S_INVALID_ARG, std::string("cannot open weight file ") + path);
+    char magic[8];
+    uint32_t ver = 0, count = 0;
+    f.read(magic, 8);
+    f.read(reinterpret_cast<char*>(&ver), 4);
+    f.read(reinterpret_cast<char*>(&count), 4);
+    if (!f || std::memcmp(magic, kMagic, 8) != 0 || ver != 1 || count != (uint32_t)NPARAM)
+        fail(B2S_INVALID_ARG, std::string("not a learned IC(0) weight file: ") + path);
+    std::vector<float> h(NPARAM);
+    uint64_t sum = 0;
+    f.read(reinterpret_cast<char*>(h.data()), NPARAM * sizeof(float));
+    f.read(reinterpret_cast<char*>(&sum), 8);
+    if (!f || sum != fnv1a(h.data(), NPARAM * sizeof(float)))
+        fail(B2S_INVALID_ARG, std::string("weight file checksum mismatch: ") + path);
+    net.set(ctx, h.data());
+}
+
+// default weights shipped next to the library: <dir of libb2s.so>/weights/learned_ic0.bin
+static std::string default_weight_path()
+{
+    Dl_info info;
+    if (dladdr(reinterpret_cast<void*>(&default_weight_path), &info) && info.dli_fname)
+    {
+        std::string p(info.dli_fname);
+        const size_t s = p.rfind('/');
+        return (s == std::string::npos ? std::string(".") : p.substr(0, s)) + "/weights/learned_ic0.bin";
+    }
+    return "";
+}
+
+static void save_weights(b2s_ctx* ctx, const Gnn& net, const char* path)
+{
+    std::vector<float> h(NPARAM);
+    d2h(ctx, h.data(), net.p.p, NPARAM * sizeof(float));
+    sync(ctx);
+    std::ofstream f(path, std::ios::binary);
+    if (!f) fail(B2S_INVALID_ARG, std::string("cannot write ") + path);
+    const uint32_t ver = 1, count = NPARAM;
+    const uint64_t sum = fnv1a(h.data(), NPARAM * sizeof(float));
+    f.write(kMagic, 8);
+    f.write(reinterpret_cast<const char*>(&ver), 4);
+    f.write(reinterpret_cast<const char*>(&count), 4);
+    f.write(reinterpret_cast<const char*>(h.data()), NPARAM * sizeof(float));
+    f.write(reinterpret_cast<const char*>(&sum), 8);
+    if (!f) fail(B2S_INVALID_ARG, std::string("write failed: ") + path);
+}
+
+std::unique_ptr<PcImpl> make_pc_learned_with(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o, const Gnn& net)
+{
+    LearnedCorrection corr(&net);
+    b2s_pc_opts oo = o;
+    return make_pc_ic0_ex(ctx, A, oo, &corr);
+}
+
+std::unique_ptr<PcImpl> make_pc_learned_ic0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o)
+{
+    Gnn net;
+    net.init(ctx, 0);
+    std::string path = o.learned_weights ? std::string(o.learned_weights) : default_weight_path();
+    if (!path.empty())
+    {
+        std::ifstream probe(path, std::ios::binary);
+        if (probe.good() || o.learned_weights) load_weights(ctx, net, path.c_str());
+    }
+    return make_pc_learned_with(ctx, A, o, net);
+}
+
+// ------------------------------------------------------------ one training step
+
+struct TrainBuffers
+{
+    DBuf<double> w, Aw, u, vres, qv, dL, scal;  // scal: [vv, aw2, scale, loss]
+};
+
+static void train_step(b2s_ctx* ctx, Gnn& net, const CsrDev& A, int nprobes, uint64_t seed, const double* host_probes,
+                       double lr, bool update, double* loss_out, float* grad_out)
+{
+    need(nprobes > 0 && nprobes <= 64, B2S_INVALID_ARG, "nprobes must be 1..64");
+    const uint32_t n = A.n;
+    // base IC(0) factor (FP64), its L^T structure
+    b2s_pc_opts o;
+    b2s_pc_opts_default(&o);
+    auto base = make_pc_ic0(ctx, A, o);
+    uint64_t sz[3];
+    base->export_data(ctx, "ic0.L", sz, nullptr, nullptr, nullptr);
+    const uint32_t Lnnz = (uint32_t)sz[1];
+    std::vector<uint32_t> hLrp(n + 1), hLci(Lnnz);
+    std::vector<double> hL0(Lnnz);
+    base->export_data(ctx, "ic0.L", sz, hLrp.data(), hLci.data(), hL0.data());
+    base->export_data(ctx, "ic0.LT", sz, nullptr, nullptr, nullptr);
+    const uint32_t Tnnz = (uint32_t)sz[1];
+    std::vector<uint32_t> hTrp(n + 1), hTci(Tnnz ? Tnnz : 1);
+    std::vector<double> hTv(Tnnz ? Tnnz : 1);
+    base->export_data(ctx, "ic0.LT", sz, hTrp.data(), hTci.data(), hTv.data());
+    auto Lrp = upload(ctx, hLrp.data(), n + 1), Lci = upload(ctx, hLci.data(), Lnnz);
+    auto L0 = upload(ctx, hL0.data(), Lnnz);
+    auto Trp = upload(ctx, hTrp.data(), n + 1), Tci = upload(ctx, hTci.data(), hTci.size());
+    DBuf<uint32_t> Tpos(hTci.size());
+    B2S_LAUNCH(ctx, k_lt_positions, stream_grid(ctx, n), kThreads, 0, n, Trp.p, Tci.p, Lrp.p, Lci.p, Tpos.p);
+
+    GnnGraph G;
+    G.build(ctx, A);
+    G.forward(ctx, net, A);
+    DBuf<double> Lv(Lnnz), dL(Lnnz);
+    DBuf<float> C(Lnnz), dC(Lnnz);
+    B2S_LAUNCH(ctx, k_head, stream_grid(ctx, n), kThreads, 0, n, Lrp.p, Lci.p, A.rp.p, A.diag.p, G.EF.p, G.Hs[NL].p,
+               net.pr.p, L0.p, Lv.p, C.p, (double*)nullptr);
+    B2S_CUDA(cudaMemsetAsync(dL.p, 0, dL.bytes(), ctx->stream));
+
+    TrainBuffers T;
+    T.w.alloc(n);
+    T.Aw.alloc(n);
+    T.u.alloc(n);
+    T.vres.alloc(n);
+    T.qv.alloc(n);
+    T.scal.alloc(4);
+    B2S_CUDA(cudaMemsetAsync(T.scal.p, 0, T.scal.bytes(), ctx->stream));
+    const unsigned gn = stream_grid(ctx, n);
+    reserve_reduction(ctx, gn);
+    for (int k = 0; k < nprobes; ++k)
+    {
+        if (host_probes)
+            h2d(ctx, T.w.p, host_probes + (size_t)k * n, n * sizeof(double));
+        else
+        {
+            B2S_LAUNCH(ctx, k_normal, gn, kThreads, 0, seed * 131 + k, n, T.w.p);
+            if (k % 2 == 1)
+                for (int s = 0; s < 10; ++s)
+                {
+                    spmv(ctx, A, T.w.p, T.Aw.p);
+                    B2S_LAUNCH(ctx, k_jacobi_probe, gn, kThreads, 0, n, T.Aw.p, A.diag.p, T.w.p);
+                }
+        }
+        spmv(ctx, A, T.w.p, T.Aw.p);
+        dot_dev(ctx, n, T.Aw.p, T.Aw.p, T.scal.p + 1);
+        B2S_LAUNCH(ctx, k_ltmul, gn, kThreads, 0, n, Lrp.p, Trp.p, Tci.p, Tpos.p, Lv.p, T.w.p, T.u.p);
+        B2S_LAUNCH(ctx, k_lmul_res, gn, kThreads, 0, n, Lrp.p, Lci.p, Lv.p, T.u.p, T.Aw.p, T.vres.p, T.scal.p,
+                   ctx->partial.p, ctx->counter.p);
+        B2S_LAUNCH(ctx, k_loss_scale, 1, 1, 0, T.scal.p, T.scal.p + 1, nprobes, T.scal.p + 2, T.scal.p + 3);
+        B2S_LAUNCH(ctx, k_ltmul, gn, kThreads, 0, n, Lrp.p, Trp.p, Tci.p, Tpos.p, Lv.p, T.vres.p, T.qv.p);
+        B2S_LAUNCH(ctx, k_dL, gn, kThreads, 0, n, Lrp.p, Lci.p, T.vres.p, T.u.p, T.w.p, T.qv.p, T.scal.p + 2, dL.p);
+    }
+    B2S_LAUNCH(ctx, k_head_dc, stream_grid(ctx, Lnnz), kThreads, 0, Lnnz, dL.p, Lv.p, L0.p, C.p, dC.p);
+
+    // backward
+    const unsigned gw = (n + 7) / 8, g64 = (n + kBwdRows - 1) / kBwdRows;
+    B2S_CUDA(cudaMemsetAsync(net.g.p, 0, net.g.bytes(), ctx->stream));
+    DBuf<float> dH(n * (size_t)H), dH2(n * (size_t)H), dSM(n * (size_t)2 * H), part;
+    part.alloc((size_t)std::max<unsigned>(gw, 1) * (H * (FE + 2) > O_SIZE ? H * (FE + 2) : O_SIZE) + 16);
+    B2S_LAUNCH(ctx, k_head_bwd, gw, 256, 0, n, Lrp.p, Lci.p, Trp.p, Tpos.p, A.rp.p, G.EF.p, G.Hs[NL].p, net.pr.p,
+               dC.p, dH.p, part.p);
+    B2S_LAUNCH(ctx, k_reduce_partials, 1, 256, 0, gw, (uint32_t)O_SIZE, (uint32_t)O_SIZE, part.p, net.g.p + OFF_OUT, 0);
+    const uint32_t rows_per = 2048;
+    const unsigned gwb = (n + rows_per - 1) / rows_per;
+    DBuf<float> wpart((size_t)gwb * (2 * H * H + 2 * H) + 16), red(H * (FE + 2));
+    for (int l = NL - 1; l >= 0; --l)
+    {
+        const __nv_bfloat16* Wl = net.pb.p + LAYER0 + l * L_SIZE;
+        float* gl = net.g.p + LAYER0 + l * L_SIZE;
+        // dH (wrt H_{l+1}) -> dpre, dSM, residual into dH2
+        B2S_LAUNCH(ctx, k_aggregate_bwd, gw, 256, 0, n, A.rp.p, A.ci.p, G.rev.p, G.EF.p, G.invdeg.p, G.SM[l].p, Wl,
+                   G.pre[l].p, dH.p, dSM.p, dH2.p, part.p);
+        // per-CTA gate partials -> ordered sum -> layer layout
+        B2S_LAUNCH(ctx, k_reduce_partials, 2, 256, 0, gw, (uint32_t)(H * (FE + 2)), (uint32_t)(H * (FE + 2)), part.p,
+                   red.p, 0);
+        B2S_LAUNCH(ctx, k_gate_grads, 1, 64, 0, red.p, gl);
+        // weights [W_s; W_m] (128 x 64): dW = dSM^T H_l ; dH_l += dSM W
+        B2S_LAUNCH(ctx, (k_linear_bwd_weight<H, 2 * H>), gwb, 256, 0, n, rows_per, dSM.p, G.Hs[l].p, wpart.p);
+        B2S_LAUNCH(ctx, k_reduce_partials, 64, 256, 0, gwb, (uint32_t)(2 * H * H + 2 * H), (uint32_t)(2 * H * H),
+                   wpart.p, gl + L_WS, 0);
+        B2S_LAUNCH(ctx, (k_linear_bwd_data<H, 2 * H>), g64, 256, 0, n, dSM.p, Wl + L_WS, dH2.p, 1);
+        std::swap(dH, dH2);
+    }
+    // input layer: dpre0 = dH0 * (pre0 > 0) ; dW_in = dpre0^T F ; db_in
+    B2S_LAUNCH(ctx, k_relu_mask, stream_grid(ctx, (uint64_t)n * H), kThreads, 0, (uint64_t)n * H, G.pre0.p, dH.p,
+               dSM.p);
+    B2S_LAUNCH(ctx, (k_linear_bwd_weight<FIN, H>), gwb, 256, 0, n, rows_per, dSM.p, G.F.p, wpart.p);
+    B2S_LAUNCH(ctx, k_reduce_partials, 4, 256, 0, gwb, (uint32_t)(H * FIN + H), (uint32_t)(H * FIN + H), wpart.p,
+               net.g.p + OFF_WIN, 0);
+
+    double lossv = 0;
+    d2h(ctx, &lossv, T.scal.p + 3, sizeof(double));
+    if (grad_out) d2h(ctx, grad_out, net.g.p, NPARAM * sizeof(float));
+    sync(ctx);
+    if (loss_out) *loss_out = lossv;
+    if (update)
+    {
+        net.step += 1;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f - std::pow(b1, (float)net.step), c2 = 1.f - std::pow(b2, (float)net.step);
+        B2S_LAUNCH(ctx, k_adam, stream_grid(ctx, NPARAM), kThreads, 0, (uint32_t)NPARAM, net.p.p, net.g.p, net.m.p,
+                   net.v.p, (float)lr, b1, b2, 1e-8f, c1, c2, net.pb.p);
+        B2S_LAUNCH(ctx, k_to_bf16, stream_grid(ctx, NPARAM), kThreads, 0, (uint32_t)NPARAM, net.p.p, net.pb.p, net.pr.p);
+        sync(ctx);
+    }
+}
+
+}  // namespace b2s
+
+using namespace b2s;
+
+extern "C" {
+
+b2s_status b2s_learner_create(b2s_ctx* ctx, uint64_t seed, b2s_learner** out)
+{
+    if (!ctx || !out) return B2S_INVALID_ARG;
+    *out = nullptr;
+    b2s_learner* L = new b2s_learner();
+    L->ctx = ctx;
+    b2s_status st = guarded(ctx, [&] {
+        B2S_CUDA(cudaSetDevice(ctx->device));
+        L->net.init(ctx, seed);
+        sync(ctx);
+    });
+    if (st != B2S_OK)
+    {
+        delete L;
+        return st;
+    }
+    *out = L;
+    return B2S_OK;
+}
+
+b2s_status b2s_learner_destroy(b2s_learner* L)
+{
+    if (!L) return B2S_INVALID_ARG;
+    cudaSetDevice(L->ctx->device);
+    delete L;
+    return B2S_OK;
+}
+
+b2s_status b2s_learner_load(b2s_learner* L, const char* path)
+{
+    if (!L || !path) return B2S_INVALID_ARG;
+    return guarded(L->ctx, [&] { load_weights(L->ctx, L->net, path); sync(L->ctx); });
+}
+
+b2s_status b2s_learner_save(b2s_learner* L, const char* path)
+{
+    if (!L || !path) return B2S_INVALID_ARG;
+    return guarded(L->ctx, [&] { save_weights(L->ctx, L->net, path); });
+}
+
+b2s_status b2s_learner_params(b2s_learner* L, float* params, uint64_t* count, int set)
+{
+    if (!L || !count) return B2S_INVALID_ARG;
+    if (!params)
+    {
+        *count = NPARAM;
+        return B2S_OK;
+    }
+    if (*count != (uint64_t)NPARAM) return B2S_SHAPE;
+    return guarded(L->ctx, [&] {
+        if (set)
+            L->net.set(L->ctx, params);
+        else
+            d2h(L->ctx, params, L->net.p.p, NPARAM * sizeof(float));
+        sync(L->ctx);
+    });
+}
+
+b2s_status b2s_learner_step(b2s_ctx* ctx, b2s_learner* L, const b2s_csr* A, int nprobes, uint64_t seed,
+                            const double* probes, double lr, int update, double* loss, float* grad)
+{
+    if (!ctx || !L || !A) return B2S_INVALID_ARG;
+    return guarded(ctx, [&] {
+        need(A->d.n == A->d.m, B2S_SHAPE, "learned IC(0) needs a square matrix");
+        train_step(ctx, L->net, A->d, nprobes, seed, probes, lr, update != 0, loss, grad);
+    });
+}
+
+b2s_status b2s_pc_create_learned(b2s_ctx* ctx, const b2s_csr* A, b2s_learner* L, const b2s_pc_opts* opts,
+                                 b2s_pc** out)
+{
+    if (!ctx || !A || !L || !out) return B2S_INVALID_ARG;
+    *out = nullptr;
+    b2s_pc_opts o;
+    b2s_pc_opts_default(&o);
+    if (opts) o = *opts;
+    b2s_pc* pc = new b2s_pc();
+    pc->ctx = ctx;
+    pc->kind = B2S_PC_LEARNED_IC0;
+    pc->n = A->d.n;
+    b2s_status st = guarded(ctx, [&] {
+        need(A->d.n == A->d.m, B2S_SHAPE, "learned IC(0) needs a square matrix");
+        pc->impl = make_pc_learned_with(ctx, A->d, o, L->net);
+        sync(ctx);
+    });
+    if (st != B2S_OK)
+    {
+        delete pc;
+        return st;
+    }
+    *out = pc;
+    return B2S_OK;
+}
+
+}  // extern "C"

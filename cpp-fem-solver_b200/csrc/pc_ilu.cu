@@ -469,7 +469,7 @@ void ic0_factor_inplace(b2s_ctx* ctx, const LevelSchedule& s, const uint32_t* Lr
     check_err(ctx, err, what);
 }
 
-std::unique_ptr<PcImpl> make_pc_ic0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o)
+std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o, Ic0Correction* corr)
 {
     need(A.n == A.m, B2S_SHAPE, "IC(0) needs a square matrix");
     auto pc = std::make_unique<PcIC0>();
@@ -485,6 +485,7 @@ std::unique_ptr<PcImpl> make_pc_ic0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_
     pc->fwd.prepare(ctx, pc->L, true, false);
     pc->fwd.d64 = pc->diag.p;
     ic0_factor_inplace(ctx, pc->fwd.sched, pc->L.rp.p, pc->L.ci.p, pc->L.v.p, pc->diag.p, "IC(0) failed");
+    if (corr) corr->correct(ctx, A, pc->L.rp.p, pc->L.ci.p, pc->L.nnz, pc->L.v.p, pc->diag.p);
     transpose_strict(ctx, pc->L, pc->LT);
     pc->bwd.prepare(ctx, pc->LT, false, false);
     pc->y.alloc(A.n ? A.n : 1);
@@ -498,6 +499,11 @@ std::unique_ptr<PcImpl> make_pc_ic0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_
     }
     sync(ctx);
     return pc;
+}
+
+std::unique_ptr<PcImpl> make_pc_ic0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o)
+{
+    return make_pc_ic0_ex(ctx, A, o, nullptr);
 }
 
 // ------------------------------------------------------------ ILU(0)

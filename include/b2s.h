@@ -184,6 +184,34 @@ b2s_status b2s_pc_export(b2s_ctx* ctx, b2s_pc* pc, const char* what, uint64_t* s
  * match).  "amg" maps to B2S_PC_SA_AMG.  Unknown names: B2S_INVALID_ARG. */
 b2s_status b2s_pc_kind_from_name(int method, const char* name, b2s_pc_kind* kind);
 
+/* ------------------------------------------------------ learned IC(0) net
+ * A message-passing network over the graph of A (3 layers, 64 hidden,
+ * BF16 weights, FP32 accumulation) that corrects the IC(0) factor values on
+ * the unchanged pattern (no counterpart in the reference).  Training runs on
+ * the GPU with this library's own forward and backward kernels. */
+typedef struct b2s_learner b2s_learner;
+
+/* New network: hidden weights from `seed`, output layer zero (the untrained
+ * network reproduces IC(0)). */
+b2s_status b2s_learner_create(b2s_ctx* ctx, uint64_t seed, b2s_learner** out);
+b2s_status b2s_learner_destroy(b2s_learner* L);
+/* Weight file: "B2SLRN01", uint32 version 1, uint32 count, float[count],
+ * uint64 FNV-1a checksum of the floats. */
+b2s_status b2s_learner_load(b2s_learner* L, const char* path);
+b2s_status b2s_learner_save(b2s_learner* L, const char* path);
+/* FP32 master parameters: get (set == 0) or set (set == 1); *count in/out. */
+b2s_status b2s_learner_params(b2s_learner* L, float* params, uint64_t* count, int set);
+/* One training step on A (SPD, structurally symmetric): loss
+ * mean_w ||(L~L~^T - A) w||^2 / ||A w||^2 over nprobes probes (generated from
+ * seed, every second one Jacobi-smoothed; or taken from `probes`, host,
+ * nprobes * n, when not NULL).  update = 1 applies one Adam step with
+ * learning rate lr.  loss and grad (host, count floats) are optional. */
+b2s_status b2s_learner_step(b2s_ctx* ctx, b2s_learner* L, const b2s_csr* A, int nprobes, uint64_t seed,
+                            const double* probes, double lr, int update, double* loss, float* grad);
+/* IC(0) corrected by this network (the same kernels as B2S_PC_LEARNED_IC0). */
+b2s_status b2s_pc_create_learned(b2s_ctx* ctx, const b2s_csr* A, b2s_learner* L, const b2s_pc_opts* opts,
+                                 b2s_pc** out);
+
 /* ----------------------------------------------------------------- solvers */
 
 typedef enum b2s_method
