@@ -212,26 +212,29 @@ def main():
         launches = ctx.kernel_launches - l0
         return e0.elapsed_time(e1), st, launches
 
-    def run(method, k_steps, warm):
+    timed_idx = list(range(args.warmup, args.warmup + args.steps))
+
+    def run(method, warm_idx):
+        """Warm-up solves on warm_idx, then one timed solve per timed system."""
+        for k in warm_idx:
+            timed_solve(*systems[k], method)
         ms, its, rel, launches = [], [], [], 0
-        for k in range(warm + k_steps):
-            n, rp, ci, v, b = systems[k % len(systems)]
-            t, st, nl = timed_solve(n, rp, ci, v, b, method)
-            if k >= warm:
-                ms.append(t)
-                its.append(st["iterations"])
-                rel.append(st["relres_true"])
-                launches += nl
+        for k in timed_idx:
+            t, st, nl = timed_solve(*systems[k], method)
+            ms.append(t)
+            its.append(st["iterations"])
+            rel.append(st["relres_true"])
+            launches += nl
         return ms, its, rel, launches
 
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        head_ms, head_its, head_rel, launches = run(args.method, args.steps, args.warmup)
+        head_ms, head_its, head_rel, launches = run(args.method, range(args.warmup))
     torch.cuda.synchronize()
     clocks = clk.summary()
-    base_ms, base_its, base_rel, _ = run("fp64_ic0", args.steps, 1) if args.method != "fp64_ic0" else (
+    base_ms, base_its, base_rel, _ = run("fp64_ic0", range(min(1, args.warmup))) if args.method != "fp64_ic0" else (
         head_ms, head_its, head_rel, 0)
 
     # e2e: host CSR + host b -> device, preconditioner, solve, x -> host (public C ABI, host pointers)

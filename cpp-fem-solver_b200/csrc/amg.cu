@@ -160,6 +160,58 @@ __global__ void k_aggregate(uint32_t nb, const uint32_t* __restrict__ sp, const 
     *nagg_out = (uint32_t)nagg;
 }
 
+// Standard three-phase smoothed-aggregation rule (no reference counterpart):
+// 1. a row whose strong neighbours are all free becomes a root and takes them
+// all; 2. a free row joins the phase-1 aggregate of its first aggregated
+// strong neighbour; 3. the remaining rows group with their free strong
+// neighbours.  One thread walks the rows in natural order (the phases are
+// order-dependent); snap holds the phase-1 aggregates.
+__global__ void k_aggregate_std(uint32_t nb, const uint32_t* __restrict__ sp, const uint32_t* __restrict__ sc,
+                                int32_t* __restrict__ agg, int32_t* __restrict__ snap, uint32_t* __restrict__ nagg_out)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    int32_t nagg = 0;
+    for (uint32_t i = 0; i < nb; ++i)
+    {
+        if (agg[i] != -1) continue;
+        const uint32_t a = __ldg(&sp[i]), b = __ldg(&sp[i + 1]);
+        bool free_all = true;
+        for (uint32_t p = a; p < b; ++p)
+            if (agg[__ldg(&sc[p])] != -1)
+            {
+                free_all = false;
+                break;
+            }
+        if (!free_all) continue;
+        agg[i] = nagg;
+        for (uint32_t p = a; p < b; ++p) agg[__ldg(&sc[p])] = nagg;
+        ++nagg;
+    }
+    for (uint32_t i = 0; i < nb; ++i) snap[i] = agg[i];
+    for (uint32_t i = 0; i < nb; ++i)
+    {
+        if (snap[i] != -1) continue;
+        for (uint32_t p = __ldg(&sp[i]); p < __ldg(&sp[i + 1]); ++p)
+        {
+            const int32_t g = snap[__ldg(&sc[p])];
+            if (g != -1)
+            {
+                agg[i] = g;
+                break;
+            }
+        }
+    }
+    for (uint32_t i = 0; i < nb; ++i)
+    {
+        if (agg[i] != -1) continue;
+        agg[i] = nagg;
+        for (uint32_t p = __ldg(&sp[i]); p < __ldg(&sp[i + 1]); ++p)
+            if (agg[__ldg(&sc[p])] == -1) agg[__ldg(&sc[p])] = nagg;
+        ++nagg;
+    }
+    *nagg_out = (uint32_t)nagg;
+}
+
 // ------------------------------------------------------------ prolongation
 
 // distinct aggregates among {agg[i]} U {agg[k] : k in row i}, ascending
@@ -655,6 +707,7 @@ struct PcAMG final : PcImpl
 {
     int bs = 1;
     bool ref_coarse = false;
+    bool ref_aggregation = false;
     std::vector<std::unique_ptr<Level>> lv;
     std::unique_ptr<BaijDev> fine_copy;  // BS=1 copy of a CSR operator
     DBuf<double> dense;
@@ -789,7 +842,14 @@ void build_hierarchy(b2s_ctx* ctx, PcAMG& pc, const BaijDev& A0, int max_levels,
         L->agg.alloc(n);
         B2S_CUDA(cudaMemsetAsync(L->agg.p, 0xFF, (size_t)n * sizeof(int32_t), ctx->stream));
         DBuf<uint32_t> nagg_d(1);
-        B2S_LAUNCH(ctx, k_aggregate, 1, 32, 0, n, sp.p, sc.p, L->agg.p, nagg_d.p);
+        if (pc.ref_aggregation)
+            B2S_LAUNCH(ctx, k_aggregate, 1, 32, 0, n, sp.p, sc.p, L->agg.p, nagg_d.p);
+        else
+        {
+            DBuf<int32_t> snap(n);
+            B2S_LAUNCH(ctx, k_aggregate_std, 1, 32, 0, n, sp.p, sc.p, L->agg.p, snap.p, nagg_d.p);
+            sync(ctx);
+        }
         uint32_t nagg = 0;
         d2h(ctx, &nagg, nagg_d.p, sizeof(uint32_t));
         sync(ctx);
@@ -855,6 +915,7 @@ std::unique_ptr<PcImpl> build_amg(b2s_ctx* ctx, const BaijDev& A, const b2s_pc_o
     auto pc = std::make_unique<PcAMG>();
     pc->bs = A.bs;
     pc->ref_coarse = o.amg_ref_coarse != 0;
+    pc->ref_aggregation = o.amg_aggregation != 0;
     pc->fine_copy = std::move(owned);
     const int max_levels = o.amg_max_levels > 0 ? o.amg_max_levels : 20;
     const uint32_t coarse_max = o.amg_coarse_max > 0 ? (uint32_t)o.amg_coarse_max : 50u;

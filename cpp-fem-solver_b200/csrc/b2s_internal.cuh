@@ -82,7 +82,16 @@ struct DBuf
     {
         release();
         n = count;
-        if (count) B2S_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        if (count)
+        {
+            const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+            if (e != cudaSuccess)
+            {
+                p = nullptr;
+                n = 0;
+                cuda_check(e, ("cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes").c_str());
+            }
+        }
     }
     // grows (never shrinks); contents are not preserved
     void reserve(size_t count)
@@ -101,7 +110,7 @@ struct DBuf
 // --------------------------------------------------------------- constants
 
 constexpr int kThreads = 256;          // block size of streaming / reduction kernels
-constexpr int kMaxRedValues = 4;       // values reduced together by one kernel
+constexpr int kMaxRedValues = 8;       // values reduced together by one kernel
 constexpr int kSpmvRowsPerCta = 256;   // staged SpMV: at most this many rows per CTA
 constexpr int kSpmvNnzPerCta = 3072;   // staged SpMV: nnz staged in shared memory per CTA
 
@@ -143,6 +152,8 @@ struct b2s_ctx
     b2s::KState* h_kstate = nullptr;  // pinned mirror
     double* h_scalar = nullptr;       // pinned, 64 doubles
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // device error word (B2S_TIMEOUT from a bounded wait); counter[32..]
+    int* errword() { return reinterpret_cast<int*>(counter.p + 32); }
 };
 
 namespace b2s {

@@ -95,8 +95,14 @@ b2s_status b2s_csr_create(b2s_ctx* ctx, uint32_t n, uint32_t m, const uint32_t* 
         d.h_ci.assign(col_idx, col_idx + nnz);
         d.h_v.assign(values, values + nnz);
         d.rp = upload(ctx, row_ptr, (size_t)n + 1);
-        d.ci = upload(ctx, col_idx, nnz);
-        d.v = upload(ctx, values, nnz);
+        // 8 elements of padding: the bulk copies of the SpMV start and end on
+        // 16-byte boundaries and may read a few elements past the last nonzero
+        d.ci.alloc((size_t)nnz + 8);
+        d.v.alloc((size_t)nnz + 8);
+        B2S_CUDA(cudaMemsetAsync(d.ci.p, 0, d.ci.bytes(), ctx->stream));
+        B2S_CUDA(cudaMemsetAsync(d.v.p, 0, d.v.bytes(), ctx->stream));
+        h2d(ctx, d.ci.p, col_idx, (size_t)nnz * sizeof(uint32_t));
+        h2d(ctx, d.v.p, values, (size_t)nnz * sizeof(double));
         std::vector<uint32_t> blk;
         build_row_blocks(row_ptr, n, 1, kSpmvRowsPerCta, kSpmvNnzPerCta, blk);
         d.nblk = (uint32_t)blk.size() - 1;

@@ -109,6 +109,7 @@ void b2s_pc_opts_default(b2s_pc_opts* o)
     o->amg_ref_coarse = 0;
     o->amg_max_levels = 0;
     o->amg_coarse_max = 0;
+    o->amg_aggregation = 0;
     o->learned_weights = nullptr;
 }
 

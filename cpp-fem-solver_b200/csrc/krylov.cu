@@ -697,6 +697,56 @@ struct BodyAxpyOne  // x += dz
     __device__ void last(const double*) const {}
 };
 
+// CGS2 pass: h_i = w . V_i for a group of up to 8 basis vectors (one pass over w)
+struct BodyGmDots
+{
+    static constexpr int NV = 8;
+    const double* w;
+    const double* V;
+    uint64_t pn;
+    int i0, cnt;
+    double* hbuf;  // this pass's h (64 entries)
+    KState* st;
+    GmSmall sm;
+    int pass;
+    __device__ void elem(uint64_t t, double* acc) const
+    {
+        const double wt = w[t];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (k < cnt) acc[k] += wt * V[(size_t)(i0 + k) * pn + t];
+    }
+    __device__ void last(const double* tot) const
+    {
+        const int j = gm_j(st);
+        for (int k = 0; k < cnt; ++k)
+        {
+            hbuf[i0 + k] = tot[k];
+            double& h = sm.H[(size_t)(i0 + k) * sm.m + j];
+            h = pass == 0 ? tot[k] : h + tot[k];
+        }
+    }
+};
+
+// w -= sum_i h_i V_i over i <= j (one pass)
+struct BodyGmUpdate
+{
+    static constexpr int NV = 0;
+    double* w;
+    const double* V;
+    uint64_t pn;
+    const double* hbuf;
+    const KState* st;
+    __device__ void elem(uint64_t t, double*) const
+    {
+        const int j = (int)st->aux[2];
+        double wt = w[t];
+        for (int i = 0; i <= j; ++i) wt -= hbuf[i] * V[(size_t)i * pn + t];
+        w[t] = wt;
+    }
+    __device__ void last(const double*) const {}
+};
+
 __global__ void k_gm_flag_to_int(const KState* st, int* flag)
 {
     // flag = 1 when the current cycle's inner loop must not run
@@ -941,6 +991,7 @@ static void run_gmres(Solve& S, const double* b, double* x, b2s_stats* stats, bo
     KState* st = S.st;
     const int* done = S.done;
     DBuf<int> gflag(1);
+    DBuf<double> hbuf((size_t)m + 8);
     auto Vj = [&](int j) { return V + pn * (size_t)j; };
     auto Zj = [&](int j) { return Z + pn * (size_t)j; };
 
@@ -971,9 +1022,23 @@ static void run_gmres(Solve& S, const double* b, double* x, b2s_stats* stats, bo
             else
                 copy(ctx, zin, Vj(j), n, g);
             S.A.apply(ctx, zin, w, g);
-            for (int i = 0; i <= j; ++i)
-                launch_vec(ctx, n, g, BodyGmMgs{w, i > 0 ? Vj(i - 1) : nullptr, Vj(i), st, sm, i});
-            launch_vec(ctx, n, g, BodyGmMgs{w, Vj(j), nullptr, st, sm, j + 1});
+            if (S.o.orth == B2S_ORTH_CGS2)
+            {
+                // classical Gram-Schmidt twice: batched dots, one update pass, repeated
+                for (int pass = 0; pass < 2; ++pass)
+                {
+                    for (int i0 = 0; i0 <= j; i0 += 8)
+                        launch_vec(ctx, n, g, BodyGmDots{w, V, pn, i0, std::min(8, j + 1 - i0), hbuf.p, st, sm, pass});
+                    launch_vec(ctx, n, g, BodyGmUpdate{w, V, pn, hbuf.p, st});
+                }
+                launch_vec(ctx, n, g, BodyGmMgs{w, nullptr, nullptr, st, sm, j + 1});
+            }
+            else
+            {
+                for (int i = 0; i <= j; ++i)
+                    launch_vec(ctx, n, g, BodyGmMgs{w, i > 0 ? Vj(i - 1) : nullptr, Vj(i), st, sm, i});
+                launch_vec(ctx, n, g, BodyGmMgs{w, Vj(j), nullptr, st, sm, j + 1});
+            }
             launch_vec(ctx, n, g, BodyGmNext{Vj(j + 1), w, st});
             B2S_LAUNCH(ctx, k_gm_advance, 1, 1, 0, st);
             if ((j + 1) % poll == 0 || j + 1 == m)

@@ -23,6 +23,7 @@
 #include <algorithm>
 
 #include "trisolve.cuh"
+#include "trsv_chunk.cuh"
 
 namespace b2s {
 
@@ -336,11 +337,17 @@ struct Tri
     const float* d32 = nullptr;
     LevelSchedule sched;
     SyncFree sf;
+    ChunkSchedule cs;
+    bool has_chunks = false;
 
-    template <typename Op>
-    void run(b2s_ctx* ctx, int mode, const Op& op, const int* done)
+    template <bool LOWER, bool UNIT, typename VT, typename XT, typename RT>
+    void run_t(b2s_ctx* ctx, int mode, const VT* v, const VT* d, const RT* rhs, XT* x, double* out64, const int* done)
     {
-        run_schedule(ctx, mode, sched, sf, op, done);
+        if (mode == B2S_TRSV_CHUNK && has_chunks && cs.smem_bytes<VT, XT, RT, UNIT>() > 0)
+            cs.run<LOWER, UNIT, VT, XT, RT>(ctx, m->rp.p, m->ci.p, v, d, rhs, x, out64, done);
+        else
+            run_schedule(ctx, mode == B2S_TRSV_LEVEL ? B2S_TRSV_LEVEL : B2S_TRSV_SYNCFREE, sched, sf,
+                         TrsvOp<LOWER, UNIT, VT, XT, RT>{m->rp.p, m->ci.p, v, d, rhs, x, out64}, done);
     }
 
     // x = T^-1 rhs; precision per the type parameters
@@ -348,16 +355,16 @@ struct Tri
     void solve(b2s_ctx* ctx, int mode, const VT* v, const VT* d, const RT* rhs, XT* x, double* out64, const int* done)
     {
         if (lower && unit)
-            run(ctx, mode, TrsvOp<true, true, VT, XT, RT>{m->rp.p, m->ci.p, v, d, rhs, x, out64}, done);
+            run_t<true, true, VT, XT, RT>(ctx, mode, v, d, rhs, x, out64, done);
         else if (lower)
-            run(ctx, mode, TrsvOp<true, false, VT, XT, RT>{m->rp.p, m->ci.p, v, d, rhs, x, out64}, done);
+            run_t<true, false, VT, XT, RT>(ctx, mode, v, d, rhs, x, out64, done);
         else if (unit)
-            run(ctx, mode, TrsvOp<false, true, VT, XT, RT>{m->rp.p, m->ci.p, v, d, rhs, x, out64}, done);
+            run_t<false, true, VT, XT, RT>(ctx, mode, v, d, rhs, x, out64, done);
         else
-            run(ctx, mode, TrsvOp<false, false, VT, XT, RT>{m->rp.p, m->ci.p, v, d, rhs, x, out64}, done);
+            run_t<false, false, VT, XT, RT>(ctx, mode, v, d, rhs, x, out64, done);
     }
 
-    void prepare(b2s_ctx* ctx, const Csr32& mat, bool lo, bool un)
+    void prepare(b2s_ctx* ctx, const Csr32& mat, bool lo, bool un, int mode)
     {
         m = &mat;
         lower = lo;
@@ -365,6 +372,15 @@ struct Tri
         n = mat.n;
         sched.build(ctx, n, mat.rp.p, mat.ci.p, lo);
         sf.init(ctx, n);
+        if (mode == B2S_TRSV_CHUNK && n)
+        {
+            std::vector<uint32_t> hrp(n + 1), hci(mat.nnz ? mat.nnz : 1);
+            d2h(ctx, hrp.data(), mat.rp.p, (n + 1) * sizeof(uint32_t));
+            d2h(ctx, hci.data(), mat.ci.p, mat.nnz * sizeof(uint32_t));
+            sync(ctx);
+            cs.build(ctx, n, hrp, hci, lo, un);
+            has_chunks = true;
+        }
     }
 };
 
@@ -380,7 +396,7 @@ static void to_f32(b2s_ctx* ctx, const DBuf<double>& a, DBuf<float>& b, uint64_t
     if (n) B2S_LAUNCH(ctx, k_f64_to_f32, stream_grid(ctx, n), kThreads, 0, a.p, b.p, n);
 }
 
-static int pick_trsv(const b2s_pc_opts& o) { return o.trsv == B2S_TRSV_LEVEL ? B2S_TRSV_LEVEL : B2S_TRSV_SYNCFREE; }
+static int pick_trsv(const b2s_pc_opts& o) { return o.trsv == B2S_TRSV_AUTO ? B2S_TRSV_CHUNK : o.trsv; }
 
 static void export_csr(b2s_ctx* ctx, const Csr32& m, uint64_t* sizes, uint32_t* rp, uint32_t* ci, double* v)
 {
@@ -482,12 +498,12 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     split(ctx, A, 0, pc->L, nullptr, err.p);
     check_err(ctx, err, "IC(0) failed");
     pc->diag.alloc(A.n ? A.n : 1);
-    pc->fwd.prepare(ctx, pc->L, true, false);
+    pc->fwd.prepare(ctx, pc->L, true, false, pc->mode);
     pc->fwd.d64 = pc->diag.p;
     ic0_factor_inplace(ctx, pc->fwd.sched, pc->L.rp.p, pc->L.ci.p, pc->L.v.p, pc->diag.p, "IC(0) failed");
     if (corr) corr->correct(ctx, A, pc->L.rp.p, pc->L.ci.p, pc->L.nnz, pc->L.v.p, pc->diag.p);
     transpose_strict(ctx, pc->L, pc->LT);
-    pc->bwd.prepare(ctx, pc->LT, false, false);
+    pc->bwd.prepare(ctx, pc->LT, false, false, pc->mode);
     pc->y.alloc(A.n ? A.n : 1);
     if (pc->fp32)
     {
@@ -569,7 +585,7 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     split(ctx, A, 1, pc->L, nullptr, err.p);
     split(ctx, A, 2, pc->U, pc->dix.p, err.p);
     check_err(ctx, err, "ILU(0) failed");
-    pc->fwd.prepare(ctx, pc->L, true, true);
+    pc->fwd.prepare(ctx, pc->L, true, true, pc->mode);
     // factor, level by level
     for (uint32_t l = 0; l < pc->fwd.sched.nlev; ++l)
     {
@@ -580,7 +596,7 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     check_err(ctx, err, "ILU(0) failed");
     pc->udiag.alloc(n ? n : 1);
     if (n) B2S_LAUNCH(ctx, k_gather_diag, stream_grid(ctx, n), kThreads, 0, n, pc->U.v.p, pc->dix.p, pc->udiag.p);
-    pc->bwd.prepare(ctx, pc->U, false, false);
+    pc->bwd.prepare(ctx, pc->U, false, false, pc->mode);
     pc->y.alloc(n ? n : 1);
     if (pc->fp32)
     {

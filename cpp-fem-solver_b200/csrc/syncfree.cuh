@@ -68,11 +68,12 @@ __global__ void __launch_bounds__(kThreads) k_syncfree(uint32_t n, const uint32_
     uint32_t row = 0;
     if (active) row = order ? __ldg(&order[pos]) : (reverse ? n - 1 - pos : pos);
     bool fin = !active;
-    unsigned spins = 0;
+    unsigned spins = 0, backoff = 32;
     for (;;)
     {
         const unsigned pending = __ballot_sync(0xffffffffu, !fin);
         if (!pending) break;
+        bool advanced = false;
         if (!fin)
         {
             if (op.ready(row, ctl.flags, epoch))
@@ -81,6 +82,7 @@ __global__ void __launch_bounds__(kThreads) k_syncfree(uint32_t n, const uint32_
                 __threadfence();
                 st_flag_release(&ctl.flags[row], epoch);
                 fin = true;
+                advanced = true;
             }
             else if (++spins > kMaxSpins)
             {
@@ -88,6 +90,15 @@ __global__ void __launch_bounds__(kThreads) k_syncfree(uint32_t n, const uint32_
                 st_flag_release(&ctl.flags[row], epoch);
                 fin = true;
             }
+        }
+        // a warp that made no progress backs off (bounded exponential sleep) so
+        // that waiting warps do not flood L2 with flag polls
+        if (__ballot_sync(0xffffffffu, advanced))
+            backoff = 32;
+        else
+        {
+            __nanosleep(backoff);
+            backoff = backoff < 1024 ? backoff * 2 : 1024;
         }
         __syncwarp();
     }

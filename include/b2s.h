@@ -138,7 +138,9 @@ typedef enum b2s_trsv
 {
     B2S_TRSV_AUTO = 0,
     B2S_TRSV_LEVEL = 1,    /* one launch per level of the dependency DAG */
-    B2S_TRSV_SYNCFREE = 2  /* one launch; rows wait on bounded per-row ready flags */
+    B2S_TRSV_SYNCFREE = 2, /* one launch; rows wait on bounded per-row ready flags */
+    B2S_TRSV_CHUNK = 3     /* one launch; row chunks staged in shared memory, local levels split by
+                              barriers, bounded flags between chunks (the AUTO choice) */
 } b2s_trsv;
 
 typedef struct b2s_pc_opts
@@ -150,6 +152,9 @@ typedef struct b2s_pc_opts
                             (blockMatrix.hpp:958-1000) bit for bit; 0: correct pivoted LU */
     int amg_max_levels;  /* 0: reference default 20 */
     int amg_coarse_max;  /* 0: reference default 50 block rows */
+    int amg_aggregation; /* 0: standard three-phase smoothed-aggregation rule (default);
+                            1: the reference's capped greedy rule (blockMatrix.hpp:1101-1111),
+                            which stalls on 3-D problems and serves parity tests */
     const char* learned_weights; /* B2S_PC_LEARNED_IC0: path of a weight file, NULL = built-in init */
 } b2s_pc_opts;
 

@@ -1336,7 +1336,7 @@ static void apply_bilu0(orc_pc* pc, const double* rhs, double* z)
 }
 
 /* ---------------- block SA-AMG (make_block_amg_preconditioner, blockMatrix.hpp:1051-1179) */
-static orc_pc* pc_amg(const orc_blk* A0, int exact, int* st, char* err, int errlen)
+static orc_pc* pc_amg(const orc_blk* A0, int exact, int std_agg, int* st, char* err, int errlen)
 {
     if (A0->nbr != A0->nbc)
     {
@@ -1385,25 +1385,73 @@ static orc_pc* pc_amg(const orc_blk* A0, int exact, int* st, char* err, int errl
             for (uint32_t p = cur->rp[i]; p < cur->rp[i + 1]; ++p)
                 if (cur->ci[p] != i && blk_fro(bs, &cur->v[(size_t)p * bv]) >= thr) sc[sp[i + 1]++] = cur->ci[p];
         }
-        /* 2. greedy aggregation, natural order, <= max_agg, blockMatrix.hpp:1101-1111 */
         int32_t* agg = L->agg = (int32_t*)xcalloc(n, 4);
         for (uint32_t i = 0; i < n; ++i) agg[i] = -1;
         int32_t nagg = 0;
-        for (uint32_t i = 0; i < n; ++i)
+        if (!std_agg)
         {
-            if (agg[i] != -1) continue;
-            agg[i] = nagg;
-            int sz = 1;
-            for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+            /* 2. greedy aggregation, natural order, <= max_agg, blockMatrix.hpp:1101-1111 */
+            for (uint32_t i = 0; i < n; ++i)
             {
-                const uint32_t j = sc[p];
-                if (agg[j] == -1 && sz < max_agg)
+                if (agg[i] != -1) continue;
+                agg[i] = nagg;
+                int sz = 1;
+                for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
                 {
-                    agg[j] = nagg;
-                    ++sz;
+                    const uint32_t j = sc[p];
+                    if (agg[j] == -1 && sz < max_agg)
+                    {
+                        agg[j] = nagg;
+                        ++sz;
+                    }
                 }
+                ++nagg;
             }
-            ++nagg;
+        }
+        else
+        {
+            /* standard smoothed-aggregation rule (no reference counterpart; the
+             * reference's capped greedy rule stalls on 3-D problems):
+             * 1. a row whose strong neighbours are all free becomes a root and
+             *    takes them all; 2. a free row joins the phase-1 aggregate of
+             *    its first aggregated strong neighbour; 3. the remaining rows
+             *    group with their free strong neighbours. */
+            for (uint32_t i = 0; i < n; ++i)
+            {
+                if (agg[i] != -1) continue;
+                int free_all = 1;
+                for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+                    if (agg[sc[p]] != -1)
+                    {
+                        free_all = 0;
+                        break;
+                    }
+                if (!free_all) continue;
+                agg[i] = nagg;
+                for (uint32_t p = sp[i]; p < sp[i + 1]; ++p) agg[sc[p]] = nagg;
+                ++nagg;
+            }
+            int32_t* snap = (int32_t*)xcalloc(n, 4);
+            memcpy(snap, agg, 4 * (size_t)n);
+            for (uint32_t i = 0; i < n; ++i)
+            {
+                if (snap[i] != -1) continue;
+                for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+                    if (snap[sc[p]] != -1)
+                    {
+                        agg[i] = snap[sc[p]];
+                        break;
+                    }
+            }
+            free(snap);
+            for (uint32_t i = 0; i < n; ++i)
+            {
+                if (agg[i] != -1) continue;
+                agg[i] = nagg;
+                for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+                    if (agg[sc[p]] == -1) agg[sc[p]] = nagg;
+                ++nagg;
+            }
         }
         free(sp);
         free(sc);
@@ -1712,7 +1760,7 @@ orc_pc* orc_pc_create(const orc_csr* A, const char* kind, double omega, int* st,
     if (!strcmp(kind, "ic0")) return pc_ic0(A, st, err, errlen);
     if (!strcmp(kind, "ilu0")) return pc_ilu0(A, st, err, errlen);
     if (!strcmp(kind, "ssor")) return pc_ssor(A, omega, st, err, errlen);
-    if (!strcmp(kind, "sa_amg") || !strcmp(kind, "sa_amg_exact"))
+    if (!strcmp(kind, "sa_amg") || !strcmp(kind, "sa_amg_exact") || !strcmp(kind, "sa_amg_std"))
     {
         if (A->n != A->m)
         {
@@ -1721,7 +1769,7 @@ orc_pc* orc_pc_create(const orc_csr* A, const char* kind, double omega, int* st,
             return NULL;
         }
         orc_blk* B = orc_blk_condense(1, A, A->n, A->m);
-        orc_pc* pc = pc_amg(B, !strcmp(kind, "sa_amg_exact"), st, err, errlen);
+        orc_pc* pc = pc_amg(B, strcmp(kind, "sa_amg") != 0, !strcmp(kind, "sa_amg_std"), st, err, errlen);
         if (pc)
             pc->owned_blk = B;
         else
@@ -1744,8 +1792,9 @@ orc_pc* orc_blk_pc_create(const orc_blk* A, const char* kind, int* st, char* err
         return pc;
     }
     if (!strcmp(kind, "ilu0")) return pc_bilu0(A, st, err, errlen);
-    if (!strcmp(kind, "amg")) return pc_amg(A, 0, st, err, errlen);
-    if (!strcmp(kind, "amg_exact")) return pc_amg(A, 1, st, err, errlen);
+    if (!strcmp(kind, "amg")) return pc_amg(A, 0, 0, st, err, errlen);
+    if (!strcmp(kind, "amg_exact")) return pc_amg(A, 1, 0, st, err, errlen);
+    if (!strcmp(kind, "amg_std")) return pc_amg(A, 1, 1, st, err, errlen);
     *st = ORC_INVALID_ARG;
     set_err(err, errlen, "unknown block preconditioner kind");
     return NULL;
@@ -2233,7 +2282,7 @@ static const char* resolve_precond(int method, const char* name)
     if (method != 2 && !strcmp(s, "incomplete_cholesky")) return "ic0";
     if (!strcmp(s, "ilu") || !strcmp(s, "ilu0")) return "ilu0";
     if (!strcmp(s, "sor") || !strcmp(s, "ssor")) return "ssor";
-    if (!strcmp(s, "amg")) return "sa_amg_exact";
+    if (!strcmp(s, "amg")) return "sa_amg_std";
     return NULL;
 }
 

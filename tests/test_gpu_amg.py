@@ -3,8 +3,10 @@
 With amg_ref_coarse=1 the whole hierarchy (aggregates, A, P, D^-1 on every
 level) and the V-cycle output equal the restatement bit for bit -- the
 restatement itself equals the compiled reference (tests/test_oracle_pin.py).
-The default coarse solve is a correct pivoted LU ("amg_exact" in the oracle),
-checked the same way; PCG with it converges where the reference's cannot."""
+The library default (standard three-phase aggregation + correct pivoted coarse
+LU, "amg_std" in the oracle) is checked the same way; PCG with it converges
+where the reference's capped greedy hierarchy stalls and blows up (32^3).
+The reference-rule modes are parity modes."""
 import numpy as np
 import pytest
 
@@ -21,16 +23,24 @@ def hier_cases(b2s):
     }
 
 
+MODES = {  # (amg_aggregation, amg_ref_coarse) -> oracle kind
+    "reference": (1, 1, "amg"),        # the reference's greedy rule and coarsest elimination
+    "ref_exact": (1, 0, "amg_exact"),  # reference greedy rule, correct coarsest LU
+    "standard": (0, 0, "amg_std"),     # the library default
+}
+
+
 @pytest.mark.parametrize("case", ["bs1_poisson2d", "bs3_mpi", "bs1_poisson3d"])
-@pytest.mark.parametrize("ref_coarse", [1, 0])
-def test_amg_hierarchy_and_vcycle(b2s, ctx, orc, case, ref_coarse):
+@pytest.mark.parametrize("mode", list(MODES))
+def test_amg_hierarchy_and_vcycle(b2s, ctx, orc, case, mode):
     bs, n, rp, ci, v = hier_cases(b2s)[case]
     Ao = orc.csr(n, n, rp, ci, v)
     Bo = orc.blk_condense(bs, Ao, n // bs, n // bs)
     brp, bci, bv = Bo.export()
     B = b2s.BAIJ(ctx, bs, n // bs, n // bs, brp, bci, bv)
-    M = b2s.Precond(ctx, B, b2s.PC_BSA_AMG, amg_ref_coarse=ref_coarse)
-    po = orc.blk_pc(Bo, "amg" if ref_coarse else "amg_exact")
+    aggm, ref_coarse, okind = MODES[mode]
+    M = b2s.Precond(ctx, B, b2s.PC_BSA_AMG, amg_ref_coarse=ref_coarse, amg_aggregation=aggm)
+    po = orc.blk_pc(Bo, okind)
     levels = orc.amg_export(po, bs)
     _, nrows, _ = M.export("amg.levels")
     assert list(nrows) == [lv["nrows"] for lv in levels]
@@ -51,7 +61,7 @@ def test_scalar_amg_string_is_sa(b2s, ctx, orc):
     n, rp, ci, v = b2s.gen_poisson3d(16)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
     M = b2s.Precond(ctx, A, b2s.pc_kind_from_name(b2s.PCG, "amg"))
-    po = orc.pc(orc.csr(n, n, rp, ci, v), "sa_amg_exact")
+    po = orc.pc(orc.csr(n, n, rp, ci, v), "sa_amg_std")
     r = b2s.uniform(8, n)
     assert np.array_equal(M.apply(r), po.apply(r))
 
@@ -63,7 +73,7 @@ def test_amg_pcg_converges(b2s, ctx, orc):
     M = b2s.Precond(ctx, A, b2s.PC_SA_AMG)
     x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-10, maxit=500)
     assert st["status"] == 0 and st["relres_true"] < 2e-10
-    xo, io = orc.solve_pc(orc.csr(n, n, rp, ci, v), 0, orc.pc(orc.csr(n, n, rp, ci, v), "sa_amg_exact"), b,
+    xo, io = orc.solve_pc(orc.csr(n, n, rp, ci, v), 0, orc.pc(orc.csr(n, n, rp, ci, v), "sa_amg_std"), b,
                           1e-10, 500)
     assert abs(st["it"] - io) <= 2
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-8

@@ -177,3 +177,30 @@ def test_graphs_match_eager(b2s, ctx):
     x1, s1 = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, use_graphs=1, check_every=8)
     x2, s2 = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, use_graphs=0, check_every=3)
     assert np.array_equal(x1, x2) and s1["it"] == s2["it"]
+
+
+@pytest.mark.parametrize("flexible", [False, True])
+def test_gmres_cgs2(b2s, ctx, orc, flexible):
+    """Classical Gram-Schmidt twice: same Krylov space as MGS, different rounding."""
+    n, rp, ci, v = P.convdiff2d(60)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(13, n)
+    M = b2s.Precond(ctx, A, b2s.PC_ILU0)
+    method = b2s.FGMRES if flexible else b2s.GMRES
+    x, st = b2s.solve(ctx, A, b, method, M, tol=1e-8, maxit=2000, restart=30, orth=b2s.ORTH_CGS2)
+    xo, io = orc.solve(orc.csr(n, n, rp, ci, v), 2, "ilu", b, 1e-8, 2000, 30)
+    assert abs(st["it"] - io) <= 2
+    assert rel(x, xo) < 1e-7
+    assert st["relres_true"] < 2e-8
+
+
+def test_fgmres_fp32_refinement(b2s, ctx):
+    """FP32 ILU(0) inside FP64 FGMRES with iterative refinement reaches 1e-10."""
+    n, rp, ci, v = b2s.gen_convdiff3d(24)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(14, n)
+    M = b2s.Precond(ctx, A, b2s.PC_ILU0, precision=b2s.FP32)
+    x, st = b2s.solve(ctx, A, b, b2s.FGMRES, M, tol=1e-10, maxit=500, restart=30, ir_steps=5, ir_inner_tol=1e-6)
+    assert st["relres_true"] < 1e-10
+    r = b - A.spmv(x)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10

@@ -23,7 +23,7 @@ def rel(a, b):
 
 
 @pytest.mark.parametrize("mat", list(MATS))
-@pytest.mark.parametrize("trsv", [1, 2])
+@pytest.mark.parametrize("trsv", [1, 2, 3])
 def test_ic0_bit_exact(b2s, ctx, orc, mat, trsv):
     n, rp, ci, v = MATS[mat](b2s)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
@@ -45,7 +45,7 @@ def test_ic0_bit_exact(b2s, ctx, orc, mat, trsv):
 
 
 @pytest.mark.parametrize("mat", ["poisson2d", "random", "poisson3d"])
-@pytest.mark.parametrize("trsv", [1, 2])
+@pytest.mark.parametrize("trsv", [1, 2, 3])
 def test_ilu0_bit_exact(b2s, ctx, orc, mat, trsv):
     n, rp, ci, v = MATS[mat](b2s) if mat != "poisson2d" else P.convdiff2d(40)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
@@ -66,7 +66,7 @@ def test_fp32_factor_apply(b2s, ctx, kind):
     k = b2s.PC_NAMES[kind]
     r = b2s.uniform(23, n)
     z64 = b2s.Precond(ctx, A, k).apply(r)
-    for trsv in (1, 2):
+    for trsv in (1, 2, 3):
         z32 = b2s.Precond(ctx, A, k, precision=b2s.FP32, trsv=trsv).apply(r)
         assert rel(z32, z64) < 1e-5
 
