@@ -237,13 +237,15 @@ __global__ void __launch_bounds__(kThreads) k_spmv_tma(const uint32_t* __restric
         const uint32_t p0 = __ldg(&rp[r0]), p1 = __ldg(&rp[r1]);
         if (p1 - p0 <= (uint32_t)kSpmvNnzPerCta)
         {
-            const double* V = sv[stage] - (p0 & ~1u);   // index with the global nnz position
-            const uint32_t* Cc = sc[stage] - (p0 & ~3u);
+            // staged copies start at the widened offsets a0 = p0 & ~1, c0 = p0 & ~3
+            const double* V = sv[stage];
+            const uint32_t* Cc = sc[stage];
+            const uint32_t a0 = p0 & ~1u, c0 = p0 & ~3u;
             for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x)
             {
                 const uint32_t a = __ldg(&rp[r]), e = __ldg(&rp[r + 1]);
                 double sum = 0.0;
-                for (uint32_t k = a; k < e; ++k) sum += V[k] * __ldg(&x[Cc[k]]);
+                for (uint32_t k = a; k < e; ++k) sum += V[k - a0] * __ldg(&x[Cc[k - c0]]);
                 epi.row(r, sum, acc);
             }
         }
