@@ -112,7 +112,7 @@ EXPORTS = [
     "b2s_solve_baij", "b2s_solve_baij_device", "b2s_gen_poisson2d", "b2s_gen_poisson3d", "b2s_gen_convdiff3d",
     "b2s_gen_elasticity_q1", "b2s_gen_grf_diffusion", "b2s_gen_uniform", "b2s_learner_create",
     "b2s_learner_destroy", "b2s_learner_load", "b2s_learner_save", "b2s_learner_params", "b2s_learner_step",
-    "b2s_pc_create_learned",
+    "b2s_pc_create_learned", "b2s_dot_noalloc",
 ]
 
 
@@ -184,6 +184,7 @@ def lib():
     f("b2s_learner_params", i32, vp, vp, C.POINTER(C.c_uint64), i32)
     f("b2s_learner_step", i32, vp, vp, vp, i32, u64, vp, f64, i32, C.POINTER(C.c_double), vp)
     f("b2s_pc_create_learned", i32, vp, vp, vp, C.POINTER(PcOpts), pp)
+    f("b2s_dot_noalloc", i32, vp, vp, u64, vp, vp)
     _lib = L
     return L
 

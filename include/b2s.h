@@ -103,6 +103,17 @@ b2s_status b2s_spmv_device(b2s_ctx* ctx, const b2s_csr* A, const double* d_x, do
 b2s_status b2s_dot(b2s_ctx* ctx, uint64_t n, const double* a, const double* b, double* out);
 b2s_status b2s_dot_device(b2s_ctx* ctx, uint64_t n, const double* d_a, const double* d_b, double* out);
 
+/* Dot product for callers that cannot allocate device memory (no reference
+ * counterpart): device pointers in and out, enqueued on `stream` (NULL = the
+ * default stream), no b2s context, no cudaMalloc / cudaFree -- the reduction
+ * scratch is a fixed 32 KiB __device__ array per device.  n above
+ * B2S_DOT_NOALLOC_MAX_N returns B2S_INVALID_ARG.  Every call shares that
+ * array: calls that overlap on the GPU race, so serialise them.  The first
+ * call on a device looks up the array's address (make it before any stream
+ * capture). */
+#define B2S_DOT_NOALLOC_MAX_N 8388608ull
+b2s_status b2s_dot_noalloc(const double* d_a, const double* d_b, uint64_t n, double* d_out, void* stream);
+
 /* BlockMatrix::matvec (blockMatrix.hpp:208-234); distributed_matvec
  * (blockMatrix.hpp:351-442) on one device-resident matrix is the same call. */
 b2s_status b2s_baij_matvec(b2s_ctx* ctx, const b2s_baij* A, const double* x, double* y);
