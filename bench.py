@@ -202,14 +202,17 @@ def main():
         flush.fill_(1.0)
         torch.cuda.synchronize()
         kind, prec = kinds[method]
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0, em, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         l0 = ctx.kernel_launches
         e0.record(stream)
         M = b2s.Precond(ctx, A, kind, precision=prec)
+        em.record(stream)
         st = b2s.solve_device(ctx, A, bt.data_ptr(), xt.data_ptr(), b2s.PCG, M, tol=TOL, maxit=MAXIT)
         e1.record(stream)
         e1.synchronize()
         launches = ctx.kernel_launches - l0
+        st["setup_ms_event"] = e0.elapsed_time(em)
+        st["iter_ms_event"] = em.elapsed_time(e1)
         return e0.elapsed_time(e1), st, launches
 
     timed_idx = list(range(args.warmup, args.warmup + args.steps))
@@ -218,13 +221,15 @@ def main():
         """Warm-up solves on warm_idx, then one timed solve per timed system."""
         for k in warm_idx:
             timed_solve(*systems[k], method)
-        ms, its, rel, launches = [], [], [], 0
+        ms, its, rel, launches, split = [], [], [], 0, []
         for k in timed_idx:
             t, st, nl = timed_solve(*systems[k], method)
             ms.append(t)
             its.append(st["iterations"])
             rel.append(st["relres_true"])
+            split.append((st["setup_ms_event"], st["iter_ms_event"]))
             launches += nl
+        run.split = split
         return ms, its, rel, launches
 
     if world > 1:
@@ -232,10 +237,12 @@ def main():
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         head_ms, head_its, head_rel, launches = run(args.method, range(args.warmup))
+    head_split = run.split
     torch.cuda.synchronize()
     clocks = clk.summary()
     base_ms, base_its, base_rel, _ = run("fp64_ic0", range(min(1, args.warmup))) if args.method != "fp64_ic0" else (
         head_ms, head_its, head_rel, 0)
+    base_split = run.split
 
     # e2e: host CSR + host b -> device, preconditioner, solve, x -> host (public C ABI, host pointers)
     e2e_ms, h2d, d2h = [], 0, 0
@@ -278,10 +285,10 @@ def main():
     tri_ms = e0.elapsed_time(e1) / reps / 2
     pk, pk_kind = peaks()
     achieved = tri_bytes / (tri_ms * 1e-3) / 1e9
-    roofline = {"kernel": "k_syncfree<TrsvOp> (IC(0) triangular solve)", "bound": "hbm",
+    roofline = {"kernel": "k_trsv_chunk (IC(0) triangular solve, one triangle per launch)", "bound": "hbm",
                 "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                 "peak_kind": pk_kind, "traffic": None, "bytes_per_launch": tri_bytes, "ms_per_launch": tri_ms,
-                "note": "latency-bound: 1023 dependency levels per triangle on the 512^2 grid"}
+                "note": "latency-bound: a 1023-level dependency chain per triangle on the 512^2 grid"}
 
     # C2 (3-D Poisson 128^3) CSR SpMV against the HBM roofline (inputs > L2)
     n3, rp3, ci3, v3 = b2s.gen_poisson3d(128)
@@ -298,7 +305,7 @@ def main():
     spmv_ms = e0.elapsed_time(e1) / 20
     spmv_bytes = 12 * len(v3) + 4 * (n3 + 1) + 16 * n3
     spmv_gbs = spmv_bytes / (spmv_ms * 1e-3) / 1e9
-    spmv = {"kernel": "k_spmv_staged", "workload": "poisson3d_128 (n=2097152, nnz=14581760)",
+    spmv = {"kernel": "k_spmv_warp", "workload": "poisson3d_128 (n=2097152, nnz=14581760)",
             "ms": spmv_ms, "achieved": spmv_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": spmv_gbs / pk["hbm_gbs"], "bytes_per_launch": spmv_bytes}
 
@@ -336,8 +343,12 @@ def main():
             "config": {"workload": "grf_diffusion_512 pcg rtol1e-8", "method": args.method, "grid": N_GRID,
                        "corr": CORR, "parallelism": f"replicas x{world}", "l2": "flushed (512 MB write) before every step"},
             "iterations_mean": float(np.mean(head_its)), "relres_true_max": float(np.max(head_rel)),
+            "setup_ms_mean": float(np.mean([a for a, _ in head_split])),
+            "iter_ms_mean": float(np.mean([b for _, b in head_split])),
             "fp64_ic0_pcg": {"ms": float(np.mean(base_ms)), "iterations_mean": float(np.mean(base_its)),
-                             "relres_true_max": float(np.max(base_rel))},
+                             "relres_true_max": float(np.max(base_rel)),
+                             "setup_ms_mean": float(np.mean([a for a, _ in base_split])),
+                             "iter_ms_mean": float(np.mean([b for _, b in base_split]))},
             "speedup_vs_fp64_ic0": float(np.mean(base_ms)) / value,
             "e2e": {"value": float(np.mean(e2e_ms)), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},

@@ -42,11 +42,10 @@ inline void cuda_check(cudaError_t e, const char* what)
 {
     if (e != cudaSuccess)
     {
-        if (e == cudaErrorMemoryAllocation)
-        {
-            cudaGetLastError();
-            fail(B2S_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
-        }
+        // clear the runtime's last-error state so a recoverable error is not
+        // reported again by the next launch check
+        cudaGetLastError();
+        if (e == cudaErrorMemoryAllocation) fail(B2S_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
         fail(B2S_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
     }
 }
@@ -379,6 +378,15 @@ DBuf<T> upload(b2s_ctx* ctx, const T* src, size_t count)
 {
     DBuf<T> b(count);
     h2d(ctx, b.p, src, count * sizeof(T));
+    return b;
+}
+
+// a device copy of a host vector; an empty vector gets one uninitialised element
+template <typename T>
+DBuf<T> upload(b2s_ctx* ctx, const std::vector<T>& src)
+{
+    DBuf<T> b(src.empty() ? 1 : src.size());
+    if (!src.empty()) h2d(ctx, b.p, src.data(), src.size() * sizeof(T));
     return b;
 }
 

@@ -8,9 +8,11 @@
 // search, right multiplication by inv(U_KK), two-pointer update of row I's U
 // blocks, Gauss-Jordan inverse of the diagonal block) -- bit-equal factors.
 // Apply: block forward substitution and block back substitution times the
-// cached inverse, per level or sync-free, in FP64 or FP32.
+// cached inverse, in FP64 or FP32: chunked (default, trsv_chunk.cuh), per
+// level or sync-free.
 #include "block_ops.cuh"
 #include "trisolve.cuh"
+#include "trsv_chunk.cuh"
 
 namespace b2s {
 
@@ -209,10 +211,26 @@ struct PcBILU0 final : PcImpl
     DBuf<float> inv32, y32, z32;
     LevelSchedule sl, su;
     SyncFree sfl, sfu;
+    ChunkSchedule csl, csu;
+    bool chunks = false;
 
     template <int BS>
     void apply_t(b2s_ctx* ctx, const double* r, double* z, const int* done)
     {
+        if (chunks)
+        {
+            if (!fp32)
+            {
+                csl.run_block<true, BS, double, double, double>(ctx, L.v.p, nullptr, r, y.p, nullptr, done);
+                csu.run_block<false, BS, double, double, double>(ctx, U.v.p, inv.p, y.p, z, nullptr, done);
+            }
+            else
+            {
+                csl.run_block<true, BS, float, float, double>(ctx, L.v32.p, nullptr, r, y32.p, nullptr, done);
+                csu.run_block<false, BS, float, float, float>(ctx, U.v32.p, inv32.p, y32.p, z32.p, z, done);
+            }
+            return;
+        }
         if (!fp32)
         {
             run_schedule(ctx, mode, sl, sfl,
@@ -293,7 +311,7 @@ std::unique_ptr<PcImpl> make_pc_bilu0(b2s_ctx* ctx, const BaijDev& A, const b2s_
     const int bs = A.bs, bv = bs * bs;
     pc->bs = bs;
     pc->nb = nb;
-    pc->mode = o.trsv == B2S_TRSV_LEVEL ? B2S_TRSV_LEVEL : B2S_TRSV_SYNCFREE;
+    pc->mode = o.trsv == B2S_TRSV_AUTO ? B2S_TRSV_CHUNK : o.trsv;
     pc->fp32 = o.precision != B2S_FP64;
     pc->udiag.alloc(nb ? nb : 1);
     DBuf<int> flags(2);
@@ -330,9 +348,25 @@ std::unique_ptr<PcImpl> make_pc_bilu0(b2s_ctx* ctx, const BaijDev& A, const b2s_
     sync(ctx);
     if (h[1] != big[1])
         fail(B2S_SINGULAR_BLOCK, "Block-ILU(0) breakdown: diagonal block " + std::to_string(h[1]) + " is singular");
-    pc->su.build(ctx, nb, pc->U.rp.p, pc->U.ci.p, false);
-    pc->sfl.init(ctx, nb);
-    pc->sfu.init(ctx, nb);
+    const uint32_t vs = pc->fp32 ? 4 : 8;
+    if (pc->mode == B2S_TRSV_CHUNK && nb)
+    {
+        std::vector<uint32_t> lrp(nb + 1), lci(pc->L.nnzb ? pc->L.nnzb : 1), urp(nb + 1), uci(pc->U.nnzb ? pc->U.nnzb : 1);
+        d2h(ctx, lrp.data(), pc->L.rp.p, (nb + 1) * sizeof(uint32_t));
+        d2h(ctx, lci.data(), pc->L.ci.p, pc->L.nnzb * sizeof(uint32_t));
+        d2h(ctx, urp.data(), pc->U.rp.p, (nb + 1) * sizeof(uint32_t));
+        d2h(ctx, uci.data(), pc->U.ci.p, pc->U.nnzb * sizeof(uint32_t));
+        sync(ctx);
+        pc->chunks = pc->csl.build(ctx, nb, lrp, lci, true, 0, vs, (uint32_t)bs) &&
+                     pc->csu.build(ctx, nb, urp, uci, false, (uint32_t)bv, vs, (uint32_t)bs);
+    }
+    if (!pc->chunks)
+    {
+        if (pc->mode == B2S_TRSV_CHUNK) pc->mode = B2S_TRSV_SYNCFREE;
+        pc->su.build(ctx, nb, pc->U.rp.p, pc->U.ci.p, false);
+        pc->sfl.init(ctx, nb);
+        pc->sfu.init(ctx, nb);
+    }
     pc->y.alloc((size_t)nb * bs + 1);
     if (pc->fp32)
     {
@@ -345,6 +379,19 @@ std::unique_ptr<PcImpl> make_pc_bilu0(b2s_ctx* ctx, const BaijDev& A, const b2s_
         cvt(pc->inv, pc->inv32, (uint64_t)nb * bv);
         pc->y32.alloc((size_t)nb * bs + 1);
         pc->z32.alloc((size_t)nb * bs + 1);
+    }
+    if (pc->chunks)
+    {
+        if (pc->fp32)
+        {
+            pc->csl.pack<float>(ctx, pc->L.v32.p, nullptr);
+            pc->csu.pack<float>(ctx, pc->U.v32.p, pc->inv32.p);
+        }
+        else
+        {
+            pc->csl.pack<double>(ctx, pc->L.v.p, nullptr);
+            pc->csu.pack<double>(ctx, pc->U.v.p, pc->inv.p);
+        }
     }
     sync(ctx);
     return pc;

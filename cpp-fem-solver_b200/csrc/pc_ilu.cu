@@ -343,8 +343,8 @@ struct Tri
     template <bool LOWER, bool UNIT, typename VT, typename XT, typename RT>
     void run_t(b2s_ctx* ctx, int mode, const VT* v, const VT* d, const RT* rhs, XT* x, double* out64, const int* done)
     {
-        if (mode == B2S_TRSV_CHUNK && has_chunks && cs.smem_bytes<VT, XT, RT, UNIT>() > 0)
-            cs.run<LOWER, UNIT, VT, XT, RT>(ctx, m->rp.p, m->ci.p, v, d, rhs, x, out64, done);
+        if (mode == B2S_TRSV_CHUNK && has_chunks && cs.usable<VT, XT, RT>())
+            cs.run<LOWER, UNIT, VT, XT, RT>(ctx, v, d, rhs, x, out64, done);
         else
             run_schedule(ctx, mode == B2S_TRSV_LEVEL ? B2S_TRSV_LEVEL : B2S_TRSV_SYNCFREE, sched, sf,
                          TrsvOp<LOWER, UNIT, VT, XT, RT>{m->rp.p, m->ci.p, v, d, rhs, x, out64}, done);
@@ -364,7 +364,8 @@ struct Tri
             run_t<false, false, VT, XT, RT>(ctx, mode, v, d, rhs, x, out64, done);
     }
 
-    void prepare(b2s_ctx* ctx, const Csr32& mat, bool lo, bool un, int mode)
+    // vs: bytes of the factor values the solves will use (8 FP64, 4 FP32)
+    void prepare(b2s_ctx* ctx, const Csr32& mat, bool lo, bool un, int mode, uint32_t vs)
     {
         m = &mat;
         lower = lo;
@@ -378,9 +379,15 @@ struct Tri
             d2h(ctx, hrp.data(), mat.rp.p, (n + 1) * sizeof(uint32_t));
             d2h(ctx, hci.data(), mat.ci.p, mat.nnz * sizeof(uint32_t));
             sync(ctx);
-            cs.build(ctx, n, hrp, hci, lo, un);
-            has_chunks = true;
+            has_chunks = cs.build(ctx, n, hrp, hci, lo, un ? 0u : 1u, vs);
         }
+    }
+
+    // lay the final factor values out for the chunk schedule (no-op otherwise)
+    template <typename VT>
+    void pack(b2s_ctx* ctx, const VT* v, const VT* d)
+    {
+        if (has_chunks && sizeof(VT) <= cs.plan_vs) cs.pack<VT>(ctx, v, d);
     }
 };
 
@@ -498,12 +505,12 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     split(ctx, A, 0, pc->L, nullptr, err.p);
     check_err(ctx, err, "IC(0) failed");
     pc->diag.alloc(A.n ? A.n : 1);
-    pc->fwd.prepare(ctx, pc->L, true, false, pc->mode);
+    pc->fwd.prepare(ctx, pc->L, true, false, pc->mode, pc->fp32 ? 4 : 8);
     pc->fwd.d64 = pc->diag.p;
     ic0_factor_inplace(ctx, pc->fwd.sched, pc->L.rp.p, pc->L.ci.p, pc->L.v.p, pc->diag.p, "IC(0) failed");
     if (corr) corr->correct(ctx, A, pc->L.rp.p, pc->L.ci.p, pc->L.nnz, pc->L.v.p, pc->diag.p);
     transpose_strict(ctx, pc->L, pc->LT);
-    pc->bwd.prepare(ctx, pc->LT, false, false, pc->mode);
+    pc->bwd.prepare(ctx, pc->LT, false, false, pc->mode, pc->fp32 ? 4 : 8);
     pc->y.alloc(A.n ? A.n : 1);
     if (pc->fp32)
     {
@@ -512,6 +519,13 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
         to_f32(ctx, pc->diag, pc->diag32, A.n);
         pc->y32.alloc(A.n ? A.n : 1);
         pc->z32.alloc(A.n ? A.n : 1);
+        pc->fwd.pack<float>(ctx, pc->L.v32.p, pc->diag32.p);
+        pc->bwd.pack<float>(ctx, pc->LT.v32.p, pc->diag32.p);
+    }
+    else
+    {
+        pc->fwd.pack<double>(ctx, pc->L.v.p, pc->diag.p);
+        pc->bwd.pack<double>(ctx, pc->LT.v.p, pc->diag.p);
     }
     sync(ctx);
     return pc;
@@ -585,7 +599,7 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     split(ctx, A, 1, pc->L, nullptr, err.p);
     split(ctx, A, 2, pc->U, pc->dix.p, err.p);
     check_err(ctx, err, "ILU(0) failed");
-    pc->fwd.prepare(ctx, pc->L, true, true, pc->mode);
+    pc->fwd.prepare(ctx, pc->L, true, true, pc->mode, pc->fp32 ? 4 : 8);
     // factor, level by level
     for (uint32_t l = 0; l < pc->fwd.sched.nlev; ++l)
     {
@@ -596,7 +610,7 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     check_err(ctx, err, "ILU(0) failed");
     pc->udiag.alloc(n ? n : 1);
     if (n) B2S_LAUNCH(ctx, k_gather_diag, stream_grid(ctx, n), kThreads, 0, n, pc->U.v.p, pc->dix.p, pc->udiag.p);
-    pc->bwd.prepare(ctx, pc->U, false, false, pc->mode);
+    pc->bwd.prepare(ctx, pc->U, false, false, pc->mode, pc->fp32 ? 4 : 8);
     pc->y.alloc(n ? n : 1);
     if (pc->fp32)
     {
@@ -605,6 +619,13 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
         to_f32(ctx, pc->udiag, pc->udiag32, n);
         pc->y32.alloc(n ? n : 1);
         pc->z32.alloc(n ? n : 1);
+        pc->fwd.pack<float>(ctx, pc->L.v32.p, (const float*)nullptr);
+        pc->bwd.pack<float>(ctx, pc->U.v32.p, pc->udiag32.p);
+    }
+    else
+    {
+        pc->fwd.pack<double>(ctx, pc->L.v.p, (const double*)nullptr);
+        pc->bwd.pack<double>(ctx, pc->U.v.p, pc->udiag.p);
     }
     sync(ctx);
     return pc;

@@ -111,163 +111,74 @@ __global__ void __launch_bounds__(kThreads) k_spmv_staged(const uint32_t* __rest
     }
 }
 
-// ------------------------------------------------------------------ TMA path
+// ------------------------------------------------------------- warp path
 //
-// Persistent, double-buffered form of the same computation.  Each CTA walks
-// row blocks b, b + grid, ...; thread 0 issues 1-D bulk copies
-// (cp.async.bulk) of block b+grid's values and column indices into the idle
-// stage while the CTA sums block b out of the other stage, so HBM streams
-// continuously.  Copies start on 16-byte boundaries: the value range is
-// widened to even indices and the index range to multiples of four (the
-// arrays carry 8 elements of padding), and the sums index from the widened
-// start.  Waits on the stage barriers are bounded; on a timeout the CTA
-// records B2S_TIMEOUT, waits (bounded) for its own copies and returns.
+// The default CSR SpMV.  A warp owns 32 consecutive rows (a "row group") and
+// walks their nonzeros [rp[r0], rp[r0+32]) in chunks of 256: each lane loads
+// eight values and column indices (coalesced, all in flight together),
+// gathers x, and writes the products to the warp's 2 KB of shared memory;
+// after a __syncwarp each lane adds the products of its own row in ascending
+// column order.  A product v*x rounded once and then added is exactly the
+// reference's `sum += v * x` without contraction, so y is bit-exact.  There
+// is no CTA-wide barrier: warps progress independently and hide each other's
+// gather latency.  Groups are dealt to warps grid-stride over a fixed grid,
+// so the epilogue's reductions have a fixed order.
 
-constexpr int kTmaStageVals = kSpmvNnzPerCta + 2;  // doubles per stage
-constexpr int kTmaStageCols = kSpmvNnzPerCta + 8;  // uint32 per stage (range widened by up to 3 + 3)
-constexpr size_t kTmaStageBytes = (size_t)kTmaStageVals * 8 + (size_t)kTmaStageCols * 4;
-constexpr unsigned kTmaWaitSpins = 1u << 24;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// bounded wait; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
-{
-    for (unsigned s = 0; s < kTmaWaitSpins; ++s)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
-}
-
-// issue the copies of row block b into stage buffers (thread 0 only)
-__device__ __forceinline__ void spmv_issue(uint32_t b, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
-                                           const double* __restrict__ v, const uint32_t* __restrict__ blk_row,
-                                           double* sv, uint32_t* sc, uint64_t* bar)
-{
-    const uint32_t r0 = blk_row[b], r1 = blk_row[b + 1];
-    const uint32_t p0 = rp[r0], p1 = rp[r1];
-    uint32_t bytes = 0;
-    if (p1 - p0 <= (uint32_t)kSpmvNnzPerCta && p1 > p0)
-    {
-        const uint32_t a0 = p0 & ~1u, a1 = (p1 + 1u) & ~1u;
-        const uint32_t c0 = p0 & ~3u, c1 = (p1 + 3u) & ~3u;
-        bytes = (a1 - a0) * 8u + (c1 - c0) * 4u;
-        mbar_arrive_expect_tx(bar, bytes);
-        bulk_load(sv, v + a0, (a1 - a0) * 8u, bar);
-        bulk_load(sc, ci + c0, (c1 - c0) * 4u, bar);
-    }
-    else
-        mbar_arrive_expect_tx(bar, 0u);
-}
+constexpr int kSpmvWarpChunk = 256;                       // products per warp per pass
+constexpr int kSpmvWarpPerLane = kSpmvWarpChunk / 32;     // loads per lane per pass
+constexpr int kSpmvWarpCtasPerSm = 6;
 
 template <typename Epi>
-__global__ void __launch_bounds__(kThreads) k_spmv_tma(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
-                                                       const double* __restrict__ v,
-                                                       const uint32_t* __restrict__ blk_row, uint32_t nblk,
-                                                       const double* __restrict__ x, const int* done, Epi epi,
-                                                       double* partial, unsigned int* counter, int* err)
+__global__ void __launch_bounds__(kThreads, kSpmvWarpCtasPerSm)
+    k_spmv_warp(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                const double* __restrict__ v, const double* __restrict__ x, const int* done, Epi epi,
+                double* partial, unsigned int* counter)
 {
     if (done && *done) return;
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ __align__(8) uint64_t bar[2];
-    double* sv[2] = {reinterpret_cast<double*>(smem), reinterpret_cast<double*>(smem + kTmaStageBytes)};
-    uint32_t* sc[2] = {reinterpret_cast<uint32_t*>(smem + (size_t)kTmaStageVals * 8),
-                       reinterpret_cast<uint32_t*>(smem + kTmaStageBytes + (size_t)kTmaStageVals * 8)};
+    __shared__ double prod[kThreads / 32][kSpmvWarpChunk];
     constexpr int NV = Epi::NV > 0 ? Epi::NV : 1;
     double acc[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-
-    if (threadIdx.x == 0)
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    double* P = prod[wid];
+    const uint32_t ngroups = (n + 31u) >> 5;
+    const uint32_t warps = gridDim.x * (kThreads / 32);
+    for (uint32_t g = blockIdx.x * (kThreads / 32) + wid; g < ngroups; g += warps)
     {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        fence_proxy_async();
-    }
-    __syncthreads();
-    uint32_t phase[2] = {0u, 0u};
-    int stage = 0;
-    bool ok = true;
-    if (threadIdx.x == 0 && blockIdx.x < nblk) spmv_issue(blockIdx.x, rp, ci, v, blk_row, sv[0], sc[0], &bar[0]);
-    for (uint32_t b = blockIdx.x; b < nblk; b += gridDim.x)
-    {
-        const uint32_t nb = b + gridDim.x;
-        if (threadIdx.x == 0 && nb < nblk)
+        const uint32_t r0 = g << 5;
+        const uint32_t r = r0 + lane;
+        const uint32_t rows = min(32u, n - r0);
+        const bool valid = lane < rows;
+        const uint32_t a = valid ? __ldg(&rp[r]) : 0u;
+        const uint32_t b = valid ? __ldg(&rp[r + 1]) : 0u;
+        const uint32_t p0 = __shfl_sync(0xffffffffu, a, 0);
+        const uint32_t p1 = __shfl_sync(0xffffffffu, b, rows - 1);
+        double sum = 0.0;
+        for (uint32_t base = p0; base < p1; base += kSpmvWarpChunk)
         {
-            fence_proxy_async();
-            spmv_issue(nb, rp, ci, v, blk_row, sv[stage ^ 1], sc[stage ^ 1], &bar[stage ^ 1]);
-        }
-        if (!mbar_wait(&bar[stage], phase[stage]))
-        {
-            ok = false;
-            break;
-        }
-        phase[stage] ^= 1u;
-        const uint32_t r0 = blk_row[b], r1 = blk_row[b + 1];
-        const uint32_t p0 = __ldg(&rp[r0]), p1 = __ldg(&rp[r1]);
-        if (p1 - p0 <= (uint32_t)kSpmvNnzPerCta)
-        {
-            // staged copies start at the widened offsets a0 = p0 & ~1, c0 = p0 & ~3
-            const double* V = sv[stage];
-            const uint32_t* Cc = sc[stage];
-            const uint32_t a0 = p0 & ~1u, c0 = p0 & ~3u;
-            for (uint32_t r = r0 + threadIdx.x; r < r1; r += blockDim.x)
+            double vv[kSpmvWarpPerLane];
+            uint32_t cc[kSpmvWarpPerLane];
+#pragma unroll
+            for (int k = 0; k < kSpmvWarpPerLane; ++k)
             {
-                const uint32_t a = __ldg(&rp[r]), e = __ldg(&rp[r + 1]);
-                double sum = 0.0;
-                for (uint32_t k = a; k < e; ++k) sum += V[k - a0] * __ldg(&x[Cc[k - c0]]);
-                epi.row(r, sum, acc);
+                const uint32_t q = base + k * 32 + lane;
+                vv[k] = q < p1 ? __ldg(&v[q]) : 0.0;
+                cc[k] = q < p1 ? __ldg(&ci[q]) : 0u;
             }
-        }
-        else if (threadIdx.x == 0)
-        {
-            for (uint32_t r = r0; r < r1; ++r)
+#pragma unroll
+            for (int k = 0; k < kSpmvWarpPerLane; ++k)
             {
-                double sum = 0.0;
-                for (uint32_t k = __ldg(&rp[r]); k < __ldg(&rp[r + 1]); ++k) sum += __ldg(&v[k]) * __ldg(&x[__ldg(&ci[k])]);
-                epi.row(r, sum, acc);
+                const uint32_t q = base + k * 32 + lane;
+                if (q < p1) P[k * 32 + lane] = vv[k] * __ldg(&x[cc[k]]);
             }
+            __syncwarp();
+            const uint32_t lo = a > base ? a : base;
+            const uint32_t hi = b < base + kSpmvWarpChunk ? b : base + kSpmvWarpChunk;
+            for (uint32_t q = lo; q < hi; ++q) sum += P[q - base];
+            __syncwarp();
         }
-        __syncthreads();
-        stage ^= 1;
-    }
-    if (!ok)
-    {
-        // record, then wait (bounded) for this CTA's copies still in flight
-        if (threadIdx.x == 0) atomicExch(err, (int)B2S_TIMEOUT);
-        mbar_wait(&bar[0], phase[0]);
-        mbar_wait(&bar[1], phase[1]);
-        __syncthreads();
+        if (valid) epi.row(r, sum, acc);
     }
     if constexpr (Epi::NV > 0)
     {
@@ -276,27 +187,21 @@ __global__ void __launch_bounds__(kThreads) k_spmv_tma(const uint32_t* __restric
     }
 }
 
-inline unsigned spmv_tma_grid(const b2s_ctx* ctx, uint32_t nblk)
+inline unsigned spmv_warp_grid(const b2s_ctx* ctx, uint32_t n)
 {
-    const unsigned g = (unsigned)ctx->sm_count * 2u;
-    return nblk < g ? (nblk ? nblk : 1u) : g;
+    const uint32_t ngroups = (n + 31u) / 32u;
+    const uint32_t ctas = (ngroups + kThreads / 32 - 1) / (kThreads / 32);
+    const unsigned g = (unsigned)ctx->sm_count * kSpmvWarpCtasPerSm;
+    return ctas < g ? (ctas ? ctas : 1u) : g;
 }
 
 template <typename Epi>
 inline void launch_spmv(b2s_ctx* ctx, const CsrDev& A, const double* x, const int* done, const Epi& epi)
 {
-    const unsigned grid = spmv_tma_grid(ctx, A.nblk);
+    const unsigned grid = spmv_warp_grid(ctx, A.n);
     if (Epi::NV > 0) reserve_reduction(ctx, grid);
-    auto kern = k_spmv_tma<Epi>;
-    const size_t smem = 2 * kTmaStageBytes;
-    static bool configured = false;
-    if (!configured)
-    {
-        B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        configured = true;
-    }
-    B2S_LAUNCH(ctx, kern, grid, kThreads, smem, A.rp.p, A.ci.p, A.v.p, A.blk_row.p, A.nblk, x, done, epi,
-               ctx->partial.p, ctx->counter.p, ctx->errword());
+    B2S_LAUNCH(ctx, k_spmv_warp<Epi>, grid, kThreads, 0, A.n, A.rp.p, A.ci.p, A.v.p, x, done, epi, ctx->partial.p,
+               ctx->counter.p);
 }
 
 }  // namespace b2s

@@ -1,156 +1,270 @@
-// Chunked triangular solve: the default schedule of the IC(0) / ILU(0)
-// solves (B2S_TRSV_CHUNK).
+// Chunked triangular solve: the default schedule of the IC(0) / ILU(0) and
+// block ILU(0) solves (B2S_TRSV_CHUNK).  Planning (chunks, positions, slots,
+// blob layout) is in trsv_plan.hpp.
 //
-// The rows, in dependency order (natural order for a lower factor, reversed
-// for an upper one), are cut into contiguous chunks that fit one CTA's shared
-// memory: the chunk's slice of the factor (values, column indices, row
-// offsets), its right-hand side and divisors are copied in with coalesced
-// loads when the CTA starts, and the chunk's solution stays in shared memory.
-// Inside a chunk the rows are ordered by their local level (the longest chain
-// of dependencies inside the chunk); the CTA walks the local levels with one
-// __syncthreads() between them, so a dependency inside the chunk costs a
-// shared-memory read.  A dependency on an earlier chunk waits on that row's
-// ready flag (bounded, B2S_TIMEOUT) and reads the value from L2.  CTAs take
-// chunks from a ticket in order, so they only wait on chunks held by CTAs
-// that started earlier.
+// One CTA per chunk; CTAs take chunks from a ticket in order, so a CTA only
+// waits on chunks held by CTAs that started before it.  A CTA:
+//   1. copies its chunk's value blob and metadata blob (16-byte cp.async) and
+//      its slice of the right-hand side (element cp.async) into shared memory;
+//   2. splits into compute warps and one producer warp.  The producer walks
+//      the chunk's slots in the order they are needed: it polls the slot's
+//      row in the exchange array until the row carries this traversal's
+//      epoch, and hands the value over in shared memory (release at CTA
+//      scope).  The compute warps walk the local levels; a level is a
+//      contiguous run of positions, separated by __syncwarp (one compute
+//      warp) or a named barrier over the compute warps.  Every operand of a
+//      row is in shared memory, so a level costs a few shared-memory round
+//      trips, a divide and a barrier.
+//   3. publishes each row that another chunk reads, right after computing
+//      it, into the exchange array: one 64-bit word per 32-bit half of each
+//      value, {epoch, bits}, written with a relaxed store.  A 64-bit access
+//      is single-copy atomic, so a reader that sees the epoch in a word also
+//      sees that word's value bits: one L2 round trip per slot and no fence
+//      on the publishing side.
+// The last CTA to finish resets the tickets and advances the epoch, so the
+// exchange array never needs clearing and the launch can be replayed from a
+// CUDA graph.  Waits spin without sleeping for a bounded number of polls (a
+// dependency normally resolves in well under a microsecond), then back off
+// with 1 us sleeps, and give up with B2S_TIMEOUT after a fixed bound.
 //
-// Every row is still summed in its column order with the reference's
-// arithmetic, so the result equals the level / sync-free schedules bit for
-// bit.  On a 2-D 5-point factor the 1023-level critical path then costs one
-// barrier per level instead of one L2 round trip per level, except at chunk
-// boundaries.
+// Every row is summed in its column order with the reference's arithmetic
+// (sum = rhs; sum -= v * x_j; x = sum / d), so the result equals the level /
+// sync-free schedules bit for bit.
 #pragma once
 #include "syncfree.cuh"
+#include "trsv_plan.hpp"
 
 namespace b2s {
 
-constexpr int kChunkThreads = 256;
-constexpr uint32_t kChunkSmemBudget = 200 * 1024;
+// wait bounds: polls without sleeping, then polls with a 1 us sleep
+constexpr unsigned kChunkFastPolls = 1u << 20;
+constexpr unsigned kChunkSlowPolls = 1u << 20;
 
 struct ChunkArgs
 {
-    const uint32_t* row_lo;     // per chunk (nchunks + 1), in processing order
-    const uint32_t* chunk_lvl;  // per chunk, offsets into lvl_ptr (nchunks + 1)
-    const uint32_t* lvl_ptr;    // level boundaries into sorted
-    const uint32_t* sorted;     // rows of every chunk, by (local level, row)
-    const uint8_t* ext;         // 1 when a row of another chunk depends on the row
-    uint32_t nchunks;
-    uint32_t max_rows, max_nnz;
-    int lower;
-    SyncFreeCtl ctl;
+    const ChunkDesc* desc;
+    const uint4* meta;
+    const uint4* vals;
+    const uint32_t* slot_row;
+    unsigned long long* xch;  // exchange words, 2 per value component
+    SyncFreeCtl ctl;          // ticket, epoch, error word
 };
 
-// shared-memory layout for element types XT (solution), RT (rhs), VT (values)
-template <typename VT, typename XT, typename RT, bool UNIT>
-struct ChunkSmem
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
 {
-    static size_t bytes(uint32_t rows, uint32_t nnz)
-    {
-        size_t b = 0;
-        b += ((size_t)rows * sizeof(XT) + 15) & ~size_t(15);
-        b += ((size_t)rows * sizeof(RT) + 15) & ~size_t(15);
-        if (!UNIT) b += ((size_t)rows * sizeof(VT) + 15) & ~size_t(15);
-        b += ((size_t)(rows + 1) * 4 + 15) & ~size_t(15);
-        b += ((size_t)nnz * sizeof(VT) + 15) & ~size_t(15);
-        b += ((size_t)nnz * 4 + 15) & ~size_t(15);
-        return b;
-    }
-};
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
 
-template <bool LOWER, bool UNIT, typename VT, typename XT, typename RT>
-__global__ void __launch_bounds__(kChunkThreads) k_trsv_chunk(ChunkArgs a, const uint32_t* __restrict__ rp,
-                                                              const uint32_t* __restrict__ ci, const VT* __restrict__ v,
-                                                              const VT* __restrict__ d, const RT* __restrict__ rhs,
-                                                              XT* __restrict__ x, double* __restrict__ out64,
-                                                              const int* done)
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void* dst, const void* src)
+{
+    static_assert(BYTES == 4 || BYTES == 8, "element size");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t ld_acquire_cta_shared(const uint32_t* p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_cta_shared(uint32_t* p, uint32_t v)
+{
+    asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// publish one value component: words w[0], w[1] = {epoch, low bits}, {epoch, high bits}
+template <typename XT>
+__device__ __forceinline__ void xch_put(unsigned long long* w, XT v, uint32_t epoch)
+{
+    const unsigned long long e = (unsigned long long)epoch << 32;
+    if constexpr (sizeof(XT) == 4)
+        st_relaxed_u64(w, e | __float_as_uint(v));
+    else
+    {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+        st_relaxed_u64(w, e | (b & 0xffffffffull));
+        st_relaxed_u64(w + 1, e | (b >> 32));
+    }
+}
+
+// read one value component; false while the words do not carry `epoch`
+template <typename XT>
+__device__ __forceinline__ bool xch_get(const unsigned long long* w, uint32_t epoch, XT& v)
+{
+    if constexpr (sizeof(XT) == 4)
+    {
+        const unsigned long long a = ld_relaxed_u64(w);
+        v = __uint_as_float((uint32_t)a);
+        return (uint32_t)(a >> 32) == epoch;
+    }
+    else
+    {
+        const unsigned long long a = ld_relaxed_u64(w), b = ld_relaxed_u64(w + 1);
+        v = __longlong_as_double((long long)(((b & 0xffffffffull) << 32) | (a & 0xffffffffull)));
+        return (uint32_t)(a >> 32) == epoch && (uint32_t)(b >> 32) == epoch;
+    }
+}
+
+// producer: fetch the BS components of row j (bounded wait)
+template <int BS, typename XT>
+__device__ __forceinline__ void xch_fetch(const unsigned long long* xch, uint32_t j, uint32_t epoch, XT* out,
+                                          int* err)
+{
+    for (unsigned polls = 0;; ++polls)
+    {
+        bool ok = true;
+#pragma unroll
+        for (int c = 0; c < BS; ++c) ok &= xch_get<XT>(xch + ((size_t)j * BS + c) * 2, epoch, out[c]);
+        if (ok) return;
+        if (polls >= kChunkFastPolls)
+        {
+            if (polls >= kChunkFastPolls + kChunkSlowPolls)
+            {
+                atomicExch(err, (int)B2S_TIMEOUT);
+                return;
+            }
+            __nanosleep(1000);
+        }
+    }
+}
+
+// compute warp: wait until the producer has filled slot s (bounded)
+__device__ __forceinline__ void slot_wait(const uint32_t* xr, uint32_t s, int* err)
+{
+    for (unsigned polls = 0; ld_acquire_cta_shared(&xr[s]) == 0u; ++polls)
+    {
+        if (polls >= 8 * kChunkFastPolls)
+        {
+            if (polls >= 8 * kChunkFastPolls + kChunkSlowPolls)
+            {
+                atomicExch(err, (int)B2S_TIMEOUT);
+                return;
+            }
+            __nanosleep(1000);
+        }
+    }
+}
+
+template <int NW>
+__device__ __forceinline__ void compute_barrier()
+{
+    if constexpr (NW == 1)
+        __syncwarp();
+    else
+        asm volatile("bar.sync 1, %0;" ::"n"(NW * 32) : "memory");
+}
+
+template <int NW>
+constexpr int chunk_block() { return (NW + 1) * 32 > 256 ? (NW + 1) * 32 : 256; }
+
+template <bool LOWER, bool UNIT, int NW, typename VT, typename XT, typename RT>
+__global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, const RT* __restrict__ rhs,
+                                                                   XT* __restrict__ x, double* __restrict__ out64,
+                                                                   const int* done)
 {
     if (done && *done) return;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t s_chunk;
-    if (threadIdx.x == 0) s_chunk = atomicAdd(&a.ctl.ticket[0], 1u);
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) s_chunk = atomicAdd(&a.ctl.ticket[0], 1u);
     __syncthreads();
-    const uint32_t c = s_chunk;
-    const uint32_t epoch = ld_flag(a.ctl.epoch);
-    const uint32_t rlo = a.row_lo[c], rhi = a.row_lo[c + 1];
-    const uint32_t lo = LOWER ? rlo : rhi, hi = LOWER ? rhi : rlo;  // row range [lo, hi)
-    const uint32_t nr = hi - lo;
-    const uint32_t p0 = __ldg(&rp[lo]), nz = __ldg(&rp[hi]) - p0;
+    const ChunkDesc D = a.desc[s_chunk];
+    const uint32_t epoch = ld_flag(a.ctl.epoch) + 1u;
+    const SmemLayout L = smem_layout(D.nr, D.nd, D.nl, D.ns, sizeof(VT), sizeof(XT), sizeof(RT), 1, UNIT ? 0 : 1);
 
-    unsigned char* ptr = smem;
-    auto carve = [&](size_t bytes) {
-        unsigned char* r = ptr;
-        ptr += (bytes + 15) & ~size_t(15);
-        return r;
-    };
-    XT* sx = reinterpret_cast<XT*>(carve((size_t)a.max_rows * sizeof(XT)));
-    RT* sr = reinterpret_cast<RT*>(carve((size_t)a.max_rows * sizeof(RT)));
-    VT* sd = UNIT ? nullptr : reinterpret_cast<VT*>(carve((size_t)a.max_rows * sizeof(VT)));
-    uint32_t* srp = reinterpret_cast<uint32_t*>(carve((size_t)(a.max_rows + 1) * 4));
-    VT* sv = reinterpret_cast<VT*>(carve((size_t)a.max_nnz * sizeof(VT)));
-    uint32_t* sc = reinterpret_cast<uint32_t*>(carve((size_t)a.max_nnz * 4));
-
-    for (uint32_t k = threadIdx.x; k < nr; k += blockDim.x)
+    // ---- 1. stage the chunk
     {
-        sr[k] = rhs[lo + k];
-        if (!UNIT) sd[k] = __ldg(&d[lo + k]);
-        srp[k] = __ldg(&rp[lo + k]) - p0;
-    }
-    if (threadIdx.x == 0) srp[nr] = nz;
-    for (uint32_t q = threadIdx.x; q < nz; q += blockDim.x)
-    {
-        sv[q] = __ldg(&v[p0 + q]);
-        sc[q] = __ldg(&ci[p0 + q]);
+        const uint4* vsrc = a.vals + (sizeof(VT) == 8 ? D.v64 : D.v32);
+        const uint4* msrc = a.meta + D.meta;
+        uint4* vdst = reinterpret_cast<uint4*>(smem + L.sv);
+        uint4* mdst = reinterpret_cast<uint4*>(smem + L.meta);
+        for (uint32_t i = tid; i < L.vals / 16; i += blockDim.x) cp_async16(vdst + i, vsrc + i);
+        for (uint32_t i = tid; i < L.m.bytes / 16; i += blockDim.x) cp_async16(mdst + i, msrc + i);
+        RT* sr = reinterpret_cast<RT*>(smem + L.sr);
+        for (uint32_t k = tid; k < D.nr; k += blockDim.x) cp_async_elem<sizeof(RT)>(sr + k, rhs + D.lo + k);
+        uint32_t* xr = reinterpret_cast<uint32_t*>(smem + L.xr);
+        for (uint32_t s = tid; s < D.ns; s += blockDim.x) xr[s] = 0u;
+        cp_async_wait_all();
     }
     __syncthreads();
 
-    const uint32_t l0 = a.chunk_lvl[c], l1 = a.chunk_lvl[c + 1];
-    for (uint32_t l = l0; l < l1; ++l)
+    const uint32_t warp = tid >> 5, lane = tid & 31u;
+    XT* xv = reinterpret_cast<XT*>(smem + L.xv);
+    uint32_t* xr = reinterpret_cast<uint32_t*>(smem + L.xr);
+
+    if (warp == (uint32_t)NW)
     {
-        const uint32_t t1 = a.lvl_ptr[l + 1];
-        for (uint32_t t = a.lvl_ptr[l] + threadIdx.x; t < t1; t += blockDim.x)
+        // ---- 2a. producer: values of earlier chunks, in the order they are needed
+        for (uint32_t s = lane; s < D.ns; s += 32)
         {
-            const uint32_t row = __ldg(&a.sorted[t]);
-            const uint32_t k = row - lo;
+            xch_fetch<1, XT>(a.xch, __ldg(&a.slot_row[D.slot + s]), epoch, &xv[s], a.ctl.err);
+            st_release_cta_shared(&xr[s], 1u);
+        }
+        return;
+    }
+    if (warp > (uint32_t)NW) return;  // helpers only stage
+
+    // ---- 2b. compute warps
+    const VT* sv = reinterpret_cast<const VT*>(smem + L.sv);
+    const VT* sd = reinterpret_cast<const VT*>(smem + L.sd);
+    const uint16_t* slc = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.slc);
+    const uint16_t* srp = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.srp);
+    const uint16_t* perm = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.perm);
+    const uint16_t* slv = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.slv);
+    XT* sx = reinterpret_cast<XT*>(smem + L.sx);
+    const RT* sr = reinterpret_cast<const RT*>(smem + L.sr);
+    for (uint32_t l = 0; l < D.nl; ++l)
+    {
+        const uint32_t t1 = slv[l + 1];
+        for (uint32_t t = slv[l] + tid; t < t1; t += NW * 32)
+        {
+            const uint32_t pr = perm[t], k = pr & 0x7fffu;
             XT sum = (XT)sr[k];
-            for (uint32_t q = srp[k]; q < srp[k + 1]; ++q)
+            const uint32_t e1 = srp[t + 1];
+            for (uint32_t e = srp[t]; e < e1; ++e)
             {
-                const uint32_t j = sc[q];
-                if (LOWER ? (j < row) : (j > row))
+                const uint32_t m = slc[e];
+                XT xj;
+                if (m & 0x8000u)
                 {
-                    XT xj;
-                    if (j >= lo && j < hi)
-                        xj = sx[j - lo];
-                    else
-                    {
-                        unsigned spins = 0, backoff = 20;
-                        while (ld_flag(&a.ctl.flags[j]) != epoch)
-                        {
-                            if (++spins > kMaxSpins)
-                            {
-                                atomicExch(a.ctl.err, (int)B2S_TIMEOUT);
-                                break;
-                            }
-                            __nanosleep(backoff);
-                            backoff = backoff < 320 ? backoff * 2 : 320;
-                        }
-                        xj = __ldcg(&x[j]);
-                    }
-                    sum -= (XT)sv[q] * xj;
+                    const uint32_t s = m & 0x7fffu;
+                    slot_wait(xr, s, a.ctl.err);
+                    xj = xv[s];
                 }
+                else
+                    xj = sx[m];
+                sum -= (XT)sv[e] * xj;
             }
-            const XT r = UNIT ? sum : sum / (XT)sd[k];
-            sx[k] = r;
+            const XT r = UNIT ? sum : sum / (XT)sd[t];
+            sx[t] = r;
+            const uint32_t row = D.lo + k;
             x[row] = r;
             if (out64) out64[row] = (double)r;
-            if (a.ext[row])
-            {
-                __threadfence();
-                st_flag_release(&a.ctl.flags[row], epoch);
-            }
+            if (pr & 0x8000u) xch_put<XT>(a.xch + (size_t)row * 2, r, epoch);
         }
-        __syncthreads();
+        compute_barrier<NW>();
     }
-    if (threadIdx.x == 0)
+
+    // ---- 3. the last CTA to finish resets the tickets and advances the epoch
+    if (tid == 0)
     {
         __threadfence();
         const uint32_t left = atomicAdd(&a.ctl.ticket[1], 1u);
@@ -158,129 +272,315 @@ __global__ void __launch_bounds__(kChunkThreads) k_trsv_chunk(ChunkArgs a, const
         {
             a.ctl.ticket[0] = 0u;
             a.ctl.ticket[1] = 0u;
+            *a.ctl.epoch = epoch;
             __threadfence();
         }
     }
 }
 
-// Host-built chunk schedule of one triangle.
+// Value blob of one chunk: dependency values (bs*bs per entry), then the
+// divisors by position (dv per row: none, a scalar or an inverse block).
+template <typename VT>
+__global__ void __launch_bounds__(kThreads) k_chunk_pack(const ChunkDesc* __restrict__ desc,
+                                                         const uint4* __restrict__ meta,
+                                                         const uint32_t* __restrict__ src, const VT* __restrict__ v,
+                                                         const VT* __restrict__ d, uint4* __restrict__ vals,
+                                                         uint32_t bs, uint32_t dv)
+{
+    const ChunkDesc D = desc[blockIdx.x];
+    const SmemLayout L = smem_layout(D.nr, D.nd, D.nl, D.ns, sizeof(VT), sizeof(VT), sizeof(VT), bs, dv);
+    const uint32_t bv = bs * bs;
+    unsigned char* out = reinterpret_cast<unsigned char*>(vals + (sizeof(VT) == 8 ? D.v64 : D.v32));
+    VT* sv = reinterpret_cast<VT*>(out + L.sv);
+    const uint32_t nv = (L.sd - L.sv) / sizeof(VT);  // values with padding
+    for (uint32_t e = threadIdx.x; e < nv; e += blockDim.x)
+        sv[e] = e < D.nd * bv ? v[(size_t)src[D.dep + e / bv] * bv + e % bv] : VT(0);
+    if (dv)
+    {
+        VT* sd = reinterpret_cast<VT*>(out + L.sd);
+        const uint16_t* perm = reinterpret_cast<const uint16_t*>(reinterpret_cast<const unsigned char*>(meta + D.meta) +
+                                                                 L.m.perm);
+        const uint32_t nd = (L.vals - L.sd) / sizeof(VT);
+        for (uint32_t e = threadIdx.x; e < nd; e += blockDim.x)
+        {
+            const uint32_t t = e / dv;
+            sd[e] = t < D.nr ? d[(size_t)(D.lo + (perm[t] & 0x7fffu)) * dv + e % dv] : VT(0);
+        }
+    }
+}
+
+// Block rows (BAIJ, bs x bs): the block forward substitution of a unit lower
+// factor (x_I = t_I) or the block back substitution times the cached inverse
+// of the diagonal block (x_I = inv_I t_I), with
+//     t_I = rhs_I - sum_J  V_IJ x_J,   (V_IJ x_J)_r = sum_c V_IJ[r][c] x_J[c],
+// each component r accumulated in the reference's order (blockMatrix.hpp:
+// 584-621).  A group of BS lanes takes one position, lane r of the group
+// component r; the upper solve gathers t across the group with shuffles.
+// Staging, producer warp, slots, levels and publication are those of
+// k_trsv_chunk.
+template <bool LOWER, int BS, int NW, typename VT, typename XT, typename RT>
+__global__ void __launch_bounds__(chunk_block<NW>()) k_btrsv_chunk(ChunkArgs a, const RT* __restrict__ rhs,
+                                                                    XT* __restrict__ x, double* __restrict__ out64,
+                                                                    const int* done)
+{
+    constexpr int BV = BS * BS;
+    constexpr uint32_t DV = LOWER ? 0 : BV;
+    constexpr uint32_t GPW = 32 / BS;  // position groups per warp
+    if (done && *done) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t s_chunk;
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) s_chunk = atomicAdd(&a.ctl.ticket[0], 1u);
+    __syncthreads();
+    const ChunkDesc D = a.desc[s_chunk];
+    const uint32_t epoch = ld_flag(a.ctl.epoch) + 1u;
+    const SmemLayout L = smem_layout(D.nr, D.nd, D.nl, D.ns, sizeof(VT), sizeof(XT), sizeof(RT), BS, DV);
+    {
+        const uint4* vsrc = a.vals + (sizeof(VT) == 8 ? D.v64 : D.v32);
+        const uint4* msrc = a.meta + D.meta;
+        uint4* vdst = reinterpret_cast<uint4*>(smem + L.sv);
+        uint4* mdst = reinterpret_cast<uint4*>(smem + L.meta);
+        for (uint32_t i = tid; i < L.vals / 16; i += blockDim.x) cp_async16(vdst + i, vsrc + i);
+        for (uint32_t i = tid; i < L.m.bytes / 16; i += blockDim.x) cp_async16(mdst + i, msrc + i);
+        RT* sr = reinterpret_cast<RT*>(smem + L.sr);
+        const RT* rsrc = rhs + (size_t)D.lo * BS;
+        for (uint32_t k = tid; k < D.nr * BS; k += blockDim.x) cp_async_elem<sizeof(RT)>(sr + k, rsrc + k);
+        uint32_t* xr = reinterpret_cast<uint32_t*>(smem + L.xr);
+        for (uint32_t s = tid; s < D.ns; s += blockDim.x) xr[s] = 0u;
+        cp_async_wait_all();
+    }
+    __syncthreads();
+
+    const uint32_t warp = tid >> 5, lane = tid & 31u;
+    XT* xv = reinterpret_cast<XT*>(smem + L.xv);
+    uint32_t* xr = reinterpret_cast<uint32_t*>(smem + L.xr);
+    if (warp == (uint32_t)NW)
+    {
+        for (uint32_t s = lane; s < D.ns; s += 32)
+        {
+            xch_fetch<BS, XT>(a.xch, __ldg(&a.slot_row[D.slot + s]), epoch, &xv[s * BS], a.ctl.err);
+            st_release_cta_shared(&xr[s], 1u);
+        }
+        return;
+    }
+    if (warp > (uint32_t)NW) return;
+
+    const VT* sv = reinterpret_cast<const VT*>(smem + L.sv);
+    const VT* sd = reinterpret_cast<const VT*>(smem + L.sd);
+    const uint16_t* slc = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.slc);
+    const uint16_t* srp = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.srp);
+    const uint16_t* perm = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.perm);
+    const uint16_t* slv = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.slv);
+    XT* sx = reinterpret_cast<XT*>(smem + L.sx);
+    const RT* sr = reinterpret_cast<const RT*>(smem + L.sr);
+    const uint32_t grp = lane / BS, r = lane % BS;
+    const uint32_t gbase = grp * BS;
+    const bool lane_ok = grp < GPW;
+    for (uint32_t l = 0; l < D.nl; ++l)
+    {
+        const uint32_t t0 = slv[l], t1 = slv[l + 1];
+        // uniform trip count across the warp: shuffles below need every lane
+        for (uint32_t tb = t0; tb < t1; tb += NW * GPW)
+        {
+            const uint32_t t = tb + warp * GPW + grp;
+            const bool act = lane_ok && t < t1;
+            XT tr = 0;
+            uint32_t pr = 0;
+            if (act)
+            {
+                pr = perm[t];
+                const uint32_t k = pr & 0x7fffu;
+                tr = (XT)sr[k * BS + r];
+                const uint32_t e1 = srp[t + 1];
+                for (uint32_t e = srp[t]; e < e1; ++e)
+                {
+                    const uint32_t m = slc[e];
+                    const XT* xj;
+                    if (m & 0x8000u)
+                    {
+                        const uint32_t s = m & 0x7fffu;
+                        slot_wait(xr, s, a.ctl.err);
+                        xj = xv + s * BS;
+                    }
+                    else
+                        xj = sx + m * BS;
+                    const VT* blk = sv + (size_t)e * BV + r * BS;
+                    XT acc = 0;
+#pragma unroll
+                    for (int c = 0; c < BS; ++c) acc += (XT)blk[c] * xj[c];
+                    tr -= acc;
+                }
+            }
+            XT xr_ = tr;
+            if constexpr (!LOWER)
+            {
+                XT tc[BS];
+#pragma unroll
+                for (int c = 0; c < BS; ++c) tc[c] = __shfl_sync(0xffffffffu, tr, (gbase + c) & 31u);
+                if (act)
+                {
+                    const VT* inv = sd + (size_t)t * BV + r * BS;
+                    XT acc = 0;
+#pragma unroll
+                    for (int c = 0; c < BS; ++c) acc += (XT)inv[c] * tc[c];
+                    xr_ = acc;
+                }
+            }
+            // the group leader stores and publishes the whole row
+            XT xc[BS];
+#pragma unroll
+            for (int c = 0; c < BS; ++c) xc[c] = __shfl_sync(0xffffffffu, xr_, (gbase + c) & 31u);
+            if (act)
+            {
+                sx[t * BS + r] = xr_;
+                if (r == 0)
+                {
+                    const uint32_t row = D.lo + (pr & 0x7fffu);
+#pragma unroll
+                    for (int c = 0; c < BS; ++c)
+                    {
+                        x[(size_t)row * BS + c] = xc[c];
+                        if (out64) out64[(size_t)row * BS + c] = (double)xc[c];
+                    }
+                    if (pr & 0x8000u)
+#pragma unroll
+                        for (int c = 0; c < BS; ++c) xch_put<XT>(a.xch + ((size_t)row * BS + c) * 2, xc[c], epoch);
+                }
+            }
+        }
+        compute_barrier<NW>();
+    }
+    if (tid == 0)
+    {
+        __threadfence();
+        const uint32_t left = atomicAdd(&a.ctl.ticket[1], 1u);
+        if (left == gridDim.x - 1)
+        {
+            a.ctl.ticket[0] = 0u;
+            a.ctl.ticket[1] = 0u;
+            *a.ctl.epoch = epoch;
+            __threadfence();
+        }
+    }
+}
+
+// Device copy of a triangle's chunk plan plus its packed values.
 struct ChunkSchedule
 {
-    uint32_t n = 0, nchunks = 0, max_rows = 0, max_nnz = 0;
+    uint32_t n = 0, nchunks = 0;
     bool lower = true;
-    DBuf<uint32_t> row_lo, chunk_lvl, lvl_ptr, sorted;
-    DBuf<uint8_t> ext;
-    SyncFree sf;  // ticket / epoch / error words and per-row flags
+    uint32_t bs = 1, dv = 1;  // block size; divisor values per row (0: unit)
+    int nw = 1;
+    uint32_t plan_vs = 8;  // value size the chunks were sized for
+    DBuf<ChunkDesc> desc;
+    DBuf<uint4> meta, vals;
+    DBuf<uint32_t> slot_row, src;
+    DBuf<unsigned long long> xch;  // exchange words: 2 per value component
+    std::vector<ChunkDesc> h_desc;
+    SyncFree sf;  // ticket / epoch / error words
+    const void* packed_v = nullptr;
+    const void* packed_d = nullptr;
+    uint32_t packed_vs = 0;
 
-    // pattern on the host; deps are j < i (lower) or j > i (upper)
-    void build(b2s_ctx* ctx, uint32_t nrows, const std::vector<uint32_t>& h_rp, const std::vector<uint32_t>& h_ci,
-               bool lo, bool unit)
+    // pattern on the host; chunks sized for values of vs bytes (8 FP64, 4 FP32)
+    bool build(b2s_ctx* ctx, uint32_t nrows, const std::vector<uint32_t>& h_rp, const std::vector<uint32_t>& h_ci,
+               bool lo, uint32_t divisor_values, uint32_t vs, uint32_t block = 1)
     {
         n = nrows;
         lower = lo;
-        std::vector<uint32_t> hrow_lo{lo ? 0u : n}, hchunk_lvl{0}, hlvl_ptr{0}, hsorted;
-        hsorted.reserve(n);
-        // bytes a row costs in shared memory (FP64 upper bound)
-        auto row_bytes = [&](uint32_t r) { return (uint64_t)(8 + 8 + (unit ? 0 : 8) + 4) + 12ull * (h_rp[r + 1] - h_rp[r]); };
-        std::vector<uint32_t> llev(n, 0), cnt;
-        uint32_t pos = 0;
-        while (pos < n)
-        {
-            // grow the chunk while it fits
-            uint64_t bytes = 64;
-            uint32_t end = pos;
-            while (end < n)
-            {
-                const uint32_t r = lo ? end : n - 1 - end;
-                const uint64_t b = row_bytes(r);
-                if (end > pos && bytes + b > kChunkSmemBudget) break;
-                bytes += b;
-                ++end;
-            }
-            const uint32_t rlo = lo ? pos : n - end, rhi = lo ? end : n - pos;  // rows [rlo, rhi)
-            // local levels in dependency order
-            uint32_t maxl = 0, nnz = 0;
-            for (uint32_t t = pos; t < end; ++t)
-            {
-                const uint32_t r = lo ? t : n - 1 - t;
-                uint32_t l = 0;
-                for (uint32_t p = h_rp[r]; p < h_rp[r + 1]; ++p)
-                {
-                    const uint32_t j = h_ci[p];
-                    const bool dep = lo ? j < r : j > r;
-                    if (dep && j >= rlo && j < rhi) l = std::max(l, llev[j] + 1);
-                }
-                llev[r] = l;
-                maxl = std::max(maxl, l);
-                nnz += h_rp[r + 1] - h_rp[r];
-            }
-            // counting sort by (level, row)
-            cnt.assign(maxl + 2, 0);
-            for (uint32_t r = rlo; r < rhi; ++r) cnt[llev[r] + 1]++;
-            for (uint32_t l = 0; l <= maxl; ++l) cnt[l + 1] += cnt[l];
-            const size_t base = hsorted.size();
-            hsorted.resize(base + (rhi - rlo));
-            std::vector<uint32_t> off(cnt.begin(), cnt.end() - 1);
-            for (uint32_t r = rlo; r < rhi; ++r) hsorted[base + off[llev[r]]++] = r;
-            for (uint32_t l = 0; l <= maxl; ++l) hlvl_ptr.push_back((uint32_t)(base + cnt[l + 1]));
-            hchunk_lvl.push_back((uint32_t)hlvl_ptr.size() - 1);
-            hrow_lo.push_back(lo ? end : n - end);
-            max_rows = std::max(max_rows, rhi - rlo);
-            max_nnz = std::max(max_nnz, nnz);
-            pos = end;
-        }
-        nchunks = (uint32_t)hrow_lo.size() - 1;
-        // rows read by a row of another chunk publish a ready flag
-        std::vector<uint32_t> chunk_of(n);
-        for (uint32_t c = 0; c < nchunks; ++c)
-        {
-            const uint32_t a = std::min(hrow_lo[c], hrow_lo[c + 1]), b = std::max(hrow_lo[c], hrow_lo[c + 1]);
-            for (uint32_t r = a; r < b; ++r) chunk_of[r] = c;
-        }
-        std::vector<uint8_t> hext(n ? n : 1, 0);
-        for (uint32_t r = 0; r < n; ++r)
-            for (uint32_t p = h_rp[r]; p < h_rp[r + 1]; ++p)
-            {
-                const uint32_t j = h_ci[p];
-                if ((lo ? j < r : j > r) && chunk_of[j] != chunk_of[r]) hext[j] = 1;
-            }
-        ext = upload(ctx, hext.data(), hext.size());
-        row_lo = upload(ctx, hrow_lo.data(), hrow_lo.size());
-        chunk_lvl = upload(ctx, hchunk_lvl.data(), hchunk_lvl.size());
-        lvl_ptr = upload(ctx, hlvl_ptr.data(), hlvl_ptr.size());
-        sorted = upload(ctx, hsorted.data(), hsorted.size() ? hsorted.size() : 1);
-        sf.init(ctx, n);
+        bs = block;
+        dv = divisor_values;
+        plan_vs = vs;
+        ChunkPlan P = plan_chunks(n, h_rp.data(), h_ci.data(), lo, dv, vs, vs, 8, kChunkSmemBudget, bs);
+        if (!P.ok) return false;
+        nchunks = (uint32_t)P.desc.size();
+        // one compute warp while a level needs at most two passes of it
+        const uint32_t per_warp = 32 / bs;
+        nw = P.max_level_rows <= 2 * per_warp ? 1 : 8;
+        h_desc = P.desc;
+        desc = upload(ctx, P.desc);
+        meta = upload(ctx, reinterpret_cast<const uint4*>(P.meta.data()), P.meta.size() / 16);
+        slot_row = upload(ctx, P.slot_row);
+        src = upload(ctx, P.src);
+        vals.alloc(std::max<uint64_t>(vs == 8 ? P.v64_units : P.v32_units, 1));
+        xch.alloc((size_t)n * bs * 2);
+        B2S_CUDA(cudaMemsetAsync(xch.p, 0, xch.bytes(), ctx->stream));
+        sf.init(ctx, 0);
+        return true;
     }
 
-    ChunkArgs args() const
-    {
-        return ChunkArgs{row_lo.p, chunk_lvl.p, lvl_ptr.p, sorted.p, ext.p, nchunks, max_rows, max_nnz, lower ? 1 : 0,
-                         sf.ctl()};
-    }
-
-    // shared memory a launch needs; 0 when the chunks do not fit one CTA
-    template <typename VT, typename XT, typename RT, bool UNIT>
+    template <typename VT, typename XT, typename RT>
     size_t smem_bytes() const
     {
-        const size_t b = ChunkSmem<VT, XT, RT, UNIT>::bytes(max_rows, max_nnz);
-        return b <= 227 * 1024 ? b : 0;
+        size_t b = 0;
+        for (const ChunkDesc& d : h_desc)
+            b = std::max<size_t>(b, smem_layout(d.nr, d.nd, d.nl, d.ns, sizeof(VT), sizeof(XT), sizeof(RT), bs, dv).total);
+        return b;
     }
 
-    template <bool LOWER, bool UNIT, typename VT, typename XT, typename RT>
-    void run(b2s_ctx* ctx, const uint32_t* rp, const uint32_t* ci, const VT* v, const VT* d, const RT* rhs, XT* x,
-             double* out64, const int* done)
+    // true when a launch with these element types fits shared memory and the value blob
+    template <typename VT, typename XT, typename RT>
+    bool usable() const
     {
-        if (!n) return;
-        auto kern = k_trsv_chunk<LOWER, UNIT, VT, XT, RT>;
-        const size_t smem = ChunkSmem<VT, XT, RT, UNIT>::bytes(max_rows, max_nnz);
-        static thread_local size_t configured = 0;
-        if (smem > configured)
+        return nchunks && sizeof(VT) <= plan_vs && smem_bytes<VT, XT, RT>() <= kChunkSmemLimit;
+    }
+
+    // gather the factor values (and divisors) into the chunk layout
+    template <typename VT>
+    void pack(b2s_ctx* ctx, const VT* v, const VT* d)
+    {
+        if (!nchunks) return;
+        B2S_LAUNCH(ctx, k_chunk_pack<VT>, nchunks, kThreads, 0, desc.p, meta.p, src.p, v, d, vals.p, bs, dv);
+        packed_v = v;
+        packed_d = d;
+        packed_vs = sizeof(VT);
+    }
+
+    template <typename Kern, typename RT, typename XT>
+    void go(b2s_ctx* ctx, Kern kern, int threads, size_t smem, const RT* rhs, XT* x, double* out64, const int* done)
+    {
+        static thread_local std::vector<std::pair<const void*, size_t>> configured;
+        size_t* have = nullptr;
+        for (auto& c : configured)
+            if (c.first == reinterpret_cast<const void*>(kern)) have = &c.second;
+        if (!have)
+        {
+            configured.emplace_back(reinterpret_cast<const void*>(kern), 0);
+            have = &configured.back().second;
+        }
+        if (smem > *have)
         {
             B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            configured = smem;
+            *have = smem;
         }
-        B2S_LAUNCH(ctx, k_epoch_bump, 1, 1, 0, sf.words.p + 2, done);
-        B2S_LAUNCH(ctx, kern, nchunks, kChunkThreads, smem, args(), rp, ci, v, d, rhs, x, out64, done);
+        const ChunkArgs a{desc.p, meta.p, vals.p, slot_row.p, xch.p, sf.ctl()};
+        B2S_LAUNCH(ctx, kern, nchunks, threads, smem, a, rhs, x, out64, done);
+    }
+
+    // scalar rows
+    template <bool LOWER, bool UNIT, typename VT, typename XT, typename RT>
+    void run(b2s_ctx* ctx, const VT* v, const VT* d, const RT* rhs, XT* x, double* out64, const int* done)
+    {
+        if (!n) return;
+        if (packed_v != v || packed_d != d || packed_vs != sizeof(VT)) pack<VT>(ctx, v, d);
+        const size_t smem = smem_bytes<VT, XT, RT>();
+        if (nw == 1)
+            go(ctx, k_trsv_chunk<LOWER, UNIT, 1, VT, XT, RT>, chunk_block<1>(), smem, rhs, x, out64, done);
+        else
+            go(ctx, k_trsv_chunk<LOWER, UNIT, 8, VT, XT, RT>, chunk_block<8>(), smem, rhs, x, out64, done);
+    }
+
+    // block rows: unit lower, or upper times the cached inverse blocks (d)
+    template <bool LOWER, int BS, typename VT, typename XT, typename RT>
+    void run_block(b2s_ctx* ctx, const VT* v, const VT* d, const RT* rhs, XT* x, double* out64, const int* done)
+    {
+        if (!n) return;
+        if (packed_v != v || packed_d != d || packed_vs != sizeof(VT)) pack<VT>(ctx, v, d);
+        const size_t smem = smem_bytes<VT, XT, RT>();
+        if (nw == 1)
+            go(ctx, k_btrsv_chunk<LOWER, BS, 1, VT, XT, RT>, chunk_block<1>(), smem, rhs, x, out64, done);
+        else
+            go(ctx, k_btrsv_chunk<LOWER, BS, 8, VT, XT, RT>, chunk_block<8>(), smem, rhs, x, out64, done);
     }
 };
 

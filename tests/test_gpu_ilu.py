@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 import problems as P
+import oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -89,7 +90,8 @@ def test_ic0_not_spd_and_missing_diag(b2s, ctx):
 
 @pytest.mark.parametrize("method,pc", [(0, "ic"), (0, "ilu"), (1, "ilu"), (2, "ilu"), (2, "ic")])
 def test_solver_parity_ilu(b2s, ctx, orc, method, pc):
-    n, rp, ci, v = P.poisson2d(50) if method == 0 else P.convdiff2d(50)
+    # IC(0) needs an SPD matrix: GMRES + "ic" runs on the Poisson matrix
+    n, rp, ci, v = P.poisson2d(50) if (method == 0 or pc == "ic") else P.convdiff2d(50)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
     b = b2s.uniform(31, n)
     M = b2s.Precond(ctx, A, b2s.pc_kind_from_name(method, pc))
@@ -98,6 +100,19 @@ def test_solver_parity_ilu(b2s, ctx, orc, method, pc):
     assert abs(st["it"] - io) <= 2, (st["it"], io)
     assert rel(x, xo) < 1e-9
     assert st["relres_true"] < 1.5e-8
+
+
+def test_ic0_nonsymmetric_raises_like_reference(b2s, ctx, orc):
+    # the reference's IC(0) throws std::runtime_error on a non-positive pivot
+    # (array.cpp:2649); on the upwind convection-diffusion matrix both
+    # sides stop at setup
+    n, rp, ci, v = P.convdiff2d(50)
+    b = b2s.uniform(31, n)
+    with pytest.raises(oracle.OracleError):
+        orc.solve(orc.csr(n, n, rp, ci, v), 2, "ic", b, 1e-8, 2000, 30)
+    with pytest.raises(RuntimeError) as e:
+        b2s.Precond(ctx, b2s.CSR(ctx, n, n, rp, ci, v), b2s.pc_kind_from_name(2, "ic"))
+    assert e.value.status == b2s.NOT_SPD
 
 
 def test_grf_ic0_pcg_parity(b2s, ctx, orc):
