@@ -117,6 +117,82 @@ def peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "of fallback"
 
 
+# ---------------------------------------------------------------- single-kernel mode
+
+KERNELS = {
+    "spmv_c2": "k_spmv_warp: CSR SpMV on the 128^3 7-point Poisson matrix (C2)",
+    "baij_c4": "k_baij_staged<3>: BAIJ 3x3 matvec on the Q1 elasticity matrix (C4, 64^3 elements)",
+    "trsv_c5": "k_trsv_chunk: FP32 IC(0) apply (L then L^T) on a 512^2 GRF system (C5)",
+    "trsv_c5_fp64": "k_trsv_chunk: FP64 IC(0) apply on a 512^2 GRF system (C5)",
+    "trsv_c2": "k_trsv_chunk: FP64 ILU(0) apply on the 128^3 Poisson matrix (C2)",
+    "btrsv_c4": "k_btrsv_chunk: FP64 block ILU(0) apply on the Q1 elasticity matrix (C4, 64^3 elements)",
+    "vcycle_c2": "SA-AMG V-cycle (k_jacobi, BAIJ matvecs, k_dense_solve) on C2",
+}
+
+
+def run_kernel(args):
+    """Launch one hot kernel `--warmup` + `--steps` times on its workload and
+    report the mean CUDA-event time per launch.  For profilers (ncu -k ...):
+    the inputs are built first, then only that kernel runs."""
+    import ctypes as C
+
+    import torch
+    b2s = load_b2s()
+    ctx = b2s.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    dev = torch.device("cuda", 0)
+    k = args.kernel
+    if k == "spmv_c2":
+        n, rp, ci, v = b2s.gen_poisson3d(128)
+        A = b2s.CSR(ctx, n, n, rp, ci, v)
+        x = torch.rand(n, dtype=torch.float64, device=dev)
+        y = torch.empty_like(x)
+        step = lambda: A.spmv_device(x.data_ptr(), y.data_ptr())
+    elif k == "baij_c4":
+        nbr, rp, ci, v = b2s.gen_elasticity_q1(64)
+        A = b2s.BAIJ(ctx, 3, nbr, nbr, rp, ci, v)
+        x = torch.rand(3 * nbr, dtype=torch.float64, device=dev)
+        y = torch.empty_like(x)
+        step = lambda: ctx.check(b2s.lib().b2s_baij_matvec_device(ctx.h, A.h, C.c_void_p(x.data_ptr()),
+                                                                  C.c_void_p(y.data_ptr())), "baij_matvec")
+    else:
+        if k in ("trsv_c5", "trsv_c5_fp64"):
+            n, rp, ci, v = b2s.gen_grf_diffusion(N_GRID, 2000, corr=CORR)
+            A = b2s.CSR(ctx, n, n, rp, ci, v)
+            M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32 if k == "trsv_c5" else b2s.FP64)
+        elif k == "trsv_c2":
+            n, rp, ci, v = b2s.gen_poisson3d(128)
+            A = b2s.CSR(ctx, n, n, rp, ci, v)
+            M = b2s.Precond(ctx, A, b2s.PC_ILU0)
+        elif k == "btrsv_c4":
+            nbr, rp, ci, v = b2s.gen_elasticity_q1(64)
+            A = b2s.BAIJ(ctx, 3, nbr, nbr, rp, ci, v)
+            n = 3 * nbr
+            M = b2s.Precond(ctx, A, b2s.PC_BILU0)
+        elif k == "vcycle_c2":
+            n, rp, ci, v = b2s.gen_poisson3d(128)
+            A = b2s.CSR(ctx, n, n, rp, ci, v)
+            M = b2s.Precond(ctx, A, b2s.PC_SA_AMG)
+        else:
+            raise SystemExit(f"unknown kernel {k}; one of {sorted(KERNELS)}")
+        r = torch.rand(n, dtype=torch.float64, device=dev)
+        z = torch.empty_like(r)
+        step = lambda: ctx.check(b2s.lib().b2s_pc_apply_device(ctx.h, M.h, C.c_void_p(r.data_ptr()),
+                                                              C.c_void_p(z.data_ptr())), "pc_apply")
+    for _ in range(args.warmup):
+        step()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    print(json.dumps({"kernel": k, "what": KERNELS[k], "launches": args.steps,
+                      "ms_per_step": e0.elapsed_time(e1) / max(args.steps, 1)}))
+    ctx.close()
+    return 0
+
+
 # ---------------------------------------------------------------- reference arm
 
 def run_reference(args):
@@ -168,9 +244,13 @@ def main():
     ap.add_argument("--impl", default="b2s", choices=["b2s", "reference"])
     ap.add_argument("--method", default="fp32_ic0", choices=["fp32_ic0", "fp64_ic0", "learned_ic0"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel", default=None, choices=sorted(KERNELS),
+                    help="run one hot kernel only (for profilers), not the benchmark")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernel:
+        return run_kernel(args)
 
     import torch
     rank, world, local = env_rank()

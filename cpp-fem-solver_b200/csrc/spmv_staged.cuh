@@ -115,7 +115,8 @@ __global__ void __launch_bounds__(kThreads) k_spmv_staged(const uint32_t* __rest
 //
 // The default CSR SpMV.  A warp owns 32 consecutive rows (a "row group") and
 // walks their nonzeros [rp[r0], rp[r0+32]) in chunks of 256: each lane loads
-// eight values and column indices (coalesced, all in flight together),
+// eight values and column indices (coalesced, all in flight together, not
+// allocated in L1 so that L1 keeps x),
 // gathers x, and writes the products to the warp's 2 KB of shared memory;
 // after a __syncwarp each lane adds the products of its own row in ascending
 // column order.  A product v*x rounded once and then added is exactly the
@@ -123,6 +124,21 @@ __global__ void __launch_bounds__(kThreads) k_spmv_staged(const uint32_t* __rest
 // is no CTA-wide barrier: warps progress independently and hide each other's
 // gather latency.  Groups are dealt to warps grid-stride over a fixed grid,
 // so the epilogue's reductions have a fixed order.
+
+// read-once matrix data: read-only path, not kept in L1 (which then holds x)
+__device__ __forceinline__ double ld_stream(const double* p)
+{
+    double v;
+    asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t* p)
+{
+    uint32_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
 
 constexpr int kSpmvWarpChunk = 256;                       // products per warp per pass
 constexpr int kSpmvWarpPerLane = kSpmvWarpChunk / 32;     // loads per lane per pass
@@ -163,8 +179,13 @@ __global__ void __launch_bounds__(kThreads, kSpmvWarpCtasPerSm)
             for (int k = 0; k < kSpmvWarpPerLane; ++k)
             {
                 const uint32_t q = base + k * 32 + lane;
-                vv[k] = q < p1 ? __ldg(&v[q]) : 0.0;
-                cc[k] = q < p1 ? __ldg(&ci[q]) : 0u;
+                vv[k] = 0.0;
+                cc[k] = 0u;
+                if (q < p1)
+                {
+                    vv[k] = ld_stream(v + q);
+                    cc[k] = ld_stream(ci + q);
+                }
             }
 #pragma unroll
             for (int k = 0; k < kSpmvWarpPerLane; ++k)

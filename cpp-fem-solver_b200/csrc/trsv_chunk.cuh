@@ -6,11 +6,11 @@
 // waits on chunks held by CTAs that started before it.  A CTA:
 //   1. copies its chunk's value blob and metadata blob (16-byte cp.async) and
 //      its slice of the right-hand side (element cp.async) into shared memory;
-//   2. splits into compute warps and one producer warp.  The producer walks
-//      the chunk's slots in the order they are needed: it polls the slot's
-//      row in the exchange array until the row carries this traversal's
-//      epoch, and hands the value over in shared memory (release at CTA
-//      scope).  The compute warps walk the local levels; a level is a
+//   2. splits into compute warps and one producer warp.  The producer's
+//      lanes serve the chunk's slots in the order they are needed: each polls
+//      its slot's row in the exchange array until the row carries this
+//      traversal's epoch, and hands the value over in shared memory (release
+//      at CTA scope).  The compute warps walk the local levels; a level is a
 //      contiguous run of positions, separated by __syncwarp (one compute
 //      warp) or a named barrier over the compute warps.  Every operand of a
 //      row is in shared memory, so a level costs a few shared-memory round
@@ -123,25 +123,43 @@ __device__ __forceinline__ bool xch_get(const unsigned long long* w, uint32_t ep
     }
 }
 
-// producer: fetch the BS components of row j (bounded wait)
+// The producer warp: lane l serves slots l, l+32, ... in order.  The loop is
+// warp-uniform: every pass, each lane with a pending slot polls it once (all
+// lanes' polls in flight together) and hands it over as soon as its words
+// carry this traversal's epoch, so no lane waits for another lane's slot.  A
+// lane that polls one slot more than the bound records B2S_TIMEOUT and hands
+// over what it read.
 template <int BS, typename XT>
-__device__ __forceinline__ void xch_fetch(const unsigned long long* xch, uint32_t j, uint32_t epoch, XT* out,
-                                          int* err)
+__device__ __forceinline__ void produce_slots(const ChunkArgs& a, const ChunkDesc& D, uint32_t epoch, uint32_t lane,
+                                              XT* xv, uint32_t* xr)
 {
-    for (unsigned polls = 0;; ++polls)
+    uint32_t s = lane;
+    uint32_t j = s < D.ns ? __ldg(&a.slot_row[D.slot + s]) : 0u;
+    unsigned polls = 0;
+    while (__any_sync(0xffffffffu, s < D.ns))
     {
-        bool ok = true;
-#pragma unroll
-        for (int c = 0; c < BS; ++c) ok &= xch_get<XT>(xch + ((size_t)j * BS + c) * 2, epoch, out[c]);
-        if (ok) return;
-        if (polls >= kChunkFastPolls)
+        if (s < D.ns)
         {
-            if (polls >= kChunkFastPolls + kChunkSlowPolls)
+            XT val[BS];
+            bool ok = true;
+#pragma unroll
+            for (int c = 0; c < BS; ++c) ok &= xch_get<XT>(a.xch + ((size_t)j * BS + c) * 2, epoch, val[c]);
+            if (!ok && ++polls >= kChunkFastPolls + kChunkSlowPolls)
             {
-                atomicExch(err, (int)B2S_TIMEOUT);
-                return;
+                atomicExch(a.ctl.err, (int)B2S_TIMEOUT);
+                ok = true;
             }
-            __nanosleep(1000);
+            if (ok)
+            {
+#pragma unroll
+                for (int c = 0; c < BS; ++c) xv[s * BS + c] = val[c];
+                st_release_cta_shared(&xr[s], 1u);
+                s += 32;
+                if (s < D.ns) j = __ldg(&a.slot_row[D.slot + s]);
+                polls = 0;
+            }
+            else if (polls >= kChunkFastPolls)
+                __nanosleep(1000);
         }
     }
 }
@@ -213,11 +231,7 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
     if (warp == (uint32_t)NW)
     {
         // ---- 2a. producer: values of earlier chunks, in the order they are needed
-        for (uint32_t s = lane; s < D.ns; s += 32)
-        {
-            xch_fetch<1, XT>(a.xch, __ldg(&a.slot_row[D.slot + s]), epoch, &xv[s], a.ctl.err);
-            st_release_cta_shared(&xr[s], 1u);
-        }
+        produce_slots<1, XT>(a, D, epoch, lane, xv, xr);
         return;
     }
     if (warp > (uint32_t)NW) return;  // helpers only stage
@@ -356,11 +370,7 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_btrsv_chunk(ChunkArgs a, 
     uint32_t* xr = reinterpret_cast<uint32_t*>(smem + L.xr);
     if (warp == (uint32_t)NW)
     {
-        for (uint32_t s = lane; s < D.ns; s += 32)
-        {
-            xch_fetch<BS, XT>(a.xch, __ldg(&a.slot_row[D.slot + s]), epoch, &xv[s * BS], a.ctl.err);
-            st_release_cta_shared(&xr[s], 1u);
-        }
+        produce_slots<BS, XT>(a, D, epoch, lane, xv, xr);
         return;
     }
     if (warp > (uint32_t)NW) return;

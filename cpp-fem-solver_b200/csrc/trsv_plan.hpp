@@ -6,8 +6,13 @@
 // A triangle's rows, in dependency order (ascending for a lower factor,
 // descending for an upper one), are cut into chunks of contiguous rows that
 // fit one CTA's shared memory.  Inside a chunk the rows are renumbered into
-// "positions" sorted by local level (the longest dependency chain inside the
-// chunk), so that a level is a contiguous run of positions.  Each row keeps
+// "positions" sorted by their global level (the longest dependency chain
+// ending at the row in the whole triangle), so that a level is a contiguous
+// run of positions.  Global rather than chunk-local levels matter: a chunk's
+// first rows often depend on the last rows of the previous chunk, and with
+// local levels they would sit in the chunk's first level and hold every
+// other row of the chunk until the previous chunk had finished; ordered by
+// global level, each chunk follows the wavefront its predecessor produces.  Each row keeps
 // only its dependency entries (j < i for lower, j > i for upper), in column
 // order; an entry names either the position of an in-chunk row or a "slot":
 // a value of an earlier chunk that the CTA's producer warp fetches into shared
@@ -165,6 +170,19 @@ inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci,
         return P;
     }
     auto is_dep = [&](uint32_t i, uint32_t j) { return lower ? j < i : j > i; };
+    // global levels, in processing order
+    std::vector<uint32_t> glev(n, 0);
+    for (uint32_t t = 0; t < n; ++t)
+    {
+        const uint32_t r = lower ? t : n - 1 - t;
+        uint32_t l = 0;
+        for (uint32_t p = rp[r]; p < rp[r + 1]; ++p)
+        {
+            const uint32_t j = ci[p];
+            if (is_dep(r, j)) l = std::max(l, glev[j] + 1);
+        }
+        glev[r] = l;
+    }
     std::vector<uint32_t> stamp(n, 0);     // chunk id + 1 when j already has a slot in the chunk
     std::vector<uint32_t> slot_of(n, 0);   // slot of j in the chunk that stamped it
     std::vector<uint32_t> llev(n, 0);      // local level
@@ -216,23 +234,21 @@ inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci,
         }
         const uint32_t nr = end - pos;
         const uint32_t lo = lower ? pos : n - end;
-        // ---- local levels, in processing order
+        // ---- the chunk's levels: its distinct global levels, compressed
         rows.clear();
-        uint32_t maxl = 0;
+        uint32_t gmin = ~0u, gmax = 0;
         for (uint32_t t = pos; t < end; ++t)
         {
             const uint32_t r = lower ? t : n - 1 - t;
-            uint32_t l = 0;
-            for (uint32_t p = rp[r]; p < rp[r + 1]; ++p)
-            {
-                const uint32_t j = ci[p];
-                if (is_dep(r, j) && j >= lo && j < lo + nr) l = std::max(l, llev[j] + 1);
-            }
-            llev[r] = l;
-            maxl = std::max(maxl, l);
+            gmin = std::min(gmin, glev[r]);
+            gmax = std::max(gmax, glev[r]);
             rows.push_back(r);
         }
-        const uint32_t nl = maxl + 1;
+        cnt.assign(gmax - gmin + 1, 0);
+        for (uint32_t r : rows) cnt[glev[r] - gmin] = 1;
+        uint32_t nl = 0;
+        for (uint32_t& c : cnt) c = c ? nl++ : 0u;  // global level -> chunk level
+        for (uint32_t r : rows) llev[r] = cnt[glev[r] - gmin];
         // counting sort by level, stable in processing order
         cnt.assign(nl + 1, 0);
         for (uint32_t r : rows) cnt[llev[r] + 1]++;
