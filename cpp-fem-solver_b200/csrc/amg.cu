@@ -212,6 +212,203 @@ __global__ void k_aggregate_std(uint32_t nb, const uint32_t* __restrict__ sp, co
     *nagg_out = (uint32_t)nagg;
 }
 
+// Parallel aggregation (the library default; no reference counterpart).
+// Deterministic, with every pass reading only state from the previous pass:
+//   roots: a distance-2 independent set of the strength graph, chosen in
+//     rounds.  Each row has a fixed key (an integer hash of the row in the
+//     high word, the row + 1 in the low word).  In a round, m1(i) is the
+//     largest key among the undecided rows of {i} U S(i), and an undecided
+//     row whose key equals the largest m1 over {i} U S(i) becomes a root.
+//     Undecided rows within two strength edges of a root then leave the set.
+//     The undecided row with the largest key always becomes a root, so the
+//     rounds end.
+//   aggregates: roots are numbered in row order; a row with a root among its
+//     strong neighbours joins the one with the largest key; a row still
+//     without an aggregate then joins the aggregate of its assigned strong
+//     neighbour with the largest key (as assigned after the first phase);
+//     the rows left over become singletons, numbered after the roots in row
+//     order.
+// S(i) are the strong columns of row i (the same strength test as above).
+
+__device__ __host__ __forceinline__ uint64_t agg_key(uint32_t i)
+{
+    // integer hash (xorshift-multiply mix) of the row, then the row itself
+    uint32_t x = i;
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return ((uint64_t)x << 32) | (uint64_t)(i + 1u);
+}
+
+enum : uint8_t { kAggUndecided = 0, kAggRoot = 1, kAggOut = 2 };
+
+__global__ void k_mis_m1(uint32_t n, const uint32_t* __restrict__ sp, const uint32_t* __restrict__ sc,
+                         const uint8_t* __restrict__ st, uint64_t* __restrict__ m1)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        uint64_t m = st[i] == kAggUndecided ? agg_key(i) : 0ull;
+        for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+        {
+            const uint32_t j = sc[p];
+            if (st[j] == kAggUndecided)
+            {
+                const uint64_t k = agg_key(j);
+                m = k > m ? k : m;
+            }
+        }
+        m1[i] = m;
+    }
+}
+
+__global__ void k_mis_select(uint32_t n, const uint32_t* __restrict__ sp, const uint32_t* __restrict__ sc,
+                             const uint64_t* __restrict__ m1, uint8_t* __restrict__ st)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        if (st[i] != kAggUndecided) continue;
+        uint64_t m = m1[i];
+        for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+        {
+            const uint64_t k = m1[sc[p]];
+            m = k > m ? k : m;
+        }
+        if (m == agg_key(i)) st[i] = kAggRoot;
+    }
+}
+
+// c1(i): i is a root or has a strong neighbour that is one
+__global__ void k_mis_cover1(uint32_t n, const uint32_t* __restrict__ sp, const uint32_t* __restrict__ sc,
+                             const uint8_t* __restrict__ st, uint8_t* __restrict__ c1)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        uint8_t c = st[i] == kAggRoot;
+        for (uint32_t p = sp[i]; p < sp[i + 1] && !c; ++p) c = st[sc[p]] == kAggRoot;
+        c1[i] = c;
+    }
+}
+
+// undecided rows with c1 on {i} U S(i) leave; counts the rows still undecided
+__global__ void k_mis_cover2(uint32_t n, const uint32_t* __restrict__ sp, const uint32_t* __restrict__ sc,
+                             const uint8_t* __restrict__ c1, uint8_t* __restrict__ st, uint32_t* __restrict__ left)
+{
+    uint32_t cnt = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        if (st[i] != kAggUndecided) continue;
+        bool c = c1[i] != 0;
+        for (uint32_t p = sp[i]; p < sp[i + 1] && !c; ++p) c = c1[sc[p]] != 0;
+        if (c)
+            st[i] = kAggOut;
+        else
+            ++cnt;
+    }
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    if ((threadIdx.x & 31u) == 0 && cnt) atomicAdd(left, cnt);
+}
+
+__global__ void k_agg_flag(uint32_t n, const uint8_t* __restrict__ st, const int32_t* __restrict__ agg, int mode,
+                           uint32_t* __restrict__ flag)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        flag[i] = mode == 0 ? (st[i] == kAggRoot) : (agg[i] < 0);
+}
+
+// roots take their number; other rows join the root neighbour with the largest key
+__global__ void k_agg_roots(uint32_t n, const uint32_t* __restrict__ sp, const uint32_t* __restrict__ sc,
+                            const uint8_t* __restrict__ st, const uint32_t* __restrict__ rank, int32_t* __restrict__ agg)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        if (st[i] == kAggRoot)
+        {
+            agg[i] = (int32_t)rank[i];
+            continue;
+        }
+        uint64_t best = 0;
+        int32_t g = -1;
+        for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+        {
+            const uint32_t j = sc[p];
+            if (st[j] != kAggRoot) continue;
+            const uint64_t k = agg_key(j);
+            if (k > best)
+            {
+                best = k;
+                g = (int32_t)rank[j];
+            }
+        }
+        agg[i] = g;
+    }
+}
+
+// rows still without an aggregate join the assigned strong neighbour with the largest key (snapshot)
+__global__ void k_agg_extend(uint32_t n, const uint32_t* __restrict__ sp, const uint32_t* __restrict__ sc,
+                             const int32_t* __restrict__ snap, int32_t* __restrict__ agg)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        if (snap[i] >= 0) continue;
+        uint64_t best = 0;
+        int32_t g = -1;
+        for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+        {
+            const uint32_t j = sc[p];
+            if (snap[j] < 0) continue;
+            const uint64_t k = agg_key(j);
+            if (k > best)
+            {
+                best = k;
+                g = snap[j];
+            }
+        }
+        agg[i] = g;
+    }
+}
+
+__global__ void k_agg_single(uint32_t n, uint32_t base, const uint32_t* __restrict__ rank, int32_t* __restrict__ agg)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (agg[i] < 0) agg[i] = (int32_t)(base + rank[i]);
+}
+
+// returns the aggregate count
+static uint32_t aggregate_parallel(b2s_ctx* ctx, uint32_t n, const uint32_t* sp, const uint32_t* sc, int32_t* agg)
+{
+    if (!n) return 0;
+    const unsigned g = stream_grid(ctx, n);
+    DBuf<uint8_t> st(n), c1(n);
+    DBuf<uint64_t> m1(n);
+    DBuf<uint32_t> left(1), flag(n + 1), rank(n + 1);
+    B2S_CUDA(cudaMemsetAsync(st.p, 0, n, ctx->stream));
+    for (uint32_t round = 0;; ++round)
+    {
+        if (round > n) fail(B2S_CUDA_ERROR, "aggregation rounds did not terminate");
+        B2S_CUDA(cudaMemsetAsync(left.p, 0, sizeof(uint32_t), ctx->stream));
+        B2S_LAUNCH(ctx, k_mis_m1, g, kThreads, 0, n, sp, sc, st.p, m1.p);
+        B2S_LAUNCH(ctx, k_mis_select, g, kThreads, 0, n, sp, sc, m1.p, st.p);
+        B2S_LAUNCH(ctx, k_mis_cover1, g, kThreads, 0, n, sp, sc, st.p, c1.p);
+        B2S_LAUNCH(ctx, k_mis_cover2, g, kThreads, 0, n, sp, sc, c1.p, st.p, left.p);
+        uint32_t h = 0;
+        d2h(ctx, &h, left.p, sizeof(uint32_t));
+        sync(ctx);
+        if (!h) break;
+    }
+    B2S_LAUNCH(ctx, k_agg_flag, g, kThreads, 0, n, st.p, (const int32_t*)nullptr, 0, flag.p);
+    const uint32_t nroots = exclusive_scan(ctx, flag.p, rank.p, n);
+    B2S_LAUNCH(ctx, k_agg_roots, g, kThreads, 0, n, sp, sc, st.p, rank.p, agg);
+    DBuf<int32_t> snap(n);
+    d2d(ctx, snap.p, agg, (size_t)n * sizeof(int32_t));
+    B2S_LAUNCH(ctx, k_agg_extend, g, kThreads, 0, n, sp, sc, snap.p, agg);
+    B2S_LAUNCH(ctx, k_agg_flag, g, kThreads, 0, n, st.p, agg, 1, flag.p);
+    const uint32_t nsingle = exclusive_scan(ctx, flag.p, rank.p, n);
+    if (nsingle) B2S_LAUNCH(ctx, k_agg_single, g, kThreads, 0, n, nroots, rank.p, agg);
+    return nroots + nsingle;
+}
+
 // ------------------------------------------------------------ prolongation
 
 // distinct aggregates among {agg[i]} U {agg[k] : k in row i}, ascending
@@ -707,7 +904,7 @@ struct PcAMG final : PcImpl
 {
     int bs = 1;
     bool ref_coarse = false;
-    bool ref_aggregation = false;
+    int aggregation = 0;  // b2s_pc_opts::amg_aggregation
     std::vector<std::unique_ptr<Level>> lv;
     std::unique_ptr<BaijDev> fine_copy;  // BS=1 copy of a CSR operator
     DBuf<double> dense;
@@ -841,18 +1038,23 @@ void build_hierarchy(b2s_ctx* ctx, PcAMG& pc, const BaijDev& A0, int max_levels,
         // aggregation
         L->agg.alloc(n);
         B2S_CUDA(cudaMemsetAsync(L->agg.p, 0xFF, (size_t)n * sizeof(int32_t), ctx->stream));
-        DBuf<uint32_t> nagg_d(1);
-        if (pc.ref_aggregation)
-            B2S_LAUNCH(ctx, k_aggregate, 1, 32, 0, n, sp.p, sc.p, L->agg.p, nagg_d.p);
+        uint32_t nagg = 0;
+        if (pc.aggregation == 0)
+            nagg = aggregate_parallel(ctx, n, sp.p, sc.p, L->agg.p);
         else
         {
-            DBuf<int32_t> snap(n);
-            B2S_LAUNCH(ctx, k_aggregate_std, 1, 32, 0, n, sp.p, sc.p, L->agg.p, snap.p, nagg_d.p);
+            DBuf<uint32_t> nagg_d(1);
+            if (pc.aggregation == 1)
+                B2S_LAUNCH(ctx, k_aggregate, 1, 32, 0, n, sp.p, sc.p, L->agg.p, nagg_d.p);
+            else
+            {
+                DBuf<int32_t> snap(n);
+                B2S_LAUNCH(ctx, k_aggregate_std, 1, 32, 0, n, sp.p, sc.p, L->agg.p, snap.p, nagg_d.p);
+                sync(ctx);
+            }
+            d2h(ctx, &nagg, nagg_d.p, sizeof(uint32_t));
             sync(ctx);
         }
-        uint32_t nagg = 0;
-        d2h(ctx, &nagg, nagg_d.p, sizeof(uint32_t));
-        sync(ctx);
         // smoothed prolongation
         L->P.bs = BS;
         L->P.nbr = n;
@@ -915,7 +1117,7 @@ std::unique_ptr<PcImpl> build_amg(b2s_ctx* ctx, const BaijDev& A, const b2s_pc_o
     auto pc = std::make_unique<PcAMG>();
     pc->bs = A.bs;
     pc->ref_coarse = o.amg_ref_coarse != 0;
-    pc->ref_aggregation = o.amg_aggregation != 0;
+    pc->aggregation = o.amg_aggregation;
     pc->fine_copy = std::move(owned);
     const int max_levels = o.amg_max_levels > 0 ? o.amg_max_levels : 20;
     const uint32_t coarse_max = o.amg_coarse_max > 0 ? (uint32_t)o.amg_coarse_max : 50u;

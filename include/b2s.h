@@ -163,9 +163,11 @@ typedef struct b2s_pc_opts
                             (blockMatrix.hpp:958-1000) bit for bit; 0: correct pivoted LU */
     int amg_max_levels;  /* 0: reference default 20 */
     int amg_coarse_max;  /* 0: reference default 50 block rows */
-    int amg_aggregation; /* 0: standard three-phase smoothed-aggregation rule (default);
+    int amg_aggregation; /* 0: parallel rule (default): distance-2 independent roots chosen in
+                               rounds by a fixed per-row key, then neighbour assignment;
                             1: the reference's capped greedy rule (blockMatrix.hpp:1101-1111),
-                            which stalls on 3-D problems and serves parity tests */
+                               which stalls on 3-D problems and serves parity tests;
+                            2: sequential three-phase smoothed-aggregation rule */
     const char* learned_weights; /* B2S_PC_LEARNED_IC0: path of a weight file, NULL = built-in init */
 } b2s_pc_opts;
 

@@ -1335,8 +1335,114 @@ static void apply_bilu0(orc_pc* pc, const double* rhs, double* z)
     }
 }
 
-/* ---------------- block SA-AMG (make_block_amg_preconditioner, blockMatrix.hpp:1051-1179) */
-static orc_pc* pc_amg(const orc_blk* A0, int exact, int std_agg, int* st, char* err, int errlen)
+/* Parallel aggregation rule of the library (no reference counterpart),
+ * restated serially with the same snapshots: distance-2 independent roots
+ * chosen in rounds by a fixed per-row key, then neighbour assignment, then
+ * singletons.  Each round reads only the previous round's state. */
+static uint64_t agg_key(uint32_t i)
+{
+    uint32_t x = i;
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return ((uint64_t)x << 32) | (uint64_t)(i + 1u);
+}
+
+static int32_t aggregate_mis(uint32_t n, const uint32_t* sp, const uint32_t* sc, int32_t* agg)
+{
+    enum { UND = 0, ROOT = 1, OUT = 2 };
+    uint8_t* st = (uint8_t*)xcalloc(n ? n : 1, 1);
+    uint8_t* c1 = (uint8_t*)xcalloc(n ? n : 1, 1);
+    uint64_t* m1 = (uint64_t*)xcalloc(n ? n : 1, 8);
+    uint32_t left = n;
+    while (left)
+    {
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            uint64_t m = st[i] == UND ? agg_key(i) : 0;
+            for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+                if (st[sc[p]] == UND && agg_key(sc[p]) > m) m = agg_key(sc[p]);
+            m1[i] = m;
+        }
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            if (st[i] != UND) continue;
+            uint64_t m = m1[i];
+            for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+                if (m1[sc[p]] > m) m = m1[sc[p]];
+            if (m == agg_key(i)) st[i] = ROOT; /* reads only m1: the order of i does not matter */
+        }
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            int c = st[i] == ROOT;
+            for (uint32_t p = sp[i]; p < sp[i + 1] && !c; ++p) c = st[sc[p]] == ROOT;
+            c1[i] = (uint8_t)c;
+        }
+        left = 0;
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            if (st[i] != UND) continue;
+            int c = c1[i];
+            for (uint32_t p = sp[i]; p < sp[i + 1] && !c; ++p) c = c1[sc[p]];
+            if (c)
+                st[i] = OUT;
+            else
+                ++left;
+        }
+    }
+    int32_t nroots = 0;
+    int32_t* rank = (int32_t*)xcalloc(n ? n : 1, 4);
+    for (uint32_t i = 0; i < n; ++i)
+        if (st[i] == ROOT) rank[i] = nroots++;
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        if (st[i] == ROOT)
+        {
+            agg[i] = rank[i];
+            continue;
+        }
+        uint64_t best = 0;
+        int32_t g = -1;
+        for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+            if (st[sc[p]] == ROOT && agg_key(sc[p]) > best)
+            {
+                best = agg_key(sc[p]);
+                g = rank[sc[p]];
+            }
+        agg[i] = g;
+    }
+    int32_t* snap = (int32_t*)xcalloc(n ? n : 1, 4);
+    memcpy(snap, agg, 4 * (size_t)n);
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        if (snap[i] >= 0) continue;
+        uint64_t best = 0;
+        int32_t g = -1;
+        for (uint32_t p = sp[i]; p < sp[i + 1]; ++p)
+            if (snap[sc[p]] >= 0 && agg_key(sc[p]) > best)
+            {
+                best = agg_key(sc[p]);
+                g = snap[sc[p]];
+            }
+        agg[i] = g;
+    }
+    int32_t nagg = nroots;
+    for (uint32_t i = 0; i < n; ++i)
+        if (agg[i] < 0) agg[i] = nagg++;
+    free(st);
+    free(c1);
+    free(m1);
+    free(rank);
+    free(snap);
+    return nagg;
+}
+
+/* ---------------- block SA-AMG (make_block_amg_preconditioner, blockMatrix.hpp:1051-1179)
+ * agg_mode: 0 the reference's capped greedy rule, 1 sequential three-phase
+ * rule, 2 the library's parallel rule (aggregate_mis). */
+static orc_pc* pc_amg(const orc_blk* A0, int exact, int agg_mode, int* st, char* err, int errlen)
 {
     if (A0->nbr != A0->nbc)
     {
@@ -1388,7 +1494,9 @@ static orc_pc* pc_amg(const orc_blk* A0, int exact, int std_agg, int* st, char* 
         int32_t* agg = L->agg = (int32_t*)xcalloc(n, 4);
         for (uint32_t i = 0; i < n; ++i) agg[i] = -1;
         int32_t nagg = 0;
-        if (!std_agg)
+        if (agg_mode == 2)
+            nagg = aggregate_mis(n, sp, sc, agg);
+        else if (agg_mode == 0)
         {
             /* 2. greedy aggregation, natural order, <= max_agg, blockMatrix.hpp:1101-1111 */
             for (uint32_t i = 0; i < n; ++i)
@@ -1760,7 +1868,8 @@ orc_pc* orc_pc_create(const orc_csr* A, const char* kind, double omega, int* st,
     if (!strcmp(kind, "ic0")) return pc_ic0(A, st, err, errlen);
     if (!strcmp(kind, "ilu0")) return pc_ilu0(A, st, err, errlen);
     if (!strcmp(kind, "ssor")) return pc_ssor(A, omega, st, err, errlen);
-    if (!strcmp(kind, "sa_amg") || !strcmp(kind, "sa_amg_exact") || !strcmp(kind, "sa_amg_std"))
+    if (!strcmp(kind, "sa_amg") || !strcmp(kind, "sa_amg_exact") || !strcmp(kind, "sa_amg_std") ||
+        !strcmp(kind, "sa_amg_mis"))
     {
         if (A->n != A->m)
         {
@@ -1769,7 +1878,8 @@ orc_pc* orc_pc_create(const orc_csr* A, const char* kind, double omega, int* st,
             return NULL;
         }
         orc_blk* B = orc_blk_condense(1, A, A->n, A->m);
-        orc_pc* pc = pc_amg(B, strcmp(kind, "sa_amg") != 0, !strcmp(kind, "sa_amg_std"), st, err, errlen);
+        const int mode = !strcmp(kind, "sa_amg_std") ? 1 : !strcmp(kind, "sa_amg_mis") ? 2 : 0;
+        orc_pc* pc = pc_amg(B, strcmp(kind, "sa_amg") != 0, mode, st, err, errlen);
         if (pc)
             pc->owned_blk = B;
         else
@@ -1795,6 +1905,7 @@ orc_pc* orc_blk_pc_create(const orc_blk* A, const char* kind, int* st, char* err
     if (!strcmp(kind, "amg")) return pc_amg(A, 0, 0, st, err, errlen);
     if (!strcmp(kind, "amg_exact")) return pc_amg(A, 1, 0, st, err, errlen);
     if (!strcmp(kind, "amg_std")) return pc_amg(A, 1, 1, st, err, errlen);
+    if (!strcmp(kind, "amg_mis")) return pc_amg(A, 1, 2, st, err, errlen);
     *st = ORC_INVALID_ARG;
     set_err(err, errlen, "unknown block preconditioner kind");
     return NULL;
@@ -2282,7 +2393,7 @@ static const char* resolve_precond(int method, const char* name)
     if (method != 2 && !strcmp(s, "incomplete_cholesky")) return "ic0";
     if (!strcmp(s, "ilu") || !strcmp(s, "ilu0")) return "ilu0";
     if (!strcmp(s, "sor") || !strcmp(s, "ssor")) return "ssor";
-    if (!strcmp(s, "amg")) return "sa_amg_std";
+    if (!strcmp(s, "amg")) return "sa_amg_mis";
     return NULL;
 }
 

@@ -64,7 +64,8 @@ double orc_dot(uint64_t n, const double* a, const double* b);
  * scalar kinds: "none", "diag", "ic0", "ilu0", "ssor", "sa_amg" (block SA-AMG
  * with BS=1 via condense, reference coarsest solve), "sa_amg_exact" (same
  * hierarchy, coarsest level solved by a correct pivoted LU), "sa_amg_std"
- * (standard three-phase aggregation + correct LU; the library's "amg"). */
+ * (sequential three-phase aggregation + correct LU), "sa_amg_mis" (the
+ * library's parallel aggregation rule + correct LU; the library's "amg"). */
 orc_pc* orc_pc_create(const orc_csr* A, const char* kind, double omega, int* st, char* err, int errlen);
 void orc_pc_apply(orc_pc* pc, const double* r, double* z);
 void orc_pc_free(orc_pc* pc);
@@ -85,7 +86,7 @@ uint32_t orc_levels(uint32_t n, const uint32_t* rp, const uint32_t* ci, int uppe
 
 /* ---- solvers (array.cpp:3445-3842, 4190-4533) ----
  * method: 0 pcg, 1 bicgstab, 2 gmres.  The preconditioner string follows each
- * solver's own alias table; "amg" maps to "sa_amg_std". */
+ * solver's own alias table; "amg" maps to "sa_amg_mis". */
 int orc_solve(const orc_csr* A, int method, const char* precond, int restart, double tol, int maxit,
               const double* b, double* x, int* it, char* err, int errlen);
 /* Same solvers with an explicit preconditioner object (the std::function
@@ -108,8 +109,9 @@ void orc_blk_matvec(const orc_blk* A, const double* x, double* y);
 
 /* block kinds: "jacobi", "ilu0", "amg" (reference aggregation and coarsest
  * solve), "amg_exact" (reference aggregation, correct coarsest LU), "amg_std"
- * (standard three-phase aggregation, correct coarsest LU: the library's
- * default, no reference counterpart) */
+ * (sequential three-phase aggregation, correct coarsest LU), "amg_mis" (the
+ * library's default parallel aggregation, correct coarsest LU; no reference
+ * counterpart) */
 orc_pc* orc_blk_pc_create(const orc_blk* A, const char* kind, int* st, char* err, int errlen);
 int orc_blk_ilu0_export(orc_pc* pc, uint32_t* sizes, uint32_t* Lrp, uint32_t* Lci, double* Lv, uint32_t* Urp,
                         uint32_t* Uci, double* Uv, uint32_t* Udiag, double* inv_diag);

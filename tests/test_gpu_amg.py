@@ -3,10 +3,12 @@
 With amg_ref_coarse=1 the whole hierarchy (aggregates, A, P, D^-1 on every
 level) and the V-cycle output equal the restatement bit for bit -- the
 restatement itself equals the compiled reference (tests/test_oracle_pin.py).
-The library default (standard three-phase aggregation + correct pivoted coarse
-LU, "amg_std" in the oracle) is checked the same way; PCG with it converges
-where the reference's capped greedy hierarchy stalls and blows up (32^3).
-The reference-rule modes are parity modes."""
+The library default (parallel aggregation: distance-2 independent roots by a
+fixed per-row key, then neighbour assignment; correct pivoted coarse LU;
+"amg_mis" in the oracle) and the sequential three-phase rule ("amg_std") are
+checked the same way; PCG with them converges where the reference's capped
+greedy hierarchy stalls and blows up (32^3).  The reference-rule modes are
+parity modes."""
 import numpy as np
 import pytest
 
@@ -26,7 +28,8 @@ def hier_cases(b2s):
 MODES = {  # (amg_aggregation, amg_ref_coarse) -> oracle kind
     "reference": (1, 1, "amg"),        # the reference's greedy rule and coarsest elimination
     "ref_exact": (1, 0, "amg_exact"),  # reference greedy rule, correct coarsest LU
-    "standard": (0, 0, "amg_std"),     # the library default
+    "parallel": (0, 0, "amg_mis"),     # the library default
+    "three_phase": (2, 0, "amg_std"),  # sequential three-phase rule
 }
 
 
@@ -61,7 +64,7 @@ def test_scalar_amg_string_is_sa(b2s, ctx, orc):
     n, rp, ci, v = b2s.gen_poisson3d(16)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
     M = b2s.Precond(ctx, A, b2s.pc_kind_from_name(b2s.PCG, "amg"))
-    po = orc.pc(orc.csr(n, n, rp, ci, v), "sa_amg_std")
+    po = orc.pc(orc.csr(n, n, rp, ci, v), "sa_amg_mis")
     r = b2s.uniform(8, n)
     assert np.array_equal(M.apply(r), po.apply(r))
 
@@ -73,10 +76,23 @@ def test_amg_pcg_converges(b2s, ctx, orc):
     M = b2s.Precond(ctx, A, b2s.PC_SA_AMG)
     x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-10, maxit=500)
     assert st["status"] == 0 and st["relres_true"] < 2e-10
-    xo, io = orc.solve_pc(orc.csr(n, n, rp, ci, v), 0, orc.pc(orc.csr(n, n, rp, ci, v), "sa_amg_std"), b,
+    xo, io = orc.solve_pc(orc.csr(n, n, rp, ci, v), 0, orc.pc(orc.csr(n, n, rp, ci, v), "sa_amg_mis"), b,
                           1e-10, 500)
     assert abs(st["it"] - io) <= 2
     assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-8
+
+
+def test_parallel_aggregation_properties(b2s, ctx, orc):
+    # aggregate ids are dense (0..nagg-1), repeated builds give the same
+    # aggregates, and they equal the oracle's serial restatement
+    n, rp, ci, v = b2s.gen_grf_diffusion(96, seed=3)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    aggs = [b2s.Precond(ctx, A, b2s.PC_SA_AMG).export("amg.0.agg")[1] for _ in range(2)]
+    assert np.array_equal(aggs[0], aggs[1])
+    a = aggs[0].astype(np.int64)
+    assert a.min() == 0 and len(np.unique(a)) == a.max() + 1
+    po = orc.pc(orc.csr(n, n, rp, ci, v), "sa_amg_mis")
+    assert np.array_equal(a.astype(np.int32), orc.amg_aggregates(po, 0, n))
 
 
 def test_block_amg_elasticity_pcg(b2s, ctx):
