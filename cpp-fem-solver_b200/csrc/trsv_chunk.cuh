@@ -240,32 +240,59 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
     const VT* sv = reinterpret_cast<const VT*>(smem + L.sv);
     const VT* sd = reinterpret_cast<const VT*>(smem + L.sd);
     const uint16_t* slc = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.slc);
-    const uint16_t* srp = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.srp);
-    const uint16_t* perm = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.perm);
+    const uint2* rec = reinterpret_cast<const uint2*>(smem + L.meta + L.m.rec);
     const uint16_t* slv = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.slv);
     XT* sx = reinterpret_cast<XT*>(smem + L.sx);
     const RT* sr = reinterpret_cast<const RT*>(smem + L.sr);
+    uint32_t t0 = 0, t1 = slv[1];
     for (uint32_t l = 0; l < D.nl; ++l)
     {
-        const uint32_t t1 = slv[l + 1];
-        for (uint32_t t = slv[l] + tid; t < t1; t += NW * 32)
+        const uint32_t tn = l + 2 <= D.nl ? slv[l + 2] : t1;  // the next level's end, read ahead
+        for (uint32_t t = t0 + tid; t < t1; t += NW * 32)
         {
-            const uint32_t pr = perm[t], k = pr & 0x7fffu;
+            const uint2 rw = rec[t];
+            const uint32_t pr = rec_perm(rw.x), k = pr & 0x7fffu;
+            const uint32_t e0 = rec_e0(rw.x), e1 = rec_e1(rw.y);
             XT sum = (XT)sr[k];
-            const uint32_t e1 = srp[t + 1];
-            for (uint32_t e = srp[t]; e < e1; ++e)
+            if (e1 - e0 <= 4)
             {
-                const uint32_t m = slc[e];
-                XT xj;
-                if (m & 0x8000u)
+                // short rows: all column entries, then all operands, then the
+                // products in column order
+                uint32_t m[4];
+                VT vv[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
                 {
-                    const uint32_t s = m & 0x7fffu;
-                    slot_wait(xr, s, a.ctl.err);
-                    xj = xv[s];
+                    const bool on = e0 + q < e1;
+                    m[q] = on ? slc[e0 + q] : 0u;
+                    vv[q] = on ? sv[e0 + q] : VT(0);
                 }
-                else
-                    xj = sx[m];
-                sum -= (XT)sv[e] * xj;
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (e0 + q < e1 && (m[q] & 0x8000u)) slot_wait(xr, m[q] & 0x7fffu, a.ctl.err);
+                XT xj[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) xj[q] = (m[q] & 0x8000u) ? xv[m[q] & 0x7fffu] : sx[m[q]];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (e0 + q < e1) sum -= (XT)vv[q] * xj[q];
+            }
+            else
+            {
+                for (uint32_t e = e0; e < e1; ++e)
+                {
+                    const uint32_t m = slc[e];
+                    XT xj;
+                    if (m & 0x8000u)
+                    {
+                        const uint32_t s = m & 0x7fffu;
+                        slot_wait(xr, s, a.ctl.err);
+                        xj = xv[s];
+                    }
+                    else
+                        xj = sx[m];
+                    sum -= (XT)sv[e] * xj;
+                }
             }
             const XT r = UNIT ? sum : sum / (XT)sd[t];
             sx[t] = r;
@@ -275,6 +302,8 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
             if (pr & 0x8000u) xch_put<XT>(a.xch + (size_t)row * 2, r, epoch);
         }
         compute_barrier<NW>();
+        t0 = t1;
+        t1 = tn;
     }
 
     // ---- 3. the last CTA to finish resets the tickets and advances the epoch
@@ -312,13 +341,13 @@ __global__ void __launch_bounds__(kThreads) k_chunk_pack(const ChunkDesc* __rest
     if (dv)
     {
         VT* sd = reinterpret_cast<VT*>(out + L.sd);
-        const uint16_t* perm = reinterpret_cast<const uint16_t*>(reinterpret_cast<const unsigned char*>(meta + D.meta) +
-                                                                 L.m.perm);
+        const uint32_t* recw = reinterpret_cast<const uint32_t*>(reinterpret_cast<const unsigned char*>(meta + D.meta) +
+                                                                 L.m.rec);
         const uint32_t nd = (L.vals - L.sd) / sizeof(VT);
         for (uint32_t e = threadIdx.x; e < nd; e += blockDim.x)
         {
             const uint32_t t = e / dv;
-            sd[e] = t < D.nr ? d[(size_t)(D.lo + (perm[t] & 0x7fffu)) * dv + e % dv] : VT(0);
+            sd[e] = t < D.nr ? d[(size_t)(D.lo + (rec_perm(recw[2 * t]) & 0x7fffu)) * dv + e % dv] : VT(0);
         }
     }
 }
@@ -378,17 +407,17 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_btrsv_chunk(ChunkArgs a, 
     const VT* sv = reinterpret_cast<const VT*>(smem + L.sv);
     const VT* sd = reinterpret_cast<const VT*>(smem + L.sd);
     const uint16_t* slc = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.slc);
-    const uint16_t* srp = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.srp);
-    const uint16_t* perm = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.perm);
+    const uint2* rec = reinterpret_cast<const uint2*>(smem + L.meta + L.m.rec);
     const uint16_t* slv = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.slv);
     XT* sx = reinterpret_cast<XT*>(smem + L.sx);
     const RT* sr = reinterpret_cast<const RT*>(smem + L.sr);
     const uint32_t grp = lane / BS, r = lane % BS;
     const uint32_t gbase = grp * BS;
     const bool lane_ok = grp < GPW;
+    uint32_t t0 = 0, t1 = slv[1];
     for (uint32_t l = 0; l < D.nl; ++l)
     {
-        const uint32_t t0 = slv[l], t1 = slv[l + 1];
+        const uint32_t tn = l + 2 <= D.nl ? slv[l + 2] : t1;  // the next level's end, read ahead
         // uniform trip count across the warp: shuffles below need every lane
         for (uint32_t tb = t0; tb < t1; tb += NW * GPW)
         {
@@ -398,11 +427,12 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_btrsv_chunk(ChunkArgs a, 
             uint32_t pr = 0;
             if (act)
             {
-                pr = perm[t];
+                const uint2 rw = rec[t];
+                pr = rec_perm(rw.x);
                 const uint32_t k = pr & 0x7fffu;
                 tr = (XT)sr[k * BS + r];
-                const uint32_t e1 = srp[t + 1];
-                for (uint32_t e = srp[t]; e < e1; ++e)
+                const uint32_t e1 = rec_e1(rw.y);
+                for (uint32_t e = rec_e0(rw.x); e < e1; ++e)
                 {
                     const uint32_t m = slc[e];
                     const XT* xj;
@@ -459,6 +489,8 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_btrsv_chunk(ChunkArgs a, 
             }
         }
         compute_barrier<NW>();
+        t0 = t1;
+        t1 = tn;
     }
     if (tid == 0)
     {

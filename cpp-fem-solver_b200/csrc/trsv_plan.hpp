@@ -26,9 +26,9 @@
 // Per chunk the planner writes a metadata blob, copied verbatim into shared
 // memory by the kernel:
 //     slc  u16[nd]    dependency entries: position, or 0x8000 | slot
-//     srp  u16[nr+1]  per position, offsets into slc
-//     perm u16[nr]    per position, local row (row - lo) | 0x8000 when rows
-//                     of another chunk depend on it (it publishes a flag)
+//     rec  u16x4[nr]  per position: local row (row - lo) | 0x8000 when rows
+//                     of another chunk depend on it (it publishes), then the
+//                     position's range [e0, e1) in slc, then 0
 //     slv  u16[nl+1]  level boundaries (positions)
 // and a value blob per precision (written on the device by k_chunk_pack):
 //     sv   VT[nd*bs*bs]  dependency values (blocks row-major), same order as slc
@@ -75,7 +75,7 @@ struct ChunkDesc
 // byte offsets inside the metadata blob (independent of the value type)
 struct MetaLayout
 {
-    uint32_t slc, srp, perm, slv, bytes;
+    uint32_t slc, rec, slv, bytes;
 };
 
 B2S_HD MetaLayout meta_layout(uint32_t nr, uint32_t nd, uint32_t nl)
@@ -84,15 +84,18 @@ B2S_HD MetaLayout meta_layout(uint32_t nr, uint32_t nd, uint32_t nl)
     uint32_t o = 0;
     m.slc = o;
     o += al16((uint64_t)nd * 2);
-    m.srp = o;
-    o += al16((uint64_t)(nr + 1) * 2);
-    m.perm = o;
-    o += al16((uint64_t)nr * 2);
+    m.rec = o;
+    o += al16((uint64_t)nr * 8);
     m.slv = o;
     o += al16((uint64_t)(nl + 1) * 2);
     m.bytes = o;
     return m;
 }
+
+// fields of a position record (two u32 words: {perm, e0}, {e1, 0})
+B2S_HD uint32_t rec_perm(uint32_t w0) { return w0 & 0xffffu; }
+B2S_HD uint32_t rec_e0(uint32_t w0) { return w0 >> 16; }
+B2S_HD uint32_t rec_e1(uint32_t w1) { return w1 & 0xffffu; }
 
 // byte offsets of the chunk's shared memory: [values][metadata][x][rhs][slot values][slot ready]
 struct SmemLayout
@@ -211,7 +214,7 @@ inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci,
                 const bool inside = lower ? j >= pos : j <= first;
                 if (!inside && stamp[j] != tag) ++nnew;
             }
-            const uint64_t b = (uint64_t)vs * (ndep * bv + dv) + 2ull * ndep + 6 + (uint64_t)bs * (xs + rs) +
+            const uint64_t b = (uint64_t)vs * (ndep * bv + dv) + 2ull * ndep + 10 + (uint64_t)bs * (xs + rs) +
                                (uint64_t)nnew * (bs * xs + 4);
             const bool fits = bytes + b <= budget && end - pos + 1 <= kChunkMaxRows && nd + ndep <= kChunkMaxDeps &&
                               ns + nnew <= kChunkMaxSlots;
@@ -279,9 +282,9 @@ inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci,
         for (uint32_t t = 0; t < nr; ++t)
         {
             const uint32_t r = sorted[t];
-            put16(M.srp, t, e);
-            put16(M.perm, t, r - lo);
-            perm_at[r] = mbase + M.perm + 2ull * t;
+            put16(M.rec, 4 * t, r - lo);
+            put16(M.rec, 4 * t + 1, e);
+            perm_at[r] = mbase + M.rec + 8ull * t;
             for (uint32_t p = rp[r]; p < rp[r + 1]; ++p)
             {
                 const uint32_t j = ci[p];
@@ -305,8 +308,8 @@ inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci,
                 P.src.push_back(p);
                 ++e;
             }
+            put16(M.rec, 4 * t + 2, e);
         }
-        put16(M.srp, nr, e);
         for (uint32_t l = 0; l <= nl; ++l) put16(M.slv, l, cnt[l]);
         D.ns = s;
         D.v64 = (uint32_t)P.v64_units;

@@ -230,7 +230,7 @@ static void run_case(const char* name, Tri T, bool lower, uint32_t dv, uint32_t 
                 const uint32_t t = e / dv;
                 if (t < D.nr)
                 {
-                    const uint32_t k = rd16(P.meta, (uint64_t)D.meta * 16 + L.m.perm + 2ull * t) & 0x7fffu;
+                    const uint32_t k = rd16(P.meta, (uint64_t)D.meta * 16 + L.m.rec + 8ull * t) & 0x7fffu;
                     CHECK(k < D.nr);
                     val = (VT)T.d[(size_t)(D.lo + k) * dv + e % dv];
                 }
@@ -272,8 +272,8 @@ static void run_case(const char* name, Tri T, bool lower, uint32_t dv, uint32_t 
             S.at<uint32_t>(L.xr, L.total, s) = 1;
         }
         // 2b. compute
-        const uint32_t mslc = L.meta + L.m.slc, msrp = L.meta + L.m.srp, mperm = L.meta + L.m.perm,
-                       mslv = L.meta + L.m.slv, mend = L.meta + L.m.bytes;
+        const uint32_t mslc = L.meta + L.m.slc, mrec = L.meta + L.m.rec, mslv = L.meta + L.m.slv,
+                       mend = L.meta + L.m.bytes;
         std::vector<int32_t> lvl_of_pos(D.nr, -1);
         CHECK(S.at<uint16_t>(mslv, mend, 0) == 0);
         CHECK(S.at<uint16_t>(mslv, mend, D.nl) == D.nr);
@@ -283,18 +283,19 @@ static void run_case(const char* name, Tri T, bool lower, uint32_t dv, uint32_t 
             CHECK(t0 < t1 && t1 <= D.nr);
             for (uint32_t t = t0; t < t1; ++t)
             {
-                const uint32_t pr = S.at<uint16_t>(mperm, mslv, t), k = pr & 0x7fffu;
+                const uint32_t pr = S.at<uint16_t>(mrec, mslv, 4 * t), k = pr & 0x7fffu;
+                const uint32_t e0 = S.at<uint16_t>(mrec, mslv, 4 * t + 1), e1 = S.at<uint16_t>(mrec, mslv, 4 * t + 2);
+                CHECK(S.at<uint16_t>(mrec, mslv, 4 * t + 3) == 0);
                 CHECK(k < D.nr);
                 // one lane per component (a single lane for scalar rows)
                 XT tr[BS];
                 for (uint32_t r = 0; r < BS; ++r)
                 {
                     tr[r] = (XT)S.at<RT>(L.sr, L.xv, k * BS + r);
-                    const uint32_t e0 = S.at<uint16_t>(msrp, mperm, t), e1 = S.at<uint16_t>(msrp, mperm, t + 1);
                     CHECK(e0 <= e1 && e1 <= D.nd);
                     for (uint32_t e = e0; e < e1; ++e)
                     {
-                        const uint32_t m = S.at<uint16_t>(mslc, msrp, e);
+                        const uint32_t m = S.at<uint16_t>(mslc, mrec, e);
                         uint32_t seg, seg_end, base;
                         if (m & 0x8000u)
                         {
