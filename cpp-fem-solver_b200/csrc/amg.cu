@@ -498,45 +498,20 @@ __global__ void k_bt_count(uint32_t nb, const uint32_t* __restrict__ rp, const u
         for (uint32_t p = rp[i]; p < rp[i + 1]; ++p) atomicAdd(&cnt[ci[p]], 1u);
 }
 
+// T's entry d = A's entry perm[d], its block transposed; rows ascending by construction
 template <int BS>
-__global__ void k_bt_fill(uint32_t nb, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
-                          const double* __restrict__ v, const uint32_t* __restrict__ trp, uint32_t* __restrict__ off,
-                          uint32_t* __restrict__ tci, double* __restrict__ tv)
+__global__ void k_bt_gather(uint32_t nnz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ row_of,
+                            const double* __restrict__ v, uint32_t* __restrict__ tci, double* __restrict__ tv)
 {
     constexpr int BV = BS * BS;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
-        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
-        {
-            const uint32_t j = ci[p];
-            const uint32_t d = trp[j] + atomicAdd(&off[j], 1u);
-            tci[d] = i;
-            for (int r = 0; r < BS; ++r)
-                for (int c = 0; c < BS; ++c) tv[(size_t)d * BV + r * BS + c] = v[(size_t)p * BV + c * BS + r];
-        }
-}
-
-template <int BS>
-__global__ void k_bt_sort(uint32_t nr, const uint32_t* __restrict__ rp, uint32_t* __restrict__ ci, double* __restrict__ v)
-{
-    constexpr int BV = BS * BS;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nr; i += gridDim.x * blockDim.x)
+    for (uint32_t d = blockIdx.x * blockDim.x + threadIdx.x; d < nnz; d += gridDim.x * blockDim.x)
     {
-        const uint32_t a = rp[i], b = rp[i + 1];
-        for (uint32_t p = a + 1; p < b; ++p)
-        {
-            const uint32_t c = ci[p];
-            double x[BV];
-            for (int k = 0; k < BV; ++k) x[k] = v[(size_t)p * BV + k];
-            uint32_t q = p;
-            while (q > a && ci[q - 1] > c)
-            {
-                ci[q] = ci[q - 1];
-                for (int k = 0; k < BV; ++k) v[(size_t)q * BV + k] = v[(size_t)(q - 1) * BV + k];
-                --q;
-            }
-            ci[q] = c;
-            for (int k = 0; k < BV; ++k) v[(size_t)q * BV + k] = x[k];
-        }
+        const uint32_t p = perm[d];
+        tci[d] = row_of[p];
+#pragma unroll
+        for (int r = 0; r < BS; ++r)
+#pragma unroll
+            for (int c = 0; c < BS; ++c) tv[(size_t)d * BV + r * BS + c] = v[(size_t)p * BV + c * BS + r];
     }
 }
 
@@ -554,11 +529,11 @@ void block_transpose(b2s_ctx* ctx, const BaijDev& A, BaijDev& T)
     const uint32_t nnz = exclusive_scan(ctx, cnt.p, T.rp.p, T.nbr);
     T.ci.alloc(nnz ? nnz : 1);
     T.v.alloc(nnz ? (size_t)nnz * BV : 1);
-    B2S_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes(), ctx->stream));
-    if (A.nbr)
-        B2S_LAUNCH(ctx, k_bt_fill<BS>, stream_grid(ctx, A.nbr), kThreads, 0, A.nbr, A.rp.p, A.ci.p, A.v.p, T.rp.p,
-                   cnt.p, T.ci.p, T.v.p);
-    if (T.nbr) B2S_LAUNCH(ctx, k_bt_sort<BS>, stream_grid(ctx, T.nbr), kThreads, 0, T.nbr, T.rp.p, T.ci.p, T.v.p);
+    DBuf<uint32_t> perm, row_of;
+    transpose_order(ctx, A.nbr, A.nbc, A.rp.p, A.ci.p, nnz, perm, row_of);
+    if (nnz)
+        B2S_LAUNCH(ctx, k_bt_gather<BS>, stream_grid(ctx, nnz), kThreads, 0, nnz, perm.p, row_of.p, A.v.p, T.ci.p,
+                   T.v.p);
     finish_baij(ctx, T);
 }
 

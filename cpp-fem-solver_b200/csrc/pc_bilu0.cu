@@ -14,6 +14,9 @@
 #include "trisolve.cuh"
 #include "trsv_chunk.cuh"
 
+#include <exception>
+#include <thread>
+
 namespace b2s {
 
 namespace {
@@ -335,7 +338,46 @@ std::unique_ptr<PcImpl> make_pc_bilu0(b2s_ctx* ctx, const BaijDev& A, const b2s_
     sync(ctx);
     if (h[0] != big[0])
         fail(B2S_MISSING_DIAG, "Block-ILU(0) failed: block row " + std::to_string(h[0]) + " has no diagonal block");
-    pc->sl.build(ctx, nb, pc->L.rp.p, pc->L.ci.p, true);
+    // host analysis: block levels of L here (for the factorisation); the chunk
+    // plans on a host thread while the device factorises
+    const uint32_t vs = pc->fp32 ? 4 : 8;
+    std::vector<uint32_t> lrp(nb + 1), lci(pc->L.nnzb ? pc->L.nnzb : 1), urp(nb + 1), uci(pc->U.nnzb ? pc->U.nnzb : 1);
+    d2h(ctx, lrp.data(), pc->L.rp.p, (nb + 1) * sizeof(uint32_t));
+    d2h(ctx, lci.data(), pc->L.ci.p, pc->L.nnzb * sizeof(uint32_t));
+    d2h(ctx, urp.data(), pc->U.rp.p, (nb + 1) * sizeof(uint32_t));
+    d2h(ctx, uci.data(), pc->U.ci.p, pc->U.nnzb * sizeof(uint32_t));
+    sync(ctx);
+    std::vector<uint32_t> llev, ulev;
+    compute_levels(nb, lrp.data(), lci.data(), true, llev);
+    if (nb) pc->sl.build_host(ctx, llev);
+    const bool chunked = pc->mode == B2S_TRSV_CHUNK && nb;
+    ChunkPlan lplan, uplan;
+    std::exception_ptr perr;
+    std::thread th([&] {
+        try
+        {
+            compute_levels(nb, urp.data(), uci.data(), false, ulev);
+            if (chunked)
+            {
+                lplan = plan_chunks(nb, lrp.data(), lci.data(), true, 0, vs, vs, 8, kChunkSmemBudget, (uint32_t)bs,
+                                    &llev);
+                uplan = plan_chunks(nb, urp.data(), uci.data(), false, (uint32_t)bv, vs, vs, 8, kChunkSmemBudget,
+                                    (uint32_t)bs, &ulev);
+            }
+        }
+        catch (...)
+        {
+            perr = std::current_exception();
+        }
+    });
+    struct Join
+    {
+        std::thread& t;
+        ~Join()
+        {
+            if (t.joinable()) t.join();
+        }
+    } join{th};
     pc->inv.alloc((size_t)nb * bv + 1);
     switch (bs)
     {
@@ -348,22 +390,13 @@ std::unique_ptr<PcImpl> make_pc_bilu0(b2s_ctx* ctx, const BaijDev& A, const b2s_
     sync(ctx);
     if (h[1] != big[1])
         fail(B2S_SINGULAR_BLOCK, "Block-ILU(0) breakdown: diagonal block " + std::to_string(h[1]) + " is singular");
-    const uint32_t vs = pc->fp32 ? 4 : 8;
-    if (pc->mode == B2S_TRSV_CHUNK && nb)
-    {
-        std::vector<uint32_t> lrp(nb + 1), lci(pc->L.nnzb ? pc->L.nnzb : 1), urp(nb + 1), uci(pc->U.nnzb ? pc->U.nnzb : 1);
-        d2h(ctx, lrp.data(), pc->L.rp.p, (nb + 1) * sizeof(uint32_t));
-        d2h(ctx, lci.data(), pc->L.ci.p, pc->L.nnzb * sizeof(uint32_t));
-        d2h(ctx, urp.data(), pc->U.rp.p, (nb + 1) * sizeof(uint32_t));
-        d2h(ctx, uci.data(), pc->U.ci.p, pc->U.nnzb * sizeof(uint32_t));
-        sync(ctx);
-        pc->chunks = pc->csl.build(ctx, nb, lrp, lci, true, 0, vs, (uint32_t)bs) &&
-                     pc->csu.build(ctx, nb, urp, uci, false, (uint32_t)bv, vs, (uint32_t)bs);
-    }
+    th.join();
+    if (perr) std::rethrow_exception(perr);
+    if (chunked) pc->chunks = pc->csl.load(ctx, lplan, vs) && pc->csu.load(ctx, uplan, vs);
     if (!pc->chunks)
     {
         if (pc->mode == B2S_TRSV_CHUNK) pc->mode = B2S_TRSV_SYNCFREE;
-        pc->su.build(ctx, nb, pc->U.rp.p, pc->U.ci.p, false);
+        if (nb) pc->su.build_host(ctx, ulev);
         pc->sfl.init(ctx, nb);
         pc->sfu.init(ctx, nb);
     }

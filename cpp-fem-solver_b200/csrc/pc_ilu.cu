@@ -25,6 +25,9 @@
 #include "trisolve.cuh"
 #include "trsv_chunk.cuh"
 
+#include <exception>
+#include <thread>
+
 namespace b2s {
 
 // ------------------------------------------------------------ pattern split
@@ -225,46 +228,27 @@ __global__ void k_tr_count(uint32_t n, const uint32_t* __restrict__ rp, const ui
             if (ci[p] < i) atomicAdd(&cnt[ci[p]], 1u);
 }
 
-__global__ void k_tr_fill(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
-                          const double* __restrict__ v, const uint32_t* __restrict__ trp, uint32_t* __restrict__ off,
-                          uint32_t* __restrict__ tci, double* __restrict__ tv)
+// strict lower part of L -> its transpose (strict upper) as sorted CSR: a
+// stable sort of L's strict entries by column gives each row of the transpose
+// its columns in ascending order
+__global__ void k_strict_flag(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                              uint32_t* __restrict__ key)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
-        {
-            const uint32_t j = ci[p];
-            if (j < i)
-            {
-                const uint32_t d = trp[j] + atomicAdd(&off[j], 1u);
-                tci[d] = i;
-                tv[d] = v[p];
-            }
-        }
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p) key[p] = ci[p] < i ? ci[p] : n;  // diagonal entries sort last
 }
 
-__global__ void k_row_sort(uint32_t n, const uint32_t* __restrict__ rp, uint32_t* __restrict__ ci, double* __restrict__ v)
+__global__ void k_tr_gather(uint32_t nnz, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ row_of,
+                            const double* __restrict__ v, uint32_t* __restrict__ tci, double* __restrict__ tv)
 {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (uint32_t d = blockIdx.x * blockDim.x + threadIdx.x; d < nnz; d += gridDim.x * blockDim.x)
     {
-        const uint32_t a = rp[i], b = rp[i + 1];
-        for (uint32_t p = a + 1; p < b; ++p)
-        {
-            const uint32_t c = ci[p];
-            const double x = v[p];
-            uint32_t q = p;
-            while (q > a && ci[q - 1] > c)
-            {
-                ci[q] = ci[q - 1];
-                v[q] = v[q - 1];
-                --q;
-            }
-            ci[q] = c;
-            v[q] = x;
-        }
+        const uint32_t p = perm[d];
+        tci[d] = row_of[p];
+        tv[d] = v[p];
     }
 }
 
-// strict lower part of L -> its transpose (strict upper) as sorted CSR
 static void transpose_strict(b2s_ctx* ctx, const Csr32& L, Csr32& T)
 {
     const uint32_t n = L.n;
@@ -276,10 +260,12 @@ static void transpose_strict(b2s_ctx* ctx, const Csr32& L, Csr32& T)
     T.nnz = exclusive_scan(ctx, cnt.p, T.rp.p, n);
     T.ci.alloc(T.nnz ? T.nnz : 1);
     T.v.alloc(T.nnz ? T.nnz : 1);
-    B2S_CUDA(cudaMemsetAsync(cnt.p, 0, cnt.bytes(), ctx->stream));
-    B2S_LAUNCH(ctx, k_tr_fill, stream_grid(ctx, n), kThreads, 0, n, L.rp.p, L.ci.p, L.v.p, T.rp.p, cnt.p, T.ci.p,
-               T.v.p);
-    B2S_LAUNCH(ctx, k_row_sort, stream_grid(ctx, n), kThreads, 0, n, T.rp.p, T.ci.p, T.v.p);
+    if (!T.nnz) return;
+    // sort keys: the column of a strict entry, n for a diagonal one (those land after all strict entries)
+    DBuf<uint32_t> key(L.nnz ? L.nnz : 1), perm, row_of;
+    B2S_LAUNCH(ctx, k_strict_flag, stream_grid(ctx, n), kThreads, 0, n, L.rp.p, L.ci.p, key.p);
+    transpose_order(ctx, n, n + 1, L.rp.p, key.p, L.nnz, perm, row_of);
+    B2S_LAUNCH(ctx, k_tr_gather, stream_grid(ctx, T.nnz), kThreads, 0, T.nnz, perm.p, row_of.p, L.v.p, T.ci.p, T.v.p);
 }
 
 // ------------------------------------------------------------ triangular solves
@@ -338,7 +324,8 @@ struct Tri
     LevelSchedule sched;
     SyncFree sf;
     ChunkSchedule cs;
-    bool has_chunks = false;
+    bool has_chunks = false, sched_ready = false;
+    std::vector<uint32_t> h_level;  // host copy of the rows' levels (compute_levels), when known
 
     template <bool LOWER, bool UNIT, typename VT, typename XT, typename RT>
     void run_t(b2s_ctx* ctx, int mode, const VT* v, const VT* d, const RT* rhs, XT* x, double* out64, const int* done)
@@ -364,23 +351,31 @@ struct Tri
             run_t<false, false, VT, XT, RT>(ctx, mode, v, d, rhs, x, out64, done);
     }
 
-    // vs: bytes of the factor values the solves will use (8 FP64, 4 FP32)
-    void prepare(b2s_ctx* ctx, const Csr32& mat, bool lo, bool un, int mode, uint32_t vs)
+    void init(const Csr32& mat, bool lo, bool un)
     {
         m = &mat;
         lower = lo;
         unit = un;
         n = mat.n;
-        sched.build(ctx, n, mat.rp.p, mat.ci.p, lo);
+    }
+
+    // level schedule: the factorisation, the level / sync-free solves and export use it
+    void ensure_sched(b2s_ctx* ctx)
+    {
+        if (sched_ready) return;
+        if (h_level.size() == n && n)
+            sched.build_host(ctx, h_level);
+        else
+            sched.build(ctx, n, m->rp.p, m->ci.p, lower);
         sf.init(ctx, n);
-        if (mode == B2S_TRSV_CHUNK && n)
-        {
-            std::vector<uint32_t> hrp(n + 1), hci(mat.nnz ? mat.nnz : 1);
-            d2h(ctx, hrp.data(), mat.rp.p, (n + 1) * sizeof(uint32_t));
-            d2h(ctx, hci.data(), mat.ci.p, mat.nnz * sizeof(uint32_t));
-            sync(ctx);
-            has_chunks = cs.build(ctx, n, hrp, hci, lo, un ? 0u : 1u, vs);
-        }
+        sched_ready = true;
+    }
+
+    // a host chunk plan -> device; falls back to the level schedule when no plan is usable
+    void load_chunks(b2s_ctx* ctx, int mode, const ChunkPlan* plan, uint32_t vs)
+    {
+        has_chunks = mode == B2S_TRSV_CHUNK && n && plan && cs.load(ctx, *plan, vs);
+        if (!has_chunks) ensure_sched(ctx);
     }
 
     // lay the final factor values out for the chunk schedule (no-op otherwise)
@@ -390,6 +385,37 @@ struct Tri
         if (has_chunks && sizeof(VT) <= cs.plan_vs) cs.pack<VT>(ctx, v, d);
     }
 };
+
+// Host analysis of a factor pair, run on a host thread while the device
+// factorises: the levels of the upper triangle and, for the chunk schedule,
+// the chunk plans of both triangles.
+struct HostAnalysis
+{
+    std::vector<uint32_t> up_rp, up_ci;  // upper pattern when it is derived on the host
+    std::vector<uint32_t> up_level;
+    ChunkPlan lo_plan, up_plan;
+    bool chunked = false;
+    std::exception_ptr error;
+    std::thread th;
+    ~HostAnalysis()
+    {
+        if (th.joinable()) th.join();
+    }
+    void wait()
+    {
+        if (th.joinable()) th.join();
+        if (error) std::rethrow_exception(error);
+    }
+};
+
+static void copy_pattern(b2s_ctx* ctx, const Csr32& M, std::vector<uint32_t>& rp, std::vector<uint32_t>& ci)
+{
+    rp.resize((size_t)M.n + 1);
+    ci.resize(M.nnz ? M.nnz : 1);
+    d2h(ctx, rp.data(), M.rp.p, ((size_t)M.n + 1) * sizeof(uint32_t));
+    d2h(ctx, ci.data(), M.ci.p, (size_t)M.nnz * sizeof(uint32_t));
+    sync(ctx);
+}
 
 __global__ void k_f64_to_f32(const double* __restrict__ a, float* __restrict__ b, uint64_t n)
 {
@@ -416,8 +442,10 @@ static void export_csr(b2s_ctx* ctx, const Csr32& m, uint64_t* sizes, uint32_t* 
     sync(ctx);
 }
 
-static void export_levels(b2s_ctx* ctx, const LevelSchedule& s, uint64_t* sizes, uint32_t* ci)
+static void export_levels(b2s_ctx* ctx, Tri& t, uint64_t* sizes, uint32_t* ci)
 {
+    t.ensure_sched(ctx);
+    const LevelSchedule& s = t.sched;
     sizes[0] = 0;
     sizes[1] = s.n;
     sizes[2] = 0;
@@ -467,8 +495,8 @@ struct PcIC0 final : PcImpl
             sync(ctx);
             return;
         }
-        if (what == "levels.L") return export_levels(ctx, fwd.sched, sizes, ci);
-        if (what == "levels.U") return export_levels(ctx, bwd.sched, sizes, ci);
+        if (what == "levels.L") return export_levels(ctx, fwd, sizes, ci);
+        if (what == "levels.U") return export_levels(ctx, bwd, sizes, ci);
         PcImpl::export_data(ctx, what, sizes, rp, ci, v);
     }
 };
@@ -496,29 +524,63 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
 {
     need(A.n == A.m, B2S_SHAPE, "IC(0) needs a square matrix");
     auto pc = std::make_unique<PcIC0>();
-    pc->n = A.n;
+    const uint32_t n = A.n;
+    pc->n = n;
     pc->mode = pick_trsv(o);
     pc->fp32 = o.precision != B2S_FP64;
+    const uint32_t vs = pc->fp32 ? 4 : 8;
     DBuf<unsigned long long> err(1);
     const unsigned long long none = ~0ull;
     h2d(ctx, err.p, &none, sizeof(none));
     split(ctx, A, 0, pc->L, nullptr, err.p);
     check_err(ctx, err, "IC(0) failed");
-    pc->diag.alloc(A.n ? A.n : 1);
-    pc->fwd.prepare(ctx, pc->L, true, false, pc->mode, pc->fp32 ? 4 : 8);
+    pc->diag.alloc(n ? n : 1);
+    // host analysis of L: levels (for the factorisation) here, the rest on a thread
+    std::vector<uint32_t> hrp, hci;
+    copy_pattern(ctx, pc->L, hrp, hci);
+    pc->fwd.init(pc->L, true, false);
+    compute_levels(n, hrp.data(), hci.data(), true, pc->fwd.h_level);
+    pc->fwd.ensure_sched(ctx);
+    HostAnalysis ha;
+    ha.chunked = pc->mode == B2S_TRSV_CHUNK && n;
+    ha.th = std::thread([&ha, &hrp, &hci, &pc, n, vs] {
+        try
+        {
+            strict_transpose(n, hrp.data(), hci.data(), true, ha.up_rp, ha.up_ci);
+            compute_levels(n, ha.up_rp.data(), ha.up_ci.data(), false, ha.up_level);
+            if (ha.chunked)
+            {
+                ha.lo_plan = plan_chunks(n, hrp.data(), hci.data(), true, 1, vs, vs, 8, kChunkSmemBudget, 1,
+                                         &pc->fwd.h_level);
+                ha.up_plan = plan_chunks(n, ha.up_rp.data(), ha.up_ci.data(), false, 1, vs, vs, 8, kChunkSmemBudget, 1,
+                                         &ha.up_level);
+            }
+        }
+        catch (...)
+        {
+            ha.error = std::current_exception();
+        }
+    });
     pc->fwd.d64 = pc->diag.p;
     ic0_factor_inplace(ctx, pc->fwd.sched, pc->L.rp.p, pc->L.ci.p, pc->L.v.p, pc->diag.p, "IC(0) failed");
     if (corr) corr->correct(ctx, A, pc->L.rp.p, pc->L.ci.p, pc->L.nnz, pc->L.v.p, pc->diag.p);
     transpose_strict(ctx, pc->L, pc->LT);
-    pc->bwd.prepare(ctx, pc->LT, false, false, pc->mode, pc->fp32 ? 4 : 8);
-    pc->y.alloc(A.n ? A.n : 1);
+    pc->y.alloc(n ? n : 1);
     if (pc->fp32)
     {
         to_f32(ctx, pc->L.v, pc->L.v32, pc->L.nnz);
         to_f32(ctx, pc->LT.v, pc->LT.v32, pc->LT.nnz);
-        to_f32(ctx, pc->diag, pc->diag32, A.n);
-        pc->y32.alloc(A.n ? A.n : 1);
-        pc->z32.alloc(A.n ? A.n : 1);
+        to_f32(ctx, pc->diag, pc->diag32, n);
+        pc->y32.alloc(n ? n : 1);
+        pc->z32.alloc(n ? n : 1);
+    }
+    ha.wait();
+    pc->bwd.init(pc->LT, false, false);
+    pc->bwd.h_level = std::move(ha.up_level);
+    pc->fwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.lo_plan : nullptr, vs);
+    pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
+    if (pc->fp32)
+    {
         pc->fwd.pack<float>(ctx, pc->L.v32.p, pc->diag32.p);
         pc->bwd.pack<float>(ctx, pc->LT.v32.p, pc->diag32.p);
     }
@@ -570,8 +632,8 @@ struct PcILU0 final : PcImpl
     {
         if (what == "ilu0.L") return export_csr(ctx, L, sizes, rp, ci, v);
         if (what == "ilu0.U") return export_csr(ctx, U, sizes, rp, ci, v);
-        if (what == "levels.L") return export_levels(ctx, fwd.sched, sizes, ci);
-        if (what == "levels.U") return export_levels(ctx, bwd.sched, sizes, ci);
+        if (what == "levels.L") return export_levels(ctx, fwd, sizes, ci);
+        if (what == "levels.U") return export_levels(ctx, bwd, sizes, ci);
         PcImpl::export_data(ctx, what, sizes, rp, ci, v);
     }
 };
@@ -592,6 +654,7 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     pc->n = n;
     pc->mode = pick_trsv(o);
     pc->fp32 = o.precision != B2S_FP64;
+    const uint32_t vs = pc->fp32 ? 4 : 8;
     DBuf<unsigned long long> err(1);
     const unsigned long long none = ~0ull;
     h2d(ctx, err.p, &none, sizeof(none));
@@ -599,7 +662,32 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     split(ctx, A, 1, pc->L, nullptr, err.p);
     split(ctx, A, 2, pc->U, pc->dix.p, err.p);
     check_err(ctx, err, "ILU(0) failed");
-    pc->fwd.prepare(ctx, pc->L, true, true, pc->mode, pc->fp32 ? 4 : 8);
+    // host analysis: levels of L here (for the factorisation), the rest on a thread
+    std::vector<uint32_t> lrp, lci, urp, uci;
+    copy_pattern(ctx, pc->L, lrp, lci);
+    copy_pattern(ctx, pc->U, urp, uci);
+    pc->fwd.init(pc->L, true, true);
+    compute_levels(n, lrp.data(), lci.data(), true, pc->fwd.h_level);
+    pc->fwd.ensure_sched(ctx);
+    HostAnalysis ha;
+    ha.chunked = pc->mode == B2S_TRSV_CHUNK && n;
+    ha.th = std::thread([&ha, &lrp, &lci, &urp, &uci, &pc, n, vs] {
+        try
+        {
+            compute_levels(n, urp.data(), uci.data(), false, ha.up_level);
+            if (ha.chunked)
+            {
+                ha.lo_plan = plan_chunks(n, lrp.data(), lci.data(), true, 0, vs, vs, 8, kChunkSmemBudget, 1,
+                                         &pc->fwd.h_level);
+                ha.up_plan = plan_chunks(n, urp.data(), uci.data(), false, 1, vs, vs, 8, kChunkSmemBudget, 1,
+                                         &ha.up_level);
+            }
+        }
+        catch (...)
+        {
+            ha.error = std::current_exception();
+        }
+    });
     // factor, level by level
     for (uint32_t l = 0; l < pc->fwd.sched.nlev; ++l)
     {
@@ -610,7 +698,6 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     check_err(ctx, err, "ILU(0) failed");
     pc->udiag.alloc(n ? n : 1);
     if (n) B2S_LAUNCH(ctx, k_gather_diag, stream_grid(ctx, n), kThreads, 0, n, pc->U.v.p, pc->dix.p, pc->udiag.p);
-    pc->bwd.prepare(ctx, pc->U, false, false, pc->mode, pc->fp32 ? 4 : 8);
     pc->y.alloc(n ? n : 1);
     if (pc->fp32)
     {
@@ -619,6 +706,14 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
         to_f32(ctx, pc->udiag, pc->udiag32, n);
         pc->y32.alloc(n ? n : 1);
         pc->z32.alloc(n ? n : 1);
+    }
+    ha.wait();
+    pc->bwd.init(pc->U, false, false);
+    pc->bwd.h_level = std::move(ha.up_level);
+    pc->fwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.lo_plan : nullptr, vs);
+    pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
+    if (pc->fp32)
+    {
         pc->fwd.pack<float>(ctx, pc->L.v32.p, (const float*)nullptr);
         pc->bwd.pack<float>(ctx, pc->U.v32.p, pc->udiag32.p);
     }

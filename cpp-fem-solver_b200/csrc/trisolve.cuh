@@ -4,6 +4,8 @@
 #pragma once
 #include <cub/cub.cuh>
 
+#include <algorithm>
+
 #include "syncfree.cuh"
 
 namespace b2s {
@@ -45,6 +47,40 @@ static __global__ void k_level_bounds(const uint32_t* __restrict__ sorted_lev, u
     }
 }
 
+// ------------------------------------------------------------ stable transpose order
+
+static __global__ void k_entry_rows(uint32_t n, const uint32_t* __restrict__ rp, uint32_t* __restrict__ row_of)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p) row_of[p] = i;
+}
+
+// Entry order of a CSR pattern's transpose: after the call, perm[d] (d in
+// column-major order) is the index of the d-th entry of the transpose in the
+// original arrays, and row_of[p] is the row of entry p.  A stable radix sort
+// by column keeps the rows of each column ascending, so the transpose rows
+// come out sorted without a per-row sort.  Entries with ci[p] >= ncols are
+// not expected.
+static inline void transpose_order(b2s_ctx* ctx, uint32_t nrows, uint32_t ncols, const uint32_t* rp,
+                                   const uint32_t* ci, uint32_t nnz, DBuf<uint32_t>& perm, DBuf<uint32_t>& row_of)
+{
+    perm.alloc(nnz ? nnz : 1);
+    row_of.alloc(nnz ? nnz : 1);
+    if (!nnz) return;
+    B2S_LAUNCH(ctx, k_entry_rows, stream_grid(ctx, nrows), kThreads, 0, nrows, rp, row_of.p);
+    DBuf<uint32_t> iota(nnz), keys_out(nnz);
+    B2S_LAUNCH(ctx, k_iota, stream_grid(ctx, nnz), kThreads, 0, iota.p, nnz);
+    int end_bit = 1;
+    while (end_bit < 32 && (ncols - 1) >> end_bit) ++end_bit;
+    size_t bytes = 0;
+    B2S_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, ci, keys_out.p, iota.p, perm.p, (int)nnz, 0, end_bit,
+                                             ctx->stream));
+    DBuf<uint8_t> tmp(bytes ? bytes : 1);
+    B2S_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, bytes, ci, keys_out.p, iota.p, perm.p, (int)nnz, 0, end_bit,
+                                             ctx->stream));
+    ctx->launches += 1;
+}
+
 // ------------------------------------------------------------ level sets
 
 template <bool LOWER>
@@ -78,6 +114,22 @@ struct LevelSchedule
     DBuf<uint32_t> level;       // level of each row
     DBuf<uint32_t> rows;        // rows sorted by (level, index)
     std::vector<uint32_t> h_ptr;  // nlev + 1
+
+    // from levels computed on the host (compute_levels): rows sorted by (level, index)
+    void build_host(b2s_ctx* ctx, const std::vector<uint32_t>& lev)
+    {
+        n = (uint32_t)lev.size();
+        uint32_t maxl = 0;
+        for (uint32_t l : lev) maxl = std::max(maxl, l);
+        nlev = n ? maxl + 1 : 0;
+        h_ptr.assign((size_t)nlev + 1, 0);
+        for (uint32_t l : lev) h_ptr[l + 1]++;
+        for (uint32_t l = 0; l < nlev; ++l) h_ptr[l + 1] += h_ptr[l];
+        std::vector<uint32_t> hrows(n ? n : 1), off(h_ptr.begin(), h_ptr.end() - 1);
+        for (uint32_t i = 0; i < n; ++i) hrows[off[lev[i]]++] = i;
+        level = upload(ctx, lev);
+        rows = upload(ctx, hrows);
+    }
 
     void build(b2s_ctx* ctx, uint32_t nrows, const uint32_t* rp, const uint32_t* ci, bool lower)
     {

@@ -237,6 +237,11 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
     if (warp > (uint32_t)NW) return;  // helpers only stage
 
     // ---- 2b. compute warps
+    // Everything a row needs except its operands' values is fixed before the
+    // traversal: its record, column entries, coefficients, right-hand side
+    // and divisor.  The warp reads those for the next level while it solves
+    // the current one, so a level's critical path is the operand loads, the
+    // products, one divide and the barrier.
     const VT* sv = reinterpret_cast<const VT*>(smem + L.sv);
     const VT* sd = reinterpret_cast<const VT*>(smem + L.sd);
     const uint16_t* slc = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.slc);
@@ -244,64 +249,84 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
     const uint16_t* slv = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.slv);
     XT* sx = reinterpret_cast<XT*>(smem + L.sx);
     const RT* sr = reinterpret_cast<const RT*>(smem + L.sr);
+    struct Ops
+    {
+        uint32_t pr = 0, e0 = 0, e1 = 0;
+        uint32_t m[4] = {0u, 0u, 0u, 0u};
+        VT vv[4] = {VT(0), VT(0), VT(0), VT(0)};
+        XT rhs = XT(0), dv = XT(1);
+    };
+    auto fetch = [&](uint32_t t, uint32_t tend, Ops& o) {
+        if (t >= tend) return;
+        const uint2 rw = rec[t];
+        o.pr = rec_perm(rw.x);
+        o.e0 = rec_e0(rw.x);
+        o.e1 = rec_e1(rw.y);
+        o.rhs = (XT)sr[o.pr & 0x7fffu];
+        if (!UNIT) o.dv = (XT)sd[t];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+        {
+            const bool on = o.e0 + q < o.e1;
+            o.m[q] = on ? slc[o.e0 + q] : 0u;
+            o.vv[q] = on ? sv[o.e0 + q] : VT(0);
+        }
+    };
+    auto solve_row = [&](uint32_t t, const Ops& o) {
+        XT sum = o.rhs;
+        if (o.e1 - o.e0 <= 4)
+        {
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (o.e0 + q < o.e1 && (o.m[q] & 0x8000u)) slot_wait(xr, o.m[q] & 0x7fffu, a.ctl.err);
+            XT xj[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) xj[q] = (o.m[q] & 0x8000u) ? xv[o.m[q] & 0x7fffu] : sx[o.m[q]];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (o.e0 + q < o.e1) sum -= (XT)o.vv[q] * xj[q];
+        }
+        else
+        {
+            for (uint32_t e = o.e0; e < o.e1; ++e)
+            {
+                const uint32_t m = slc[e];
+                XT xj;
+                if (m & 0x8000u)
+                {
+                    const uint32_t s = m & 0x7fffu;
+                    slot_wait(xr, s, a.ctl.err);
+                    xj = xv[s];
+                }
+                else
+                    xj = sx[m];
+                sum -= (XT)sv[e] * xj;
+            }
+        }
+        const XT r = UNIT ? sum : sum / o.dv;
+        sx[t] = r;
+        const uint32_t row = D.lo + (o.pr & 0x7fffu);
+        x[row] = r;
+        if (out64) out64[row] = (double)r;
+        if (o.pr & 0x8000u) xch_put<XT>(a.xch + (size_t)row * 2, r, epoch);
+    };
     uint32_t t0 = 0, t1 = slv[1];
+    Ops cur;
+    fetch(tid, t1, cur);
     for (uint32_t l = 0; l < D.nl; ++l)
     {
-        const uint32_t tn = l + 2 <= D.nl ? slv[l + 2] : t1;  // the next level's end, read ahead
-        for (uint32_t t = t0 + tid; t < t1; t += NW * 32)
+        const uint32_t tn = l + 2 <= D.nl ? slv[l + 2] : t1;  // the next level's end
+        Ops nxt;
+        fetch(t1 + tid, tn, nxt);  // the next level's first pass, read ahead
+        if (t0 + tid < t1) solve_row(t0 + tid, cur);
+        for (uint32_t t = t0 + tid + NW * 32; t < t1; t += NW * 32)
         {
-            const uint2 rw = rec[t];
-            const uint32_t pr = rec_perm(rw.x), k = pr & 0x7fffu;
-            const uint32_t e0 = rec_e0(rw.x), e1 = rec_e1(rw.y);
-            XT sum = (XT)sr[k];
-            if (e1 - e0 <= 4)
-            {
-                // short rows: all column entries, then all operands, then the
-                // products in column order
-                uint32_t m[4];
-                VT vv[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                {
-                    const bool on = e0 + q < e1;
-                    m[q] = on ? slc[e0 + q] : 0u;
-                    vv[q] = on ? sv[e0 + q] : VT(0);
-                }
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    if (e0 + q < e1 && (m[q] & 0x8000u)) slot_wait(xr, m[q] & 0x7fffu, a.ctl.err);
-                XT xj[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) xj[q] = (m[q] & 0x8000u) ? xv[m[q] & 0x7fffu] : sx[m[q]];
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    if (e0 + q < e1) sum -= (XT)vv[q] * xj[q];
-            }
-            else
-            {
-                for (uint32_t e = e0; e < e1; ++e)
-                {
-                    const uint32_t m = slc[e];
-                    XT xj;
-                    if (m & 0x8000u)
-                    {
-                        const uint32_t s = m & 0x7fffu;
-                        slot_wait(xr, s, a.ctl.err);
-                        xj = xv[s];
-                    }
-                    else
-                        xj = sx[m];
-                    sum -= (XT)sv[e] * xj;
-                }
-            }
-            const XT r = UNIT ? sum : sum / (XT)sd[t];
-            sx[t] = r;
-            const uint32_t row = D.lo + k;
-            x[row] = r;
-            if (out64) out64[row] = (double)r;
-            if (pr & 0x8000u) xch_put<XT>(a.xch + (size_t)row * 2, r, epoch);
+            Ops o;
+            fetch(t, t1, o);
+            solve_row(t, o);
         }
         compute_barrier<NW>();
+        cur = nxt;
         t0 = t1;
         t1 = tn;
     }
@@ -528,12 +553,19 @@ struct ChunkSchedule
     bool build(b2s_ctx* ctx, uint32_t nrows, const std::vector<uint32_t>& h_rp, const std::vector<uint32_t>& h_ci,
                bool lo, uint32_t divisor_values, uint32_t vs, uint32_t block = 1)
     {
-        n = nrows;
-        lower = lo;
-        bs = block;
-        dv = divisor_values;
+        return load(ctx, plan_chunks(nrows, h_rp.data(), h_ci.data(), lo, divisor_values, vs, vs, 8, kChunkSmemBudget,
+                                     block),
+                    vs);
+    }
+
+    // a plan made on the host (plan_chunks with xs = vs, rs = 8) -> device
+    bool load(b2s_ctx* ctx, const ChunkPlan& P, uint32_t vs)
+    {
+        n = P.n;
+        lower = P.lower;
+        bs = P.bs;
+        dv = P.dv;
         plan_vs = vs;
-        ChunkPlan P = plan_chunks(n, h_rp.data(), h_ci.data(), lo, dv, vs, vs, 8, kChunkSmemBudget, bs);
         if (!P.ok) return false;
         nchunks = (uint32_t)P.desc.size();
         // one compute warp while a level needs at most two passes of it

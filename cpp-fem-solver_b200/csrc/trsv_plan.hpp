@@ -153,13 +153,50 @@ struct ChunkPlan
     }
 };
 
+// Global level of each row: the longest dependency chain ending at it (0 for
+// a row without dependencies).  Dependencies are j < i (lower) or j > i (upper).
+inline void compute_levels(uint32_t n, const uint32_t* rp, const uint32_t* ci, bool lower, std::vector<uint32_t>& lev)
+{
+    lev.assign(n, 0);
+    for (uint32_t t = 0; t < n; ++t)
+    {
+        const uint32_t r = lower ? t : n - 1 - t;
+        uint32_t l = 0;
+        for (uint32_t p = rp[r]; p < rp[r + 1]; ++p)
+        {
+            const uint32_t j = ci[p];
+            if (lower ? j < r : j > r) l = std::max(l, lev[j] + 1);
+        }
+        lev[r] = l;
+    }
+}
+
+// Pattern of the strict transpose of a triangle (j < i entries of rp/ci for
+// lower -> rows j with columns i ascending), on the host.
+inline void strict_transpose(uint32_t n, const uint32_t* rp, const uint32_t* ci, bool lower,
+                             std::vector<uint32_t>& trp, std::vector<uint32_t>& tci)
+{
+    trp.assign((size_t)n + 1, 0);
+    for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+            if (lower ? ci[p] < i : ci[p] > i) trp[ci[p] + 1]++;
+    for (uint32_t i = 0; i < n; ++i) trp[i + 1] += trp[i];
+    tci.resize(trp[n] ? trp[n] : 1);
+    std::vector<uint32_t> off(trp.begin(), trp.end() - 1);
+    for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+            if (lower ? ci[p] < i : ci[p] > i) tci[off[ci[p]]++] = i;
+}
+
 // Plan the chunks of a triangle with (block) CSR pattern rp/ci (dependency
 // entries are j < i for lower, j > i for upper; other entries are ignored).
 // vs, xs, rs: element sizes of values, solution and right-hand side the chunks
 // are sized for; bs: block size; dv: divisor values per row (0 for a unit
 // triangle, 1 for a scalar divisor, bs*bs for an inverse block).
+// glev: the rows' global levels when the caller has them (compute_levels).
 inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci, bool lower, uint32_t dv, uint32_t vs,
-                             uint32_t xs, uint32_t rs, uint32_t budget = kChunkSmemBudget, uint32_t bs = 1)
+                             uint32_t xs, uint32_t rs, uint32_t budget = kChunkSmemBudget, uint32_t bs = 1,
+                             const std::vector<uint32_t>* glev_in = nullptr)
 {
     ChunkPlan P;
     P.n = n;
@@ -173,19 +210,9 @@ inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci,
         return P;
     }
     auto is_dep = [&](uint32_t i, uint32_t j) { return lower ? j < i : j > i; };
-    // global levels, in processing order
-    std::vector<uint32_t> glev(n, 0);
-    for (uint32_t t = 0; t < n; ++t)
-    {
-        const uint32_t r = lower ? t : n - 1 - t;
-        uint32_t l = 0;
-        for (uint32_t p = rp[r]; p < rp[r + 1]; ++p)
-        {
-            const uint32_t j = ci[p];
-            if (is_dep(r, j)) l = std::max(l, glev[j] + 1);
-        }
-        glev[r] = l;
-    }
+    std::vector<uint32_t> glev_own;
+    if (!glev_in) compute_levels(n, rp, ci, lower, glev_own);
+    const std::vector<uint32_t>& glev = glev_in ? *glev_in : glev_own;
     std::vector<uint32_t> stamp(n, 0);     // chunk id + 1 when j already has a slot in the chunk
     std::vector<uint32_t> slot_of(n, 0);   // slot of j in the chunk that stamped it
     std::vector<uint32_t> llev(n, 0);      // local level
