@@ -28,8 +28,9 @@
 // with 1 us sleeps, and give up with B2S_TIMEOUT after a fixed bound.
 //
 // Every row is summed in its column order with the reference's arithmetic
-// (sum = rhs; sum -= v * x_j; x = sum / d), so the result equals the level /
-// sync-free schedules bit for bit.
+// (sum = rhs; sum -= v * x_j; x = sum / d), so in FP64 the result equals the
+// level / sync-free schedules bit for bit.  The FP32 solves multiply by a
+// reciprocal of d packed once per factorisation (one extra rounding).
 #pragma once
 #include "syncfree.cuh"
 #include "trsv_plan.hpp"
@@ -303,7 +304,8 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
                 sum -= (XT)sv[e] * xj;
             }
         }
-        const XT r = UNIT ? sum : sum / o.dv;
+        // FP64 divides, as the reference; FP32 multiplies by the packed reciprocal
+        const XT r = UNIT ? sum : (sizeof(XT) == 4 ? sum * o.dv : sum / o.dv);
         sx[t] = r;
         const uint32_t row = D.lo + (o.pr & 0x7fffu);
         x[row] = r;
@@ -348,12 +350,14 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
 
 // Value blob of one chunk: dependency values (bs*bs per entry), then the
 // divisors by position (dv per row: none, a scalar or an inverse block).
+// recip: store 1/d, rounded once from FP64, instead of d (the FP32 scalar
+// solves multiply by it).
 template <typename VT>
 __global__ void __launch_bounds__(kThreads) k_chunk_pack(const ChunkDesc* __restrict__ desc,
                                                          const uint4* __restrict__ meta,
                                                          const uint32_t* __restrict__ src, const VT* __restrict__ v,
                                                          const VT* __restrict__ d, uint4* __restrict__ vals,
-                                                         uint32_t bs, uint32_t dv)
+                                                         uint32_t bs, uint32_t dv, int recip)
 {
     const ChunkDesc D = desc[blockIdx.x];
     const SmemLayout L = smem_layout(D.nr, D.nd, D.nl, D.ns, sizeof(VT), sizeof(VT), sizeof(VT), bs, dv);
@@ -372,7 +376,8 @@ __global__ void __launch_bounds__(kThreads) k_chunk_pack(const ChunkDesc* __rest
         for (uint32_t e = threadIdx.x; e < nd; e += blockDim.x)
         {
             const uint32_t t = e / dv;
-            sd[e] = t < D.nr ? d[(size_t)(D.lo + (rec_perm(recw[2 * t]) & 0x7fffu)) * dv + e % dv] : VT(0);
+            const VT dd = t < D.nr ? d[(size_t)(D.lo + (rec_perm(recw[2 * t]) & 0x7fffu)) * dv + e % dv] : VT(0);
+            sd[e] = (recip && t < D.nr) ? (VT)(1.0 / (double)dd) : dd;
         }
     }
 }
@@ -604,7 +609,8 @@ struct ChunkSchedule
     void pack(b2s_ctx* ctx, const VT* v, const VT* d)
     {
         if (!nchunks) return;
-        B2S_LAUNCH(ctx, k_chunk_pack<VT>, nchunks, kThreads, 0, desc.p, meta.p, src.p, v, d, vals.p, bs, dv);
+        const int recip = sizeof(VT) == 4 && bs == 1 && dv == 1;
+        B2S_LAUNCH(ctx, k_chunk_pack<VT>, nchunks, kThreads, 0, desc.p, meta.p, src.p, v, d, vals.p, bs, dv, recip);
         packed_v = v;
         packed_d = d;
         packed_vs = sizeof(VT);
