@@ -630,6 +630,63 @@ __global__ void k_mm_numeric(uint32_t nr, const uint32_t* __restrict__ arp, cons
     }
 }
 
+// The same product, one warp per C row: the warp walks A's row entries pa in
+// order and its lanes take the entries pb of B's row k in parallel.  The
+// entries of one B row have distinct columns, so within a pa no two lanes add
+// into the same C block, and a __syncwarp between pa keeps every C block's
+// additions in pa order -- the order of k_mm_numeric.  Used when B's rows are
+// long (R (A P)); for short rows (A P) the thread-per-row kernel is faster.
+template <int BS>
+__global__ void k_mm_numeric_warp(uint32_t nr, const uint32_t* __restrict__ arp, const uint32_t* __restrict__ aci,
+                                  const double* __restrict__ av, const uint32_t* __restrict__ brp,
+                                  const uint32_t* __restrict__ bci, const double* __restrict__ bv,
+                                  const uint32_t* __restrict__ crp, const uint32_t* __restrict__ cci,
+                                  double* __restrict__ cv)
+{
+    constexpr int BV = BS * BS;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < nr; i += warps)
+    {
+        const uint32_t c0 = crp[i], c1 = crp[i + 1];
+        for (uint32_t s = c0 * BV + lane; s < c1 * BV; s += 32) cv[s] = 0.0;
+        __syncwarp();
+        for (uint32_t pa = arp[i]; pa < arp[i + 1]; ++pa)
+        {
+            const uint32_t k = aci[pa];
+            double ab[BV];
+#pragma unroll
+            for (int q = 0; q < BV; ++q) ab[q] = av[(size_t)pa * BV + q];
+            for (uint32_t pb = brp[k] + lane; pb < brp[k + 1]; pb += 32)
+            {
+                const uint32_t j = bci[pb];
+                uint32_t lo = c0, hi = c1;
+                while (lo < hi)
+                {
+                    const uint32_t mid = (lo + hi) / 2;
+                    if (cci[mid] < j)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                const double* bb = &bv[(size_t)pb * BV];
+                double* cb = &cv[(size_t)lo * BV];
+#pragma unroll
+                for (int r = 0; r < BS; ++r)
+#pragma unroll
+                    for (int c = 0; c < BS; ++c)
+                    {
+                        double sum = 0.0;
+#pragma unroll
+                        for (int m = 0; m < BS; ++m) sum += ab[r * BS + m] * bb[m * BS + c];
+                        cb[r * BS + c] += sum;
+                    }
+            }
+            __syncwarp();
+        }
+    }
+}
+
 template <int BS>
 void block_matmul(b2s_ctx* ctx, const BaijDev& A, const BaijDev& B, BaijDev& C)
 {
@@ -661,8 +718,17 @@ void block_matmul(b2s_ctx* ctx, const BaijDev& A, const BaijDev& B, BaijDev& C)
     if (nr)
     {
         B2S_LAUNCH(ctx, k_mm_unique_fill, stream_grid(ctx, nr), kThreads, 0, nr, off.p, sorted.p, C.rp.p, C.ci.p);
-        B2S_LAUNCH(ctx, k_mm_numeric<BS>, stream_grid(ctx, nr), kThreads, 0, nr, A.rp.p, A.ci.p, A.v.p, B.rp.p, B.ci.p,
-                   B.v.p, C.rp.p, C.ci.p, C.v.p);
+        // B's mean row length decides: warp per C row for long rows, thread per C row otherwise
+        if (B.nbr && B.nnzb >= 8ull * B.nbr)
+        {
+            const uint64_t warps = nr, ctas = (warps + kThreads / 32 - 1) / (kThreads / 32);
+            const unsigned grid = (unsigned)std::min<uint64_t>(ctas, (uint64_t)ctx->sm_count * 8);
+            B2S_LAUNCH(ctx, k_mm_numeric_warp<BS>, grid, kThreads, 0, nr, A.rp.p, A.ci.p, A.v.p, B.rp.p, B.ci.p,
+                       B.v.p, C.rp.p, C.ci.p, C.v.p);
+        }
+        else
+            B2S_LAUNCH(ctx, k_mm_numeric<BS>, stream_grid(ctx, nr), kThreads, 0, nr, A.rp.p, A.ci.p, A.v.p, B.rp.p,
+                       B.ci.p, B.v.p, C.rp.p, C.ci.p, C.v.p);
     }
     finish_baij(ctx, C);
 }

@@ -52,18 +52,46 @@ inline void cuda_check(cudaError_t e, const char* what)
 
 #define B2S_CUDA(call) ::b2s::cuda_check((call), #call)
 
-// ------------------------------------------------------------ device buffer
+// ---------------------------------------------------------- device memory
+//
+// Device memory comes from the device's stream-ordered pool and goes back to
+// it, so repeated set-ups reuse memory instead of paying for cudaMalloc and
+// for cudaFree's device-wide synchronisation (ctx.cu).  Allocations run on a
+// per-device allocation stream that is synchronised at once, so the memory is
+// ready for any stream.  A buffer remembers the stream of the context whose
+// API call allocated it, and its free is ordered after the work already on
+// that stream (an event the allocation stream waits on); when that stream is
+// gone the free is synchronous.
+namespace mem {
+struct Block
+{
+    void* p = nullptr;
+    cudaStream_t alloc_stream = nullptr;  // the pool's allocation stream of the block's device
+    cudaStream_t owner = nullptr;         // stream of the allocating context, or null
+};
+Block alloc(size_t bytes);  // throws Error on failure
+void free(const Block& b);
+cudaStream_t& current_stream();  // thread-local: the stream of the API call in progress
+void register_stream(cudaStream_t s);
+void unregister_stream(cudaStream_t s);
+}  // namespace mem
 
 template <typename T>
 struct DBuf
 {
     T* p = nullptr;
     size_t n = 0;
+    mem::Block blk;
     DBuf() = default;
     explicit DBuf(size_t count) { alloc(count); }
     DBuf(const DBuf&) = delete;
     DBuf& operator=(const DBuf&) = delete;
-    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), blk(o.blk)
+    {
+        o.p = nullptr;
+        o.n = 0;
+        o.blk = mem::Block{};
+    }
     DBuf& operator=(DBuf&& o) noexcept
     {
         if (this != &o)
@@ -71,8 +99,10 @@ struct DBuf
             release();
             p = o.p;
             n = o.n;
+            blk = o.blk;
             o.p = nullptr;
             o.n = 0;
+            o.blk = mem::Block{};
         }
         return *this;
     }
@@ -80,16 +110,11 @@ struct DBuf
     void alloc(size_t count)
     {
         release();
-        n = count;
         if (count)
         {
-            const cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-            if (e != cudaSuccess)
-            {
-                p = nullptr;
-                n = 0;
-                cuda_check(e, ("cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes").c_str());
-            }
+            blk = mem::alloc(count * sizeof(T));
+            p = static_cast<T*>(blk.p);
+            n = count;
         }
     }
     // grows (never shrinks); contents are not preserved
@@ -99,9 +124,10 @@ struct DBuf
     }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p) mem::free(blk);
         p = nullptr;
         n = 0;
+        blk = mem::Block{};
     }
     size_t bytes() const { return n * sizeof(T); }
 };
@@ -232,6 +258,13 @@ namespace b2s {
 template <typename F>
 b2s_status guarded(b2s_ctx* ctx, F&& f)
 {
+    // device buffers allocated by this call belong to the context's stream
+    struct StreamScope
+    {
+        cudaStream_t saved;
+        explicit StreamScope(cudaStream_t s) : saved(mem::current_stream()) { mem::current_stream() = s; }
+        ~StreamScope() { mem::current_stream() = saved; }
+    } scope(ctx ? ctx->stream : nullptr);
     try
     {
         f();

@@ -2,12 +2,14 @@
 //   BlockMatrix storage / cache_diag / matvec: blockMatrix.hpp:139-234
 //   BlockMatrix::gmres "blockjacobi":         blockMatrix.hpp:714-733
 //
-// The block matvec is staged like the CSR SpMV: a CTA copies the contiguous
-// block values [rp[r0], rp[r1]) * bs^2 doubles and their column indices into
-// shared memory with 16-byte loads (blocks are 72 bytes for bs = 3, so a
-// block is not 16-byte aligned on its own, but the CTA's whole range is read
-// as one coalesced stream), then one thread per (block row, component) sums
-// its row block by block, in the reference's order.
+// Block matvec (bs >= 2): a warp owns 32/bs consecutive block rows (one lane
+// per output component) and walks their blocks min(32, 256/bs^2) at a time.  The
+// lanes stream the blocks' values into the warp's shared memory (coalesced,
+// no L1 allocation), lane b gathers x_J of block b and forms the block's bs
+// row dots with the reference's association (blk_row_dot), and the lane of
+// output component (I, r) adds the dots of row I in block order -- the
+// reference's order, so y is bit-exact.  No CTA-wide barrier.  bs = 1 (the
+// scalar AMG levels, whose coarse rows are long) keeps the staged kernel.
 #include "block_ops.cuh"
 #include "spmv_staged.cuh"
 
@@ -19,6 +21,93 @@ struct BaijCap
     static constexpr int value = BS == 1 ? 3072 : BS == 2 ? 1024 : BS == 3 ? 512 : 256;
 };
 
+constexpr int kBaijCtasPerSm = 4;
+
+template <int BS>
+__global__ void __launch_bounds__(kThreads, kBaijCtasPerSm)
+    k_baij_warp(uint32_t nbr, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                const double* __restrict__ v, const double* __restrict__ x, double* __restrict__ y, const int* done)
+{
+    if (done && *done) return;
+    constexpr int BV = BS * BS;
+    constexpr int GR = 32 / BS;                        // block rows per warp group
+    constexpr int NB = 256 / BV < 32 ? 256 / BV : 32;  // blocks per pass: one lane per block
+    constexpr int PER = (NB * BV + 31) / 32;           // value loads per lane per pass
+    __shared__ double sval[kThreads / 32][NB * BV];
+    __shared__ double sdot[kThreads / 32][NB * BS];
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    double* V = sval[wid];
+    double* P = sdot[wid];
+    // one pass's operands in registers: its values and this lane's block column
+    auto load_pass = [&](uint32_t base, uint32_t nb, double* tv, uint32_t& J) {
+        const double* vb = v + (size_t)base * BV;
+#pragma unroll
+        for (int k = 0; k < PER; ++k)
+        {
+            const uint32_t q = k * 32 + lane;
+            tv[k] = q < nb * BV ? ld_stream(vb + q) : 0.0;
+        }
+        J = lane < nb ? ld_stream(ci + base + lane) : 0u;
+    };
+    const uint32_t ngroups = (nbr + GR - 1) / GR;
+    for (uint32_t g = blockIdx.x * (kThreads / 32) + wid; g < ngroups; g += gridDim.x * (kThreads / 32))
+    {
+        const uint32_t I0 = g * GR;
+        const uint32_t rows = min((uint32_t)GR, nbr - I0);
+        const bool out = lane < rows * BS;
+        const uint32_t I = I0 + lane / BS;
+        const uint32_t r = lane % BS;
+        const uint32_t a = out ? __ldg(&rp[I]) : 0u, b = out ? __ldg(&rp[I + 1]) : 0u;
+        const uint32_t p0 = __shfl_sync(0xffffffffu, a, 0);
+        const uint32_t p1 = __shfl_sync(0xffffffffu, b, (rows - 1) * BS);
+        double acc = 0.0;
+        double tv[PER];
+        uint32_t J = 0;
+        if (p0 < p1) load_pass(p0, min((uint32_t)NB, p1 - p0), tv, J);
+        for (uint32_t base = p0; base < p1; base += NB)
+        {
+            const uint32_t nb = min((uint32_t)NB, p1 - base);
+#pragma unroll
+            for (int k = 0; k < PER; ++k)
+            {
+                const uint32_t q = k * 32 + lane;
+                if (q < nb * BV) V[q] = tv[k];
+            }
+            double xv[BS];
+            if (lane < nb)
+#pragma unroll
+                for (int c = 0; c < BS; ++c) xv[c] = __ldg(&x[(size_t)J * BS + c]);
+            // the next pass's operands load while this pass computes
+            const uint32_t nbase = base + NB;
+            if (nbase < p1) load_pass(nbase, min((uint32_t)NB, p1 - nbase), tv, J);
+            __syncwarp();
+            if (lane < nb)
+#pragma unroll
+                for (int r2 = 0; r2 < BS; ++r2) P[lane * BS + r2] = blk_row_dot<BS>(&V[lane * BV + r2 * BS], xv);
+            __syncwarp();
+            if (out)
+            {
+                const uint32_t lo = a > base ? a : base, hi = b < base + nb ? b : base + nb;
+                for (uint32_t k = lo; k < hi; ++k) acc += P[(k - base) * BS + r];
+            }
+            __syncwarp();
+        }
+        if (out) y[(size_t)I * BS + r] = acc;
+    }
+}
+
+template <int BS>
+static void launch_baij(b2s_ctx* ctx, const BaijDev& A, const double* x, double* y, const int* done)
+{
+    constexpr int GR = 32 / BS;
+    const uint32_t groups = (A.nbr + GR - 1) / GR;
+    const uint32_t ctas = (groups + kThreads / 32 - 1) / (kThreads / 32);
+    const uint32_t cap = (uint32_t)ctx->sm_count * kBaijCtasPerSm;
+    B2S_LAUNCH(ctx, k_baij_warp<BS>, ctas < cap ? ctas : cap, kThreads, 0, A.nbr, A.rp.p, A.ci.p, A.v.p, x, y, done);
+}
+
+// 1x1 blocks (the AMG hierarchies' operators, rows of 7 to 100+ entries): a CTA
+// stages a contiguous block range in shared memory and one thread per row sums it.
 template <int BS>
 __global__ void __launch_bounds__(kThreads) k_baij_staged(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
                                                           const double* __restrict__ v,
@@ -80,15 +169,16 @@ __global__ void __launch_bounds__(kThreads) k_baij_staged(const uint32_t* __rest
     }
 }
 
+
 void baij_matvec(b2s_ctx* ctx, const BaijDev& A, const double* x, double* y, const int* done)
 {
     if (A.nbr == 0) return;
     switch (A.bs)
     {
         case 1: B2S_LAUNCH(ctx, k_baij_staged<1>, A.nblk, kThreads, 0, A.rp.p, A.ci.p, A.v.p, A.blk_row.p, x, y, done); break;
-        case 2: B2S_LAUNCH(ctx, k_baij_staged<2>, A.nblk, kThreads, 0, A.rp.p, A.ci.p, A.v.p, A.blk_row.p, x, y, done); break;
-        case 3: B2S_LAUNCH(ctx, k_baij_staged<3>, A.nblk, kThreads, 0, A.rp.p, A.ci.p, A.v.p, A.blk_row.p, x, y, done); break;
-        case 4: B2S_LAUNCH(ctx, k_baij_staged<4>, A.nblk, kThreads, 0, A.rp.p, A.ci.p, A.v.p, A.blk_row.p, x, y, done); break;
+        case 2: launch_baij<2>(ctx, A, x, y, done); break;
+        case 3: launch_baij<3>(ctx, A, x, y, done); break;
+        case 4: launch_baij<4>(ctx, A, x, y, done); break;
         default: fail(B2S_UNSUPPORTED, "block size must be 1..4");
     }
 }

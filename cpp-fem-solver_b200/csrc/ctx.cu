@@ -1,9 +1,116 @@
 // Context, status names and matrix handles of the b2s C ABI.
+#include <mutex>
+#include <unordered_map>
+#include <unordered_set>
+
 #include "b2s_internal.cuh"
 
 #include <algorithm>
 
 using namespace b2s;
+
+namespace b2s {
+namespace mem {
+
+namespace {
+std::mutex g_mu;
+std::unordered_set<cudaStream_t> g_live;          // streams of live contexts
+std::unordered_map<int, cudaStream_t> g_alloc;    // per-device allocation stream
+
+cudaStream_t alloc_stream_of(int dev)
+{
+    std::lock_guard<std::mutex> lock(g_mu);
+    auto it = g_alloc.find(dev);
+    if (it != g_alloc.end()) return it->second;
+    cudaStream_t s = nullptr;
+    cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreateWithFlags (allocation stream)");
+    // keep freed memory in the pool rather than returning it at every synchronisation
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+    {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    g_alloc[dev] = s;
+    return s;
+}
+
+bool live(cudaStream_t s)
+{
+    std::lock_guard<std::mutex> lock(g_mu);
+    return g_live.count(s) != 0;
+}
+}  // namespace
+
+cudaStream_t& current_stream()
+{
+    static thread_local cudaStream_t s = nullptr;
+    return s;
+}
+
+void register_stream(cudaStream_t s)
+{
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_live.insert(s);
+}
+
+void unregister_stream(cudaStream_t s)
+{
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_live.erase(s);
+}
+
+Block alloc(size_t bytes)
+{
+    int dev = 0;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    Block b;
+    b.alloc_stream = alloc_stream_of(dev);
+    b.owner = current_stream();
+    cudaError_t e = cudaMallocAsync(&b.p, bytes, b.alloc_stream);
+    if (e == cudaErrorMemoryAllocation)
+    {
+        // give the pool's cached memory back to the device and try once more
+        cudaGetLastError();
+        cudaMemPool_t pool;
+        cudaStreamSynchronize(b.alloc_stream);
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+        e = cudaMallocAsync(&b.p, bytes, b.alloc_stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b.alloc_stream);
+    if (e != cudaSuccess)
+    {
+        b.p = nullptr;
+        cuda_check(e, ("device allocation of " + std::to_string(bytes) + " bytes").c_str());
+    }
+    return b;
+}
+
+void free(const Block& b)
+{
+    if (!b.p) return;
+    if (b.owner && live(b.owner))
+    {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        cudaEvent_t ev = nullptr;
+        if (cudaStreamIsCapturing(b.owner, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone &&
+            cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess)
+        {
+            const bool ok = cudaEventRecord(ev, b.owner) == cudaSuccess &&
+                            cudaStreamWaitEvent(b.alloc_stream, ev, 0) == cudaSuccess &&
+                            cudaFreeAsync(b.p, b.alloc_stream) == cudaSuccess;
+            cudaEventDestroy(ev);
+            if (ok) return;
+        }
+        cudaGetLastError();
+    }
+    cudaFree(b.p);  // synchronous
+    cudaGetLastError();
+}
+
+}  // namespace mem
+}  // namespace b2s
 
 extern "C" {
 
@@ -29,6 +136,8 @@ b2s_status b2s_ctx_create(int device, b2s_ctx** out)
                                                        std::to_string(prop.major) + std::to_string(prop.minor));
         ctx->sm_count = prop.multiProcessorCount;
         B2S_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        mem::register_stream(ctx->stream);
+        mem::current_stream() = ctx->stream;
         ctx->partial.alloc((size_t)ctx->sm_count * 8 * kMaxRedValues);
         ctx->counter.alloc(64);
         B2S_CUDA(cudaMemset(ctx->counter.p, 0, ctx->counter.bytes()));
@@ -60,7 +169,11 @@ b2s_status b2s_ctx_destroy(b2s_ctx* ctx)
     if (ctx->h_scalar) cudaFreeHost(ctx->h_scalar);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->stream)
+    {
+        mem::unregister_stream(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+    }
     delete ctx;
     return B2S_OK;
 }

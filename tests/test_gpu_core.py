@@ -61,7 +61,7 @@ def test_dot_deterministic(b2s, ctx):
         assert abs(d1 - ref) <= 1e-13 * max(1.0, np.abs(a * b).sum())
 
 
-@pytest.mark.parametrize("bs", [1, 3])
+@pytest.mark.parametrize("bs", [1, 2, 3, 4])
 def test_baij_matvec_bit_exact(b2s, ctx, orc, bs):
     n, rp, ci, v = P.make_test_scalar(40, 3) if bs == 3 else P.poisson2d(60)
     Ao = orc.csr(n, n, rp, ci, v)
@@ -70,6 +70,25 @@ def test_baij_matvec_bit_exact(b2s, ctx, orc, bs):
     brp, bci, bv = Bo.export()
     B = b2s.BAIJ(ctx, bs, nb, nb, brp, bci, bv)
     x = P.drand(np.arange(n))
+    assert np.array_equal(B.matvec(x), orc.blk_matvec(Bo, x))
+
+
+@pytest.mark.parametrize("bs", [2, 3, 4])
+def test_baij_matvec_irregular(b2s, ctx, orc, bs):
+    # ragged block rows: empty rows, single blocks and rows of 100+ blocks,
+    # which span several passes of the warp kernel
+    rng = np.random.default_rng(bs)
+    nb = 700
+    lens = rng.integers(0, 12, nb)
+    lens[::97] = 0
+    lens[5] = 150
+    lens[400] = 90
+    rp = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint32)
+    ci = np.concatenate([np.sort(rng.choice(nb, size=k, replace=False)) for k in lens]).astype(np.uint32)
+    v = rng.uniform(-1, 1, len(ci) * bs * bs)
+    B = b2s.BAIJ(ctx, bs, nb, nb, rp, ci, v)
+    Bo = orc.blk(bs, nb, nb, rp, ci, v)
+    x = rng.uniform(-1, 1, nb * bs)
     assert np.array_equal(B.matvec(x), orc.blk_matvec(Bo, x))
 
 
