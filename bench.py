@@ -127,6 +127,8 @@ KERNELS = {
     "trsv_c2": "k_trsv_chunk: FP64 ILU(0) apply on the 128^3 Poisson matrix (C2)",
     "btrsv_c4": "k_btrsv_chunk: FP64 block ILU(0) apply on the Q1 elasticity matrix (C4, 64^3 elements)",
     "vcycle_c2": "SA-AMG V-cycle (k_jacobi, BAIJ matvecs, k_dense_solve) on C2",
+    "dense_c5": "k_linear_tc<64,128>: the learned network's tcgen05 dense layer on the 512^2 grid's node states "
+                "(n=262144 rows, 64 -> 128)",
 }
 
 
@@ -155,6 +157,16 @@ def run_kernel(args):
         y = torch.empty_like(x)
         step = lambda: ctx.check(b2s.lib().b2s_baij_matvec_device(ctx.h, A.h, C.c_void_p(x.data_ptr()),
                                                                   C.c_void_p(y.data_ptr())), "baij_matvec")
+    elif k == "dense_c5":
+        n = N_GRID * N_GRID
+        g = torch.Generator(device=dev).manual_seed(5)
+        x = torch.randn(n, 64, generator=g, device=dev, dtype=torch.float32)
+        w = (0.1 * torch.randn(128, 64, generator=g, device=dev)).to(torch.bfloat16)
+        y = torch.empty(n, 128, dtype=torch.float32, device=dev)
+        torch.cuda.synchronize()
+        step = lambda: ctx.check(b2s.lib().b2s_dense_bf16_device(ctx.h, n, 64, 128, C.c_void_p(x.data_ptr()),
+                                                                C.c_void_p(w.data_ptr()), None,
+                                                                C.c_void_p(y.data_ptr())), "dense_bf16")
     else:
         if k in ("trsv_c5", "trsv_c5_fp64"):
             n, rp, ci, v = b2s.gen_grf_diffusion(N_GRID, 2000, corr=CORR)
@@ -187,8 +199,16 @@ def run_kernel(args):
         step()
     e1.record(stream)
     e1.synchronize()
-    print(json.dumps({"kernel": k, "what": KERNELS[k], "launches": args.steps,
-                      "ms_per_step": e0.elapsed_time(e1) / max(args.steps, 1)}))
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    out = {"kernel": k, "what": KERNELS[k], "launches": args.steps, "ms_per_step": ms}
+    if k == "dense_c5":
+        # X read once (n x 64 FP32), Y written once (n x 128 FP32), W (128 x 64 BF16)
+        nbytes = n * (64 + 128) * 4 + 128 * 64 * 2
+        pk, which = peaks()
+        out.update({"algorithmic_bytes": nbytes, "achieved_gbs": nbytes / (ms * 1e-3) / 1e9,
+                    "frac_hbm": nbytes / (ms * 1e-3) / 1e9 / pk["hbm_gbs"], "peak": which,
+                    "tflops": 2.0 * n * 64 * 128 / (ms * 1e-3) / 1e12})
+    print(json.dumps(out))
     ctx.close()
     return 0
 
@@ -220,7 +240,7 @@ def run_reference(args):
             times.append(dt * 1e3)
             its.append(it)
     ms = float(np.mean(times))
-    line = {"metric": "time-to-rtol 1e-8 (PCG, 512^2 random-coefficient diffusion)", "value": ms, "unit": "ms",
+    line = {"metric": "time-to-rtol 1e-8 & iters: learned/mixed-prec PCG vs plain FP64 PCG, 1 B200", "value": ms, "unit": "ms",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded GRF diffusion, held-out seeds 2000+)", "impl": "reference",
@@ -242,7 +262,7 @@ def main():
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b2s", choices=["b2s", "reference"])
-    ap.add_argument("--method", default="fp32_ic0", choices=["fp32_ic0", "fp64_ic0", "learned_ic0"])
+    ap.add_argument("--method", default="learned_ic0", choices=["fp32_ic0", "fp64_ic0", "learned_ic0"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel", default=None, choices=sorted(KERNELS),
                     help="run one hot kernel only (for profilers), not the benchmark")
@@ -301,7 +321,7 @@ def main():
         """Warm-up solves on warm_idx, then one timed solve per timed system."""
         for k in warm_idx:
             timed_solve(*systems[k], method)
-        ms, its, rel, launches, split = [], [], [], 0, []
+        ms, its, rel, launches, split, fb = [], [], [], 0, [], 0
         for k in timed_idx:
             t, st, nl = timed_solve(*systems[k], method)
             ms.append(t)
@@ -309,7 +329,9 @@ def main():
             rel.append(st["relres_true"])
             split.append((st["setup_ms_event"], st["iter_ms_event"]))
             launches += nl
+            fb += st["fallbacks"]
         run.split = split
+        run.fallbacks = fb
         return ms, its, rel, launches
 
     if world > 1:
@@ -318,6 +340,7 @@ def main():
     with ClockSampler(local) as clk:
         head_ms, head_its, head_rel, launches = run(args.method, range(args.warmup))
     head_split = run.split
+    head_fallbacks = run.fallbacks
     torch.cuda.synchronize()
     clocks = clk.summary()
     base_ms, base_its, base_rel, _ = run("fp64_ic0", range(min(1, args.warmup))) if args.method != "fp64_ic0" else (
@@ -370,6 +393,33 @@ def main():
                 "peak_kind": pk_kind, "traffic": None, "bytes_per_launch": tri_bytes, "ms_per_launch": tri_ms,
                 "note": "latency-bound: a 1023-level dependency chain per triangle on the 512^2 grid"}
 
+    # the learned network's tcgen05 dense layer (64 -> 128) on this grid's node
+    # states: X read once, Y written once
+    nd = N_GRID * N_GRID
+    gx = torch.Generator(device=dev).manual_seed(5)
+    xd = torch.randn(nd, 64, generator=gx, device=dev, dtype=torch.float32)
+    wd = (0.1 * torch.randn(128, 64, generator=gx, device=dev)).to(torch.bfloat16)
+    yd = torch.empty(nd, 128, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    dense = lambda: ctx.check(b2s.lib().b2s_dense_bf16_device(ctx.h, nd, 64, 128, b2s.C.c_void_p(xd.data_ptr()),
+                                                             b2s.C.c_void_p(wd.data_ptr()), None,
+                                                             b2s.C.c_void_p(yd.data_ptr())), "dense_bf16")
+    for _ in range(3):
+        dense()
+    e0.record(stream)
+    for _ in range(20):
+        dense()
+    e1.record(stream)
+    e1.synchronize()
+    dense_ms = e0.elapsed_time(e1) / 20
+    dense_bytes = nd * (64 + 128) * 4 + 128 * 64 * 2
+    dense_gbs = dense_bytes / (dense_ms * 1e-3) / 1e9
+    dense_layer = {"kernel": "k_linear_tc<64,128> (tcgen05.mma kind::f16, BF16 x BF16 -> FP32 in TMEM)",
+                   "workload": f"{nd} node states x 64 -> 128", "ms": dense_ms, "achieved": dense_gbs,
+                   "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": dense_gbs / pk["hbm_gbs"],
+                   "bytes_per_launch": dense_bytes, "tflops": 2.0 * nd * 64 * 128 / (dense_ms * 1e-3) / 1e12}
+    del xd, yd
+
     # C2 (3-D Poisson 128^3) CSR SpMV against the HBM roofline (inputs > L2)
     n3, rp3, ci3, v3 = b2s.gen_poisson3d(128)
     A3 = b2s.CSR(ctx, n3, n3, rp3, ci3, v3)
@@ -415,7 +465,7 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": "time-to-rtol 1e-8 (PCG, 512^2 random-coefficient diffusion)",
+            "metric": "time-to-rtol 1e-8 & iters: learned/mixed-prec PCG vs plain FP64 PCG, 1 B200",
             "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 outer / f32 preconditioner" if prec == b2s.FP32 else "f64",
@@ -423,6 +473,7 @@ def main():
             "config": {"workload": "grf_diffusion_512 pcg rtol1e-8", "method": args.method, "grid": N_GRID,
                        "corr": CORR, "parallelism": f"replicas x{world}", "l2": "flushed (512 MB write) before every step"},
             "iterations_mean": float(np.mean(head_its)), "relres_true_max": float(np.max(head_rel)),
+            "fallbacks": int(head_fallbacks),
             "setup_ms_mean": float(np.mean([a for a, _ in head_split])),
             "iter_ms_mean": float(np.mean([b for _, b in head_split])),
             "fp64_ic0_pcg": {"ms": float(np.mean(base_ms)), "iterations_mean": float(np.mean(base_its)),
@@ -435,6 +486,7 @@ def main():
             "gpu_launches": int(launches),
             "roofline": roofline,
             "spmv_c2": spmv,
+            "dense_layer": dense_layer,
             "cpu_baseline": cpu,
             "clocks": clocks,
         }

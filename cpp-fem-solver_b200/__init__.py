@@ -85,13 +85,14 @@ class PcOpts(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("tol", C.c_double), ("maxit", C.c_int), ("restart", C.c_int), ("orth", C.c_int),
                 ("ir_steps", C.c_int), ("ir_inner_tol", C.c_double), ("check_every", C.c_int),
-                ("use_graphs", C.c_int)]
+                ("use_graphs", C.c_int), ("stall_window", C.c_int)]
 
 
 class Stats(C.Structure):
     _fields_ = [("it", C.c_int), ("iterations", C.c_int), ("spmvs", C.c_int), ("pc_applies", C.c_int),
                 ("restarts", C.c_int), ("status", C.c_int), ("relres", C.c_double), ("relres_true", C.c_double),
-                ("setup_ms", C.c_double), ("solve_ms", C.c_double)]
+                ("setup_ms", C.c_double), ("solve_ms", C.c_double), ("fallbacks", C.c_int),
+                ("stalled_at", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -112,7 +113,7 @@ EXPORTS = [
     "b2s_solve_baij", "b2s_solve_baij_device", "b2s_gen_poisson2d", "b2s_gen_poisson3d", "b2s_gen_convdiff3d",
     "b2s_gen_elasticity_q1", "b2s_gen_grf_diffusion", "b2s_gen_uniform", "b2s_learner_create",
     "b2s_learner_destroy", "b2s_learner_load", "b2s_learner_save", "b2s_learner_params", "b2s_learner_step",
-    "b2s_pc_create_learned", "b2s_dot_noalloc",
+    "b2s_pc_create_learned", "b2s_dot_noalloc", "b2s_dense_bf16_device",
 ]
 
 
@@ -185,6 +186,7 @@ def lib():
     f("b2s_learner_step", i32, vp, vp, vp, i32, u64, vp, f64, i32, C.POINTER(C.c_double), vp)
     f("b2s_pc_create_learned", i32, vp, vp, vp, C.POINTER(PcOpts), pp)
     f("b2s_dot_noalloc", i32, vp, vp, u64, vp, vp)
+    f("b2s_dense_bf16_device", i32, vp, u64, i32, i32, vp, vp, vp, vp)
     _lib = L
     return L
 
@@ -447,11 +449,12 @@ class Learner:
 
 
 def solve_opts(tol=1e-10, maxit=2000, restart=30, orth=ORTH_MGS, ir_steps=0, ir_inner_tol=0.0, check_every=0,
-               use_graphs=1) -> SolveOpts:
+               use_graphs=1, stall_window=0) -> SolveOpts:
     o = SolveOpts()
     lib().b2s_solve_opts_default(C.byref(o))
     o.tol, o.maxit, o.restart, o.orth = tol, maxit, restart, orth
     o.ir_steps, o.ir_inner_tol, o.check_every, o.use_graphs = ir_steps, ir_inner_tol, check_every, use_graphs
+    o.stall_window = stall_window
     return o
 
 

@@ -207,7 +207,19 @@ void* b2s_ctx_stream(b2s_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; 
 b2s_status b2s_ctx_synchronize(b2s_ctx* ctx)
 {
     if (!ctx) return B2S_INVALID_ARG;
-    return guarded(ctx, [&] { sync(ctx); });
+    return guarded(ctx, [&] {
+        // asynchronous entry points (b2s_dense_bf16_device) report a bounded
+        // device wait that gave up through the context's error word
+        int h = 0;
+        B2S_CUDA(cudaMemcpyAsync(&h, ctx->errword(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        sync(ctx);
+        if (h)
+        {
+            B2S_CUDA(cudaMemsetAsync(ctx->errword(), 0, sizeof(int), ctx->stream));
+            sync(ctx);
+            fail((b2s_status)h, "a device-side wait gave up");
+        }
+    });
 }
 
 uint64_t b2s_ctx_kernel_launches(const b2s_ctx* ctx) { return ctx ? ctx->launches : 0; }

@@ -785,6 +785,11 @@ struct Solve
     int* done;  // &st->done
     int poll_every;
     bool graphs;
+    // stall guard (learned IC(0)): the recursive residual must halve within
+    // stall_window iterations, checked at every host poll; 0 = off
+    int stall_window = 0;
+    bool stalled = false;
+    int stalled_at = 0;
 
     Solve(b2s_ctx* c, const Operator& op, PcImpl* p, const b2s_solve_opts& opts) : ctx(c), A(op), pc(p), o(opts)
     {
@@ -833,6 +838,8 @@ struct Solve
             B2S_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
             B2S_CUDA(cudaGraphInstantiate(&exec, graph, 0));
         }
+        double best = HUGE_VAL;
+        int best_at = 0;
         for (;;)
         {
             if (exec)
@@ -841,6 +848,23 @@ struct Solve
                 for (int k = 0; k < poll_every; ++k) body();
             KState h = read_state();
             if (h.done) break;
+            if (stall_window > 0)
+            {
+                if (h.relres < 0.5 * best)
+                {
+                    best = h.relres;
+                    best_at = h.iters;
+                }
+                else if (h.iters - best_at >= stall_window)
+                {
+                    // stop here: the remaining kernels see done and skip
+                    stalled = true;
+                    stalled_at = h.iters;
+                    const int one = 1;
+                    h2d(ctx, done, &one, sizeof(int));
+                    break;
+                }
+            }
         }
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -1162,6 +1186,87 @@ static void run_refined(b2s_ctx* ctx, const Operator& A, PcImpl* pc, b2s_method 
     }
 }
 
+// Learned IC(0) with its fallback: the solve runs under the stall guard; if it
+// stalls, breaks down (NOT_SPD / BREAKDOWN / DIVERGED) or ends unconverged,
+// plain FP64 IC(0) takes over from the learned solve's iterate (from x = 0 if
+// that is not finite): r = b - A x, solve A d = r to tol ||b|| / ||r||, x += d.
+constexpr int kStallWindow = 200;
+
+static void run_learned(b2s_ctx* ctx, const Operator& A, PcImpl* pc, b2s_method method, const b2s_solve_opts& o,
+                        const double* b, double* x, b2s_stats* stats)
+{
+    b2s_stats s1;
+    std::memset(&s1, 0, sizeof(s1));
+    bool stalled = false;
+    int stalled_at = 0;
+    {
+        Solve S(ctx, A, pc, o);
+        S.stall_window = o.stall_window > 0 ? o.stall_window : kStallWindow;
+        run_method(S, method, b, x, &s1);
+        stalled = S.stalled;
+        stalled_at = S.stalled_at;
+    }
+    const bool failed = s1.status == B2S_NOT_SPD || s1.status == B2S_BREAKDOWN || s1.status == B2S_DIVERGED;
+    const bool unconverged = s1.status == B2S_OK && !(s1.relres_true < o.tol);
+    if (!(stalled || failed || unconverged))
+    {
+        if (stats) *stats = s1;
+        return;
+    }
+    const uint64_t n = A.n;
+    DBuf<double> r(n), d(n), Ax(n);
+    const double normb = std::sqrt(dot_host(ctx, n, b, b));
+    KState* st = ctx->kstate.p;
+    double normr = normb;
+    if (std::isfinite(s1.relres_true))
+    {
+        A.apply(ctx, x, Ax.p, nullptr);
+        launch_vec(ctx, n, nullptr, BodyResidual{r.p, b, Ax.p, st});
+        d2h(ctx, ctx->h_kstate, st, sizeof(KState));
+        sync(ctx);
+        normr = ctx->h_kstate->aux[0];
+    }
+    if (!std::isfinite(normr) || !std::isfinite(s1.relres_true))
+    {
+        fill(ctx, x, 0.0, n);
+        copy(ctx, r.p, b, n);
+        normr = normb;
+    }
+    b2s_pc_opts po;
+    b2s_pc_opts_default(&po);
+    auto ic0 = make_pc_ic0(ctx, *A.csr, po);
+    b2s_solve_opts in = o;
+    in.tol = normr > 0 ? o.tol * normb / normr : o.tol;
+    b2s_stats s2;
+    std::memset(&s2, 0, sizeof(s2));
+    if (normr > 0 && normb > 0 && normr / normb >= o.tol)
+    {
+        Solve S(ctx, A, ic0.get(), in);
+        run_method(S, method, r.p, d.p, &s2);
+        launch_vec(ctx, n, nullptr, BodyAxpyOne{x, d.p});
+    }
+    // FP64 true residual of the combined iterate
+    A.apply(ctx, x, Ax.p, nullptr);
+    launch_vec(ctx, n, nullptr, BodyResidual{r.p, b, Ax.p, st});
+    d2h(ctx, ctx->h_kstate, st, sizeof(KState));
+    sync(ctx);
+    const double rel = normb > 0 ? ctx->h_kstate->aux[0] / normb : 0.0;
+    if (stats)
+    {
+        stats->it = s1.it + s2.it + 1;
+        stats->iterations = s1.iterations + s2.iterations;
+        stats->spmvs = s1.spmvs + s2.spmvs + 2;
+        stats->pc_applies = s1.pc_applies + s2.pc_applies;
+        stats->restarts = s1.restarts + s2.restarts;
+        stats->status = s2.status;
+        stats->relres = rel;
+        stats->relres_true = rel;
+        stats->solve_ms = s1.solve_ms + s2.solve_ms;
+        stats->fallbacks = 1;
+        stats->stalled_at = stalled ? stalled_at : s1.iterations;
+    }
+}
+
 static b2s_status solve_common(b2s_ctx* ctx, const Operator& A, b2s_pc* pc, b2s_method method,
                                const b2s_solve_opts* opts, const double* d_b, double* d_x, b2s_stats* stats)
 {
@@ -1173,8 +1278,11 @@ static b2s_status solve_common(b2s_ctx* ctx, const Operator& A, b2s_pc* pc, b2s_
     need(o.maxit >= 0, B2S_INVALID_ARG, "maxit must be >= 0");
     need(method != B2S_GMRES || o.restart > 0, B2S_INVALID_ARG, "GMRES restart must be > 0");
     PcImpl* impl = pc ? pc->impl.get() : nullptr;
+    const bool learned = pc && pc->kind == B2S_PC_LEARNED_IC0 && A.csr && o.stall_window >= 0;
     if (o.ir_steps > 0)
         run_refined(ctx, A, impl, method, o, d_b, d_x, stats);
+    else if (learned)
+        run_learned(ctx, A, impl, method, o, d_b, d_x, stats);
     else
     {
         Solve S(ctx, A, impl, o);

@@ -36,6 +36,7 @@
 #include <fstream>
 
 #include "b2s_internal.cuh"
+#include "tc_linear.cuh"
 
 struct b2s_learner;
 
@@ -226,8 +227,9 @@ __global__ void __launch_bounds__(256) k_linear_bwd_data(uint32_t n, const float
         }
 }
 
-// per-CTA partial of dW (NO x K) = dY^T X and db = sum dY over a row chunk
-template <int K, int NO>
+// per-CTA partial of dW (NO x K) = dY^T X and db = sum dY over a row chunk;
+// RX: X rounded to BF16 first, the operand the tensor-core forward multiplied
+template <int K, int NO, bool RX>
 __global__ void __launch_bounds__(256) k_linear_bwd_weight(uint32_t n, uint32_t rows_per_cta, const float* __restrict__ dY,
                                                            const float* __restrict__ X, float* __restrict__ partial)
 {
@@ -251,7 +253,8 @@ __global__ void __launch_bounds__(256) k_linear_bwd_weight(uint32_t n, uint32_t 
         for (int t = threadIdx.x; t < TILE * K; t += blockDim.x)
         {
             const int rr = t / K, k = t % K;
-            Xs[rr][k] = (t0 + rr < r_end) ? X[(size_t)(t0 + rr) * K + k] : 0.f;
+            const float x = (t0 + rr < r_end) ? X[(size_t)(t0 + rr) * K + k] : 0.f;
+            Xs[rr][k] = RX ? __bfloat162float(__float2bfloat16_rn(x)) : x;
         }
         __syncthreads();
 #pragma unroll
@@ -673,6 +676,21 @@ __global__ void k_gate_grads(const float* __restrict__ red, float* __restrict__ 
 
 // ------------------------------------------------------------ network state
 
+// Y = bf16(X) W^T [+ bias] on the tensor cores (tc_linear.cuh)
+template <int K, int NO>
+static void linear_tc(b2s_ctx* ctx, uint32_t n, const float* X, const __nv_bfloat16* W, const float* bias, float* Y,
+                      int* err)
+{
+    using S = tc::LinearShape<K, NO>;
+    if (!n) return;
+    need((((uintptr_t)X | (uintptr_t)W | (uintptr_t)Y | (uintptr_t)bias) & 15) == 0, B2S_INVALID_ARG,
+         "tensor-core layer: operands must be 16-byte aligned");
+    B2S_CUDA(cudaFuncSetAttribute(tc::k_linear_tc<K, NO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::kSmem));
+    const uint32_t tiles = (n + tc::kTileRows - 1) / tc::kTileRows;
+    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)ctx->sm_count * S::kCtasPerSm);
+    B2S_LAUNCH(ctx, (tc::k_linear_tc<K, NO>), grid, tc::kThreadsTc, S::kSmem, n, X, W, bias, Y, err);
+}
+
 struct Gnn
 {
     DBuf<float> p;                 // FP32 master parameters
@@ -733,11 +751,14 @@ struct GnnGraph
     DBuf<float> F, EF, invdeg;
     DBuf<float> Hs[NL + 1], SM[NL], pre[NL], pre0;
     DBuf<double> logd;
+    DBuf<int> err;  // B2S_TIMEOUT from the tensor-core layer's bounded wait
 
     void build(b2s_ctx* ctx, const CsrDev& A)
     {
         n = A.n;
         nnz = A.nnz;
+        err.alloc(1);
+        B2S_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), ctx->stream));
         rev.alloc(nnz ? nnz : 1);
         DBuf<int> nonsym(1);
         B2S_CUDA(cudaMemsetAsync(nonsym.p, 0, sizeof(int), ctx->stream));
@@ -776,12 +797,20 @@ struct GnnGraph
         for (int l = 0; l < NL; ++l)
         {
             const __nv_bfloat16* Wl = net.pb.p + LAYER0 + l * L_SIZE;
-            // [W_s ; W_m] are contiguous: one 128 x 64 weight
-            B2S_LAUNCH(ctx, (k_linear<H, 2 * H, false>), g64, 256, 0, n, Hs[l].p, Wl + L_WS, (const float*)nullptr,
-                       SM[l].p, (float*)nullptr);
+            // [W_s ; W_m] are contiguous: one 128 x 64 weight, on the tensor cores
+            linear_tc<H, 2 * H>(ctx, n, Hs[l].p, Wl + L_WS, nullptr, SM[l].p, err.p);
             B2S_LAUNCH(ctx, k_aggregate, gw, 256, 0, n, A.rp.p, A.ci.p, EF.p, invdeg.p, SM[l].p, Wl, Hs[l].p,
                        pre[l].p, Hs[l + 1].p);
         }
+    }
+
+    // after a synchronisation: fail with B2S_TIMEOUT if a layer's wait gave up
+    void check(b2s_ctx* ctx)
+    {
+        int h = 0;
+        d2h(ctx, &h, err.p, sizeof(int));
+        sync(ctx);
+        if (h) fail(B2S_TIMEOUT, "tensor-core layer: wait for the MMA completion gave up");
     }
 };
 
@@ -801,7 +830,7 @@ struct LearnedCorrection final : Ic0Correction
         DBuf<float> C(Lnnz ? Lnnz : 1);
         B2S_LAUNCH(ctx, k_head, stream_grid(ctx, A.n), kThreads, 0, A.n, Lrp, Lci, A.rp.p, A.diag.p, G.EF.p,
                    G.Hs[NL].p, net->pr.p, L0.p, Lv, C.p, diag);
-        sync(ctx);
+        G.check(ctx);
     }
 };
 
@@ -1001,7 +1030,7 @@ static void train_step(b2s_ctx* ctx, Gnn& net, const CsrDev& A, int nprobes, uin
                    red.p, 0);
         B2S_LAUNCH(ctx, k_gate_grads, 1, 64, 0, red.p, gl);
         // weights [W_s; W_m] (128 x 64): dW = dSM^T H_l ; dH_l += dSM W
-        B2S_LAUNCH(ctx, (k_linear_bwd_weight<H, 2 * H>), gwb, 256, 0, n, rows_per, dSM.p, G.Hs[l].p, wpart.p);
+        B2S_LAUNCH(ctx, (k_linear_bwd_weight<H, 2 * H, true>), gwb, 256, 0, n, rows_per, dSM.p, G.Hs[l].p, wpart.p);
         B2S_LAUNCH(ctx, k_reduce_partials, 64, 256, 0, gwb, (uint32_t)(2 * H * H + 2 * H), (uint32_t)(2 * H * H),
                    wpart.p, gl + L_WS, 0);
         B2S_LAUNCH(ctx, (k_linear_bwd_data<H, 2 * H>), g64, 256, 0, n, dSM.p, Wl + L_WS, dH2.p, 1);
@@ -1010,14 +1039,14 @@ static void train_step(b2s_ctx* ctx, Gnn& net, const CsrDev& A, int nprobes, uin
     // input layer: dpre0 = dH0 * (pre0 > 0) ; dW_in = dpre0^T F ; db_in
     B2S_LAUNCH(ctx, k_relu_mask, stream_grid(ctx, (uint64_t)n * H), kThreads, 0, (uint64_t)n * H, G.pre0.p, dH.p,
                dSM.p);
-    B2S_LAUNCH(ctx, (k_linear_bwd_weight<FIN, H>), gwb, 256, 0, n, rows_per, dSM.p, G.F.p, wpart.p);
+    B2S_LAUNCH(ctx, (k_linear_bwd_weight<FIN, H, false>), gwb, 256, 0, n, rows_per, dSM.p, G.F.p, wpart.p);
     B2S_LAUNCH(ctx, k_reduce_partials, 4, 256, 0, gwb, (uint32_t)(H * FIN + H), (uint32_t)(H * FIN + H), wpart.p,
                net.g.p + OFF_WIN, 0);
 
     double lossv = 0;
     d2h(ctx, &lossv, T.scal.p + 3, sizeof(double));
     if (grad_out) d2h(ctx, grad_out, net.g.p, NPARAM * sizeof(float));
-    sync(ctx);
+    G.check(ctx);
     if (loss_out) *loss_out = lossv;
     if (update)
     {
@@ -1102,6 +1131,23 @@ b2s_status b2s_learner_step(b2s_ctx* ctx, b2s_learner* L, const b2s_csr* A, int 
     return guarded(ctx, [&] {
         need(A->d.n == A->d.m, B2S_SHAPE, "learned IC(0) needs a square matrix");
         train_step(ctx, L->net, A->d, nprobes, seed, probes, lr, update != 0, loss, grad);
+    });
+}
+
+b2s_status b2s_dense_bf16_device(b2s_ctx* ctx, uint64_t n, int k, int no, const float* d_x, const uint16_t* d_w,
+                                 const float* d_bias, float* d_y)
+{
+    if (!ctx) return B2S_INVALID_ARG;
+    if (n && (!d_x || !d_w || !d_y)) return B2S_INVALID_ARG;
+    if (n > UINT32_MAX - tc::kTileRows) return B2S_UNSUPPORTED;
+    return guarded(ctx, [&] {
+        const auto* w = reinterpret_cast<const __nv_bfloat16*>(d_w);
+        if (k == 64 && no == 128)
+            linear_tc<64, 128>(ctx, (uint32_t)n, d_x, w, d_bias, d_y, ctx->errword());
+        else if (k == 64 && no == 64)
+            linear_tc<64, 64>(ctx, (uint32_t)n, d_x, w, d_bias, d_y, ctx->errword());
+        else
+            fail(B2S_UNSUPPORTED, "dense layer: supported shapes are k = 64 with no = 128 or 64");
     });
 }
 

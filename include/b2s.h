@@ -229,6 +229,15 @@ b2s_status b2s_learner_step(b2s_ctx* ctx, b2s_learner* L, const b2s_csr* A, int 
 /* IC(0) corrected by this network (the same kernels as B2S_PC_LEARNED_IC0). */
 b2s_status b2s_pc_create_learned(b2s_ctx* ctx, const b2s_csr* A, b2s_learner* L, const b2s_pc_opts* opts,
                                  b2s_pc** out);
+/* The network's hidden dense layer on the tensor cores (tcgen05, BF16 x BF16,
+ * FP32 accumulation), device pointers on the context's stream:
+ * d_y (n x no, FP32, row-major) = bf16(d_x) (n x k, FP32, row-major) W^T
+ * [+ d_bias], W (no x k, BF16 bits, row-major); bf16() rounds to nearest even.
+ * Supported: k = 64, no = 128 (the message-passing layers' [W_s; W_m]) and
+ * k = 64, no = 64; other shapes return B2S_UNSUPPORTED.  All pointers 16-byte
+ * aligned; d_bias may be NULL.  No counterpart in the reference. */
+b2s_status b2s_dense_bf16_device(b2s_ctx* ctx, uint64_t n, int k, int no, const float* d_x, const uint16_t* d_w,
+                                 const float* d_bias, float* d_y);
 
 /* ----------------------------------------------------------------- solvers */
 
@@ -258,6 +267,10 @@ typedef struct b2s_solve_opts
     double ir_inner_tol; /* relative tolerance of each refinement solve (0: 1e-4) */
     int check_every; /* host polls convergence every this many iterations (0: auto) */
     int use_graphs;  /* 1: replay iteration bodies as CUDA graphs */
+    int stall_window; /* B2S_PC_LEARNED_IC0: the solve counts as stalled when the recursive
+                         residual has not halved within this many iterations (0: 200,
+                         < 0: never); a stalled, broken-down or unconverged learned solve
+                         continues with plain FP64 IC(0) from its iterate (b2s_stats.fallbacks) */
 } b2s_solve_opts;
 
 void b2s_solve_opts_default(b2s_solve_opts* opts);
@@ -274,6 +287,8 @@ typedef struct b2s_stats
     double relres_true;   /* ||b - A x|| / ||b|| recomputed in FP64 on exit */
     double setup_ms;      /* preconditioner setup inside this call (0 when given one) */
     double solve_ms;      /* iteration time, device events */
+    int fallbacks;        /* 1 when a learned IC(0) solve handed over to plain IC(0) */
+    int stalled_at;       /* iterations run with the learned preconditioner before that */
 } b2s_stats;
 
 /* Solves A x = b from x0 = 0.  pc may be NULL (identity).  Host pointers. */

@@ -76,7 +76,10 @@ def loss_and_grad(params, n, rp, ci, v, Lrp, Lci, L0, probes):
         Wg = P[b0 + L_WG:b0 + L_WG + H * FE].view(H, FE)
         bg = P[b0 + L_BG:b0 + L_BG + H]
         bl = P[b0 + L_B:b0 + L_B + H]
-        S, M = h @ Ws.T, h @ Wm.T
+        # the tensor-core layer multiplies BF16-rounded node states; the
+        # rounding passes the gradient straight through (dH = dS Ws + dM Wm)
+        hb = h + (h.detach().to(torch.float32).to(torch.bfloat16).to(torch.float64) - h.detach())
+        S, M = hb @ Ws.T, hb @ Wm.T
         g = torch.sigmoid(Ef @ Wg.T + bg)
         agg = torch.zeros(n, H, dtype=torch.float64).index_add(0, src, g * M[dst])
         pre = S + bl + invdeg[:, None] * agg

@@ -77,3 +77,62 @@ def test_training_reduces_loss_and_stays_spd(b2s, ctx, tmp_path):
         f.write(b"\x00\x01")
     with pytest.raises(ValueError):
         L2.load(path)
+
+
+def _grf512(b2s, seed):
+    n, rp, ci, v = b2s.gen_grf_diffusion(512, seed=seed, corr=0.05)
+    return n, rp, ci, v, b2s.uniform(seed, n)
+
+
+def test_trained_network_gains_over_ic0(b2s, ctx):
+    """The shipped weights against the method without them: PCG on a held-out
+    512^2 random-coefficient system (seed outside the training range) with
+    the learned preconditioner needs at most 70% of plain IC(0)'s iterations,
+    both verified to rtol 1e-8 by the FP64 true residual, with no fallback."""
+    n, rp, ci, v, b = _grf512(b2s, 2001)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    M0 = b2s.Precond(ctx, A, b2s.PC_IC0)
+    _, s0 = b2s.solve(ctx, A, b, b2s.PCG, M0, tol=1e-8, maxit=20000)
+    ML = b2s.Precond(ctx, A, b2s.PC_LEARNED_IC0, precision=b2s.FP32)
+    _, sl = b2s.solve(ctx, A, b, b2s.PCG, ML, tol=1e-8, maxit=20000)
+    assert s0["relres_true"] < 1e-8 and sl["relres_true"] < 1e-8
+    assert sl["fallbacks"] == 0
+    assert sl["iterations"] <= 0.7 * s0["iterations"], (sl["iterations"], s0["iterations"])
+
+
+def test_learned_falls_back_on_stall(b2s, ctx):
+    """A stall window of one iteration makes the guard fire at the first poll
+    where the residual has not halved (on the 512^2 system PCG needs about 17
+    iterations per halving, polls come every 8); plain FP64 IC(0) continues
+    from the learned iterate to the same tolerance."""
+    n, rp, ci, v, b = _grf512(b2s, 2002)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    M = b2s.Precond(ctx, A, b2s.PC_LEARNED_IC0, precision=b2s.FP32)
+    x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=20000, stall_window=1)
+    assert st["fallbacks"] == 1 and 0 < st["stalled_at"] < st["iterations"]
+    assert st["status"] == 0 and st["relres_true"] < 1e-8
+    # the residual checked on the host, independently of the device's FP64 check
+    import scipy.sparse as sp
+    Ah = sp.csr_matrix((v, ci, rp), shape=(n, n))
+    assert np.linalg.norm(b - Ah @ x) < 1e-8 * np.linalg.norm(b)
+    # the guard off: the learned solve runs to the tolerance on its own
+    x2, s2 = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=20000, stall_window=-1)
+    assert s2["fallbacks"] == 0 and s2["relres_true"] < 1e-8
+
+
+def test_learned_falls_back_on_divergence(b2s, ctx):
+    """A network whose output layer is NaN gives a NaN factor: PCG stops with
+    B2S_DIVERGED, and plain IC(0) restarts from x = 0 and converges."""
+    n, rp, ci, v = system(b2s, N=32, seed=6)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    L = b2s.Learner(ctx, seed=3)
+    p = L.params()
+    import gnn_ref
+    p[gnn_ref.OFF_OUT:] = np.nan
+    L.set_params(p)
+    M = L.precond(A)
+    b = b2s.uniform(10, n)
+    x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=3000)
+    assert st["fallbacks"] == 1
+    assert st["status"] == 0 and st["relres_true"] < 1e-8
+    assert np.all(np.isfinite(x))
