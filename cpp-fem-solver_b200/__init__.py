@@ -114,6 +114,7 @@ EXPORTS = [
     "b2s_gen_elasticity_q1", "b2s_gen_grf_diffusion", "b2s_gen_uniform", "b2s_learner_create",
     "b2s_learner_destroy", "b2s_learner_load", "b2s_learner_save", "b2s_learner_params", "b2s_learner_step",
     "b2s_pc_create_learned", "b2s_dot_noalloc", "b2s_dense_bf16_device",
+    "b2s_learner_set_loss",
 ]
 
 
@@ -187,6 +188,7 @@ def lib():
     f("b2s_pc_create_learned", i32, vp, vp, vp, C.POINTER(PcOpts), pp)
     f("b2s_dot_noalloc", i32, vp, vp, u64, vp, vp)
     f("b2s_dense_bf16_device", i32, vp, u64, i32, i32, vp, vp, vp, vp)
+    f("b2s_learner_set_loss", i32, vp, i32)
     _lib = L
     return L
 
@@ -387,18 +389,23 @@ class HostPrecond:
 
 
 WEIGHTS = os.path.join(HERE, "weights", "learned_ic0.bin")
+LOSS_PRECOND, LOSS_FACTOR = 0, 1
 
 
 class Learner:
     """The learned-IC(0) message-passing network (b2s_learner)."""
 
-    def __init__(self, ctx: Context, seed: int = 0, weights: str | None = None):
+    def __init__(self, ctx: Context, seed: int = 0, weights: str | None = None, loss: int = LOSS_PRECOND):
         self.ctx = ctx
         h = C.c_void_p()
         ctx.check(lib().b2s_learner_create(ctx.h, seed, C.byref(h)), "learner_create")
         self.h = h
+        self.set_loss(loss)
         if weights:
             self.load(weights)
+
+    def set_loss(self, kind: int):
+        self.ctx.check(lib().b2s_learner_set_loss(self.h, int(kind)), "learner_set_loss")
 
     @property
     def nparams(self) -> int:

@@ -226,6 +226,13 @@ struct PcImpl
     {
         fail(B2S_UNSUPPORTED, "export '" + what + "' not available for this preconditioner");
     }
+    // one triangle of a factored preconditioner M = L L^T (FP64 storage):
+    // out = L^{-1} in (upper = false) or L^{-T} in (upper = true)
+    virtual void solve_factor(b2s_ctx*, bool upper, const double* in, double* out, const int* done)
+    {
+        (void)upper, (void)in, (void)out, (void)done;
+        fail(B2S_UNSUPPORTED, "no triangular factor solve for this preconditioner");
+    }
 };
 
 }  // namespace b2s

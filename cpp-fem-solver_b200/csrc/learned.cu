@@ -18,12 +18,18 @@
 //   (positive-pivot guard), so L~ L~^T stays SPD.
 // The output layer starts at zero: an untrained network returns IC(0).
 //
-// Training loss on probe vectors w (half standard normal, half smoothed by
+// Training losses on probe vectors w (half standard normal, half smoothed by
 // ten 2/3-Jacobi sweeps, the modes IC(0) resolves worst):
-//   loss = mean_w ||(L~ L~^T - A) w||^2 / ||A w||^2
-// whose gradient in L~ needs only products with L~ and L~^T:
-//   dloss/dL~_ij = 2 (v_i u_j + w_i q_j) / ||Aw||^2,  u = L~^T w,
-//   v = L~ u - A w,  q = L~^T v.
+//   preconditioned residual (B2S_LOSS_PRECOND, the default):
+//     loss = mean_w ||w - M^{-1} A w||^2 / ||w||^2,   M = L~ L~^T
+//     y = L~^{-1} A w, z = L~^{-T} y, g = -2 (w - z) / (P ||w||^2),
+//     a = L~^{-1} g, b = L~^{-T} a:  dloss/dL~_ij = -(z_i a_j + b_i y_j)
+//     (four triangular solves per probe, on the FP64 chunk schedules)
+//   factorisation residual (B2S_LOSS_FACTOR):
+//     loss = mean_w ||(L~ L~^T - A) w||^2 / ||A w||^2
+//     whose gradient needs only products with L~ and L~^T:
+//     dloss/dL~_ij = 2 (v_i u_j + w_i q_j) / ||Aw||^2,  u = L~^T w,
+//     v = L~ u - A w,  q = L~^T v.
 // All parameter gradients are reduced in a fixed order (per-CTA partials,
 // then one ordered sum), so training is deterministic.
 #include <cuda_bf16.h>
@@ -572,6 +578,41 @@ __global__ void k_dL(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_
         }
 }
 
+// preconditioned-residual loss: e = w - z
+__global__ void k_sub(uint32_t n, const double* __restrict__ w, const double* __restrict__ z, double* __restrict__ e)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) e[i] = w[i] - z[i];
+}
+
+// g = -scale * e
+__global__ void k_neg_scale(uint32_t n, const double* __restrict__ e, const double* __restrict__ scale,
+                            double* __restrict__ g)
+{
+    const double s = *scale;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) g[i] = -s * e[i];
+}
+
+// dL~_ij -= z_i a_j + b_i y_j
+__global__ void k_dL_pc(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lci,
+                        const double* __restrict__ z, const double* __restrict__ a, const double* __restrict__ b,
+                        const double* __restrict__ y, double* __restrict__ dL)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        for (uint32_t q = Lrp[i]; q < Lrp[i + 1]; ++q)
+        {
+            const uint32_t j = Lci[q];
+            dL[q] -= z[i] * a[j] + b[i] * y[j];
+        }
+}
+
+// diag[i] = L_ii, the last entry of row i of L (columns ascending, j <= i)
+__global__ void k_diag_from_rows(uint32_t n, const uint32_t* __restrict__ Lrp, const double* __restrict__ Lv,
+                                 double* __restrict__ diag)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        diag[i] = Lv[Lrp[i + 1] - 1];
+}
+
 // scale = 2 / (P ||Aw||^2), loss += ||v||^2 / (P ||Aw||^2)
 __global__ void k_loss_scale(const double* vv, const double* aw2, int nprobes, double* scale, double* loss)
 {
@@ -834,6 +875,20 @@ struct LearnedCorrection final : Ic0Correction
     }
 };
 
+// a factor computed elsewhere (the training step's L~) placed into an IC(0)
+// preconditioner on the same pattern, so its triangular solves can be reused
+struct GivenFactor final : Ic0Correction
+{
+    const double* src;
+    explicit GivenFactor(const double* s) : src(s) {}
+    void correct(b2s_ctx* ctx, const CsrDev& A, const uint32_t* Lrp, const uint32_t*, uint32_t Lnnz, double* Lv,
+                 double* diag) override
+    {
+        d2d(ctx, Lv, src, Lnnz * sizeof(double));
+        B2S_LAUNCH(ctx, k_diag_from_rows, stream_grid(ctx, A.n), kThreads, 0, A.n, Lrp, Lv, diag);
+    }
+};
+
 }  // namespace b2s
 
 // ------------------------------------------------------------ learner handle
@@ -842,6 +897,7 @@ struct b2s_learner
 {
     b2s_ctx* ctx = nullptr;
     b2s::Gnn net;
+    int loss = B2S_LOSS_PRECOND;
 };
 
 namespace b2s {
@@ -938,7 +994,7 @@ struct TrainBuffers
 };
 
 static void train_step(b2s_ctx* ctx, Gnn& net, const CsrDev& A, int nprobes, uint64_t seed, const double* host_probes,
-                       double lr, bool update, double* loss_out, float* grad_out)
+                       double lr, bool update, double* loss_out, float* grad_out, int loss_kind)
 {
     need(nprobes > 0 && nprobes <= 64, B2S_INVALID_ARG, "nprobes must be 1..64");
     const uint32_t n = A.n;
@@ -979,6 +1035,19 @@ static void train_step(b2s_ctx* ctx, Gnn& net, const CsrDev& A, int nprobes, uin
     T.vres.alloc(n);
     T.qv.alloc(n);
     T.scal.alloc(4);
+    // preconditioned-residual loss: M = L~ L~^T as an FP64 IC(0) on the same
+    // pattern (its chunk-scheduled triangular solves), two more work vectors
+    std::unique_ptr<PcImpl> M;
+    DBuf<double> ya, yb;
+    if (loss_kind == B2S_LOSS_PRECOND)
+    {
+        b2s_pc_opts o64;
+        b2s_pc_opts_default(&o64);
+        GivenFactor gf(Lv.p);
+        M = make_pc_ic0_ex(ctx, A, o64, &gf);
+        ya.alloc(n);
+        yb.alloc(n);
+    }
     B2S_CUDA(cudaMemsetAsync(T.scal.p, 0, T.scal.bytes(), ctx->stream));
     const unsigned gn = stream_grid(ctx, n);
     reserve_reduction(ctx, gn);
@@ -997,6 +1066,22 @@ static void train_step(b2s_ctx* ctx, Gnn& net, const CsrDev& A, int nprobes, uin
                 }
         }
         spmv(ctx, A, T.w.p, T.Aw.p);
+        if (loss_kind == B2S_LOSS_PRECOND)
+        {
+            // y = L~^-1 Aw (u), z = L~^-T y (qv), e = w - z (vres)
+            M->solve_factor(ctx, false, T.Aw.p, T.u.p, nullptr);
+            M->solve_factor(ctx, true, T.u.p, T.qv.p, nullptr);
+            B2S_LAUNCH(ctx, k_sub, gn, kThreads, 0, n, T.w.p, T.qv.p, T.vres.p);
+            dot_dev(ctx, n, T.vres.p, T.vres.p, T.scal.p);
+            dot_dev(ctx, n, T.w.p, T.w.p, T.scal.p + 1);
+            B2S_LAUNCH(ctx, k_loss_scale, 1, 1, 0, T.scal.p, T.scal.p + 1, nprobes, T.scal.p + 2, T.scal.p + 3);
+            // g = -scale e (Aw is free now), a = L~^-1 g, b = L~^-T a
+            B2S_LAUNCH(ctx, k_neg_scale, gn, kThreads, 0, n, T.vres.p, T.scal.p + 2, T.Aw.p);
+            M->solve_factor(ctx, false, T.Aw.p, ya.p, nullptr);
+            M->solve_factor(ctx, true, ya.p, yb.p, nullptr);
+            B2S_LAUNCH(ctx, k_dL_pc, gn, kThreads, 0, n, Lrp.p, Lci.p, T.qv.p, ya.p, yb.p, T.u.p, dL.p);
+            continue;
+        }
         dot_dev(ctx, n, T.Aw.p, T.Aw.p, T.scal.p + 1);
         B2S_LAUNCH(ctx, k_ltmul, gn, kThreads, 0, n, Lrp.p, Trp.p, Tci.p, Tpos.p, Lv.p, T.w.p, T.u.p);
         B2S_LAUNCH(ctx, k_lmul_res, gn, kThreads, 0, n, Lrp.p, Lci.p, Lv.p, T.u.p, T.Aw.p, T.vres.p, T.scal.p,
@@ -1130,8 +1215,15 @@ b2s_status b2s_learner_step(b2s_ctx* ctx, b2s_learner* L, const b2s_csr* A, int 
     if (!ctx || !L || !A) return B2S_INVALID_ARG;
     return guarded(ctx, [&] {
         need(A->d.n == A->d.m, B2S_SHAPE, "learned IC(0) needs a square matrix");
-        train_step(ctx, L->net, A->d, nprobes, seed, probes, lr, update != 0, loss, grad);
+        train_step(ctx, L->net, A->d, nprobes, seed, probes, lr, update != 0, loss, grad, L->loss);
     });
+}
+
+b2s_status b2s_learner_set_loss(b2s_learner* L, int kind)
+{
+    if (!L || (kind != B2S_LOSS_PRECOND && kind != B2S_LOSS_FACTOR)) return B2S_INVALID_ARG;
+    L->loss = kind;
+    return B2S_OK;
 }
 
 b2s_status b2s_dense_bf16_device(b2s_ctx* ctx, uint64_t n, int k, int no, const float* d_x, const uint16_t* d_w,

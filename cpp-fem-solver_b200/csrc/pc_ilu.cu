@@ -481,6 +481,15 @@ struct PcIC0 final : PcImpl
         }
     }
 
+    void solve_factor(b2s_ctx* ctx, bool upper, const double* in, double* out, const int* done) override
+    {
+        need(!fp32, B2S_UNSUPPORTED, "triangular factor solves need an FP64 IC(0)");
+        if (upper)
+            bwd.solve<double, double, double>(ctx, mode, LT.v.p, diag.p, in, out, nullptr, done);
+        else
+            fwd.solve<double, double, double>(ctx, mode, L.v.p, diag.p, in, out, nullptr, done);
+    }
+
     void export_data(b2s_ctx* ctx, const std::string& what, uint64_t* sizes, uint32_t* rp, uint32_t* ci,
                      double* v) override
     {

@@ -219,11 +219,15 @@ b2s_status b2s_learner_load(b2s_learner* L, const char* path);
 b2s_status b2s_learner_save(b2s_learner* L, const char* path);
 /* FP32 master parameters: get (set == 0) or set (set == 1); *count in/out. */
 b2s_status b2s_learner_params(b2s_learner* L, float* params, uint64_t* count, int set);
-/* One training step on A (SPD, structurally symmetric): loss
- * mean_w ||(L~L~^T - A) w||^2 / ||A w||^2 over nprobes probes (generated from
- * seed, every second one Jacobi-smoothed; or taken from `probes`, host,
- * nprobes * n, when not NULL).  update = 1 applies one Adam step with
- * learning rate lr.  loss and grad (host, count floats) are optional. */
+/* Training loss of b2s_learner_step, over probe vectors w: */
+#define B2S_LOSS_PRECOND 0 /* preconditioned residual mean_w ||w - (L~L~^T)^{-1} A w||^2 / ||w||^2 (default) */
+#define B2S_LOSS_FACTOR 1  /* factorisation residual mean_w ||(L~L~^T - A) w||^2 / ||A w||^2 */
+b2s_status b2s_learner_set_loss(b2s_learner* L, int kind);
+/* One training step on A (SPD, structurally symmetric) with the learner's
+ * loss over nprobes probes (generated from seed, every second one
+ * Jacobi-smoothed; or taken from `probes`, host, nprobes * n, when not NULL).
+ * update = 1 applies one Adam step with learning rate lr.  loss and grad
+ * (host, count floats) are optional. */
 b2s_status b2s_learner_step(b2s_ctx* ctx, b2s_learner* L, const b2s_csr* A, int nprobes, uint64_t seed,
                             const double* probes, double lr, int update, double* loss, float* grad);
 /* IC(0) corrected by this network (the same kernels as B2S_PC_LEARNED_IC0). */

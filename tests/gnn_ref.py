@@ -57,8 +57,13 @@ def features(n, rp, ci, v):
             invdeg.astype(np.float32).astype(np.float64), diag)
 
 
-def loss_and_grad(params, n, rp, ci, v, Lrp, Lci, L0, probes):
-    """params: FP32 master parameters (rounded to BF16 as the GPU forward does)."""
+LOSS_PRECOND, LOSS_FACTOR = 0, 1
+
+
+def loss_and_grad(params, n, rp, ci, v, Lrp, Lci, L0, probes, loss_kind=LOSS_PRECOND):
+    """params: FP32 master parameters (rounded to BF16 as the GPU forward does).
+    loss_kind: LOSS_PRECOND, mean_w ||w - (L~L~^T)^{-1} A w||^2 / ||w||^2, or
+    LOSS_FACTOR, mean_w ||(L~L~^T - A) w||^2 / ||A w||^2."""
     P = bf16_round(params).requires_grad_(True)
     F, EF, invdeg, diag = features(n, rp, ci, v)
     F, EF, invdeg = map(torch.from_numpy, (F, EF, invdeg))
@@ -101,7 +106,13 @@ def loss_and_grad(params, n, rp, ci, v, Lrp, Lci, L0, probes):
                                 (n, n)).to_dense()
     W = torch.from_numpy(np.asarray(probes).reshape(-1, n).T)
     AW = A @ W
-    E = Lmat @ (Lmat.T @ W) - AW
-    loss = ((E ** 2).sum(0) / (AW ** 2).sum(0)).mean()
+    if loss_kind == LOSS_PRECOND:
+        Y = torch.linalg.solve_triangular(Lmat, AW, upper=False)
+        Z = torch.linalg.solve_triangular(Lmat.T, Y, upper=True)
+        E = W - Z
+        loss = ((E ** 2).sum(0) / (W ** 2).sum(0)).mean()
+    else:
+        E = Lmat @ (Lmat.T @ W) - AW
+        loss = ((E ** 2).sum(0) / (AW ** 2).sum(0)).mean()
     loss.backward()
     return float(loss), P.grad.numpy(), Lt.detach().numpy()
