@@ -124,6 +124,7 @@ KERNELS = {
     "baij_c4": "k_baij_warp<3>: BAIJ 3x3 matvec on the Q1 elasticity matrix (C4, 64^3 elements)",
     "trsv_c5": "k_trsv_chunk: FP32 IC(0) apply (L then L^T) on a 512^2 GRF system (C5)",
     "trsv_c5_fp64": "k_trsv_chunk: FP64 IC(0) apply on a 512^2 GRF system (C5)",
+    "trsv_c5_j8": "k_trsv_band: FP32 IC(0) apply with 8 Jacobi sweeps per triangle on a 512^2 GRF system (C5)",
     "trsv_c2": "k_trsv_chunk: FP64 ILU(0) apply on the 128^3 Poisson matrix (C2)",
     "btrsv_c4": "k_btrsv_chunk: FP64 block ILU(0) apply on the Q1 elasticity matrix (C4, 64^3 elements)",
     "vcycle_c2": "SA-AMG V-cycle (k_jacobi, BAIJ matvecs, k_dense_solve) on C2",
@@ -168,10 +169,13 @@ def run_kernel(args):
                                                                 C.c_void_p(w.data_ptr()), None,
                                                                 C.c_void_p(y.data_ptr())), "dense_bf16")
     else:
-        if k in ("trsv_c5", "trsv_c5_fp64"):
+        if k in ("trsv_c5", "trsv_c5_fp64", "trsv_c5_j8"):
             n, rp, ci, v = b2s.gen_grf_diffusion(N_GRID, 2000, corr=CORR)
             A = b2s.CSR(ctx, n, n, rp, ci, v)
-            M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32 if k == "trsv_c5" else b2s.FP64)
+            if k == "trsv_c5_j8":
+                M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8)
+            else:
+                M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32 if k == "trsv_c5" else b2s.FP64)
         elif k == "trsv_c2":
             n, rp, ci, v = b2s.gen_poisson3d(128)
             A = b2s.CSR(ctx, n, n, rp, ci, v)
@@ -262,7 +266,8 @@ def main():
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b2s", choices=["b2s", "reference"])
-    ap.add_argument("--method", default="learned_ic0", choices=["fp32_ic0", "fp64_ic0", "learned_ic0"])
+    ap.add_argument("--method", default="learned_ic0_j8",
+                    choices=["learned_ic0_j8", "learned_ic0", "fp32_ic0_j8", "fp32_ic0", "fp64_ic0"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel", default=None, choices=sorted(KERNELS),
                     help="run one hot kernel only (for profilers), not the benchmark")
@@ -290,8 +295,16 @@ def main():
     seeds = [2000 + rank * 100000 + k for k in range(args.warmup + args.steps)]
     systems = [make_system(b2s, s) for s in seeds]
 
-    kinds = {"fp32_ic0": (b2s.PC_IC0, b2s.FP32), "fp64_ic0": (b2s.PC_IC0, b2s.FP64),
-             "learned_ic0": (b2s.PC_LEARNED_IC0, b2s.FP32)}
+    # method -> (preconditioner, precision, triangular-solve schedule, sweeps)
+    kinds = {"learned_ic0_j8": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_JACOBI, 8),
+             "learned_ic0": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_AUTO, 0),
+             "fp32_ic0_j8": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_JACOBI, 8),
+             "fp32_ic0": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_AUTO, 0),
+             "fp64_ic0": (b2s.PC_IC0, b2s.FP64, b2s.TRSV_AUTO, 0)}
+
+    def make_pc(A, method):
+        kind, prec, trsv, sweeps = kinds[method]
+        return b2s.Precond(ctx, A, kind, precision=prec, trsv=trsv, trsv_sweeps=sweeps)
 
     def timed_solve(n, rp, ci, v, b, method):
         """Device-resident inputs; returns (ms, stats, relres_true)."""
@@ -301,11 +314,10 @@ def main():
         torch.cuda.synchronize()
         flush.fill_(1.0)
         torch.cuda.synchronize()
-        kind, prec = kinds[method]
         e0, em, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         l0 = ctx.kernel_launches
         e0.record(stream)
-        M = b2s.Precond(ctx, A, kind, precision=prec)
+        M = make_pc(A, method)
         em.record(stream)
         st = b2s.solve_device(ctx, A, bt.data_ptr(), xt.data_ptr(), b2s.PCG, M, tol=TOL, maxit=MAXIT)
         e1.record(stream)
@@ -346,10 +358,21 @@ def main():
     base_ms, base_its, base_rel, _ = run("fp64_ic0", range(min(1, args.warmup))) if args.method != "fp64_ic0" else (
         head_ms, head_its, head_rel, 0)
     base_split = run.split
+    # the other methods on the same systems (context for the headline: what
+    # the learned values and the sweep solves each contribute)
+    variants = {}
+    for m in kinds:
+        if m in (args.method, "fp64_ic0"):
+            continue
+        v_ms, v_its, v_rel, _ = run(m, range(min(1, args.warmup)))
+        variants[m] = {"ms": float(np.mean(v_ms)), "iterations_mean": float(np.mean(v_its)),
+                       "relres_true_max": float(np.max(v_rel)), "fallbacks": int(run.fallbacks),
+                       "setup_ms_mean": float(np.mean([a for a, _ in run.split])),
+                       "speedup_vs_fp64_ic0": float(np.mean(base_ms)) / float(np.mean(v_ms))}
 
     # e2e: host CSR + host b -> device, preconditioner, solve, x -> host (public C ABI, host pointers)
     e2e_ms, h2d, d2h = [], 0, 0
-    kind, prec = kinds[args.method]
+    kind, prec, trsv, sweeps = kinds[args.method]
     for k in range(args.steps):
         n, rp, ci, v, b = systems[args.warmup + k]
         torch.cuda.synchronize()
@@ -357,25 +380,36 @@ def main():
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         A = b2s.CSR(ctx, n, n, rp, ci, v)
-        M = b2s.Precond(ctx, A, kind, precision=prec)
+        M = make_pc(A, args.method)
         x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=TOL, maxit=MAXIT)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
         h2d = rp.nbytes + ci.nbytes + v.nbytes + b.nbytes
         d2h = x.nbytes
         del A, M
 
-    # roofline of the dominant kernel: the sync-free triangular solve of the
-    # preconditioner apply (forward L, backward L^T).  Algorithmic bytes of one
-    # triangle: factor values + column indices + row pointers + rhs + solution
-    # + diagonal, each read or written once.
+    # roofline of the dominant kernel: one triangle of the preconditioner
+    # apply (forward L, backward L^T).  Sweep schedule (k_trsv_band): per row
+    # W packed strict entries (u16 offset + FP32 value), the FP32 reciprocal,
+    # the rhs (FP64 forward / FP32 backward) and the FP32 result, each read or
+    # written once (the FP64 copy of the backward result is not counted).
+    # Exact schedule (k_trsv_chunk): factor values + column indices + row
+    # pointers + rhs + solution + diagonal.
     n, rp, ci, v, b = systems[args.warmup]
     A = b2s.CSR(ctx, n, n, rp, ci, v)
-    M = b2s.Precond(ctx, A, kind, precision=prec)
+    M = make_pc(A, args.method)
     r = torch.from_numpy(b).to(dev)
     z = torch.empty_like(r)
     nnz_l = (len(v) + n) // 2
     vb = 4 if prec == b2s.FP32 else 8
-    tri_bytes = nnz_l * (vb + 4) + 4 * (n + 1) + 3 * vb * n
+    if trsv == b2s.TRSV_JACOBI:
+        tri_bytes = n * (2 * 6 + 4 + 6 + 4)
+        tri_kernel = f"k_trsv_band (Jacobi-sweep triangle, {sweeps} sweeps in one launch)"
+        tri_note = ("one launch per triangle; the halo rows (k*B = 4096 per 1,792-row tile) are re-read and "
+                    "recomputed by each tile, so the kernel moves about 3.3x the algorithmic bytes, from L2")
+    else:
+        tri_bytes = nnz_l * (vb + 4) + 4 * (n + 1) + 3 * vb * n
+        tri_kernel = "k_trsv_chunk (IC(0) triangular solve, one triangle per launch)"
+        tri_note = "latency-bound: a 1023-level dependency chain per triangle on the 512^2 grid"
     for _ in range(3):
         b2s.lib().b2s_pc_apply_device(ctx.h, M.h, b2s.C.c_void_p(r.data_ptr()), b2s.C.c_void_p(z.data_ptr()))
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -388,10 +422,10 @@ def main():
     tri_ms = e0.elapsed_time(e1) / reps / 2
     pk, pk_kind = peaks()
     achieved = tri_bytes / (tri_ms * 1e-3) / 1e9
-    roofline = {"kernel": "k_trsv_chunk (IC(0) triangular solve, one triangle per launch)", "bound": "hbm",
+    roofline = {"kernel": tri_kernel, "bound": "hbm",
                 "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                 "peak_kind": pk_kind, "traffic": None, "bytes_per_launch": tri_bytes, "ms_per_launch": tri_ms,
-                "note": "latency-bound: a 1023-level dependency chain per triangle on the 512^2 grid"}
+                "note": tri_note}
 
     # the learned network's tcgen05 dense layer (64 -> 128) on this grid's node
     # states: X read once, Y written once
@@ -469,6 +503,12 @@ def main():
             "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 outer / f32 preconditioner" if prec == b2s.FP32 else "f64",
+            "method": {"learned_ic0_j8": "learned IC(0) values (tcgen05 network), FP32 factor, 8 Jacobi sweeps per "
+                                         "triangle (banded one-launch kernel), FP64 PCG and true residual",
+                       "learned_ic0": "learned IC(0) values, FP32 factor, exact chunk-scheduled triangular solves",
+                       "fp32_ic0_j8": "plain IC(0), FP32 factor, 8 Jacobi sweeps per triangle",
+                       "fp32_ic0": "plain IC(0), FP32 factor, exact triangular solves",
+                       "fp64_ic0": "plain IC(0), FP64, exact triangular solves"}[args.method],
             "data": "synthetic (seeded GRF diffusion, held-out seeds 2000+)",
             "config": {"workload": "grf_diffusion_512 pcg rtol1e-8", "method": args.method, "grid": N_GRID,
                        "corr": CORR, "parallelism": f"replicas x{world}", "l2": "flushed (512 MB write) before every step"},
@@ -481,6 +521,7 @@ def main():
                              "setup_ms_mean": float(np.mean([a for a, _ in base_split])),
                              "iter_ms_mean": float(np.mean([b for _, b in base_split]))},
             "speedup_vs_fp64_ic0": float(np.mean(base_ms)) / value,
+            "variants": variants,
             "e2e": {"value": float(np.mean(e2e_ms)), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),

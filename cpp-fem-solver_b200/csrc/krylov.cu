@@ -831,19 +831,27 @@ struct Solve
     {
         cudaGraphExec_t exec = nullptr;
         cudaGraph_t graph = nullptr;
+        uint64_t per_replay = 0;  // kernels in the captured batch
         if (graphs)
         {
+            const uint64_t l0 = ctx->launches;
             B2S_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
             for (int k = 0; k < poll_every; ++k) body();
             B2S_CUDA(cudaStreamEndCapture(ctx->stream, &graph));
             B2S_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+            // captured launches did not run; every replay runs them once
+            per_replay = ctx->launches - l0;
+            ctx->launches = l0;
         }
         double best = HUGE_VAL;
         int best_at = 0;
         for (;;)
         {
             if (exec)
+            {
                 B2S_CUDA(cudaGraphLaunch(exec, ctx->stream));
+                ctx->launches += per_replay;
+            }
             else
                 for (int k = 0; k < poll_every; ++k) body();
             KState h = read_state();

@@ -314,6 +314,7 @@ std::unique_ptr<PcImpl> make_pc_bilu0(b2s_ctx* ctx, const BaijDev& A, const b2s_
     const int bs = A.bs, bv = bs * bs;
     pc->bs = bs;
     pc->nb = nb;
+    need(o.trsv != B2S_TRSV_JACOBI, B2S_UNSUPPORTED, "block ILU(0): Jacobi-sweep triangular solves are not provided");
     pc->mode = o.trsv == B2S_TRSV_AUTO ? B2S_TRSV_CHUNK : o.trsv;
     pc->fp32 = o.precision != B2S_FP64;
     pc->udiag.alloc(nb ? nb : 1);

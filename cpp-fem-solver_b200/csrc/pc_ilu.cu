@@ -24,6 +24,7 @@
 
 #include "trisolve.cuh"
 #include "trsv_chunk.cuh"
+#include "trsv_band.cuh"
 
 #include <exception>
 #include <thread>
@@ -313,6 +314,54 @@ struct TrsvOp
     __device__ void compute(uint32_t row) const { row_compute<true>(row); }
 };
 
+// D^-1 a in a Jacobi sweep: FP64 divides (the exact solves' arithmetic, so
+// enough sweeps reproduce them bit for bit); FP32 multiplies by the FP32
+// reciprocal 1/d, the value the banded kernel packs.
+template <typename XT>
+__device__ __forceinline__ XT jacobi_scale(XT a, XT d)
+{
+    if constexpr (sizeof(XT) == 4)
+        return a * (1.f / d);
+    else
+        return a / d;
+}
+
+// One Jacobi sweep of a triangle T = D + N (B2S_TRSV_JACOBI):
+//   y_out = D^-1 (rhs - N y_in),  y_in = D^-1 rhs on the first sweep (FIRST),
+// so k sweeps give the k-term truncated Neumann series of T^-1 rhs.  Every row
+// is independent: one thread per row, the row's strict entries in column
+// order, FP32 or FP64 as the factor.
+template <bool LOWER, bool UNIT, bool FIRST, typename VT, typename XT, typename RT>
+__global__ void __launch_bounds__(kThreads) k_trsv_sweep(uint32_t n, const uint32_t* __restrict__ rp,
+                                                         const uint32_t* __restrict__ ci, const VT* __restrict__ v,
+                                                         const VT* __restrict__ d, const RT* __restrict__ rhs,
+                                                         const XT* __restrict__ yin, XT* __restrict__ yout,
+                                                         double* __restrict__ out64, const int* done)
+{
+    if (done && *done) return;
+    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x)
+    {
+        XT sum = (XT)rhs[row];
+        const uint32_t a = __ldg(&rp[row]), b = __ldg(&rp[row + 1]);
+        for (uint32_t p = a; p < b; ++p)
+        {
+            const uint32_t j = __ldg(&ci[p]);
+            if (LOWER ? (j < row) : (j > row))
+            {
+                XT xj;
+                if (FIRST)
+                    xj = UNIT ? (XT)rhs[j] : jacobi_scale<XT>((XT)rhs[j], (XT)__ldg(&d[j]));
+                else
+                    xj = yin[j];
+                sum -= (XT)__ldg(&v[p]) * xj;
+            }
+        }
+        const XT r = UNIT ? sum : jacobi_scale<XT>(sum, (XT)__ldg(&d[row]));
+        yout[row] = r;
+        if (out64) out64[row] = (double)r;
+    }
+}
+
 // A triangular factor ready for solves: CSR rows + divisor + schedule.
 struct Tri
 {
@@ -326,11 +375,91 @@ struct Tri
     ChunkSchedule cs;
     bool has_chunks = false, sched_ready = false;
     std::vector<uint32_t> h_level;  // host copy of the rows' levels (compute_levels), when known
+    int sweeps = 8;                 // B2S_TRSV_JACOBI
+    DBuf<double> jw64[2];           // sweep ping-pong buffers, made at setup
+    DBuf<float> jw32[2];
+    BandPlan band;                  // FP32 banded triangles: all sweeps in one launch
+    DBuf<uint16_t> band_off;        // packed strict entries and reciprocals (k_band_pack)
+    DBuf<float> band_val, band_dinv;
+
+    // hrp / hci: the triangle's pattern on the host (for the band plan)
+    void prepare_sweeps(b2s_ctx* ctx, int k, bool fp32, const uint32_t* hrp, const uint32_t* hci)
+    {
+        sweeps = k > 0 ? k : 8;
+        if (fp32 && hrp && hci) band = plan_band(n, hrp, hci, lower, sweeps, ctx->sm_count);
+        if (band.T)
+        {
+            band_off.alloc((size_t)band.W * n);
+            band_val.alloc((size_t)band.W * n);
+            band_dinv.alloc(n);
+            return;
+        }
+        for (int b = 0; b < 2; ++b)
+        {
+            if (fp32)
+                jw32[b].alloc(n ? n : 1);
+            else
+                jw64[b].alloc(n ? n : 1);
+        }
+    }
+
+    template <bool LOWER, typename RT>
+    void run_band(b2s_ctx* ctx, const RT* rhs, float* x, double* out64, const int* done)
+    {
+        if (band.W == 2)
+        {
+            auto kern = k_trsv_band<LOWER, 2, RT>;
+            B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)band.smem));
+            B2S_LAUNCH(ctx, kern, band.ntiles, band_threads(2), band.smem, n, band.T, band.B, band.Rmax, sweeps,
+                       band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done);
+        }
+        else
+        {
+            auto kern = k_trsv_band<LOWER, 4, RT>;
+            B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)band.smem));
+            B2S_LAUNCH(ctx, kern, band.ntiles, band_threads(4), band.smem, n, band.T, band.B, band.Rmax, sweeps,
+                       band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done);
+        }
+    }
+
+    template <bool LOWER, bool UNIT, typename VT, typename XT, typename RT>
+    void run_sweeps(b2s_ctx* ctx, const VT* v, const VT* d, const RT* rhs, XT* x, double* out64, const int* done)
+    {
+        if constexpr (sizeof(VT) == 4 && sizeof(XT) == 4)
+        {
+            if (band.T)
+            {
+                if (n) run_band<LOWER, RT>(ctx, rhs, x, out64, done);
+                return;
+            }
+        }
+        XT* buf[2];
+        if constexpr (sizeof(XT) == 4)
+            buf[0] = jw32[0].p, buf[1] = jw32[1].p;
+        else
+            buf[0] = jw64[0].p, buf[1] = jw64[1].p;
+        need(buf[0] && buf[1], B2S_INVALID_ARG, "Jacobi triangular solve: sweep buffers not prepared");
+        const unsigned g = stream_grid(ctx, n);
+        for (int s = 0; s < sweeps; ++s)
+        {
+            const bool last = s == sweeps - 1;
+            XT* out = last ? x : buf[s & 1];
+            double* o64 = last ? out64 : nullptr;
+            if (s == 0)
+                B2S_LAUNCH(ctx, (k_trsv_sweep<LOWER, UNIT, true, VT, XT, RT>), g, kThreads, 0, n, m->rp.p, m->ci.p, v, d,
+                           rhs, (const XT*)nullptr, out, o64, done);
+            else
+                B2S_LAUNCH(ctx, (k_trsv_sweep<LOWER, UNIT, false, VT, XT, RT>), g, kThreads, 0, n, m->rp.p, m->ci.p, v,
+                           d, rhs, buf[(s - 1) & 1], out, o64, done);
+        }
+    }
 
     template <bool LOWER, bool UNIT, typename VT, typename XT, typename RT>
     void run_t(b2s_ctx* ctx, int mode, const VT* v, const VT* d, const RT* rhs, XT* x, double* out64, const int* done)
     {
-        if (mode == B2S_TRSV_CHUNK && has_chunks && cs.usable<VT, XT, RT>())
+        if (mode == B2S_TRSV_JACOBI)
+            run_sweeps<LOWER, UNIT, VT, XT, RT>(ctx, v, d, rhs, x, out64, done);
+        else if (mode == B2S_TRSV_CHUNK && has_chunks && cs.usable<VT, XT, RT>())
             cs.run<LOWER, UNIT, VT, XT, RT>(ctx, v, d, rhs, x, out64, done);
         else
             run_schedule(ctx, mode == B2S_TRSV_LEVEL ? B2S_TRSV_LEVEL : B2S_TRSV_SYNCFREE, sched, sf,
@@ -375,7 +504,7 @@ struct Tri
     void load_chunks(b2s_ctx* ctx, int mode, const ChunkPlan* plan, uint32_t vs)
     {
         has_chunks = mode == B2S_TRSV_CHUNK && n && plan && cs.load(ctx, *plan, vs);
-        if (!has_chunks) ensure_sched(ctx);
+        if (!has_chunks && mode != B2S_TRSV_JACOBI) ensure_sched(ctx);
     }
 
     // lay the final factor values out for the chunk schedule (no-op otherwise)
@@ -383,6 +512,12 @@ struct Tri
     void pack(b2s_ctx* ctx, const VT* v, const VT* d)
     {
         if (has_chunks && sizeof(VT) <= cs.plan_vs) cs.pack<VT>(ctx, v, d);
+        if constexpr (sizeof(VT) == 4)
+        {
+            if (band.T && n)
+                B2S_LAUNCH(ctx, k_band_pack, stream_grid(ctx, n), kThreads, 0, n, band.W, lower ? 1 : 0,
+                           unit ? 1 : 0, m->rp.p, m->ci.p, v, d, band_off.p, band_val.p, band_dinv.p);
+        }
     }
 };
 
@@ -429,7 +564,12 @@ static void to_f32(b2s_ctx* ctx, const DBuf<double>& a, DBuf<float>& b, uint64_t
     if (n) B2S_LAUNCH(ctx, k_f64_to_f32, stream_grid(ctx, n), kThreads, 0, a.p, b.p, n);
 }
 
-static int pick_trsv(const b2s_pc_opts& o) { return o.trsv == B2S_TRSV_AUTO ? B2S_TRSV_CHUNK : o.trsv; }
+static int pick_trsv(const b2s_pc_opts& o)
+{
+    need(o.trsv >= B2S_TRSV_AUTO && o.trsv <= B2S_TRSV_JACOBI, B2S_INVALID_ARG, "unknown triangular-solve schedule");
+    need(o.trsv_sweeps >= 0 && o.trsv_sweeps <= 1024, B2S_INVALID_ARG, "trsv_sweeps must be 0..1024");
+    return o.trsv == B2S_TRSV_AUTO ? B2S_TRSV_CHUNK : o.trsv;
+}
 
 static void export_csr(b2s_ctx* ctx, const Csr32& m, uint64_t* sizes, uint32_t* rp, uint32_t* ci, double* v)
 {
@@ -588,6 +728,11 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     pc->bwd.h_level = std::move(ha.up_level);
     pc->fwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.lo_plan : nullptr, vs);
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
+    if (pc->mode == B2S_TRSV_JACOBI)
+    {
+        pc->fwd.prepare_sweeps(ctx, o.trsv_sweeps, pc->fp32, hrp.data(), hci.data());
+        pc->bwd.prepare_sweeps(ctx, o.trsv_sweeps, pc->fp32, ha.up_rp.data(), ha.up_ci.data());
+    }
     if (pc->fp32)
     {
         pc->fwd.pack<float>(ctx, pc->L.v32.p, pc->diag32.p);
@@ -721,6 +866,11 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     pc->bwd.h_level = std::move(ha.up_level);
     pc->fwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.lo_plan : nullptr, vs);
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
+    if (pc->mode == B2S_TRSV_JACOBI)
+    {
+        pc->fwd.prepare_sweeps(ctx, o.trsv_sweeps, pc->fp32, lrp.data(), lci.data());
+        pc->bwd.prepare_sweeps(ctx, o.trsv_sweeps, pc->fp32, urp.data(), uci.data());
+    }
     if (pc->fp32)
     {
         pc->fwd.pack<float>(ctx, pc->L.v32.p, (const float*)nullptr);

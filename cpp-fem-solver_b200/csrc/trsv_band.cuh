@@ -1,0 +1,191 @@
+// Jacobi-sweep triangular solve of a banded triangle in one launch
+// (B2S_TRSV_JACOBI, FP32 factors whose strict entries lie within B rows of
+// the diagonal -- natural-order 2-D grids, for example).
+//
+// k sweeps of  y_s = D^-1 (rhs - N y_{s-1}),  y_0 = D^-1 rhs,  T = D + N
+// (FP32: D^-1 is the packed reciprocal 1/d): row i of y_s depends on rows
+// i-B .. i-1 of y_{s-1} (lower; i+1 .. i+B upper), so the rows [lo, hi) of
+// y_k depend only on rows [lo - kB, hi) of the input.  A CTA loads that
+// extended range once -- each thread keeps its rows' strict entries (u16
+// offsets, FP32 values), right-hand side and reciprocal in registers -- and
+// runs all k sweeps with only the sweep vectors in shared memory, separated
+// by __syncthreads.  At sweep s it computes only the rows whose inputs are
+// still exact (from the range start plus s*B on), so nothing it reads is
+// stale and rows [lo, hi) equal the one-launch-per-sweep schedule bit for
+// bit.  The halo is recomputed by the neighbouring tiles (redundant work
+// instead of communication): no CTA waits on another.  The strict entries
+// and reciprocals are packed once per factorisation (k_band_pack).
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+
+namespace b2s {
+
+constexpr uint32_t kBandRowsPerThread = 8;
+
+// W = 2: 768 threads, W = 4: 512 (register budget: 8 rows of W offsets and
+// values, rhs and reciprocal per thread)
+__host__ __device__ constexpr uint32_t band_threads(uint32_t W) { return W <= 2 ? 768u : 512u; }
+
+struct BandPlan
+{
+    uint32_t T = 0;      // rows per tile (0: not usable)
+    uint32_t B = 0;      // bandwidth: max |i - j| over strict entries
+    uint32_t W = 0;      // strict entries per row slot (2 or 4)
+    uint32_t Rmax = 0;   // extended rows per tile (T + k B)
+    uint32_t smem = 0;   // dynamic shared memory per CTA (two sweep vectors)
+    uint32_t ntiles = 0;
+};
+
+// Host planning from the triangle's pattern (rows in CSR, column-sorted);
+// lower: strict entries j < i, upper: j > i.  T is chosen so that the tiles
+// fill the SMs once while each thread holds at most kBandRowsPerThread rows.
+inline BandPlan plan_band(uint32_t n, const uint32_t* rp, const uint32_t* ci, bool lower, int k, int sm_count)
+{
+    BandPlan p;
+    if (!n || k <= 0) return p;
+    uint64_t B = 0, W = 0;
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        uint64_t w = 0;
+        for (uint32_t q = rp[i]; q < rp[i + 1]; ++q)
+        {
+            const uint32_t j = ci[q];
+            if (lower ? j < i : j > i)
+            {
+                ++w;
+                B = std::max<uint64_t>(B, lower ? i - j : j - i);
+            }
+        }
+        W = std::max(W, w);
+    }
+    if (B == 0) B = 1;
+    if (W > 4 || B > 65535) return p;
+    const uint32_t w = W <= 2 ? 2 : 4;
+    const uint64_t cap = (uint64_t)band_threads(w) * kBandRowsPerThread;
+    const uint64_t halo = (uint64_t)k * B;
+    uint64_t T = (n + (uint64_t)sm_count - 1) / (uint64_t)sm_count;
+    T = (T + 31) / 32 * 32;
+    if (T < 64) T = 64;
+    if (halo > 8 * T) return p;  // redundant work would dominate
+    const uint64_t Rm = std::min<uint64_t>(T + halo, n);
+    if (Rm > cap) return p;
+    p.T = (uint32_t)T;
+    p.B = (uint32_t)B;
+    p.W = w;
+    p.Rmax = (uint32_t)Rm;
+    p.smem = (uint32_t)(2 * Rm * sizeof(float));
+    p.ntiles = (uint32_t)((n + T - 1) / T);
+    return p;
+}
+
+// Setup: the triangle's strict entries as W column-major slots over all rows
+// (slot e of row i at e*n + i, in column order; offset 0 = no entry) and the
+// FP32 reciprocal of the divisor, so a tile loads its extended range with
+// independent, coalesced loads.
+__global__ void k_band_pack(uint32_t n, uint32_t W, int lower, int unit, const uint32_t* __restrict__ rp,
+                            const uint32_t* __restrict__ ci, const float* __restrict__ v, const float* __restrict__ d,
+                            uint16_t* __restrict__ eoff, float* __restrict__ eval, float* __restrict__ dinv)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        uint32_t e = 0;
+        for (uint32_t q = rp[i]; q < rp[i + 1] && e < W; ++q)
+        {
+            const uint32_t j = ci[q];
+            if (lower ? j < i : j > i)
+            {
+                eoff[(size_t)e * n + i] = (uint16_t)(lower ? i - j : j - i);
+                eval[(size_t)e * n + i] = v[q];
+                ++e;
+            }
+        }
+        for (; e < W; ++e)
+        {
+            eoff[(size_t)e * n + i] = 0;
+            eval[(size_t)e * n + i] = 0.f;
+        }
+        dinv[i] = unit ? 1.f : 1.f / d[i];
+    }
+}
+
+template <bool LOWER, int W, typename RT>
+__global__ void __launch_bounds__(band_threads(W)) k_trsv_band(uint32_t n, uint32_t T, uint32_t B, uint32_t Rmax,
+                                                             int k, const uint16_t* __restrict__ eoff,
+                                                             const float* __restrict__ eval,
+                                                             const float* __restrict__ dinv,
+                                                             const RT* __restrict__ rhs, float* __restrict__ x,
+                                                             double* __restrict__ out64, const int* done)
+{
+    constexpr uint32_t NT = band_threads(W), Q = kBandRowsPerThread;
+    if (done && *done) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* const y0 = reinterpret_cast<float*>(smem);
+    float* const y1 = y0 + Rmax;
+
+    const uint32_t lo = blockIdx.x * T;
+    if (lo >= n) return;
+    const uint32_t hi = min(n, lo + T);
+    const uint32_t halo = (uint32_t)k * B;
+    const uint32_t elo = LOWER ? (lo > halo ? lo - halo : 0u) : lo;
+    const uint32_t ehi = LOWER ? hi : (uint32_t)min((uint64_t)n, (uint64_t)hi + halo);
+    const uint32_t R = ehi - elo;  // <= Rmax <= NT * Q by the plan
+    const bool cut = LOWER ? elo > 0 : ehi < n;  // the range is truncated: the halo goes stale
+
+    // ---- this thread's rows t = tid + NT q: entries, rhs, reciprocal; y_0
+    uint32_t off[Q][W];
+    float val[Q][W], rr[Q], di[Q];
+#pragma unroll
+    for (uint32_t q = 0; q < Q; ++q)
+    {
+        const uint32_t t = threadIdx.x + NT * q;
+        const bool in = t < R;
+        const uint32_t i = elo + (in ? t : 0u);
+#pragma unroll
+        for (int e = 0; e < W; ++e)
+        {
+            off[q][e] = in ? (uint32_t)__ldg(&eoff[(size_t)e * n + i]) : 0u;
+            val[q][e] = in ? __ldg(&eval[(size_t)e * n + i]) : 0.f;
+        }
+        rr[q] = in ? (float)rhs[i] : 0.f;
+        di[q] = in ? __ldg(&dinv[i]) : 0.f;
+        if (in) y0[t] = rr[q] * di[q];
+    }
+    __syncthreads();
+
+    // ---- k sweeps; at sweep s the rows [s B, R) (lower) / [0, R - s B) (upper) are exact
+    for (int s = 1; s <= k; ++s)
+    {
+        const uint32_t shrink = cut ? (uint32_t)s * B : 0u;
+        const uint32_t t0 = LOWER ? shrink : 0u;
+        const uint32_t t1 = LOWER ? R : (R > shrink ? R - shrink : 0u);
+        const float* yin = (s & 1) ? y0 : y1;
+        float* yout = (s & 1) ? y1 : y0;
+#pragma unroll
+        for (uint32_t q = 0; q < Q; ++q)
+        {
+            const uint32_t t = threadIdx.x + NT * q;
+            if (t >= t0 && t < t1)
+            {
+                float sum = rr[q];
+#pragma unroll
+                for (int e = 0; e < W; ++e)
+                    if (off[q][e]) sum -= val[q][e] * yin[LOWER ? t - off[q][e] : t + off[q][e]];
+                yout[t] = sum * di[q];
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- rows [lo, hi) of y_k
+    const float* yk = (k & 1) ? y1 : y0;
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += NT)
+    {
+        const float r = yk[i - elo];
+        x[i] = r;
+        if (out64) out64[i] = (double)r;
+    }
+}
+
+}  // namespace b2s

@@ -125,3 +125,116 @@ def test_grf_ic0_pcg_parity(b2s, ctx, orc):
     assert abs(st["it"] - io) <= 2
     # ill-conditioned (k spans several decades): solutions agree to 1e-7
     assert rel(x, xo) < 1e-7
+
+
+@pytest.mark.parametrize("kind", ["ic0", "ilu0"])
+def test_jacobi_sweeps_exact_beyond_depth(b2s, ctx, kind):
+    """B2S_TRSV_JACOBI is a truncated Neumann series of a nilpotent iteration:
+    after as many sweeps as the triangle's DAG depth (23 levels on 12x12) it
+    reproduces the exact FP64 solve bit for bit (same per-row order)."""
+    n, rp, ci, v = P.poisson2d(12) if kind == "ic0" else P.convdiff2d(12)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    k = b2s.PC_NAMES[kind]
+    r = b2s.uniform(41, n)
+    z = b2s.Precond(ctx, A, k).apply(r)
+    zj = b2s.Precond(ctx, A, k, trsv=b2s.TRSV_JACOBI, trsv_sweeps=24).apply(r)
+    assert np.array_equal(zj, z)
+    # fewer sweeps: an approximation, not the solve
+    z2 = b2s.Precond(ctx, A, k, trsv=b2s.TRSV_JACOBI, trsv_sweeps=2).apply(r)
+    assert not np.array_equal(z2, z)
+
+
+def _sweeps_f32(rp, ci, vals, d, r, k, lower):
+    """k Jacobi sweeps in float32, each row in column order with one rounding
+    per product and difference, then a product with the float32 reciprocal
+    1/d -- the kernels' arithmetic."""
+    n = len(rp) - 1
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    strict = (ci < rows) if lower else (ci > rows)
+    rr, cc, vv = rows[strict], ci[strict].astype(np.int64), vals[strict].astype(np.float32)
+    # ELL slots in column order
+    slot = np.zeros(len(rr), np.int64)
+    for t in range(1, len(rr)):
+        slot[t] = slot[t - 1] + 1 if rr[t] == rr[t - 1] else 0
+    W = int(slot.max()) + 1 if len(rr) else 0
+    d32, r32 = d.astype(np.float32), r.astype(np.float32)
+    dinv = np.float32(1.0) / d32
+    y = r32 * dinv
+    for s in range(1, k + 1):
+        acc = r32.copy()
+        for e in range(W):
+            m = slot == e
+            acc[rr[m]] = acc[rr[m]] - vv[m] * y[cc[m]]
+        y = acc * dinv
+    return y
+
+
+def test_jacobi_band_kernel_bit_exact_f32(b2s, ctx):
+    """FP32 IC(0) with 5 sweeps on a 96x96 grid (bandwidth 96: the one-launch
+    banded kernel) against a float32 emulation of the sweeps, bit for bit."""
+    import scipy.sparse as sp
+    n, rp, ci, v = b2s.gen_grf_diffusion(96, seed=12, corr=0.1)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=5)
+    Lrp, Lci, Lv = M.export("ic0.L")
+    d = sp.csr_matrix((Lv, Lci, Lrp), shape=(n, n)).diagonal()
+    LT = sp.csr_matrix((Lv, Lci, Lrp), shape=(n, n)).T.tocsr()
+    LT.sort_indices()
+    r = b2s.uniform(43, n)
+    y = _sweeps_f32(Lrp, Lci, Lv, d, r, 5, True)
+    z = _sweeps_f32(LT.indptr, LT.indices, LT.data, d, y, 5, False)
+    assert np.array_equal(M.apply(r), z.astype(np.float64))
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_jacobi_sweeps_match_series(b2s, ctx, orc, prec):
+    """k sweeps against the series computed with numpy from the exported
+    IC(0) factor: y = D^-1 r, k times y = D^-1 (r - N y); then the same on
+    L^T.  FP64 to 1e-13, FP32 to 1e-5 (relative)."""
+    import scipy.sparse as sp
+    n, rp, ci, v = b2s.gen_grf_diffusion(40, seed=8)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    fp = b2s.FP32 if prec == "fp32" else b2s.FP64
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=fp, trsv=b2s.TRSV_JACOBI, trsv_sweeps=3)
+    Lrp, Lci, Lv = M.export("ic0.L")
+    L = sp.csr_matrix((Lv, Lci, Lrp), shape=(n, n))
+    d = L.diagonal()
+    N = sp.tril(L, -1).tocsr()
+    r = b2s.uniform(42, n)
+    y = r / d
+    for _ in range(3):
+        y = (r - N @ y) / d
+    z = y / d
+    for _ in range(3):
+        z = (y - N.T @ z) / d
+    tol = 1e-5 if prec == "fp32" else 1e-13
+    assert rel(M.apply(r), z) < tol
+
+
+def test_jacobi_sweeps_pcg(b2s, ctx):
+    """PCG with 8-sweep IC(0) applies (FP32) converges to the FP64-verified
+    tolerance within 15 % of the exact solves' iteration count."""
+    n, rp, ci, v = b2s.gen_grf_diffusion(128, seed=2003, corr=0.05)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(3, n)
+    _, s0 = b2s.solve(ctx, A, b, b2s.PCG, b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32), tol=1e-8, maxit=5000)
+    Mj = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8)
+    _, sj = b2s.solve(ctx, A, b, b2s.PCG, Mj, tol=1e-8, maxit=5000)
+    assert sj["status"] == 0 and sj["relres_true"] < 1e-8
+    assert sj["iterations"] <= 1.15 * s0["iterations"], (sj["iterations"], s0["iterations"])
+
+
+def test_jacobi_mode_checks(b2s, ctx):
+    n, rp, ci, v = P.poisson2d(8)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    with pytest.raises(ValueError) as e:
+        b2s.Precond(ctx, A, b2s.PC_IC0, trsv=7)
+    assert e.value.status == b2s.INVALID_ARG
+    with pytest.raises(ValueError) as e:
+        b2s.Precond(ctx, A, b2s.PC_IC0, trsv=b2s.TRSV_JACOBI, trsv_sweeps=-1)
+    assert e.value.status == b2s.INVALID_ARG
+    nb, brp, bci, bv = b2s.gen_elasticity_q1(3)
+    B = b2s.BAIJ(ctx, 3, nb, nb, brp, bci, bv)
+    with pytest.raises(b2s.B2SError) as e:
+        b2s.Precond(ctx, B, b2s.PC_BILU0, trsv=b2s.TRSV_JACOBI)
+    assert e.value.status == b2s.UNSUPPORTED
