@@ -191,6 +191,7 @@ struct CsrDev
     DBuf<float> v32;            // FP32 copy, created on demand
     DBuf<uint32_t> blk_row;     // staged-SpMV row partition (nblk+1)
     uint32_t nblk = 0;
+    uint32_t max_row = 0;       // longest row (nonzeros); 0 = not known
     DBuf<double> diag;          // diagonal entries (0 where missing)
     std::vector<uint32_t> h_rp, h_ci;  // host copies of the pattern (setup code)
     std::vector<double> h_v;
@@ -225,6 +226,14 @@ struct PcImpl
                              double* v)
     {
         fail(B2S_UNSUPPORTED, "export '" + what + "' not available for this preconditioner");
+    }
+    // PCG fusion: z = M^-1 r, then rz = r.z and the PCG scalar step
+    // (pcg_next) on the device, in the apply's own launches; false (nothing
+    // enqueued) when the preconditioner cannot fuse them
+    virtual bool apply_rz(b2s_ctx*, const double* r, double* z, KState* st, const int* done)
+    {
+        (void)r, (void)z, (void)st, (void)done;
+        return false;
     }
     // one triangle of a factored preconditioner M = L L^T (FP64 storage):
     // out = L^{-1} in (upper = false) or L^{-T} in (upper = true)
@@ -332,11 +341,13 @@ inline void reserve_reduction(b2s_ctx* ctx, unsigned blocks)
 
 // --------------------------------------------------- device-side reductions
 
-// Fixed-order block reduction of NV values (all threads receive the result).
-template <int NV>
+// Fixed-order block reduction of NV values (all threads receive the result);
+// NT = the block's thread count (a multiple of 32, at most 1024).
+template <int NV, int NT = kThreads>
 __device__ __forceinline__ void block_reduce(double (&v)[NV])
 {
-    __shared__ double sred[NV][kThreads / 32];
+    static_assert(NT % 32 == 0 && NT <= 1024, "block size");
+    __shared__ double sred[NV][NT / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < NV; ++k)
@@ -352,7 +363,7 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV])
 #pragma unroll
         for (int k = 0; k < NV; ++k)
         {
-            double a = lane < (kThreads / 32) ? sred[k][lane] : 0.0;
+            double a = lane < (NT / 32) ? sred[k][lane] : 0.0;
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) a += __shfl_down_sync(0xffffffffu, a, off);
             if (lane == 0) sred[k][0] = a;
@@ -368,11 +379,11 @@ __device__ __forceinline__ void block_reduce(double (&v)[NV])
 // in the last block to arrive, where v then holds the grid total (summed over
 // block partials in block order).  Must be called by all threads of every
 // block exactly once per kernel.
-template <int NV>
+template <int NV, int NT = kThreads>
 __device__ __forceinline__ bool grid_reduce_last(double (&v)[NV], double* partial, unsigned int* counter)
 {
     __shared__ bool s_last;
-    block_reduce<NV>(v);
+    block_reduce<NV, NT>(v);
     if (threadIdx.x == 0)
     {
 #pragma unroll
@@ -392,9 +403,35 @@ __device__ __forceinline__ bool grid_reduce_last(double (&v)[NV], double* partia
             a += __ldcg(&partial[(size_t)k * gridDim.x + b]);
         v[k] = a;
     }
-    block_reduce<NV>(v);
+    block_reduce<NV, NT>(v);
     if (threadIdx.x == 0) *counter = 0u;
     return true;
+}
+
+// ------------------------------------------------- PCG scalar steps (device)
+
+__device__ __forceinline__ void finish(KState* st, int status)
+{
+    st->status = status;
+    st->done = 1;
+}
+
+// rz_new = r.z: beta, the iteration counters and the NOT_SPD / maxit stops
+// (array.cpp:3575-3593)
+__device__ __forceinline__ void pcg_next(KState* st, double rz_new)
+{
+    if (rz_new <= 0.0)
+    {
+        st->iters = st->it + 1;
+        finish(st, B2S_NOT_SPD);
+        return;
+    }
+    st->beta = rz_new / st->rz_old;
+    st->rz_old = rz_new;
+    st->it_end = st->it;
+    st->it += 1;
+    st->iters = st->it;
+    if (st->it >= st->maxit) finish(st, B2S_OK);
 }
 
 // ---------------------------------------------------------- host helpers

@@ -92,6 +92,7 @@ b2s_status b2s_csr_create(b2s_ctx* ctx, uint32_t n, uint32_t m, const uint32_t* 
         d.m = m;
         d.nnz = nnz;
         d.h_rp.assign(row_ptr, row_ptr + n + 1);
+        for (uint32_t i = 0; i < n; ++i) d.max_row = std::max(d.max_row, row_ptr[i + 1] - row_ptr[i]);
         d.h_ci.assign(col_idx, col_idx + nnz);
         d.h_v.assign(values, values + nnz);
         d.rp = upload(ctx, row_ptr, (size_t)n + 1);

@@ -33,7 +33,10 @@ struct Operator
     const CsrDev* csr = nullptr;
     const BaijDev* baij = nullptr;
     uint64_t n = 0;
-    unsigned red_blocks(const b2s_ctx* ctx) const { return csr ? csr->nblk : stream_grid(ctx, n); }
+    unsigned red_blocks(const b2s_ctx* ctx) const
+    {
+        return csr ? std::max(csr->nblk, spmv_grid(ctx, *csr)) : stream_grid(ctx, n);
+    }
     void apply(b2s_ctx* ctx, const double* x, double* y, const int* done) const
     {
         if (csr)
@@ -104,11 +107,6 @@ void launch_vec(b2s_ctx* ctx, uint64_t n, const int* done, const Body& body)
     B2S_LAUNCH(ctx, k_vec<Body>, g, kThreads, 0, n, done, body, ctx->partial.p, ctx->counter.p);
 }
 
-__device__ __forceinline__ void finish(KState* st, int status)
-{
-    st->status = status;
-    st->done = 1;
-}
 
 // ----------------------------------------------------------------- common
 
@@ -218,21 +216,7 @@ __device__ __forceinline__ bool pcg_check_converged(KState* st, double rr)
     return false;
 }
 
-__device__ __forceinline__ void pcg_next(KState* st, double rz_new)
-{
-    if (rz_new <= 0.0)
-    {
-        st->iters = st->it + 1;
-        finish(st, B2S_NOT_SPD);
-        return;
-    }
-    st->beta = rz_new / st->rz_old;
-    st->rz_old = rz_new;
-    st->it_end = st->it;
-    st->it += 1;
-    st->iters = st->it;
-    if (st->it >= st->maxit) finish(st, B2S_OK);
-}
+
 
 // x += alpha p; r -= alpha Ap; rr = r.r; FUSE 1: z = r, 2: z = r / d (array.cpp:3559-3578)
 template <int FUSE>
@@ -934,8 +918,12 @@ static void run_pcg(Solve& S, const double* b, double* x, b2s_stats* stats)
             else
             {
                 launch_vec(ctx, n, done, BodyPcgUpdate<0>{x, r, z, p, Ap, nullptr, st});
-                S.pc_apply(r, z);
-                launch_vec(ctx, n, done, BodyRZ{r, z, st});
+                // a preconditioner may fuse r.z and the scalar step into its apply
+                if (!(S.pc && S.pc->apply_rz(ctx, r, z, st, done)))
+                {
+                    S.pc_apply(r, z);
+                    launch_vec(ctx, n, done, BodyRZ{r, z, st});
+                }
             }
             launch_vec(ctx, n, done, BodyPUpdate{p, z, st});
         };

@@ -389,6 +389,7 @@ struct Tri
         if (fp32 && hrp && hci) band = plan_band(n, hrp, hci, lower, sweeps, ctx->sm_count);
         if (band.T)
         {
+            reserve_reduction(ctx, band.ntiles);  // the fused r.z of apply_rz
             band_off.alloc((size_t)band.W * n);
             band_val.alloc((size_t)band.W * n);
             band_dinv.alloc(n);
@@ -403,22 +404,22 @@ struct Tri
         }
     }
 
-    template <bool LOWER, typename RT>
-    void run_band(b2s_ctx* ctx, const RT* rhs, float* x, double* out64, const int* done)
+    template <bool LOWER, typename RT, bool RZ = false>
+    void run_band(b2s_ctx* ctx, const RT* rhs, float* x, double* out64, const int* done, BandRz rz = BandRz())
     {
         if (band.W == 2)
         {
-            auto kern = k_trsv_band<LOWER, 2, RT>;
+            auto kern = k_trsv_band<LOWER, 2, RT, RZ>;
             B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)band.smem));
             B2S_LAUNCH(ctx, kern, band.ntiles, band_threads(2), band.smem, n, band.T, band.B, band.Rmax, sweeps,
-                       band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done);
+                       band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done, rz);
         }
         else
         {
-            auto kern = k_trsv_band<LOWER, 4, RT>;
+            auto kern = k_trsv_band<LOWER, 4, RT, RZ>;
             B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)band.smem));
             B2S_LAUNCH(ctx, kern, band.ntiles, band_threads(4), band.smem, n, band.T, band.B, band.Rmax, sweeps,
-                       band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done);
+                       band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done, rz);
         }
     }
 
@@ -619,6 +620,14 @@ struct PcIC0 final : PcImpl
             fwd.solve<float, float, double>(ctx, mode, L.v32.p, diag32.p, r, y32.p, nullptr, done);
             bwd.solve<float, float, float>(ctx, mode, LT.v32.p, diag32.p, y32.p, z32.p, z, done);
         }
+    }
+
+    bool apply_rz(b2s_ctx* ctx, const double* r, double* z, KState* st, const int* done) override
+    {
+        if (!(fp32 && mode == B2S_TRSV_JACOBI && fwd.band.T && bwd.band.T)) return false;
+        fwd.run_band<true, double>(ctx, r, y32.p, nullptr, done);
+        bwd.run_band<false, float, true>(ctx, y32.p, z32.p, z, done, BandRz{r, st, ctx->partial.p, ctx->counter.p});
+        return true;
     }
 
     void solve_factor(b2s_ctx* ctx, bool upper, const double* in, double* out, const int* done) override

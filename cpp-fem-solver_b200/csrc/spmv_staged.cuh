@@ -208,6 +208,53 @@ __global__ void __launch_bounds__(kThreads, kSpmvWarpCtasPerSm)
     }
 }
 
+// One thread per row, for matrices of short rows whose working set stays in
+// L2 (n <= kSpmvRowMaxN, rows <= kSpmvRowMaxLen): every row's loads are
+// independent and the whole grid is one wave, where the warp kernel above
+// would run a second, mostly idle wave of 32-row groups.  The row is summed
+// from 0 in column order, as in the warp kernel, so both give the same bits.
+constexpr uint32_t kSpmvRowMaxLen = 32;
+constexpr uint32_t kSpmvRowMaxN = 1u << 20;
+
+template <typename Epi>
+__global__ void __launch_bounds__(kThreads) k_spmv_row(uint32_t n, const uint32_t* __restrict__ rp,
+                                                       const uint32_t* __restrict__ ci, const double* __restrict__ v,
+                                                       const double* __restrict__ x, const int* done, Epi epi,
+                                                       double* partial, unsigned int* counter)
+{
+    if (done && *done) return;
+    constexpr int NV = Epi::NV > 0 ? Epi::NV : 1;
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < n)
+    {
+        const uint32_t a = __ldg(&rp[r]), b = __ldg(&rp[r + 1]);
+        double sum = 0.0;
+        for (uint32_t q0 = a; q0 < b; q0 += 8)
+        {
+            double vv[8], xx[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+            {
+                const uint32_t q = q0 + k;
+                vv[k] = q < b ? __ldg(&v[q]) : 0.0;
+                xx[k] = q < b ? __ldg(&x[__ldg(&ci[q])]) : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (q0 + k < b) sum += vv[k] * xx[k];
+        }
+        epi.row(r, sum, acc);
+    }
+    if constexpr (Epi::NV > 0)
+    {
+        if (grid_reduce_last<Epi::NV>(acc, partial, counter))
+            if (threadIdx.x == 0) epi.last(acc);
+    }
+}
+
 inline unsigned spmv_warp_grid(const b2s_ctx* ctx, uint32_t n)
 {
     const uint32_t ngroups = (n + 31u) / 32u;
@@ -216,9 +263,28 @@ inline unsigned spmv_warp_grid(const b2s_ctx* ctx, uint32_t n)
     return ctas < g ? (ctas ? ctas : 1u) : g;
 }
 
+inline bool spmv_by_rows(const CsrDev& A)
+{
+    return A.n && A.max_row && A.max_row <= kSpmvRowMaxLen && A.n <= kSpmvRowMaxN;
+}
+
+// the SpMV's grid (reduction partials to reserve before a graph capture)
+inline unsigned spmv_grid(const b2s_ctx* ctx, const CsrDev& A)
+{
+    return spmv_by_rows(A) ? (A.n + kThreads - 1) / kThreads : spmv_warp_grid(ctx, A.n);
+}
+
 template <typename Epi>
 inline void launch_spmv(b2s_ctx* ctx, const CsrDev& A, const double* x, const int* done, const Epi& epi)
 {
+    if (spmv_by_rows(A))
+    {
+        const unsigned grid = (A.n + kThreads - 1) / kThreads;
+        if (Epi::NV > 0) reserve_reduction(ctx, grid);
+        B2S_LAUNCH(ctx, k_spmv_row<Epi>, grid, kThreads, 0, A.n, A.rp.p, A.ci.p, A.v.p, x, done, epi, ctx->partial.p,
+                   ctx->counter.p);
+        return;
+    }
     const unsigned grid = spmv_warp_grid(ctx, A.n);
     if (Epi::NV > 0) reserve_reduction(ctx, grid);
     B2S_LAUNCH(ctx, k_spmv_warp<Epi>, grid, kThreads, 0, A.n, A.rp.p, A.ci.p, A.v.p, x, done, epi, ctx->partial.p,

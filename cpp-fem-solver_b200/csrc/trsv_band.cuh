@@ -20,6 +20,8 @@
 #include <algorithm>
 #include <cstdint>
 
+#include "b2s_internal.cuh"
+
 namespace b2s {
 
 constexpr uint32_t kBandRowsPerThread = 8;
@@ -110,13 +112,25 @@ __global__ void k_band_pack(uint32_t n, uint32_t W, int lower, int unit, const u
     }
 }
 
-template <bool LOWER, int W, typename RT>
+// PCG fusion (RZ, upper triangle of the apply): the epilogue also reduces
+// r.z over the written rows (FP64, fixed order: per block, then the blocks in
+// order) and the last block applies the PCG scalar step pcg_next.
+struct BandRz
+{
+    const double* r = nullptr;
+    KState* st = nullptr;
+    double* partial = nullptr;
+    unsigned int* counter = nullptr;
+};
+
+template <bool LOWER, int W, typename RT, bool RZ = false>
 __global__ void __launch_bounds__(band_threads(W)) k_trsv_band(uint32_t n, uint32_t T, uint32_t B, uint32_t Rmax,
                                                              int k, const uint16_t* __restrict__ eoff,
                                                              const float* __restrict__ eval,
                                                              const float* __restrict__ dinv,
                                                              const RT* __restrict__ rhs, float* __restrict__ x,
-                                                             double* __restrict__ out64, const int* done)
+                                                             double* __restrict__ out64, const int* done,
+                                                             BandRz rz = BandRz())
 {
     constexpr uint32_t NT = band_threads(W), Q = kBandRowsPerThread;
     if (done && *done) return;
@@ -124,8 +138,7 @@ __global__ void __launch_bounds__(band_threads(W)) k_trsv_band(uint32_t n, uint3
     float* const y0 = reinterpret_cast<float*>(smem);
     float* const y1 = y0 + Rmax;
 
-    const uint32_t lo = blockIdx.x * T;
-    if (lo >= n) return;
+    const uint32_t lo = blockIdx.x * T;  // < n: the grid has ceil(n / T) tiles
     const uint32_t hi = min(n, lo + T);
     const uint32_t halo = (uint32_t)k * B;
     const uint32_t elo = LOWER ? (lo > halo ? lo - halo : 0u) : lo;
@@ -180,11 +193,18 @@ __global__ void __launch_bounds__(band_threads(W)) k_trsv_band(uint32_t n, uint3
 
     // ---- rows [lo, hi) of y_k
     const float* yk = (k & 1) ? y1 : y0;
+    double acc[1] = {0.0};
     for (uint32_t i = lo + threadIdx.x; i < hi; i += NT)
     {
         const float r = yk[i - elo];
         x[i] = r;
         if (out64) out64[i] = (double)r;
+        if (RZ) acc[0] += rz.r[i] * (double)r;
+    }
+    if constexpr (RZ)
+    {
+        if (grid_reduce_last<1, NT>(acc, rz.partial, rz.counter))
+            if (threadIdx.x == 0) pcg_next(rz.st, acc[0]);
     }
 }
 

@@ -30,8 +30,11 @@ def long_row_matrix(n=5000):
     return n, rp, ci, v
 
 
-@pytest.mark.parametrize("case", ["poisson", "random", "longrow", "tiny", "rect"])
+@pytest.mark.parametrize("case", ["poisson", "random", "longrow", "tiny", "rect", "big3d", "rows33"])
 def test_spmv_bit_exact(b2s, ctx, orc, case):
+    # one thread per row below 2^20 rows of <= 32 nonzeros ("poisson", "random",
+    # "rect", "tiny"); the warp kernel above ("big3d": 102^3 rows; "longrow",
+    # "rows33": a row longer than 32)
     if case == "rect":
         n, m = 300, 500
         rng = np.random.default_rng(0)
@@ -41,6 +44,7 @@ def test_spmv_bit_exact(b2s, ctx, orc, case):
         v = dense[dense != 0]
     else:
         n, rp, ci, v = {"poisson": lambda: P.poisson2d(100), "random": lambda: P.random_spd(3000, 0.004, 1),
+                        "big3d": lambda: b2s.gen_poisson3d(102), "rows33": lambda: long_row_matrix(33),
                         "longrow": long_row_matrix, "tiny": lambda: P.coo_to_csr(1, 1, [0], [0], [3.0]) and
                         (1, *P.coo_to_csr(1, 1, [0], [0], [3.0]))}[case]()
         m = n
