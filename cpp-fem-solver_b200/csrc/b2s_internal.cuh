@@ -235,6 +235,16 @@ struct PcImpl
         (void)r, (void)z, (void)st, (void)done;
         return false;
     }
+    // PCG fusion of a whole iteration after the SpMV (given Ap and alpha in
+    // st): x += alpha p, r_new = r_old - alpha Ap with the convergence test,
+    // z = M^-1 r_new, r_new.z and the scalar step
+    virtual bool can_fuse_pcg() const { return false; }
+    virtual void pcg_update_apply(b2s_ctx*, double* x, const double* p, const double* Ap, const double* r_old,
+                                  double* r_new, double* z, KState* st, const int* done)
+    {
+        (void)x, (void)p, (void)Ap, (void)r_old, (void)r_new, (void)z, (void)st, (void)done;
+        fail(B2S_UNSUPPORTED, "this preconditioner does not fuse the PCG update");
+    }
     // one triangle of a factored preconditioner M = L L^T (FP64 storage):
     // out = L^{-1} in (upper = false) or L^{-T} in (upper = true)
     virtual void solve_factor(b2s_ctx*, bool upper, const double* in, double* out, const int* done)
@@ -414,6 +424,30 @@ __device__ __forceinline__ void finish(KState* st, int status)
 {
     st->status = status;
     st->done = 1;
+}
+
+// rr = r.r after the update: relative residual, the tolerance and NaN / Inf
+// stops (array.cpp:3560-3573)
+__device__ __forceinline__ bool pcg_check_converged(KState* st, double rr)
+{
+    const double normr = sqrt(rr);
+    st->normr = normr;
+    st->relres = normr / st->normb;
+    if (st->relres < st->tol)
+    {
+        st->it_end = st->it > 0 ? st->it - 1 : 0;
+        st->iters = st->it + 1;
+        finish(st, B2S_OK);
+        return true;
+    }
+    if (!(normr == normr) || isinf(normr))
+    {
+        st->iters = st->it + 1;
+        st->it_end = st->maxit - 1;
+        finish(st, B2S_DIVERGED);
+        return true;
+    }
+    return false;
 }
 
 // rz_new = r.z: beta, the iteration counters and the NOT_SPD / maxit stops

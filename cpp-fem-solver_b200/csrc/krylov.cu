@@ -162,6 +162,16 @@ struct BodyRZInit  // rz_old = r.z (array.cpp:3524-3531)
     }
 };
 
+// p_j = z_j + beta p_old_j formed where the SpMV gathers it (array.cpp:3590-3593)
+struct XPNew
+{
+    const double *z, *p;
+    const KState* st;
+    double beta;
+    __device__ void init() { beta = st->beta; }
+    __device__ double at(uint32_t j) const { return __ldg(&z[j]) + beta * __ldg(&p[j]); }
+};
+
 struct EpiPAp  // Ap = A p; pAp = p.Ap; checks; alpha (array.cpp:3540-3557)
 {
     static constexpr int NV = 1;
@@ -193,28 +203,25 @@ struct EpiPAp  // Ap = A p; pAp = p.Ap; checks; alpha (array.cpp:3540-3557)
     }
 };
 
-// residual check at the end of a PCG iteration; returns true when the solve ended
-__device__ __forceinline__ bool pcg_check_converged(KState* st, double rr)
+// EpiPAp with the direction update folded in: p_new = z + beta p_old (the
+// row's own value, stored), Ap = A p_new, pAp = p_new.Ap
+struct EpiPApUpd
 {
-    const double normr = sqrt(rr);
-    st->normr = normr;
-    st->relres = normr / st->normb;
-    if (st->relres < st->tol)
+    static constexpr int NV = 1;
+    double *Ap, *pnew;
+    const double *z, *pold;
+    KState* st;
+    __device__ void row(uint32_t r, double s, double* acc) const
     {
-        st->it_end = st->it > 0 ? st->it - 1 : 0;
-        st->iters = st->it + 1;
-        finish(st, B2S_OK);
-        return true;
+        const double pr = z[r] + st->beta * pold[r];
+        pnew[r] = pr;
+        Ap[r] = s;
+        acc[0] += pr * s;
     }
-    if (!(normr == normr) || isinf(normr))
-    {
-        st->iters = st->it + 1;
-        st->it_end = st->maxit - 1;
-        finish(st, B2S_DIVERGED);
-        return true;
-    }
-    return false;
-}
+    __device__ void last(const double* t) const { EpiPAp{Ap, pnew, st}.last(t); }
+};
+
+// residual check at the end of a PCG iteration; returns true when the solve ended
 
 
 
@@ -887,8 +894,9 @@ static void run_pcg(Solve& S, const double* b, double* x, b2s_stats* stats)
 {
     b2s_ctx* ctx = S.ctx;
     const uint64_t n = S.A.n;
-    Work W(ctx, 5 * padded(n));
+    Work W(ctx, 7 * padded(n));
     double *r = W.take(n), *z = W.take(n), *p = W.take(n), *Ap = W.take(n);
+    double *r1 = W.take(n), *p1 = W.take(n);  // second residual / direction (fused iteration)
     KState* st = S.st;
     const int* done = S.done;
     S.init_state();
@@ -909,6 +917,29 @@ static void run_pcg(Solve& S, const double* b, double* x, b2s_stats* stats)
         const PcImpl* pc = S.pc;
         const double* dfuse = pc ? pc->fused_diag() : nullptr;
         const int fuse = (!pc || pc->is_identity()) ? 1 : (dfuse ? 2 : 0);
+        if (fuse == 0 && S.A.csr && pc->can_fuse_pcg())
+        {
+            // Three launches per iteration: the SpMV forms p = z + beta p_old
+            // as it gathers and reduces p.Ap; the preconditioner's first
+            // launch forms r = r_old - alpha Ap as it stages, updates x and
+            // tests convergence; its second reduces r.z and steps beta.  The
+            // residual and direction alternate between two buffers, so a
+            // captured batch has an even number of iterations.
+            if (S.poll_every & 1) S.poll_every += 1;
+            int parity = 0;
+            auto body = [&] {
+                double* pold = parity ? p1 : p;
+                double* pnew = parity ? p : p1;
+                const double* rold = parity ? r1 : r;
+                double* rnew = parity ? r : r1;
+                launch_spmv_op(ctx, *S.A.csr, XPNew{z, pold, st, 0.0}, done, EpiPApUpd{Ap, pnew, z, pold, st});
+                S.pc->pcg_update_apply(ctx, x, pnew, Ap, rold, rnew, z, st, done);
+                parity ^= 1;
+            };
+            S.loop(body);
+        }
+        else
+        {
         auto body = [&] {
             op_apply_epi(ctx, S.A, p, Ap, done, EpiPAp{Ap, p, st});
             if (fuse == 1)
@@ -928,6 +959,7 @@ static void run_pcg(Solve& S, const double* b, double* x, b2s_stats* stats)
             launch_vec(ctx, n, done, BodyPUpdate{p, z, st});
         };
         S.loop(body);
+        }
     }
     B2S_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     S.true_residual(b, x, Ap);

@@ -404,22 +404,23 @@ struct Tri
         }
     }
 
-    template <bool LOWER, typename RT, bool RZ = false>
-    void run_band(b2s_ctx* ctx, const RT* rhs, float* x, double* out64, const int* done, BandRz rz = BandRz())
+    template <bool LOWER, typename RT, bool RZ = false, bool UPD = false>
+    void run_band(b2s_ctx* ctx, const RT* rhs, float* x, double* out64, const int* done, BandRz rz = BandRz(),
+                  BandUpd up = BandUpd())
     {
         if (band.W == 2)
         {
-            auto kern = k_trsv_band<LOWER, 2, RT, RZ>;
+            auto kern = k_trsv_band<LOWER, 2, RT, RZ, UPD>;
             B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)band.smem));
             B2S_LAUNCH(ctx, kern, band.ntiles, band_threads(2), band.smem, n, band.T, band.B, band.Rmax, sweeps,
-                       band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done, rz);
+                       band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done, rz, up);
         }
         else
         {
-            auto kern = k_trsv_band<LOWER, 4, RT, RZ>;
+            auto kern = k_trsv_band<LOWER, 4, RT, RZ, UPD>;
             B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)band.smem));
             B2S_LAUNCH(ctx, kern, band.ntiles, band_threads(4), band.smem, n, band.T, band.B, band.Rmax, sweeps,
-                       band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done, rz);
+                       band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done, rz, up);
         }
     }
 
@@ -620,6 +621,17 @@ struct PcIC0 final : PcImpl
             fwd.solve<float, float, double>(ctx, mode, L.v32.p, diag32.p, r, y32.p, nullptr, done);
             bwd.solve<float, float, float>(ctx, mode, LT.v32.p, diag32.p, y32.p, z32.p, z, done);
         }
+    }
+
+    bool can_fuse_pcg() const override { return fp32 && mode == B2S_TRSV_JACOBI && fwd.band.T && bwd.band.T; }
+
+    void pcg_update_apply(b2s_ctx* ctx, double* x, const double* p, const double* Ap, const double* r_old,
+                          double* r_new, double* z, KState* st, const int* done) override
+    {
+        fwd.run_band<true, double, false, true>(
+            ctx, r_old, y32.p, nullptr, done, BandRz(),
+            BandUpd{r_old, Ap, p, x, r_new, st, ctx->partial.p, ctx->counter.p});
+        bwd.run_band<false, float, true>(ctx, y32.p, z32.p, z, done, BandRz{r_new, st, ctx->partial.p, ctx->counter.p});
     }
 
     bool apply_rz(b2s_ctx* ctx, const double* r, double* z, KState* st, const int* done) override

@@ -140,17 +140,27 @@ __device__ __forceinline__ uint32_t ld_stream(const uint32_t* p)
     return v;
 }
 
+// The SpMV's operand x_j.  XDirect reads a vector; other operands (the PCG
+// direction p = z + beta p_old, formed where it is gathered) supply at(j).
+struct XDirect
+{
+    const double* x;
+    __device__ void init() {}
+    __device__ double at(uint32_t j) const { return __ldg(&x[j]); }
+};
+
 constexpr int kSpmvWarpChunk = 256;                       // products per warp per pass
 constexpr int kSpmvWarpPerLane = kSpmvWarpChunk / 32;     // loads per lane per pass
 constexpr int kSpmvWarpCtasPerSm = 6;
 
-template <typename Epi>
+template <typename Epi, typename Xop = XDirect>
 __global__ void __launch_bounds__(kThreads, kSpmvWarpCtasPerSm)
     k_spmv_warp(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
-                const double* __restrict__ v, const double* __restrict__ x, const int* done, Epi epi,
-                double* partial, unsigned int* counter)
+                const double* __restrict__ v, Xop x, const int* done, Epi epi, double* partial,
+                unsigned int* counter)
 {
     if (done && *done) return;
+    x.init();
     __shared__ double prod[kThreads / 32][kSpmvWarpChunk];
     constexpr int NV = Epi::NV > 0 ? Epi::NV : 1;
     double acc[NV];
@@ -191,7 +201,7 @@ __global__ void __launch_bounds__(kThreads, kSpmvWarpCtasPerSm)
             for (int k = 0; k < kSpmvWarpPerLane; ++k)
             {
                 const uint32_t q = base + k * 32 + lane;
-                if (q < p1) P[k * 32 + lane] = vv[k] * __ldg(&x[cc[k]]);
+                if (q < p1) P[k * 32 + lane] = vv[k] * x.at(cc[k]);
             }
             __syncwarp();
             const uint32_t lo = a > base ? a : base;
@@ -216,13 +226,14 @@ __global__ void __launch_bounds__(kThreads, kSpmvWarpCtasPerSm)
 constexpr uint32_t kSpmvRowMaxLen = 32;
 constexpr uint32_t kSpmvRowMaxN = 1u << 20;
 
-template <typename Epi>
+template <typename Epi, typename Xop = XDirect>
 __global__ void __launch_bounds__(kThreads) k_spmv_row(uint32_t n, const uint32_t* __restrict__ rp,
                                                        const uint32_t* __restrict__ ci, const double* __restrict__ v,
-                                                       const double* __restrict__ x, const int* done, Epi epi,
-                                                       double* partial, unsigned int* counter)
+                                                       Xop x, const int* done, Epi epi, double* partial,
+                                                       unsigned int* counter)
 {
     if (done && *done) return;
+    x.init();
     constexpr int NV = Epi::NV > 0 ? Epi::NV : 1;
     double acc[NV];
 #pragma unroll
@@ -240,7 +251,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_row(uint32_t n, const uint32_
             {
                 const uint32_t q = q0 + k;
                 vv[k] = q < b ? __ldg(&v[q]) : 0.0;
-                xx[k] = q < b ? __ldg(&x[__ldg(&ci[q])]) : 0.0;
+                xx[k] = q < b ? x.at(__ldg(&ci[q])) : 0.0;
             }
 #pragma unroll
             for (int k = 0; k < 8; ++k)
@@ -274,21 +285,27 @@ inline unsigned spmv_grid(const b2s_ctx* ctx, const CsrDev& A)
     return spmv_by_rows(A) ? (A.n + kThreads - 1) / kThreads : spmv_warp_grid(ctx, A.n);
 }
 
-template <typename Epi>
-inline void launch_spmv(b2s_ctx* ctx, const CsrDev& A, const double* x, const int* done, const Epi& epi)
+template <typename Epi, typename Xop>
+inline void launch_spmv_op(b2s_ctx* ctx, const CsrDev& A, const Xop& x, const int* done, const Epi& epi)
 {
     if (spmv_by_rows(A))
     {
         const unsigned grid = (A.n + kThreads - 1) / kThreads;
         if (Epi::NV > 0) reserve_reduction(ctx, grid);
-        B2S_LAUNCH(ctx, k_spmv_row<Epi>, grid, kThreads, 0, A.n, A.rp.p, A.ci.p, A.v.p, x, done, epi, ctx->partial.p,
-                   ctx->counter.p);
+        B2S_LAUNCH(ctx, (k_spmv_row<Epi, Xop>), grid, kThreads, 0, A.n, A.rp.p, A.ci.p, A.v.p, x, done, epi,
+                   ctx->partial.p, ctx->counter.p);
         return;
     }
     const unsigned grid = spmv_warp_grid(ctx, A.n);
     if (Epi::NV > 0) reserve_reduction(ctx, grid);
-    B2S_LAUNCH(ctx, k_spmv_warp<Epi>, grid, kThreads, 0, A.n, A.rp.p, A.ci.p, A.v.p, x, done, epi, ctx->partial.p,
-               ctx->counter.p);
+    B2S_LAUNCH(ctx, (k_spmv_warp<Epi, Xop>), grid, kThreads, 0, A.n, A.rp.p, A.ci.p, A.v.p, x, done, epi,
+               ctx->partial.p, ctx->counter.p);
+}
+
+template <typename Epi>
+inline void launch_spmv(b2s_ctx* ctx, const CsrDev& A, const double* x, const int* done, const Epi& epi)
+{
+    launch_spmv_op(ctx, A, XDirect{x}, done, epi);
 }
 
 }  // namespace b2s

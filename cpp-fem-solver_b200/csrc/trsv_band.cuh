@@ -123,17 +123,37 @@ struct BandRz
     unsigned int* counter = nullptr;
 };
 
-template <bool LOWER, int W, typename RT, bool RZ = false>
+// PCG fusion (UPD, lower triangle of the apply): the right-hand side is the
+// updated residual r_old - alpha Ap, formed for every row of the extended
+// range; the owned rows also store it (r_new) and update the iterate
+// (xk += alpha p), and r_new.r_new is reduced for the convergence test
+// pcg_check_converged (array.cpp:3559-3573).
+struct BandUpd
+{
+    const double* r_old = nullptr;
+    const double* Ap = nullptr;
+    const double* p = nullptr;
+    double* xk = nullptr;
+    double* r_new = nullptr;
+    KState* st = nullptr;
+    double* partial = nullptr;
+    unsigned int* counter = nullptr;
+};
+
+template <bool LOWER, int W, typename RT, bool RZ = false, bool UPD = false>
 __global__ void __launch_bounds__(band_threads(W)) k_trsv_band(uint32_t n, uint32_t T, uint32_t B, uint32_t Rmax,
                                                              int k, const uint16_t* __restrict__ eoff,
                                                              const float* __restrict__ eval,
                                                              const float* __restrict__ dinv,
                                                              const RT* __restrict__ rhs, float* __restrict__ x,
                                                              double* __restrict__ out64, const int* done,
-                                                             BandRz rz = BandRz())
+                                                             BandRz rz = BandRz(), BandUpd up = BandUpd())
 {
+    static_assert(!(RZ && UPD), "one fused reduction per launch");
     constexpr uint32_t NT = band_threads(W), Q = kBandRowsPerThread;
     if (done && *done) return;
+    double alpha = 0.0;
+    if constexpr (UPD) alpha = up.st->alpha;
     extern __shared__ __align__(16) unsigned char smem[];
     float* const y0 = reinterpret_cast<float*>(smem);
     float* const y1 = y0 + Rmax;
@@ -161,7 +181,10 @@ __global__ void __launch_bounds__(band_threads(W)) k_trsv_band(uint32_t n, uint3
             off[q][e] = in ? (uint32_t)__ldg(&eoff[(size_t)e * n + i]) : 0u;
             val[q][e] = in ? __ldg(&eval[(size_t)e * n + i]) : 0.f;
         }
-        rr[q] = in ? (float)rhs[i] : 0.f;
+        if constexpr (UPD)
+            rr[q] = in ? (float)(up.r_old[i] - alpha * up.Ap[i]) : 0.f;
+        else
+            rr[q] = in ? (float)rhs[i] : 0.f;
         di[q] = in ? __ldg(&dinv[i]) : 0.f;
         if (in) y0[t] = rr[q] * di[q];
     }
@@ -200,11 +223,23 @@ __global__ void __launch_bounds__(band_threads(W)) k_trsv_band(uint32_t n, uint3
         x[i] = r;
         if (out64) out64[i] = (double)r;
         if (RZ) acc[0] += rz.r[i] * (double)r;
+        if constexpr (UPD)
+        {
+            up.xk[i] += alpha * up.p[i];
+            const double ri = up.r_old[i] - alpha * up.Ap[i];
+            up.r_new[i] = ri;
+            acc[0] += ri * ri;
+        }
     }
     if constexpr (RZ)
     {
         if (grid_reduce_last<1, NT>(acc, rz.partial, rz.counter))
             if (threadIdx.x == 0) pcg_next(rz.st, acc[0]);
+    }
+    if constexpr (UPD)
+    {
+        if (grid_reduce_last<1, NT>(acc, up.partial, up.counter))
+            if (threadIdx.x == 0) pcg_check_converged(up.st, acc[0]);
     }
 }
 

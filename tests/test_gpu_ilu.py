@@ -238,3 +238,68 @@ def test_jacobi_mode_checks(b2s, ctx):
     with pytest.raises(b2s.B2SError) as e:
         b2s.Precond(ctx, B, b2s.PC_BILU0, trsv=b2s.TRSV_JACOBI)
     assert e.value.status == b2s.UNSUPPORTED
+
+
+def test_fused_pcg_iteration_graph_and_polling_invariant(b2s, ctx):
+    """The banded sweep preconditioner runs PCG as three fused launches per
+    iteration with the residual and direction in alternating buffers.  The
+    result must not depend on how the iterations are batched: CUDA graphs on
+    or off, and any polling interval (an odd one is rounded up to keep the
+    buffer roles), give the same iterate bit for bit."""
+    n, rp, ci, v = b2s.gen_grf_diffusion(128, seed=2005, corr=0.05)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(5, n)
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8)
+    runs = [b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=5000, use_graphs=g, check_every=c)
+            for g, c in ((1, 0), (0, 0), (1, 3), (0, 5))]
+    x0, s0 = runs[0]
+    assert s0["status"] == 0 and s0["relres_true"] < 1e-8
+    for x, s in runs[1:]:
+        assert np.array_equal(x, x0) and s["iterations"] == s0["iterations"]
+
+
+def test_fused_pcg_matches_host_pcg(b2s, ctx):
+    """Fused PCG with the 8-sweep FP32 IC(0) against a float64 host PCG with
+    the same (float64) sweep preconditioner: iteration counts within 3, and
+    both iterates meet the tolerance."""
+    import scipy.sparse as sp
+    n, rp, ci, v = b2s.gen_grf_diffusion(64, seed=2006, corr=0.1)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(6, n)
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8)
+    x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=5000)
+    Lrp, Lci, Lv = M.export("ic0.L")
+    L = sp.csr_matrix((Lv, Lci, Lrp), shape=(n, n))
+    d = L.diagonal()
+    N = sp.tril(L, -1).tocsr()
+    Ah = sp.csr_matrix((v, ci, rp), shape=(n, n))
+
+    def pc(r):
+        y = r / d
+        for _ in range(8):
+            y = (r - N @ y) / d
+        z = y / d
+        for _ in range(8):
+            z = (y - N.T @ z) / d
+        return z
+
+    xh = np.zeros(n)
+    r = b.copy()
+    z = pc(r)
+    p = z.copy()
+    rz = r @ z
+    it = 0
+    while np.linalg.norm(r) >= 1e-8 * np.linalg.norm(b) and it < 5000:
+        Ap = Ah @ p
+        a = rz / (p @ Ap)
+        xh += a * p
+        r -= a * Ap
+        it += 1
+        if np.linalg.norm(r) < 1e-8 * np.linalg.norm(b):
+            break
+        z = pc(r)
+        rz2 = r @ z
+        p = z + (rz2 / rz) * p
+        rz = rz2
+    assert st["relres_true"] < 1e-8
+    assert abs(st["iterations"] - it) <= 3, (st["iterations"], it)
