@@ -124,12 +124,13 @@ static void check_err(b2s_ctx* ctx, DBuf<unsigned long long>& err, const char* w
 // ------------------------------------------------------------ factorisation
 
 // IC(0) row, array.cpp:2577-2655
-__global__ void k_ic0_level(const uint32_t* __restrict__ rows, uint32_t count, const uint32_t* __restrict__ Lrp,
-                            const uint32_t* __restrict__ Lci, double* Lv, double* diag, unsigned long long* err)
+// IC(0) of row i in place (array.cpp:2560-2660): l_ij = (a_ij - sum_k l_ik l_jk) / l_jj
+// for the strict entries in column order, then l_ii = sqrt(a_ii - sum_k l_ik^2);
+// rows j < i must be final.  A missing diagonal or a pivot <= 1e-14 records
+// (i << 8 | status) in *err (the smallest row wins) and leaves diag[i] = 1.
+__device__ __forceinline__ void ic0_row(uint32_t i, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lci,
+                                        double* Lv, double* diag, unsigned long long* err)
 {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    const uint32_t i = rows[t];
     const uint32_t rs = Lrp[i], re = Lrp[i + 1];
     for (uint32_t p = rs; p < re; ++p)
     {
@@ -178,6 +179,36 @@ __global__ void k_ic0_level(const uint32_t* __restrict__ rows, uint32_t count, c
     }
     Lv[dp] = sqrt(dv);
     diag[i] = Lv[dp];
+}
+
+__global__ void k_ic0_level(const uint32_t* __restrict__ rows, uint32_t count, const uint32_t* __restrict__ Lrp,
+                            const uint32_t* __restrict__ Lci, double* Lv, double* diag, unsigned long long* err)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    ic0_row(rows[t], Lrp, Lci, Lv, diag, err);
+}
+
+// The whole factorisation in one CTA when every level is narrow: the CTA
+// walks the levels in order, its threads take a level's rows, and a
+// __syncthreads separates the levels (the block barrier orders the global
+// writes of one level before the reads of the next).  No launch per level
+// and no cross-CTA waits.
+constexpr uint32_t kIc0OneCtaThreads = 1024;
+constexpr uint32_t kIc0OneCtaMaxWidth = 4 * kIc0OneCtaThreads;
+
+__global__ void __launch_bounds__(kIc0OneCtaThreads) k_ic0_one_cta(const uint32_t* __restrict__ rows,
+                                                                  const uint32_t* __restrict__ lptr, uint32_t nlev,
+                                                                  const uint32_t* __restrict__ Lrp,
+                                                                  const uint32_t* __restrict__ Lci, double* Lv,
+                                                                  double* diag, unsigned long long* err)
+{
+    for (uint32_t l = 0; l < nlev; ++l)
+    {
+        const uint32_t a = lptr[l], b = lptr[l + 1];
+        for (uint32_t t = a + threadIdx.x; t < b; t += blockDim.x) ic0_row(rows[t], Lrp, Lci, Lv, diag, err);
+        __syncthreads();
+    }
 }
 
 // ILU(0) row, array.cpp:2840-2898 (IKJ; fill-in dropped)
@@ -382,11 +413,11 @@ struct Tri
     DBuf<uint16_t> band_off;        // packed strict entries and reciprocals (k_band_pack)
     DBuf<float> band_val, band_dinv;
 
-    // hrp / hci: the triangle's pattern on the host (for the band plan)
-    void prepare_sweeps(b2s_ctx* ctx, int k, bool fp32, const uint32_t* hrp, const uint32_t* hci)
+    // plan: the triangle's band plan (plan_band), usable for FP32 factors
+    void prepare_sweeps(b2s_ctx* ctx, int k, bool fp32, const BandPlan* plan)
     {
         sweeps = k > 0 ? k : 8;
-        if (fp32 && hrp && hci) band = plan_band(n, hrp, hci, lower, sweeps, ctx->sm_count);
+        if (fp32 && plan) band = *plan;
         if (band.T)
         {
             reserve_reduction(ctx, band.ntiles);  // the fused r.z of apply_rz
@@ -531,6 +562,7 @@ struct HostAnalysis
     std::vector<uint32_t> up_rp, up_ci;  // upper pattern when it is derived on the host
     std::vector<uint32_t> up_level;
     ChunkPlan lo_plan, up_plan;
+    BandPlan lo_band, up_band;
     bool chunked = false;
     std::exception_ptr error;
     std::thread th;
@@ -675,12 +707,24 @@ struct PcIC0 final : PcImpl
 
 // factor IC(0) on the pattern of tril(A) with values Lv (already placed);
 // shared with the learned preconditioner, which factors corrected values.
+// Narrow levels (at most kIc0OneCtaMaxWidth rows each): one CTA walks them
+// all; otherwise one launch per level.  Every row is computed by ic0_row in
+// level order either way, so the factor is the same bits.
 void ic0_factor_inplace(b2s_ctx* ctx, const LevelSchedule& s, const uint32_t* Lrp, const uint32_t* Lci, double* Lv,
                         double* diag, const char* what)
 {
     DBuf<unsigned long long> err(1);
     const unsigned long long none = ~0ull;
     h2d(ctx, err.p, &none, sizeof(none));
+    uint32_t width = 0;
+    for (uint32_t l = 0; l < s.nlev; ++l) width = std::max(width, s.h_ptr[l + 1] - s.h_ptr[l]);
+    if (s.nlev && width <= kIc0OneCtaMaxWidth)
+    {
+        auto lptr = upload(ctx, s.h_ptr);
+        B2S_LAUNCH(ctx, k_ic0_one_cta, 1, kIc0OneCtaThreads, 0, s.rows.p, lptr.p, s.nlev, Lrp, Lci, Lv, diag, err.p);
+        check_err(ctx, err, what);  // synchronises before lptr is released
+        return;
+    }
     for (uint32_t l = 0; l < s.nlev; ++l)
     {
         const uint32_t a = s.h_ptr[l], cnt = s.h_ptr[l + 1] - a;
@@ -705,18 +749,35 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     split(ctx, A, 0, pc->L, nullptr, err.p);
     check_err(ctx, err, "IC(0) failed");
     pc->diag.alloc(n ? n : 1);
-    // host analysis of L: levels (for the factorisation) here, the rest on a thread
+    // Host analysis of L.  The exact schedules need the levels of both
+    // triangles (and the chunk plans); the sweep schedule needs only the band
+    // plans.  What the factorisation does not need runs on a host thread
+    // while the device factorises.
+    const bool sweeps = pc->mode == B2S_TRSV_JACOBI;
+    const int nsweeps = o.trsv_sweeps > 0 ? o.trsv_sweeps : 8;
     std::vector<uint32_t> hrp, hci;
     copy_pattern(ctx, pc->L, hrp, hci);
     pc->fwd.init(pc->L, true, false);
+    // the levels of L order the factorisation (a warp's rows are independent)
     compute_levels(n, hrp.data(), hci.data(), true, pc->fwd.h_level);
     pc->fwd.ensure_sched(ctx);
     HostAnalysis ha;
     ha.chunked = pc->mode == B2S_TRSV_CHUNK && n;
-    ha.th = std::thread([&ha, &hrp, &hci, &pc, n, vs] {
+    const int sm_count = ctx->sm_count;
+    const bool fp32 = pc->fp32;
+    ha.th = std::thread([&ha, &hrp, &hci, &pc, n, vs, sweeps, nsweeps, sm_count, fp32] {
         try
         {
             strict_transpose(n, hrp.data(), hci.data(), true, ha.up_rp, ha.up_ci);
+            if (sweeps)
+            {
+                if (fp32)
+                {
+                    ha.lo_band = plan_band(n, hrp.data(), hci.data(), true, nsweeps, sm_count);
+                    ha.up_band = plan_band(n, ha.up_rp.data(), ha.up_ci.data(), false, nsweeps, sm_count);
+                }
+                return;
+            }
             compute_levels(n, ha.up_rp.data(), ha.up_ci.data(), false, ha.up_level);
             if (ha.chunked)
             {
@@ -749,10 +810,10 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     pc->bwd.h_level = std::move(ha.up_level);
     pc->fwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.lo_plan : nullptr, vs);
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
-    if (pc->mode == B2S_TRSV_JACOBI)
+    if (sweeps)
     {
-        pc->fwd.prepare_sweeps(ctx, o.trsv_sweeps, pc->fp32, hrp.data(), hci.data());
-        pc->bwd.prepare_sweeps(ctx, o.trsv_sweeps, pc->fp32, ha.up_rp.data(), ha.up_ci.data());
+        pc->fwd.prepare_sweeps(ctx, nsweeps, pc->fp32, &ha.lo_band);
+        pc->bwd.prepare_sweeps(ctx, nsweeps, pc->fp32, &ha.up_band);
     }
     if (pc->fp32)
     {
@@ -889,8 +950,15 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
     if (pc->mode == B2S_TRSV_JACOBI)
     {
-        pc->fwd.prepare_sweeps(ctx, o.trsv_sweeps, pc->fp32, lrp.data(), lci.data());
-        pc->bwd.prepare_sweeps(ctx, o.trsv_sweeps, pc->fp32, urp.data(), uci.data());
+        const int k = o.trsv_sweeps > 0 ? o.trsv_sweeps : 8;
+        BandPlan lo, up;
+        if (pc->fp32)
+        {
+            lo = plan_band(n, lrp.data(), lci.data(), true, k, ctx->sm_count);
+            up = plan_band(n, urp.data(), uci.data(), false, k, ctx->sm_count);
+        }
+        pc->fwd.prepare_sweeps(ctx, k, pc->fp32, &lo);
+        pc->bwd.prepare_sweeps(ctx, k, pc->fp32, &up);
     }
     if (pc->fp32)
     {
