@@ -323,22 +323,43 @@ __global__ void __launch_bounds__(256) k_aggregate(uint32_t n, const uint32_t* _
     if (i >= n) return;
     float a0 = 0.f, a1 = 0.f;
     const int c0 = lane, c1 = lane + 32;
-    for (uint32_t p = rp[i]; p < rp[i + 1]; ++p)
+    // neighbours eight at a time: their indices, edge features and messages
+    // are all in flight before the gates are formed (same summation order)
+    const uint32_t pa = rp[i], pe = rp[i + 1];
+    for (uint32_t pb = pa; pb < pe; pb += 8)
     {
-        const uint32_t j = ci[p];
-        if (j == i) continue;
-        const float* e = EF + (size_t)p * FE;
-        const float e0 = e[0], e1 = e[1], e2 = e[2], e3 = e[3];
-        const float g0 = sigm(bg[c0] + wg[c0][0] * e0 + wg[c0][1] * e1 + wg[c0][2] * e2 + wg[c0][3] * e3);
-        const float g1 = sigm(bg[c1] + wg[c1][0] * e0 + wg[c1][1] * e1 + wg[c1][2] * e2 + wg[c1][3] * e3);
-        a0 += g0 * SM[(size_t)j * 2 * H + H + c0];
-        a1 += g1 * SM[(size_t)j * 2 * H + H + c1];
+        uint32_t jj[8];
+        float4 ee[8];
+        float m0[8], m1[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) jj[k] = pb + k < pe ? ci[pb + k] : i;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+        {
+            const bool on = jj[k] != i;
+            ee[k] = on ? *reinterpret_cast<const float4*>(EF + (size_t)(pb + k) * FE) : make_float4(0.f, 0.f, 0.f, 0.f);
+            m0[k] = on ? SM[(size_t)jj[k] * 2 * H + H + c0] : 0.f;
+            m1[k] = on ? SM[(size_t)jj[k] * 2 * H + H + c1] : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+        {
+            if (jj[k] == i) continue;
+            const float4 e = ee[k];
+            const float g0 = sigm(bg[c0] + wg[c0][0] * e.x + wg[c0][1] * e.y + wg[c0][2] * e.z + wg[c0][3] * e.w);
+            const float g1 = sigm(bg[c1] + wg[c1][0] * e.x + wg[c1][1] * e.y + wg[c1][2] * e.z + wg[c1][3] * e.w);
+            a0 += g0 * m0[k];
+            a1 += g1 * m1[k];
+        }
     }
     const float id = invdeg[i];
     const float p0 = SM[(size_t)i * 2 * H + c0] + bl[c0] + id * a0;
     const float p1 = SM[(size_t)i * 2 * H + c1] + bl[c1] + id * a1;
-    pre[(size_t)i * H + c0] = p0;
-    pre[(size_t)i * H + c1] = p1;
+    if (pre)  // kept for the backward pass (training only)
+    {
+        pre[(size_t)i * H + c0] = p0;
+        pre[(size_t)i * H + c1] = p1;
+    }
     Hout[(size_t)i * H + c0] = fmaxf(p0, 0.f) + Hin[(size_t)i * H + c0];
     Hout[(size_t)i * H + c1] = fmaxf(p1, 0.f) + Hin[(size_t)i * H + c1];
 }
@@ -428,27 +449,72 @@ __device__ __forceinline__ float head_edge(const float* P, const float* hi, cons
 
 // Lv <- L0 * exp(s tanh c) on the pattern of L (rows with diagonal last).  The
 // head uses FP32 parameters (Pf) rounded to BF16 by the caller.  C receives c.
+// Per-node projections of the head: proj[3i..3i+2] = (u.h_i, v.h_i, d.h_i).
+// Half a warp per node, four features per lane, a fixed shuffle tree: the
+// sums do not depend on the launch.
+__global__ void k_head_proj(uint32_t n, const float* __restrict__ Hf, const float* __restrict__ Pf,
+                            float* __restrict__ proj)
+{
+    const uint32_t lane = threadIdx.x & 15u;
+    // u and v start on 16-byte boundaries; d (at O_D = 133) does not
+    static_assert(((OFF_OUT + O_U) % 4) == 0 && ((OFF_OUT + O_V) % 4) == 0, "u, v alignment");
+    const float4 u = *reinterpret_cast<const float4*>(Pf + OFF_OUT + O_U + 4 * lane);
+    const float4 v = *reinterpret_cast<const float4*>(Pf + OFF_OUT + O_V + 4 * lane);
+    const float* dp = Pf + OFF_OUT + O_D + 4 * lane;
+    const float4 dd = make_float4(dp[0], dp[1], dp[2], dp[3]);
+    const uint32_t stride = (gridDim.x * blockDim.x) >> 4;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 4; i < n; i += stride)
+    {
+        const float4 h = *reinterpret_cast<const float4*>(Hf + (size_t)i * H + 4 * lane);
+        float a = u.x * h.x + u.y * h.y + u.z * h.z + u.w * h.w;
+        float b = v.x * h.x + v.y * h.y + v.z * h.z + v.w * h.w;
+        float c = dd.x * h.x + dd.y * h.y + dd.z * h.z + dd.w * h.w;
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1)
+        {
+            // the two half-warps may run different trip counts: each shuffles alone
+            const unsigned half = 0xFFFFu << (threadIdx.x & 16u);
+            a += __shfl_xor_sync(half, a, o, 16);
+            b += __shfl_xor_sync(half, b, o, 16);
+            c += __shfl_xor_sync(half, c, o, 16);
+        }
+        if (lane == 0)
+        {
+            proj[3 * (size_t)i] = a;
+            proj[3 * (size_t)i + 1] = b;
+            proj[3 * (size_t)i + 2] = c;
+        }
+    }
+}
+
+// c_ij = b_o + u.h_i + v.h_j + w.e_ij (j < i),  c_ii = b_d + d.h_i, from the
+// node projections; Lv <- L0 * exp(s tanh c) on the pattern of L (rows with
+// diagonal last).  The head uses FP32 parameters (Pf) rounded to BF16 by the
+// caller.  C receives c.
 __global__ void k_head(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lci,
                        const uint32_t* __restrict__ Arp, const double* __restrict__ Adiag, const float* __restrict__ EF,
-                       const float* __restrict__ Hf, const float* __restrict__ Pf, const double* __restrict__ L0,
+                       const float* __restrict__ proj, const float* __restrict__ Pf, const double* __restrict__ L0,
                        double* __restrict__ Lv, float* __restrict__ C, double* __restrict__ diag_out)
 {
+    const float bo = Pf[OFF_OUT + O_BO], bd = Pf[OFF_OUT + O_BD];
+    float w[FE];
+#pragma unroll
+    for (int k = 0; k < FE; ++k) w[k] = Pf[OFF_OUT + O_W + k];
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
-        const float* hi = Hf + (size_t)i * H;
+        const float ai = proj[3 * (size_t)i], di = proj[3 * (size_t)i + 2];
         for (uint32_t q = Lrp[i]; q < Lrp[i + 1]; ++q)
         {
             const uint32_t j = Lci[q];
             float c;
             if (j == i)
-            {
-                c = Pf[OFF_OUT + O_BD];
-                for (int k = 0; k < H; ++k) c += Pf[OFF_OUT + O_D + k] * hi[k];
-            }
+                c = bd + di;
             else
             {
                 const uint32_t pA = Arp[i] + (q - Lrp[i]);  // L row i is a prefix of A row i
-                c = head_edge(Pf, hi, Hf + (size_t)j * H, EF + (size_t)pA * FE);
+                const float4 e = *reinterpret_cast<const float4*>(EF + (size_t)pA * FE);
+                c = bo + ai + proj[3 * (size_t)j + 1];
+                c += w[0] * e.x + w[1] * e.y + w[2] * e.z + w[3] * e.w;
             }
             C[q] = c;
             double val = L0[q] * exp((double)(kScale * tanhf(c)));
@@ -790,12 +856,21 @@ struct GnnGraph
     uint32_t n = 0, nnz = 0;
     DBuf<uint32_t> rev;
     DBuf<float> F, EF, invdeg;
+    // Activations.  Training keeps every layer's (Hs[0..NL], SM, pre, pre0)
+    // for the backward pass; inference keeps two node-state buffers and one
+    // [s | m] buffer, reused layer after layer.
     DBuf<float> Hs[NL + 1], SM[NL], pre[NL], pre0;
     DBuf<double> logd;
     DBuf<int> err;  // B2S_TIMEOUT from the tensor-core layer's bounded wait
+    bool training = false;
 
-    void build(b2s_ctx* ctx, const CsrDev& A)
+    const float* state(int l) const { return training ? Hs[l].p : Hs[l & 1].p; }
+    float* state_mut(int l) { return training ? Hs[l].p : Hs[l & 1].p; }
+    float* sm(int l) { return training ? SM[l].p : SM[0].p; }
+
+    void build(b2s_ctx* ctx, const CsrDev& A, bool train = false)
     {
+        training = train;
         n = A.n;
         nnz = A.nnz;
         err.alloc(1);
@@ -821,28 +896,48 @@ struct GnnGraph
         sync(ctx);
         B2S_LAUNCH(ctx, k_features, stream_grid(ctx, n), kThreads, 0, n, A.rp.p, A.ci.p, A.v.p, A.diag.p, mean, F.p,
                    EF.p, invdeg.p);
-        for (int l = 0; l <= NL; ++l) Hs[l].alloc((size_t)n * H);
-        for (int l = 0; l < NL; ++l)
+        if (training)
         {
-            SM[l].alloc((size_t)n * 2 * H);
-            pre[l].alloc((size_t)n * H);
+            for (int l = 0; l <= NL; ++l) Hs[l].alloc((size_t)n * H);
+            for (int l = 0; l < NL; ++l)
+            {
+                SM[l].alloc((size_t)n * 2 * H);
+                pre[l].alloc((size_t)n * H);
+            }
+            pre0.alloc((size_t)n * H);
         }
-        pre0.alloc((size_t)n * H);
+        else
+        {
+            Hs[0].alloc((size_t)n * H);
+            Hs[1].alloc((size_t)n * H);
+            SM[0].alloc((size_t)n * 2 * H);
+        }
     }
 
     void forward(b2s_ctx* ctx, const Gnn& net, const CsrDev& A)
     {
         const unsigned g64 = (n + kFwdRows - 1) / kFwdRows, gw = (n + 7) / 8;
-        B2S_LAUNCH(ctx, (k_linear<FIN, H, true>), g64, 256, 0, n, F.p, net.pb.p + OFF_WIN, net.pr.p + OFF_BIN, Hs[0].p,
-                   pre0.p);
+        B2S_LAUNCH(ctx, (k_linear<FIN, H, true>), g64, 256, 0, n, F.p, net.pb.p + OFF_WIN, net.pr.p + OFF_BIN,
+                   state_mut(0), training ? pre0.p : (float*)nullptr);
         for (int l = 0; l < NL; ++l)
         {
             const __nv_bfloat16* Wl = net.pb.p + LAYER0 + l * L_SIZE;
             // [W_s ; W_m] are contiguous: one 128 x 64 weight, on the tensor cores
-            linear_tc<H, 2 * H>(ctx, n, Hs[l].p, Wl + L_WS, nullptr, SM[l].p, err.p);
-            B2S_LAUNCH(ctx, k_aggregate, gw, 256, 0, n, A.rp.p, A.ci.p, EF.p, invdeg.p, SM[l].p, Wl, Hs[l].p,
-                       pre[l].p, Hs[l + 1].p);
+            linear_tc<H, 2 * H>(ctx, n, state(l), Wl + L_WS, nullptr, sm(l), err.p);
+            B2S_LAUNCH(ctx, k_aggregate, gw, 256, 0, n, A.rp.p, A.ci.p, EF.p, invdeg.p, sm(l), Wl, state(l),
+                       training ? pre[l].p : (float*)nullptr, state_mut(l + 1));
         }
+    }
+
+    // the output head on the final node states
+    void head(b2s_ctx* ctx, const Gnn& net, const CsrDev& A, const uint32_t* Lrp, const uint32_t* Lci,
+              const double* L0, double* Lv, float* C, double* diag)
+    {
+        DBuf<float> proj((size_t)3 * n + 1);
+        const unsigned gp = (unsigned)std::min<uint64_t>(((uint64_t)n * 16 + 255) / 256, (uint64_t)ctx->sm_count * 8);
+        B2S_LAUNCH(ctx, k_head_proj, gp ? gp : 1u, 256, 0, n, state(NL), net.pr.p, proj.p);
+        B2S_LAUNCH(ctx, k_head, stream_grid(ctx, n), kThreads, 0, n, Lrp, Lci, A.rp.p, A.diag.p, EF.p, proj.p,
+                   net.pr.p, L0, Lv, C, diag);
     }
 
     // after a synchronisation: fail with B2S_TIMEOUT if a layer's wait gave up
@@ -869,8 +964,7 @@ struct LearnedCorrection final : Ic0Correction
         DBuf<double> L0(Lnnz ? Lnnz : 1);
         d2d(ctx, L0.p, Lv, Lnnz * sizeof(double));
         DBuf<float> C(Lnnz ? Lnnz : 1);
-        B2S_LAUNCH(ctx, k_head, stream_grid(ctx, A.n), kThreads, 0, A.n, Lrp, Lci, A.rp.p, A.diag.p, G.EF.p,
-                   G.Hs[NL].p, net->pr.p, L0.p, Lv, C.p, diag);
+        G.head(ctx, *net, A, Lrp, Lci, L0.p, Lv, C.p, diag);
         G.check(ctx);
     }
 };
@@ -1020,12 +1114,11 @@ static void train_step(b2s_ctx* ctx, Gnn& net, const CsrDev& A, int nprobes, uin
     B2S_LAUNCH(ctx, k_lt_positions, stream_grid(ctx, n), kThreads, 0, n, Trp.p, Tci.p, Lrp.p, Lci.p, Tpos.p);
 
     GnnGraph G;
-    G.build(ctx, A);
+    G.build(ctx, A, true);
     G.forward(ctx, net, A);
     DBuf<double> Lv(Lnnz), dL(Lnnz);
     DBuf<float> C(Lnnz), dC(Lnnz);
-    B2S_LAUNCH(ctx, k_head, stream_grid(ctx, n), kThreads, 0, n, Lrp.p, Lci.p, A.rp.p, A.diag.p, G.EF.p, G.Hs[NL].p,
-               net.pr.p, L0.p, Lv.p, C.p, (double*)nullptr);
+    G.head(ctx, net, A, Lrp.p, Lci.p, L0.p, Lv.p, C.p, (double*)nullptr);
     B2S_CUDA(cudaMemsetAsync(dL.p, 0, dL.bytes(), ctx->stream));
 
     TrainBuffers T;

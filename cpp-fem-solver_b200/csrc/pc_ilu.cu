@@ -357,39 +357,47 @@ __device__ __forceinline__ XT jacobi_scale(XT a, XT d)
         return a / d;
 }
 
-// One Jacobi sweep of a triangle T = D + N (B2S_TRSV_JACOBI):
-//   y_out = D^-1 (rhs - N y_in),  y_in = D^-1 rhs on the first sweep (FIRST),
-// so k sweeps give the k-term truncated Neumann series of T^-1 rhs.  Every row
-// is independent: one thread per row, the row's strict entries in column
-// order, FP32 or FP64 as the factor.
-template <bool LOWER, bool UNIT, bool FIRST, typename VT, typename XT, typename RT>
-__global__ void __launch_bounds__(kThreads) k_trsv_sweep(uint32_t n, const uint32_t* __restrict__ rp,
+// One pass of the sweep schedule (B2S_TRSV_JACOBI) over a triangle T = D + N,
+// one thread per segment of S consecutive rows (global index / S), rows in
+// dependency order inside the segment:
+//   y[i] = D^-1 (rhs_i - sum_{j in segment} N_ij y[j] - sum_{j outside} N_ij yin[j]),
+// the strict entries in column order; pass 0 has no yin (each segment solved
+// on its own), passes 1..k are the sweeps.  S = 1 is plain Jacobi.
+template <bool LOWER, bool UNIT, typename VT, typename XT, typename RT>
+__global__ void __launch_bounds__(kThreads) k_trsv_sweep(uint32_t n, uint32_t S, int pass,
+                                                         const uint32_t* __restrict__ rp,
                                                          const uint32_t* __restrict__ ci, const VT* __restrict__ v,
                                                          const VT* __restrict__ d, const RT* __restrict__ rhs,
-                                                         const XT* __restrict__ yin, XT* __restrict__ yout,
+                                                         const XT* __restrict__ yin, XT* yout,
                                                          double* __restrict__ out64, const int* done)
 {
     if (done && *done) return;
-    for (uint32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x)
+    const uint32_t nseg = (n + S - 1) / S;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < nseg; g += gridDim.x * blockDim.x)
     {
-        XT sum = (XT)rhs[row];
-        const uint32_t a = __ldg(&rp[row]), b = __ldg(&rp[row + 1]);
-        for (uint32_t p = a; p < b; ++p)
+        const uint32_t a = g * S, b = min(n, a + S);
+        for (uint32_t u = 0; u < b - a; ++u)
         {
-            const uint32_t j = __ldg(&ci[p]);
-            if (LOWER ? (j < row) : (j > row))
+            const uint32_t row = LOWER ? a + u : b - 1 - u;
+            XT sum = (XT)rhs[row];
+            const uint32_t p0 = __ldg(&rp[row]), p1 = __ldg(&rp[row + 1]);
+            for (uint32_t p = p0; p < p1; ++p)
             {
+                const uint32_t j = __ldg(&ci[p]);
+                if (!(LOWER ? (j < row) : (j > row))) continue;
                 XT xj;
-                if (FIRST)
-                    xj = UNIT ? (XT)rhs[j] : jacobi_scale<XT>((XT)rhs[j], (XT)__ldg(&d[j]));
-                else
+                if (j >= a && j < b)
+                    xj = yout[j];  // this pass, written above by this thread
+                else if (pass > 0)
                     xj = yin[j];
+                else
+                    continue;
                 sum -= (XT)__ldg(&v[p]) * xj;
             }
+            const XT r = UNIT ? sum : jacobi_scale<XT>(sum, (XT)__ldg(&d[row]));
+            yout[row] = r;
+            if (out64) out64[row] = (double)r;
         }
-        const XT r = UNIT ? sum : jacobi_scale<XT>(sum, (XT)__ldg(&d[row]));
-        yout[row] = r;
-        if (out64) out64[row] = (double)r;
     }
 }
 
@@ -406,7 +414,8 @@ struct Tri
     ChunkSchedule cs;
     bool has_chunks = false, sched_ready = false;
     std::vector<uint32_t> h_level;  // host copy of the rows' levels (compute_levels), when known
-    int sweeps = 8;                 // B2S_TRSV_JACOBI
+    int sweeps = 8;                 // B2S_TRSV_JACOBI: sweeps after pass 0
+    uint32_t segment = 8;           // rows per Gauss-Seidel segment
     DBuf<double> jw64[2];           // sweep ping-pong buffers, made at setup
     DBuf<float> jw32[2];
     BandPlan band;                  // FP32 banded triangles: all sweeps in one launch
@@ -414,9 +423,10 @@ struct Tri
     DBuf<float> band_val, band_dinv;
 
     // plan: the triangle's band plan (plan_band), usable for FP32 factors
-    void prepare_sweeps(b2s_ctx* ctx, int k, bool fp32, const BandPlan* plan)
+    void prepare_sweeps(b2s_ctx* ctx, int k, uint32_t seg, bool fp32, const BandPlan* plan)
     {
-        sweeps = k > 0 ? k : 8;
+        sweeps = k;
+        segment = seg;
         if (fp32 && plan) band = *plan;
         if (band.T)
         {
@@ -441,14 +451,14 @@ struct Tri
     {
         if (band.W == 2)
         {
-            auto kern = k_trsv_band<LOWER, 2, RT, RZ, UPD>;
+            auto kern = segment == 1 ? k_trsv_band<LOWER, 2, 1, RT, RZ, UPD> : k_trsv_band<LOWER, 2, 8, RT, RZ, UPD>;
             B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)band.smem));
             B2S_LAUNCH(ctx, kern, band.ntiles, band_threads(2), band.smem, n, band.T, band.B, band.Rmax, sweeps,
                        band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done, rz, up);
         }
         else
         {
-            auto kern = k_trsv_band<LOWER, 4, RT, RZ, UPD>;
+            auto kern = segment == 1 ? k_trsv_band<LOWER, 4, 1, RT, RZ, UPD> : k_trsv_band<LOWER, 4, 8, RT, RZ, UPD>;
             B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)band.smem));
             B2S_LAUNCH(ctx, kern, band.ntiles, band_threads(4), band.smem, n, band.T, band.B, band.Rmax, sweeps,
                        band_off.p, band_val.p, band_dinv.p, rhs, x, out64, done, rz, up);
@@ -472,18 +482,15 @@ struct Tri
         else
             buf[0] = jw64[0].p, buf[1] = jw64[1].p;
         need(buf[0] && buf[1], B2S_INVALID_ARG, "Jacobi triangular solve: sweep buffers not prepared");
-        const unsigned g = stream_grid(ctx, n);
-        for (int s = 0; s < sweeps; ++s)
+        const unsigned g = stream_grid(ctx, ((uint64_t)n + segment - 1) / segment);
+        for (int s = 0; s <= sweeps; ++s)
         {
-            const bool last = s == sweeps - 1;
+            const bool last = s == sweeps;
             XT* out = last ? x : buf[s & 1];
             double* o64 = last ? out64 : nullptr;
-            if (s == 0)
-                B2S_LAUNCH(ctx, (k_trsv_sweep<LOWER, UNIT, true, VT, XT, RT>), g, kThreads, 0, n, m->rp.p, m->ci.p, v, d,
-                           rhs, (const XT*)nullptr, out, o64, done);
-            else
-                B2S_LAUNCH(ctx, (k_trsv_sweep<LOWER, UNIT, false, VT, XT, RT>), g, kThreads, 0, n, m->rp.p, m->ci.p, v,
-                           d, rhs, buf[(s - 1) & 1], out, o64, done);
+            const XT* in = s ? buf[(s - 1) & 1] : nullptr;
+            B2S_LAUNCH(ctx, (k_trsv_sweep<LOWER, UNIT, VT, XT, RT>), g, kThreads, 0, n, segment, s, m->rp.p, m->ci.p,
+                       v, d, rhs, in, out, o64, done);
         }
     }
 
@@ -598,10 +605,18 @@ static void to_f32(b2s_ctx* ctx, const DBuf<double>& a, DBuf<float>& b, uint64_t
     if (n) B2S_LAUNCH(ctx, k_f64_to_f32, stream_grid(ctx, n), kThreads, 0, a.p, b.p, n);
 }
 
+// B2S_TRSV_JACOBI defaults: 8 sweeps of plain Jacobi (segments of one row).
+// On the 512^2 benchmark systems 8-row Gauss-Seidel segments needed fewer
+// sweeps for the same iterations but cost more per pass (a chain of dependent
+// rows per thread), and were slower end to end.
+static int sweep_count(const b2s_pc_opts& o) { return o.trsv_sweeps > 0 ? o.trsv_sweeps : 8; }
+static uint32_t sweep_segment(const b2s_pc_opts& o) { return o.trsv_segment > 0 ? (uint32_t)o.trsv_segment : 1u; }
+
 static int pick_trsv(const b2s_pc_opts& o)
 {
     need(o.trsv >= B2S_TRSV_AUTO && o.trsv <= B2S_TRSV_JACOBI, B2S_INVALID_ARG, "unknown triangular-solve schedule");
     need(o.trsv_sweeps >= 0 && o.trsv_sweeps <= 1024, B2S_INVALID_ARG, "trsv_sweeps must be 0..1024");
+    need(o.trsv_segment >= 0 && o.trsv_segment <= 32, B2S_INVALID_ARG, "trsv_segment must be 0..32");
     return o.trsv == B2S_TRSV_AUTO ? B2S_TRSV_CHUNK : o.trsv;
 }
 
@@ -754,7 +769,8 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     // plans.  What the factorisation does not need runs on a host thread
     // while the device factorises.
     const bool sweeps = pc->mode == B2S_TRSV_JACOBI;
-    const int nsweeps = o.trsv_sweeps > 0 ? o.trsv_sweeps : 8;
+    const int nsweeps = sweep_count(o);
+    const uint32_t seg = sweep_segment(o);
     std::vector<uint32_t> hrp, hci;
     copy_pattern(ctx, pc->L, hrp, hci);
     pc->fwd.init(pc->L, true, false);
@@ -765,7 +781,7 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     ha.chunked = pc->mode == B2S_TRSV_CHUNK && n;
     const int sm_count = ctx->sm_count;
     const bool fp32 = pc->fp32;
-    ha.th = std::thread([&ha, &hrp, &hci, &pc, n, vs, sweeps, nsweeps, sm_count, fp32] {
+    ha.th = std::thread([&ha, &hrp, &hci, &pc, n, vs, sweeps, nsweeps, seg, sm_count, fp32] {
         try
         {
             strict_transpose(n, hrp.data(), hci.data(), true, ha.up_rp, ha.up_ci);
@@ -773,8 +789,8 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
             {
                 if (fp32)
                 {
-                    ha.lo_band = plan_band(n, hrp.data(), hci.data(), true, nsweeps, sm_count);
-                    ha.up_band = plan_band(n, ha.up_rp.data(), ha.up_ci.data(), false, nsweeps, sm_count);
+                    ha.lo_band = plan_band(n, hrp.data(), hci.data(), true, nsweeps, sm_count, seg);
+                    ha.up_band = plan_band(n, ha.up_rp.data(), ha.up_ci.data(), false, nsweeps, sm_count, seg);
                 }
                 return;
             }
@@ -812,8 +828,8 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
     if (sweeps)
     {
-        pc->fwd.prepare_sweeps(ctx, nsweeps, pc->fp32, &ha.lo_band);
-        pc->bwd.prepare_sweeps(ctx, nsweeps, pc->fp32, &ha.up_band);
+        pc->fwd.prepare_sweeps(ctx, nsweeps, seg, pc->fp32, &ha.lo_band);
+        pc->bwd.prepare_sweeps(ctx, nsweeps, seg, pc->fp32, &ha.up_band);
     }
     if (pc->fp32)
     {
@@ -950,15 +966,16 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
     if (pc->mode == B2S_TRSV_JACOBI)
     {
-        const int k = o.trsv_sweeps > 0 ? o.trsv_sweeps : 8;
+        const int k = sweep_count(o);
+        const uint32_t seg = sweep_segment(o);
         BandPlan lo, up;
         if (pc->fp32)
         {
-            lo = plan_band(n, lrp.data(), lci.data(), true, k, ctx->sm_count);
-            up = plan_band(n, urp.data(), uci.data(), false, k, ctx->sm_count);
+            lo = plan_band(n, lrp.data(), lci.data(), true, k, ctx->sm_count, seg);
+            up = plan_band(n, urp.data(), uci.data(), false, k, ctx->sm_count, seg);
         }
-        pc->fwd.prepare_sweeps(ctx, k, pc->fp32, &lo);
-        pc->bwd.prepare_sweeps(ctx, k, pc->fp32, &up);
+        pc->fwd.prepare_sweeps(ctx, k, seg, pc->fp32, &lo);
+        pc->bwd.prepare_sweeps(ctx, k, seg, pc->fp32, &up);
     }
     if (pc->fp32)
     {

@@ -1,20 +1,31 @@
-// Jacobi-sweep triangular solve of a banded triangle in one launch
-// (B2S_TRSV_JACOBI, FP32 factors whose strict entries lie within B rows of
-// the diagonal -- natural-order 2-D grids, for example).
+// Sweep (B2S_TRSV_JACOBI) triangular solve of a banded triangle in one
+// launch (FP32 factors whose strict entries lie within B rows of the
+// diagonal -- natural-order 2-D grids, for example).
 //
-// k sweeps of  y_s = D^-1 (rhs - N y_{s-1}),  y_0 = D^-1 rhs,  T = D + N
-// (FP32: D^-1 is the packed reciprocal 1/d): row i of y_s depends on rows
-// i-B .. i-1 of y_{s-1} (lower; i+1 .. i+B upper), so the rows [lo, hi) of
-// y_k depend only on rows [lo - kB, hi) of the input.  A CTA loads that
-// extended range once -- each thread keeps its rows' strict entries (u16
-// offsets, FP32 values), right-hand side and reciprocal in registers -- and
-// runs all k sweeps with only the sweep vectors in shared memory, separated
-// by __syncthreads.  At sweep s it computes only the rows whose inputs are
-// still exact (from the range start plus s*B on), so nothing it reads is
-// stale and rows [lo, hi) equal the one-launch-per-sweep schedule bit for
-// bit.  The halo is recomputed by the neighbouring tiles (redundant work
-// instead of communication): no CTA waits on another.  The strict entries
-// and reciprocals are packed once per factorisation (k_band_pack).
+// Rows are grouped into segments of S consecutive rows (global index / S).
+// Pass 0 solves every segment on its own (the strict entries inside the
+// segment, forward substitution); each of the k sweeps then recomputes every
+// row from the previous pass's values outside its segment and the current
+// pass's values inside it (block Jacobi over segments, Gauss-Seidel within):
+//   y_s[i] = D^-1 (rhs_i - sum_{j outside} N_ij y_{s-1}[j] - sum_{j inside} N_ij y_s[j])
+// with every row's strict entries taken in column order (FP32: D^-1 is the
+// reciprocal 1/d).  S = 1 is plain Jacobi (a truncated Neumann series).
+// The splitting of the upper triangle is the transpose of the lower one's,
+// so the apply F^T F stays symmetric positive definite; with more passes
+// than the dependency depth it is the exact solve.
+//
+// Row i of pass s reads rows back to i - (B + S - 1) of the earlier pass
+// (lower; forward for upper), so the rows [lo, hi) of pass k depend only on
+// rows [lo - k Bs, hi), Bs = B rounded up to a multiple of S.  A CTA loads
+// that extended range once -- each thread keeps its rows' strict entries
+// (u16 offsets, FP32 values), right-hand side and reciprocal in registers --
+// and runs every pass with only the pass vectors in shared memory,
+// separated by __syncthreads.  At pass s it computes only the segments whose
+// inputs are still exact (from the range start plus s Bs on), so nothing it
+// reads is stale and rows [lo, hi) equal the one-launch-per-pass schedule
+// bit for bit.  The halo is recomputed by the neighbouring tiles (redundant
+// work instead of communication): no CTA waits on another.  The strict
+// entries and reciprocals are packed once per factorisation (k_band_pack).
 #pragma once
 
 #include <algorithm>
@@ -43,7 +54,14 @@ struct BandPlan
 // Host planning from the triangle's pattern (rows in CSR, column-sorted);
 // lower: strict entries j < i, upper: j > i.  T is chosen so that the tiles
 // fill the SMs once while each thread holds at most kBandRowsPerThread rows.
-inline BandPlan plan_band(uint32_t n, const uint32_t* rp, const uint32_t* ci, bool lower, int k, int sm_count)
+// halo rows of k passes with segments of S rows
+__host__ __device__ constexpr uint32_t band_halo(uint32_t k, uint32_t B, uint32_t S)
+{
+    return k * ((B + S - 1) / S * S);
+}
+
+inline BandPlan plan_band(uint32_t n, const uint32_t* rp, const uint32_t* ci, bool lower, int k, int sm_count,
+                          uint32_t S)
 {
     BandPlan p;
     if (!n || k <= 0) return p;
@@ -66,9 +84,10 @@ inline BandPlan plan_band(uint32_t n, const uint32_t* rp, const uint32_t* ci, bo
     if (W > 4 || B > 65535) return p;
     const uint32_t w = W <= 2 ? 2 : 4;
     const uint64_t cap = (uint64_t)band_threads(w) * kBandRowsPerThread;
-    const uint64_t halo = (uint64_t)k * B;
+    if (S != 1 && S != kBandRowsPerThread) return p;
+    const uint64_t halo = band_halo((uint32_t)k, (uint32_t)B, S);
     uint64_t T = (n + (uint64_t)sm_count - 1) / (uint64_t)sm_count;
-    T = (T + 31) / 32 * 32;
+    T = (T + 31) / 32 * 32;  // a multiple of S
     if (T < 64) T = 64;
     if (halo > 8 * T) return p;  // redundant work would dominate
     const uint64_t Rm = std::min<uint64_t>(T + halo, n);
@@ -140,7 +159,7 @@ struct BandUpd
     unsigned int* counter = nullptr;
 };
 
-template <bool LOWER, int W, typename RT, bool RZ = false, bool UPD = false>
+template <bool LOWER, int W, int S, typename RT, bool RZ = false, bool UPD = false>
 __global__ void __launch_bounds__(band_threads(W)) k_trsv_band(uint32_t n, uint32_t T, uint32_t B, uint32_t Rmax,
                                                              int k, const uint16_t* __restrict__ eoff,
                                                              const float* __restrict__ eval,
@@ -151,6 +170,7 @@ __global__ void __launch_bounds__(band_threads(W)) k_trsv_band(uint32_t n, uint3
 {
     static_assert(!(RZ && UPD), "one fused reduction per launch");
     constexpr uint32_t NT = band_threads(W), Q = kBandRowsPerThread;
+    static_assert(S == 1 || S == Q, "segments: single rows, or one segment of Q rows per thread");
     if (done && *done) return;
     double alpha = 0.0;
     if constexpr (UPD) alpha = up.st->alpha;
@@ -158,21 +178,23 @@ __global__ void __launch_bounds__(band_threads(W)) k_trsv_band(uint32_t n, uint3
     float* const y0 = reinterpret_cast<float*>(smem);
     float* const y1 = y0 + Rmax;
 
-    const uint32_t lo = blockIdx.x * T;  // < n: the grid has ceil(n / T) tiles
+    const uint32_t lo = blockIdx.x * T;  // < n: the grid has ceil(n / T) tiles; a multiple of S
     const uint32_t hi = min(n, lo + T);
-    const uint32_t halo = (uint32_t)k * B;
+    const uint32_t Bs = (B + S - 1) / S * S;
+    const uint32_t halo = (uint32_t)k * Bs;
     const uint32_t elo = LOWER ? (lo > halo ? lo - halo : 0u) : lo;
     const uint32_t ehi = LOWER ? hi : (uint32_t)min((uint64_t)n, (uint64_t)hi + halo);
     const uint32_t R = ehi - elo;  // <= Rmax <= NT * Q by the plan
     const bool cut = LOWER ? elo > 0 : ehi < n;  // the range is truncated: the halo goes stale
 
-    // ---- this thread's rows t = tid + NT q: entries, rhs, reciprocal; y_0
+    // this thread's rows: strided (S = 1) or one segment of Q consecutive rows
+    auto row_of = [&](uint32_t q) -> uint32_t { return S == 1 ? threadIdx.x + NT * q : Q * threadIdx.x + q; };
     uint32_t off[Q][W];
     float val[Q][W], rr[Q], di[Q];
 #pragma unroll
     for (uint32_t q = 0; q < Q; ++q)
     {
-        const uint32_t t = threadIdx.x + NT * q;
+        const uint32_t t = row_of(q);
         const bool in = t < R;
         const uint32_t i = elo + (in ? t : 0u);
 #pragma unroll
@@ -186,35 +208,72 @@ __global__ void __launch_bounds__(band_threads(W)) k_trsv_band(uint32_t n, uint3
         else
             rr[q] = in ? (float)rhs[i] : 0.f;
         di[q] = in ? __ldg(&dinv[i]) : 0.f;
-        if (in) y0[t] = rr[q] * di[q];
     }
-    __syncthreads();
 
-    // ---- k sweeps; at sweep s the rows [s B, R) (lower) / [0, R - s B) (upper) are exact
-    for (int s = 1; s <= k; ++s)
+    // pass s writes ybuf[s & 1]; pass 0 reads nothing outside the segments
+    for (int s = 0; s <= k; ++s)
     {
-        const uint32_t shrink = cut ? (uint32_t)s * B : 0u;
-        const uint32_t t0 = LOWER ? shrink : 0u;
-        const uint32_t t1 = LOWER ? R : (R > shrink ? R - shrink : 0u);
         const float* yin = (s & 1) ? y0 : y1;
         float* yout = (s & 1) ? y1 : y0;
-#pragma unroll
-        for (uint32_t q = 0; q < Q; ++q)
+        const uint32_t shrink = (cut && s > 0) ? (uint32_t)s * Bs : 0u;
+        if constexpr (S == 1)
         {
-            const uint32_t t = threadIdx.x + NT * q;
-            if (t >= t0 && t < t1)
-            {
-                float sum = rr[q];
+            const uint32_t t0 = LOWER ? shrink : 0u;
+            const uint32_t t1 = LOWER ? R : (R > shrink ? R - shrink : 0u);
 #pragma unroll
-                for (int e = 0; e < W; ++e)
-                    if (off[q][e]) sum -= val[q][e] * yin[LOWER ? t - off[q][e] : t + off[q][e]];
-                yout[t] = sum * di[q];
+            for (uint32_t q = 0; q < Q; ++q)
+            {
+                const uint32_t t = row_of(q);
+                if (t >= t0 && t < t1)
+                {
+                    float sum = rr[q];
+                    if (s > 0)
+                    {
+#pragma unroll
+                        for (int e = 0; e < W; ++e)
+                            if (off[q][e]) sum -= val[q][e] * yin[LOWER ? t - off[q][e] : t + off[q][e]];
+                    }
+                    yout[t] = sum * di[q];
+                }
+            }
+        }
+        else
+        {
+            // the segment [Q tid, Q tid + Q) is computed when all of it is exact
+            const uint32_t g0 = Q * threadIdx.x;
+            const bool live = g0 < R && (LOWER ? g0 >= shrink : min(g0 + Q, R) + shrink <= R);
+            if (live)
+            {
+                float prev = 0.f;  // the row before (after, upper) in this segment, this pass
+#pragma unroll
+                for (uint32_t u = 0; u < Q; ++u)
+                {
+                    const uint32_t q = LOWER ? u : Q - 1 - u;
+                    const uint32_t t = g0 + q;
+                    if (t >= R) continue;
+                    float sum = rr[q];
+#pragma unroll
+                    for (int e = 0; e < W; ++e)
+                    {
+                        const uint32_t o = off[q][e];
+                        if (!o) continue;
+                        const bool inside = LOWER ? o <= q : o <= Q - 1 - q;
+                        const uint32_t jj = LOWER ? t - o : t + o;
+                        if (inside)
+                            sum -= val[q][e] * (o == 1 ? prev : yout[jj]);
+                        else if (s > 0)
+                            sum -= val[q][e] * yin[jj];
+                    }
+                    const float yv = sum * di[q];
+                    yout[t] = yv;
+                    prev = yv;
+                }
             }
         }
         __syncthreads();
     }
 
-    // ---- rows [lo, hi) of y_k
+    // ---- rows [lo, hi) of pass k
     const float* yk = (k & 1) ? y1 : y0;
     double acc[1] = {0.0};
     for (uint32_t i = lo + threadIdx.x; i < hi; i += NT)

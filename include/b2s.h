@@ -152,10 +152,12 @@ typedef enum b2s_trsv
     B2S_TRSV_SYNCFREE = 2, /* one launch; rows wait on bounded per-row ready flags */
     B2S_TRSV_CHUNK = 3,    /* one launch; row chunks staged in shared memory, local levels split by
                               barriers, bounded flags between chunks (the AUTO choice) */
-    B2S_TRSV_JACOBI = 4    /* inexact: trsv_sweeps Jacobi sweeps x <- D^-1 (b - N x) from x = D^-1 b
-                              (a truncated Neumann series of the triangle), one fully parallel launch
-                              per sweep; the IC(0) apply stays symmetric positive definite
-                              (M^-1 = F^T F), but no longer equals the exact factor solve */
+    B2S_TRSV_JACOBI = 4    /* inexact: rows grouped into segments of trsv_segment consecutive rows;
+                              each segment solved on its own, then trsv_sweeps block-Jacobi sweeps
+                              (Gauss-Seidel inside a segment, the previous sweep's values outside);
+                              segment 1 is plain Jacobi, a truncated Neumann series.  Fully
+                              parallel passes; the IC(0) apply stays symmetric positive definite
+                              (M^-1 = F^T F) but is no longer the exact factor solve */
 } b2s_trsv;
 
 typedef struct b2s_pc_opts
@@ -173,7 +175,8 @@ typedef struct b2s_pc_opts
                                which stalls on 3-D problems and serves parity tests;
                             2: sequential three-phase smoothed-aggregation rule */
     const char* learned_weights; /* B2S_PC_LEARNED_IC0: path of a weight file, NULL = built-in init */
-    int trsv_sweeps;     /* B2S_TRSV_JACOBI: sweeps per triangle (0: 8) */
+    int trsv_sweeps;     /* B2S_TRSV_JACOBI: sweeps per triangle after the segment solve (0: 8) */
+    int trsv_segment;    /* B2S_TRSV_JACOBI: rows per segment, 1..32 (0: 1, plain Jacobi) */
 } b2s_pc_opts;
 
 /* Fills opts with the reference's defaults. */

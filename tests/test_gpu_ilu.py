@@ -144,45 +144,76 @@ def test_jacobi_sweeps_exact_beyond_depth(b2s, ctx, kind):
     assert not np.array_equal(z2, z)
 
 
-def _sweeps_f32(rp, ci, vals, d, r, k, lower):
-    """k Jacobi sweeps in float32, each row in column order with one rounding
-    per product and difference, then a product with the float32 reciprocal
-    1/d -- the kernels' arithmetic."""
+def _sweeps_f32(rp, ci, vals, d, r, k, lower, S=1):
+    """Pass 0 (each segment of S rows solved on its own) and k sweeps in
+    float32: rows of a segment in dependency order, each row's strict entries
+    in column order (current-pass values inside the segment, previous-pass
+    values outside), one rounding per product and difference, then a product
+    with the float32 reciprocal 1/d -- the kernels' arithmetic."""
     n = len(rp) - 1
     rows = np.repeat(np.arange(n), np.diff(rp))
     strict = (ci < rows) if lower else (ci > rows)
     rr, cc, vv = rows[strict], ci[strict].astype(np.int64), vals[strict].astype(np.float32)
-    # ELL slots in column order
     slot = np.zeros(len(rr), np.int64)
     for t in range(1, len(rr)):
         slot[t] = slot[t - 1] + 1 if rr[t] == rr[t - 1] else 0
     W = int(slot.max()) + 1 if len(rr) else 0
     d32, r32 = d.astype(np.float32), r.astype(np.float32)
     dinv = np.float32(1.0) / d32
-    y = r32 * dinv
-    for s in range(1, k + 1):
+    inside = (cc // S) == (rr // S)
+    pos = rr % S
+    yprev = None
+    for s in range(k + 1):
+        y = np.zeros(n, np.float32)
         acc = r32.copy()
-        for e in range(W):
-            m = slot == e
-            acc[rr[m]] = acc[rr[m]] - vv[m] * y[cc[m]]
-        y = acc * dinv
+        for q in (range(S) if lower else range(S - 1, -1, -1)):
+            rows_q = np.arange(q, n, S)
+            for e in range(W):
+                m = (slot == e) & (pos == q)
+                use = m & (inside | (s > 0))
+                src = np.where(inside[use], y[cc[use]], yprev[cc[use]] if s > 0 else np.float32(0))
+                acc[rr[use]] = acc[rr[use]] - vv[use] * src.astype(np.float32)
+            y[rows_q] = acc[rows_q] * dinv[rows_q]
+        yprev = y
     return y
 
 
-def test_jacobi_band_kernel_bit_exact_f32(b2s, ctx):
+@pytest.mark.parametrize("seg", [1, 8])
+def test_jacobi_band_kernel_bit_exact_f32(b2s, ctx, seg):
     """FP32 IC(0) with 5 sweeps on a 96x96 grid (bandwidth 96: the one-launch
-    banded kernel) against a float32 emulation of the sweeps, bit for bit."""
+    banded kernel) against a float32 emulation of the passes, bit for bit;
+    plain Jacobi (segment 1) and 8-row Gauss-Seidel segments."""
     import scipy.sparse as sp
     n, rp, ci, v = b2s.gen_grf_diffusion(96, seed=12, corr=0.1)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
-    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=5)
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=5,
+                    trsv_segment=seg)
     Lrp, Lci, Lv = M.export("ic0.L")
     d = sp.csr_matrix((Lv, Lci, Lrp), shape=(n, n)).diagonal()
     LT = sp.csr_matrix((Lv, Lci, Lrp), shape=(n, n)).T.tocsr()
     LT.sort_indices()
     r = b2s.uniform(43, n)
-    y = _sweeps_f32(Lrp, Lci, Lv, d, r, 5, True)
-    z = _sweeps_f32(LT.indptr, LT.indices, LT.data, d, y, 5, False)
+    y = _sweeps_f32(Lrp, Lci, Lv, d, r, 5, True, seg)
+    z = _sweeps_f32(LT.indptr, LT.indices, LT.data, d, y, 5, False, seg)
+    assert np.array_equal(M.apply(r), z.astype(np.float64))
+
+
+def test_segment_global_kernel_bit_exact_f32(b2s, ctx):
+    """A 12-row segment is not a banded-kernel width, so the one-launch-per-pass
+    kernel runs; it must match the float32 emulation bit for bit."""
+    import scipy.sparse as sp
+    n, rp, ci, v = b2s.gen_grf_diffusion(40, seed=13, corr=0.1)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=3,
+                    trsv_segment=12)
+    Lrp, Lci, Lv = M.export("ic0.L")
+    L = sp.csr_matrix((Lv, Lci, Lrp), shape=(n, n))
+    d = L.diagonal()
+    LT = L.T.tocsr()
+    LT.sort_indices()
+    r = b2s.uniform(44, n)
+    y = _sweeps_f32(Lrp, Lci, Lv, d, r, 3, True, 12)
+    z = _sweeps_f32(LT.indptr, LT.indices, LT.data, d, y, 3, False, 12)
     assert np.array_equal(M.apply(r), z.astype(np.float64))
 
 
@@ -195,7 +226,7 @@ def test_jacobi_sweeps_match_series(b2s, ctx, orc, prec):
     n, rp, ci, v = b2s.gen_grf_diffusion(40, seed=8)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
     fp = b2s.FP32 if prec == "fp32" else b2s.FP64
-    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=fp, trsv=b2s.TRSV_JACOBI, trsv_sweeps=3)
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=fp, trsv=b2s.TRSV_JACOBI, trsv_sweeps=3, trsv_segment=1)
     Lrp, Lci, Lv = M.export("ic0.L")
     L = sp.csr_matrix((Lv, Lci, Lrp), shape=(n, n))
     d = L.diagonal()
@@ -233,6 +264,9 @@ def test_jacobi_mode_checks(b2s, ctx):
     with pytest.raises(ValueError) as e:
         b2s.Precond(ctx, A, b2s.PC_IC0, trsv=b2s.TRSV_JACOBI, trsv_sweeps=-1)
     assert e.value.status == b2s.INVALID_ARG
+    with pytest.raises(ValueError) as e:
+        b2s.Precond(ctx, A, b2s.PC_IC0, trsv=b2s.TRSV_JACOBI, trsv_segment=33)
+    assert e.value.status == b2s.INVALID_ARG
     nb, brp, bci, bv = b2s.gen_elasticity_q1(3)
     B = b2s.BAIJ(ctx, 3, nb, nb, brp, bci, bv)
     with pytest.raises(b2s.B2SError) as e:
@@ -266,7 +300,7 @@ def test_fused_pcg_matches_host_pcg(b2s, ctx):
     n, rp, ci, v = b2s.gen_grf_diffusion(64, seed=2006, corr=0.1)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
     b = b2s.uniform(6, n)
-    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8)
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8, trsv_segment=1)
     x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=5000)
     Lrp, Lci, Lv = M.export("ic0.L")
     L = sp.csr_matrix((Lv, Lci, Lrp), shape=(n, n))
