@@ -130,6 +130,8 @@ KERNELS = {
     "vcycle_c2": "SA-AMG V-cycle (k_jacobi, BAIJ matvecs, k_dense_solve) on C2",
     "dense_c5": "k_linear_tc<64,128>: the learned network's tcgen05 dense layer on the 512^2 grid's node states "
                 "(n=262144 rows, 64 -> 128)",
+    "solve_c5": "one learned IC(0) PCG solve (8 Jacobi sweeps per triangle, fused iteration) on a 512^2 GRF system; "
+                "a step is setup + solve",
 }
 
 
@@ -158,6 +160,17 @@ def run_kernel(args):
         y = torch.empty_like(x)
         step = lambda: ctx.check(b2s.lib().b2s_baij_matvec_device(ctx.h, A.h, C.c_void_p(x.data_ptr()),
                                                                   C.c_void_p(y.data_ptr())), "baij_matvec")
+    elif k == "solve_c5":
+        n, rp, ci, v = b2s.gen_grf_diffusion(N_GRID, 2003, corr=CORR)
+        A = b2s.CSR(ctx, n, n, rp, ci, v)
+        bt = torch.from_numpy(b2s.uniform(2003, n)).to(dev)
+        xt = torch.zeros(n, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+
+        def step():
+            M = b2s.Precond(ctx, A, b2s.PC_LEARNED_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8,
+                            factor_sweeps=5)
+            b2s.solve_device(ctx, A, bt.data_ptr(), xt.data_ptr(), b2s.PCG, M, tol=TOL, maxit=MAXIT)
     elif k == "dense_c5":
         n = N_GRID * N_GRID
         g = torch.Generator(device=dev).manual_seed(5)
@@ -295,16 +308,16 @@ def main():
     seeds = [2000 + rank * 100000 + k for k in range(args.warmup + args.steps)]
     systems = [make_system(b2s, s) for s in seeds]
 
-    # method -> (preconditioner, precision, triangular-solve schedule, sweeps)
-    kinds = {"learned_ic0_j8": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_JACOBI, 8),
-             "learned_ic0": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_AUTO, 0),
-             "fp32_ic0_j8": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_JACOBI, 8),
-             "fp32_ic0": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_AUTO, 0),
-             "fp64_ic0": (b2s.PC_IC0, b2s.FP64, b2s.TRSV_AUTO, 0)}
+    # method -> (preconditioner, precision, triangular-solve schedule, sweeps, factorisation sweeps)
+    kinds = {"learned_ic0_j8": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_JACOBI, 8, 5),
+             "learned_ic0": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_AUTO, 0, 0),
+             "fp32_ic0_j8": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_JACOBI, 8, 5),
+             "fp32_ic0": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_AUTO, 0, 0),
+             "fp64_ic0": (b2s.PC_IC0, b2s.FP64, b2s.TRSV_AUTO, 0, 0)}
 
     def make_pc(A, method):
-        kind, prec, trsv, sweeps = kinds[method]
-        return b2s.Precond(ctx, A, kind, precision=prec, trsv=trsv, trsv_sweeps=sweeps)
+        kind, prec, trsv, sweeps, fsweeps = kinds[method]
+        return b2s.Precond(ctx, A, kind, precision=prec, trsv=trsv, trsv_sweeps=sweeps, factor_sweeps=fsweeps)
 
     def timed_solve(n, rp, ci, v, b, method):
         """Device-resident inputs; returns (ms, stats, relres_true)."""
@@ -372,7 +385,7 @@ def main():
 
     # e2e: host CSR + host b -> device, preconditioner, solve, x -> host (public C ABI, host pointers)
     e2e_ms, h2d, d2h = [], 0, 0
-    kind, prec, trsv, sweeps = kinds[args.method]
+    kind, prec, trsv, sweeps, _ = kinds[args.method]
     for k in range(args.steps):
         n, rp, ci, v, b = systems[args.warmup + k]
         torch.cuda.synchronize()
@@ -503,10 +516,12 @@ def main():
             "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 outer / f32 preconditioner" if prec == b2s.FP32 else "f64",
-            "method": {"learned_ic0_j8": "learned IC(0) values (tcgen05 network), FP32 factor, 8 Jacobi sweeps per "
-                                         "triangle (banded one-launch kernel), FP64 PCG and true residual",
-                       "learned_ic0": "learned IC(0) values, FP32 factor, exact chunk-scheduled triangular solves",
-                       "fp32_ic0_j8": "plain IC(0), FP32 factor, 8 Jacobi sweeps per triangle",
+            "method": {"learned_ic0_j8": "learned IC(0) values (tcgen05 network) on a 5-sweep fixed-point IC(0) "
+                                         "factor, FP32, 8 Jacobi sweeps per triangle (banded one-launch kernel, "
+                                         "fused PCG iteration), FP64 PCG and true residual",
+                       "learned_ic0": "learned IC(0) values on the exact factor, FP32, exact chunk-scheduled "
+                                      "triangular solves",
+                       "fp32_ic0_j8": "plain IC(0) (5-sweep fixed-point factor), FP32, 8 Jacobi sweeps per triangle",
                        "fp32_ic0": "plain IC(0), FP32 factor, exact triangular solves",
                        "fp64_ic0": "plain IC(0), FP64, exact triangular solves"}[args.method],
             "data": "synthetic (seeded GRF diffusion, held-out seeds 2000+)",

@@ -79,7 +79,8 @@ def _raise(status: int, msg: str):
 class PcOpts(C.Structure):
     _fields_ = [("omega", C.c_double), ("precision", C.c_int), ("trsv", C.c_int), ("amg_ref_coarse", C.c_int),
                 ("amg_max_levels", C.c_int), ("amg_coarse_max", C.c_int), ("amg_aggregation", C.c_int),
-                ("learned_weights", C.c_char_p), ("trsv_sweeps", C.c_int), ("trsv_segment", C.c_int)]
+                ("learned_weights", C.c_char_p), ("trsv_sweeps", C.c_int), ("trsv_segment", C.c_int),
+                ("factor_sweeps", C.c_int)]
 
 
 class SolveOpts(C.Structure):
@@ -312,11 +313,11 @@ class BAIJ:
 
 
 def pc_opts(omega=1.2, precision=FP64, trsv=TRSV_AUTO, amg_ref_coarse=0, amg_max_levels=0, amg_coarse_max=0,
-            amg_aggregation=0, learned_weights=None, trsv_sweeps=0, trsv_segment=0) -> PcOpts:
+            amg_aggregation=0, learned_weights=None, trsv_sweeps=0, trsv_segment=0, factor_sweeps=0) -> PcOpts:
     o = PcOpts()
     lib().b2s_pc_opts_default(C.byref(o))
     o.omega, o.precision, o.trsv, o.trsv_sweeps = omega, precision, trsv, trsv_sweeps
-    o.trsv_segment = trsv_segment
+    o.trsv_segment, o.factor_sweeps = trsv_segment, factor_sweeps
     o.amg_ref_coarse, o.amg_max_levels, o.amg_coarse_max = amg_ref_coarse, amg_max_levels, amg_coarse_max
     o.amg_aggregation = amg_aggregation
     o.learned_weights = learned_weights.encode() if learned_weights else None

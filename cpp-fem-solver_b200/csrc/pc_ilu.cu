@@ -189,6 +189,96 @@ __global__ void k_ic0_level(const uint32_t* __restrict__ rows, uint32_t count, c
     ic0_row(rows[t], Lrp, Lci, Lv, diag, err);
 }
 
+// Fixed-point IC(0) (Chow and Patel, "Fine-grained parallel incomplete LU
+// factorization", SIAM J. Sci. Comput. 37 (2015)): every entry of L is
+// recomputed from the previous sweep's values,
+//   l_ij = (a_ij - sum_{k<j} l_ik l_jk) / l_jj   (j < i),
+//   l_ii = sqrt(a_ii - sum_{k<i} l_ik^2),
+// the sums over the common columns in column order (the exact row
+// factorisation's arithmetic, so a sweep count above the dependency depth
+// reproduces it bit for bit).  Sweep 0 starts from l_ij = a_ij / sqrt(a_jj),
+// l_ii = sqrt(a_ii).  Rows hold the diagonal last (tril of a matrix with a
+// full diagonal; checked by k_ic0_par_init).
+__global__ void k_ic0_par_init(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lci,
+                               const double* __restrict__ a, double* __restrict__ l, unsigned long long* err)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const uint32_t rs = Lrp[i], re = Lrp[i + 1];
+        if (re == rs || Lci[re - 1] != i)
+        {
+            atomicMin(err, ((unsigned long long)i << 8) | B2S_MISSING_DIAG);
+            for (uint32_t p = rs; p < re; ++p) l[p] = 0.0;
+            continue;
+        }
+        for (uint32_t p = rs; p < re; ++p)
+        {
+            const uint32_t j = Lci[p];
+            const double ajj = a[Lrp[j + 1] - 1];
+            l[p] = j == i ? sqrt(fabs(a[p])) : a[p] / sqrt(fabs(ajj));
+        }
+    }
+}
+
+__global__ void k_ic0_par_sweep(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lci,
+                                const double* __restrict__ a, const double* __restrict__ lin,
+                                double* __restrict__ lout)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const uint32_t rs = Lrp[i], re = Lrp[i + 1];
+        for (uint32_t p = rs; p < re; ++p)
+        {
+            const uint32_t j = Lci[p];
+            if (j < i)
+            {
+                double sum = 0.0;
+                uint32_t pi = rs, pj = Lrp[j];
+                const uint32_t ej = Lrp[j + 1];
+                while (pi < p && pj < ej)
+                {
+                    const uint32_t ki = Lci[pi], kj = Lci[pj];
+                    if (ki == kj)
+                    {
+                        sum += lin[pi] * lin[pj];
+                        ++pi;
+                        ++pj;
+                    }
+                    else if (ki < kj)
+                        ++pi;
+                    else
+                        ++pj;
+                }
+                lout[p] = (a[p] - sum) / lin[ej - 1];
+            }
+            else
+            {
+                double sd = 0.0;
+                for (uint32_t q = rs; q < p; ++q) sd += lin[q] * lin[q];
+                const double dv = a[p] - sd;
+                lout[p] = dv > 0.0 ? sqrt(dv) : 0.0;  // a non-positive pivot is caught after the last sweep
+            }
+        }
+    }
+}
+
+// after the last sweep: diag[i] = l_ii, a pivot <= 1e-14 (or NaN) is NOT_SPD
+__global__ void k_ic0_par_finish(uint32_t n, const uint32_t* __restrict__ Lrp, const double* __restrict__ l,
+                                 double* __restrict__ diag, unsigned long long* err)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const double d = l[Lrp[i + 1] - 1];
+        if (!(d * d > 1e-14))
+        {
+            atomicMin(err, ((unsigned long long)i << 8) | B2S_NOT_SPD);
+            diag[i] = 1.0;
+        }
+        else
+            diag[i] = d;
+    }
+}
+
 // The whole factorisation in one CTA when every level is narrow: the CTA
 // walks the levels in order, its threads take a level's rows, and a
 // __syncthreads separates the levels (the block barrier orders the global
@@ -617,6 +707,7 @@ static int pick_trsv(const b2s_pc_opts& o)
     need(o.trsv >= B2S_TRSV_AUTO && o.trsv <= B2S_TRSV_JACOBI, B2S_INVALID_ARG, "unknown triangular-solve schedule");
     need(o.trsv_sweeps >= 0 && o.trsv_sweeps <= 1024, B2S_INVALID_ARG, "trsv_sweeps must be 0..1024");
     need(o.trsv_segment >= 0 && o.trsv_segment <= 32, B2S_INVALID_ARG, "trsv_segment must be 0..32");
+    need(o.factor_sweeps >= 0 && o.factor_sweeps <= 1024, B2S_INVALID_ARG, "factor_sweeps must be 0..1024");
     return o.trsv == B2S_TRSV_AUTO ? B2S_TRSV_CHUNK : o.trsv;
 }
 
@@ -749,6 +840,36 @@ void ic0_factor_inplace(b2s_ctx* ctx, const LevelSchedule& s, const uint32_t* Lr
     check_err(ctx, err, what);
 }
 
+// k fixed-point sweeps on L (values: tril(A) in, the approximate factor
+// out).  False when a pivot failed (the caller then factors exactly from the
+// saved tril(A)); other failures throw like the exact factorisation.
+static bool ic0_factor_fixed_point(b2s_ctx* ctx, Csr32& L, double* diag, int k, const DBuf<double>& a)
+{
+    const uint32_t n = L.n;
+    DBuf<unsigned long long> err(1);
+    const unsigned long long none = ~0ull;
+    h2d(ctx, err.p, &none, sizeof(none));
+    DBuf<double> tmp(L.nnz ? L.nnz : 1);
+    const unsigned g = stream_grid(ctx, n);
+    // ping-pong so that the last sweep lands in L.v
+    double* buf[2] = {L.v.p, tmp.p};
+    int cur = (k & 1) ? 1 : 0;
+    B2S_LAUNCH(ctx, k_ic0_par_init, g, kThreads, 0, n, L.rp.p, L.ci.p, a.p, buf[cur], err.p);
+    for (int s = 0; s < k; ++s)
+    {
+        B2S_LAUNCH(ctx, k_ic0_par_sweep, g, kThreads, 0, n, L.rp.p, L.ci.p, a.p, buf[cur], buf[cur ^ 1]);
+        cur ^= 1;
+    }
+    B2S_LAUNCH(ctx, k_ic0_par_finish, g, kThreads, 0, n, L.rp.p, L.v.p, diag, err.p);
+    unsigned long long e = 0;
+    d2h(ctx, &e, err.p, sizeof(e));
+    sync(ctx);
+    if (e == ~0ull) return true;
+    if ((e & 0xff) == B2S_NOT_SPD) return false;
+    check_err(ctx, err, "IC(0) failed");  // MISSING_DIAG: the exact factorisation's error
+    return false;
+}
+
 std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o, Ic0Correction* corr)
 {
     need(A.n == A.m, B2S_SHAPE, "IC(0) needs a square matrix");
@@ -771,12 +892,16 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     const bool sweeps = pc->mode == B2S_TRSV_JACOBI;
     const int nsweeps = sweep_count(o);
     const uint32_t seg = sweep_segment(o);
+    const int fsweeps = o.factor_sweeps;
     std::vector<uint32_t> hrp, hci;
     copy_pattern(ctx, pc->L, hrp, hci);
     pc->fwd.init(pc->L, true, false);
-    // the levels of L order the factorisation (a warp's rows are independent)
-    compute_levels(n, hrp.data(), hci.data(), true, pc->fwd.h_level);
-    pc->fwd.ensure_sched(ctx);
+    // the levels of L order the exact factorisation and the exact solves
+    auto levels = [&] {
+        compute_levels(n, hrp.data(), hci.data(), true, pc->fwd.h_level);
+        pc->fwd.ensure_sched(ctx);
+    };
+    if (!(sweeps && fsweeps > 0)) levels();
     HostAnalysis ha;
     ha.chunked = pc->mode == B2S_TRSV_CHUNK && n;
     const int sm_count = ctx->sm_count;
@@ -809,7 +934,20 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
         }
     });
     pc->fwd.d64 = pc->diag.p;
-    ic0_factor_inplace(ctx, pc->fwd.sched, pc->L.rp.p, pc->L.ci.p, pc->L.v.p, pc->diag.p, "IC(0) failed");
+    bool factored = false;
+    if (fsweeps > 0)
+    {
+        DBuf<double> a(pc->L.nnz ? pc->L.nnz : 1);  // tril(A), the sweeps' right-hand side
+        d2d(ctx, a.p, pc->L.v.p, (size_t)pc->L.nnz * sizeof(double));
+        factored = ic0_factor_fixed_point(ctx, pc->L, pc->diag.p, fsweeps, a);
+        if (!factored)  // a pivot failed: the exact factorisation decides (and reports)
+        {
+            d2d(ctx, pc->L.v.p, a.p, (size_t)pc->L.nnz * sizeof(double));
+            if (!pc->fwd.sched_ready) levels();
+        }
+    }
+    if (!factored)
+        ic0_factor_inplace(ctx, pc->fwd.sched, pc->L.rp.p, pc->L.ci.p, pc->L.v.p, pc->diag.p, "IC(0) failed");
     if (corr) corr->correct(ctx, A, pc->L.rp.p, pc->L.ci.p, pc->L.nnz, pc->L.v.p, pc->diag.p);
     transpose_strict(ctx, pc->L, pc->LT);
     pc->y.alloc(n ? n : 1);

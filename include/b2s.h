@@ -177,6 +177,9 @@ typedef struct b2s_pc_opts
     const char* learned_weights; /* B2S_PC_LEARNED_IC0: path of a weight file, NULL = built-in init */
     int trsv_sweeps;     /* B2S_TRSV_JACOBI: sweeps per triangle after the segment solve (0: 8) */
     int trsv_segment;    /* B2S_TRSV_JACOBI: rows per segment, 1..32 (0: 1, plain Jacobi) */
+    int factor_sweeps;   /* IC(0): 0 = the exact factorisation (level order, the reference's values);
+                            k > 0 = k fixed-point sweeps over all entries at once (Chow-Patel), an
+                            approximate factor; a failed pivot falls back to the exact factorisation */
 } b2s_pc_opts;
 
 /* Fills opts with the reference's defaults. */

@@ -337,3 +337,49 @@ def test_fused_pcg_matches_host_pcg(b2s, ctx):
         rz = rz2
     assert st["relres_true"] < 1e-8
     assert abs(st["iterations"] - it) <= 3, (st["iterations"], it)
+
+
+def test_fixed_point_factor_exact_beyond_depth(b2s, ctx):
+    """Fixed-point IC(0) sweeps use the exact row arithmetic, so with enough
+    sweeps the factor equals the exact factorisation bit for bit: on 12x12
+    the DAG has 23 levels and each level takes two sweeps (the off-diagonal
+    entries of a row, then its pivot from them), so 50 suffice.  With 3
+    sweeps the factor is close but not equal."""
+    n, rp, ci, v = P.poisson2d(12)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    exact = b2s.Precond(ctx, A, b2s.PC_IC0).export("ic0.L")[2]
+    deep = b2s.Precond(ctx, A, b2s.PC_IC0, factor_sweeps=50).export("ic0.L")[2]
+    assert np.array_equal(deep, exact)
+    few = b2s.Precond(ctx, A, b2s.PC_IC0, factor_sweeps=3).export("ic0.L")[2]
+    assert not np.array_equal(few, exact)
+    assert np.abs(few - exact).max() < 1e-2 * np.abs(exact).max()
+
+
+def test_fixed_point_factor_pcg(b2s, ctx):
+    """3 fixed-point sweeps with 8 Jacobi sweeps per triangle (the benchmark's
+    learned configuration without the network): PCG meets the FP64-verified
+    tolerance within 5% of the exact factor's iterations."""
+    n, rp, ci, v = b2s.gen_grf_diffusion(128, seed=2004, corr=0.05)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(4, n)
+    opts = dict(precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8)
+    _, s0 = b2s.solve(ctx, A, b, b2s.PCG, b2s.Precond(ctx, A, b2s.PC_IC0, **opts), tol=1e-8, maxit=5000)
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, factor_sweeps=3, **opts)
+    _, s1 = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=5000)
+    assert s1["status"] == 0 and s1["relres_true"] < 1e-8
+    assert s1["iterations"] <= 1.05 * s0["iterations"], (s1["iterations"], s0["iterations"])
+
+
+def test_fixed_point_factor_errors_like_exact(b2s, ctx):
+    n, rp, ci, v = P.poisson2d(8)
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    v2 = v.copy()
+    v2[(rows == ci) & (rows == 10)] = 0.5
+    with pytest.raises(RuntimeError) as e:
+        b2s.Precond(ctx, b2s.CSR(ctx, n, n, rp, ci, v2), b2s.PC_IC0, factor_sweeps=3)
+    assert e.value.status == b2s.NOT_SPD
+    keep = ~((rows == ci) & (rows == 7))
+    rp3 = np.concatenate([[0], np.cumsum(np.bincount(rows[keep], minlength=n))]).astype(np.uint32)
+    with pytest.raises(RuntimeError) as e:
+        b2s.Precond(ctx, b2s.CSR(ctx, n, n, rp3, ci[keep], v[keep]), b2s.PC_IC0, factor_sweeps=3)
+    assert e.value.status == b2s.MISSING_DIAG
