@@ -193,8 +193,9 @@ struct CsrDev
     uint32_t nblk = 0;
     uint32_t max_row = 0;       // longest row (nonzeros); 0 = not known
     DBuf<double> diag;          // diagonal entries (0 where missing)
-    std::vector<uint32_t> h_rp, h_ci;  // host copies of the pattern (setup code)
-    std::vector<double> h_v;
+    // host copy of the pattern, made on demand by the setup code that needs it
+    mutable std::vector<uint32_t> h_rp, h_ci;
+    void host_pattern(b2s_ctx* ctx) const;
     void ensure_fp32(b2s_ctx* ctx);
 };
 

@@ -32,6 +32,16 @@ __global__ void k_to_f32(const double* __restrict__ a, float* __restrict__ b, ui
         b[i] = (float)a[i];
 }
 
+void CsrDev::host_pattern(b2s_ctx* ctx) const
+{
+    if (h_rp.size() == (size_t)n + 1) return;
+    h_rp.resize((size_t)n + 1);
+    h_ci.resize(nnz ? nnz : 1);
+    d2h(ctx, h_rp.data(), rp.p, ((size_t)n + 1) * sizeof(uint32_t));
+    if (nnz) d2h(ctx, h_ci.data(), ci.p, (size_t)nnz * sizeof(uint32_t));
+    sync(ctx);
+}
+
 void CsrDev::ensure_fp32(b2s_ctx* ctx)
 {
     if (v32.p || nnz == 0) return;
@@ -77,24 +87,37 @@ b2s_status b2s_csr_create(b2s_ctx* ctx, uint32_t n, uint32_t m, const uint32_t* 
     b2s_status st = guarded(ctx, [&] {
         B2S_CUDA(cudaSetDevice(ctx->device));
         need(row_ptr[0] == 0, B2S_INVALID_ARG, "row_ptr[0] must be 0");
-        for (uint32_t i = 0; i < n; ++i) need(row_ptr[i + 1] >= row_ptr[i], B2S_INVALID_ARG, "row_ptr must be non-decreasing");
         const uint32_t nnz = row_ptr[n];
         need(nnz == 0 || (col_idx && values), B2S_INVALID_ARG, "null col_idx / values");
-        for (uint32_t i = 0; i < n; ++i)
-            for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+        // one pass: row pointers non-decreasing, columns in range and strictly ascending
+        uint32_t max_row = 0;
+        bool ok_rp = true, ok_range = true, ok_order = true;
+        for (uint32_t i = 0; i < n && ok_rp; ++i)
+        {
+            const uint32_t a = row_ptr[i], b = row_ptr[i + 1];
+            if (b < a || b > nnz)
             {
-                need(col_idx[k] < m, B2S_INVALID_ARG, "column index out of range");
-                need(k == row_ptr[i] || col_idx[k] > col_idx[k - 1], B2S_INVALID_ARG,
-                     "columns must be strictly ascending within a row");
+                ok_rp = false;
+                break;
             }
+            max_row = std::max(max_row, b - a);
+            uint32_t prev = 0;
+            for (uint32_t k = a; k < b; ++k)
+            {
+                const uint32_t c = col_idx[k];
+                ok_range &= c < m;
+                ok_order &= k == a || c > prev;
+                prev = c;
+            }
+        }
+        need(ok_rp, B2S_INVALID_ARG, "row_ptr must be non-decreasing");
+        need(ok_range, B2S_INVALID_ARG, "column index out of range");
+        need(ok_order, B2S_INVALID_ARG, "columns must be strictly ascending within a row");
         CsrDev& d = A->d;
         d.n = n;
         d.m = m;
         d.nnz = nnz;
-        d.h_rp.assign(row_ptr, row_ptr + n + 1);
-        for (uint32_t i = 0; i < n; ++i) d.max_row = std::max(d.max_row, row_ptr[i + 1] - row_ptr[i]);
-        d.h_ci.assign(col_idx, col_idx + nnz);
-        d.h_v.assign(values, values + nnz);
+        d.max_row = max_row;
         d.rp = upload(ctx, row_ptr, (size_t)n + 1);
         // 8 elements of padding: the bulk copies of the SpMV start and end on
         // 16-byte boundaries and may read a few elements past the last nonzero

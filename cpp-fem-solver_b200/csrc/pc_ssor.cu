@@ -241,6 +241,7 @@ std::unique_ptr<PcImpl> make_pc_ssor(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     pc->n = n;
     pc->omega = o.omega;
     std::vector<int> colour;
+    A.host_pattern(ctx);
     colour_graph(n, A.h_rp, A.h_ci, colour);
     uint32_t nc = 0;
     for (uint32_t i = 0; i < n; ++i) nc = std::max<uint32_t>(nc, (uint32_t)colour[i] + 1);
