@@ -153,7 +153,8 @@ struct KState
     int done;     // 1 once converged / failed / stopped
     int status;   // b2s_status
     int iters;    // iterations executed (SpMVs in the loop)
-    int pad[2];
+    int stalled;  // 1: a device-side stall guard stopped the solve
+    int pad;
 };
 
 }  // namespace b2s
@@ -245,6 +246,17 @@ struct PcImpl
     {
         (void)x, (void)p, (void)Ap, (void)r_old, (void)r_new, (void)z, (void)st, (void)done;
         fail(B2S_UNSUPPORTED, "this preconditioner does not fuse the PCG update");
+    }
+    // The whole PCG loop in one persistent launch (from the state after
+    // the first z = M^-1 r, p = z, rz_old): r, p in two buffers each, x
+    // updated in place, st on exit as the iteration-by-iteration loop would
+    // leave it (st->stalled when the stall guard stopped it).  False, with
+    // nothing enqueued, when the preconditioner cannot run it.
+    virtual bool pcg_persistent(b2s_ctx*, const CsrDev& A, double* x, double* r0, double* r1, double* p0,
+                                double* p1, double* z, double* Ap, KState* st, int stall_window)
+    {
+        (void)A, (void)x, (void)r0, (void)r1, (void)p0, (void)p1, (void)z, (void)Ap, (void)st, (void)stall_window;
+        return false;
     }
     // one triangle of a factored preconditioner M = L L^T (FP64 storage):
     // out = L^{-1} in (upper = false) or L^{-T} in (upper = true)

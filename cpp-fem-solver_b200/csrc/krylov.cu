@@ -925,6 +925,17 @@ static void run_pcg(Solve& S, const double* b, double* x, b2s_stats* stats)
             // tests convergence; its second reduces r.z and steps beta.  The
             // residual and direction alternate between two buffers, so a
             // captured batch has an even number of iterations.
+            // all iterations in one persistent launch when the preconditioner can
+            if (S.pc->pcg_persistent(ctx, *S.A.csr, x, r, r1, p, p1, z, Ap, st, S.stall_window))
+            {
+                const KState hs = S.read_state();
+                if (hs.stalled)
+                {
+                    S.stalled = true;
+                    S.stalled_at = hs.iters;
+                }
+                goto done_iterating;
+            }
             if (S.poll_every & 1) S.poll_every += 1;
             int parity = 0;
             auto body = [&] {
@@ -961,6 +972,7 @@ static void run_pcg(Solve& S, const double* b, double* x, b2s_stats* stats)
         S.loop(body);
         }
     }
+done_iterating:
     B2S_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     S.true_residual(b, x, Ap);
     h = S.read_state();

@@ -25,6 +25,7 @@
 #include "trisolve.cuh"
 #include "trsv_chunk.cuh"
 #include "trsv_band.cuh"
+#include "pcg_band.cuh"
 
 #include <exception>
 #include <thread>
@@ -762,6 +763,66 @@ struct PcIC0 final : PcImpl
     }
 
     bool can_fuse_pcg() const override { return fp32 && mode == B2S_TRSV_JACOBI && fwd.band.T && bwd.band.T; }
+
+    DBuf<unsigned> pcg_ctl;  // grid-barrier counter, error word
+
+    bool pcg_persistent(b2s_ctx* ctx, const CsrDev& A, double* x, double* r0, double* r1, double* p0, double* p1,
+                        double* z, double* Ap, KState* st, int stall_window) override
+    {
+        const BandPlan &lb = fwd.band, &ub = bwd.band;
+        if (!(can_fuse_pcg() && fwd.segment == 1 && bwd.segment == 1 && lb.W == 2 && ub.W == 2 && lb.T == ub.T &&
+              lb.B == ub.B && lb.Rmax == ub.Rmax && lb.ntiles == ub.ntiles && fwd.sweeps == bwd.sweeps &&
+              A.n == n && n > 0 && lb.ntiles <= (uint32_t)ctx->sm_count && lb.T <= 3 * kPcgBandThreads))
+            return false;
+        if (!pcg_ctl.p) pcg_ctl.alloc(2);
+        B2S_CUDA(cudaMemsetAsync(pcg_ctl.p, 0, 2 * sizeof(unsigned), ctx->stream));
+        reserve_reduction(ctx, 3 * lb.ntiles);
+        PcgBandArgs a{};
+        a.n = n;
+        a.T = lb.T;
+        a.B = lb.B;
+        a.Rmax = lb.Rmax;
+        a.k = fwd.sweeps;
+        a.Arp = A.rp.p;
+        a.Aci = A.ci.p;
+        a.Av = A.v.p;
+        a.loff = fwd.band_off.p;
+        a.lval = fwd.band_val.p;
+        a.ldinv = fwd.band_dinv.p;
+        a.uoff = bwd.band_off.p;
+        a.uval = bwd.band_val.p;
+        a.udinv = bwd.band_dinv.p;
+        a.x = x;
+        a.r[0] = r0;
+        a.r[1] = r1;
+        a.p[0] = p0;
+        a.p[1] = p1;
+        a.z = z;
+        a.Ap = Ap;
+        a.red = ctx->partial.p;
+        a.y32 = y32.p;
+        a.st = st;
+        a.bar = pcg_ctl.p;
+        a.err = reinterpret_cast<int*>(pcg_ctl.p + 1);
+        a.stall_window = stall_window;
+        const size_t smem = 2 * (size_t)lb.Rmax * sizeof(float);
+        B2S_CUDA(cudaFuncSetAttribute(k_pcg_band, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        void* params[] = {&a};
+        const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_band, dim3(lb.ntiles),
+                                                          dim3(kPcgBandThreads), params, smem, ctx->stream);
+        if (e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported)
+        {
+            cudaGetLastError();  // the CTAs could not all be resident: the caller iterates launch by launch
+            return false;
+        }
+        B2S_CUDA(e);
+        note_launch(ctx, "k_pcg_band");
+        int err = 0;
+        d2h(ctx, &err, pcg_ctl.p + 1, sizeof(int));
+        sync(ctx);
+        if (err) fail(B2S_TIMEOUT, "persistent PCG: a grid barrier wait gave up");
+        return true;
+    }
 
     void pcg_update_apply(b2s_ctx* ctx, double* x, const double* p, const double* Ap, const double* r_old,
                           double* r_new, double* z, KState* st, const int* done) override

@@ -275,15 +275,16 @@ def test_jacobi_mode_checks(b2s, ctx):
 
 
 def test_fused_pcg_iteration_graph_and_polling_invariant(b2s, ctx):
-    """The banded sweep preconditioner runs PCG as three fused launches per
-    iteration with the residual and direction in alternating buffers.  The
-    result must not depend on how the iterations are batched: CUDA graphs on
-    or off, and any polling interval (an odd one is rounded up to keep the
-    buffer roles), give the same iterate bit for bit."""
+    """With 8-row segments the banded sweep preconditioner runs PCG as three
+    fused launches per iteration with the residual and direction in
+    alternating buffers.  The result must not depend on how the iterations
+    are batched: CUDA graphs on or off, and any polling interval (an odd one
+    is rounded up to keep the buffer roles), give the same iterate bit for
+    bit."""
     n, rp, ci, v = b2s.gen_grf_diffusion(128, seed=2005, corr=0.05)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
     b = b2s.uniform(5, n)
-    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8)
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=4, trsv_segment=8)
     runs = [b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=5000, use_graphs=g, check_every=c)
             for g, c in ((1, 0), (0, 0), (1, 3), (0, 5))]
     x0, s0 = runs[0]
@@ -383,3 +384,37 @@ def test_fixed_point_factor_errors_like_exact(b2s, ctx):
     with pytest.raises(RuntimeError) as e:
         b2s.Precond(ctx, b2s.CSR(ctx, n, n, rp3, ci[keep], v[keep]), b2s.PC_IC0, factor_sweeps=3)
     assert e.value.status == b2s.MISSING_DIAG
+
+
+def test_persistent_pcg_matches_launch_per_phase(b2s, ctx):
+    """Plain Jacobi sweeps on a banded FP32 factor run the whole PCG loop in
+    one cooperative persistent launch.  Against the same sweeps in FP64
+    (one launch per sweep, host-driven loop): both meet the tolerance, the
+    iteration counts agree within 3 and the iterates to 1e-6."""
+    n, rp, ci, v = b2s.gen_grf_diffusion(256, seed=2007, corr=0.05)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(7, n)
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8)
+    l0 = ctx.kernel_launches
+    x1, s1 = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=5000)
+    launches = ctx.kernel_launches - l0
+    assert s1["status"] == 0 and s1["relres_true"] < 1e-8
+    assert launches < 20, launches  # setup of the solve + one persistent launch
+    ref = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP64, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8)
+    x2, s2 = b2s.solve(ctx, A, b, b2s.PCG, ref, tol=1e-8, maxit=5000)
+    assert s2["status"] == 0 and s2["relres_true"] < 1e-8
+    assert abs(s1["iterations"] - s2["iterations"]) <= 3
+    assert np.linalg.norm(x1 - x2) <= 1e-6 * np.linalg.norm(x2)
+
+
+def test_persistent_pcg_stall_guard(b2s, ctx):
+    """The persistent loop carries the learned solve's stall guard: with a
+    one-iteration window it stops at once and plain IC(0) finishes."""
+    n, rp, ci, v = b2s.gen_grf_diffusion(256, seed=2008, corr=0.05)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(8, n)
+    M = b2s.Precond(ctx, A, b2s.PC_LEARNED_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8,
+                    factor_sweeps=5)
+    x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=20000, stall_window=1)
+    assert st["fallbacks"] == 1 and 0 < st["stalled_at"] < st["iterations"]
+    assert st["status"] == 0 and st["relres_true"] < 1e-8
