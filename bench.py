@@ -280,7 +280,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b2s", choices=["b2s", "reference"])
     ap.add_argument("--method", default="learned_ic0_j8",
-                    choices=["learned_ic0_j8", "learned_ic0", "fp32_ic0_j8", "fp32_ic0", "fp64_ic0"])
+                    choices=["learned_ic0_j8", "learned_ic0", "fp32_ic0_j8", "fp32_ic0", "fp64_ic0", "sa_amg"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel", default=None, choices=sorted(KERNELS),
                     help="run one hot kernel only (for profilers), not the benchmark")
@@ -313,7 +313,8 @@ def main():
              "learned_ic0": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_AUTO, 0, 0),
              "fp32_ic0_j8": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_JACOBI, 8, 5),
              "fp32_ic0": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_AUTO, 0, 0),
-             "fp64_ic0": (b2s.PC_IC0, b2s.FP64, b2s.TRSV_AUTO, 0, 0)}
+             "fp64_ic0": (b2s.PC_IC0, b2s.FP64, b2s.TRSV_AUTO, 0, 0),
+             "sa_amg": (b2s.PC_SA_AMG, b2s.FP64, b2s.TRSV_AUTO, 0, 0)}
 
     def make_pc(A, method):
         kind, prec, trsv, sweeps, fsweeps = kinds[method]
@@ -523,7 +524,8 @@ def main():
                                       "triangular solves",
                        "fp32_ic0_j8": "plain IC(0) (5-sweep fixed-point factor), FP32, 8 Jacobi sweeps per triangle",
                        "fp32_ic0": "plain IC(0), FP32 factor, exact triangular solves",
-                       "fp64_ic0": "plain IC(0), FP64, exact triangular solves"}[args.method],
+                       "fp64_ic0": "plain IC(0), FP64, exact triangular solves",
+                       "sa_amg": "smoothed-aggregation AMG V-cycle (FP64)"}[args.method],
             "data": "synthetic (seeded GRF diffusion, held-out seeds 2000+)",
             "config": {"workload": "grf_diffusion_512 pcg rtol1e-8", "method": args.method, "grid": N_GRID,
                        "corr": CORR, "parallelism": f"replicas x{world}", "l2": "flushed (512 MB write) before every step"},

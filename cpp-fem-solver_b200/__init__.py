@@ -115,7 +115,7 @@ EXPORTS = [
     "b2s_gen_elasticity_q1", "b2s_gen_grf_diffusion", "b2s_gen_uniform", "b2s_learner_create",
     "b2s_learner_destroy", "b2s_learner_load", "b2s_learner_save", "b2s_learner_params", "b2s_learner_step",
     "b2s_pc_create_learned", "b2s_dot_noalloc", "b2s_dense_bf16_device",
-    "b2s_learner_set_loss",
+    "b2s_learner_set_loss", "b2s_sor", "b2s_sor_device",
 ]
 
 
@@ -190,6 +190,8 @@ def lib():
     f("b2s_dot_noalloc", i32, vp, vp, u64, vp, vp)
     f("b2s_dense_bf16_device", i32, vp, u64, i32, i32, vp, vp, vp, vp)
     f("b2s_learner_set_loss", i32, vp, i32)
+    f("b2s_sor", i32, vp, vp, i32, f64, f64, i32, _f64p, _f64p, C.POINTER(Stats))
+    f("b2s_sor_device", i32, vp, vp, i32, f64, f64, i32, vp, vp, C.POINTER(Stats))
     _lib = L
     return L
 
@@ -476,6 +478,15 @@ def solve(ctx: Context, A, b, method=PCG, pc=None, raise_on_error=True, **opts):
     rc = fn(ctx.h, A.h, pc.h if pc is not None else None, method, C.byref(o), _f64(b), x, C.byref(st))
     if rc != OK and raise_on_error:
         ctx.check(rc, "solve")
+    return x, st.as_dict()
+
+
+def sor(ctx: Context, A, b, omega, tol=1e-10, maxit=2000, red_black=False):
+    """x, stats = sor(ctx, A, b, omega, tol, maxit, red_black): SMatrix::sor / sor_rb."""
+    st = Stats()
+    x = np.zeros(A.n)
+    ctx.check(lib().b2s_sor(ctx.h, A.h, 1 if red_black else 0, float(omega), float(tol), int(maxit), _f64(b), x,
+                            C.byref(st)), "sor_rb" if red_black else "sor")
     return x, st.as_dict()
 
 

@@ -543,6 +543,19 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
 std::unique_ptr<PcImpl> make_pc_diag(b2s_ctx* ctx, const CsrDev& A);
 std::unique_ptr<PcImpl> make_pc_identity(uint64_t n);
 std::unique_ptr<PcImpl> make_pc_ic0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);
+
+// The reference's colouring and colour-by-colour renumbering of a square
+// CSR matrix (multicolour SSOR and red-black SOR): colour c owns the new rows
+// [h_cptr[c], h_cptr[c+1]); row ni of A2 is row perm[ni] of A with columns
+// new_id[] sorted; d2 its diagonal (MISSING_DIAG when absent or < 1e-300).
+struct RedBlack
+{
+    uint32_t n = 0, ncolor = 0;
+    std::vector<uint32_t> h_cptr, h_new_id;
+    DBuf<uint32_t> perm, new_id, rp2, ci2;
+    DBuf<double> v2, d2;
+};
+void build_redblack(b2s_ctx* ctx, const CsrDev& A, RedBlack& rb, const char* what);
 std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);
 std::unique_ptr<PcImpl> make_pc_ssor(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);
 std::unique_ptr<PcImpl> make_pc_amg_csr(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);

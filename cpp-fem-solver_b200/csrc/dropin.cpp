@@ -321,4 +321,32 @@ namespace sparse
     {
         return detail::solve_csr(A, b, B2S_BICGSTAB, nullptr, &solveM, 30, tol, max_iter);
     }
+
+    namespace detail
+    {
+        std::tuple<std::vector<double>, int> sor_csr(const SMatrix& A, const std::vector<double>& b, int red_black,
+                                                     double omega, double tol, int max_iter)
+        {
+            if (A.rows() != A.cols())
+                throw std::invalid_argument(red_black ? "red-black SOR needs a square matrix" : "SOR needs a square matrix");
+            if (A.cols() != b.size()) throw std::invalid_argument("SOR: matrix columns differ from vector length");
+            std::vector<double> x(A.rows(), 0.0);
+            b2s_stats st;
+            check(b2s_sor(context(), A.device(), red_black, omega, tol, max_iter, b.data(), x.data(), &st),
+                  red_black ? "red-black SOR" : "SOR");
+            return {x, st.it};
+        }
+    }
+
+    std::tuple<std::vector<double>, int> SMatrix::sor(const SMatrix& A, const std::vector<double>& b, double omega,
+                                                      double tol, int max_iter)
+    {
+        return detail::sor_csr(A, b, 0, omega, tol, max_iter);
+    }
+
+    std::tuple<std::vector<double>, int> SMatrix::sor_rb(const SMatrix& A, const std::vector<double>& b, double omega,
+                                                         double tol, int max_iter)
+    {
+        return detail::sor_csr(A, b, 1, omega, tol, max_iter);
+    }
 }

@@ -232,6 +232,49 @@ struct PcSSOR final : PcImpl
 
 }  // namespace
 
+// The reference's colouring of the graph of A + A^T (two colours by BFS when
+// it is bipartite, greedy colours otherwise), rows renumbered colour by
+// colour, and A2 = P A P^T with each row's columns sorted in the new
+// numbering (array.cpp:2947-3040 for SSOR, 3946-4110 for red-black SOR).
+void build_redblack(b2s_ctx* ctx, const CsrDev& A, RedBlack& rb, const char* what)
+{
+    const uint32_t n = A.n;
+    rb.n = n;
+    std::vector<int> colour;
+    A.host_pattern(ctx);
+    colour_graph(n, A.h_rp, A.h_ci, colour);
+    uint32_t nc = 0;
+    for (uint32_t i = 0; i < n; ++i) nc = std::max<uint32_t>(nc, (uint32_t)colour[i] + 1);
+    rb.ncolor = nc;
+    rb.h_cptr.assign(nc + 1, 0);
+    for (uint32_t i = 0; i < n; ++i) rb.h_cptr[colour[i] + 1]++;
+    for (uint32_t c = 0; c < nc; ++c) rb.h_cptr[c + 1] += rb.h_cptr[c];
+    rb.h_new_id.resize(n);
+    std::vector<uint32_t> off(rb.h_cptr.begin(), rb.h_cptr.end() - 1), perm(n);
+    for (uint32_t i = 0; i < n; ++i) rb.h_new_id[i] = off[colour[i]]++;
+    for (uint32_t i = 0; i < n; ++i) perm[rb.h_new_id[i]] = i;
+    rb.perm = upload(ctx, perm.data(), n);
+    rb.new_id = upload(ctx, rb.h_new_id.data(), n);
+    std::vector<uint32_t> rp2(n + 1, 0);
+    for (uint32_t ni = 0; ni < n; ++ni) rp2[ni + 1] = rp2[ni] + (A.h_rp[perm[ni] + 1] - A.h_rp[perm[ni]]);
+    rb.rp2 = upload(ctx, rp2.data(), n + 1);
+    rb.ci2.alloc(A.nnz ? A.nnz : 1);
+    rb.v2.alloc(A.nnz ? A.nnz : 1);
+    rb.d2.alloc(n ? n : 1);
+    DBuf<int> bad(1);
+    const int big = 0x7fffffff;
+    h2d(ctx, bad.p, &big, sizeof(int));
+    if (n)
+        B2S_LAUNCH(ctx, k_perm_fill, stream_grid(ctx, n), kThreads, 0, n, A.rp.p, A.ci.p, A.v.p, rb.perm.p,
+                   rb.new_id.p, rb.rp2.p, rb.ci2.p, rb.v2.p, rb.d2.p, bad.p);
+    int h = big;
+    d2h(ctx, &h, bad.p, sizeof(int));
+    sync(ctx);
+    if (h != big)
+        fail(B2S_MISSING_DIAG, std::string(what) + " failed: missing nonzero diagonal (renumbered row " +
+                                   std::to_string(h) + ")");
+}
+
 std::unique_ptr<PcImpl> make_pc_ssor(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o)
 {
     need(A.n == A.m, B2S_SHAPE, "SSOR needs a square matrix");
@@ -240,40 +283,19 @@ std::unique_ptr<PcImpl> make_pc_ssor(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     const uint32_t n = A.n;
     pc->n = n;
     pc->omega = o.omega;
-    std::vector<int> colour;
-    A.host_pattern(ctx);
-    colour_graph(n, A.h_rp, A.h_ci, colour);
-    uint32_t nc = 0;
-    for (uint32_t i = 0; i < n; ++i) nc = std::max<uint32_t>(nc, (uint32_t)colour[i] + 1);
-    pc->ncolor = nc;
-    pc->h_cptr.assign(nc + 1, 0);
-    for (uint32_t i = 0; i < n; ++i) pc->h_cptr[colour[i] + 1]++;
-    for (uint32_t c = 0; c < nc; ++c) pc->h_cptr[c + 1] += pc->h_cptr[c];
-    pc->h_new_id.resize(n);
-    std::vector<uint32_t> off(pc->h_cptr.begin(), pc->h_cptr.end() - 1), perm(n);
-    for (uint32_t i = 0; i < n; ++i) pc->h_new_id[i] = off[colour[i]]++;
-    for (uint32_t i = 0; i < n; ++i) perm[pc->h_new_id[i]] = i;
-    pc->perm = upload(ctx, perm.data(), n);
-    pc->new_id = upload(ctx, pc->h_new_id.data(), n);
-    std::vector<uint32_t> rp2(n + 1, 0);
-    for (uint32_t ni = 0; ni < n; ++ni) rp2[ni + 1] = rp2[ni] + (A.h_rp[perm[ni] + 1] - A.h_rp[perm[ni]]);
-    pc->rp2 = upload(ctx, rp2.data(), n + 1);
-    pc->ci2.alloc(A.nnz ? A.nnz : 1);
-    pc->v2.alloc(A.nnz ? A.nnz : 1);
-    pc->d2.alloc(n ? n : 1);
+    RedBlack rb;
+    build_redblack(ctx, A, rb, "SSOR/red-black");
+    pc->ncolor = rb.ncolor;
+    pc->h_cptr = std::move(rb.h_cptr);
+    pc->h_new_id = std::move(rb.h_new_id);
+    pc->perm = std::move(rb.perm);
+    pc->new_id = std::move(rb.new_id);
+    pc->rp2 = std::move(rb.rp2);
+    pc->ci2 = std::move(rb.ci2);
+    pc->v2 = std::move(rb.v2);
+    pc->d2 = std::move(rb.d2);
     pc->w.alloc(n ? n : 1);
     pc->z2.alloc(n ? n : 1);
-    DBuf<int> bad(1);
-    const int big = 0x7fffffff;
-    h2d(ctx, bad.p, &big, sizeof(int));
-    if (n)
-        B2S_LAUNCH(ctx, k_perm_fill, stream_grid(ctx, n), kThreads, 0, n, A.rp.p, A.ci.p, A.v.p, pc->perm.p,
-                   pc->new_id.p, pc->rp2.p, pc->ci2.p, pc->v2.p, pc->d2.p, bad.p);
-    int h = big;
-    d2h(ctx, &h, bad.p, sizeof(int));
-    sync(ctx);
-    if (h != big) fail(B2S_MISSING_DIAG, "SSOR/red-black failed: missing nonzero diagonal (renumbered row " +
-                                             std::to_string(h) + ")");
     return pc;
 }
 

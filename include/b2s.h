@@ -311,6 +311,20 @@ b2s_status b2s_solve(b2s_ctx* ctx, const b2s_csr* A, b2s_pc* pc, b2s_method meth
                      const double* b, double* x, b2s_stats* stats);
 b2s_status b2s_solve_device(b2s_ctx* ctx, const b2s_csr* A, b2s_pc* pc, b2s_method method,
                             const b2s_solve_opts* opts, const double* d_b, double* d_x, b2s_stats* stats);
+/* SMatrix::sor (array.cpp:3843-3945), red_black = 0, and SMatrix::sor_rb
+ * (array.cpp:3946-4189), red_black = 1: SOR sweeps from x0 = 0 until
+ * ||b - A x|| / ||b|| < tol or maxit sweeps; stats->it is the reference's
+ * returned index of the last sweep.  Natural order follows the reference's
+ * sequential Gauss-Seidel order (one sync-free traversal per sweep);
+ * red-black uses its colouring and renumbering.  Iterates equal the
+ * reference's bit for bit.  Errors as the reference: a non-square matrix
+ * (B2S_SHAPE), 0 < omega < 2 violated (B2S_INVALID_ARG, checked after a zero
+ * right-hand side returns x = 0), a missing or zero diagonal
+ * (B2S_MISSING_DIAG), NaN/Inf in the residual (B2S_DIVERGED). */
+b2s_status b2s_sor(b2s_ctx* ctx, const b2s_csr* A, int red_black, double omega, double tol, int maxit, const double* b,
+                   double* x, b2s_stats* stats);
+b2s_status b2s_sor_device(b2s_ctx* ctx, const b2s_csr* A, int red_black, double omega, double tol, int maxit,
+                          const double* d_b, double* d_x, b2s_stats* stats);
 /* Same on a BAIJ operator (BlockMatrix::gmres; block PCG is an extension). */
 b2s_status b2s_solve_baij(b2s_ctx* ctx, const b2s_baij* A, b2s_pc* pc, b2s_method method, const b2s_solve_opts* opts,
                           const double* b, double* x, b2s_stats* stats);

@@ -112,6 +112,11 @@ namespace sparse
             static std::tuple<std::vector<double>, int> gmres(const SMatrix& A, const std::vector<double>& b,
                                                               const Precond& solveM, int restart, double tol = 1e-10,
                                                               int max_iter = 2000);
+            // SOR, natural order and red-black (array.hpp:351-365)
+            static std::tuple<std::vector<double>, int> sor(const SMatrix& A, const std::vector<double>& b,
+                                                            double omega, double tol = 1e-10, int max_iter = 2000);
+            static std::tuple<std::vector<double>, int> sor_rb(const SMatrix& A, const std::vector<double>& b,
+                                                               double omega, double tol = 1e-10, int max_iter = 2000);
             // extensions with a functor preconditioner
             static std::tuple<std::vector<double>, int> pcg(const SMatrix& A, const std::vector<double>& b,
                                                             const Precond& solveM, double tol = 1e-10,

@@ -311,6 +311,7 @@ class Ref(_Lib):
         self._spmv = self._f("spmv", None, vp, f64p, f64p)
         self._dot = self._f("dot", f64, f64p, f64p, u64)
         self._solve = self._f("solve", i32, vp, i32, cp, i32, f64, i32, f64p, f64p, ip, cp, i32)
+        self._sor = self._f("sor", i32, vp, i32, f64, f64, i32, f64p, f64p, ip, cp, i32)
         self._pc_create = self._f("pc_create", vp, vp, cp, f64, cp, i32)
         self._gmres_pc = self._f("gmres_pc", i32, vp, vp, i32, f64, i32, f64p, f64p, ip, cp, i32)
         self._ic0_export = self._f("ic0_export", i32, vp, u32p, vp, vp, vp, vp, vp, vp, vp)
@@ -363,6 +364,14 @@ class Ref(_Lib):
         x = np.zeros(A.n, np.float64)
         it, err = C.c_int(0), C.create_string_buffer(512)
         st = self._solve(A.h, method, precond.encode(), restart, tol, maxit, _f64(b), x, C.byref(it), err, 512)
+        self._check(st, err)
+        return x, it.value
+
+    def sor(self, A, b, omega, tol=1e-10, maxit=2000, red_black=False):
+        """SMatrix::sor / sor_rb of the compiled reference: (x, it)."""
+        x = np.zeros(A.n, np.float64)
+        it, err = C.c_int(0), C.create_string_buffer(512)
+        st = self._sor(A.h, 1 if red_black else 0, omega, tol, maxit, _f64(b), x, C.byref(it), err, 512)
         self._check(st, err)
         return x, it.value
 

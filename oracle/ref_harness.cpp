@@ -173,6 +173,19 @@ int ref_solve(void* A, int method, const char* precond, int restart, double tol,
     });
 }
 
+// ---------------- SOR solvers (array.cpp:3843-4189) ----------------
+int ref_sor(void* A, int red_black, double omega, double tol, int maxit, const double* b, double* x, int* it,
+            char* err, int errlen)
+{
+    const SMatrix& M = *static_cast<SMatrix*>(A);
+    return guarded(err, errlen, [&] {
+        std::vector<double> bv(b, b + M.rows());
+        auto res = red_black ? SMatrix::sor_rb(M, bv, omega, tol, maxit) : SMatrix::sor(M, bv, omega, tol, maxit);
+        std::memcpy(x, std::get<0>(res).data(), sizeof(double) * M.rows());
+        *it = std::get<1>(res);
+    });
+}
+
 // ---------------- Preconditioner factories (array.cpp:2450-3398) ----------------
 void* ref_pc_create(void* A, const char* kind, double omega, char* err, int errlen)
 {

@@ -120,6 +120,20 @@ int main()
         auto [x2, it2] = SMatrix::gmres(A, b, p, 30, 1e-8, 2000);
         CHECK(relres(A, x2, b) < 2e-8, "gmres %s", p);
     }
+    // SOR, natural order and red-black (array.hpp:351-365)
+    {
+        SMatrix S = poisson2d(24);
+        std::vector<double> bs(S.rows());
+        for (uint32_t i = 0; i < S.rows(); ++i) bs[i] = 2.0 * drand(i + 7) - 1.0;
+        auto [xs, its] = SMatrix::sor(S, bs, 1.6, 1e-8, 5000);
+        CHECK(relres(S, xs, bs) < 1e-8, "sor relres");
+        auto [xr, itr] = SMatrix::sor_rb(S, bs, 1.6, 1e-8, 5000);
+        CHECK(relres(S, xr, bs) < 1e-8, "sor_rb relres");
+        std::printf("[sor] it=%d  [sor_rb] it=%d\n", its, itr);
+        bool bad = false;
+        try { SMatrix::sor(S, bs, 2.5); } catch (const std::invalid_argument&) { bad = true; }
+        CHECK(bad, "sor with omega >= 2 must throw std::invalid_argument");
+    }
     // exceptions
     bool threw = false;
     try { SMatrix::pcg(A, b, "bogus"); } catch (const std::invalid_argument&) { threw = true; }

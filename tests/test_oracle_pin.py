@@ -154,3 +154,45 @@ def test_levels_restatement(orc):
     assert np.array_equal(lev, i + j)
     levu, nlu = orc.levels(n, rp, ci, upper=True)
     assert nlu == nl and np.array_equal(levu, (8 - i) + (8 - j))
+
+
+def _sor_restated(n, rp, ci, v, b, omega, tol, maxit):
+    """SMatrix::sor (array.cpp:3843-3945) restated row by row in Python floats."""
+    diag = np.zeros(n)
+    for i in range(n):
+        for p in range(rp[i], rp[i + 1]):
+            if ci[p] == i:
+                diag[i] = v[p]
+    x = [0.0] * n
+    normb = float(np.sqrt(sum(bi * bi for bi in b)))
+    it_end = 0
+    for it in range(maxit):
+        for i in range(n):
+            sigma = float(b[i])
+            for p in range(rp[i], rp[i + 1]):
+                j = int(ci[p])
+                if j != i:
+                    sigma -= float(v[p]) * x[j]
+            x[i] += omega * (sigma / float(diag[i]) - x[i])
+        err = 0.0
+        for i in range(n):
+            ri = float(b[i])
+            for p in range(rp[i], rp[i + 1]):
+                ri -= float(v[p]) * x[int(ci[p])]
+            err += ri * ri
+        it_end = it
+        if np.sqrt(err) / normb < tol:
+            break
+    return np.array(x), it_end
+
+
+def test_sor_reference_pinned(ref):
+    """The compiled reference's SOR against a row-by-row restatement (one
+    OpenMP thread, so the residual sums in row order): same iterates, same
+    count."""
+    import problems as P
+    n, rp, ci, v = P.convdiff2d(8)
+    b = np.random.default_rng(4).uniform(-1, 1, n)
+    x, it = ref.sor(ref.csr(n, n, rp, ci, v), b, 1.3, 1e-9, 500)
+    xr, itr = _sor_restated(n, rp, ci, v, b, 1.3, 1e-9, 500)
+    assert it == itr and np.array_equal(x, xr)
