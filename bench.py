@@ -230,6 +230,107 @@ def run_kernel(args):
     return 0
 
 
+# ---------------------------------------------------------------- config suite
+
+def run_suite(args):
+    """The other configurations of the benchmark definition (C1-C4), one JSON
+    line per solver: GPU setup and solve time (CUDA events on the library's
+    stream, inputs resident, best of `reps` after one warm-up), iterations and
+    the FP64 true residual; beside it the reference's solver on the host cores
+    (`oracle/_ref`, one run) where it has the same solver.  Documentation of
+    the other configurations, not the benchmark line."""
+    import torch
+    b2s = load_b2s()
+    ctx = b2s.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    dev = torch.device("cuda", 0)
+    ref = None
+    if not args.no_ref:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle
+            ref = oracle.Ref()
+            ref.set_threads(os.cpu_count() or 1)
+        except Exception as e:  # the compiled reference did not travel
+            print(json.dumps({"suite": "reference unavailable", "why": str(e)[:200]}), flush=True)
+
+    def gpu(A, n, kind, method, tol, maxit, reps=3, pco=None, so=None):
+        bt = torch.from_numpy(b2s.uniform(7, n)).to(dev)
+        best = None
+        for r in range(reps + 1):
+            xt = torch.zeros(n, dtype=torch.float64, device=dev)
+            torch.cuda.synchronize()
+            e0, em, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record(stream)
+            M = b2s.Precond(ctx, A, kind, **(pco or {})) if kind is not None else None
+            em.record(stream)
+            st = b2s.solve_device(ctx, A, bt.data_ptr(), xt.data_ptr(), method, M, tol=tol, maxit=maxit,
+                                  **(so or {}))
+            e1.record(stream)
+            e1.synchronize()
+            del M
+            if r == 0:
+                continue
+            cur = {"setup_ms": round(e0.elapsed_time(em), 3), "solve_ms": round(em.elapsed_time(e1), 3),
+                   "iterations": st["iterations"], "relres_true": st["relres_true"], "status": st["status"]}
+            cur["total_ms"] = round(cur["setup_ms"] + cur["solve_ms"], 3)
+            if best is None or cur["total_ms"] < best["total_ms"]:
+                best = cur
+        return best
+
+    def cpu(rp, ci, v, n, method, pc, tol, maxit):
+        if ref is None:
+            return None
+        Ar = ref.csr(n, n, rp, ci, v)
+        t0 = time.perf_counter()
+        _, it = ref.solve(Ar, method, pc, b2s.uniform(7, n), tol, maxit)
+        return {"ms": round((time.perf_counter() - t0) * 1e3, 1), "it": it, "cores": os.cpu_count()}
+
+    def emit(config, solver, g, r):
+        line = {"config": config, "solver": solver, "gpu": g, "reference_cpu": r}
+        if isinstance(r, dict) and g:
+            line["speedup"] = round(r["ms"] / g["total_ms"], 1)
+        print(json.dumps(line), flush=True)
+
+    c = "C1 poisson2d 256^2, rtol 1e-8"
+    n, rp, ci, v = b2s.gen_poisson2d(256)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    emit(c, "pcg+diag", gpu(A, n, b2s.PC_DIAG, b2s.PCG, 1e-8, 20000), cpu(rp, ci, v, n, 0, "diag", 1e-8, 20000))
+    emit(c, "pcg+ic0", gpu(A, n, b2s.PC_IC0, b2s.PCG, 1e-8, 20000), cpu(rp, ci, v, n, 0, "ic", 1e-8, 20000))
+    del A
+
+    c = "C2 poisson3d 128^3, rtol 1e-10"
+    n, rp, ci, v = b2s.gen_poisson3d(128)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    emit(c, "pcg+sa_amg", gpu(A, n, b2s.PC_SA_AMG, b2s.PCG, 1e-10, 2000),
+         "not run: the reference's aggregation does not coarsen this operator")
+    emit(c, "pcg+ilu0", gpu(A, n, b2s.PC_ILU0, b2s.PCG, 1e-10, 2000, reps=1),
+         cpu(rp, ci, v, n, 0, "ilu", 1e-10, 2000))
+    del A
+
+    c = "C3 convdiff3d 96^3, rtol 1e-8"
+    n, rp, ci, v = b2s.gen_convdiff3d(96)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    emit(c, "bicgstab+ilu0", gpu(A, n, b2s.PC_ILU0, b2s.BICGSTAB, 1e-8, 2000),
+         cpu(rp, ci, v, n, 1, "ilu", 1e-8, 2000))
+    emit(c, "gmres30+ilu0", gpu(A, n, b2s.PC_ILU0, b2s.GMRES, 1e-8, 2000, so={"restart": 30}),
+         cpu(rp, ci, v, n, 2, "ilu", 1e-8, 2000))
+    emit(c, "fgmres30+ilu0_fp32+ir", gpu(A, n, b2s.PC_ILU0, b2s.FGMRES, 1e-8, 2000, pco={"precision": b2s.FP32},
+                                        so={"restart": 30, "ir_steps": 5, "ir_inner_tol": 1e-4}), None)
+    del A
+
+    c = "C4 elasticity Q1 64^3 elements (3x3 BAIJ), rtol 1e-8"
+    nbr, rp, ci, v = b2s.gen_elasticity_q1(64)
+    B = b2s.BAIJ(ctx, 3, nbr, nbr, rp, ci, v)
+    for name, kind, prec in (("bilu0_fp64", b2s.PC_BILU0, b2s.FP64), ("bilu0_fp32", b2s.PC_BILU0, b2s.FP32),
+                             ("bsa_amg_fp64", b2s.PC_BSA_AMG, b2s.FP64)):
+        emit(c, f"cg+{name}", gpu(B, 3 * nbr, kind, b2s.PCG, 1e-8, 5000, reps=1, pco={"precision": prec}),
+             "not run: the reference's block matrix has GMRES only")
+    del B
+    ctx.close()
+    return 0
+
+
 # ---------------------------------------------------------------- reference arm
 
 def run_reference(args):
@@ -284,7 +385,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel", default=None, choices=sorted(KERNELS),
                     help="run one hot kernel only (for profilers), not the benchmark")
+    ap.add_argument("--suite", action="store_true",
+                    help="time the other configurations (C1-C4), one JSON line each; not the benchmark")
+    ap.add_argument("--no-ref", action="store_true", help="--suite without the reference's CPU timings")
     args = ap.parse_args()
+    if args.suite:
+        return run_suite(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.kernel:
