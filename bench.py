@@ -326,6 +326,14 @@ def run_suite(args):
                              ("bsa_amg_fp64", b2s.PC_BSA_AMG, b2s.FP64)):
         emit(c, f"cg+{name}", gpu(B, 3 * nbr, kind, b2s.PCG, 1e-8, 5000, reps=1, pco={"precision": prec}),
              "not run: the reference's block matrix has GMRES only")
+    # the reference's block solver: GMRES(30) with block ILU(0)
+    r = None
+    if ref is not None:
+        Br = ref.blk(3, nbr, nbr, rp, ci, v)
+        t0 = time.perf_counter()
+        _, it = ref.blk_gmres(Br, b2s.uniform(7, 3 * nbr), "blockilu", 1e-8, 1000, 30)
+        r = {"ms": round((time.perf_counter() - t0) * 1e3, 1), "it": it, "cores": os.cpu_count()}
+    emit(c, "gmres30+bilu0_fp64", gpu(B, 3 * nbr, b2s.PC_BILU0, b2s.GMRES, 1e-8, 1000, reps=1, so={"restart": 30}), r)
     del B
     ctx.close()
     return 0

@@ -1375,18 +1375,16 @@ b2s_status b2s_solve(b2s_ctx* ctx, const b2s_csr* A, b2s_pc* pc, b2s_method meth
         Operator op;
         op.csr = &A->d;
         op.n = n;
-        b2s_status st = B2S_OK;
         try
         {
             solve_common(ctx, op, pc, method, opts, db.p, dx.p, stats);
         }
-        catch (const Error& e)
+        catch (const Error&)
         {
-            d2h(ctx, x, dx.p, dx.bytes());
+            d2h(ctx, x, dx.p, dx.bytes());  // the last iterate goes back with the error status
             sync(ctx);
             throw;
         }
-        (void)st;
         d2h(ctx, x, dx.p, dx.bytes());
         sync(ctx);
     });

@@ -357,14 +357,20 @@ std::unique_ptr<PcImpl> make_pc_bilu0(b2s_ctx* ctx, const BaijDev& A, const b2s_
     std::thread th([&] {
         try
         {
-            compute_levels(nb, urp.data(), uci.data(), false, ulev);
-            if (chunked)
-            {
-                lplan = plan_chunks(nb, lrp.data(), lci.data(), true, 0, vs, vs, 8, kChunkSmemBudget, (uint32_t)bs,
-                                    &llev);
-                uplan = plan_chunks(nb, urp.data(), uci.data(), false, (uint32_t)bv, vs, vs, 8, kChunkSmemBudget,
-                                    (uint32_t)bs, &ulev);
-            }
+            // the two triangles' plans run side by side
+            plan_parallel(2, 2, [&](uint32_t side, unsigned) {
+                if (side == 0)
+                {
+                    if (chunked)
+                        lplan = plan_chunks(nb, lrp.data(), lci.data(), true, 0, vs, vs, 8, kChunkSmemBudget,
+                                            (uint32_t)bs, &llev);
+                    return;
+                }
+                compute_levels(nb, urp.data(), uci.data(), false, ulev);
+                if (chunked)
+                    uplan = plan_chunks(nb, urp.data(), uci.data(), false, (uint32_t)bv, vs, vs, 8, kChunkSmemBudget,
+                                        (uint32_t)bs, &ulev);
+            });
         }
         catch (...)
         {

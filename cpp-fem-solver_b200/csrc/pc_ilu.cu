@@ -980,14 +980,20 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
                 }
                 return;
             }
-            compute_levels(n, ha.up_rp.data(), ha.up_ci.data(), false, ha.up_level);
-            if (ha.chunked)
-            {
-                ha.lo_plan = plan_chunks(n, hrp.data(), hci.data(), true, 1, vs, vs, 8, kChunkSmemBudget, 1,
-                                         &pc->fwd.h_level);
-                ha.up_plan = plan_chunks(n, ha.up_rp.data(), ha.up_ci.data(), false, 1, vs, vs, 8, kChunkSmemBudget, 1,
-                                         &ha.up_level);
-            }
+            // the two triangles' plans run side by side
+            plan_parallel(2, 2, [&](uint32_t side, unsigned) {
+                if (side == 0)
+                {
+                    if (ha.chunked)
+                        ha.lo_plan = plan_chunks(n, hrp.data(), hci.data(), true, 1, vs, vs, 8, kChunkSmemBudget, 1,
+                                                 &pc->fwd.h_level);
+                    return;
+                }
+                compute_levels(n, ha.up_rp.data(), ha.up_ci.data(), false, ha.up_level);
+                if (ha.chunked)
+                    ha.up_plan = plan_chunks(n, ha.up_rp.data(), ha.up_ci.data(), false, 1, vs, vs, 8,
+                                             kChunkSmemBudget, 1, &ha.up_level);
+            });
         }
         catch (...)
         {
@@ -1125,14 +1131,20 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     ha.th = std::thread([&ha, &lrp, &lci, &urp, &uci, &pc, n, vs] {
         try
         {
-            compute_levels(n, urp.data(), uci.data(), false, ha.up_level);
-            if (ha.chunked)
-            {
-                ha.lo_plan = plan_chunks(n, lrp.data(), lci.data(), true, 0, vs, vs, 8, kChunkSmemBudget, 1,
-                                         &pc->fwd.h_level);
-                ha.up_plan = plan_chunks(n, urp.data(), uci.data(), false, 1, vs, vs, 8, kChunkSmemBudget, 1,
-                                         &ha.up_level);
-            }
+            // the two triangles' plans run side by side
+            plan_parallel(2, 2, [&](uint32_t side, unsigned) {
+                if (side == 0)
+                {
+                    if (ha.chunked)
+                        ha.lo_plan = plan_chunks(n, lrp.data(), lci.data(), true, 0, vs, vs, 8, kChunkSmemBudget, 1,
+                                                 &pc->fwd.h_level);
+                    return;
+                }
+                compute_levels(n, urp.data(), uci.data(), false, ha.up_level);
+                if (ha.chunked)
+                    ha.up_plan = plan_chunks(n, urp.data(), uci.data(), false, 1, vs, vs, 8, kChunkSmemBudget, 1,
+                                             &ha.up_level);
+            });
         }
         catch (...)
         {

@@ -39,7 +39,14 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
 #include <cstring>
+#include <exception>
+#include <new>
+#include <mutex>
+#include <stdexcept>
+#include <thread>
 #include <vector>
 
 #ifdef __CUDACC__
@@ -188,15 +195,130 @@ inline void strict_transpose(uint32_t n, const uint32_t* rp, const uint32_t* ci,
             if (lower ? ci[p] < i : ci[p] > i) tci[off[ci[p]]++] = i;
 }
 
+// Run f(c, worker) for c in [0, count) on up to 16 host threads; chunks are
+// handed out one at a time.  The first exception thrown by any call is
+// rethrown after every worker has stopped.
+template <class F>
+inline void plan_parallel(uint32_t count, unsigned max_workers, F&& f)
+{
+    unsigned hw = std::thread::hardware_concurrency();
+    unsigned nt = std::min(std::min(hw ? hw : 1u, max_workers), count ? count : 1u);
+    std::atomic<uint32_t> next{0};
+    std::atomic<bool> failed{false};
+    std::exception_ptr err;
+    std::mutex m;
+    auto work = [&](unsigned t) {
+        try
+        {
+            for (uint32_t c; !failed.load(std::memory_order_relaxed) && (c = next.fetch_add(1)) < count;) f(c, t);
+        }
+        catch (...)
+        {
+            std::lock_guard<std::mutex> g(m);
+            if (!err) err = std::current_exception();
+            failed = true;
+        }
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t)
+    {
+        try
+        {
+            th.emplace_back(work, t);
+        }
+        catch (...)
+        {
+            break;  // fewer workers when a thread cannot start
+        }
+    }
+    work(0);
+    for (std::thread& x : th) x.join();
+    if (err) std::rethrow_exception(err);
+}
+
+// A chunk's range of positions in processing order and its counts.
+struct ChunkSpan
+{
+    uint32_t pos, end, nd, ns, nl, max_rows;
+};
+
+// Pass 1 of plan_chunks: grow each chunk over consecutive rows (in processing
+// order) while its shared-memory footprint fits.  A dependency on a row of an
+// earlier chunk costs a slot the first time the chunk meets it.  False when a
+// single row does not fit.
+template <bool LOWER>
+inline bool plan_grow(uint32_t n, const uint32_t* rp, const uint32_t* ci, uint32_t dv, uint32_t vs, uint32_t xs,
+                      uint32_t rs, uint32_t budget, uint32_t bs, std::vector<ChunkSpan>& span)
+{
+    const uint64_t bv = (uint64_t)bs * bs;
+    const uint64_t row_fixed = (uint64_t)vs * dv + 10 + (uint64_t)bs * (xs + rs);
+    const uint64_t per_dep = (uint64_t)vs * bv + 2, per_slot = (uint64_t)bs * xs + 4;
+    std::vector<uint32_t> stamp(n, 0);  // chunk id + 1 when j already has a slot in the chunk
+    std::vector<uint32_t> fresh;        // rows stamped by the row being tried
+    const uint32_t slack = 16 * 10;
+    uint32_t pos = 0;
+    while (pos < n)
+    {
+        uint64_t bytes = slack;
+        uint32_t end = pos, nd = 0, ns = 0;
+        // rows of the chunk so far: [pos, r) for lower, (r, n-1-pos] for upper
+        const uint32_t edge = LOWER ? pos : n - 1 - pos;
+        const uint32_t tag = (uint32_t)span.size() + 1;
+        while (end < n)
+        {
+            const uint32_t r = LOWER ? end : n - 1 - end;
+            uint32_t ndep = 0, nnew = 0;
+            fresh.clear();
+            for (uint32_t p = rp[r]; p < rp[r + 1]; ++p)
+            {
+                const uint32_t j = ci[p];
+                if (LOWER ? j >= r : j <= r) continue;
+                ++ndep;
+                const bool inside = LOWER ? j >= edge : j <= edge;
+                if (!inside && stamp[j] != tag)
+                {
+                    stamp[j] = tag;
+                    fresh.push_back(j);
+                    ++nnew;
+                }
+            }
+            const uint64_t b = row_fixed + per_dep * ndep + per_slot * nnew;
+            const bool fits = bytes + b <= budget && end - pos + 1 <= kChunkMaxRows && nd + ndep <= kChunkMaxDeps &&
+                              ns + nnew <= kChunkMaxSlots;
+            if (!fits)
+            {
+                for (uint32_t j : fresh) stamp[j] = 0;  // the row starts the next chunk
+                if (end == pos) return false;
+                break;
+            }
+            bytes += b;
+            nd += ndep;
+            ns += nnew;
+            ++end;
+        }
+        span.push_back({pos, end, nd, ns, 0, 0});
+        pos = end;
+    }
+    return true;
+}
+
 // Plan the chunks of a triangle with (block) CSR pattern rp/ci (dependency
 // entries are j < i for lower, j > i for upper; other entries are ignored).
 // vs, xs, rs: element sizes of values, solution and right-hand side the chunks
 // are sized for; bs: block size; dv: divisor values per row (0 for a unit
 // triangle, 1 for a scalar divisor, bs*bs for an inverse block).
 // glev: the rows' global levels when the caller has them (compute_levels).
+//
+// Three passes: (1) serially, grow each chunk over consecutive rows while its
+// shared-memory footprint fits (this fixes the chunk boundaries, dependency
+// and slot counts); (2) per chunk in parallel, order the rows by global
+// level; (3) after a prefix sum of the blob sizes, per chunk in parallel,
+// write the metadata blob, the slot rows and the value sources.  Slots are
+// numbered per chunk in the order of first need, so the plan does not depend
+// on the number of threads.
 inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci, bool lower, uint32_t dv, uint32_t vs,
                              uint32_t xs, uint32_t rs, uint32_t budget = kChunkSmemBudget, uint32_t bs = 1,
-                             const std::vector<uint32_t>* glev_in = nullptr)
+                             const std::vector<uint32_t>* glev_in = nullptr, unsigned max_workers = 16)
 {
     ChunkPlan P;
     P.n = n;
@@ -213,152 +335,147 @@ inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci,
     std::vector<uint32_t> glev_own;
     if (!glev_in) compute_levels(n, rp, ci, lower, glev_own);
     const std::vector<uint32_t>& glev = glev_in ? *glev_in : glev_own;
-    std::vector<uint32_t> stamp(n, 0);     // chunk id + 1 when j already has a slot in the chunk
-    std::vector<uint32_t> slot_of(n, 0);   // slot of j in the chunk that stamped it
-    std::vector<uint32_t> llev(n, 0);      // local level
-    std::vector<uint32_t> pos_of(n, 0);    // position inside its chunk
-    std::vector<uint64_t> perm_at(n, 0);   // byte offset of the row's perm entry in P.meta
-    std::vector<uint8_t> publish(n, 0);
-    std::vector<uint32_t> rows, cnt;
-    const uint32_t slack = 16 * 10;
-    uint32_t pos = 0, cid = 0;
-    while (pos < n)
-    {
-        // ---- grow the chunk while it fits
-        uint64_t bytes = slack;
-        uint32_t end = pos, nd = 0, ns = 0;
-        const uint32_t first = lower ? pos : n - 1 - pos;  // first row in processing order
-        const uint32_t tag = cid + 1;
-        while (end < n)
-        {
-            const uint32_t r = lower ? end : n - 1 - end;
-            uint32_t ndep = 0, nnew = 0;
-            for (uint32_t p = rp[r]; p < rp[r + 1]; ++p)
-            {
-                const uint32_t j = ci[p];
-                if (!is_dep(r, j)) continue;
-                ++ndep;
-                const bool inside = lower ? j >= pos : j <= first;
-                if (!inside && stamp[j] != tag) ++nnew;
-            }
-            const uint64_t b = (uint64_t)vs * (ndep * bv + dv) + 2ull * ndep + 10 + (uint64_t)bs * (xs + rs) +
-                               (uint64_t)nnew * (bs * xs + 4);
-            const bool fits = bytes + b <= budget && end - pos + 1 <= kChunkMaxRows && nd + ndep <= kChunkMaxDeps &&
-                              ns + nnew <= kChunkMaxSlots;
-            if (!fits)
-            {
-                if (end == pos) return P;  // a single row does not fit: ok stays false
-                break;
-            }
-            bytes += b;
-            nd += ndep;
-            ns += nnew;
-            for (uint32_t p = rp[r]; p < rp[r + 1]; ++p)
-            {
-                const uint32_t j = ci[p];
-                if (!is_dep(r, j)) continue;
-                const bool inside = lower ? j >= pos : j <= first;
-                if (!inside) stamp[j] = tag;
-            }
-            ++end;
-        }
-        const uint32_t nr = end - pos;
-        const uint32_t lo = lower ? pos : n - end;
-        // ---- the chunk's levels: its distinct global levels, compressed
-        rows.clear();
+    // ---- pass 1: chunk boundaries, dependency entries and slots
+    std::vector<ChunkSpan> span;
+    const bool grown = lower ? plan_grow<true>(n, rp, ci, dv, vs, xs, rs, budget, bs, span)
+                             : plan_grow<false>(n, rp, ci, dv, vs, xs, rs, budget, bs, span);
+    if (!grown) return P;  // a single row does not fit a chunk: ok stays false
+    const uint32_t nchunks = (uint32_t)span.size();
+    // ---- pass 2: each chunk's rows by global level (order[pos..end): rows by position)
+    std::vector<uint32_t> order(n), llev(n), pos_of(n);
+    plan_parallel(nchunks, max_workers, [&](uint32_t c, unsigned) {
+        ChunkSpan& S = span[c];
         uint32_t gmin = ~0u, gmax = 0;
-        for (uint32_t t = pos; t < end; ++t)
+        for (uint32_t t = S.pos; t < S.end; ++t)
         {
             const uint32_t r = lower ? t : n - 1 - t;
             gmin = std::min(gmin, glev[r]);
             gmax = std::max(gmax, glev[r]);
-            rows.push_back(r);
         }
-        cnt.assign(gmax - gmin + 1, 0);
-        for (uint32_t r : rows) cnt[glev[r] - gmin] = 1;
+        // the chunk's distinct global levels, compressed
+        std::vector<uint32_t> cnt(gmax - gmin + 1, 0);
+        for (uint32_t t = S.pos; t < S.end; ++t) cnt[glev[lower ? t : n - 1 - t] - gmin] = 1;
         uint32_t nl = 0;
-        for (uint32_t& c : cnt) c = c ? nl++ : 0u;  // global level -> chunk level
-        for (uint32_t r : rows) llev[r] = cnt[glev[r] - gmin];
+        for (uint32_t& x : cnt) x = x ? nl++ : 0u;  // global level -> chunk level
+        for (uint32_t t = S.pos; t < S.end; ++t)
+        {
+            const uint32_t r = lower ? t : n - 1 - t;
+            llev[r] = cnt[glev[r] - gmin];
+        }
         // counting sort by level, stable in processing order
-        cnt.assign(nl + 1, 0);
-        for (uint32_t r : rows) cnt[llev[r] + 1]++;
-        for (uint32_t l = 0; l < nl; ++l) cnt[l + 1] += cnt[l];
-        for (uint32_t l = 0; l < nl; ++l) P.max_level_rows = std::max(P.max_level_rows, cnt[l + 1] - cnt[l]);
-        std::vector<uint32_t> sorted(nr), off(cnt.begin(), cnt.end() - 1);
-        for (uint32_t r : rows) sorted[off[llev[r]]++] = r;
-        for (uint32_t t = 0; t < nr; ++t) pos_of[sorted[t]] = t;
-        // ---- emit the metadata blob
-        const MetaLayout M = meta_layout(nr, nd, nl);
-        const uint64_t mbase = P.meta.size();
-        P.meta.resize(mbase + M.bytes, 0);
-        uint8_t* mb = P.meta.data() + mbase;
+        std::vector<uint32_t> off(nl + 1, 0);
+        for (uint32_t t = S.pos; t < S.end; ++t) off[llev[lower ? t : n - 1 - t] + 1]++;
+        uint32_t mx = 0;
+        for (uint32_t l = 0; l < nl; ++l)
+        {
+            mx = std::max(mx, off[l + 1]);
+            off[l + 1] += off[l];
+        }
+        for (uint32_t t = S.pos; t < S.end; ++t)
+        {
+            const uint32_t r = lower ? t : n - 1 - t;
+            const uint32_t q = off[llev[r]]++;
+            order[S.pos + q] = r;
+            pos_of[r] = q;
+        }
+        S.nl = nl;
+        S.max_rows = mx;
+    });
+    // ---- blob offsets
+    P.desc.resize(nchunks);
+    uint64_t meta_bytes = 0, ndeps = 0, nslots = 0;
+    for (uint32_t c = 0; c < nchunks; ++c)
+    {
+        const ChunkSpan& S = span[c];
+        const uint32_t nr = S.end - S.pos;
+        ChunkDesc& D = P.desc[c];
+        D = ChunkDesc{};
+        D.lo = lower ? S.pos : n - S.end;
+        D.nr = nr;
+        D.nd = S.nd;
+        D.nl = S.nl;
+        D.ns = S.ns;
+        D.meta = (uint32_t)(meta_bytes / 16);
+        D.slot = (uint32_t)nslots;
+        D.dep = (uint32_t)ndeps;
+        D.v64 = (uint32_t)P.v64_units;
+        D.v32 = (uint32_t)P.v32_units;
+        meta_bytes += meta_layout(nr, S.nd, S.nl).bytes;
+        ndeps += S.nd;
+        nslots += S.ns;
+        P.v64_units += (al16((uint64_t)S.nd * bv * 8) + al16((uint64_t)nr * dv * 8)) / 16;
+        P.v32_units += (al16((uint64_t)S.nd * bv * 4) + al16((uint64_t)nr * dv * 4)) / 16;
+        P.max_level_rows = std::max(P.max_level_rows, S.max_rows);
+    }
+    P.meta.assign(meta_bytes ? meta_bytes : 16, 0);
+    std::vector<uint64_t> rec_at(n);  // byte offset of each row's position record in P.meta
+    P.src.resize(ndeps);
+    P.slot_row.resize(nslots);
+    // ---- pass 3: metadata blobs, slot rows, value sources
+    // per worker: slot + 1 of row j in the current chunk, 0 when none.  calloc
+    // leaves the pages untouched until a chunk's slot rows reach them.
+    struct Scratch
+    {
+        uint32_t* slot_of = nullptr;
+        ~Scratch() { std::free(slot_of); }
+    };
+    std::vector<Scratch> scratch(std::max(1u, std::min(max_workers, 64u)));
+    plan_parallel(nchunks, (unsigned)scratch.size(), [&](uint32_t c, unsigned w) {
+        const ChunkSpan& S = span[c];
+        const ChunkDesc& D = P.desc[c];
+        uint32_t*& slot_of = scratch[w].slot_of;
+        if (!slot_of && !(slot_of = (uint32_t*)std::calloc(n, sizeof(uint32_t)))) throw std::bad_alloc();
+        const MetaLayout M = meta_layout(D.nr, D.nd, D.nl);
+        uint8_t* mb = P.meta.data() + (uint64_t)D.meta * 16;
         auto put16 = [&](uint32_t off_bytes, uint32_t idx, uint32_t val) {
             const uint16_t v16 = (uint16_t)val;
             std::memcpy(mb + off_bytes + 2ull * idx, &v16, 2);
         };
-        ChunkDesc D{};
-        D.lo = lo;
-        D.nr = nr;
-        D.nd = nd;
-        D.nl = nl;
-        D.meta = (uint32_t)(mbase / 16);
-        D.slot = (uint32_t)P.slot_row.size();
-        D.dep = (uint32_t)P.src.size();
-        uint32_t e = 0, s = 0;
-        std::vector<uint32_t>& slot_rows = P.slot_row;
-        for (uint32_t t = 0; t < nr; ++t)
+        uint32_t e = 0, s = 0, l = 0;
+        for (uint32_t t = 0; t < D.nr; ++t)
         {
-            const uint32_t r = sorted[t];
-            put16(M.rec, 4 * t, r - lo);
+            const uint32_t r = order[S.pos + t];
+            while (l <= llev[r]) put16(M.slv, l++, t);
+            put16(M.rec, 4 * t, r - D.lo);
             put16(M.rec, 4 * t + 1, e);
-            perm_at[r] = mbase + M.rec + 8ull * t;
+            rec_at[r] = (uint64_t)D.meta * 16 + M.rec + 8ull * t;
             for (uint32_t p = rp[r]; p < rp[r + 1]; ++p)
             {
                 const uint32_t j = ci[p];
                 if (!is_dep(r, j)) continue;
                 uint32_t m;
-                if (j >= lo && j < lo + nr)
+                if (j >= D.lo && j < D.lo + D.nr)
                     m = pos_of[j];
                 else
                 {
-                    // number the slots in the order of first need
                     if (slot_of[j] == 0)
                     {
+                        if (s >= D.ns) throw std::logic_error("plan_chunks: slot count");
                         slot_of[j] = s + 1;
-                        slot_rows.push_back(j);
-                        publish[j] = 1;
+                        P.slot_row[D.slot + s] = j;
                         ++s;
                     }
                     m = 0x8000u | (slot_of[j] - 1);
                 }
+                if (e >= D.nd) throw std::logic_error("plan_chunks: dependency count");
                 put16(M.slc, e, m);
-                P.src.push_back(p);
+                P.src[D.dep + e] = p;
                 ++e;
             }
             put16(M.rec, 4 * t + 2, e);
         }
-        for (uint32_t l = 0; l <= nl; ++l) put16(M.slv, l, cnt[l]);
-        D.ns = s;
-        D.v64 = (uint32_t)P.v64_units;
-        D.v32 = (uint32_t)P.v32_units;
-        P.v64_units += (al16((uint64_t)nd * bv * 8) + al16((uint64_t)nr * dv * 8)) / 16;
-        P.v32_units += (al16((uint64_t)nd * bv * 4) + al16((uint64_t)nr * dv * 4)) / 16;
-        P.desc.push_back(D);
-        // slot numbering reuses slot_of; clear it for the rows of this chunk's slots
-        for (uint32_t q = D.slot; q < D.slot + s; ++q) slot_of[P.slot_row[q]] = 0;
-        pos = end;
-        ++cid;
+        put16(M.slv, D.nl, D.nr);
+        for (uint32_t q = 0; q < s; ++q) slot_of[P.slot_row[D.slot + q]] = 0;
+        if (e != D.nd || s != D.ns) throw std::logic_error("plan_chunks: chunk counts");
+    });
+    // rows read by another chunk publish a ready flag (bit 15 of the record's local-row field)
+    for (uint32_t j : P.slot_row)
+    {
+        uint16_t v16;
+        std::memcpy(&v16, P.meta.data() + rec_at[j], 2);
+        v16 |= 0x8000u;
+        std::memcpy(P.meta.data() + rec_at[j], &v16, 2);
     }
-    // rows read by another chunk publish a ready flag
-    for (uint32_t r = 0; r < n; ++r)
-        if (publish[r])
-        {
-            uint16_t v16;
-            std::memcpy(&v16, P.meta.data() + perm_at[r], 2);
-            v16 |= 0x8000u;
-            std::memcpy(P.meta.data() + perm_at[r], &v16, 2);
-        }
-    if (P.meta.empty()) P.meta.resize(16, 0);
     P.ok = true;
     return P;
 }
