@@ -2,11 +2,11 @@
 // blockMatrix.hpp:455-623).
 //
 // Setup: the block pattern is split into L (J < I) and U (J >= I), the level
-// sets of L's dependency DAG are computed on the device, and the factor runs
-// one launch per level with one thread per block row, repeating the
-// reference's block arithmetic exactly (left sum L_IJ U_JK found by binary
-// search, right multiplication by inv(U_KK), two-pointer update of row I's U
-// blocks, Gauss-Jordan inverse of the diagonal block) -- bit-equal factors.
+// sets of L's dependency DAG are computed, and the factor runs one launch per
+// level with one warp per block row, repeating the reference's block
+// arithmetic exactly (left sum L_IJ U_JK found by binary search, right
+// multiplication by inv(U_KK), update of row I's U blocks, Gauss-Jordan
+// inverse of the diagonal block) -- bit-equal factors.
 // Apply: block forward substitution and block back substitution times the
 // cached inverse, in FP64 or FP32: chunked (default, trsv_chunk.cuh), per
 // level or sync-free.
@@ -83,55 +83,84 @@ __device__ __forceinline__ uint32_t bfind(const uint32_t* rp, const uint32_t* ci
     return 0xFFFFFFFFu;
 }
 
-// block row I of the factor, blockMatrix.hpp:528-575
+// Block row I of the factor (blockMatrix.hpp:528-575), one warp per block
+// row of the level.  Lane e < BS*BS owns entry
+// (e / BS, e % BS) of the block L_IK being formed and accumulates it in the
+// reference's order (left products L_IJ U_JK by ascending J, then the right
+// multiplication by inv(U_KK)), so every entry is rounded exactly as in the
+// one-thread form.  The row update spreads row I's U blocks over the lanes:
+// each lane finds its block's column in row K by binary search and applies
+// the block product, which the reference applies in the same per-block
+// arithmetic.  Rows with at most kBiluPairRows L blocks look up all their
+// U_JK positions up front, in parallel, into shared memory.
+constexpr uint32_t kBiluPairRows = 32;
+
 template <int BS>
-__global__ void k_bilu0_level(const uint32_t* __restrict__ rows, uint32_t count, const uint32_t* __restrict__ Lrp,
-                              const uint32_t* __restrict__ Lci, double* Lv, const uint32_t* __restrict__ Urp,
-                              const uint32_t* __restrict__ Uci, double* Uv, const uint32_t* __restrict__ Udiag,
-                              double* inv, int* singular)
+__global__ void __launch_bounds__(kThreads) k_bilu0_level_warp(const uint32_t* __restrict__ rows, uint32_t count,
+                                                               const uint32_t* __restrict__ Lrp,
+                                                               const uint32_t* __restrict__ Lci, double* Lv,
+                                                               const uint32_t* __restrict__ Urp,
+                                                               const uint32_t* __restrict__ Uci, double* Uv,
+                                                               const uint32_t* __restrict__ Udiag, double* inv,
+                                                               int* singular)
 {
     constexpr int BV = BS * BS;
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
-    const uint32_t I = rows[t];
+    constexpr uint32_t NONE = 0xFFFFFFFFu;
+    __shared__ uint32_t spair[kThreads / 32][kBiluPairRows * (kBiluPairRows - 1) / 2];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= count) return;  // the whole warp
+    uint32_t* pair = spair[threadIdx.x >> 5];
+    const uint32_t I = rows[w];
     const uint32_t Ls = Lrp[I], Le = Lrp[I + 1], Us = Urp[I], Ue = Urp[I + 1];
-    for (uint32_t pL = Ls; pL < Le; ++pL)
+    const uint32_t m = Le - Ls;
+    const bool cached = m <= kBiluPairRows;
+    if (cached)
+        for (uint32_t a = 1; a < m; ++a)
+            for (uint32_t b = lane; b < a; b += 32) pair[a * (a - 1) / 2 + b] = bfind(Urp, Uci, Lci[Ls + b], Lci[Ls + a]);
+    __syncwarp();
+    const uint32_t e = lane < (uint32_t)BV ? lane : 0u;  // lanes past BV shadow entry 0
+    const int r = (int)e / BS, c = (int)e % BS;
+    for (uint32_t a = 0; a < m; ++a)
     {
-        const uint32_t K = Lci[pL];
-        double LIK[BV];
-        for (int k = 0; k < BV; ++k) LIK[k] = Lv[(size_t)pL * BV + k];
-        for (uint32_t q = Ls; q < pL; ++q)
+        const uint32_t pL = Ls + a, K = Lci[pL];
+        double lik = Lv[(size_t)pL * BV + e];
+        for (uint32_t b = 0; b < a; ++b)
         {
-            const uint32_t J = Lci[q];
-            const uint32_t pJK = bfind(Urp, Uci, J, K);
-            if (pJK != 0xFFFFFFFFu) blk_mma<BS>(&Lv[(size_t)q * BV], &Uv[(size_t)pJK * BV], LIK);
+            const uint32_t pJK = cached ? pair[a * (a - 1) / 2 + b] : bfind(Urp, Uci, Lci[Ls + b], K);
+            if (pJK == NONE) continue;
+            const double* A = Lv + (size_t)(Ls + b) * BV + r * BS;
+            const double* B = Uv + (size_t)pJK * BV + c;
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < BS; ++k) s += A[k] * B[k * BS];
+            lik -= s;
         }
-        blk_rmul<BS>(LIK, &inv[(size_t)K * BV]);
-        for (int k = 0; k < BV; ++k) Lv[(size_t)pL * BV + k] = LIK[k];
-        uint32_t pi = Us, pk = Urp[K];
-        const uint32_t ek = Urp[K + 1];
-        while (pi < Ue && pk < ek)
+        double s = 0.0;
+#pragma unroll
+        for (int k = 0; k < BS; ++k) s += __shfl_sync(0xffffffffu, lik, r * BS + k) * inv[(size_t)K * BV + k * BS + c];
+        lik = s;
+        if (lane < (uint32_t)BV) Lv[(size_t)pL * BV + e] = lik;
+        double Lb[BV];
+#pragma unroll
+        for (int q = 0; q < BV; ++q) Lb[q] = __shfl_sync(0xffffffffu, lik, q);
+        for (uint32_t pi = Us + lane; pi < Ue; pi += 32)
         {
-            const uint32_t ci_ = Uci[pi], ck = Uci[pk];
-            if (ci_ == ck)
-            {
-                blk_mma<BS>(LIK, &Uv[(size_t)pk * BV], &Uv[(size_t)pi * BV]);
-                ++pi;
-                ++pk;
-            }
-            else if (ci_ < ck)
-                ++pi;
-            else
-                ++pk;
+            const uint32_t pk = bfind(Urp, Uci, K, Uci[pi]);
+            if (pk != NONE) blk_mma<BS>(Lb, &Uv[(size_t)pk * BV], &Uv[(size_t)pi * BV]);
         }
+        __syncwarp();  // L_IK and row I's U blocks are visible to every lane
     }
-    double Mi[BV];
-    if (!blk_inv<BS>(&Uv[(size_t)Udiag[I] * BV], Mi))
+    if (lane == 0)
     {
-        atomicMin(singular, (int)I);
-        for (int k = 0; k < BV; ++k) Mi[k] = 0.0;
+        double Mi[BV];
+        if (!blk_inv<BS>(&Uv[(size_t)Udiag[I] * BV], Mi))
+        {
+            atomicMin(singular, (int)I);
+            for (int k = 0; k < BV; ++k) Mi[k] = 0.0;
+        }
+        for (int k = 0; k < BV; ++k) inv[(size_t)I * BV + k] = Mi[k];
     }
-    for (int k = 0; k < BV; ++k) inv[(size_t)I * BV + k] = Mi[k];
 }
 
 // block forward / backward substitution rows (blockMatrix.hpp:584-621)
@@ -299,8 +328,9 @@ void bilu0_factor(b2s_ctx* ctx, PcBILU0& pc, int* singular)
     for (uint32_t l = 0; l < pc.sl.nlev; ++l)
     {
         const uint32_t a = pc.sl.h_ptr[l], cnt = pc.sl.h_ptr[l + 1] - a;
-        B2S_LAUNCH(ctx, k_bilu0_level<BS>, (cnt + kThreads - 1) / kThreads, kThreads, 0, pc.sl.rows.p + a, cnt,
-                   pc.L.rp.p, pc.L.ci.p, pc.L.v.p, pc.U.rp.p, pc.U.ci.p, pc.U.v.p, pc.udiag.p, pc.inv.p, singular);
+        B2S_LAUNCH(ctx, k_bilu0_level_warp<BS>, (cnt + kThreads / 32 - 1) / (kThreads / 32), kThreads, 0,
+                   pc.sl.rows.p + a, cnt, pc.L.rp.p, pc.L.ci.p, pc.L.v.p, pc.U.rp.p, pc.U.ci.p, pc.U.v.p,
+                   pc.udiag.p, pc.inv.p, singular);
     }
 }
 

@@ -37,6 +37,50 @@ def test_bilu0_bit_exact(b2s, ctx, orc, bs, trsv):
     assert np.array_equal(M.apply(r), po.apply(r))
 
 
+def _bilu0_factor_equal(M, e):
+    for what, keys in (("bilu0.L", ("Lrp", "Lci", "Lv")), ("bilu0.U", ("Urp", "Uci", "Uv"))):
+        got = M.export(what)
+        assert all(np.array_equal(g, e[k]) for g, k in zip(got, keys)), what
+    _, ud, inv = M.export("bilu0.inv")
+    assert np.array_equal(ud, e["Udiag"]) and np.array_equal(inv, e["inv_diag"])
+
+
+def test_bilu0_factor_elasticity_bit_exact(b2s, ctx, orc):
+    """27-point block rows (13 lower blocks): the warp-per-row factor with its
+    U_JK lookups cached in shared memory gives the reference's factors."""
+    nbr, rp, ci, v = b2s.gen_elasticity_q1(6)
+    B = b2s.BAIJ(ctx, 3, nbr, nbr, rp, ci, v)
+    Bo = orc.blk(3, nbr, nbr, rp, ci, v)
+    _bilu0_factor_equal(b2s.Precond(ctx, B, b2s.PC_BILU0), orc.blk_ilu0_export(orc.blk_pc(Bo, "ilu0"), 3))
+
+
+@pytest.mark.parametrize("bs", [2, 4])
+def test_bilu0_factor_wide_rows_bit_exact(b2s, ctx, orc, bs):
+    """Rows of up to 40 lower blocks (more than the 32 whose lookups are
+    cached): the lookups run inline and the factors still match."""
+    nb, w = 96, 40
+    rng = np.random.default_rng(11 + bs)
+    rp, ci, vals = [0], [], []
+    for i in range(nb):
+        cols = [j for j in range(max(0, i - w), min(nb, i + 6)) if j == i or rng.random() < 0.85]
+        for j in cols:
+            blk = rng.uniform(-1.0, 1.0, (bs, bs))
+            if j == i:
+                blk += np.eye(bs) * (4.0 * w)
+            vals.append(blk.ravel())
+        ci += cols
+        rp.append(len(ci))
+    rp, ci, v = np.array(rp, np.uint32), np.array(ci, np.uint32), np.concatenate(vals)
+    assert max(int(np.sum(ci[rp[i]:rp[i + 1]] < i)) for i in range(nb)) > 32
+    B = b2s.BAIJ(ctx, bs, nb, nb, rp, ci, v)
+    Bo = orc.blk(bs, nb, nb, rp, ci, v)
+    M = b2s.Precond(ctx, B, b2s.PC_BILU0)
+    po = orc.blk_pc(Bo, "ilu0")
+    _bilu0_factor_equal(M, orc.blk_ilu0_export(po, bs))
+    r = b2s.uniform(3, nb * bs)
+    assert np.array_equal(M.apply(r), po.apply(r))
+
+
 def test_bilu0_elasticity(b2s, ctx, orc):
     nbr, rp, ci, v = b2s.gen_elasticity_q1(8)
     B = b2s.BAIJ(ctx, 3, nbr, nbr, rp, ci, v)
