@@ -302,8 +302,9 @@ def run_suite(args):
     c = "C2 poisson3d 128^3, rtol 1e-10"
     n, rp, ci, v = b2s.gen_poisson3d(128)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
-    emit(c, "pcg+sa_amg", gpu(A, n, b2s.PC_SA_AMG, b2s.PCG, 1e-10, 2000),
-         "not run: the reference's aggregation does not coarsen this operator")
+    for prec, pname in ((b2s.FP64, "fp64"), (b2s.FP32, "fp32")):
+        emit(c, f"pcg+sa_amg_{pname}", gpu(A, n, b2s.PC_SA_AMG, b2s.PCG, 1e-10, 2000, pco={"precision": prec}),
+             "not run: the reference's aggregation does not coarsen this operator")
     emit(c, "pcg+ilu0", gpu(A, n, b2s.PC_ILU0, b2s.PCG, 1e-10, 2000, reps=1),
          cpu(rp, ci, v, n, 0, "ilu", 1e-10, 2000))
     del A
@@ -323,7 +324,7 @@ def run_suite(args):
     nbr, rp, ci, v = b2s.gen_elasticity_q1(64)
     B = b2s.BAIJ(ctx, 3, nbr, nbr, rp, ci, v)
     for name, kind, prec in (("bilu0_fp64", b2s.PC_BILU0, b2s.FP64), ("bilu0_fp32", b2s.PC_BILU0, b2s.FP32),
-                             ("bsa_amg_fp64", b2s.PC_BSA_AMG, b2s.FP64)):
+                             ("bsa_amg_fp64", b2s.PC_BSA_AMG, b2s.FP64), ("bsa_amg_fp32", b2s.PC_BSA_AMG, b2s.FP32)):
         emit(c, f"cg+{name}", gpu(B, 3 * nbr, kind, b2s.PCG, 1e-8, 5000, reps=1, pco={"precision": prec}),
              "not run: the reference's block matrix has GMRES only")
     # the reference's block solver: GMRES(30) with block ILU(0)

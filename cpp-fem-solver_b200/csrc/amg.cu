@@ -939,12 +939,26 @@ struct Level
     uint32_t nrows = 0;
     bool has_p = false;
     DBuf<double> tmp, r, rc, ec, sol;  // V-cycle work (rc / ec sized for the next level)
+    DBuf<float> A32, P32, R32, dinv32;  // FP32 copies of the values (precision FP32)
 };
+
+__global__ void k_amg_to_f32(const double* __restrict__ a, float* __restrict__ b, uint64_t n)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+static void amg_to_f32(b2s_ctx* ctx, const double* a, DBuf<float>& b, uint64_t n)
+{
+    b.alloc(n ? n : 1);
+    if (n) B2S_LAUNCH(ctx, k_amg_to_f32, stream_grid(ctx, n), kThreads, 0, a, b.p, n);
+}
 
 struct PcAMG final : PcImpl
 {
     int bs = 1;
     bool ref_coarse = false;
+    bool fp32 = false;  // V-cycle reads FP32 copies of A, P, R and D^-1 (FP64 arithmetic and vectors)
     int aggregation = 0;  // b2s_pc_opts::amg_aggregation
     std::vector<std::unique_ptr<Level>> lv;
     std::unique_ptr<BaijDev> fine_copy;  // BS=1 copy of a CSR operator
@@ -963,10 +977,19 @@ struct PcAMG final : PcImpl
             B2S_LAUNCH(ctx, k_dense_solve, 1, 32, 0, dense.p, sz, ref_coarse ? 1 : 0, piv.p, rhs, sol, done);
             return;
         }
-        B2S_LAUNCH(ctx, (k_smooth0<BS, double>), g, kThreads, 0, L.nrows, L.dinv.p, rhs, sol, done);
-        baij_matvec(ctx, *L.A, sol, L.tmp.p, done);
+        auto mv = [&](const BaijDev& M, const DBuf<float>& v32, const double* x, double* y) {
+            if (fp32)
+                baij_matvec_f32(ctx, M, v32.p, x, y, done);
+            else
+                baij_matvec(ctx, M, x, y, done);
+        };
+        if (fp32)
+            B2S_LAUNCH(ctx, (k_smooth0<BS, float>), g, kThreads, 0, L.nrows, L.dinv32.p, rhs, sol, done);
+        else
+            B2S_LAUNCH(ctx, (k_smooth0<BS, double>), g, kThreads, 0, L.nrows, L.dinv.p, rhs, sol, done);
+        mv(*L.A, L.A32, sol, L.tmp.p);
         B2S_LAUNCH(ctx, k_sub, gd, kThreads, 0, ndof, rhs, L.tmp.p, L.r.p, done);
-        baij_matvec(ctx, L.R, L.r.p, L.rc.p, done);
+        mv(L.R, L.R32, L.r.p, L.rc.p);
         const uint64_t nc = (uint64_t)L.R.nbr * BS;
         if (l + 1 < (int)lv.size() - 1)
             vcycle<BS>(ctx, l + 1, L.rc.p, L.ec.p, done);
@@ -975,10 +998,13 @@ struct PcAMG final : PcImpl
             B2S_LAUNCH(ctx, k_zero, stream_grid(ctx, nc), kThreads, 0, nc, L.ec.p, done);
             vcycle<BS>(ctx, l + 1, L.rc.p, L.ec.p, done);
         }
-        baij_matvec(ctx, L.P, L.ec.p, L.tmp.p, done);
+        mv(L.P, L.P32, L.ec.p, L.tmp.p);
         B2S_LAUNCH(ctx, k_add, gd, kThreads, 0, ndof, L.tmp.p, sol, done);
-        baij_matvec(ctx, *L.A, sol, L.tmp.p, done);
-        B2S_LAUNCH(ctx, (k_jacobi<BS, double>), g, kThreads, 0, L.nrows, L.dinv.p, rhs, L.tmp.p, sol, done);
+        mv(*L.A, L.A32, sol, L.tmp.p);
+        if (fp32)
+            B2S_LAUNCH(ctx, (k_jacobi<BS, float>), g, kThreads, 0, L.nrows, L.dinv32.p, rhs, L.tmp.p, sol, done);
+        else
+            B2S_LAUNCH(ctx, (k_jacobi<BS, double>), g, kThreads, 0, L.nrows, L.dinv.p, rhs, L.tmp.p, sol, done);
     }
 
     void apply(b2s_ctx* ctx, const double* r, double* z, const int* done) override
@@ -1142,6 +1168,16 @@ void build_hierarchy(b2s_ctx* ctx, PcAMG& pc, const BaijDev& A0, int max_levels,
         B2S_LAUNCH(ctx, k_dense_from_baij<BS>, stream_grid(ctx, C.nrows), kThreads, 0, C.nrows, C.A->rp.p, C.A->ci.p,
                    C.A->v.p, pc.dense.p, pc.sz);
     B2S_LAUNCH(ctx, k_dense_factor, 1, kThreads, 0, pc.dense.p, pc.sz, pc.ref_coarse ? 1 : 0, pc.piv.p);
+    // FP32 copies of every operator the V-cycle multiplies by (the coarsest level is the dense LU, kept in FP64)
+    if (pc.fp32)
+        for (size_t k = 0; k + 1 < pc.lv.size(); ++k)
+        {
+            Level& L = *pc.lv[k];
+            amg_to_f32(ctx, L.A->v.p, L.A32, (uint64_t)L.A->nnzb * BV);
+            amg_to_f32(ctx, L.P.v.p, L.P32, (uint64_t)L.P.nnzb * BV);
+            amg_to_f32(ctx, L.R.v.p, L.R32, (uint64_t)L.R.nnzb * BV);
+            amg_to_f32(ctx, L.dinv.p, L.dinv32, (uint64_t)L.nrows * BV);
+        }
     sync(ctx);
 }
 
@@ -1158,6 +1194,7 @@ std::unique_ptr<PcImpl> build_amg(b2s_ctx* ctx, const BaijDev& A, const b2s_pc_o
     auto pc = std::make_unique<PcAMG>();
     pc->bs = A.bs;
     pc->ref_coarse = o.amg_ref_coarse != 0;
+    pc->fp32 = o.precision != B2S_FP64;
     pc->aggregation = o.amg_aggregation;
     pc->fine_copy = std::move(owned);
     const int max_levels = o.amg_max_levels > 0 ? o.amg_max_levels : 20;

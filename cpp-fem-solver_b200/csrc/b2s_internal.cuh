@@ -525,6 +525,9 @@ void fill(b2s_ctx* ctx, double* x, double v, uint64_t n);
 void copy(b2s_ctx* ctx, double* dst, const double* src, uint64_t n, const int* done = nullptr);
 // BAIJ matvec (baij.cu)
 void baij_matvec(b2s_ctx* ctx, const BaijDev& A, const double* x, double* y, const int* done = nullptr);
+// the same product with A's pattern and FP32 values v32 (FP64 arithmetic)
+void baij_matvec_f32(b2s_ctx* ctx, const BaijDev& A, const float* v32, const double* x, double* y,
+                     const int* done = nullptr);
 // row partition for staged kernels (csr.cu)
 void build_row_blocks(const uint32_t* rp, uint32_t nrows, uint32_t unit, uint32_t max_rows, uint32_t max_units,
                       std::vector<uint32_t>& out);

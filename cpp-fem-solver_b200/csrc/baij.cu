@@ -23,10 +23,12 @@ struct BaijCap
 
 constexpr int kBaijCtasPerSm = 4;
 
-template <int BS>
+// VT: stored value type (double, or float for the FP32 copies of the AMG
+// hierarchy); products and sums are FP64 either way.
+template <int BS, typename VT>
 __global__ void __launch_bounds__(kThreads, kBaijCtasPerSm)
     k_baij_warp(uint32_t nbr, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
-                const double* __restrict__ v, const double* __restrict__ x, double* __restrict__ y, const int* done)
+                const VT* __restrict__ v, const double* __restrict__ x, double* __restrict__ y, const int* done)
 {
     if (done && *done) return;
     constexpr int BV = BS * BS;
@@ -40,12 +42,12 @@ __global__ void __launch_bounds__(kThreads, kBaijCtasPerSm)
     double* P = sdot[wid];
     // one pass's operands in registers: its values and this lane's block column
     auto load_pass = [&](uint32_t base, uint32_t nb, double* tv, uint32_t& J) {
-        const double* vb = v + (size_t)base * BV;
+        const VT* vb = v + (size_t)base * BV;
 #pragma unroll
         for (int k = 0; k < PER; ++k)
         {
             const uint32_t q = k * 32 + lane;
-            tv[k] = q < nb * BV ? ld_stream(vb + q) : 0.0;
+            tv[k] = q < nb * BV ? (double)ld_stream(vb + q) : 0.0;
         }
         J = lane < nb ? ld_stream(ci + base + lane) : 0u;
     };
@@ -96,28 +98,35 @@ __global__ void __launch_bounds__(kThreads, kBaijCtasPerSm)
     }
 }
 
-template <int BS>
-static void launch_baij(b2s_ctx* ctx, const BaijDev& A, const double* x, double* y, const int* done)
+template <int BS, typename VT>
+static void launch_baij(b2s_ctx* ctx, const BaijDev& A, const VT* v, const double* x, double* y, const int* done)
 {
     constexpr int GR = 32 / BS;
     const uint32_t groups = (A.nbr + GR - 1) / GR;
     const uint32_t ctas = (groups + kThreads / 32 - 1) / (kThreads / 32);
     const uint32_t cap = (uint32_t)ctx->sm_count * kBaijCtasPerSm;
-    B2S_LAUNCH(ctx, k_baij_warp<BS>, ctas < cap ? ctas : cap, kThreads, 0, A.nbr, A.rp.p, A.ci.p, A.v.p, x, y, done);
+    B2S_LAUNCH(ctx, (k_baij_warp<BS, VT>), ctas < cap ? ctas : cap, kThreads, 0, A.nbr, A.rp.p, A.ci.p, v, x, y, done);
+}
+
+__device__ __forceinline__ void stage_vals(double* s, const double* g, uint32_t cnt) { stage_f64(s, g, cnt); }
+
+__device__ __forceinline__ void stage_vals(float* s, const float* g, uint32_t cnt)
+{
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) s[i] = __ldg(&g[i]);
 }
 
 // 1x1 blocks (the AMG hierarchies' operators, rows of 7 to 100+ entries): a CTA
 // stages a contiguous block range in shared memory and one thread per row sums it.
-template <int BS>
+template <int BS, typename VT>
 __global__ void __launch_bounds__(kThreads) k_baij_staged(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
-                                                          const double* __restrict__ v,
+                                                          const VT* __restrict__ v,
                                                           const uint32_t* __restrict__ blk_row,
                                                           const double* __restrict__ x, double* __restrict__ y,
                                                           const int* done)
 {
     if (done && *done) return;
     constexpr int BV = BS * BS, CAP = BaijCap<BS>::value;
-    __shared__ double sv[CAP * BV];
+    __shared__ VT sv[CAP * BV];
     __shared__ uint32_t sc[CAP];
     const uint32_t r0 = blk_row[blockIdx.x], r1 = blk_row[blockIdx.x + 1];
     const uint32_t p0 = __ldg(&rp[r0]), p1 = __ldg(&rp[r1]);
@@ -125,7 +134,7 @@ __global__ void __launch_bounds__(kThreads) k_baij_staged(const uint32_t* __rest
     const uint32_t nthr = (r1 - r0) * BS;
     if (cnt <= (uint32_t)CAP)
     {
-        stage_f64(sv, v + (size_t)p0 * BV, cnt * BV);
+        stage_vals(sv, v + (size_t)p0 * BV, cnt * BV);
         stage_u32(sc, ci + p0, cnt);
         __syncthreads();
         for (uint32_t t = threadIdx.x; t < nthr; t += blockDim.x)
@@ -137,10 +146,14 @@ __global__ void __launch_bounds__(kThreads) k_baij_staged(const uint32_t* __rest
             for (uint32_t k = a; k < b; ++k)
             {
                 const double* xj = x + (size_t)sc[k] * BS;
-                double xv[BS];
+                double xv[BS], brow[BS];
 #pragma unroll
-                for (int c = 0; c < BS; ++c) xv[c] = __ldg(&xj[c]);
-                yr += blk_row_dot<BS>(&sv[(size_t)k * BV + r * BS], xv);
+                for (int c = 0; c < BS; ++c)
+                {
+                    xv[c] = __ldg(&xj[c]);
+                    brow[c] = (double)sv[(size_t)k * BV + r * BS + c];
+                }
+                yr += blk_row_dot<BS>(brow, xv);
             }
             y[(size_t)br * BS + r] = yr;
         }
@@ -160,7 +173,7 @@ __global__ void __launch_bounds__(kThreads) k_baij_staged(const uint32_t* __rest
                 for (int c = 0; c < BS; ++c)
                 {
                     xv[c] = __ldg(&xj[c]);
-                    brow[c] = __ldg(&v[(size_t)k * BV + r * BS + c]);
+                    brow[c] = (double)__ldg(&v[(size_t)k * BV + r * BS + c]);
                 }
                 yr += blk_row_dot<BS>(brow, xv);
             }
@@ -170,17 +183,30 @@ __global__ void __launch_bounds__(kThreads) k_baij_staged(const uint32_t* __rest
 }
 
 
-void baij_matvec(b2s_ctx* ctx, const BaijDev& A, const double* x, double* y, const int* done)
+template <typename VT>
+static void baij_matvec_t(b2s_ctx* ctx, const BaijDev& A, const VT* v, const double* x, double* y, const int* done)
 {
     if (A.nbr == 0) return;
     switch (A.bs)
     {
-        case 1: B2S_LAUNCH(ctx, k_baij_staged<1>, A.nblk, kThreads, 0, A.rp.p, A.ci.p, A.v.p, A.blk_row.p, x, y, done); break;
-        case 2: launch_baij<2>(ctx, A, x, y, done); break;
-        case 3: launch_baij<3>(ctx, A, x, y, done); break;
-        case 4: launch_baij<4>(ctx, A, x, y, done); break;
+        case 1:
+            B2S_LAUNCH(ctx, (k_baij_staged<1, VT>), A.nblk, kThreads, 0, A.rp.p, A.ci.p, v, A.blk_row.p, x, y, done);
+            break;
+        case 2: launch_baij<2, VT>(ctx, A, v, x, y, done); break;
+        case 3: launch_baij<3, VT>(ctx, A, v, x, y, done); break;
+        case 4: launch_baij<4, VT>(ctx, A, v, x, y, done); break;
         default: fail(B2S_UNSUPPORTED, "block size must be 1..4");
     }
+}
+
+void baij_matvec(b2s_ctx* ctx, const BaijDev& A, const double* x, double* y, const int* done)
+{
+    baij_matvec_t<double>(ctx, A, A.v.p, x, y, done);
+}
+
+void baij_matvec_f32(b2s_ctx* ctx, const BaijDev& A, const float* v32, const double* x, double* y, const int* done)
+{
+    baij_matvec_t<float>(ctx, A, v32, x, y, done);
 }
 
 static uint32_t baij_cap(int bs)

@@ -133,6 +133,13 @@ __device__ __forceinline__ double ld_stream(const double* p)
     return v;
 }
 
+__device__ __forceinline__ float ld_stream(const float* p)
+{
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+
 __device__ __forceinline__ uint32_t ld_stream(const uint32_t* p)
 {
     uint32_t v;

@@ -140,8 +140,11 @@ typedef enum b2s_pc_kind
 typedef enum b2s_precision
 {
     B2S_FP64 = 0,
-    B2S_FP32 = 1, /* factors / hierarchy stored FP32, applied with FP32 accumulation */
-    B2S_BF16 = 2  /* AMG: BF16 fine-level operator storage, FP32 elsewhere */
+    B2S_FP32 = 1, /* IC(0)/ILU(0)/block ILU(0)/learned IC(0): factors stored FP32, solves
+                     accumulate in FP32; SA-AMG: FP32 copies of A, P, R and D^-1 on every level,
+                     FP64 vectors and arithmetic, the coarsest dense LU in FP64; the diagonal,
+                     block-Jacobi and SSOR preconditioners ignore it */
+    B2S_BF16 = 2  /* accepted and treated as B2S_FP32 (no BF16 storage path) */
 } b2s_precision;
 
 /* Triangular-solve schedule for IC(0)/ILU(0)/block ILU(0). */

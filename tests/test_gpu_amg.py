@@ -17,6 +17,10 @@ import problems as P
 pytestmark = pytest.mark.gpu
 
 
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
 def hier_cases(b2s):
     return {
         "bs1_poisson2d": (1,) + P.poisson2d(40),
@@ -102,3 +106,28 @@ def test_block_amg_elasticity_pcg(b2s, ctx):
     M = b2s.Precond(ctx, B, b2s.PC_BSA_AMG)
     x, st = b2s.solve(ctx, B, b, b2s.PCG, M, tol=1e-8, maxit=2000)
     assert st["status"] == 0 and st["relres_true"] < 2e-8
+
+
+@pytest.mark.parametrize("case", ["poisson3d", "elasticity"])
+def test_amg_fp32_values(b2s, ctx, case):
+    """precision=FP32 keeps FP32 copies of A, P, R and D^-1 on every level
+    (FP64 vectors and arithmetic): the V-cycle agrees with the FP64 one to
+    single-precision accuracy, and PCG reaches the same FP64-verified
+    tolerance within a couple of iterations of it."""
+    if case == "poisson3d":
+        n, rp, ci, v = b2s.gen_poisson3d(32)
+        A, kind = b2s.CSR(ctx, n, n, rp, ci, v), b2s.PC_SA_AMG
+    else:
+        nbr, rp, ci, v = b2s.gen_elasticity_q1(12)
+        A, kind, n = b2s.BAIJ(ctx, 3, nbr, nbr, rp, ci, v), b2s.PC_BSA_AMG, 3 * nbr
+    M64 = b2s.Precond(ctx, A, kind)
+    M32 = b2s.Precond(ctx, A, kind, precision=b2s.FP32)
+    r = b2s.uniform(4, n)
+    z64, z32 = M64.apply(r), M32.apply(r)
+    assert not np.array_equal(z32, z64)
+    assert rel(z32, z64) < 1e-5
+    b = b2s.uniform(1, n)
+    _, s64 = b2s.solve(ctx, A, b, b2s.PCG, M64, tol=1e-8, maxit=2000)
+    _, s32 = b2s.solve(ctx, A, b, b2s.PCG, M32, tol=1e-8, maxit=2000)
+    assert s32["status"] == 0 and s32["relres_true"] < 2e-8
+    assert abs(s32["iterations"] - s64["iterations"]) <= 2
