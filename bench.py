@@ -128,6 +128,7 @@ KERNELS = {
     "trsv_c2": "k_trsv_chunk: FP64 ILU(0) apply on the 128^3 Poisson matrix (C2)",
     "btrsv_c4": "k_btrsv_chunk: FP64 block ILU(0) apply on the Q1 elasticity matrix (C4, 64^3 elements)",
     "vcycle_c2": "SA-AMG V-cycle (k_jacobi, BAIJ matvecs, k_dense_solve) on C2",
+    "vcycle_c4": "block SA-AMG V-cycle on the Q1 elasticity matrix (C4, 64^3 elements, 3x3 blocks)",
     "dense_c5": "k_linear_tc<64,128>: the learned network's tcgen05 dense layer on the 512^2 grid's node states "
                 "(n=262144 rows, 64 -> 128)",
     "solve_c5": "one learned IC(0) PCG solve (8 Jacobi sweeps per triangle, fused iteration) on a 512^2 GRF system; "
@@ -202,6 +203,11 @@ def run_kernel(args):
             n, rp, ci, v = b2s.gen_poisson3d(128)
             A = b2s.CSR(ctx, n, n, rp, ci, v)
             M = b2s.Precond(ctx, A, b2s.PC_SA_AMG)
+        elif k == "vcycle_c4":
+            nbr, rp, ci, v = b2s.gen_elasticity_q1(64)
+            A = b2s.BAIJ(ctx, 3, nbr, nbr, rp, ci, v)
+            n = 3 * nbr
+            M = b2s.Precond(ctx, A, b2s.PC_BSA_AMG)
         else:
             raise SystemExit(f"unknown kernel {k}; one of {sorted(KERNELS)}")
         r = torch.rand(n, dtype=torch.float64, device=dev)

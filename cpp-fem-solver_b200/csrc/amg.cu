@@ -586,6 +586,104 @@ __global__ void k_mm_unique_fill(uint32_t nr, const uint32_t* __restrict__ off, 
     }
 }
 
+// Symbolic product, one warp per row i of C = A B: the distinct columns of
+// the row are collected in a per-warp open-addressing hash table in shared
+// memory (inserted with atomicCAS; the lanes take B's row entries in
+// parallel).  COUNT: cnt[i] = their number.  Otherwise they are written in
+// ascending order (rank sort, the columns being distinct) to cci[crp[i]...].
+// A row whose columns do not fit the table raises *overflow and writes
+// nothing; the caller then uses the sort-based symbolic product.
+constexpr uint32_t kMmHashBits = 9;
+constexpr uint32_t kMmHashSlots = 1u << kMmHashBits;  // per warp
+constexpr uint32_t kMmEmpty = 0xFFFFFFFFu;
+
+template <bool COUNT>
+__global__ void __launch_bounds__(kThreads) k_mm_hash(uint32_t nr, const uint32_t* __restrict__ arp,
+                                                      const uint32_t* __restrict__ aci,
+                                                      const uint32_t* __restrict__ brp,
+                                                      const uint32_t* __restrict__ bci, uint32_t* __restrict__ cnt,
+                                                      const uint32_t* __restrict__ crp, uint32_t* __restrict__ cci,
+                                                      int* overflow)
+{
+    __shared__ uint32_t table[kThreads / 32][kMmHashSlots];
+    __shared__ uint32_t list[COUNT ? 1 : kThreads / 32][COUNT ? 1 : kMmHashSlots];
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    uint32_t* T = table[wid];
+    if (COUNT && blockIdx.x == 0 && threadIdx.x == 0) cnt[nr] = 0;
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t i = blockIdx.x * (blockDim.x >> 5) + wid; i < nr; i += warps)
+    {
+        for (uint32_t s = lane; s < kMmHashSlots; s += 32) T[s] = kMmEmpty;
+        __syncwarp();
+        uint32_t added = 0;
+        bool full = false;
+        const uint32_t a1 = arp[i + 1];
+        for (uint32_t pa = arp[i]; pa < a1 && !full; ++pa)
+        {
+            const uint32_t k = aci[pa];
+            const uint32_t b1 = brp[k + 1];
+            for (uint32_t pb = brp[k] + lane; pb < b1; pb += 32)
+            {
+                const uint32_t j = bci[pb];
+                uint32_t h = (j * 2654435761u) >> (32 - kMmHashBits);
+                for (uint32_t probes = 0;; ++probes)
+                {
+                    if (probes == kMmHashSlots)
+                    {
+                        full = true;
+                        break;
+                    }
+                    const uint32_t old = atomicCAS(&T[h], kMmEmpty, j);
+                    if (old == kMmEmpty) ++added;
+                    if (old == kMmEmpty || old == j) break;
+                    h = (h + 1) & (kMmHashSlots - 1);
+                }
+            }
+        }
+        __syncwarp();
+        if (__any_sync(0xffffffffu, full))
+        {
+            if (lane == 0)
+            {
+                atomicExch(overflow, 1);
+                if (COUNT) cnt[i] = 0;
+            }
+            __syncwarp();
+            continue;
+        }
+        uint32_t tot = added;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+        if (COUNT)
+        {
+            if (lane == 0) cnt[i] = tot;
+        }
+        else
+        {
+            uint32_t* Lst = list[wid];
+            uint32_t base = 0;
+            for (uint32_t s0 = 0; s0 < kMmHashSlots; s0 += 32)
+            {
+                const uint32_t v = T[s0 + lane];
+                const bool has = v != kMmEmpty;
+                const uint32_t m = __ballot_sync(0xffffffffu, has);
+                if (has) Lst[base + __popc(m & ((1u << lane) - 1u))] = v;
+                base += __popc(m);
+            }
+            __syncwarp();
+            const uint32_t out = crp[i];
+            for (uint32_t a = lane; a < base; a += 32)
+            {
+                const uint32_t v = Lst[a];
+                uint32_t r = 0;
+                for (uint32_t b = 0; b < base; ++b) r += Lst[b] < v;
+                cci[out + r] = v;
+            }
+        }
+        __syncwarp();  // the table and list are reused by the next row
+    }
+}
+
 // C row i: every (pa, pb) product added into its column's block in the
 // reference's order (blk_matmul, blockMatrix.hpp:883-932)
 template <int BS>
@@ -695,29 +793,55 @@ void block_matmul(b2s_ctx* ctx, const BaijDev& A, const BaijDev& B, BaijDev& C)
     C.bs = BS;
     C.nbr = nr;
     C.nbc = B.nbc;
-    DBuf<uint32_t> cnt(nr + 1), off(nr + 1);
-    if (nr) B2S_LAUNCH(ctx, k_mm_ub, stream_grid(ctx, nr), kThreads, 0, nr, A.rp.p, A.ci.p, B.rp.p, cnt.p);
-    const uint32_t total = exclusive_scan(ctx, cnt.p, off.p, nr);
-    DBuf<uint32_t> cand(total ? total : 1), sorted(total ? total : 1);
-    if (nr) B2S_LAUNCH(ctx, k_mm_cand, stream_grid(ctx, nr), kThreads, 0, nr, A.rp.p, A.ci.p, B.rp.p, B.ci.p, off.p, cand.p);
-    if (total)
-    {
-        size_t bytes = 0;
-        B2S_CUDA(cub::DeviceSegmentedSort::SortKeys(nullptr, bytes, cand.p, sorted.p, (int64_t)total, (int64_t)nr, off.p,
-                                                    off.p + 1, ctx->stream));
-        DBuf<uint8_t> tmp(bytes ? bytes : 1);
-        B2S_CUDA(cub::DeviceSegmentedSort::SortKeys(tmp.p, bytes, cand.p, sorted.p, (int64_t)total, (int64_t)nr, off.p,
-                                                    off.p + 1, ctx->stream));
-        ctx->launches += 1;
-    }
-    if (nr) B2S_LAUNCH(ctx, k_mm_unique_count, stream_grid(ctx, nr), kThreads, 0, nr, off.p, sorted.p, cnt.p);
+    DBuf<uint32_t> cnt(nr + 1);
     C.rp.alloc(nr + 1);
-    const uint32_t nnz = exclusive_scan(ctx, cnt.p, C.rp.p, nr);
-    C.ci.alloc(nnz ? nnz : 1);
+    // symbolic: per-warp hash tables; rows too wide for them send the whole
+    // product to the candidate-sort path
+    DBuf<int> overflow(1);
+    B2S_CUDA(cudaMemsetAsync(overflow.p, 0, sizeof(int), ctx->stream));
+    const uint64_t hash_ctas = ((uint64_t)nr + kThreads / 32 - 1) / (kThreads / 32);
+    const unsigned hash_grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(hash_ctas, (uint64_t)ctx->sm_count * 8));
+    if (nr)
+        B2S_LAUNCH(ctx, k_mm_hash<true>, hash_grid, kThreads, 0, nr, A.rp.p, A.ci.p, B.rp.p, B.ci.p, cnt.p,
+                   (const uint32_t*)nullptr, (uint32_t*)nullptr, overflow.p);
+    uint32_t nnz = exclusive_scan(ctx, cnt.p, C.rp.p, nr);
+    int wide = 0;
+    d2h(ctx, &wide, overflow.p, sizeof(int));
+    sync(ctx);
+    if (!wide)
+    {
+        C.ci.alloc(nnz ? nnz : 1);
+        if (nr)
+            B2S_LAUNCH(ctx, k_mm_hash<false>, hash_grid, kThreads, 0, nr, A.rp.p, A.ci.p, B.rp.p, B.ci.p,
+                       (uint32_t*)nullptr, C.rp.p, C.ci.p, overflow.p);
+    }
+    else
+    {
+        DBuf<uint32_t> off(nr + 1);
+        if (nr) B2S_LAUNCH(ctx, k_mm_ub, stream_grid(ctx, nr), kThreads, 0, nr, A.rp.p, A.ci.p, B.rp.p, cnt.p);
+        const uint32_t total = exclusive_scan(ctx, cnt.p, off.p, nr);
+        DBuf<uint32_t> cand(total ? total : 1), sorted(total ? total : 1);
+        if (nr)
+            B2S_LAUNCH(ctx, k_mm_cand, stream_grid(ctx, nr), kThreads, 0, nr, A.rp.p, A.ci.p, B.rp.p, B.ci.p, off.p,
+                       cand.p);
+        if (total)
+        {
+            size_t bytes = 0;
+            B2S_CUDA(cub::DeviceSegmentedSort::SortKeys(nullptr, bytes, cand.p, sorted.p, (int64_t)total, (int64_t)nr,
+                                                        off.p, off.p + 1, ctx->stream));
+            DBuf<uint8_t> tmp(bytes ? bytes : 1);
+            B2S_CUDA(cub::DeviceSegmentedSort::SortKeys(tmp.p, bytes, cand.p, sorted.p, (int64_t)total, (int64_t)nr,
+                                                        off.p, off.p + 1, ctx->stream));
+            ctx->launches += 1;
+        }
+        if (nr) B2S_LAUNCH(ctx, k_mm_unique_count, stream_grid(ctx, nr), kThreads, 0, nr, off.p, sorted.p, cnt.p);
+        nnz = exclusive_scan(ctx, cnt.p, C.rp.p, nr);
+        C.ci.alloc(nnz ? nnz : 1);
+        if (nr) B2S_LAUNCH(ctx, k_mm_unique_fill, stream_grid(ctx, nr), kThreads, 0, nr, off.p, sorted.p, C.rp.p, C.ci.p);
+    }
     C.v.alloc(nnz ? (size_t)nnz * BV : 1);
     if (nr)
     {
-        B2S_LAUNCH(ctx, k_mm_unique_fill, stream_grid(ctx, nr), kThreads, 0, nr, off.p, sorted.p, C.rp.p, C.ci.p);
         // B's mean row length decides: warp per C row for long rows, thread per C row otherwise
         if (B.nbr && B.nnzb >= 8ull * B.nbr)
         {

@@ -131,3 +131,35 @@ def test_amg_fp32_values(b2s, ctx, case):
     _, s32 = b2s.solve(ctx, A, b, b2s.PCG, M32, tol=1e-8, maxit=2000)
     assert s32["status"] == 0 and s32["relres_true"] < 2e-8
     assert abs(s32["iterations"] - s64["iterations"]) <= 2
+
+
+def test_amg_wide_galerkin_rows(b2s, ctx, orc):
+    """A row and column that touch every node (weak couplings, so the
+    aggregates stay those of the grid) give Galerkin rows with more distinct
+    columns than the symbolic product's per-warp hash table holds: the
+    product takes the candidate-sort path and the hierarchy still equals the
+    restatement bit for bit."""
+    n0, rp0, ci0, v0 = P.poisson2d(80)
+    rows = [dict(zip(ci0[rp0[i]:rp0[i + 1]].tolist(), v0[rp0[i]:rp0[i + 1]].tolist())) for i in range(n0)]
+    for i in range(1, n0):
+        w = -1e-3 * (1.0 + (i % 7) / 7.0)
+        rows[0][i] = rows[0].get(i, 0.0) + w
+        rows[i][0] = rows[i].get(0, 0.0) + w
+    rows[0][0] += 2.0 * n0 * 1e-3
+    rp, ci, v = [0], [], []
+    for r in rows:
+        for j in sorted(r):
+            ci.append(j)
+            v.append(r[j])
+        rp.append(len(ci))
+    rp, ci, v = np.array(rp, np.uint32), np.array(ci, np.uint32), np.array(v)
+    B = b2s.BAIJ(ctx, 1, n0, n0, rp, ci, v)
+    Bo = orc.blk_condense(1, orc.csr(n0, n0, rp, ci, v), n0, n0)
+    M = b2s.Precond(ctx, B, b2s.PC_BSA_AMG)
+    levels = orc.amg_export(orc.blk_pc(Bo, "amg_mis"), 1)
+    assert max(np.diff(levels[1]["Arp"])) > 512  # wider than the hash table
+    _, nrows, _ = M.export("amg.levels")
+    assert list(nrows) == [lv["nrows"] for lv in levels]
+    for k, lv in enumerate(levels):
+        Arp, Aci, Av = M.export(f"amg.{k}.A")
+        assert np.array_equal(Arp, lv["Arp"]) and np.array_equal(Aci, lv["Aci"]) and np.array_equal(Av, lv["Av"]), k
