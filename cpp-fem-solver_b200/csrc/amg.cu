@@ -29,6 +29,7 @@
 
 #include <algorithm>
 
+#include "baij_mv.cuh"
 #include "block_ops.cuh"
 #include "trisolve.cuh"
 
@@ -56,21 +57,21 @@ __global__ void k_find_diag(uint32_t nb, const uint32_t* __restrict__ rp, const 
     }
 }
 
-// finalise a device-built BAIJ (diag pointers, staged-matvec partition)
+// finalise a device-built BAIJ: diagonal pointers and the block count
 void finish_baij(b2s_ctx* ctx, BaijDev& M)
 {
     M.diag_ptr.alloc(M.nbr ? M.nbr : 1);
     if (M.nbr)
         B2S_LAUNCH(ctx, k_find_diag, stream_grid(ctx, M.nbr), kThreads, 0, M.nbr, M.rp.p, M.ci.p, M.diag_ptr.p);
-    M.h_rp.resize(M.nbr + 1);
-    d2h(ctx, M.h_rp.data(), M.rp.p, (M.nbr + 1) * sizeof(uint32_t));
+    d2h(ctx, &M.nnzb, M.rp.p + M.nbr, sizeof(uint32_t));
     sync(ctx);
-    M.nnzb = M.h_rp[M.nbr];
-    const uint32_t cap = M.bs == 1 ? 3072 : M.bs == 2 ? 1024 : M.bs == 3 ? 512 : 256;
-    std::vector<uint32_t> blk;
-    build_row_blocks(M.h_rp.data(), M.nbr, 1, (uint32_t)(kThreads / M.bs), cap, blk);
-    M.nblk = (uint32_t)blk.size() - 1;
-    M.blk_row = upload(ctx, blk.data(), blk.size());
+    if (M.bs == 1 && M.nbr && M.nnzb >= (uint64_t)kBaijStagedMinRow * M.nbr)
+    {
+        std::vector<uint32_t> h_rp(M.nbr + 1);
+        d2h(ctx, h_rp.data(), M.rp.p, (M.nbr + 1) * sizeof(uint32_t));
+        sync(ctx);
+        baij_partition(ctx, M, h_rp.data());
+    }
 }
 
 template <int BS>
@@ -961,6 +962,8 @@ __global__ void k_dense_solve(const double* __restrict__ D, int sz, int ref, con
 {
     if (done && *done) return;
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    // Each row's running value stays in a register while its terms are
+    // subtracted in the same order as an in-place x[i] -= ... loop would.
     if (ref)
     {
         for (int i = 0; i < sz; ++i) x[i] = rhs[i];
@@ -968,25 +971,31 @@ __global__ void k_dense_solve(const double* __restrict__ D, int sz, int ref, con
         {
             double d = D[(size_t)k * sz + k];
             if (fabs(d) < 1e-14) d = (d >= 0 ? 1e-14 : -1e-14);
-            for (int i = k + 1; i < sz; ++i) x[i] -= (D[(size_t)i * sz + k] / d) * x[k];
+            const double xk = x[k];
+            for (int i = k + 1; i < sz; ++i) x[i] -= (D[(size_t)i * sz + k] / d) * xk;
         }
         for (int i = sz - 1; i >= 0; --i)
         {
-            for (int j = i + 1; j < sz; ++j) x[i] -= D[(size_t)i * sz + j] * x[j];
+            double xi = x[i];
+            for (int j = i + 1; j < sz; ++j) xi -= D[(size_t)i * sz + j] * x[j];
             double d = D[(size_t)i * sz + i];
             if (fabs(d) < 1e-14) d = (d >= 0 ? 1e-14 : -1e-14);
-            x[i] /= d;
+            x[i] = xi / d;
         }
     }
     else
     {
-        for (int i = 0; i < sz; ++i) x[i] = rhs[piv[i]];
         for (int i = 0; i < sz; ++i)
-            for (int j = 0; j < i; ++j) x[i] -= D[(size_t)i * sz + j] * x[j];
+        {
+            double xi = rhs[piv[i]];
+            for (int j = 0; j < i; ++j) xi -= D[(size_t)i * sz + j] * x[j];
+            x[i] = xi;
+        }
         for (int i = sz - 1; i >= 0; --i)
         {
-            for (int j = i + 1; j < sz; ++j) x[i] -= D[(size_t)i * sz + j] * x[j];
-            x[i] /= D[(size_t)i * sz + i];
+            double xi = x[i];
+            for (int j = i + 1; j < sz; ++j) xi -= D[(size_t)i * sz + j] * x[j];
+            x[i] = xi / D[(size_t)i * sz + i];
         }
     }
 }
@@ -1009,40 +1018,66 @@ __global__ void k_smooth0(uint32_t nb, const T* __restrict__ dinv, const double*
         }
 }
 
-// sol += omega * dinv * (rhs - Asol)
-template <int BS, typename T>
-__global__ void k_jacobi(uint32_t nb, const T* __restrict__ dinv, const double* __restrict__ rhs,
-                         const double* __restrict__ Asol, double* __restrict__ sol, const int* done)
+// Epilogues of the V-cycle's block products (baij_mv.cuh).  Each repeats the
+// arithmetic of the separate vector pass it replaces, so the cycle's output is
+// unchanged bit for bit.
+
+// res = rhs - A sol
+struct EpiResidual
 {
-    if (done && *done) return;
-    constexpr int BV = BS * BS;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += gridDim.x * blockDim.x)
+    const double* rhs;
+    double* res;
+    template <int BS>
+    __device__ __forceinline__ void put(uint32_t I, int r, double v, bool valid, uint32_t) const
     {
-        double r[BS];
-        for (int c = 0; c < BS; ++c) r[c] = rhs[(size_t)i * BS + c] - Asol[(size_t)i * BS + c];
-        for (int c = 0; c < BS; ++c)
-        {
-            double corr = 0.0;
-            for (int rr = 0; rr < BS; ++rr) corr += (double)dinv[(size_t)i * BV + c * BS + rr] * r[rr];
-            sol[(size_t)i * BS + c] += kOmega * corr;
-        }
+        if (!valid) return;
+        const size_t i = (size_t)I * BS + r;
+        res[i] = rhs[i] - v;
     }
-}
+};
 
-__global__ void k_sub(uint64_t n, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ r,
-                      const int* done)
+// dst = sol + P e (coarse-grid correction)
+struct EpiAddTo
 {
-    if (done && *done) return;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        r[i] = a[i] - b[i];
-}
+    const double* sol;
+    double* dst;
+    template <int BS>
+    __device__ __forceinline__ void put(uint32_t I, int r, double v, bool valid, uint32_t) const
+    {
+        if (!valid) return;
+        const size_t i = (size_t)I * BS + r;
+        dst[i] = sol[i] + v;
+    }
+};
 
-__global__ void k_add(uint64_t n, const double* __restrict__ a, double* __restrict__ x, const int* done)
+// post-smoothing: sol = mid + omega * dinv * (rhs - A mid).  A block row's
+// residual components come from the BS lanes of its row.
+template <typename T>
+struct EpiJacobi
 {
-    if (done && *done) return;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        x[i] += a[i];
-}
+    const T* dinv;
+    const double* rhs;
+    const double* mid;
+    double* sol;
+    template <int BS>
+    __device__ __forceinline__ void put(uint32_t I, int r, double v, bool valid, uint32_t lane) const
+    {
+        constexpr int BV = BS * BS;
+        const size_t i = (size_t)I * BS + r;
+        const double res = valid ? rhs[i] - v : 0.0;
+        double rv[BS];
+        if constexpr (BS == 1)
+            rv[0] = res;
+        else
+#pragma unroll
+            for (int q = 0; q < BS; ++q) rv[q] = __shfl_sync(0xffffffffu, res, (lane / BS) * BS + q);
+        if (!valid) return;
+        double corr = 0.0;
+#pragma unroll
+        for (int q = 0; q < BS; ++q) corr += (double)dinv[(size_t)I * BV + r * BS + q] * rv[q];
+        sol[i] = mid[i] + kOmega * corr;
+    }
+};
 
 __global__ void k_zero(uint64_t n, double* __restrict__ x, const int* done)
 {
@@ -1094,26 +1129,26 @@ struct PcAMG final : PcImpl
     void vcycle(b2s_ctx* ctx, int l, const double* rhs, double* sol, const int* done)
     {
         Level& L = *lv[l];
-        const uint64_t ndof = (uint64_t)L.nrows * BS;
-        const unsigned g = stream_grid(ctx, L.nrows), gd = stream_grid(ctx, ndof);
+        const unsigned g = stream_grid(ctx, L.nrows);
         if (l == (int)lv.size() - 1)
         {
             B2S_LAUNCH(ctx, k_dense_solve, 1, 32, 0, dense.p, sz, ref_coarse ? 1 : 0, piv.p, rhs, sol, done);
             return;
         }
-        auto mv = [&](const BaijDev& M, const DBuf<float>& v32, const double* x, double* y) {
+        // products on FP64 or FP32 values, each with its epilogue
+        auto mv = [&](const BaijDev& M, const DBuf<float>& v32, const double* x, auto epi) {
             if (fp32)
-                baij_matvec_f32(ctx, M, v32.p, x, y, done);
+                baij_mv<BS>(ctx, M, v32.p, x, epi, done);
             else
-                baij_matvec(ctx, M, x, y, done);
+                baij_mv<BS>(ctx, M, M.v.p, x, epi, done);
         };
+        // pre-smoothing from zero, residual, restriction
         if (fp32)
             B2S_LAUNCH(ctx, (k_smooth0<BS, float>), g, kThreads, 0, L.nrows, L.dinv32.p, rhs, sol, done);
         else
             B2S_LAUNCH(ctx, (k_smooth0<BS, double>), g, kThreads, 0, L.nrows, L.dinv.p, rhs, sol, done);
-        mv(*L.A, L.A32, sol, L.tmp.p);
-        B2S_LAUNCH(ctx, k_sub, gd, kThreads, 0, ndof, rhs, L.tmp.p, L.r.p, done);
-        mv(L.R, L.R32, L.r.p, L.rc.p);
+        mv(*L.A, L.A32, sol, EpiResidual{rhs, L.r.p});
+        mv(L.R, L.R32, L.r.p, EpiStoreY{L.rc.p});
         const uint64_t nc = (uint64_t)L.R.nbr * BS;
         if (l + 1 < (int)lv.size() - 1)
             vcycle<BS>(ctx, l + 1, L.rc.p, L.ec.p, done);
@@ -1122,13 +1157,12 @@ struct PcAMG final : PcImpl
             B2S_LAUNCH(ctx, k_zero, stream_grid(ctx, nc), kThreads, 0, nc, L.ec.p, done);
             vcycle<BS>(ctx, l + 1, L.rc.p, L.ec.p, done);
         }
-        mv(L.P, L.P32, L.ec.p, L.tmp.p);
-        B2S_LAUNCH(ctx, k_add, gd, kThreads, 0, ndof, L.tmp.p, sol, done);
-        mv(*L.A, L.A32, sol, L.tmp.p);
+        // coarse-grid correction into tmp, then post-smoothing back into sol
+        mv(L.P, L.P32, L.ec.p, EpiAddTo{sol, L.tmp.p});
         if (fp32)
-            B2S_LAUNCH(ctx, (k_jacobi<BS, float>), g, kThreads, 0, L.nrows, L.dinv32.p, rhs, L.tmp.p, sol, done);
+            mv(*L.A, L.A32, L.tmp.p, EpiJacobi<float>{L.dinv32.p, rhs, L.tmp.p, sol});
         else
-            B2S_LAUNCH(ctx, (k_jacobi<BS, double>), g, kThreads, 0, L.nrows, L.dinv.p, rhs, L.tmp.p, sol, done);
+            mv(*L.A, L.A32, L.tmp.p, EpiJacobi<double>{L.dinv.p, rhs, L.tmp.p, sol});
     }
 
     void apply(b2s_ctx* ctx, const double* r, double* z, const int* done) override

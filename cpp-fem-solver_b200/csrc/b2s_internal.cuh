@@ -207,11 +207,13 @@ struct BaijDev
     DBuf<uint32_t> rp, ci;
     DBuf<double> v;
     DBuf<uint32_t> diag_ptr;    // UINT32_MAX when missing
-    DBuf<uint32_t> blk_row;     // staged matvec row partition
-    uint32_t nblk = 0;
-    std::vector<uint32_t> h_rp, h_ci, h_diag;
-    std::vector<double> h_v;
+    DBuf<uint32_t> blk_row;     // bs = 1 with long rows: staged-matvec row partition (nblk + 1)
+    uint32_t nblk = 0;          // 0: the matvec needs no partition
 };
+
+// Row partition of a bs = 1 BAIJ with long rows for its staged matvec
+// (nothing for other operators); h_rp: the host row pointers.
+void baij_partition(b2s_ctx* ctx, BaijDev& M, const uint32_t* h_rp);
 
 // Preconditioner implementation.  apply() enqueues z = M^-1 r on ctx->stream
 // (device pointers).  `done` (device, may be null) lets the Krylov drivers

@@ -2,199 +2,20 @@
 //   BlockMatrix storage / cache_diag / matvec: blockMatrix.hpp:139-234
 //   BlockMatrix::gmres "blockjacobi":         blockMatrix.hpp:714-733
 //
-// Block matvec (bs >= 2): a warp owns 32/bs consecutive block rows (one lane
-// per output component) and walks their blocks min(32, 256/bs^2) at a time.  The
-// lanes stream the blocks' values into the warp's shared memory (coalesced,
-// no L1 allocation), lane b gathers x_J of block b and forms the block's bs
-// row dots with the reference's association (blk_row_dot), and the lane of
-// output component (I, r) adds the dots of row I in block order -- the
-// reference's order, so y is bit-exact.  No CTA-wide barrier.  bs = 1 (the
-// scalar AMG levels, whose coarse rows are long) keeps the staged kernel.
-#include "block_ops.cuh"
-#include "spmv_staged.cuh"
+// The block matvec kernels are in baij_mv.cuh.
+#include "baij_mv.cuh"
 
 namespace b2s {
-
-template <int BS>
-struct BaijCap
-{
-    static constexpr int value = BS == 1 ? 3072 : BS == 2 ? 1024 : BS == 3 ? 512 : 256;
-};
-
-constexpr int kBaijCtasPerSm = 4;
-
-// VT: stored value type (double, or float for the FP32 copies of the AMG
-// hierarchy); products and sums are FP64 either way.
-template <int BS, typename VT>
-__global__ void __launch_bounds__(kThreads, kBaijCtasPerSm)
-    k_baij_warp(uint32_t nbr, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
-                const VT* __restrict__ v, const double* __restrict__ x, double* __restrict__ y, const int* done)
-{
-    if (done && *done) return;
-    constexpr int BV = BS * BS;
-    constexpr int GR = 32 / BS;                        // block rows per warp group
-    constexpr int NB = 256 / BV < 32 ? 256 / BV : 32;  // blocks per pass: one lane per block
-    constexpr int PER = (NB * BV + 31) / 32;           // value loads per lane per pass
-    __shared__ double sval[kThreads / 32][NB * BV];
-    __shared__ double sdot[kThreads / 32][NB * BS];
-    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-    double* V = sval[wid];
-    double* P = sdot[wid];
-    // one pass's operands in registers: its values and this lane's block column
-    auto load_pass = [&](uint32_t base, uint32_t nb, double* tv, uint32_t& J) {
-        const VT* vb = v + (size_t)base * BV;
-#pragma unroll
-        for (int k = 0; k < PER; ++k)
-        {
-            const uint32_t q = k * 32 + lane;
-            tv[k] = q < nb * BV ? (double)ld_stream(vb + q) : 0.0;
-        }
-        J = lane < nb ? ld_stream(ci + base + lane) : 0u;
-    };
-    const uint32_t ngroups = (nbr + GR - 1) / GR;
-    for (uint32_t g = blockIdx.x * (kThreads / 32) + wid; g < ngroups; g += gridDim.x * (kThreads / 32))
-    {
-        const uint32_t I0 = g * GR;
-        const uint32_t rows = min((uint32_t)GR, nbr - I0);
-        const bool out = lane < rows * BS;
-        const uint32_t I = I0 + lane / BS;
-        const uint32_t r = lane % BS;
-        const uint32_t a = out ? __ldg(&rp[I]) : 0u, b = out ? __ldg(&rp[I + 1]) : 0u;
-        const uint32_t p0 = __shfl_sync(0xffffffffu, a, 0);
-        const uint32_t p1 = __shfl_sync(0xffffffffu, b, (rows - 1) * BS);
-        double acc = 0.0;
-        double tv[PER];
-        uint32_t J = 0;
-        if (p0 < p1) load_pass(p0, min((uint32_t)NB, p1 - p0), tv, J);
-        for (uint32_t base = p0; base < p1; base += NB)
-        {
-            const uint32_t nb = min((uint32_t)NB, p1 - base);
-#pragma unroll
-            for (int k = 0; k < PER; ++k)
-            {
-                const uint32_t q = k * 32 + lane;
-                if (q < nb * BV) V[q] = tv[k];
-            }
-            double xv[BS];
-            if (lane < nb)
-#pragma unroll
-                for (int c = 0; c < BS; ++c) xv[c] = __ldg(&x[(size_t)J * BS + c]);
-            // the next pass's operands load while this pass computes
-            const uint32_t nbase = base + NB;
-            if (nbase < p1) load_pass(nbase, min((uint32_t)NB, p1 - nbase), tv, J);
-            __syncwarp();
-            if (lane < nb)
-#pragma unroll
-                for (int r2 = 0; r2 < BS; ++r2) P[lane * BS + r2] = blk_row_dot<BS>(&V[lane * BV + r2 * BS], xv);
-            __syncwarp();
-            if (out)
-            {
-                const uint32_t lo = a > base ? a : base, hi = b < base + nb ? b : base + nb;
-                for (uint32_t k = lo; k < hi; ++k) acc += P[(k - base) * BS + r];
-            }
-            __syncwarp();
-        }
-        if (out) y[(size_t)I * BS + r] = acc;
-    }
-}
-
-template <int BS, typename VT>
-static void launch_baij(b2s_ctx* ctx, const BaijDev& A, const VT* v, const double* x, double* y, const int* done)
-{
-    constexpr int GR = 32 / BS;
-    const uint32_t groups = (A.nbr + GR - 1) / GR;
-    const uint32_t ctas = (groups + kThreads / 32 - 1) / (kThreads / 32);
-    const uint32_t cap = (uint32_t)ctx->sm_count * kBaijCtasPerSm;
-    B2S_LAUNCH(ctx, (k_baij_warp<BS, VT>), ctas < cap ? ctas : cap, kThreads, 0, A.nbr, A.rp.p, A.ci.p, v, x, y, done);
-}
-
-__device__ __forceinline__ void stage_vals(double* s, const double* g, uint32_t cnt) { stage_f64(s, g, cnt); }
-
-__device__ __forceinline__ void stage_vals(float* s, const float* g, uint32_t cnt)
-{
-    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) s[i] = __ldg(&g[i]);
-}
-
-// 1x1 blocks (the AMG hierarchies' operators, rows of 7 to 100+ entries): a CTA
-// stages a contiguous block range in shared memory and one thread per row sums it.
-template <int BS, typename VT>
-__global__ void __launch_bounds__(kThreads) k_baij_staged(const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
-                                                          const VT* __restrict__ v,
-                                                          const uint32_t* __restrict__ blk_row,
-                                                          const double* __restrict__ x, double* __restrict__ y,
-                                                          const int* done)
-{
-    if (done && *done) return;
-    constexpr int BV = BS * BS, CAP = BaijCap<BS>::value;
-    __shared__ VT sv[CAP * BV];
-    __shared__ uint32_t sc[CAP];
-    const uint32_t r0 = blk_row[blockIdx.x], r1 = blk_row[blockIdx.x + 1];
-    const uint32_t p0 = __ldg(&rp[r0]), p1 = __ldg(&rp[r1]);
-    const uint32_t cnt = p1 - p0;
-    const uint32_t nthr = (r1 - r0) * BS;
-    if (cnt <= (uint32_t)CAP)
-    {
-        stage_vals(sv, v + (size_t)p0 * BV, cnt * BV);
-        stage_u32(sc, ci + p0, cnt);
-        __syncthreads();
-        for (uint32_t t = threadIdx.x; t < nthr; t += blockDim.x)
-        {
-            const uint32_t br = r0 + t / BS;
-            const int r = (int)(t % BS);
-            const uint32_t a = __ldg(&rp[br]) - p0, b = __ldg(&rp[br + 1]) - p0;
-            double yr = 0.0;
-            for (uint32_t k = a; k < b; ++k)
-            {
-                const double* xj = x + (size_t)sc[k] * BS;
-                double xv[BS], brow[BS];
-#pragma unroll
-                for (int c = 0; c < BS; ++c)
-                {
-                    xv[c] = __ldg(&xj[c]);
-                    brow[c] = (double)sv[(size_t)k * BV + r * BS + c];
-                }
-                yr += blk_row_dot<BS>(brow, xv);
-            }
-            y[(size_t)br * BS + r] = yr;
-        }
-    }
-    else
-    {
-        for (uint32_t t = threadIdx.x; t < nthr; t += blockDim.x)
-        {
-            const uint32_t br = r0 + t / BS;
-            const int r = (int)(t % BS);
-            double yr = 0.0;
-            for (uint32_t k = __ldg(&rp[br]); k < __ldg(&rp[br + 1]); ++k)
-            {
-                const double* xj = x + (size_t)__ldg(&ci[k]) * BS;
-                double xv[BS], brow[BS];
-#pragma unroll
-                for (int c = 0; c < BS; ++c)
-                {
-                    xv[c] = __ldg(&xj[c]);
-                    brow[c] = (double)__ldg(&v[(size_t)k * BV + r * BS + c]);
-                }
-                yr += blk_row_dot<BS>(brow, xv);
-            }
-            y[(size_t)br * BS + r] = yr;
-        }
-    }
-}
-
 
 template <typename VT>
 static void baij_matvec_t(b2s_ctx* ctx, const BaijDev& A, const VT* v, const double* x, double* y, const int* done)
 {
-    if (A.nbr == 0) return;
     switch (A.bs)
     {
-        case 1:
-            B2S_LAUNCH(ctx, (k_baij_staged<1, VT>), A.nblk, kThreads, 0, A.rp.p, A.ci.p, v, A.blk_row.p, x, y, done);
-            break;
-        case 2: launch_baij<2, VT>(ctx, A, v, x, y, done); break;
-        case 3: launch_baij<3, VT>(ctx, A, v, x, y, done); break;
-        case 4: launch_baij<4, VT>(ctx, A, v, x, y, done); break;
+        case 1: baij_mv<1>(ctx, A, v, x, EpiStoreY{y}, done); break;
+        case 2: baij_mv<2>(ctx, A, v, x, EpiStoreY{y}, done); break;
+        case 3: baij_mv<3>(ctx, A, v, x, EpiStoreY{y}, done); break;
+        case 4: baij_mv<4>(ctx, A, v, x, EpiStoreY{y}, done); break;
         default: fail(B2S_UNSUPPORTED, "block size must be 1..4");
     }
 }
@@ -209,15 +30,14 @@ void baij_matvec_f32(b2s_ctx* ctx, const BaijDev& A, const float* v32, const dou
     baij_matvec_t<float>(ctx, A, v32, x, y, done);
 }
 
-static uint32_t baij_cap(int bs)
+void baij_partition(b2s_ctx* ctx, BaijDev& M, const uint32_t* h_rp)
 {
-    switch (bs)
-    {
-        case 1: return BaijCap<1>::value;
-        case 2: return BaijCap<2>::value;
-        case 3: return BaijCap<3>::value;
-        default: return BaijCap<4>::value;
-    }
+    M.nblk = 0;
+    if (M.bs != 1 || M.nbr == 0 || M.nnzb < (uint64_t)kBaijStagedMinRow * M.nbr) return;
+    std::vector<uint32_t> blk;
+    build_row_blocks(h_rp, M.nbr, 1, kThreads, kBaijStagedCap, blk);
+    M.nblk = (uint32_t)blk.size() - 1;
+    M.blk_row = upload(ctx, blk.data(), blk.size());
 }
 
 // ------------------------------------------------------------ block Jacobi
@@ -330,26 +150,20 @@ b2s_status b2s_baij_create(b2s_ctx* ctx, int bs, uint32_t nbr, uint32_t nbc, con
         d.nbr = nbr;
         d.nbc = nbc;
         d.nnzb = nnzb;
-        d.h_rp.assign(row_ptr, row_ptr + nbr + 1);
-        d.h_ci.assign(col_idx, col_idx + nnzb);
-        d.h_v.assign(values, values + (size_t)nnzb * bs * bs);
-        d.h_diag.assign(nbr, 0xFFFFFFFFu);
+        std::vector<uint32_t> diag(nbr, 0xFFFFFFFFu);
         for (uint32_t i = 0; i < nbr; ++i)
             for (uint32_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
             {
                 need(col_idx[k] < nbc, B2S_INVALID_ARG, "block column index out of range");
                 need(k == row_ptr[i] || col_idx[k] > col_idx[k - 1], B2S_INVALID_ARG,
                      "block columns must be strictly ascending within a row");
-                if (col_idx[k] == i && d.h_diag[i] == 0xFFFFFFFFu) d.h_diag[i] = k;
+                if (col_idx[k] == i && diag[i] == 0xFFFFFFFFu) diag[i] = k;
             }
         d.rp = upload(ctx, row_ptr, (size_t)nbr + 1);
         d.ci = upload(ctx, col_idx, nnzb);
         d.v = upload(ctx, values, (size_t)nnzb * bs * bs);
-        d.diag_ptr = upload(ctx, d.h_diag.data(), nbr);
-        std::vector<uint32_t> blk;
-        build_row_blocks(row_ptr, nbr, 1, (uint32_t)(kThreads / bs), baij_cap(bs), blk);
-        d.nblk = (uint32_t)blk.size() - 1;
-        d.blk_row = upload(ctx, blk.data(), blk.size());
+        d.diag_ptr = upload(ctx, diag.data(), nbr);
+        baij_partition(ctx, d, row_ptr);
         sync(ctx);
     });
     if (st != B2S_OK)

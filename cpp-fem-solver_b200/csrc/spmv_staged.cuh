@@ -160,10 +160,12 @@ constexpr int kSpmvWarpChunk = 256;                       // products per warp p
 constexpr int kSpmvWarpPerLane = kSpmvWarpChunk / 32;     // loads per lane per pass
 constexpr int kSpmvWarpCtasPerSm = 6;
 
-template <typename Epi, typename Xop = XDirect>
+// VT: stored value type (double; float for the FP32 copies of an AMG
+// hierarchy's operators), products and sums in FP64 either way.
+template <typename Epi, typename Xop = XDirect, typename VT = double>
 __global__ void __launch_bounds__(kThreads, kSpmvWarpCtasPerSm)
     k_spmv_warp(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
-                const double* __restrict__ v, Xop x, const int* done, Epi epi, double* partial,
+                const VT* __restrict__ v, Xop x, const int* done, Epi epi, double* partial,
                 unsigned int* counter)
 {
     if (done && *done) return;
@@ -200,7 +202,7 @@ __global__ void __launch_bounds__(kThreads, kSpmvWarpCtasPerSm)
                 cc[k] = 0u;
                 if (q < p1)
                 {
-                    vv[k] = ld_stream(v + q);
+                    vv[k] = (double)ld_stream(v + q);
                     cc[k] = ld_stream(ci + q);
                 }
             }
