@@ -1339,12 +1339,6 @@ void build_hierarchy(b2s_ctx* ctx, PcAMG& pc, const BaijDev& A0, int max_levels,
     sync(ctx);
 }
 
-__global__ void k_copy_u32(const uint32_t* __restrict__ a, uint32_t* __restrict__ b, uint64_t n)
-{
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-        b[i] = a[i];
-}
-
 std::unique_ptr<PcImpl> build_amg(b2s_ctx* ctx, const BaijDev& A, const b2s_pc_opts& o,
                                   std::unique_ptr<BaijDev> owned)
 {

@@ -541,8 +541,6 @@ __global__ void k_gm_cycle_begin(KState* st, GmSmall sm)
     st->aux[5] = 0.0;  // cycle_end
 }
 
-__device__ __forceinline__ bool gm_inactive(const KState* st) { return st->done || st->aux[5] != 0.0; }
-
 // MGS step i for column j (array.cpp:4307-4316):
 //   if i > 0: w -= H[i-1][j] V[i-1];   acc = w . V[i]  -> H[i][j]
 // For i == j+1 the dot is w.w and the column's tail runs (norm, Givens, check).

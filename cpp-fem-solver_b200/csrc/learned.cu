@@ -439,14 +439,6 @@ __global__ void __launch_bounds__(256) k_aggregate_bwd(uint32_t n, const uint32_
 
 // ------------------------------------------------------------ output head
 
-__device__ __forceinline__ float head_edge(const float* P, const float* hi, const float* hj, const float* e)
-{
-    float c = P[OFF_OUT + O_BO];
-    for (int k = 0; k < H; ++k) c += P[OFF_OUT + O_U + k] * hi[k] + P[OFF_OUT + O_V + k] * hj[k];
-    for (int k = 0; k < FE; ++k) c += P[OFF_OUT + O_W + k] * e[k];
-    return c;
-}
-
 // Lv <- L0 * exp(s tanh c) on the pattern of L (rows with diagonal last).  The
 // head uses FP32 parameters (Pf) rounded to BF16 by the caller.  C receives c.
 // Per-node projections of the head: proj[3i..3i+2] = (u.h_i, v.h_i, d.h_i).

@@ -96,13 +96,6 @@ void colour_graph(uint32_t n, const std::vector<uint32_t>& rp, const std::vector
 }
 
 // A2 row ni = A row perm[ni] with columns renumbered, then sorted
-__global__ void k_perm_count(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ perm,
-                             uint32_t* __restrict__ cnt)
-{
-    for (uint32_t ni = blockIdx.x * blockDim.x + threadIdx.x; ni < n; ni += gridDim.x * blockDim.x)
-        cnt[ni + 1] = rp[perm[ni] + 1] - rp[perm[ni]];
-}
-
 __global__ void k_perm_fill(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
                             const double* __restrict__ v, const uint32_t* __restrict__ perm,
                             const uint32_t* __restrict__ new_id, const uint32_t* __restrict__ rp2,
