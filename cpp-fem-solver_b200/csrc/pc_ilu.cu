@@ -970,16 +970,19 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     ha.th = std::thread([&ha, &hrp, &hci, &pc, n, vs, sweeps, nsweeps, seg, sm_count, fp32] {
         try
         {
-            strict_transpose(n, hrp.data(), hci.data(), true, ha.up_rp, ha.up_ci);
             if (sweeps)
             {
+                // both band plans from L's pattern (L^T's is not needed on the host)
                 if (fp32)
-                {
-                    ha.lo_band = plan_band(n, hrp.data(), hci.data(), true, nsweeps, sm_count, seg);
-                    ha.up_band = plan_band(n, ha.up_rp.data(), ha.up_ci.data(), false, nsweeps, sm_count, seg);
-                }
+                    plan_parallel(2, 2, [&](uint32_t side, unsigned) {
+                        if (side == 0)
+                            ha.lo_band = plan_band(n, hrp.data(), hci.data(), true, nsweeps, sm_count, seg);
+                        else
+                            ha.up_band = plan_band_transposed(n, hrp.data(), hci.data(), nsweeps, sm_count, seg);
+                    });
                 return;
             }
+            strict_transpose(n, hrp.data(), hci.data(), true, ha.up_rp, ha.up_ci);
             // the two triangles' plans run side by side
             plan_parallel(2, 2, [&](uint32_t side, unsigned) {
                 if (side == 0)

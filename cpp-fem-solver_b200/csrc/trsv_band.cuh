@@ -60,11 +60,14 @@ __host__ __device__ constexpr uint32_t band_halo(uint32_t k, uint32_t B, uint32_
     return k * ((B + S - 1) / S * S);
 }
 
+// The plan from a triangle's bandwidth B (largest |i - j| of a dependency
+// entry) and widest row W (dependency entries); empty when the banded kernel
+// does not apply.
+inline BandPlan plan_band_from(uint32_t n, uint64_t B, uint64_t W, int k, int sm_count, uint32_t S);
+
 inline BandPlan plan_band(uint32_t n, const uint32_t* rp, const uint32_t* ci, bool lower, int k, int sm_count,
                           uint32_t S)
 {
-    BandPlan p;
-    if (!n || k <= 0) return p;
     uint64_t B = 0, W = 0;
     for (uint32_t i = 0; i < n; ++i)
     {
@@ -80,6 +83,34 @@ inline BandPlan plan_band(uint32_t n, const uint32_t* rp, const uint32_t* ci, bo
         }
         W = std::max(W, w);
     }
+    return plan_band_from(n, B, W, k, sm_count, S);
+}
+
+// The plan of the strict transpose of a lower triangle, from the lower
+// triangle's pattern: the same bandwidth, and the widest column as the
+// widest row.  Equal to plan_band on the transposed pattern.
+inline BandPlan plan_band_transposed(uint32_t n, const uint32_t* rp, const uint32_t* ci, int k, int sm_count,
+                                     uint32_t S)
+{
+    uint64_t B = 0, W = 0;
+    std::vector<uint32_t> cols(n, 0);
+    for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t q = rp[i]; q < rp[i + 1]; ++q)
+        {
+            const uint32_t j = ci[q];
+            if (j < i)
+            {
+                B = std::max<uint64_t>(B, i - j);
+                W = std::max<uint64_t>(W, ++cols[j]);
+            }
+        }
+    return plan_band_from(n, B, W, k, sm_count, S);
+}
+
+inline BandPlan plan_band_from(uint32_t n, uint64_t B, uint64_t W, int k, int sm_count, uint32_t S)
+{
+    BandPlan p;
+    if (!n || k <= 0) return p;
     if (B == 0) B = 1;
     if (W > 4 || B > 65535) return p;
     const uint32_t w = W <= 2 ? 2 : 4;

@@ -1,0 +1,73 @@
+// Host check of the band planner (csrc/trsv_band.cuh): the plan of a lower
+// triangle's strict transpose made from the lower pattern
+// (plan_band_transposed) equals plan_band on the transposed pattern, for
+// grid stencils and random lower patterns.  Prints OK.
+#include <cstdio>
+#include <random>
+#include <vector>
+
+#include "../../cpp-fem-solver_b200/csrc/trsv_band.cuh"
+#include "../../cpp-fem-solver_b200/csrc/trsv_plan.hpp"
+
+using namespace b2s;
+
+static bool same(const BandPlan& a, const BandPlan& b)
+{
+    return a.T == b.T && a.B == b.B && a.W == b.W && a.Rmax == b.Rmax && a.smem == b.smem && a.ntiles == b.ntiles;
+}
+
+static int check(const char* name, uint32_t n, const std::vector<uint32_t>& rp, const std::vector<uint32_t>& ci)
+{
+    std::vector<uint32_t> trp, tci;
+    strict_transpose(n, rp.data(), ci.data(), true, trp, tci);
+    int bad = 0;
+    for (int k : {1, 4, 8})
+        for (uint32_t S : {1u, 8u})
+        {
+            const BandPlan a = plan_band_transposed(n, rp.data(), ci.data(), k, 148, S);
+            const BandPlan b = plan_band(n, trp.data(), tci.data(), false, k, 148, S);
+            if (!same(a, b))
+            {
+                std::printf("%s k=%d S=%u: T %u/%u B %u/%u W %u/%u ntiles %u/%u\n", name, k, S, a.T, b.T, a.B, b.B, a.W,
+                            b.W, a.ntiles, b.ntiles);
+                ++bad;
+            }
+        }
+    return bad;
+}
+
+int main()
+{
+    int bad = 0;
+    for (uint32_t N : {16u, 100u, 512u})  // 5-point lower (with diagonal), N x N
+    {
+        const uint32_t n = N * N;
+        std::vector<uint32_t> rp{0}, ci;
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            if (i >= N) ci.push_back(i - N);
+            if (i % N) ci.push_back(i - 1);
+            ci.push_back(i);
+            rp.push_back((uint32_t)ci.size());
+        }
+        bad += check("grid5", n, rp, ci);
+    }
+    std::mt19937 g(7);
+    for (uint32_t n : {50u, 3000u, 20000u})  // random lower patterns of bandwidth <= 700
+        for (int w : {1, 3, 6})
+        {
+            std::vector<uint32_t> rp{0}, ci;
+            for (uint32_t i = 0; i < n; ++i)
+            {
+                std::vector<uint32_t> c{i};
+                for (int t = 0; t < w && i > 0; ++t) c.push_back(i - 1 - g() % std::min<uint32_t>(i, 700));
+                std::sort(c.begin(), c.end());
+                c.erase(std::unique(c.begin(), c.end()), c.end());
+                ci.insert(ci.end(), c.begin(), c.end());
+                rp.push_back((uint32_t)ci.size());
+            }
+            bad += check("random", n, rp, ci);
+        }
+    std::printf(bad ? "FAIL\n" : "OK\n");
+    return bad ? 1 : 0;
+}
