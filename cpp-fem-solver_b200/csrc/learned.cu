@@ -319,49 +319,51 @@ __global__ void __launch_bounds__(256) k_aggregate(uint32_t n, const uint32_t* _
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const uint32_t i = blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (i >= n) return;
-    float a0 = 0.f, a1 = 0.f;
     const int c0 = lane, c1 = lane + 32;
-    // neighbours eight at a time: their indices, edge features and messages
-    // are all in flight before the gates are formed (same summation order)
-    const uint32_t pa = rp[i], pe = rp[i + 1];
-    for (uint32_t pb = pa; pb < pe; pb += 8)
+    // grid-stride over nodes, so the weights above are staged once per CTA
+    for (uint32_t i = blockIdx.x * 8 + (threadIdx.x >> 5); i < n; i += gridDim.x * 8)
     {
-        uint32_t jj[8];
-        float4 ee[8];
-        float m0[8], m1[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) jj[k] = pb + k < pe ? ci[pb + k] : i;
-#pragma unroll
-        for (int k = 0; k < 8; ++k)
+        float a0 = 0.f, a1 = 0.f;
+        // neighbours eight at a time: their indices, edge features and messages
+        // are all in flight before the gates are formed (same summation order)
+        const uint32_t pa = rp[i], pe = rp[i + 1];
+        for (uint32_t pb = pa; pb < pe; pb += 8)
         {
-            const bool on = jj[k] != i;
-            ee[k] = on ? *reinterpret_cast<const float4*>(EF + (size_t)(pb + k) * FE) : make_float4(0.f, 0.f, 0.f, 0.f);
-            m0[k] = on ? SM[(size_t)jj[k] * 2 * H + H + c0] : 0.f;
-            m1[k] = on ? SM[(size_t)jj[k] * 2 * H + H + c1] : 0.f;
-        }
+            uint32_t jj[8];
+            float4 ee[8];
+            float m0[8], m1[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
-        {
-            if (jj[k] == i) continue;
-            const float4 e = ee[k];
-            const float g0 = sigm(bg[c0] + wg[c0][0] * e.x + wg[c0][1] * e.y + wg[c0][2] * e.z + wg[c0][3] * e.w);
-            const float g1 = sigm(bg[c1] + wg[c1][0] * e.x + wg[c1][1] * e.y + wg[c1][2] * e.z + wg[c1][3] * e.w);
-            a0 += g0 * m0[k];
-            a1 += g1 * m1[k];
+            for (int k = 0; k < 8; ++k) jj[k] = pb + k < pe ? ci[pb + k] : i;
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+            {
+                const bool on = jj[k] != i;
+                ee[k] = on ? *reinterpret_cast<const float4*>(EF + (size_t)(pb + k) * FE) : make_float4(0.f, 0.f, 0.f, 0.f);
+                m0[k] = on ? SM[(size_t)jj[k] * 2 * H + H + c0] : 0.f;
+                m1[k] = on ? SM[(size_t)jj[k] * 2 * H + H + c1] : 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+            {
+                if (jj[k] == i) continue;
+                const float4 e = ee[k];
+                const float g0 = sigm(bg[c0] + wg[c0][0] * e.x + wg[c0][1] * e.y + wg[c0][2] * e.z + wg[c0][3] * e.w);
+                const float g1 = sigm(bg[c1] + wg[c1][0] * e.x + wg[c1][1] * e.y + wg[c1][2] * e.z + wg[c1][3] * e.w);
+                a0 += g0 * m0[k];
+                a1 += g1 * m1[k];
+            }
         }
+        const float id = invdeg[i];
+        const float p0 = SM[(size_t)i * 2 * H + c0] + bl[c0] + id * a0;
+        const float p1 = SM[(size_t)i * 2 * H + c1] + bl[c1] + id * a1;
+        if (pre)  // kept for the backward pass (training only)
+        {
+            pre[(size_t)i * H + c0] = p0;
+            pre[(size_t)i * H + c1] = p1;
+        }
+        Hout[(size_t)i * H + c0] = fmaxf(p0, 0.f) + Hin[(size_t)i * H + c0];
+        Hout[(size_t)i * H + c1] = fmaxf(p1, 0.f) + Hin[(size_t)i * H + c1];
     }
-    const float id = invdeg[i];
-    const float p0 = SM[(size_t)i * 2 * H + c0] + bl[c0] + id * a0;
-    const float p1 = SM[(size_t)i * 2 * H + c1] + bl[c1] + id * a1;
-    if (pre)  // kept for the backward pass (training only)
-    {
-        pre[(size_t)i * H + c0] = p0;
-        pre[(size_t)i * H + c1] = p1;
-    }
-    Hout[(size_t)i * H + c0] = fmaxf(p0, 0.f) + Hin[(size_t)i * H + c0];
-    Hout[(size_t)i * H + c1] = fmaxf(p1, 0.f) + Hin[(size_t)i * H + c1];
 }
 
 // backward of k_aggregate for one layer.
@@ -908,7 +910,8 @@ struct GnnGraph
 
     void forward(b2s_ctx* ctx, const Gnn& net, const CsrDev& A)
     {
-        const unsigned g64 = (n + kFwdRows - 1) / kFwdRows, gw = (n + 7) / 8;
+        const unsigned g64 = (n + kFwdRows - 1) / kFwdRows;
+        const unsigned gw = std::min<unsigned>((n + 7) / 8, (unsigned)ctx->sm_count * 8);
         B2S_LAUNCH(ctx, (k_linear<FIN, H, true>), g64, 256, 0, n, F.p, net.pb.p + OFF_WIN, net.pr.p + OFF_BIN,
                    state_mut(0), training ? pre0.p : (float*)nullptr);
         for (int l = 0; l < NL; ++l)
