@@ -53,14 +53,22 @@ __device__ __forceinline__ unsigned ld_acquire_gpu_u32(const unsigned* p)
     return v;
 }
 
-// all CTAs of the (cooperative) grid arrive; false after a timeout
+__device__ __forceinline__ void red_release_gpu_add(unsigned* p, unsigned v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// All CTAs of the (cooperative) grid arrive; false after a timeout.  The
+// block barrier orders the CTA's writes before thread 0's release add, and
+// the acquire load that sees every arrival orders the other CTAs' writes
+// before the block barrier that releases this CTA (release / acquire at gpu
+// scope, cumulative through the block barriers; no separate fences).
 __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned target, int* err, int* s_ok)
 {
     __syncthreads();
     if (threadIdx.x == 0)
     {
-        __threadfence();
-        atomicAdd(bar, 1u);
+        red_release_gpu_add(bar, 1u);
         int ok = 1;
         for (unsigned polls = 0; ld_acquire_gpu_u32(bar) < target; ++polls)
             if (polls >= kGridBarrierPolls)
@@ -69,7 +77,6 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned target, int
                 ok = 0;
                 break;
             }
-        __threadfence();
         *s_ok = ok;
     }
     __syncthreads();
