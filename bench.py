@@ -409,8 +409,9 @@ def main():
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b2s", choices=["b2s", "reference"])
-    ap.add_argument("--method", default="learned_ic0_j8",
-                    choices=["learned_ic0_j8", "learned_ic0", "fp32_ic0_j8", "fp32_ic0", "fp64_ic0", "sa_amg"])
+    ap.add_argument("--method", default="learned_ic0_j6",
+                    choices=["learned_ic0_j6", "learned_ic0_j8", "learned_ic0", "fp32_ic0_j6", "fp32_ic0_j8",
+                             "fp32_ic0", "fp64_ic0", "sa_amg"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel", default=None, choices=sorted(KERNELS),
                     help="run one hot kernel only (for profilers), not the benchmark")
@@ -444,8 +445,10 @@ def main():
     systems = [make_system(b2s, s) for s in seeds]
 
     # method -> (preconditioner, precision, triangular-solve schedule, sweeps, factorisation sweeps)
-    kinds = {"learned_ic0_j8": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_JACOBI, 8, 5),
+    kinds = {"learned_ic0_j6": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_JACOBI, 6, 5),
+             "learned_ic0_j8": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_JACOBI, 8, 5),
              "learned_ic0": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_AUTO, 0, 0),
+             "fp32_ic0_j6": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_JACOBI, 6, 5),
              "fp32_ic0_j8": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_JACOBI, 8, 5),
              "fp32_ic0": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_AUTO, 0, 0),
              "fp64_ic0": (b2s.PC_IC0, b2s.FP64, b2s.TRSV_AUTO, 0, 0),
@@ -682,11 +685,13 @@ def main():
             "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 outer / f32 preconditioner" if prec == b2s.FP32 else "f64",
-            "method": {"learned_ic0_j8": "learned IC(0) values (tcgen05 network) on a 5-sweep fixed-point IC(0) "
-                                         "factor, FP32, 8 Jacobi sweeps per triangle (banded one-launch kernel, "
-                                         "fused PCG iteration), FP64 PCG and true residual",
+            "method": {"learned_ic0_j6": "learned IC(0) values (tcgen05 network) on a 5-sweep fixed-point IC(0) "
+                                         "factor, FP32, 6 Jacobi sweeps per triangle, the whole PCG loop in one "
+                                         "persistent launch, FP64 PCG and true residual",
+                       "learned_ic0_j8": "the same with 8 Jacobi sweeps per triangle",
                        "learned_ic0": "learned IC(0) values on the exact factor, FP32, exact chunk-scheduled "
                                       "triangular solves",
+                       "fp32_ic0_j6": "plain IC(0) (5-sweep fixed-point factor), FP32, 6 Jacobi sweeps per triangle",
                        "fp32_ic0_j8": "plain IC(0) (5-sweep fixed-point factor), FP32, 8 Jacobi sweeps per triangle",
                        "fp32_ic0": "plain IC(0), FP32 factor, exact triangular solves",
                        "fp64_ic0": "plain IC(0), FP64, exact triangular solves",
