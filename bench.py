@@ -28,6 +28,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -61,7 +62,8 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{device}.csv")
+        out_dir = os.environ.get("B2S_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out_dir, f"clocks_bench_{device}.csv")
 
     def __enter__(self):
         try:
@@ -111,8 +113,9 @@ def make_system(b2s, seed):
 
 
 # DRAM bytes (read + write) of one k_pcg_band launch on the 512^2 learned
-# solve: dram__bytes.sum.per_second x gpu__time_duration.sum of the ncu
-# capture summarised in profiles/k_pcg_band_grf512_ic0_j8.md.
+# solve: dram__bytes.sum.per_second x gpu__time_duration.sum of an ncu
+# capture of `bench.py --kernel solve_c5` (SpeedOfLight and
+# MemoryWorkloadAnalysis sections, one launch).
 PCG_BAND_DRAM_BYTES = 33.7e6
 
 
