@@ -1,8 +1,10 @@
-// Host check of the band planner (csrc/trsv_band.cuh): the plan of a lower
-// triangle's strict transpose made from the lower pattern
-// (plan_band_transposed) equals plan_band on the transposed pattern, for
-// grid stencils and random lower patterns.  Prints OK.
+// Host checks of the planners: the band plan of a lower triangle's strict
+// transpose made from the lower pattern (plan_band_transposed, trsv_band.cuh)
+// equals plan_band on the transposed pattern, for grid stencils and random
+// lower patterns; and the chunk plan (trsv_plan.hpp) is the same with one
+// host thread and with sixteen.  Prints OK.
 #include <cstdio>
+#include <cstring>
 #include <random>
 #include <vector>
 
@@ -68,6 +70,45 @@ int main()
             }
             bad += check("random", n, rp, ci);
         }
+    // the chunk planner's output does not depend on its number of host threads
+    for (uint32_t N : {24u, 64u})
+    {
+        const uint32_t n = N * N * N;
+        std::vector<uint32_t> rp{0}, ci;
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            const uint32_t x = i % N, y = (i / N) % N, z = i / (N * N);
+            if (z) ci.push_back(i - N * N);
+            if (y) ci.push_back(i - N);
+            if (x) ci.push_back(i - 1);
+            ci.push_back(i);
+            rp.push_back((uint32_t)ci.size());
+        }
+        for (int lower = 0; lower < 2; ++lower)
+        {
+            std::vector<uint32_t> trp, tci;
+            const uint32_t* prp = rp.data();
+            const uint32_t* pci = ci.data();
+            if (!lower)
+            {
+                strict_transpose(n, rp.data(), ci.data(), true, trp, tci);
+                prp = trp.data();
+                pci = tci.data();
+            }
+            const ChunkPlan a = plan_chunks(n, prp, pci, lower, 1, 8, 8, 8, kChunkSmemBudget, 1, nullptr, 1);
+            const ChunkPlan b = plan_chunks(n, prp, pci, lower, 1, 8, 8, 8, kChunkSmemBudget, 1, nullptr, 16);
+            const bool eq = a.ok == b.ok && a.desc.size() == b.desc.size() &&
+                            std::memcmp(a.desc.data(), b.desc.data(), a.desc.size() * sizeof(ChunkDesc)) == 0 &&
+                            a.meta == b.meta && a.slot_row == b.slot_row && a.src == b.src &&
+                            a.v64_units == b.v64_units && a.v32_units == b.v32_units &&
+                            a.max_level_rows == b.max_level_rows;
+            if (!eq)
+            {
+                std::printf("plan_chunks N=%u lower=%d: 1 and 16 workers differ\n", N, lower);
+                ++bad;
+            }
+        }
+    }
     std::printf(bad ? "FAIL\n" : "OK\n");
     return bad ? 1 : 0;
 }

@@ -1,7 +1,8 @@
-"""The band planner (csrc/trsv_band.cuh) on the CPU: tests/band_plan/band_plan.cu
-checks that the plan of a lower triangle's strict transpose made from the
-lower pattern equals the plan made from the transposed pattern (host code,
-compiled by nvcc, no GPU needed)."""
+"""The planners on the CPU (host code compiled by nvcc, no GPU needed):
+tests/band_plan/band_plan.cu checks that the band plan of a lower
+triangle's strict transpose made from the lower pattern equals the plan made
+from the transposed pattern (csrc/trsv_band.cuh), and that the chunk plan
+(csrc/trsv_plan.hpp) does not depend on the number of host threads."""
 import os
 import shutil
 import subprocess
