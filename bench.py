@@ -41,6 +41,7 @@ CORR = 0.05
 TOL = 1e-8
 MAXIT = 20000
 L2_FLUSH_BYTES = 512 << 20
+METRIC = "time-to-rtol 1e-8 & iters: learned/mixed-prec PCG vs plain FP64 PCG, 1 B200"
 
 
 def load_b2s():
@@ -365,15 +366,26 @@ def run_suite(args):
 
 # ---------------------------------------------------------------- reference arm
 
+def arm_config(args, world):
+    """The workload's `config` object, the same for both arms."""
+    return {"workload": "grf_diffusion_512 pcg rtol1e-8", "method": args.method, "grid": N_GRID, "corr": CORR,
+            "parallelism": f"replicas x{world}", "l2": "flushed (512 MB write) before every step"}
+
+
 def run_reference(args):
+    """The reference's own SMatrix::pcg(A, b, "ic") (oracle/_ref/libref.so,
+    compiled from its sources) on all host cores, on the systems the GPU arm
+    solves.  The systems come from oracle/_ref/libgen.so (the library's
+    generators built on their own), so this process maps only the reference
+    and the generators, never the product library."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
-    b2s = load_b2s()
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     try:
         ref = oracle.Ref()
+        gen = oracle.Gen()
     except Exception as e:
         print(json.dumps({"impl": "reference", "unavailable": f"reference library not built: {e}"}))
         return 0
@@ -381,7 +393,9 @@ def run_reference(args):
     ref.set_threads(cores)
     times, its = [], []
     for k in range(args.warmup + args.steps):
-        n, rp, ci, v, b = make_system(b2s, 2000 + k)
+        seed = 2000 + k
+        n, rp, ci, v = gen.grf_diffusion(N_GRID, seed, corr=CORR)
+        b = gen.uniform(seed, n)
         A = ref.csr(n, n, rp, ci, v)
         t0 = time.perf_counter()
         x, it = ref.solve(A, 0, "ic", b, TOL, MAXIT)
@@ -390,12 +404,13 @@ def run_reference(args):
             times.append(dt * 1e3)
             its.append(it)
     ms = float(np.mean(times))
-    line = {"metric": "time-to-rtol 1e-8 & iters: learned/mixed-prec PCG vs plain FP64 PCG, 1 B200", "value": ms, "unit": "ms",
+    line = {"metric": METRIC, "value": ms, "unit": "ms",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded GRF diffusion, held-out seeds 2000+)", "impl": "reference",
-            "config": {"workload": "grf_diffusion_512 pcg rtol1e-8", "solver": "SMatrix::pcg(A,b,\"ic\")",
-                       "grid": N_GRID, "corr": CORR, "seeds": [2000 + args.warmup, 2000 + args.warmup + args.steps - 1]},
+            "config": arm_config(args, world),
+            "reference_solver": {"call": "SMatrix::pcg(A, b, \"ic\", 1e-8, 20000)",
+                                 "seeds": [2000 + args.warmup, 2000 + args.warmup + args.steps - 1]},
             "iterations_mean": float(np.mean(its)),
             "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "reference",
                              "sample": f"{args.steps} full solves (one system each)"},
@@ -684,7 +699,7 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": "time-to-rtol 1e-8 & iters: learned/mixed-prec PCG vs plain FP64 PCG, 1 B200",
+            "metric": METRIC,
             "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": value, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 outer / f32 preconditioner" if prec == b2s.FP32 else "f64",
@@ -700,8 +715,7 @@ def main():
                        "fp64_ic0": "plain IC(0), FP64, exact triangular solves",
                        "sa_amg": "smoothed-aggregation AMG V-cycle (FP64)"}[args.method],
             "data": "synthetic (seeded GRF diffusion, held-out seeds 2000+)",
-            "config": {"workload": "grf_diffusion_512 pcg rtol1e-8", "method": args.method, "grid": N_GRID,
-                       "corr": CORR, "parallelism": f"replicas x{world}", "l2": "flushed (512 MB write) before every step"},
+            "config": arm_config(args, world),
             "iterations_mean": float(np.mean(head_its)), "relres_true_max": float(np.max(head_rel)),
             "fallbacks": int(head_fallbacks),
             "setup_ms_mean": float(np.mean([a for a, _ in head_split])),

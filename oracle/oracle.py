@@ -10,6 +10,9 @@ imports it.
 * ``Ref`` -- ``oracle/_ref/libref.so``, the reference library itself
   (ode-solver/src/math/array.cpp + include/math/blockMatrix.hpp) compiled from
   its sources by ``oracle/Makefile`` through ``oracle/ref_harness.cpp``.
+* ``Gen`` -- ``oracle/_ref/libgen.so``, the library's CPU problem generators
+  built on their own, so that the benchmark's reference arm makes the same
+  systems without loading the product library.
 
 Both expose the same Python surface so tests can run one case through either.
 """
@@ -38,8 +41,8 @@ class OracleError(Exception):
 
 
 def build(quiet: bool = True) -> None:
-    """Build oracle/_ref/liborc.so (always) and libref.so (when the
-    reference sources are present)."""
+    """Build oracle/_ref/liborc.so and libgen.so (always) and libref.so (when
+    B2S_REFERENCE_SRC names the reference's ode-solver directory)."""
     subprocess.run(["make", "-C", HERE], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
 
@@ -475,3 +478,47 @@ def _amg_export(fn, pc, bs):
             lv.update(Prp=Prp, Pci=Pci[:nnzP], Pv=Pv[: nnzP * bv])
         out.append(lv)
     return out
+
+
+class Gen:
+    """The problem generators of ``cpp-fem-solver_b200/csrc/gen.cpp`` from
+    ``oracle/_ref/libgen.so`` (same source and flags as the product build, so
+    the same systems bit for bit)."""
+
+    def __init__(self, path=os.path.join(REF_DIR, "libgen.so")):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = C.CDLL(path)
+        self.path = path
+        vp, u32, f64, u64 = C.c_void_p, C.c_uint32, C.c_double, C.c_uint64
+        pu = C.POINTER(C.c_uint32)
+        self._grf = self.lib.b2s_gen_grf_diffusion
+        self._grf.restype = C.c_int
+        self._grf.argtypes = [u32, f64, f64, u64, pu, pu, vp, vp, vp, vp]
+        self._uni = self.lib.b2s_gen_uniform
+        self._uni.restype = C.c_int
+        self._uni.argtypes = [u64, u64, vp]
+
+    def uniform(self, seed: int, n: int) -> np.ndarray:
+        """Counter-based uniform[-1, 1) vector (splitmix64), as b2s.uniform."""
+        out = np.zeros(n, np.float64)
+        if self._uni(seed, n, _ptr(out)) != 0:
+            raise OracleError(1, "uniform generator failed")
+        return out
+
+    def grf_variance(self, seed: int) -> float:
+        """Per-instance log-k variance in [1, 4], as b2s.grf_variance."""
+        u = self.uniform(seed ^ 0x7F4A7C15, 1)[0]
+        return 1.0 + 1.5 * (u + 1.0)
+
+    def grf_diffusion(self, N: int, seed: int, corr: float = 0.05):
+        """512^2-style GRF diffusion system: (n, rp, ci, v), as b2s.gen_grf_diffusion."""
+        var = self.grf_variance(seed)
+        n, nnz = C.c_uint32(), C.c_uint32()
+        if self._grf(N, corr, var, seed, C.byref(n), C.byref(nnz), None, None, None, None) != 0:
+            raise OracleError(1, "GRF generator failed")
+        rp = np.zeros(n.value + 1, np.uint32)
+        ci = np.zeros(nnz.value, np.uint32)
+        v = np.zeros(nnz.value, np.float64)
+        self._grf(N, corr, var, seed, C.byref(n), C.byref(nnz), _ptr(rp), _ptr(ci), _ptr(v), None)
+        return n.value, rp, ci, v
