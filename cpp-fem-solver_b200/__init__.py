@@ -39,7 +39,7 @@ CUDA_ERROR, NO_DEVICE, OUT_OF_MEMORY, UNSUPPORTED = 10, 11, 12, 13
 
 # preconditioner kinds / methods / options (b2s.h)
 PC_NONE, PC_DIAG, PC_IC0, PC_ILU0, PC_SSOR, PC_SA_AMG, PC_LEARNED_IC0, PC_BJACOBI, PC_BILU0, PC_BSA_AMG = range(10)
-PCG, BICGSTAB, GMRES, FGMRES, BLOCK_GMRES = range(5)
+PCG, BICGSTAB, GMRES, FGMRES, BLOCK_GMRES, STATIONARY = range(6)
 FP64, FP32, BF16 = range(3)
 TRSV_AUTO, TRSV_LEVEL, TRSV_SYNCFREE, TRSV_CHUNK, TRSV_JACOBI = range(5)
 ORTH_MGS, ORTH_CGS2 = range(2)
@@ -115,7 +115,7 @@ EXPORTS = [
     "b2s_gen_elasticity_q1", "b2s_gen_grf_diffusion", "b2s_gen_uniform", "b2s_learner_create",
     "b2s_learner_destroy", "b2s_learner_load", "b2s_learner_save", "b2s_learner_params", "b2s_learner_step",
     "b2s_pc_create_learned", "b2s_dot_noalloc", "b2s_dense_bf16_device",
-    "b2s_learner_set_loss", "b2s_sor", "b2s_sor_device",
+    "b2s_learner_set_loss", "b2s_sor", "b2s_sor_device", "b2s_csr_matmul", "b2s_csr_transpose", "b2s_csr_export",
 ]
 
 
@@ -192,6 +192,9 @@ def lib():
     f("b2s_learner_set_loss", i32, vp, i32)
     f("b2s_sor", i32, vp, vp, i32, f64, f64, i32, _f64p, _f64p, C.POINTER(Stats))
     f("b2s_sor_device", i32, vp, vp, i32, f64, f64, i32, vp, vp, C.POINTER(Stats))
+    f("b2s_csr_matmul", i32, vp, vp, vp, pp)
+    f("b2s_csr_transpose", i32, vp, vp, pp)
+    f("b2s_csr_export", i32, vp, vp, vp, vp, vp)
     _lib = L
     return L
 
@@ -277,6 +280,31 @@ class CSR:
 
     def spmv_device(self, x_ptr: int, y_ptr: int):
         self.ctx.check(lib().b2s_spmv_device(self.ctx.h, self.h, C.c_void_p(x_ptr), C.c_void_p(y_ptr)), "spmv")
+
+    @classmethod
+    def _adopt(cls, ctx: Context, h) -> "CSR":
+        """A handle made on the device (product, transpose), with its host arrays."""
+        n, m, nnz = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        lib().b2s_csr_info(h, C.byref(n), C.byref(m), C.byref(nnz))
+        out = cls.__new__(cls)
+        out.ctx, out.n, out.m, out.h = ctx, n.value, m.value, h
+        out.rp = np.zeros(n.value + 1, np.uint32)
+        out.ci = np.zeros(nnz.value, np.uint32)
+        out.v = np.zeros(nnz.value, np.float64)
+        ctx.check(lib().b2s_csr_export(ctx.h, h, _ptr(out.rp), _ptr(out.ci), _ptr(out.v)), "csr_export")
+        return out
+
+    def transpose(self) -> "CSR":
+        """A^T on the device (SMatrix::transpose)."""
+        h = C.c_void_p()
+        self.ctx.check(lib().b2s_csr_transpose(self.ctx.h, self.h, C.byref(h)), "csr_transpose")
+        return CSR._adopt(self.ctx, h)
+
+    def matmul(self, B: "CSR") -> "CSR":
+        """A B on the device (SMatrix::operator*)."""
+        h = C.c_void_p()
+        self.ctx.check(lib().b2s_csr_matmul(self.ctx.h, self.h, B.h, C.byref(h)), "csr_matmul")
+        return CSR._adopt(self.ctx, h)
 
     def __del__(self):
         try:
@@ -710,6 +738,48 @@ class SMatrix:
     @staticmethod
     def gmres(A, b, precond, restart, tol=1e-10, max_iter=2000):
         return SMatrix._solve(A, b, GMRES, precond, tol, max_iter, restart)
+
+    @staticmethod
+    def sor(A, b, omega, tol=1e-10, max_iter=2000):
+        if A._rows != A._cols:
+            raise ValueError("SOR needs a square matrix")
+        x, st = sor(SMatrix.context(), A.device(), _f64(b), omega, tol, max_iter)
+        return x, st["it"]
+
+    @staticmethod
+    def sor_rb(A, b, omega, tol=1e-10, max_iter=2000):
+        if A._rows != A._cols:
+            raise ValueError("red-black SOR needs a square matrix")
+        x, st = sor(SMatrix.context(), A.device(), _f64(b), omega, tol, max_iter, red_black=True)
+        return x, st["it"]
+
+    @staticmethod
+    def amg(A, b, tol=1e-10, max_iter=2000):
+        """SMatrix::amg (array.cpp:4534-4563): x += one V-cycle of the residual
+        from x = 0 until ||b - A x|| / ||b|| < tol; smoothed aggregation."""
+        if A._rows != A._cols:
+            raise ValueError("AMG needs a square matrix")
+        if A._cols != len(b):
+            raise ValueError("AMG: matrix columns differ from vector length")
+        b = _f64(b)
+        if float(np.sqrt(np.dot(b, b))) < 1e-300:
+            return np.zeros(len(b)), 0
+        ctx = SMatrix.context()
+        pc = Precond(ctx, A.device(), PC_SA_AMG)
+        x, st = solve(ctx, A.device(), b, STATIONARY, pc, raise_on_error=False, tol=tol, maxit=max_iter)
+        if st["status"] not in (OK, DIVERGED):
+            ctx.check(st["status"], "amg")
+        return x, st["it"]
+
+    def transpose(self) -> "SMatrix":
+        T = self.device().transpose()
+        return SMatrix(self._cols, self._rows, T.v, row_ptr=T.rp, col_idx=T.ci)
+
+    def __mul__(self, B: "SMatrix") -> "SMatrix":
+        if self._cols != B._rows:
+            raise ValueError("matrix product: columns of A differ from rows of B")
+        P = self.device().matmul(B.device())
+        return SMatrix(self._rows, B._cols, P.v, row_ptr=P.rp, col_idx=P.ci)
 
 
 def load_extension() -> str:

@@ -1389,4 +1389,9 @@ std::unique_ptr<PcImpl> make_pc_amg_csr(b2s_ctx* ctx, const CsrDev& A, const b2s
     return build_amg(ctx, ref, o, std::move(B));
 }
 
+// scalar (bs = 1) product and transpose for general CSR operators: the
+// C ABI's b2s_csr_matmul / b2s_csr_transpose (csr.cu)
+void scalar_matmul(b2s_ctx* ctx, const BaijDev& A, const BaijDev& B, BaijDev& C) { block_matmul<1>(ctx, A, B, C); }
+void scalar_transpose(b2s_ctx* ctx, const BaijDev& A, BaijDev& T) { block_transpose<1>(ctx, A, T); }
+
 }  // namespace b2s

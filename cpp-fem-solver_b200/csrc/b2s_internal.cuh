@@ -564,6 +564,12 @@ void build_redblack(b2s_ctx* ctx, const CsrDev& A, RedBlack& rb, const char* wha
 std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);
 std::unique_ptr<PcImpl> make_pc_ssor(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);
 std::unique_ptr<PcImpl> make_pc_amg_csr(b2s_ctx* ctx, const CsrDev& A, const b2s_pc_opts& o);
+// C = A B and T = A^T for bs = 1 operators on the device (amg.cu): sorted
+// columns, sums in the reference's order (SMatrix::operator*,
+// array.cpp:2336-2447; SMatrix::transpose, array.cpp:2201-2234)
+void scalar_matmul(b2s_ctx* ctx, const BaijDev& A, const BaijDev& B, BaijDev& C);
+void scalar_transpose(b2s_ctx* ctx, const BaijDev& A, BaijDev& T);
+
 std::unique_ptr<PcImpl> make_pc_amg_baij(b2s_ctx* ctx, const BaijDev& A, const b2s_pc_opts& o);
 std::unique_ptr<PcImpl> make_pc_bjacobi(b2s_ctx* ctx, const BaijDev& A);
 std::unique_ptr<PcImpl> make_pc_bilu0(b2s_ctx* ctx, const BaijDev& A, const b2s_pc_opts& o);

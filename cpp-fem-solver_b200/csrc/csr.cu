@@ -65,6 +65,57 @@ __global__ void k_extract_diag(uint32_t n, const uint32_t* __restrict__ rp, cons
     }
 }
 
+// A device-built pattern (row pointers on the device) becomes a CSR handle's
+// storage: padded copies of the columns and values, the host-side row
+// partition of the SpMV, the longest row and the diagonal -- what
+// b2s_csr_create derives from host arrays.
+static void csr_adopt(b2s_ctx* ctx, CsrDev& d, uint32_t n, uint32_t m, DBuf<uint32_t>&& rp, const uint32_t* ci,
+                      const double* v)
+{
+    std::vector<uint32_t> h_rp((size_t)n + 1);
+    d2h(ctx, h_rp.data(), rp.p, h_rp.size() * sizeof(uint32_t));
+    sync(ctx);
+    const uint32_t nnz = h_rp[n];
+    uint32_t max_row = 0;
+    for (uint32_t i = 0; i < n; ++i) max_row = std::max(max_row, h_rp[i + 1] - h_rp[i]);
+    d.n = n;
+    d.m = m;
+    d.nnz = nnz;
+    d.max_row = max_row;
+    d.rp = std::move(rp);
+    d.ci.alloc((size_t)nnz + 8);
+    d.v.alloc((size_t)nnz + 8);
+    B2S_CUDA(cudaMemsetAsync(d.ci.p, 0, d.ci.bytes(), ctx->stream));
+    B2S_CUDA(cudaMemsetAsync(d.v.p, 0, d.v.bytes(), ctx->stream));
+    d2d(ctx, d.ci.p, ci, (size_t)nnz * sizeof(uint32_t));
+    d2d(ctx, d.v.p, v, (size_t)nnz * sizeof(double));
+    std::vector<uint32_t> blk;
+    build_row_blocks(h_rp.data(), n, 1, kSpmvRowsPerCta, kSpmvNnzPerCta, blk);
+    d.nblk = (uint32_t)blk.size() - 1;
+    d.blk_row = upload(ctx, blk.data(), blk.size());
+    if (n == m && n > 0)
+    {
+        d.diag.alloc(n);
+        B2S_LAUNCH(ctx, k_extract_diag, stream_grid(ctx, n), kThreads, 0, n, d.rp.p, d.ci.p, d.v.p, d.diag.p);
+    }
+    sync(ctx);
+}
+
+// a bs = 1 block view of a CSR handle (device copies)
+static void csr_as_scalar_blocks(b2s_ctx* ctx, const CsrDev& A, BaijDev& B)
+{
+    B.bs = 1;
+    B.nbr = A.n;
+    B.nbc = A.m;
+    B.nnzb = A.nnz;
+    B.rp.alloc((size_t)A.n + 1);
+    B.ci.alloc(A.nnz ? A.nnz : 1);
+    B.v.alloc(A.nnz ? A.nnz : 1);
+    d2d(ctx, B.rp.p, A.rp.p, ((size_t)A.n + 1) * sizeof(uint32_t));
+    d2d(ctx, B.ci.p, A.ci.p, (size_t)A.nnz * sizeof(uint32_t));
+    d2d(ctx, B.v.p, A.v.p, (size_t)A.nnz * sizeof(double));
+}
+
 void spmv(b2s_ctx* ctx, const CsrDev& A, const double* x, double* y, const int* done)
 {
     if (A.n == 0) return;
@@ -178,6 +229,63 @@ b2s_status b2s_spmv(b2s_ctx* ctx, const b2s_csr* A, const double* x, double* y)
         h2d(ctx, dx.p, x, dx.bytes());
         spmv(ctx, A->d, dx.p, dy.p);
         d2h(ctx, y, dy.p, dy.bytes());
+        sync(ctx);
+    });
+}
+
+b2s_status b2s_csr_matmul(b2s_ctx* ctx, const b2s_csr* A, const b2s_csr* B, b2s_csr** out)
+{
+    if (!ctx || !A || !B || !out) return B2S_INVALID_ARG;
+    *out = nullptr;
+    b2s_csr* C = new b2s_csr();
+    C->ctx = ctx;
+    const b2s_status st = guarded(ctx, [&] {
+        B2S_CUDA(cudaSetDevice(ctx->device));
+        need(A->d.m == B->d.n, B2S_SHAPE, "matmul: columns of A differ from rows of B");
+        BaijDev a, b, c;
+        csr_as_scalar_blocks(ctx, A->d, a);
+        csr_as_scalar_blocks(ctx, B->d, b);
+        scalar_matmul(ctx, a, b, c);
+        csr_adopt(ctx, C->d, A->d.n, B->d.m, std::move(c.rp), c.ci.p, c.v.p);
+    });
+    if (st != B2S_OK)
+    {
+        delete C;
+        return st;
+    }
+    *out = C;
+    return B2S_OK;
+}
+
+b2s_status b2s_csr_transpose(b2s_ctx* ctx, const b2s_csr* A, b2s_csr** out)
+{
+    if (!ctx || !A || !out) return B2S_INVALID_ARG;
+    *out = nullptr;
+    b2s_csr* T = new b2s_csr();
+    T->ctx = ctx;
+    const b2s_status st = guarded(ctx, [&] {
+        B2S_CUDA(cudaSetDevice(ctx->device));
+        BaijDev a, t;
+        csr_as_scalar_blocks(ctx, A->d, a);
+        scalar_transpose(ctx, a, t);
+        csr_adopt(ctx, T->d, A->d.m, A->d.n, std::move(t.rp), t.ci.p, t.v.p);
+    });
+    if (st != B2S_OK)
+    {
+        delete T;
+        return st;
+    }
+    *out = T;
+    return B2S_OK;
+}
+
+b2s_status b2s_csr_export(b2s_ctx* ctx, const b2s_csr* A, uint32_t* row_ptr, uint32_t* col_idx, double* values)
+{
+    if (!ctx || !A) return B2S_INVALID_ARG;
+    return guarded(ctx, [&] {
+        if (row_ptr) d2h(ctx, row_ptr, A->d.rp.p, ((size_t)A->d.n + 1) * sizeof(uint32_t));
+        if (col_idx) d2h(ctx, col_idx, A->d.ci.p, (size_t)A->d.nnz * sizeof(uint32_t));
+        if (values) d2h(ctx, values, A->d.v.p, (size_t)A->d.nnz * sizeof(double));
         sync(ctx);
     });
 }

@@ -1,5 +1,6 @@
 // sparse::SMatrix drop-in (include/b2s/math/array.hpp) over the b2s C ABI.
-//   constructors / accessors / transpose / operator*: array.cpp:2072-2447
+//   constructors / accessors: array.cpp:2072-2198; transpose / operator*
+//   (on the device): array.cpp:2201-2447
 //   factories: array.cpp:2450-3398; solvers: array.cpp:3445-4533
 // Host-side containers keep the reference's CSR semantics; every solve runs
 // on the GPU against a device copy uploaded once per matrix.
@@ -191,57 +192,34 @@ namespace sparse
         return dev_.get();
     }
 
+    namespace detail
+    {
+        // a device-built CSR handle back into host vectors
+        static SMatrix from_device(b2s_csr* h, uint32_t rows, uint32_t cols)
+        {
+            std::shared_ptr<b2s_csr> keep(h, [](b2s_csr* p) { b2s_csr_destroy(p); });
+            uint32_t n = 0, m = 0, nnz = 0;
+            check(b2s_csr_info(h, &n, &m, &nnz), "matrix info");
+            std::vector<uint32_t> rp((size_t)rows + 1), ci(nnz);
+            std::vector<double> vv(nnz);
+            check(b2s_csr_export(context(), h, rp.data(), ci.data(), vv.data()), "matrix download");
+            return SMatrix(rows, cols, std::move(rp), std::move(ci), std::move(vv));
+        }
+    }
+
     SMatrix SMatrix::transpose() const
     {
-        std::vector<uint32_t> rp(cols_ + 1, 0);
-        for (uint32_t p = 0; p < nnz(); ++p) rp[col_idx_[p] + 1]++;
-        for (uint32_t i = 0; i < cols_; ++i) rp[i + 1] += rp[i];
-        std::vector<uint32_t> ci(nnz()), off(rp.begin(), rp.end() - 1);
-        std::vector<double> vv(nnz());
-        for (uint32_t i = 0; i < rows_; ++i)
-            for (uint32_t p = row_ptr_[i]; p < row_ptr_[i + 1]; ++p)
-            {
-                const uint32_t q = off[col_idx_[p]]++;
-                ci[q] = i;
-                vv[q] = values_[p];
-            }
-        return SMatrix(cols_, rows_, std::move(rp), std::move(ci), std::move(vv));
+        b2s_csr* t = nullptr;
+        detail::check(b2s_csr_transpose(detail::context(), device(), &t), "transpose");
+        return detail::from_device(t, cols_, rows_);
     }
 
     SMatrix SMatrix::operator*(const SMatrix& B) const
     {
-        const uint32_t n = rows_, m = B.cols_;
-        std::vector<int64_t> marker(m, -1);
-        std::vector<double> acc(m, 0.0);
-        std::vector<uint32_t> rp(n + 1, 0), ci, cols;
-        std::vector<double> vv;
-        for (uint32_t i = 0; i < n; ++i)
-        {
-            cols.clear();
-            for (uint32_t p = row_ptr_[i]; p < row_ptr_[i + 1]; ++p)
-            {
-                const uint32_t j = col_idx_[p];
-                for (uint32_t q = B.row_ptr_[j]; q < B.row_ptr_[j + 1]; ++q)
-                {
-                    const uint32_t k = B.col_idx_[q];
-                    if (marker[k] != (int64_t)i)
-                    {
-                        marker[k] = i;
-                        cols.push_back(k);
-                    }
-                    acc[k] += values_[p] * B.values_[q];
-                }
-            }
-            std::sort(cols.begin(), cols.end());
-            for (uint32_t k : cols)
-            {
-                ci.push_back(k);
-                vv.push_back(acc[k]);
-                acc[k] = 0.0;
-            }
-            rp[i + 1] = (uint32_t)ci.size();
-        }
-        return SMatrix(n, m, std::move(rp), std::move(ci), std::move(vv));
+        if (cols_ != B.rows_) throw std::invalid_argument("matrix product: columns of A differ from rows of B");
+        b2s_csr* c = nullptr;
+        detail::check(b2s_csr_matmul(detail::context(), device(), B.device(), &c), "matrix product");
+        return detail::from_device(c, rows_, B.cols_);
     }
 
     double SMatrix::dot(const std::vector<double>& a, const std::vector<double>& b)
@@ -348,5 +326,20 @@ namespace sparse
                                                          double tol, int max_iter)
     {
         return detail::sor_csr(A, b, 1, omega, tol, max_iter);
+    }
+
+    std::tuple<std::vector<double>, int> SMatrix::amg(const SMatrix& A, const std::vector<double>& b, double tol,
+                                                      int max_iter)
+    {
+        if (A.rows() != A.cols()) throw std::invalid_argument("AMG needs a square matrix");
+        if (A.cols() != b.size()) throw std::invalid_argument("AMG: matrix columns differ from vector length");
+        const uint32_t n = A.rows();
+        double nb = 0.0;
+        for (double v : b) nb += v * v;
+        if (std::sqrt(nb) < 1e-300) return {std::vector<double>(n, 0.0), 0};
+        b2s_pc* h = nullptr;
+        detail::check(b2s_pc_create(detail::context(), A.device(), B2S_PC_SA_AMG, nullptr, &h), "AMG setup");
+        std::shared_ptr<b2s_pc> pc(h, [](b2s_pc* p) { b2s_pc_destroy(p); });
+        return detail::solve_op(A.device(), nullptr, n, b, B2S_STATIONARY, pc.get(), nullptr, 30, tol, max_iter);
     }
 }

@@ -13,6 +13,7 @@
 // the extra iterations enqueued past convergence cost only launch time.
 //
 // The returned iteration counts follow the reference exactly:
+//   stationary (SMatrix::amg) it_end = index of the last residual check
 //   pcg      it_end = index of the last fully completed iteration
 //   bicgstab it_end = index of the last iteration (it_end = it before the check)
 //   gmres    it_end = total Arnoldi steps - 1
@@ -1151,6 +1152,98 @@ struct BodyResidual  // r = b - Ax (Ax given), rr
     __device__ void last(const double* t) const { st->aux[0] = sqrt(t[0]); }
 };
 
+// ------------------------------------------------- stationary iteration
+// SMatrix::amg (array.cpp:4534-4563): from x = 0, at index it: r = b - A x;
+// stop with it_end = it when ||r|| / ||b|| < tol, else x += M^-1 r (one
+// V-cycle from zero).  Running out of max_iter leaves it_end = max_iter - 1
+// with every correction applied.
+
+// r = b - A x per row, rr; the stopping test at index st->it
+struct EpiStatRes
+{
+    static constexpr int NV = 1;
+    double* r;
+    const double* b;
+    KState* st;
+    __device__ void row(uint32_t i, double s, double* acc) const
+    {
+        const double d = b[i] - s;
+        r[i] = d;
+        acc[0] += d * d;
+    }
+    __device__ void last(const double* t) const
+    {
+        const double normr = sqrt(t[0]);
+        st->normr = normr;
+        st->relres = normr / st->normb;
+        st->it_end = st->it;
+        st->iters = st->it;
+        if (st->relres < st->tol)
+            finish(st, B2S_OK);
+        else if (!(normr == normr) || isinf(normr))
+        {
+            st->it_end = st->maxit - 1;  // the reference runs on with NaN to max_iter
+            finish(st, B2S_DIVERGED);
+        }
+    }
+};
+
+// x += d; next index; max_iter stop
+struct BodyStatStep
+{
+    static constexpr int NV = 1;
+    double* x;
+    const double* d;
+    KState* st;
+    __device__ void elem(uint64_t i, double* acc) const
+    {
+        (void)acc;
+        x[i] += d[i];
+    }
+    __device__ void last(const double* t) const
+    {
+        (void)t;
+        st->it += 1;
+        st->iters = st->it;
+        if (st->it >= st->maxit) finish(st, B2S_OK);
+    }
+};
+
+static void run_stationary(Solve& S, const double* b, double* x, b2s_stats* stats)
+{
+    b2s_ctx* ctx = S.ctx;
+    const uint64_t n = S.A.n;
+    Work W(ctx, 3 * padded(n));
+    double *r = W.take(n), *d = W.take(n), *tmp = W.take(n);
+    KState* st = S.st;
+    const int* done = S.done;
+    S.init_state();
+    B2S_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    fill(ctx, x, 0.0, n);
+    launch_vec(ctx, n, done, BodyNormB{b, st});
+    KState h = S.read_state();
+    if (!h.done && S.o.maxit == 0)  // the reference's loop body never runs
+    {
+        h.done = 1;
+        h2d(ctx, &st->done, &h.done, sizeof(int));
+    }
+    if (!h.done)
+    {
+        auto body = [&] {
+            op_apply_epi(ctx, S.A, x, tmp, done, EpiStatRes{r, b, st});
+            S.pc_apply(r, d);
+            launch_vec(ctx, n, done, BodyStatStep{x, d, st});
+        };
+        S.loop(body);
+    }
+    B2S_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    S.true_residual(b, x, tmp);
+    h = S.read_state();
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    S.finish_stats(stats, h, ms);
+}
+
 static void run_method(Solve& S, b2s_method method, const double* b, double* x, b2s_stats* stats)
 {
     switch (method)
@@ -1160,6 +1253,7 @@ static void run_method(Solve& S, b2s_method method, const double* b, double* x, 
         case B2S_GMRES:
         case B2S_BLOCK_GMRES: run_gmres(S, b, x, stats, false); break;
         case B2S_FGMRES: run_gmres(S, b, x, stats, true); break;
+        case B2S_STATIONARY: run_stationary(S, b, x, stats); break;
         default: fail(B2S_INVALID_ARG, "unknown Krylov method");
     }
 }

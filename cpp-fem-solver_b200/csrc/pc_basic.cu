@@ -130,6 +130,8 @@ b2s_status b2s_pc_create(b2s_ctx* ctx, const b2s_csr* A, b2s_pc_kind kind, const
     b2s_status st = guarded(ctx, [&] {
         B2S_CUDA(cudaSetDevice(ctx->device));
         need(A->d.n == A->d.m, B2S_SHAPE, "preconditioner needs a square matrix");
+        need(o.precision == B2S_FP64 || o.precision == B2S_FP32, B2S_UNSUPPORTED,
+             "preconditioner precision: only B2S_FP64 and B2S_FP32 storage exist");
         const double t0 = now_ms();
         switch (kind)
         {
@@ -169,6 +171,8 @@ b2s_status b2s_pc_create_baij(b2s_ctx* ctx, const b2s_baij* A, b2s_pc_kind kind,
     b2s_status st = guarded(ctx, [&] {
         B2S_CUDA(cudaSetDevice(ctx->device));
         need(A->d.nbr == A->d.nbc, B2S_SHAPE, "block preconditioner needs a square block matrix");
+        need(o.precision == B2S_FP64 || o.precision == B2S_FP32, B2S_UNSUPPORTED,
+             "preconditioner precision: only B2S_FP64 and B2S_FP32 storage exist");
         const double t0 = now_ms();
         switch (kind)
         {

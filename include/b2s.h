@@ -84,6 +84,22 @@ b2s_status b2s_csr_create(b2s_ctx* ctx, uint32_t n, uint32_t m, const uint32_t* 
 b2s_status b2s_csr_destroy(b2s_csr* A);
 b2s_status b2s_csr_info(const b2s_csr* A, uint32_t* n, uint32_t* m, uint32_t* nnz);
 
+/* C = A B on the device (SMatrix::operator*, array.cpp:2336-2447): columns
+ * ascending in every row, each entry the sum of its products in the
+ * reference's order (A's row entries ascending, then B's), so the values equal
+ * the reference's bit for bit; entries that sum to zero are kept, as the
+ * reference keeps them.  One difference: a product column that only one row
+ * of A B touches is kept here, while the reference leaves that slot as
+ * (column 0, value 0) because its marker array is not reset between its
+ * symbolic and numeric passes (array.cpp:2357-2443). */
+b2s_status b2s_csr_matmul(b2s_ctx* ctx, const b2s_csr* A, const b2s_csr* B, b2s_csr** out);
+/* T = A^T on the device (SMatrix::transpose, array.cpp:2201-2234): every row
+ * of T lists its entries in ascending column order, values copied. */
+b2s_status b2s_csr_transpose(b2s_ctx* ctx, const b2s_csr* A, b2s_csr** out);
+/* Copies a handle's arrays to host memory: row_ptr (n+1), col_idx and values
+ * (nnz each); a NULL array is skipped. */
+b2s_status b2s_csr_export(b2s_ctx* ctx, const b2s_csr* A, uint32_t* row_ptr, uint32_t* col_idx, double* values);
+
 /* Block-CSR (BAIJ) matrix, BlockMatrix<double,BS> constructor
  * (blockMatrix.hpp:175-186).  bs in {1, 2, 3, 4}.  values holds
  * nnzb*bs*bs doubles, row-major inside each block; vectors are node-major. */
@@ -144,7 +160,8 @@ typedef enum b2s_precision
                      accumulate in FP32; SA-AMG: FP32 copies of A, P, R and D^-1 on every level,
                      FP64 vectors and arithmetic, the coarsest dense LU in FP64; the diagonal,
                      block-Jacobi and SSOR preconditioners ignore it */
-    B2S_BF16 = 2  /* accepted and treated as B2S_FP32 (no BF16 storage path) */
+    B2S_BF16 = 2  /* reserved: no preconditioner stores BF16 values, so b2s_pc_create* returns
+                     B2S_UNSUPPORTED (FP32 AMG values already left the V-cycle time unchanged) */
 } b2s_precision;
 
 /* Triangular-solve schedule for IC(0)/ILU(0)/block ILU(0). */
@@ -265,7 +282,11 @@ typedef enum b2s_method
     B2S_BICGSTAB = 1,  /* SMatrix::bicgstab, array.cpp:3602-3842 */
     B2S_GMRES = 2,     /* SMatrix::gmres, array.cpp:4190-4533; BlockMatrix::gmres */
     B2S_FGMRES = 3,    /* flexible GMRES (Z stored), for variable / low-precision preconditioners */
-    B2S_BLOCK_GMRES = 4 /* name table of BlockMatrix::gmres for b2s_pc_kind_from_name only */
+    B2S_BLOCK_GMRES = 4, /* name table of BlockMatrix::gmres for b2s_pc_kind_from_name only */
+    B2S_STATIONARY = 5   /* x += M^-1 (b - A x) from x = 0 with the true residual checked before every
+                            correction: SMatrix::amg (array.cpp:4534-4563) when M is an AMG
+                            preconditioner (one V-cycle per correction); it = index of the last check,
+                            max_iter - 1 when the loop runs out */
 } b2s_method;
 
 /* Gram-Schmidt variant for (F)GMRES. */

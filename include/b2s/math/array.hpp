@@ -12,14 +12,17 @@
 //   constructors (COO uint32 vectors: sorted, duplicates merged, zeros
 //   dropped; CSR vectors taken as given), rows/cols/nnz/values/row_ptr/
 //   col_idx, transpose, operator*, dot, spmv, the make_*_preconditioner
-//   factories, pcg / bicgstab / gmres (both overloads) returning
-//   std::tuple<std::vector<double>, int> with the reference's iteration
-//   counts, and the same exception types (std::invalid_argument for argument
-//   and shape errors, std::runtime_error for numerical breakdown).
+//   factories, pcg / bicgstab / gmres (both overloads) / sor / sor_rb / amg
+//   returning std::tuple<std::vector<double>, int> with the reference's
+//   iteration counts, and the same exception types (std::invalid_argument for
+//   argument and shape errors, std::runtime_error for numerical breakdown).
 // Differences, by design:
 //   - "amg" is smoothed aggregation (the reference's classical C/F AMG
-//     produces NaN at the benchmark sizes); sor / sor_rb / amg stand-alone
-//     solvers are not provided.
+//     produces NaN at the benchmark sizes), in the "amg" preconditioner string,
+//     make_amg_preconditioner and the stand-alone amg solver alike.
+//   - transpose and operator* run on the GPU; operator* keeps every product
+//     column (the reference's drops a column that only one row of the product
+//     touches, because its marker array is not reset between its passes).
 //   - Extensions: pcg and bicgstab also accept a std::function preconditioner;
 //     a preconditioner returned by a make_* factory here runs on the GPU even
 //     when passed through std::function to gmres/pcg.
@@ -117,6 +120,11 @@ namespace sparse
                                                             double omega, double tol = 1e-10, int max_iter = 2000);
             static std::tuple<std::vector<double>, int> sor_rb(const SMatrix& A, const std::vector<double>& b,
                                                                double omega, double tol = 1e-10, int max_iter = 2000);
+            // stand-alone AMG (array.hpp:367-372, array.cpp:4534-4563): from x = 0,
+            // x += one V-cycle of the residual until ||b - A x|| / ||b|| < tol;
+            // returns the index of the last residual check
+            static std::tuple<std::vector<double>, int> amg(const SMatrix& A, const std::vector<double>& b,
+                                                            double tol = 1e-10, int max_iter = 2000);
             // extensions with a functor preconditioner
             static std::tuple<std::vector<double>, int> pcg(const SMatrix& A, const std::vector<double>& b,
                                                             const Precond& solveM, double tol = 1e-10,

@@ -2397,9 +2397,46 @@ static const char* resolve_precond(int method, const char* name)
     return NULL;
 }
 
+/* SMatrix::amg main loop, array.cpp:4534-4563, with the preconditioner given
+ * (one V-cycle from zero per correction when it is an AMG): from x = 0, at
+ * index k: r = b - A x, rr summed in row order; stop with it = k when
+ * sqrt(rr) / ||b|| < tol, else x += M^-1 r.  Running out leaves it = maxit - 1. */
+static int stationary(const void* A, matvec_fn mv, uint32_t n, orc_pc* pc, const double* b, double tol, int maxit,
+                      double* x, int* itout)
+{
+    memset(x, 0, 8 * (size_t)n);
+    *itout = 0;
+    const double normb = sqrt(orc_dot(n, b, b));
+    if (normb < 1e-300) return ORC_OK;
+    double* r = (double*)xcalloc(n, 8);
+    double* d = (double*)xcalloc(n, 8);
+    double* Ax = (double*)xcalloc(n, 8);
+    int it_end = 0;
+    for (int k = 0; k < maxit; ++k)
+    {
+        mv(A, x, Ax);
+        double rr = 0.0;
+        for (uint32_t i = 0; i < n; ++i)
+        {
+            r[i] = b[i] - Ax[i];
+            rr += r[i] * r[i];
+        }
+        it_end = k;
+        if (sqrt(rr) / normb < tol) break;
+        pc_apply_or_copy(pc, n, r, d);
+        for (uint32_t i = 0; i < n; ++i) x[i] += d[i];
+    }
+    *itout = it_end;
+    free(r);
+    free(d);
+    free(Ax);
+    return ORC_OK;
+}
+
 static int run_method(const void* A, matvec_fn mv, uint32_t n, int method, orc_pc* pc, int restart, double tol,
                       int maxit, const double* b, double* x, int* it, char* err, int errlen)
 {
+    if (method == 5) return stationary(A, mv, n, pc, b, tol, maxit, x, it);
     if (method == 0) return krylov_pcg(A, mv, n, pc, b, tol, maxit, x, it, err, errlen);
     if (method == 1) return krylov_bicgstab(A, mv, n, pc, b, tol, maxit, x, it, err, errlen);
     return krylov_gmres(A, mv, n, pc, b, restart, tol, maxit, x, it, err, errlen);

@@ -85,7 +85,9 @@ int orc_colour_export(orc_pc* pc, uint32_t* ncolor, uint32_t* color_ptr, uint32_
 uint32_t orc_levels(uint32_t n, const uint32_t* rp, const uint32_t* ci, int upper, uint32_t* level);
 
 /* ---- solvers (array.cpp:3445-3842, 4190-4533) ----
- * method: 0 pcg, 1 bicgstab, 2 gmres.  The preconditioner string follows each
+ * method: 0 pcg, 1 bicgstab, 2 gmres, 5 the stationary loop of SMatrix::amg
+ * (array.cpp:4534-4563: x += M^-1 (b - A x) from x = 0 with the true residual
+ * checked before every correction).  The preconditioner string follows each
  * solver's own alias table; "amg" maps to "sa_amg_mis". */
 int orc_solve(const orc_csr* A, int method, const char* precond, int restart, double tol, int maxit,
               const double* b, double* x, int* it, char* err, int errlen);

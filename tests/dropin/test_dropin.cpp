@@ -1,6 +1,7 @@
 // Exercises the C++ drop-in headers (include/b2s/math/*.hpp) the way the
 // reference's own test programs use sparse::SMatrix and block::BlockMatrix:
 // known-answer checks with manufactured solutions, exit code 0 on success.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <stdexcept>
@@ -133,6 +134,30 @@ int main()
         bool bad = false;
         try { SMatrix::sor(S, bs, 2.5); } catch (const std::invalid_argument&) { bad = true; }
         CHECK(bad, "sor with omega >= 2 must throw std::invalid_argument");
+    }
+    // stand-alone AMG (array.hpp:367-372): x += V-cycle(r) until the true residual passes
+    {
+        auto [xa, ita] = SMatrix::amg(A, b, 1e-8, 200);
+        const double ra = relres(A, xa, b);
+        std::printf("[amg] it=%d relres=%.2e\n", ita, ra);
+        CHECK(ra < 1e-8 && ita > 0 && ita < 200, "amg relres %.3e it %d", ra, ita);
+        auto [x0, it0] = SMatrix::amg(A, std::vector<double>(A.rows(), 0.0));
+        CHECK(it0 == 0 && x0.size() == A.rows(), "amg zero rhs");
+    }
+    // transpose and product on the device (array.cpp:2201-2447)
+    {
+        const SMatrix T = A.transpose();
+        CHECK(T.rows() == A.cols() && T.nnz() == A.nnz() && T.row_ptr() == A.row_ptr() && T.col_idx() == A.col_idx() &&
+                  T.values() == A.values(),
+              "transpose of a symmetric matrix is itself");
+        const SMatrix A2 = A * A;
+        const std::vector<double> y1 = SMatrix::spmv(A2, b), y2 = SMatrix::spmv(A, SMatrix::spmv(A, b));
+        double e = 0.0, nrm = 0.0;
+        for (size_t i = 0; i < y1.size(); ++i) { e = std::max(e, std::fabs(y1[i] - y2[i])); nrm = std::max(nrm, std::fabs(y2[i])); }
+        CHECK(e <= 1e-12 * nrm, "(A A) b == A (A b): %.3e", e);
+        bool bad = false;
+        try { (void)(A * SMatrix(3, 3, std::vector<uint32_t>(4, 0), {}, {})); } catch (const std::invalid_argument&) { bad = true; }
+        CHECK(bad, "product with mismatched shapes must throw std::invalid_argument");
     }
     // exceptions
     bool threw = false;

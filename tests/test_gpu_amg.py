@@ -163,3 +163,46 @@ def test_amg_wide_galerkin_rows(b2s, ctx, orc):
     for k, lv in enumerate(levels):
         Arp, Aci, Av = M.export(f"amg.{k}.A")
         assert np.array_equal(Arp, lv["Arp"]) and np.array_equal(Aci, lv["Aci"]) and np.array_equal(Av, lv["Av"]), k
+
+
+@pytest.mark.parametrize("case", ["poisson2d_48", "poisson3d_16", "maxit"])
+def test_stationary_amg(b2s, ctx, orc, case):
+    """SMatrix::amg (array.cpp:4534-4563) as B2S_STATIONARY with the SA V-cycle:
+    x += V-cycle(b - A x) from x = 0, the true residual checked before every
+    correction.  The V-cycle equals the oracle's bit for bit and x is updated
+    elementwise, so the iterates are the oracle's bit for bit; only the norm's
+    association differs, which could move a stop by one check at most."""
+    if case == "poisson3d_16":
+        n, rp, ci, v = b2s.gen_poisson3d(16)
+    else:
+        n, rp, ci, v = P.poisson2d(48)
+    tol, maxit = (1e-10, 200) if case != "maxit" else (1e-14, 5)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(11, n)
+    M = b2s.Precond(ctx, A, b2s.PC_SA_AMG)
+    x, st = b2s.solve(ctx, A, b, b2s.STATIONARY, M, tol=tol, maxit=maxit)
+    Ao = orc.csr(n, n, rp, ci, v)
+    xo, io = orc.solve_pc(Ao, 5, orc.pc(Ao, "sa_amg_mis"), b, tol, maxit)
+    assert st["status"] == 0
+    if case == "maxit":
+        assert st["it"] == io == maxit - 1 and st["iterations"] == maxit
+        assert np.array_equal(x, xo)
+    else:
+        assert abs(st["it"] - io) <= 1
+        if st["it"] == io:
+            assert np.array_equal(x, xo)
+        assert st["relres_true"] < tol and 0 < st["it"] < maxit
+    # the Python mirror of the drop-in call
+    Ms = b2s.SMatrix(n, n, v, row_ptr=rp, col_idx=ci)
+    xs, its = b2s.SMatrix.amg(Ms, b, tol, maxit)
+    assert its == st["it"] and np.array_equal(xs, x)
+
+
+def test_stationary_zero_rhs_and_maxit0(b2s, ctx):
+    n, rp, ci, v = P.poisson2d(16)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    M = b2s.Precond(ctx, A, b2s.PC_SA_AMG)
+    x, st = b2s.solve(ctx, A, np.zeros(n), b2s.STATIONARY, M, tol=1e-10, maxit=50)
+    assert st["it"] == 0 and not x.any()
+    x, st = b2s.solve(ctx, A, b2s.uniform(2, n), b2s.STATIONARY, M, tol=1e-10, maxit=0)
+    assert st["it"] == 0 and not x.any()

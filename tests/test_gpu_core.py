@@ -227,3 +227,65 @@ def test_fgmres_fp32_refinement(b2s, ctx):
     assert st["relres_true"] < 1e-10
     r = b - A.spmv(x)
     assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10
+
+
+def rect_random(n, m, density, seed):
+    rng = np.random.default_rng(seed)
+    dense = (rng.random((n, m)) < density) * rng.uniform(-1, 1, (n, m))
+    rp = np.concatenate([[0], np.cumsum((dense != 0).sum(1))]).astype(np.uint32)
+    return rp, np.nonzero(dense)[1].astype(np.uint32), dense[dense != 0]
+
+
+@pytest.mark.parametrize("case", ["poisson_sq", "rect", "wide", "diag"])
+def test_csr_matmul_transpose(b2s, ctx, orc, ref, case):
+    """C = A B and A^T on the device (b2s_csr_matmul / b2s_csr_transpose) equal
+    the restatement bit for bit: sorted columns, each entry summed in the
+    reference's order.  Where every product column is touched by two or more
+    rows the compiled reference gives the same arrays; "diag" is a product
+    whose columns are each touched by one row, where the reference's marker
+    array (not reset between its passes) drops them (tested on the CPU in
+    test_oracle_pin.py::test_reference_spgemm_single_touch_defect)."""
+    if case == "poisson_sq":
+        n, rp, ci, v = P.poisson2d(40)
+        a, b = (n, n, rp, ci, v), (n, n, rp, ci, v)
+    elif case == "rect":
+        a = (300, 500) + rect_random(300, 500, 0.02, 1)
+        b = (500, 200) + rect_random(500, 200, 0.03, 2)
+    elif case == "wide":  # product rows wider than the symbolic hash table (512 columns)
+        a = (64, 64) + rect_random(64, 64, 0.5, 3)
+        b = (64, 2000) + rect_random(64, 2000, 0.5, 4)
+    else:
+        n = 1000
+        rp = np.arange(n + 1, dtype=np.uint32)
+        d = np.linspace(1.0, 2.0, n)
+        a = b = (n, n, rp, rp[:-1].copy(), d)
+    A, B = b2s.CSR(ctx, *a), b2s.CSR(ctx, *b)
+    C = A.matmul(B)
+    Ao, Bo = orc.csr(*a), orc.csr(*b)
+    Co = orc.matmul(Ao, Bo).export()
+    assert np.array_equal(C.rp, Co[0]) and np.array_equal(C.ci, Co[1]) and np.array_equal(C.v, Co[2])
+    if case != "diag":
+        Cr = ref.matmul(ref.csr(*a), ref.csr(*b)).export()
+        assert all(np.array_equal(x, y) for x, y in zip(Co, Cr))
+    T = A.transpose()
+    To = orc.transpose(Ao).export()
+    assert (T.n, T.m) == (a[1], a[0])
+    assert np.array_equal(T.rp, To[0]) and np.array_equal(T.ci, To[1]) and np.array_equal(T.v, To[2])
+    Tr = ref.transpose(ref.csr(*a)).export()
+    assert all(np.array_equal(x, y) for x, y in zip(To, Tr))
+    # the product is a usable operator: its SpMV equals A (B x)
+    x = np.random.default_rng(6).uniform(-1, 1, b[1])
+    assert rel(C.spmv(x), A.spmv(B.spmv(x))) < 1e-13
+
+
+def test_csr_matmul_shape_error(b2s, ctx):
+    n, rp, ci, v = P.poisson2d(8)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    B = b2s.CSR(ctx, 3, 3, np.zeros(4, np.uint32), np.zeros(0, np.uint32), np.zeros(0))
+    with pytest.raises(b2s.B2SInvalidArgument):
+        A.matmul(B)
+    M = b2s.SMatrix(n, n, v, row_ptr=rp, col_idx=ci)
+    with pytest.raises(ValueError):
+        M * b2s.SMatrix(3, 3, np.zeros(0), row_ptr=np.zeros(4, np.uint32), col_idx=np.zeros(0, np.uint32))
+    P2 = M * M
+    assert P2.rows() == n and np.array_equal(M.transpose().col_idx(), ci)

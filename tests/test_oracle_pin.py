@@ -37,6 +37,47 @@ def test_csr_spmv_and_coo(orc, ref, gen):
         assert np.array_equal(a, b)
 
 
+def test_reference_spgemm_single_touch_defect(orc, ref):
+    """The reference's SMatrix::operator* (array.cpp:2336-2447) shares its
+    marker array between the symbolic and the numeric pass without resetting
+    it, so in the numeric pass a column that only one row of the product
+    touches still carries that row's mark from the symbolic pass and is
+    skipped: its slot keeps (column 0, value 0).  At one thread a diagonal
+    times a diagonal loses every entry.  The restatement (and the library)
+    keep them; every other product is equal bit for bit."""
+    n = 6
+    rp = np.arange(n + 1, dtype=np.uint32)
+    ci = rp[:-1].copy()
+    d = np.arange(1.0, n + 1)
+    Cr = ref.matmul(ref.csr(n, n, rp, ci, d), ref.csr(n, n, rp, ci, d)).export()
+    Co = orc.matmul(orc.csr(n, n, rp, ci, d), orc.csr(n, n, rp, ci, d)).export()
+    assert np.array_equal(Cr[0], rp) and not Cr[1].any() and not Cr[2].any()
+    assert np.array_equal(Co[1], ci) and np.array_equal(Co[2], d * d)
+
+
+def test_stationary_loop(orc):
+    """The restatement of SMatrix::amg's loop (array.cpp:4534-4563) with an
+    identity preconditioner is Richardson's iteration x += (b - A x): on a
+    matrix scaled so that I - A is a contraction it stops at the first index
+    whose true residual passes, and it = maxit - 1 when the loop runs out."""
+    n, rp, ci, v = P.poisson2d(6)
+    v = v / 8.0
+    Ao = orc.csr(n, n, rp, ci, v)
+    b = np.linspace(-1.0, 1.0, n)
+    x, it = orc.solve_pc(Ao, 5, None, b, 1e-6, 10000)
+    xs, rel = np.zeros(n), []
+    for k in range(it + 1):
+        r = b - orc.spmv(Ao, xs)
+        rel.append(np.sqrt(np.sum(r * r)) / np.sqrt(np.sum(b * b)))
+        if rel[-1] < 1e-6:
+            break
+        xs = xs + r
+    assert len(rel) == it + 1 and rel[-1] < 1e-6 and min(rel[:-1]) >= 1e-6
+    assert np.array_equal(x, xs)
+    x5, it5 = orc.solve_pc(Ao, 5, None, b, 1e-30, 5)
+    assert it5 == 4
+
+
 def test_coo_out_of_range(orc, ref):
     import oracle
     for lib in (orc, ref):
