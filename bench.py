@@ -270,7 +270,8 @@ def run_suite(args):
         except Exception as e:  # the compiled reference did not travel
             print(json.dumps({"suite": "reference unavailable", "why": str(e)[:200]}), flush=True)
 
-    def gpu(A, n, kind, method, tol, maxit, reps=3, pco=None, so=None):
+    def gpu(A, n, kind, method, tol, maxit, reps=3, pco=None, so=None, x64=None):
+        """Best of `reps` timed solves; error_vs_fp64 = ||x - x64|| / ||x64||."""
         bt = torch.from_numpy(b2s.uniform(7, n)).to(dev)
         best = None
         for r in range(reps + 1):
@@ -290,9 +291,19 @@ def run_suite(args):
             cur = {"setup_ms": round(e0.elapsed_time(em), 3), "solve_ms": round(em.elapsed_time(e1), 3),
                    "iterations": st["iterations"], "relres_true": st["relres_true"], "status": st["status"]}
             cur["total_ms"] = round(cur["setup_ms"] + cur["solve_ms"], 3)
+            if x64 is not None:
+                x = xt.cpu().numpy()
+                cur["error_vs_fp64"] = float(np.linalg.norm(x - x64) / np.linalg.norm(x64))
             if best is None or cur["total_ms"] < best["total_ms"]:
                 best = cur
         return best
+
+    def fp64_solution(A, n, kind, method, so=None):
+        """FP64 solution to rtol 1e-12 (the yardstick of each line's error)."""
+        M = b2s.Precond(ctx, A, kind)
+        x, st = b2s.solve(ctx, A, b2s.uniform(7, n), method, M, tol=1e-12, maxit=5000, **(so or {}))
+        assert st["relres_true"] < 1e-11, st
+        return x
 
     def cpu(rp, ci, v, n, method, pc, tol, maxit):
         if ref is None:
@@ -311,45 +322,57 @@ def run_suite(args):
     # the B200-native apply for comparison: FP32 factor, 8 Jacobi sweeps per triangle (not the exact solve)
     sweeps8 = {"precision": b2s.FP32, "trsv": b2s.TRSV_JACOBI, "trsv_sweeps": 8}
 
+    # every line's error is against the FP64 solution of the same system to
+    # rtol 1e-12 (SA-AMG PCG for the SPD systems, GMRES(30) + ILU(0) for C3)
     c = "C1 poisson2d 256^2, rtol 1e-8"
     n, rp, ci, v = b2s.gen_poisson2d(256)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
-    emit(c, "pcg+diag", gpu(A, n, b2s.PC_DIAG, b2s.PCG, 1e-8, 20000), cpu(rp, ci, v, n, 0, "diag", 1e-8, 20000))
-    emit(c, "pcg+ic0", gpu(A, n, b2s.PC_IC0, b2s.PCG, 1e-8, 20000), cpu(rp, ci, v, n, 0, "ic", 1e-8, 20000))
-    emit(c, "pcg+ic0_fp32_j8 (inexact apply)", gpu(A, n, b2s.PC_IC0, b2s.PCG, 1e-8, 20000, pco=sweeps8), None)
+    x64 = fp64_solution(A, n, b2s.PC_SA_AMG, b2s.PCG)
+    emit(c, "pcg+diag", gpu(A, n, b2s.PC_DIAG, b2s.PCG, 1e-8, 20000, x64=x64),
+         cpu(rp, ci, v, n, 0, "diag", 1e-8, 20000))
+    emit(c, "pcg+ic0", gpu(A, n, b2s.PC_IC0, b2s.PCG, 1e-8, 20000, x64=x64), cpu(rp, ci, v, n, 0, "ic", 1e-8, 20000))
+    emit(c, "pcg+ic0_fp32_j8 (inexact apply)", gpu(A, n, b2s.PC_IC0, b2s.PCG, 1e-8, 20000, pco=sweeps8, x64=x64),
+         None)
     del A
 
     c = "C2 poisson3d 128^3, rtol 1e-10"
     n, rp, ci, v = b2s.gen_poisson3d(128)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
+    x64 = fp64_solution(A, n, b2s.PC_SA_AMG, b2s.PCG)
     for prec, pname in ((b2s.FP64, "fp64"), (b2s.FP32, "fp32")):
-        emit(c, f"pcg+sa_amg_{pname}", gpu(A, n, b2s.PC_SA_AMG, b2s.PCG, 1e-10, 2000, pco={"precision": prec}),
+        emit(c, f"pcg+sa_amg_{pname}", gpu(A, n, b2s.PC_SA_AMG, b2s.PCG, 1e-10, 2000, pco={"precision": prec},
+                                           x64=x64),
              "not run: the reference's aggregation does not coarsen this operator")
-    emit(c, "pcg+ilu0", gpu(A, n, b2s.PC_ILU0, b2s.PCG, 1e-10, 2000, reps=1),
+    emit(c, "pcg+ilu0", gpu(A, n, b2s.PC_ILU0, b2s.PCG, 1e-10, 2000, reps=1, x64=x64),
          cpu(rp, ci, v, n, 0, "ilu", 1e-10, 2000))
-    emit(c, "pcg+ilu0_fp32_j8 (inexact apply)", gpu(A, n, b2s.PC_ILU0, b2s.PCG, 1e-10, 2000, reps=1, pco=sweeps8),
-         None)
+    emit(c, "pcg+ilu0_fp32_j8 (inexact apply)", gpu(A, n, b2s.PC_ILU0, b2s.PCG, 1e-10, 2000, reps=1, pco=sweeps8,
+                                                    x64=x64), None)
     del A
 
     c = "C3 convdiff3d 96^3, rtol 1e-8"
     n, rp, ci, v = b2s.gen_convdiff3d(96)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
-    emit(c, "bicgstab+ilu0", gpu(A, n, b2s.PC_ILU0, b2s.BICGSTAB, 1e-8, 2000),
+    x64 = fp64_solution(A, n, b2s.PC_ILU0, b2s.GMRES, so={"restart": 30})
+    emit(c, "bicgstab+ilu0", gpu(A, n, b2s.PC_ILU0, b2s.BICGSTAB, 1e-8, 2000, x64=x64),
          cpu(rp, ci, v, n, 1, "ilu", 1e-8, 2000))
-    emit(c, "bicgstab+ilu0_fp32_j8 (inexact apply)", gpu(A, n, b2s.PC_ILU0, b2s.BICGSTAB, 1e-8, 2000, pco=sweeps8),
-         None)
-    emit(c, "gmres30+ilu0", gpu(A, n, b2s.PC_ILU0, b2s.GMRES, 1e-8, 2000, so={"restart": 30}),
+    emit(c, "bicgstab+ilu0_fp32_j8 (inexact apply)", gpu(A, n, b2s.PC_ILU0, b2s.BICGSTAB, 1e-8, 2000, pco=sweeps8,
+                                                         x64=x64), None)
+    emit(c, "gmres30+ilu0", gpu(A, n, b2s.PC_ILU0, b2s.GMRES, 1e-8, 2000, so={"restart": 30}, x64=x64),
          cpu(rp, ci, v, n, 2, "ilu", 1e-8, 2000))
     emit(c, "fgmres30+ilu0_fp32+ir", gpu(A, n, b2s.PC_ILU0, b2s.FGMRES, 1e-8, 2000, pco={"precision": b2s.FP32},
-                                        so={"restart": 30, "ir_steps": 5, "ir_inner_tol": 1e-4}), None)
+                                        so={"restart": 30, "ir_steps": 5, "ir_inner_tol": 1e-4}, x64=x64), None)
+    emit(c, "gmres30+ilu0_fp32 (FP32 factors and solves inside FP64 GMRES)",
+         gpu(A, n, b2s.PC_ILU0, b2s.GMRES, 1e-8, 2000, pco={"precision": b2s.FP32}, so={"restart": 30}, x64=x64),
+         None)
     del A
 
     c = "C4 elasticity Q1 64^3 elements (3x3 BAIJ), rtol 1e-8"
     nbr, rp, ci, v = b2s.gen_elasticity_q1(64)
     B = b2s.BAIJ(ctx, 3, nbr, nbr, rp, ci, v)
+    x64 = fp64_solution(B, 3 * nbr, b2s.PC_BSA_AMG, b2s.PCG)
     for name, kind, prec in (("bilu0_fp64", b2s.PC_BILU0, b2s.FP64), ("bilu0_fp32", b2s.PC_BILU0, b2s.FP32),
                              ("bsa_amg_fp64", b2s.PC_BSA_AMG, b2s.FP64), ("bsa_amg_fp32", b2s.PC_BSA_AMG, b2s.FP32)):
-        emit(c, f"cg+{name}", gpu(B, 3 * nbr, kind, b2s.PCG, 1e-8, 5000, reps=1, pco={"precision": prec}),
+        emit(c, f"cg+{name}", gpu(B, 3 * nbr, kind, b2s.PCG, 1e-8, 5000, reps=1, pco={"precision": prec}, x64=x64),
              "not run: the reference's block matrix has GMRES only")
     # the reference's block solver: GMRES(30) with block ILU(0)
     r = None
@@ -358,7 +381,8 @@ def run_suite(args):
         t0 = time.perf_counter()
         _, it = ref.blk_gmres(Br, b2s.uniform(7, 3 * nbr), "blockilu", 1e-8, 1000, 30)
         r = {"ms": round((time.perf_counter() - t0) * 1e3, 1), "it": it, "cores": os.cpu_count()}
-    emit(c, "gmres30+bilu0_fp64", gpu(B, 3 * nbr, b2s.PC_BILU0, b2s.GMRES, 1e-8, 1000, reps=1, so={"restart": 30}), r)
+    emit(c, "gmres30+bilu0_fp64", gpu(B, 3 * nbr, b2s.PC_BILU0, b2s.GMRES, 1e-8, 1000, reps=1, so={"restart": 30},
+                                      x64=x64), r)
     del B
     ctx.close()
     return 0
@@ -476,8 +500,22 @@ def main():
         kind, prec, trsv, sweeps, fsweeps = kinds[method]
         return b2s.Precond(ctx, A, kind, precision=prec, trsv=trsv, trsv_sweeps=sweeps, factor_sweeps=fsweeps)
 
+    x64_cache = {}
+
+    def fp64_solution(k):
+        """The FP64 solution of system k to rtol 1e-12 (FP64 SA-AMG PCG), the
+        yardstick of every method's error."""
+        if k not in x64_cache:
+            n, rp, ci, v, b = systems[k]
+            A = b2s.CSR(ctx, n, n, rp, ci, v)
+            M = b2s.Precond(ctx, A, b2s.PC_SA_AMG)
+            x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-12, maxit=MAXIT)
+            assert st["relres_true"] < 1e-11, st
+            x64_cache[k] = x
+        return x64_cache[k]
+
     def timed_solve(n, rp, ci, v, b, method):
-        """Device-resident inputs; returns (ms, stats, relres_true)."""
+        """Device-resident inputs; returns (ms, stats, launches, x on the host)."""
         A = b2s.CSR(ctx, n, n, rp, ci, v)
         bt = torch.from_numpy(b).to(dev)
         xt = torch.zeros(n, dtype=torch.float64, device=dev)
@@ -495,7 +533,7 @@ def main():
         launches = ctx.kernel_launches - l0
         st["setup_ms_event"] = e0.elapsed_time(em)
         st["iter_ms_event"] = em.elapsed_time(e1)
-        return e0.elapsed_time(e1), st, launches
+        return e0.elapsed_time(e1), st, launches, xt.cpu().numpy()
 
     timed_idx = list(range(args.warmup, args.warmup + args.steps))
 
@@ -503,18 +541,26 @@ def main():
         """Warm-up solves on warm_idx, then one timed solve per timed system."""
         for k in warm_idx:
             timed_solve(*systems[k], method)
-        ms, its, rel, launches, split, fb = [], [], [], 0, [], 0
+        ms, its, rel, launches, split, fb, errs = [], [], [], 0, [], 0, []
         for k in timed_idx:
-            t, st, nl = timed_solve(*systems[k], method)
+            t, st, nl, x = timed_solve(*systems[k], method)
             ms.append(t)
             its.append(st["iterations"])
             rel.append(st["relres_true"])
             split.append((st["setup_ms_event"], st["iter_ms_event"]))
             launches += nl
             fb += st["fallbacks"]
+            errs.append((k, x))
         run.split = split
         run.fallbacks = fb
+        run.errors = errs
         return ms, its, rel, launches
+
+    def error_summary(errs):
+        """||x - x_FP64|| / ||x_FP64|| over the timed systems (computed after timing)."""
+        e = [float(np.linalg.norm(x - fp64_solution(k)) / np.linalg.norm(fp64_solution(k))) for k, x in errs]
+        return {"max": max(e), "mean": float(np.mean(e)),
+                "against": "FP64 SA-AMG PCG to rtol 1e-12 on the same system"}
 
     if world > 1:
         torch.distributed.barrier()
@@ -523,11 +569,13 @@ def main():
         head_ms, head_its, head_rel, launches = run(args.method, range(args.warmup))
     head_split = run.split
     head_fallbacks = run.fallbacks
+    head_err = error_summary(run.errors)
     torch.cuda.synchronize()
     clocks = clk.summary()
     base_ms, base_its, base_rel, _ = run("fp64_ic0", range(min(1, args.warmup))) if args.method != "fp64_ic0" else (
         head_ms, head_its, head_rel, 0)
     base_split = run.split
+    base_err = error_summary(run.errors) if args.method != "fp64_ic0" else head_err
     # the other methods on the same systems (context for the headline: what
     # the learned values and the sweep solves each contribute)
     variants = {}
@@ -538,6 +586,7 @@ def main():
         variants[m] = {"ms": float(np.mean(v_ms)), "iterations_mean": float(np.mean(v_its)),
                        "relres_true_max": float(np.max(v_rel)), "fallbacks": int(run.fallbacks),
                        "setup_ms_mean": float(np.mean([a for a, _ in run.split])),
+                       "error_vs_fp64": error_summary(run.errors),
                        "speedup_vs_fp64_ic0": float(np.mean(base_ms)) / float(np.mean(v_ms))}
 
     # e2e: host CSR + host b -> device, preconditioner, solve, x -> host (public C ABI, host pointers).
@@ -718,10 +767,12 @@ def main():
             "config": arm_config(args, world),
             "iterations_mean": float(np.mean(head_its)), "relres_true_max": float(np.max(head_rel)),
             "fallbacks": int(head_fallbacks),
+            "error_vs_fp64": head_err,
             "setup_ms_mean": float(np.mean([a for a, _ in head_split])),
             "iter_ms_mean": float(np.mean([b for _, b in head_split])),
             "fp64_ic0_pcg": {"ms": float(np.mean(base_ms)), "iterations_mean": float(np.mean(base_its)),
                              "relres_true_max": float(np.max(base_rel)),
+                             "error_vs_fp64": base_err,
                              "setup_ms_mean": float(np.mean([a for a, _ in base_split])),
                              "iter_ms_mean": float(np.mean([b for _, b in base_split]))},
             "speedup_vs_fp64_ic0": float(np.mean(base_ms)) / value,

@@ -116,6 +116,7 @@ EXPORTS = [
     "b2s_learner_destroy", "b2s_learner_load", "b2s_learner_save", "b2s_learner_params", "b2s_learner_step",
     "b2s_pc_create_learned", "b2s_dot_noalloc", "b2s_dense_bf16_device",
     "b2s_learner_set_loss", "b2s_sor", "b2s_sor_device", "b2s_csr_matmul", "b2s_csr_transpose", "b2s_csr_export",
+    "b2s_ctx_set_wait_limits",
 ]
 
 
@@ -195,6 +196,7 @@ def lib():
     f("b2s_csr_matmul", i32, vp, vp, vp, pp)
     f("b2s_csr_transpose", i32, vp, vp, pp)
     f("b2s_csr_export", i32, vp, vp, vp, vp, vp)
+    f("b2s_ctx_set_wait_limits", i32, vp, u32, u32)
     _lib = L
     return L
 
@@ -240,6 +242,10 @@ class Context:
 
     def synchronize(self):
         self.check(lib().b2s_ctx_synchronize(self.h), "synchronize")
+
+    def set_wait_limits(self, spin_polls: int = 0, sleep_polls: int = 0):
+        """Bounds of the chunked triangular solves' device waits ((0, 0): defaults)."""
+        self.check(lib().b2s_ctx_set_wait_limits(self.h, int(spin_polls), int(sleep_polls)), "set_wait_limits")
 
     def close(self):
         if getattr(self, "h", None):

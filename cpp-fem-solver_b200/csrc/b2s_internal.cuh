@@ -180,7 +180,16 @@ struct b2s_ctx
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // device error word (B2S_TIMEOUT from a bounded wait); counter[32..]
     int* errword() { return reinterpret_cast<int*>(counter.p + 32); }
+    // bounds of the chunked triangular solves' waits (b2s_ctx_set_wait_limits)
+    unsigned wait_fast_polls = 1u << 20;
+    unsigned wait_slow_polls = 1u << 20;
 };
+
+namespace b2s {
+// Reads the context's device error word (synchronises); a set word is
+// cleared and raised as its status (B2S_TIMEOUT: a bounded wait gave up).
+void check_device_error(b2s_ctx* ctx, const char* where);
+}
 
 namespace b2s {
 

@@ -112,6 +112,23 @@ void free(const Block& b)
 }  // namespace mem
 }  // namespace b2s
 
+namespace b2s {
+
+void check_device_error(b2s_ctx* ctx, const char* where)
+{
+    int h = 0;
+    B2S_CUDA(cudaMemcpyAsync(&h, ctx->errword(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    sync(ctx);
+    if (h)
+    {
+        B2S_CUDA(cudaMemsetAsync(ctx->errword(), 0, sizeof(int), ctx->stream));
+        sync(ctx);
+        fail((b2s_status)h, where);
+    }
+}
+
+}  // namespace b2s
+
 extern "C" {
 
 b2s_status b2s_ctx_create(int device, b2s_ctx** out)
@@ -207,19 +224,17 @@ void* b2s_ctx_stream(b2s_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; 
 b2s_status b2s_ctx_synchronize(b2s_ctx* ctx)
 {
     if (!ctx) return B2S_INVALID_ARG;
-    return guarded(ctx, [&] {
-        // asynchronous entry points (b2s_dense_bf16_device) report a bounded
-        // device wait that gave up through the context's error word
-        int h = 0;
-        B2S_CUDA(cudaMemcpyAsync(&h, ctx->errword(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        sync(ctx);
-        if (h)
-        {
-            B2S_CUDA(cudaMemsetAsync(ctx->errword(), 0, sizeof(int), ctx->stream));
-            sync(ctx);
-            fail((b2s_status)h, "a device-side wait gave up");
-        }
-    });
+    // asynchronous entry points (b2s_dense_bf16_device, b2s_pc_apply_device)
+    // report a bounded device wait that gave up through the error word
+    return guarded(ctx, [&] { check_device_error(ctx, "a device-side wait gave up"); });
+}
+
+b2s_status b2s_ctx_set_wait_limits(b2s_ctx* ctx, uint32_t spin_polls, uint32_t sleep_polls)
+{
+    if (!ctx) return B2S_INVALID_ARG;
+    ctx->wait_fast_polls = spin_polls ? spin_polls : (1u << 20);
+    ctx->wait_slow_polls = (spin_polls || sleep_polls) ? sleep_polls : (1u << 20);
+    return B2S_OK;
 }
 
 uint64_t b2s_ctx_kernel_launches(const b2s_ctx* ctx) { return ctx ? ctx->launches : 0; }

@@ -1421,6 +1421,8 @@ static b2s_status solve_common(b2s_ctx* ctx, const Operator& A, b2s_pc* pc, b2s_
         run_method(S, method, d_b, d_x, stats);
     }
     if (stats && pc) stats->setup_ms = 0.0;
+    // a bounded wait of a triangular solve that gave up fails the solve
+    check_device_error(ctx, "a triangular-solve wait gave up during the solve");
     const int st = stats ? stats->status : B2S_OK;
     if (!stats)
     {

@@ -1304,6 +1304,7 @@ b2s_status b2s_learner_step(b2s_ctx* ctx, b2s_learner* L, const b2s_csr* A, int 
     return guarded(ctx, [&] {
         need(A->d.n == A->d.m, B2S_SHAPE, "learned IC(0) needs a square matrix");
         train_step(ctx, L->net, A->d, nprobes, seed, probes, lr, update != 0, loss, grad, L->loss);
+        check_device_error(ctx, "a triangular-solve wait gave up during the training step");
     });
 }
 
@@ -1347,6 +1348,7 @@ b2s_status b2s_pc_create_learned(b2s_ctx* ctx, const b2s_csr* A, b2s_learner* L,
         need(A->d.n == A->d.m, B2S_SHAPE, "learned IC(0) needs a square matrix");
         pc->impl = make_pc_learned_with(ctx, A->d, o, L->net);
         sync(ctx);
+        check_device_error(ctx, "a device-side wait gave up during the set-up");
     });
     if (st != B2S_OK)
     {

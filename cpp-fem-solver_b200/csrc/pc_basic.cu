@@ -145,6 +145,7 @@ b2s_status b2s_pc_create(b2s_ctx* ctx, const b2s_csr* A, b2s_pc_kind kind, const
             default: fail(B2S_INVALID_ARG, "preconditioner kind not valid for a CSR matrix");
         }
         sync(ctx);
+        check_device_error(ctx, "a device-side wait gave up during the set-up");
         pc->setup_ms = now_ms() - t0;
     });
     if (st != B2S_OK)
@@ -184,6 +185,7 @@ b2s_status b2s_pc_create_baij(b2s_ctx* ctx, const b2s_baij* A, b2s_pc_kind kind,
             default: fail(B2S_INVALID_ARG, "preconditioner kind not valid for a BAIJ matrix");
         }
         sync(ctx);
+        check_device_error(ctx, "a device-side wait gave up during the set-up");
         pc->setup_ms = now_ms() - t0;
     });
     if (st != B2S_OK)
@@ -230,6 +232,7 @@ b2s_status b2s_pc_apply(b2s_ctx* ctx, b2s_pc* pc, const double* r, double* z)
         pc->impl->apply(ctx, dr.p, dz.p, nullptr);
         d2h(ctx, z, dz.p, dz.bytes());
         sync(ctx);
+        check_device_error(ctx, "a triangular-solve wait gave up during the apply");
     });
 }
 

@@ -37,7 +37,9 @@
 
 namespace b2s {
 
-// wait bounds: polls without sleeping, then polls with a 1 us sleep
+// default wait bounds (b2s_ctx_set_wait_limits changes them per context):
+// polls of one slot without sleeping, and polls with a 1 us sleep that one
+// lane may spend over a whole launch
 constexpr unsigned kChunkFastPolls = 1u << 20;
 constexpr unsigned kChunkSlowPolls = 1u << 20;
 
@@ -48,8 +50,17 @@ struct ChunkArgs
     const uint4* vals;
     const uint32_t* slot_row;
     unsigned long long* xch;  // exchange words, 2 per value component
-    SyncFreeCtl ctl;          // ticket, epoch, error word
+    SyncFreeCtl ctl;          // ticket, epoch, error word (the context's)
+    unsigned fast_polls;      // polls of one slot without sleeping
+    unsigned slow_polls;      // sleeping polls per lane and launch
 };
+
+__device__ __forceinline__ int ld_err(const int* p)
+{
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -127,16 +138,21 @@ __device__ __forceinline__ bool xch_get(const unsigned long long* w, uint32_t ep
 // The producer warp: lane l serves slots l, l+32, ... in order.  The loop is
 // warp-uniform: every pass, each lane with a pending slot polls it once (all
 // lanes' polls in flight together) and hands it over as soon as its words
-// carry this traversal's epoch, so no lane waits for another lane's slot.  A
-// lane that polls one slot more than the bound records B2S_TIMEOUT and hands
-// over what it read.
+// carry this traversal's epoch, so no lane waits for another lane's slot.
+// A slot is polled fast_polls times without sleeping, then with 1 us sleeps
+// drawn from the lane's budget of slow_polls for the whole launch.  A lane
+// gives up when that budget is spent or when another wait of the launch has
+// already given up (the error word is set): it records B2S_TIMEOUT, hands
+// over what it read, and from then on hands over its remaining slots without
+// waiting, so a launch that fails ends within one budget.
 template <int BS, typename XT>
 __device__ __forceinline__ void produce_slots(const ChunkArgs& a, const ChunkDesc& D, uint32_t epoch, uint32_t lane,
                                               XT* xv, uint32_t* xr)
 {
     uint32_t s = lane;
     uint32_t j = s < D.ns ? __ldg(&a.slot_row[D.slot + s]) : 0u;
-    unsigned polls = 0;
+    unsigned polls = 0, slept = 0;
+    bool gave_up = false;
     while (__any_sync(0xffffffffu, s < D.ns))
     {
         if (s < D.ns)
@@ -145,10 +161,20 @@ __device__ __forceinline__ void produce_slots(const ChunkArgs& a, const ChunkDes
             bool ok = true;
 #pragma unroll
             for (int c = 0; c < BS; ++c) ok &= xch_get<XT>(a.xch + ((size_t)j * BS + c) * 2, epoch, val[c]);
-            if (!ok && ++polls >= kChunkFastPolls + kChunkSlowPolls)
+            if (!ok && (gave_up || ++polls >= a.fast_polls))
             {
-                atomicExch(a.ctl.err, (int)B2S_TIMEOUT);
-                ok = true;
+                if (!gave_up && (slept >= a.slow_polls || ld_err(a.ctl.err) != 0))
+                {
+                    atomicCAS(a.ctl.err, 0, (int)B2S_TIMEOUT);
+                    gave_up = true;
+                }
+                if (gave_up)
+                    ok = true;
+                else
+                {
+                    ++slept;
+                    __nanosleep(1000);
+                }
             }
             if (ok)
             {
@@ -159,24 +185,27 @@ __device__ __forceinline__ void produce_slots(const ChunkArgs& a, const ChunkDes
                 if (s < D.ns) j = __ldg(&a.slot_row[D.slot + s]);
                 polls = 0;
             }
-            else if (polls >= kChunkFastPolls)
-                __nanosleep(1000);
         }
     }
 }
 
-// compute warp: wait until the producer has filled slot s (bounded)
-__device__ __forceinline__ void slot_wait(const uint32_t* xr, uint32_t s, int* err)
+// compute warp: wait until the producer has filled slot s.  8 x fast_polls
+// polls without sleeping, then 1 us sleeps from the thread's budget of
+// slow_polls for the whole launch; gives up (B2S_TIMEOUT) when the budget is
+// spent or another wait of the launch has given up.
+__device__ __forceinline__ void slot_wait(const uint32_t* xr, uint32_t s, const ChunkArgs& a, unsigned& slept)
 {
     for (unsigned polls = 0; ld_acquire_cta_shared(&xr[s]) == 0u; ++polls)
     {
-        if (polls >= 8 * kChunkFastPolls)
+        if (polls >= 8 * a.fast_polls)
         {
-            if (polls >= 8 * kChunkFastPolls + kChunkSlowPolls)
+            if (slept >= a.slow_polls || ld_err(a.ctl.err) != 0)
             {
-                atomicExch(err, (int)B2S_TIMEOUT);
+                atomicCAS(a.ctl.err, 0, (int)B2S_TIMEOUT);
+                slept = a.slow_polls;
                 return;
             }
+            ++slept;
             __nanosleep(1000);
         }
     }
@@ -257,6 +286,7 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
         VT vv[4] = {VT(0), VT(0), VT(0), VT(0)};
         XT rhs = XT(0), dv = XT(1);
     };
+    unsigned slept = 0;  // this thread's sleeping polls in slot waits (bounded per launch)
     auto fetch = [&](uint32_t t, uint32_t tend, Ops& o) {
         if (t >= tend) return;
         const uint2 rw = rec[t];
@@ -279,7 +309,7 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
         {
 #pragma unroll
             for (int q = 0; q < 4; ++q)
-                if (o.e0 + q < o.e1 && (o.m[q] & 0x8000u)) slot_wait(xr, o.m[q] & 0x7fffu, a.ctl.err);
+                if (o.e0 + q < o.e1 && (o.m[q] & 0x8000u)) slot_wait(xr, o.m[q] & 0x7fffu, a, slept);
             XT xj[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) xj[q] = (o.m[q] & 0x8000u) ? xv[o.m[q] & 0x7fffu] : sx[o.m[q]];
@@ -296,7 +326,7 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
                 if (m & 0x8000u)
                 {
                     const uint32_t s = m & 0x7fffu;
-                    slot_wait(xr, s, a.ctl.err);
+                    slot_wait(xr, s, a, slept);
                     xj = xv[s];
                 }
                 else
@@ -444,6 +474,7 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_btrsv_chunk(ChunkArgs a, 
     const uint32_t grp = lane / BS, r = lane % BS;
     const uint32_t gbase = grp * BS;
     const bool lane_ok = grp < GPW;
+    unsigned slept = 0;  // this thread's sleeping polls in slot waits (bounded per launch)
     uint32_t t0 = 0, t1 = slv[1];
     for (uint32_t l = 0; l < D.nl; ++l)
     {
@@ -469,7 +500,7 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_btrsv_chunk(ChunkArgs a, 
                     if (m & 0x8000u)
                     {
                         const uint32_t s = m & 0x7fffu;
-                        slot_wait(xr, s, a.ctl.err);
+                        slot_wait(xr, s, a, slept);
                         xj = xv + s * BS;
                     }
                     else
@@ -633,7 +664,9 @@ struct ChunkSchedule
             B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             *have = smem;
         }
-        const ChunkArgs a{desc.p, meta.p, vals.p, slot_row.p, xch.p, sf.ctl()};
+        SyncFreeCtl c = sf.ctl();
+        c.err = ctx->errword();  // read back by check_device_error at the next synchronisation
+        const ChunkArgs a{desc.p, meta.p, vals.p, slot_row.p, xch.p, c, ctx->wait_fast_polls, ctx->wait_slow_polls};
         B2S_LAUNCH(ctx, kern, nchunks, threads, smem, a, rhs, x, out64, done);
     }
 

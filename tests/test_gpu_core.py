@@ -204,16 +204,22 @@ def test_graphs_match_eager(b2s, ctx):
 
 @pytest.mark.parametrize("flexible", [False, True])
 def test_gmres_cgs2(b2s, ctx, orc, flexible):
-    """Classical Gram-Schmidt twice: same Krylov space as MGS, different rounding."""
+    """Classical Gram-Schmidt twice is a different algorithm from the
+    reference's MGS (the same Krylov space, other rounding), so it is held to
+    accuracy, not to the reference's iterates: the same iteration count within
+    +/-2, and an error against the FP64 solution (rtol 1e-13) no larger than
+    twice the reference MGS solve's own error at the same tolerance."""
     n, rp, ci, v = P.convdiff2d(60)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
     b = b2s.uniform(13, n)
     M = b2s.Precond(ctx, A, b2s.PC_ILU0)
     method = b2s.FGMRES if flexible else b2s.GMRES
     x, st = b2s.solve(ctx, A, b, method, M, tol=1e-8, maxit=2000, restart=30, orth=b2s.ORTH_CGS2)
-    xo, io = orc.solve(orc.csr(n, n, rp, ci, v), 2, "ilu", b, 1e-8, 2000, 30)
+    Ao = orc.csr(n, n, rp, ci, v)
+    xo, io = orc.solve(Ao, 2, "ilu", b, 1e-8, 2000, 30)
+    xt, _ = orc.solve(Ao, 2, "ilu", b, 1e-13, 2000, 30)
     assert abs(st["it"] - io) <= 2
-    assert rel(x, xo) < 1e-7
+    assert rel(x, xt) <= 2 * rel(xo, xt) + 1e-13, (rel(x, xt), rel(xo, xt))
     assert st["relres_true"] < 2e-8
 
 
