@@ -44,6 +44,23 @@ L2_FLUSH_BYTES = 512 << 20
 METRIC = "time-to-rtol 1e-8 & iters: learned/mixed-prec PCG vs plain FP64 PCG, 1 B200"
 
 
+def replica_seeds(rank: int, count: int) -> list:
+    """Seeds of the systems one replica solves: held-out seeds 2000+ on rank
+    0, a disjoint range per further rank."""
+    return [2000 + rank * 100000 + k for k in range(count)]
+
+
+def max_over_ranks(value: float, device) -> float:
+    """The largest value over all ranks (the whole job's time per step)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def load_b2s():
     import __graft_entry__ as ge
     return ge._load()
@@ -483,7 +500,7 @@ def main():
     dev = torch.device("cuda", local)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
-    seeds = [2000 + rank * 100000 + k for k in range(args.warmup + args.steps)]
+    seeds = replica_seeds(rank, args.warmup + args.steps)
     systems = [make_system(b2s, s) for s in seeds]
 
     # method -> (preconditioner, precision, triangular-solve schedule, sweeps, factorisation sweeps)
@@ -722,11 +739,7 @@ def main():
             "ms": spmv_ms, "achieved": spmv_gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": spmv_gbs / pk["hbm_gbs"], "bytes_per_launch": spmv_bytes}
 
-    value = float(np.mean(head_ms))
-    if world > 1:
-        t = torch.tensor([value], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        value = float(t.item())
+    value = max_over_ranks(float(np.mean(head_ms)), dev)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -116,7 +116,8 @@ EXPORTS = [
     "b2s_learner_destroy", "b2s_learner_load", "b2s_learner_save", "b2s_learner_params", "b2s_learner_step",
     "b2s_pc_create_learned", "b2s_dot_noalloc", "b2s_dense_bf16_device",
     "b2s_learner_set_loss", "b2s_sor", "b2s_sor_device", "b2s_csr_matmul", "b2s_csr_transpose", "b2s_csr_export",
-    "b2s_ctx_set_wait_limits",
+    "b2s_ctx_set_wait_limits", "b2s_baij_set_halo", "b2s_baij_halo_info", "b2s_baij_halo_pack_device",
+    "b2s_baij_dist_matvec_owned_device", "b2s_baij_dist_matvec_ghost_device",
 ]
 
 
@@ -197,6 +198,12 @@ def lib():
     f("b2s_csr_transpose", i32, vp, vp, pp)
     f("b2s_csr_export", i32, vp, vp, vp, vp, vp)
     f("b2s_ctx_set_wait_limits", i32, vp, u32, u32)
+    i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+    f("b2s_baij_set_halo", i32, vp, vp, i32, i32p, i32p, _u32p, i32, i32p, i32p, _u32p, u32)
+    f("b2s_baij_halo_info", i32, vp, u32ptr, u32ptr, u32ptr)
+    f("b2s_baij_halo_pack_device", i32, vp, vp, vp, vp)
+    f("b2s_baij_dist_matvec_owned_device", i32, vp, vp, vp, vp)
+    f("b2s_baij_dist_matvec_ghost_device", i32, vp, vp, vp, vp)
     _lib = L
     return L
 
@@ -339,6 +346,31 @@ class BAIJ:
         y = np.zeros(self.nbr * self.bs)
         self.ctx.check(lib().b2s_baij_matvec(self.ctx.h, self.h, _f64(x), y), "baij_matvec")
         return y
+
+    def set_halo(self, recv_procs, recv_cnts, recv_global, send_procs, send_cnts, send_local, owned_global_start):
+        """BlockMatrix::set_halo: this handle holds one rank's block rows (global columns)."""
+        i32 = lambda a: np.ascontiguousarray(a, np.int32)
+        rp_, rc_, sp_, sc_ = i32(recv_procs), i32(recv_cnts), i32(send_procs), i32(send_cnts)
+        self.ctx.check(lib().b2s_baij_set_halo(self.ctx.h, self.h, len(rp_), rp_, rc_, _u32(recv_global), len(sp_),
+                                               sp_, sc_, _u32(send_local), int(owned_global_start)), "set_halo")
+
+    def halo_info(self):
+        """(n_owned, n_ghost, n_send) block rows of the halo set by set_halo."""
+        a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        self.ctx.check(lib().b2s_baij_halo_info(self.h, C.byref(a), C.byref(b), C.byref(c)), "halo_info")
+        return a.value, b.value, c.value
+
+    def halo_pack_device(self, x_ptr: int, buf_ptr: int):
+        self.ctx.check(lib().b2s_baij_halo_pack_device(self.ctx.h, self.h, C.c_void_p(x_ptr), C.c_void_p(buf_ptr)),
+                       "halo_pack")
+
+    def dist_matvec_owned_device(self, xfull_ptr: int, y_ptr: int):
+        self.ctx.check(lib().b2s_baij_dist_matvec_owned_device(self.ctx.h, self.h, C.c_void_p(xfull_ptr),
+                                                                C.c_void_p(y_ptr)), "dist_matvec_owned")
+
+    def dist_matvec_ghost_device(self, xfull_ptr: int, y_ptr: int):
+        self.ctx.check(lib().b2s_baij_dist_matvec_ghost_device(self.ctx.h, self.h, C.c_void_p(xfull_ptr),
+                                                                C.c_void_p(y_ptr)), "dist_matvec_ghost")
 
     def __del__(self):
         try:
@@ -532,6 +564,13 @@ def solve_device(ctx: Context, A, b_ptr: int, x_ptr: int, method=PCG, pc=None, *
     ctx.check(fn(ctx.h, A.h, pc.h if pc is not None else None, method, C.byref(o), C.c_void_p(b_ptr),
                  C.c_void_p(x_ptr), C.byref(st)), "solve")
     return st.as_dict()
+
+
+def dot_device(ctx: Context, n: int, a_ptr: int, b_ptr: int) -> float:
+    """SMatrix::dot of two device vectors (fixed-order reduction, on ctx's stream)."""
+    out = C.c_double()
+    ctx.check(lib().b2s_dot_device(ctx.h, int(n), C.c_void_p(a_ptr), C.c_void_p(b_ptr), C.byref(out)), "dot")
+    return out.value
 
 
 def dot(ctx: Context, a, b) -> float:

@@ -286,10 +286,24 @@ struct b2s_csr
     b2s::CsrDev d;
 };
 
+namespace b2s {
+// set_halo state of a BAIJ that holds one rank's block rows with global block
+// columns (BlockMatrix::set_halo, blockMatrix.hpp:317-348)
+struct HaloDev
+{
+    bool set = false;
+    uint32_t n_owned = 0, n_ghost = 0, n_send = 0, start = 0;
+    DBuf<uint32_t> lci;         // local column of every block: owned g - start, ghost n_owned + k
+    DBuf<uint32_t> send_local;  // owned block rows that other ranks read, grouped by destination
+    std::vector<int> recv_procs, recv_cnts, send_procs, send_cnts;
+};
+}  // namespace b2s
+
 struct b2s_baij
 {
     b2s_ctx* ctx = nullptr;
     b2s::BaijDev d;
+    b2s::HaloDev halo;
 };
 
 struct b2s_pc

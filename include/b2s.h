@@ -145,6 +145,31 @@ b2s_status b2s_dot_noalloc(const double* d_a, const double* d_b, uint64_t n, dou
 b2s_status b2s_baij_matvec(b2s_ctx* ctx, const b2s_baij* A, const double* x, double* y);
 b2s_status b2s_baij_matvec_device(b2s_ctx* ctx, const b2s_baij* A, const double* d_x, double* d_y);
 
+/* ------------------------------------------------- row-partitioned BAIJ
+ * One rank's block rows of a matrix partitioned by contiguous block rows
+ * (the BAIJ handle holds nbr local rows and nbc = the GLOBAL block column
+ * count, columns in global numbering).  BlockMatrix::set_halo
+ * (blockMatrix.hpp:317-348), same arguments: the ghost columns this rank
+ * receives, grouped by source rank (recv_global, sum(recv_cnts) entries),
+ * the owned rows it sends, grouped by destination (send_local, local
+ * numbering), and the global number of its first row.  A block column that
+ * is neither owned nor listed is rejected (B2S_INVALID_ARG). */
+b2s_status b2s_baij_set_halo(b2s_ctx* ctx, b2s_baij* A, int nrecv, const int* recv_procs, const int* recv_cnts,
+                             const uint32_t* recv_global, int nsend, const int* send_procs, const int* send_cnts,
+                             const uint32_t* send_local, uint32_t owned_global_start);
+b2s_status b2s_baij_halo_info(const b2s_baij* A, uint32_t* n_owned, uint32_t* n_ghost, uint32_t* n_send);
+/* The device steps of BlockMatrix::distributed_matvec (blockMatrix.hpp:
+ * 351-437) around the caller's exchange (NCCL, MPI, ...), on the context's
+ * stream.  x_full = [x_owned (n_owned*bs) | ghosts (n_ghost*bs, recv order)].
+ *   pack:  send_buf = x_owned rows listed in send_local (n_send*bs values)
+ *   owned: y  = the owned columns' blocks times x_full (reads no ghost)
+ *   ghost: y += the ghost columns' blocks times x_full
+ * Sums as the reference's MPI branch: y from zero, owned blocks in row order,
+ * then the ghost blocks, each block component summed in column order. */
+b2s_status b2s_baij_halo_pack_device(b2s_ctx* ctx, const b2s_baij* A, const double* d_x_owned, double* d_send_buf);
+b2s_status b2s_baij_dist_matvec_owned_device(b2s_ctx* ctx, const b2s_baij* A, const double* d_x_full, double* d_y);
+b2s_status b2s_baij_dist_matvec_ghost_device(b2s_ctx* ctx, const b2s_baij* A, const double* d_x_full, double* d_y);
+
 /* --------------------------------------------------------- preconditioners */
 
 typedef enum b2s_pc_kind

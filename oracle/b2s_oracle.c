@@ -474,6 +474,36 @@ void orc_blk_matvec(const orc_blk* A, const double* x, double* y)
     }
 }
 
+/* BlockMatrix::distributed_matvec with MPI, blockMatrix.hpp:351-437, after
+ * the halo exchange: one rank's block rows with local columns (lci: an owned
+ * column j < n_owned, a ghost column n_owned + k), x_full = [owned | ghosts].
+ * y starts at zero; pass 1 adds the owned columns' blocks in row order, pass
+ * 2 the ghost columns'; each block contributes acc = sum_c B[r][c] x_j[c]
+ * summed in c order (this loop carries no omp simd, unlike matvec). */
+void orc_blk_dist_matvec(int bs, uint32_t nbr, const uint32_t* rp, const uint32_t* lci, const double* v,
+                         uint32_t n_owned, const double* x_full, double* y)
+{
+    const int bv = bs * bs;
+    for (size_t i = 0; i < (size_t)nbr * bs; ++i) y[i] = 0.0;
+    for (int pass = 0; pass < 2; ++pass)
+        for (uint32_t bi = 0; bi < nbr; ++bi)
+        {
+            double* yi = &y[(size_t)bi * bs];
+            for (uint32_t p = rp[bi]; p < rp[bi + 1]; ++p)
+            {
+                if ((lci[p] >= n_owned) != (pass == 1)) continue;
+                const double* B = &v[(size_t)p * bv];
+                const double* xj = &x_full[(size_t)lci[p] * bs];
+                for (int r = 0; r < bs; ++r)
+                {
+                    double acc = 0.0;
+                    for (int c = 0; c < bs; ++c) acc += B[r * bs + c] * xj[c];
+                    yi[r] += acc;
+                }
+            }
+        }
+}
+
 /* BlockMatrix::transpose, blockMatrix.hpp:237-267 */
 orc_blk* orc_blk_transpose(const orc_blk* A)
 {

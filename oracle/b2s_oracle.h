@@ -97,6 +97,12 @@ int orc_solve(const orc_csr* A, int method, const char* precond, int restart, do
 int orc_solve_pc(const orc_csr* A, int method, orc_pc* pc, int restart, double tol, int maxit,
                  const double* b, double* x, int* it, char* err, int errlen);
 
+/* ---- distributed BlockMatrix (blockMatrix.hpp:317-437) ----
+ * distributed_matvec after the halo exchange on one rank's rows: local
+ * columns (owned < n_owned, ghosts after), owned pass then ghost pass. */
+void orc_blk_dist_matvec(int bs, uint32_t nbr, const uint32_t* rp, const uint32_t* lci, const double* v,
+                         uint32_t n_owned, const double* x_full, double* y);
+
 /* ---- BlockMatrix (blockMatrix.hpp:139-315) ---- */
 orc_blk* orc_blk_create(int bs, uint32_t nbr, uint32_t nbc, const uint32_t* rp, const uint32_t* ci,
                         const double* v);

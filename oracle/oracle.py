@@ -212,9 +212,17 @@ class Orc(_Lib):
         self._blk_amg_export = self._f("blk_amg_export", i32, vp, i32, u32p, vp, vp, vp, vp, vp, vp, vp)
         self._blk_amg_aggregates = self._f("blk_amg_aggregates", i32, vp, i32, i32p)
         self._blk_solve_pc = self._f("blk_solve_pc", i32, vp, i32, vp, i32, f64, i32, f64p, f64p, ip, cp, i32)
+        self._blk_dist_matvec = self._f("blk_dist_matvec", None, i32, u32, u32p, u32p, f64p, u32, f64p, f64p)
 
     def csr(self, n, m, rp, ci, v):
         return _CSR(self, self._csr_copy(n, m, _u32(rp), _u32(ci), _f64(v)), n, m)
+
+    def blk_dist_matvec(self, bs, rp, lci, v, n_owned, x_full):
+        """BlockMatrix::distributed_matvec after the exchange (owned pass, then ghosts)."""
+        nbr = len(rp) - 1
+        y = np.zeros(nbr * bs, np.float64)
+        self._blk_dist_matvec(bs, nbr, _u32(rp), _u32(lci), _f64(v), n_owned, _f64(x_full), y)
+        return y
 
     def csr_from_coo(self, n, m, v, r, c):
         st = C.c_int(0)

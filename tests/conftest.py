@@ -17,7 +17,8 @@ def load_b2s():
     if "b2s" in sys.modules:
         return sys.modules["b2s"]
     path = os.path.join(ROOT, "cpp-fem-solver_b200", "__init__.py")
-    spec = importlib.util.spec_from_file_location("b2s", path)
+    spec = importlib.util.spec_from_file_location("b2s", path,
+                                                  submodule_search_locations=[os.path.dirname(path)])
     mod = importlib.util.module_from_spec(spec)
     sys.modules["b2s"] = mod
     spec.loader.exec_module(mod)
