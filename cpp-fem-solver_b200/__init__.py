@@ -39,6 +39,7 @@ CUDA_ERROR, NO_DEVICE, OUT_OF_MEMORY, UNSUPPORTED = 10, 11, 12, 13
 
 # preconditioner kinds / methods / options (b2s.h)
 PC_NONE, PC_DIAG, PC_IC0, PC_ILU0, PC_SSOR, PC_SA_AMG, PC_LEARNED_IC0, PC_BJACOBI, PC_BILU0, PC_BSA_AMG = range(10)
+PC_SCHUR, PC_SCALED = 10, 11
 PCG, BICGSTAB, GMRES, FGMRES, BLOCK_GMRES, STATIONARY = range(6)
 FP64, FP32, BF16 = range(3)
 TRSV_AUTO, TRSV_LEVEL, TRSV_SYNCFREE, TRSV_CHUNK, TRSV_JACOBI = range(5)
@@ -117,7 +118,8 @@ EXPORTS = [
     "b2s_pc_create_learned", "b2s_dot_noalloc", "b2s_dense_bf16_device",
     "b2s_learner_set_loss", "b2s_sor", "b2s_sor_device", "b2s_csr_matmul", "b2s_csr_transpose", "b2s_csr_export",
     "b2s_ctx_set_wait_limits", "b2s_baij_set_halo", "b2s_baij_halo_info", "b2s_baij_halo_pack_device",
-    "b2s_baij_dist_matvec_owned_device", "b2s_baij_dist_matvec_ghost_device",
+    "b2s_baij_dist_matvec_owned_device", "b2s_baij_dist_matvec_ghost_device", "b2s_pc_create_schur",
+    "b2s_pc_create_scaled",
 ]
 
 
@@ -204,6 +206,8 @@ def lib():
     f("b2s_baij_halo_pack_device", i32, vp, vp, vp, vp)
     f("b2s_baij_dist_matvec_owned_device", i32, vp, vp, vp, vp)
     f("b2s_baij_dist_matvec_ghost_device", i32, vp, vp, vp, vp)
+    f("b2s_pc_create_schur", i32, vp, u64, u64, vp, vp, vp, vp, pp)
+    f("b2s_pc_create_scaled", i32, vp, vp, f64, pp)
     _lib = L
     return L
 
@@ -427,6 +431,31 @@ class Precond:
                 lib().b2s_pc_destroy(self.h)
         except Exception:
             pass
+
+
+class SchurPrecond(Precond):
+    """make_schur_preconditioner (blockMatrix.hpp:637-685) on the device:
+    A_pc for the velocity block, S_pc (None = identity) for the pressure
+    block, B (n_pres x n_vel) and Bt (n_vel x n_pres) CSR handles."""
+
+    def __init__(self, ctx: Context, n_vel: int, n_pres: int, B: "CSR", Bt: "CSR", A_pc, S_pc=None):
+        self.ctx, self.kind, self.n = ctx, PC_SCHUR, int(n_vel) + int(n_pres)
+        self._keep = (B, Bt, A_pc, S_pc)  # the parts must outlive the composition
+        h = C.c_void_p()
+        ctx.check(lib().b2s_pc_create_schur(ctx.h, int(n_vel), int(n_pres), B.h, Bt.h, A_pc.h,
+                                            S_pc.h if S_pc is not None else None, C.byref(h)), "pc_create_schur")
+        self.h = h
+
+
+class ScaledPrecond(Precond):
+    """z = alpha * M^-1 r for a device preconditioner M."""
+
+    def __init__(self, ctx: Context, inner, alpha: float):
+        self.ctx, self.kind, self.n = ctx, PC_SCALED, inner.n
+        self._keep = inner
+        h = C.c_void_p()
+        ctx.check(lib().b2s_pc_create_scaled(ctx.h, inner.h, float(alpha), C.byref(h)), "pc_create_scaled")
+        self.h = h
 
 
 class HostPrecond:

@@ -184,7 +184,9 @@ typedef enum b2s_pc_kind
     B2S_PC_LEARNED_IC0 = 6, /* IC(0) pattern with values from the message-passing network */
     B2S_PC_BJACOBI = 7,     /* BlockMatrix::gmres "blockjacobi", blockMatrix.hpp:714-733 */
     B2S_PC_BILU0 = 8,       /* make_block_ilu0_preconditioner, blockMatrix.hpp:455-623 */
-    B2S_PC_BSA_AMG = 9      /* make_block_amg_preconditioner on a BAIJ matrix */
+    B2S_PC_BSA_AMG = 9,     /* make_block_amg_preconditioner on a BAIJ matrix */
+    B2S_PC_SCHUR = 10,      /* make_schur_preconditioner (b2s_pc_create_schur) */
+    B2S_PC_SCALED = 11      /* alpha times another preconditioner (b2s_pc_create_scaled) */
 } b2s_pc_kind;
 
 /* Storage / arithmetic precision of a preconditioner. */
@@ -248,6 +250,23 @@ b2s_status b2s_pc_create_baij(b2s_ctx* ctx, const b2s_baij* A, b2s_pc_kind kind,
 typedef int (*b2s_host_pc_fn)(void* user, const double* r, double* z, uint64_t n);
 b2s_status b2s_pc_create_host(b2s_ctx* ctx, uint64_t n, b2s_host_pc_fn fn, void* user, b2s_pc** out);
 b2s_status b2s_pc_destroy(b2s_pc* pc);
+/* Block-triangular saddle-point preconditioner, make_schur_preconditioner
+ * (blockMatrix.hpp:637-685), on the device.  For r = [r_u (n_vel); r_p (n_pres)]:
+ *   w_u = A^-1 r_u;  r_p' = B w_u - r_p;  z_p = S^-1 r_p';
+ *   r_u' = r_u - B^T z_p;  z_u = A^-1 r_u';  z = [z_u; z_p]
+ * A_pc (n_vel rows) and S_pc (n_pres rows; NULL = identity) are preconditioners
+ * of this context, B (n_pres x n_vel) and Bt (n_vel x n_pres) its CSR handles;
+ * all of them must outlive the Schur preconditioner.  Every step stays on the
+ * device (no host round trip per apply); each step's arithmetic is the
+ * reference's, so with bit-exact parts the apply equals the reference's bit
+ * for bit. */
+b2s_status b2s_pc_create_schur(b2s_ctx* ctx, uint64_t n_vel, uint64_t n_pres, const b2s_csr* B, const b2s_csr* Bt,
+                               b2s_pc* A_pc, b2s_pc* S_pc, b2s_pc** out);
+/* z = alpha * M^-1 r for a preconditioner M of this context (which must
+ * outlive it): the scaled pressure AMG of the reference's 3-D Stokes test
+ * (test_BlockMatrix_schur3d.cpp:150-160, z[i] = scale * w[i]). */
+b2s_status b2s_pc_create_scaled(b2s_ctx* ctx, b2s_pc* inner, double alpha, b2s_pc** out);
+
 /* z = M^-1 r (the functor returned by the reference factories). */
 b2s_status b2s_pc_apply(b2s_ctx* ctx, b2s_pc* pc, const double* r, double* z);
 b2s_status b2s_pc_apply_device(b2s_ctx* ctx, b2s_pc* pc, const double* d_r, double* d_z);

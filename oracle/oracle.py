@@ -333,6 +333,7 @@ class Ref(_Lib):
         self._blk_pc_create = self._f("blk_pc_create", vp, vp, cp, cp, i32)
         self._blk_ilu0_export = self._f("blk_ilu0_export", i32, vp, i32, u32p, vp, vp, vp, vp, vp, vp, vp, vp)
         self._blk_amg_export = self._f("blk_amg_export", i32, vp, i32, i32, u32p, vp, vp, vp, vp, vp, vp, vp)
+        self._schur_create = self._f("schur_create", vp, u32, u32, vp, vp, vp, vp, f64)
 
     def set_threads(self, t: int):
         self._set_threads(int(t))
@@ -392,6 +393,14 @@ class Ref(_Lib):
         st = self._gmres_pc(A.h, pc.h, restart, tol, maxit, _f64(b), x, C.byref(it), err, 512)
         self._check(st, err)
         return x, it.value
+
+    def schur(self, n_vel, n_pres, B, Bt, A_pc, S_pc=None, scale=1.0):
+        """The reference's make_schur_preconditioner with these parts (S_pc
+        None: identity; else z = scale * S_pc(r))."""
+        h = self._schur_create(n_vel, n_pres, B.h, Bt.h, A_pc.h, S_pc.h if S_pc is not None else None, scale)
+        pc = _PC(self, h, n_vel + n_pres, "schur")
+        pc._keep = (B, Bt, A_pc, S_pc)
+        return pc
 
     def redblack(self, A):
         n = A.n

@@ -228,6 +228,39 @@ int ref_gmres_pc(void* A, void* p, int restart, double tol, int maxit, const dou
     });
 }
 
+// make_schur_preconditioner (blockMatrix.hpp:637-685) over the reference's
+// own SMatrix::spmv of B and B^T, with the velocity preconditioner A_pc and
+// the pressure preconditioner S_pc scaled by s_scale (z[i] = s_scale * w[i],
+// the S_pre of test_BlockMatrix_schur3d.cpp:150-160), or the identity
+// (z = r, test_BlockMatrix_schur.cpp:95) when S_pc is null.
+void* ref_schur_create(uint32_t n_vel, uint32_t n_pres, void* B, void* Bt, void* A_pc, void* S_pc, double s_scale)
+{
+    const SMatrix Bm = *static_cast<SMatrix*>(B), Btm = *static_cast<SMatrix*>(Bt);
+    block::SaddlePointSystem sys;
+    sys.n_vel = n_vel;
+    sys.n_pres = n_pres;
+    sys.spmv_B = [Bm](const std::vector<double>& x, std::vector<double>& y) { y = SMatrix::spmv(Bm, x); };
+    sys.spmv_Bt = [Btm](const std::vector<double>& x, std::vector<double>& y) { y = SMatrix::spmv(Btm, x); };
+    PC Sf;
+    if (S_pc)
+    {
+        const PC inner = static_cast<RefPC*>(S_pc)->f;
+        Sf = [inner, s_scale](const std::vector<double>& r, std::vector<double>& z) {
+            std::vector<double> w;
+            inner(r, w);
+            z.resize(r.size());
+            for (size_t i = 0; i < r.size(); ++i) z[i] = s_scale * w[i];
+        };
+    }
+    else
+        Sf = [](const std::vector<double>& r, std::vector<double>& z) { z = r; };
+    RefPC* pc = new RefPC();
+    pc->kind = "schur";
+    pc->n = n_vel + n_pres;
+    pc->f = block::make_schur_preconditioner(sys, static_cast<RefPC*>(A_pc)->f, Sf);
+    return pc;
+}
+
 // IC(0) factor of a "ic0" preconditioner (IC0_Data, array.cpp:2510-2521).
 // sizes[0] = nnz(L) incl. diagonal, sizes[1] = nnz(L^T strict).  Pass null
 // arrays to query sizes.  Returns 0 on success, -1 if the object is not IC0.

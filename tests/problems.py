@@ -90,3 +90,88 @@ def drand(i):
     """test_BlockMatrix_mpi.cpp:22-23 deterministic hash."""
     s = np.sin(np.asarray(i, np.float64) * 0.371 + 1.7) * 43758.5453
     return s - np.floor(s)
+
+
+def coo_merge(n, m, r, c, v):
+    """CSR from COO with duplicates summed in input order (as the reference's
+    COO constructor merges them), explicit zeros kept out."""
+    acc = {}
+    for i, j, x in zip(r, c, v):
+        acc[(i, j)] = acc.get((i, j), 0.0) + x
+    keys = [k for k in acc if acc[k] != 0.0]
+    return coo_to_csr(n, m, [k[0] for k in keys], [k[1] for k in keys], [acc[k] for k in keys])
+
+
+def stokes1d(N_vel):
+    """1-D Stokes saddle point of test_BlockMatrix_schur.cpp:34-80: K, A, B, B^T
+    as (rows, cols, rp, ci, v)."""
+    N_pres = N_vel - 1
+    N = N_vel + N_pres
+    R, Cc, V = [], [], []
+    for i in range(N_vel):
+        R.append(i); Cc.append(i); V.append(2.0)
+        if i > 0: R.append(i); Cc.append(i - 1); V.append(-1.0)
+        if i < N_vel - 1: R.append(i); Cc.append(i + 1); V.append(-1.0)
+    for i in range(N_pres):
+        R += [i + N_vel, i + N_vel, i, i + 1]
+        Cc += [i, i + 1, i + N_vel, i + N_vel]
+        V += [-1.0, 1.0, -1.0, 1.0]
+    return split_saddle(N_vel, N_pres, R, Cc, V)
+
+
+def split_saddle(N_vel, N_pres, R, Cc, V):
+    N = N_vel + N_pres
+    parts = {"A": ([], [], []), "B": ([], [], []), "Bt": ([], [], [])}
+    for r, c, v in zip(R, Cc, V):
+        if r < N_vel and c < N_vel:
+            key, rr, cc = "A", r, c
+        elif r >= N_vel and c < N_vel:
+            key, rr, cc = "B", r - N_vel, c
+        elif r < N_vel and c >= N_vel:
+            key, rr, cc = "Bt", r, c - N_vel
+        else:
+            continue
+        parts[key][0].append(rr); parts[key][1].append(cc); parts[key][2].append(v)
+    K = (N, N) + coo_merge(N, N, R, Cc, V)
+    A = (N_vel, N_vel) + coo_merge(N_vel, N_vel, *parts["A"])
+    B = (N_pres, N_vel) + coo_merge(N_pres, N_vel, *parts["B"])
+    Bt = (N_vel, N_pres) + coo_merge(N_vel, N_pres, *parts["Bt"])
+    return K, A, B, Bt
+
+
+def stokes3d(N, alpha=0.1):
+    """3-D periodic MAC Stokes of test_BlockMatrix_schur3d.cpp:39-133: K, A,
+    B, B^T and the pressure Laplacian Lp, as (rows, cols, rp, ci, v)."""
+    N3 = N * N * N
+    N_vel, N_pres = 3 * N3, N3
+    idx = lambda i, j, k: i + j * N + k * N * N
+    R, Cc, V = [], [], []
+    for comp in range(3):
+        off = comp * N3
+        for k in range(N):
+            for j in range(N):
+                for i in range(N):
+                    r = off + idx(i, j, k)
+                    R.append(r); Cc.append(r); V.append(6.0 + alpha)
+                    for (a, b_, c_) in (((i + 1) % N, j, k), ((i - 1 + N) % N, j, k), (i, (j + 1) % N, k),
+                                        (i, (j - 1 + N) % N, k), (i, j, (k + 1) % N), (i, j, (k - 1 + N) % N)):
+                        R.append(r); Cc.append(off + idx(a, b_, c_)); V.append(-1.0)
+    LR, LC, LV = [], [], []
+    for k in range(N):
+        for j in range(N):
+            for i in range(N):
+                p = idx(i, j, k)
+                rp_ = N_vel + p
+                LR.append(p); LC.append(p); LV.append(6.0 + 1e-8)
+                for (a, b_, c_) in (((i + 1) % N, j, k), ((i - 1 + N) % N, j, k), (i, (j + 1) % N, k),
+                                    (i, (j - 1 + N) % N, k), (i, j, (k + 1) % N), (i, j, (k - 1 + N) % N)):
+                    LR.append(p); LC.append(idx(a, b_, c_)); LV.append(-1.0)
+                for comp, prev in ((0, idx((i - 1 + N) % N, j, k)), (1, idx(i, (j - 1 + N) % N, k)),
+                                   (2, idx(i, j, (k - 1 + N) % N))):
+                    uc, up = comp * N3 + p, comp * N3 + prev
+                    R += [rp_, rp_, uc, up]
+                    Cc += [uc, up, rp_, rp_]
+                    V += [1.0, -1.0, 1.0, -1.0]
+    K, A, B, Bt = split_saddle(N_vel, N_pres, R, Cc, V)
+    Lp = (N_pres, N_pres) + coo_merge(N_pres, N_pres, LR, LC, LV)
+    return K, A, B, Bt, Lp

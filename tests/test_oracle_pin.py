@@ -237,3 +237,25 @@ def test_sor_reference_pinned(ref):
     x, it = ref.sor(ref.csr(n, n, rp, ci, v), b, 1.3, 1e-9, 500)
     xr, itr = _sor_restated(n, rp, ci, v, b, 1.3, 1e-9, 500)
     assert it == itr and np.array_equal(x, xr)
+
+
+def schur_restated(orc, Ao_pc, So_pc, scale, B, Bt, nv, r):
+    """make_schur_preconditioner's seven steps (blockMatrix.hpp:637-685)."""
+    ru, rp = r[:nv], r[nv:]
+    wu = Ao_pc.apply(ru)
+    rpm = orc.spmv(B, wu) - rp
+    zp = rpm.copy() if So_pc is None else scale * So_pc.apply(rpm)
+    rum = ru - orc.spmv(Bt, zp)
+    return np.concatenate([Ao_pc.apply(rum), zp])
+
+
+def test_schur_composition_pinned(orc, ref):
+    """The reference's Schur composition (compiled) equals its seven steps over
+    the restatement's ILU(0), SpMVs and the identity, bit for bit."""
+    K, A, B, Bt = P.stokes1d(60)
+    nv, np_ = A[0], B[0]
+    Ar, Br, Btr = (ref.csr(*m) for m in (A, B, Bt))
+    Ao, Bo, Bto = (orc.csr(*m) for m in (A, B, Bt))
+    pc = ref.schur(nv, np_, Br, Btr, ref.pc(Ar, "ilu0"))
+    r = P.drand(np.arange(nv + np_) + 3)
+    assert np.array_equal(pc.apply(r), schur_restated(orc, orc.pc(Ao, "ilu0"), None, 1.0, Bo, Bto, nv, r))
