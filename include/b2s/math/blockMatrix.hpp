@@ -274,4 +274,49 @@ namespace block
             std::copy(k.z_p.begin(), k.z_p.end(), z.begin() + nv);
         };
     }
+
+    // Extension: the same composition resident on the device, given B and
+    // B^T as matrices.  A_precond must come from this library's factories
+    // (make_*_preconditioner); an empty S_precond is the identity.  No step of
+    // an apply leaves the GPU (b2s_pc_create_schur), and the result equals the
+    // composition above bit for bit.
+    inline sparse::Precond make_schur_preconditioner(const SaddlePointSystem& sys, const sparse::SMatrix& B,
+                                                     const sparse::SMatrix& Bt, const sparse::Precond& A_precond,
+                                                     const sparse::Precond& S_precond = sparse::Precond())
+    {
+        using sparse::detail::DevicePrecond;
+        const DevicePrecond* Ad = A_precond.target<DevicePrecond>();
+        const DevicePrecond* Sd = S_precond ? S_precond.target<DevicePrecond>() : nullptr;
+        if (!Ad || (S_precond && !Sd))
+            throw std::invalid_argument("device Schur preconditioner: A_precond and S_precond must be device "
+                                        "preconditioners from the make_*_preconditioner factories");
+        b2s_pc* h = nullptr;
+        sparse::detail::check(b2s_pc_create_schur(sparse::detail::context(), sys.n_vel, sys.n_pres, B.device(),
+                                                  Bt.device(), Ad->pc.get(), Sd ? Sd->pc.get() : nullptr, &h),
+                              "Schur preconditioner");
+        DevicePrecond d;
+        d.pc.reset(h, [](b2s_pc* p) { b2s_pc_destroy(p); });
+        d.n = sys.n_vel + sys.n_pres;
+        // the parts stay alive as long as the composition
+        d.keep = std::make_shared<std::tuple<sparse::Precond, sparse::Precond, sparse::SMatrix, sparse::SMatrix>>(
+            A_precond, S_precond, B, Bt);
+        return sparse::Precond(d);
+    }
+
+    // Extension: z = alpha M^-1 r for a device preconditioner M (the scaled
+    // pressure AMG of the reference's 3-D Stokes test), on the device.
+    inline sparse::Precond make_scaled_preconditioner(const sparse::Precond& M, double alpha)
+    {
+        using sparse::detail::DevicePrecond;
+        const DevicePrecond* Md = M.target<DevicePrecond>();
+        if (!Md) throw std::invalid_argument("scaled preconditioner: M must be a device preconditioner");
+        b2s_pc* h = nullptr;
+        sparse::detail::check(b2s_pc_create_scaled(sparse::detail::context(), Md->pc.get(), alpha, &h),
+                              "scaled preconditioner");
+        DevicePrecond d;
+        d.pc.reset(h, [](b2s_pc* p) { b2s_pc_destroy(p); });
+        d.n = Md->n;
+        d.keep = std::make_shared<sparse::Precond>(M);
+        return sparse::Precond(d);
+    }
 }

@@ -99,6 +99,20 @@ static void test_schur_1d(uint32_t N_vel)
     for (uint32_t i = 0; i < N; ++i) err += (x[i] - xe[i]) * (x[i] - xe[i]);
     std::printf("[Schur] N_vel=%u GMRES it=%d err=%.3e\n", N_vel, it + 1, std::sqrt(err));
     CHECK(std::sqrt(err) < 1e-6, "Schur 1-D N_vel=%u err=%.3e", N_vel, std::sqrt(err));
+    // the device-resident composition (extension): the same iterates
+    auto schur_dev = make_schur_preconditioner(sys, B, Bt, Ap);
+    auto [xd, itd] = SMatrix::gmres(K, b, schur_dev, 50);
+    double dd = 0;
+    for (uint32_t i = 0; i < N; ++i) dd = std::max(dd, std::fabs(xd[i] - x[i]));
+    CHECK(itd == it && dd == 0.0, "device Schur N_vel=%u: it %d vs %d, max diff %.3e", N_vel, itd, it, dd);
+    auto scaled = make_scaled_preconditioner(Ap, 2.0);
+    std::vector<double> r1(N_vel), z1, z2;
+    for (uint32_t i = 0; i < N_vel; ++i) r1[i] = drand(i + 3);
+    Ap(r1, z1);
+    scaled(r1, z2);
+    bool same = z1.size() == z2.size();
+    for (size_t i = 0; same && i < z1.size(); ++i) same = z2[i] == 2.0 * z1[i];
+    CHECK(same, "scaled preconditioner");
 }
 
 int main()
