@@ -160,6 +160,11 @@ KERNELS = {
                 "(n=262144 rows, 64 -> 128)",
     "solve_c5": "one learned IC(0) PCG solve (8 Jacobi sweeps per triangle, fused iteration) on a 512^2 GRF system; "
                 "a step is setup + solve",
+    "pcg_c2_diag": "one PCG + diagonal solve on the 128^3 Poisson matrix (C2) to rtol 1e-10, no graphs: the "
+                   "fused k_vec updates and the CSR SpMV",
+    "gmres_c3_cgs2": "one GMRES(30) + ILU(0) solve with CGS2 orthogonalisation on the 96^3 convection-diffusion "
+                     "matrix (C3): the batched Arnoldi dots and updates",
+    "bilu0_setup_c4": "block ILU(0) factorisation of the Q1 elasticity matrix (C4, 64^3 elements)",
 }
 
 
@@ -199,6 +204,27 @@ def run_kernel(args):
             M = b2s.Precond(ctx, A, b2s.PC_LEARNED_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8,
                             factor_sweeps=5)
             b2s.solve_device(ctx, A, bt.data_ptr(), xt.data_ptr(), b2s.PCG, M, tol=TOL, maxit=MAXIT)
+    elif k in ("pcg_c2_diag", "gmres_c3_cgs2"):
+        if k == "pcg_c2_diag":
+            n, rp, ci, v = b2s.gen_poisson3d(128)
+            A = b2s.CSR(ctx, n, n, rp, ci, v)
+            M = b2s.Precond(ctx, A, b2s.PC_DIAG)
+            method, so = b2s.PCG, {"tol": 1e-10, "maxit": 2000, "use_graphs": 0}
+        else:
+            n, rp, ci, v = b2s.gen_convdiff3d(96)
+            A = b2s.CSR(ctx, n, n, rp, ci, v)
+            M = b2s.Precond(ctx, A, b2s.PC_ILU0)
+            method, so = b2s.GMRES, {"tol": 1e-8, "maxit": 2000, "restart": 30, "orth": b2s.ORTH_CGS2,
+                                     "use_graphs": 0}
+        bt = torch.from_numpy(b2s.uniform(7, n)).to(dev)
+        xt = torch.zeros(n, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        step = lambda: b2s.solve_device(ctx, A, bt.data_ptr(), xt.data_ptr(), method, M, **so)
+    elif k == "bilu0_setup_c4":
+        nbr, rp, ci, v = b2s.gen_elasticity_q1(64)
+        A = b2s.BAIJ(ctx, 3, nbr, nbr, rp, ci, v)
+        torch.cuda.synchronize()
+        step = lambda: b2s.Precond(ctx, A, b2s.PC_BILU0)
     elif k == "dense_c5":
         n = N_GRID * N_GRID
         g = torch.Generator(device=dev).manual_seed(5)
