@@ -130,11 +130,11 @@ def make_system(b2s, seed):
     return n, rp, ci, v, b
 
 
-# DRAM bytes (read + write) of one k_pcg_band launch on the 512^2 learned
-# solve: dram__bytes.sum.per_second x gpu__time_duration.sum of an ncu
+# DRAM bytes (read + write) of one persistent PCG launch on the 512^2
+# learned solve: dram__bytes.sum.per_second x gpu__time_duration.sum of an ncu
 # capture of `bench.py --kernel solve_c5` (SpeedOfLight and
-# MemoryWorkloadAnalysis sections, one launch).
-PCG_BAND_DRAM_BYTES = 33.7e6
+# MemoryWorkloadAnalysis sections, one launch); None until captured.
+PCG_DRAM_BYTES = {"k_pcg_band": 33.7e6, "k_pcg_tile": None}
 
 
 def peaks():
@@ -158,8 +158,8 @@ KERNELS = {
     "vcycle_c4": "block SA-AMG V-cycle on the Q1 elasticity matrix (C4, 64^3 elements, 3x3 blocks)",
     "dense_c5": "k_linear_tc<64,128>: the learned network's tcgen05 dense layer on the 512^2 grid's node states "
                 "(n=262144 rows, 64 -> 128)",
-    "solve_c5": "one learned IC(0) PCG solve (8 Jacobi sweeps per triangle, fused iteration) on a 512^2 GRF system; "
-                "a step is setup + solve",
+    "solve_c5": "one learned IC(0) PCG solve (6 Jacobi sweeps per triangle, the whole loop in the persistent "
+                "kernel) on a 512^2 GRF system; a step is setup + solve",
     "pcg_c2_diag": "one PCG + diagonal solve on the 128^3 Poisson matrix (C2) to rtol 1e-10, no graphs: the "
                    "fused k_vec updates and the CSR SpMV",
     "gmres_c3_cgs2": "one GMRES(30) + ILU(0) solve with CGS2 orthogonalisation on the 96^3 convection-diffusion "
@@ -201,7 +201,7 @@ def run_kernel(args):
         torch.cuda.synchronize()
 
         def step():
-            M = b2s.Precond(ctx, A, b2s.PC_LEARNED_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=8,
+            M = b2s.Precond(ctx, A, b2s.PC_LEARNED_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=6,
                             factor_sweeps=5)
             b2s.solve_device(ctx, A, bt.data_ptr(), xt.data_ptr(), b2s.PCG, M, tol=TOL, maxit=MAXIT)
     elif k in ("pcg_c2_diag", "gmres_c3_cgs2"):
@@ -496,7 +496,7 @@ def main():
     ap.add_argument("--impl", default="b2s", choices=["b2s", "reference"])
     ap.add_argument("--method", default="learned_ic0_j6",
                     choices=["learned_ic0_j6", "learned_ic0_j8", "learned_ic0", "fp32_ic0_j6", "fp32_ic0_j8",
-                             "fp32_ic0", "fp64_ic0", "sa_amg"])
+                             "fp32_ic0", "fp64_ic0", "learned_ic0_j6_strips", "sa_amg"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel", default=None, choices=sorted(KERNELS),
                     help="run one hot kernel only (for profilers), not the benchmark")
@@ -537,7 +537,10 @@ def main():
              "fp32_ic0_j8": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_JACOBI, 8, 5),
              "fp32_ic0": (b2s.PC_IC0, b2s.FP32, b2s.TRSV_AUTO, 0, 0),
              "fp64_ic0": (b2s.PC_IC0, b2s.FP64, b2s.TRSV_AUTO, 0, 0),
+             "learned_ic0_j6_strips": (b2s.PC_LEARNED_IC0, b2s.FP32, b2s.TRSV_JACOBI, 6, 5),
              "sa_amg": (b2s.PC_SA_AMG, b2s.FP64, b2s.TRSV_AUTO, 0, 0)}
+    # the persistent PCG kernel: 2-D tiles when they can be planned (default), or row strips
+    persist = {"learned_ic0_j6_strips": b2s.PERSIST_STRIPS}
 
     def make_pc(A, method):
         kind, prec, trsv, sweeps, fsweeps = kinds[method]
@@ -570,7 +573,8 @@ def main():
         e0.record(stream)
         M = make_pc(A, method)
         em.record(stream)
-        st = b2s.solve_device(ctx, A, bt.data_ptr(), xt.data_ptr(), b2s.PCG, M, tol=TOL, maxit=MAXIT)
+        st = b2s.solve_device(ctx, A, bt.data_ptr(), xt.data_ptr(), b2s.PCG, M, tol=TOL, maxit=MAXIT,
+                              persistent=persist.get(method, b2s.PERSIST_AUTO))
         e1.record(stream)
         e1.synchronize()
         launches = ctx.kernel_launches - l0
@@ -710,14 +714,18 @@ def main():
         launch_bytes = it_bytes * float(np.mean(head_its))
         solve_ms = float(np.mean([b for _, b in head_split]))
         achieved = launch_bytes / (solve_ms * 1e-3) / 1e9
-        roofline = {"kernel": "k_pcg_band (persistent cooperative PCG, the whole solve in one launch)",
+        tiles = M.sizes("pcg.tiles")[0] if persist.get(args.method, b2s.PERSIST_AUTO) == b2s.PERSIST_AUTO else 0
+        kname = "k_pcg_tile" if tiles else "k_pcg_band"
+        kdesc = (f"k_pcg_tile (persistent cooperative PCG over {tiles} 2-D tiles, the whole solve in one launch)"
+                 if tiles else "k_pcg_band (persistent cooperative PCG over row strips, the whole solve in one launch)")
+        roofline = {"kernel": kdesc,
                     "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                    "frac": achieved / pk["hbm_gbs"], "peak_kind": pk_kind, "traffic": PCG_BAND_DRAM_BYTES,
+                    "frac": achieved / pk["hbm_gbs"], "peak_kind": pk_kind, "traffic": PCG_DRAM_BYTES[kname],
                     "bytes_per_launch": launch_bytes, "bytes_per_iteration": it_bytes, "ms_per_launch": solve_ms,
                     "note": "duration = the event-timed solve phase of the timed steps (the launch plus the final "
                             "FP64 residual check); the operator, factors and vectors stay in L2, so DRAM traffic "
-                            "(ncu, one launch) is ~0.1% of the algorithmic bytes and the kernel is bound by its "
-                            "barriers, not by HBM"}
+                            "(ncu, one launch) is a small fraction of the algorithmic bytes and the kernel is bound "
+                            "by its per-iteration synchronisation, not by HBM"}
 
     # the learned network's tcgen05 dense layer (64 -> 128) on this grid's node
     # states: X read once, Y written once
@@ -801,6 +809,8 @@ def main():
                        "fp32_ic0_j8": "plain IC(0) (5-sweep fixed-point factor), FP32, 8 Jacobi sweeps per triangle",
                        "fp32_ic0": "plain IC(0), FP32 factor, exact triangular solves",
                        "fp64_ic0": "plain IC(0), FP64, exact triangular solves",
+                       "learned_ic0_j6_strips": "learned_ic0_j6 with the whole PCG loop in the row-strip "
+                                                "persistent kernel (k_pcg_band) instead of the 2-D tile one",
                        "sa_amg": "smoothed-aggregation AMG V-cycle (FP64)"}[args.method],
             "data": "synthetic (seeded GRF diffusion, held-out seeds 2000+)",
             "config": arm_config(args, world),

@@ -87,7 +87,7 @@ class PcOpts(C.Structure):
 class SolveOpts(C.Structure):
     _fields_ = [("tol", C.c_double), ("maxit", C.c_int), ("restart", C.c_int), ("orth", C.c_int),
                 ("ir_steps", C.c_int), ("ir_inner_tol", C.c_double), ("check_every", C.c_int),
-                ("use_graphs", C.c_int), ("stall_window", C.c_int)]
+                ("use_graphs", C.c_int), ("stall_window", C.c_int), ("persistent", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -414,6 +414,12 @@ class Precond:
         self.ctx.check(lib().b2s_pc_apply(self.ctx.h, self.h, _f64(r), z), "pc_apply")
         return z
 
+    def sizes(self, what: str):
+        """The three sizes b2s_pc_export reports for `what` (no arrays)."""
+        sizes = (C.c_uint64 * 3)()
+        self.ctx.check(lib().b2s_pc_export(self.ctx.h, self.h, what.encode(), sizes, None, None, None), "pc_export")
+        return tuple(int(x) for x in sizes)
+
     def export(self, what: str):
         """(rp, ci, v) arrays of an internal factor (see b2s_pc_export)."""
         sizes = (C.c_uint64 * 3)()
@@ -554,13 +560,17 @@ class Learner:
             pass
 
 
+PERSIST_AUTO, PERSIST_STRIPS, PERSIST_OFF = range(3)
+
+
 def solve_opts(tol=1e-10, maxit=2000, restart=30, orth=ORTH_MGS, ir_steps=0, ir_inner_tol=0.0, check_every=0,
-               use_graphs=1, stall_window=0) -> SolveOpts:
+               use_graphs=1, stall_window=0, persistent=PERSIST_AUTO) -> SolveOpts:
     o = SolveOpts()
     lib().b2s_solve_opts_default(C.byref(o))
     o.tol, o.maxit, o.restart, o.orth = tol, maxit, restart, orth
     o.ir_steps, o.ir_inner_tol, o.check_every, o.use_graphs = ir_steps, ir_inner_tol, check_every, use_graphs
     o.stall_window = stall_window
+    o.persistent = persistent
     return o
 
 

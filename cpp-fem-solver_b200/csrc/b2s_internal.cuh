@@ -261,12 +261,14 @@ struct PcImpl
     // The whole PCG loop in one persistent launch (from the state after
     // the first z = M^-1 r, p = z, rz_old): r, p in two buffers each, x
     // updated in place, st on exit as the iteration-by-iteration loop would
-    // leave it (st->stalled when the stall guard stopped it).  False, with
-    // nothing enqueued, when the preconditioner cannot run it.
+    // leave it (st->stalled when the stall guard stopped it).  which: the
+    // b2s_solve_opts.persistent choice.  False, with nothing enqueued, when
+    // the preconditioner cannot run it.
     virtual bool pcg_persistent(b2s_ctx*, const CsrDev& A, double* x, double* r0, double* r1, double* p0,
-                                double* p1, double* z, double* Ap, KState* st, int stall_window)
+                                double* p1, double* z, double* Ap, KState* st, int stall_window, int which)
     {
         (void)A, (void)x, (void)r0, (void)r1, (void)p0, (void)p1, (void)z, (void)Ap, (void)st, (void)stall_window;
+        (void)which;
         return false;
     }
     // one triangle of a factored preconditioner M = L L^T (FP64 storage):

@@ -925,7 +925,8 @@ static void run_pcg(Solve& S, const double* b, double* x, b2s_stats* stats)
             // residual and direction alternate between two buffers, so a
             // captured batch has an even number of iterations.
             // all iterations in one persistent launch when the preconditioner can
-            if (S.pc->pcg_persistent(ctx, *S.A.csr, x, r, r1, p, p1, z, Ap, st, S.stall_window))
+            if (S.o.persistent != 2 &&
+                S.pc->pcg_persistent(ctx, *S.A.csr, x, r, r1, p, p1, z, Ap, st, S.stall_window, S.o.persistent))
             {
                 const KState hs = S.read_state();
                 if (hs.stalled)

@@ -26,6 +26,7 @@
 #include "trsv_chunk.cuh"
 #include "trsv_band.cuh"
 #include "pcg_band.cuh"
+#include "pcg_tile.cuh"
 
 #include <exception>
 #include <thread>
@@ -661,6 +662,7 @@ struct HostAnalysis
     std::vector<uint32_t> up_level;
     ChunkPlan lo_plan, up_plan;
     BandPlan lo_band, up_band;
+    TilePlan tiles;  // the tiled persistent PCG kernel's plan (sweep schedule, FP32)
     bool chunked = false;
     std::exception_ptr error;
     std::thread th;
@@ -766,9 +768,109 @@ struct PcIC0 final : PcImpl
 
     DBuf<unsigned> pcg_ctl;  // grid-barrier counter, error word
 
-    bool pcg_persistent(b2s_ctx* ctx, const CsrDev& A, double* x, double* r0, double* r1, double* p0, double* p1,
-                        double* z, double* Ap, KState* st, int stall_window) override
+    // the tiled persistent PCG kernel (pcg_tile.cuh), when its plan was made
+    // and A's pattern matched it
+    bool tiles_ready = false;
+    uint32_t tile_n = 0, tile_count = 0, tile_Q = 0, tile_smem = 0, tile_work = 0, tile_ystride = 0;
+    DBuf<TileDesc> tile_desc;
+    DBuf<uint8_t> tile_idx, tile_vals;
+    DBuf<unsigned long long> tile_slots;
+
+    // uploads the plan and packs the value blobs from A and the band arrays
+    void load_tiles(b2s_ctx* ctx, const CsrDev& A, const TilePlan& P)
     {
+        tiles_ready = false;
+        if (!P.ok || A.n != n) return;
+        tile_desc = upload(ctx, P.desc);
+        tile_idx = upload(ctx, P.idx.data(), P.idx.size());
+        tile_vals.alloc(P.vbytes ? P.vbytes : 16);
+        tile_slots.alloc(6ull * P.ntiles);
+        DBuf<int> bad(1);
+        B2S_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream));
+        B2S_LAUNCH(ctx, k_tile_pack, P.ntiles, kThreads, 0, tile_desc.p, tile_idx.p, tile_vals.p, n, A.rp.p, A.ci.p,
+                   A.v.p, fwd.band_off.p, fwd.band_val.p, fwd.band_dinv.p, bwd.band_off.p, bwd.band_val.p,
+                   bwd.band_dinv.p, bad.p);
+        int hb = 0;
+        d2h(ctx, &hb, bad.p, sizeof(int));
+        sync(ctx);
+        if (hb) return;  // A is not the structurally symmetric matrix of L's pattern: the banded kernel runs
+        tile_n = n;
+        tile_count = P.ntiles;
+        tile_Q = P.Q;
+        tile_smem = P.smem;
+        tile_work = P.work;
+        tile_ystride = tile_align16(4ull * P.max_ext) / 4;
+        tiles_ready = true;
+    }
+
+    template <uint32_t Q>
+    bool launch_tiles(b2s_ctx* ctx, PcgTileArgs& a)
+    {
+        B2S_CUDA(cudaFuncSetAttribute(k_pcg_tile<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem));
+        void* params[] = {&a};
+        const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_tile<Q>, dim3(tile_count),
+                                                          dim3(kTileThreads), params, tile_smem, ctx->stream);
+        if (e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported)
+        {
+            cudaGetLastError();
+            return false;
+        }
+        B2S_CUDA(e);
+        note_launch(ctx, "k_pcg_tile");
+        return true;
+    }
+
+    // the whole PCG loop as one k_pcg_tile launch; false (nothing enqueued) when it cannot run
+    bool pcg_tiles(b2s_ctx* ctx, const CsrDev& A, double* x, double* r0, double* r1, double* p0, double* p1,
+                   double* z, double* Ap, KState* st, int stall_window)
+    {
+        if (!tiles_ready || A.n != tile_n || A.rp.p == nullptr || fwd.sweeps != bwd.sweeps) return false;
+        if (!pcg_ctl.p) pcg_ctl.alloc(2);
+        B2S_CUDA(cudaMemsetAsync(pcg_ctl.p, 0, 2 * sizeof(unsigned), ctx->stream));
+        B2S_CUDA(cudaMemsetAsync(tile_slots.p, 0, tile_slots.bytes(), ctx->stream));
+        PcgTileArgs a{};
+        a.n = n;
+        a.ntiles = tile_count;
+        a.work = tile_work;
+        a.ystride = tile_ystride;
+        a.k = fwd.sweeps;
+        a.desc = tile_desc.p;
+        a.vals = reinterpret_cast<const uint4*>(tile_vals.p);
+        a.idx = reinterpret_cast<const uint4*>(tile_idx.p);
+        a.x = x;
+        a.r[0] = r0;
+        a.r[1] = r1;
+        a.p[0] = p0;
+        a.p[1] = p1;
+        a.z = z;
+        a.Ap = Ap;
+        a.y32 = y32.p;
+        a.slots = tile_slots.p;
+        a.st = st;
+        a.err = reinterpret_cast<int*>(pcg_ctl.p + 1);
+        a.stall_window = stall_window;
+        bool ok = false;
+        switch (tile_Q)
+        {
+            case 1: ok = launch_tiles<1>(ctx, a); break;
+            case 2: ok = launch_tiles<2>(ctx, a); break;
+            case 3: ok = launch_tiles<3>(ctx, a); break;
+            case 4: ok = launch_tiles<4>(ctx, a); break;
+            default: return false;
+        }
+        if (!ok) return false;
+        int err = 0;
+        d2h(ctx, &err, pcg_ctl.p + 1, sizeof(int));
+        sync(ctx);
+        if (err) fail(B2S_TIMEOUT, "persistent PCG: a tile's all-reduce wait gave up");
+        return true;
+    }
+
+    bool pcg_persistent(b2s_ctx* ctx, const CsrDev& A, double* x, double* r0, double* r1, double* p0, double* p1,
+                        double* z, double* Ap, KState* st, int stall_window, int which) override
+    {
+        if (can_fuse_pcg() && which == 0 && pcg_tiles(ctx, A, x, r0, r1, p0, p1, z, Ap, st, stall_window))
+            return true;
         const BandPlan &lb = fwd.band, &ub = bwd.band;
         if (!(can_fuse_pcg() && fwd.segment == 1 && bwd.segment == 1 && lb.W == 2 && ub.W == 2 && lb.T == ub.T &&
               lb.B == ub.B && lb.Rmax == ub.Rmax && lb.ntiles == ub.ntiles && fwd.sweeps == bwd.sweeps &&
@@ -866,6 +968,13 @@ struct PcIC0 final : PcImpl
         }
         if (what == "levels.L") return export_levels(ctx, fwd, sizes, ci);
         if (what == "levels.U") return export_levels(ctx, bwd, sizes, ci);
+        if (what == "pcg.tiles")  // the tiled persistent PCG kernel: tiles (0: not planned), rows per thread, smem
+        {
+            sizes[0] = tiles_ready ? tile_count : 0;
+            sizes[1] = tiles_ready ? tile_Q : 0;
+            sizes[2] = tiles_ready ? tile_smem : 0;
+            return;
+        }
         PcImpl::export_data(ctx, what, sizes, rp, ci, v);
     }
 };
@@ -967,7 +1076,10 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     ha.chunked = pc->mode == B2S_TRSV_CHUNK && n;
     const int sm_count = ctx->sm_count;
     const bool fp32 = pc->fp32;
-    ha.th = std::thread([&ha, &hrp, &hci, &pc, n, vs, sweeps, nsweeps, seg, sm_count, fp32] {
+    int smem_optin = 0;
+    B2S_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    const uint32_t tile_smem = smem_optin > 4096 ? (uint32_t)smem_optin - 4096u : 0u;  // static shared memory aside
+    ha.th = std::thread([&ha, &hrp, &hci, &pc, n, vs, sweeps, nsweeps, seg, sm_count, fp32, tile_smem] {
         try
         {
             if (sweeps)
@@ -980,6 +1092,16 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
                         else
                             ha.up_band = plan_band_transposed(n, hrp.data(), hci.data(), nsweeps, sm_count, seg);
                     });
+                // the tiled persistent PCG kernel: plain Jacobi, two strict entries per row
+                if (fp32 && seg == 1 && ha.lo_band.T && ha.up_band.T && ha.lo_band.W == 2 && ha.up_band.W == 2 &&
+                    nsweeps <= kTileMaxSweeps)
+                {
+                    std::vector<uint32_t> lrp, lci, urp, uci;
+                    strict_lower(n, hrp.data(), hci.data(), lrp, lci);
+                    strict_transpose(n, hrp.data(), hci.data(), true, urp, uci);
+                    ha.tiles = plan_tiles(n, lrp.data(), lci.data(), urp.data(), uci.data(), nsweeps, sm_count,
+                                          tile_smem, 8);
+                }
                 return;
             }
             strict_transpose(n, hrp.data(), hci.data(), true, ha.up_rp, ha.up_ci);
@@ -1043,6 +1165,7 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     {
         pc->fwd.pack<float>(ctx, pc->L.v32.p, pc->diag32.p);
         pc->bwd.pack<float>(ctx, pc->LT.v32.p, pc->diag32.p);
+        if (sweeps && ha.tiles.ok && pc->fwd.band.T && pc->bwd.band.T) pc->load_tiles(ctx, A, ha.tiles);
     }
     else
     {

@@ -1,0 +1,428 @@
+// The whole PCG loop in one persistent kernel over 2-D tiles (tile_plan.hpp),
+// for an IC(0)-type preconditioner whose two FP32 triangles are applied by k
+// plain Jacobi sweeps (at most two strict entries per row).
+//
+// A cooperative launch of one CTA per tile (all resident, one per SM).  At
+// launch a CTA copies its tile's two blobs into shared memory: the global
+// rows of its owned rows and halos, every extended row's two dependencies as
+// local indices, the triangles' strict entries and reciprocals, and its
+// owned rows of A with local columns.  Nothing static is read from global
+// memory again.  Each iteration is three phases:
+//   1. p = z + beta p_old staged for the SpMV's columns; Ap = A p and p.Ap
+//      for the owned rows (CSR order);
+//   2. the forward sweeps over the tile's lower extended set, the right-hand
+//      side r_old - alpha Ap gathered for every row of it; the owned rows
+//      store y, r and x += alpha p and reduce r.r;
+//   3. the backward sweeps over the upper extended set on y; the owned rows
+//      store z and reduce r.z.
+// Sweep s computes the rows of layers 0..k-s (a prefix of the local order),
+// so the owned rows equal the global sweep definition bit for bit, as the
+// banded kernel's do.  The arithmetic of every row is that of k_pcg_band;
+// only the association of the three per-iteration dot products differs (the
+// tiles are other row sets).
+//
+// A phase ends with an all-reduce that is also the grid barrier: thread 0
+// publishes the tile's partial as two 64-bit words {epoch, 32 value bits}
+// with release stores, and warp 0 of every CTA polls all tiles' words with
+// acquire loads (every lane its tiles at once) until they carry the phase's
+// epoch, then sums them in tile order -- one L2 round trip where a barrier
+// and a separate read of the partials took two.  Every CTA gets the same bits
+// and takes the same scalar step.  Each wait is bounded (kGridBarrierPolls
+// polls); a CTA that gives up records B2S_TIMEOUT and leaves, and the others
+// give up at their next all-reduce, so the launch always ends.
+#pragma once
+
+#include "pcg_band.cuh"
+#include "tile_plan.hpp"
+#include "trsv_chunk.cuh"
+
+namespace b2s {
+
+constexpr uint32_t kTileMaxTilesPerLane = 5;  // all-reduce over at most 160 tiles
+
+struct PcgTileArgs
+{
+    uint32_t n, ntiles, work, ystride;
+    int k;
+    const TileDesc* desc;
+    const uint4* vals;  // value blobs
+    const uint4* idx;   // index blobs
+    double* x;
+    double* r[2];
+    double* p[2];
+    double *z, *Ap;
+    float* y32;
+    unsigned long long* slots;  // 3 phases x ntiles x 2 words, zero at launch
+    KState* st;
+    int* err;
+    int stall_window;
+};
+
+__device__ __forceinline__ void st_release_gpu_u64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_gpu_u64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Thread 0 holds this tile's partial `part`.  Publishes it for `epoch`, waits
+// for every tile's, and leaves their sum (tile order; the same bits in every
+// CTA) in *out.  False, with B2S_TIMEOUT recorded, when a wait gives up.
+__device__ __forceinline__ bool tile_allreduce(unsigned long long* slots, uint32_t tile, uint32_t ntiles,
+                                               uint32_t epoch, double part, double* out, int* err, int* s_ok)
+{
+    if (threadIdx.x == 0)
+    {
+        const unsigned long long e = (unsigned long long)epoch << 32;
+        const unsigned long long b = (unsigned long long)__double_as_longlong(part);
+        st_release_gpu_u64(&slots[2 * tile], e | (b & 0xffffffffull));
+        st_release_gpu_u64(&slots[2 * tile + 1], e | (b >> 32));
+    }
+    if (threadIdx.x < 32)
+    {
+        const uint32_t lane = threadIdx.x;
+        double v[kTileMaxTilesPerLane];
+        bool ok = false;
+        for (unsigned polls = 0; polls < kGridBarrierPolls; ++polls)
+        {
+            bool all = true;
+#pragma unroll
+            for (uint32_t j = 0; j < kTileMaxTilesPerLane; ++j)
+            {
+                const uint32_t b = lane + 32 * j;
+                v[j] = 0.0;
+                if (b < ntiles)
+                {
+                    const unsigned long long w0 = ld_acquire_gpu_u64(&slots[2 * b]);
+                    const unsigned long long w1 = ld_acquire_gpu_u64(&slots[2 * b + 1]);
+                    all &= (uint32_t)(w0 >> 32) == epoch && (uint32_t)(w1 >> 32) == epoch;
+                    v[j] = __longlong_as_double((long long)(((w1 & 0xffffffffull) << 32) | (w0 & 0xffffffffull)));
+                }
+            }
+            if (__all_sync(0xffffffffu, all))
+            {
+                ok = true;
+                break;
+            }
+        }
+        double t = 0.0;
+#pragma unroll
+        for (uint32_t j = 0; j < kTileMaxTilesPerLane; ++j)
+            if (lane + 32 * j < ntiles) t += v[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (lane == 0)
+        {
+            *out = t;
+            *s_ok = ok ? 1 : 0;
+            if (!ok) atomicExch(err, (int)B2S_TIMEOUT);
+        }
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+
+// k + 1 passes over the extended set; rows of layers 0..k-s at pass s.
+// Returns the buffer holding pass k.
+template <uint32_t Q>
+__device__ __forceinline__ const float* tile_sweeps(int k, const uint16_t* cnt, const uint32_t (&dep)[Q],
+                                                    const float2 (&val)[Q], const float (&di)[Q],
+                                                    const float (&rr)[Q], float* y0, float* y1)
+{
+    constexpr uint32_t NT = kTileThreads;
+    for (int s = 0; s <= k; ++s)
+    {
+        const float* yin = (s & 1) ? y0 : y1;
+        float* yout = (s & 1) ? y1 : y0;
+        const uint32_t t1 = cnt[k - s];
+#pragma unroll
+        for (uint32_t q = 0; q < Q; ++q)
+        {
+            const uint32_t t = threadIdx.x + NT * q;
+            if (t < t1)
+            {
+                float sum = rr[q];
+                if (s > 0)
+                {
+                    const uint32_t d0 = dep[q] & 0xFFFFu, d1 = dep[q] >> 16;
+                    if (d0 != kTileNoDep) sum -= val[q].x * yin[d0];
+                    if (d1 != kTileNoDep) sum -= val[q].y * yin[d1];
+                }
+                yout[t] = sum * di[q];
+            }
+        }
+        __syncthreads();
+    }
+    return (k & 1) ? y1 : y0;
+}
+
+template <uint32_t Q>
+__global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
+{
+    constexpr uint32_t NT = kTileThreads;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ KState sst;
+    __shared__ int s_ok;
+    __shared__ double s_best, s_sum;
+    __shared__ int s_best_at;
+    const uint32_t tile = blockIdx.x, ntiles = a.ntiles, tid = threadIdx.x;
+    const TileDesc& Dg = a.desc[tile];
+    const uint32_t n_own = Dg.n_own, n_el = Dg.n_el, n_eu = Dg.n_eu, n_ae = Dg.n_ae;
+    // ---- the tile's blobs -> shared memory (16-byte copies)
+    {
+        const uint4* vs = a.vals + Dg.vbase / 16;
+        const uint4* is = a.idx + Dg.ibase / 16;
+        uint4* vd = reinterpret_cast<uint4*>(smem);
+        uint4* id = reinterpret_cast<uint4*>(smem + Dg.vbytes);
+        for (uint32_t i = tid; i < Dg.vbytes / 16; i += NT) cp_async16(vd + i, vs + i);
+        for (uint32_t i = tid; i < Dg.ibytes / 16; i += NT) cp_async16(id + i, is + i);
+        cp_async_wait_all();
+    }
+    __shared__ uint16_t s_lcnt[kTileMaxSweeps + 1], s_ucnt[kTileMaxSweeps + 1];
+    if (tid <= (uint32_t)a.k)
+    {
+        s_lcnt[tid] = Dg.lcnt[tid];
+        s_ucnt[tid] = Dg.ucnt[tid];
+    }
+    if (tid == 0)
+    {
+        sst = *a.st;
+        s_best = HUGE_VAL;
+        s_best_at = 0;
+    }
+    __syncthreads();
+    const unsigned char* ib = smem + Dg.vbytes;
+    const double* aval = reinterpret_cast<const double*>(smem + Dg.o_aval);
+    const float2* lvals = reinterpret_cast<const float2*>(smem + Dg.o_lvals);
+    const float2* uvals = reinterpret_cast<const float2*>(smem + Dg.o_uvals);
+    const float* ldinv = reinterpret_cast<const float*>(smem + Dg.o_ldinv);
+    const float* udinv = reinterpret_cast<const float*>(smem + Dg.o_udinv);
+    const uint32_t* owned = reinterpret_cast<const uint32_t*>(ib + Dg.o_owned);
+    const uint32_t* lhalo = reinterpret_cast<const uint32_t*>(ib + Dg.o_lhalo);
+    const uint32_t* ldeps = reinterpret_cast<const uint32_t*>(ib + Dg.o_ldeps);
+    const uint32_t* uhalo = reinterpret_cast<const uint32_t*>(ib + Dg.o_uhalo);
+    const uint32_t* udeps = reinterpret_cast<const uint32_t*>(ib + Dg.o_udeps);
+    const uint32_t* ahalo = reinterpret_cast<const uint32_t*>(ib + Dg.o_ahalo);
+    const uint32_t* arp = reinterpret_cast<const uint32_t*>(ib + Dg.o_arp);
+    const uint16_t* acol = reinterpret_cast<const uint16_t*>(ib + Dg.o_acol);
+    float* const y0 = reinterpret_cast<float*>(smem + a.work);
+    float* const y1 = y0 + a.ystride;
+    double* const pe = reinterpret_cast<double*>(smem + a.work);  // phase 1 only (aliases y0 / y1)
+
+    uint32_t epoch = 0;
+    int parity = 0;
+    double pv[Q], rd[Q];  // the owned rows' p and updated r (thread's rows t = tid + NT q)
+#pragma unroll
+    for (uint32_t q = 0; q < Q; ++q) pv[q] = rd[q] = 0.0;
+    while (!sst.done)
+    {
+        const double* pold = a.p[parity];
+        double* pnew = a.p[parity ^ 1];
+        const double* rold = a.r[parity];
+        double* rnew = a.r[parity ^ 1];
+        // ---- 1. p = z + beta p_old at the SpMV's columns; Ap; p.Ap
+        {
+            const double beta = sst.beta;
+            for (uint32_t t = tid; t < n_ae; t += NT)
+            {
+                const uint32_t g = t < n_own ? owned[t] : ahalo[t - n_own];
+                pe[t] = __ldcg(&a.z[g]) + beta * __ldcg(&pold[g]);
+            }
+            __syncthreads();
+            double acc[1] = {0.0};
+#pragma unroll
+            for (uint32_t q = 0; q < Q; ++q)
+            {
+                const uint32_t t = tid + NT * q;
+                if (t < n_own)
+                {
+                    double sum = 0.0;
+                    for (uint32_t e = arp[t]; e < arp[t + 1]; ++e) sum += aval[e] * pe[acol[e]];
+                    const double pr = pe[t];
+                    const uint32_t g = owned[t];
+                    pnew[g] = pr;
+                    a.Ap[g] = sum;
+                    acc[0] += pr * sum;
+                    pv[q] = pr;
+                }
+            }
+            block_reduce<1, NT>(acc);
+            if (!tile_allreduce(a.slots, tile, ntiles, ++epoch, acc[0], &s_sum, a.err, &s_ok)) break;
+            if (tid == 0) pcg_alpha(&sst, s_sum);
+            __syncthreads();
+            if (sst.done) break;
+        }
+        // ---- 2. forward sweeps on r = r_old - alpha Ap; x, r; r.r
+        {
+            const double alpha = sst.alpha;
+            uint32_t dep[Q];
+            float2 val[Q];
+            float di[Q], rr[Q];
+#pragma unroll
+            for (uint32_t q = 0; q < Q; ++q)
+            {
+                const uint32_t t = tid + NT * q;
+                const bool in = t < n_el;
+                const uint32_t g = in ? (t < n_own ? owned[t] : lhalo[t - n_own]) : 0u;
+                dep[q] = in ? ldeps[t] : 0xFFFFFFFFu;
+                val[q] = in ? lvals[t] : make_float2(0.f, 0.f);
+                di[q] = in ? ldinv[t] : 0.f;
+                const double rv = in ? __ldcg(&rold[g]) - alpha * __ldcg(&a.Ap[g]) : 0.0;
+                rr[q] = (float)rv;
+                if (t < n_own) rd[q] = rv;
+            }
+            const float* yk = tile_sweeps<Q>(a.k, s_lcnt, dep, val, di, rr, y0, y1);
+            double acc[1] = {0.0};
+#pragma unroll
+            for (uint32_t q = 0; q < Q; ++q)
+            {
+                const uint32_t t = tid + NT * q;
+                if (t < n_own)
+                {
+                    const uint32_t g = owned[t];
+                    a.y32[g] = yk[t];
+                    a.x[g] += alpha * pv[q];
+                    rnew[g] = rd[q];
+                    acc[0] += rd[q] * rd[q];
+                }
+            }
+            block_reduce<1, NT>(acc);
+            if (!tile_allreduce(a.slots + 2ull * ntiles, tile, ntiles, ++epoch, acc[0], &s_sum, a.err, &s_ok))
+                break;
+            if (tid == 0)
+            {
+                if (!pcg_check_converged(&sst, s_sum) && a.stall_window > 0)
+                {
+                    if (sst.relres < 0.5 * s_best)
+                    {
+                        s_best = sst.relres;
+                        s_best_at = sst.it;
+                    }
+                    else if (sst.it - s_best_at >= a.stall_window)
+                    {
+                        sst.stalled = 1;
+                        sst.iters = sst.it + 1;
+                        finish(&sst, B2S_OK);
+                    }
+                }
+            }
+            __syncthreads();
+            if (sst.done) break;
+        }
+        // ---- 3. backward sweeps on y; z; r.z and beta
+        {
+            uint32_t dep[Q];
+            float2 val[Q];
+            float di[Q], rr[Q];
+#pragma unroll
+            for (uint32_t q = 0; q < Q; ++q)
+            {
+                const uint32_t t = tid + NT * q;
+                const bool in = t < n_eu;
+                const uint32_t g = in ? (t < n_own ? owned[t] : uhalo[t - n_own]) : 0u;
+                dep[q] = in ? udeps[t] : 0xFFFFFFFFu;
+                val[q] = in ? uvals[t] : make_float2(0.f, 0.f);
+                di[q] = in ? udinv[t] : 0.f;
+                rr[q] = in ? __ldcg(&a.y32[g]) : 0.f;
+            }
+            const float* yk = tile_sweeps<Q>(a.k, s_ucnt, dep, val, di, rr, y0, y1);
+            double acc[1] = {0.0};
+#pragma unroll
+            for (uint32_t q = 0; q < Q; ++q)
+            {
+                const uint32_t t = tid + NT * q;
+                if (t < n_own)
+                {
+                    const double zi = (double)yk[t];
+                    a.z[owned[t]] = zi;
+                    acc[0] += rd[q] * zi;
+                }
+            }
+            block_reduce<1, NT>(acc);
+            if (!tile_allreduce(a.slots + 4ull * ntiles, tile, ntiles, ++epoch, acc[0], &s_sum, a.err, &s_ok))
+                break;
+            if (tid == 0) pcg_next(&sst, s_sum);
+            __syncthreads();
+        }
+        parity ^= 1;
+    }
+    if (tile == 0 && tid == 0) *a.st = sst;
+}
+
+// Fills the value blobs after factorisation: A's values for the owned rows
+// (checking that A's row holds exactly the planned columns), the triangles'
+// strict entries and reciprocals from the banded sweep arrays (slot e of row
+// g at e*n + g, checking the planned dependency's offset).  *bad = 1 when A's
+// pattern or the factor's differs from the plan.
+__global__ void k_tile_pack(const TileDesc* __restrict__ desc, const uint8_t* __restrict__ idx,
+                            uint8_t* __restrict__ vals, uint32_t n, const uint32_t* __restrict__ Arp,
+                            const uint32_t* __restrict__ Aci, const double* __restrict__ Av,
+                            const uint16_t* __restrict__ loff, const float* __restrict__ lval,
+                            const float* __restrict__ ldinv, const uint16_t* __restrict__ uoff,
+                            const float* __restrict__ uval, const float* __restrict__ udinv, int* bad)
+{
+    const TileDesc D = desc[blockIdx.x];
+    const uint8_t* ib = idx + D.ibase;
+    uint8_t* vb = vals + D.vbase;
+    const uint32_t* owned = reinterpret_cast<const uint32_t*>(ib + D.o_owned);
+    const uint32_t* lhalo = reinterpret_cast<const uint32_t*>(ib + D.o_lhalo);
+    const uint32_t* ldeps = reinterpret_cast<const uint32_t*>(ib + D.o_ldeps);
+    const uint32_t* uhalo = reinterpret_cast<const uint32_t*>(ib + D.o_uhalo);
+    const uint32_t* udeps = reinterpret_cast<const uint32_t*>(ib + D.o_udeps);
+    const uint32_t* ahalo = reinterpret_cast<const uint32_t*>(ib + D.o_ahalo);
+    const uint32_t* arp = reinterpret_cast<const uint32_t*>(ib + D.o_arp);
+    const uint16_t* acol = reinterpret_cast<const uint16_t*>(ib + D.o_acol);
+    double* aval = reinterpret_cast<double*>(vb + D.o_aval);
+    float2* lv = reinterpret_cast<float2*>(vb + D.o_lvals);
+    float2* uv = reinterpret_cast<float2*>(vb + D.o_uvals);
+    float* ld = reinterpret_cast<float*>(vb + D.o_ldinv);
+    float* ud = reinterpret_cast<float*>(vb + D.o_udinv);
+    auto ae_global = [&](uint32_t c) { return c < D.n_own ? owned[c] : ahalo[c - D.n_own]; };
+    for (uint32_t q = threadIdx.x; q < D.n_own; q += blockDim.x)
+    {
+        const uint32_t g = owned[q];
+        const uint32_t a0 = Arp[g], cntA = Arp[g + 1] - a0, e0 = arp[q], cntP = arp[q + 1] - e0;
+        if (cntA != cntP)
+        {
+            atomicExch(bad, 1);
+            continue;
+        }
+        for (uint32_t e = 0; e < cntP; ++e)
+        {
+            if (Aci[a0 + e] != ae_global(acol[e0 + e])) atomicExch(bad, 1);
+            aval[e0 + e] = Av[a0 + e];
+        }
+    }
+    // one triangle's extended rows: values and reciprocal from the band slots
+    auto tri = [&](uint32_t ne, const uint32_t* halo, const uint32_t* deps, const uint16_t* off, const float* val,
+                   const float* dinv, float2* outv, float* outd, bool lower) {
+        auto glob = [&](uint32_t t) { return t < D.n_own ? owned[t] : halo[t - D.n_own]; };
+        for (uint32_t t = threadIdx.x; t < ne; t += blockDim.x)
+        {
+            const uint32_t g = glob(t);
+            const uint32_t dp[2] = {deps[t] & 0xFFFFu, deps[t] >> 16};
+            float v2[2];
+            for (int e = 0; e < 2; ++e)
+            {
+                const uint32_t o = off[(size_t)e * n + g];
+                v2[e] = val[(size_t)e * n + g];
+                if (dp[e] != kTileNoDep)  // (an entry of a layer-k row may point outside the set: never read)
+                {
+                    const uint32_t j = glob(dp[e]);
+                    if (o != (lower ? g - j : j - g)) atomicExch(bad, 1);
+                }
+            }
+            outv[t] = make_float2(v2[0], v2[1]);
+            outd[t] = dinv[g];
+        }
+    };
+    tri(D.n_el, lhalo, ldeps, loff, lval, ldinv, lv, ld, true);
+    tri(D.n_eu, uhalo, udeps, uoff, uval, udinv, uv, ud, false);
+}
+
+}  // namespace b2s

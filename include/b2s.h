@@ -277,6 +277,8 @@ b2s_status b2s_pc_apply_device(b2s_ctx* ctx, b2s_pc* pc, const double* d_r, doub
  *   "ssor.colour": rp = color_ptr (ncolor+1), ci = new_id (n); v = diag2
  *   "bilu0.L" / "bilu0.U" / "bilu0.inv": block factors (v = nnzb*bs*bs)
  *   "amg.N.A", "amg.N.P": level N operator / prolongation; "amg.N.agg": aggregates in ci
+ *   "pcg.tiles": sizes = {tiles of the tiled persistent PCG kernel (0: none), rows per thread,
+ *                shared memory per CTA}; no arrays
  * Query sizes with NULL arrays: sizes[0] = rows (+1 for rp), sizes[1] = nnz, sizes[2] = values. */
 b2s_status b2s_pc_export(b2s_ctx* ctx, b2s_pc* pc, const char* what, uint64_t* sizes, uint32_t* rp, uint32_t* ci,
                          double* v);
@@ -364,6 +366,9 @@ typedef struct b2s_solve_opts
                          residual has not halved within this many iterations (0: 200,
                          < 0: never); a stalled, broken-down or unconverged learned solve
                          continues with plain FP64 IC(0) from its iterate (b2s_stats.fallbacks) */
+    int persistent;   /* PCG with an FP32 IC(0)-type preconditioner applied by plain Jacobi sweeps:
+                         0 = the whole loop in one launch, over 2-D tiles when they can be planned,
+                         else over row strips; 1 = row strips only; 2 = three launches per iteration */
 } b2s_solve_opts;
 
 void b2s_solve_opts_default(b2s_solve_opts* opts);

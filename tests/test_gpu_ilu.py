@@ -447,3 +447,49 @@ def test_persistent_pcg_stall_guard(b2s, ctx):
     x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=20000, stall_window=1)
     assert st["fallbacks"] == 1 and 0 < st["stalled_at"] < st["iterations"]
     assert st["status"] == 0 and st["relres_true"] < 1e-8
+
+
+@pytest.mark.parametrize("kind,k", [("ic0", 6), ("learned_ic0", 6), ("ic0", 8)])
+def test_tiled_persistent_pcg(b2s, ctx, kind, k):
+    """The benchmark's configuration on 512^2 GRF systems: FP32 IC(0) (plain
+    or learned values, 5 fixed-point sweeps) applied by k Jacobi sweeps per
+    triangle.  The 2-D tiled persistent kernel is planned (one CTA per SM at
+    most) and runs the whole PCG loop in one launch.  Its rows compute what
+    the strip kernel's do, so against it (persistent = 1) and against the
+    three-launch iteration (persistent = 2) the iteration counts agree within
+    2 and the iterates within 1e-6 (only the dots' association differs), and
+    all three meet the FP64-verified tolerance."""
+    n, rp, ci, v = b2s.gen_grf_diffusion(512, 2011, corr=0.05)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(2011, n)
+    M = b2s.Precond(ctx, A, b2s.PC_NAMES[kind], precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=k,
+                    factor_sweeps=5)
+    ntiles, q, smem = M.sizes("pcg.tiles")
+    assert 0 < ntiles <= 148 and 1 <= q <= 4 and smem <= 227 * 1024, (ntiles, q, smem)
+    runs = {}
+    for mode in (b2s.PERSIST_AUTO, b2s.PERSIST_STRIPS, b2s.PERSIST_OFF):
+        l0 = ctx.kernel_launches
+        x, st = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-8, maxit=20000, stall_window=-1, persistent=mode)
+        runs[mode] = (x, st, ctx.kernel_launches - l0)
+        assert st["status"] == 0 and st["relres_true"] < 1e-8, (mode, st)
+    x0, s0, l0 = runs[b2s.PERSIST_AUTO]
+    assert l0 < 20, l0  # the solve's setup launches and one persistent launch
+    for mode in (b2s.PERSIST_STRIPS, b2s.PERSIST_OFF):
+        x1, s1, _ = runs[mode]
+        assert abs(s1["iterations"] - s0["iterations"]) <= 2, (mode, s0["iterations"], s1["iterations"])
+        assert np.linalg.norm(x1 - x0) <= 1e-6 * np.linalg.norm(x1)
+
+
+def test_tiled_pcg_small_grid_and_repeat(b2s, ctx):
+    """A 64^2 grid (tiles of a few dozen rows, one row per thread) and a
+    repeated solve with the same preconditioner: the same iterate bit for
+    bit (the all-reduce sums in tile order) and the FP64 tolerance met."""
+    n, rp, ci, v = b2s.gen_grf_diffusion(64, 2012, corr=0.1)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(2012, n)
+    M = b2s.Precond(ctx, A, b2s.PC_IC0, precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=4)
+    assert M.sizes("pcg.tiles")[0] > 0
+    x1, s1 = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-10, maxit=5000)
+    x2, s2 = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-10, maxit=5000)
+    assert s1["status"] == 0 and s1["relres_true"] < 1e-10
+    assert np.array_equal(x1, x2) and s1["iterations"] == s2["iterations"]

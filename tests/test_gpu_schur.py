@@ -112,7 +112,10 @@ def test_schur_3d_stokes(b2s, ctx, ref, N):
 def test_schur_library_amg_and_graphs(b2s, ctx):
     """The library's own SA-AMG on the pressure Laplacian (no reference rule):
     the known answer holds, and the whole solve replays from CUDA graphs
-    (every part of the composition is device work)."""
+    (every part of the composition is device work).  (The scaled pressure
+    AMG is not always the better Schur approximation at these sizes: 42
+    GMRES steps against the identity's 33 at N = 12; the reference prints
+    both counts and asserts neither.)"""
     K, A, B, Bt, Lp = P.stokes3d(12)
     nv, np_ = A[0], B[0]
     Ad, Bd, Btd = parts(b2s, ctx, A, B, Bt)
@@ -128,10 +131,6 @@ def test_schur_library_amg_and_graphs(b2s, ctx):
     du, dp = known_answer_modulo_pressure_constant(x1, xe, nv)
     assert du < 1e-6 and dp < 1e-6, (du, dp)
     assert np.array_equal(x1, x2) and s1["it"] == s2["it"]
-    # the pressure AMG takes fewer iterations than the identity
-    _, s3 = b2s.solve(ctx, Kd, b, b2s.GMRES, b2s.SchurPrecond(ctx, nv, np_, Bd, Btd, Ag), tol=1e-10, maxit=2000,
-                      restart=100)
-    assert s1["it"] < s3["it"], (s1["it"], s3["it"])
 
 
 def test_schur_shape_errors(b2s, ctx):
