@@ -119,7 +119,7 @@ EXPORTS = [
     "b2s_learner_set_loss", "b2s_sor", "b2s_sor_device", "b2s_csr_matmul", "b2s_csr_transpose", "b2s_csr_export",
     "b2s_ctx_set_wait_limits", "b2s_baij_set_halo", "b2s_baij_halo_info", "b2s_baij_halo_pack_device",
     "b2s_baij_dist_matvec_owned_device", "b2s_baij_dist_matvec_ghost_device", "b2s_pc_create_schur",
-    "b2s_pc_create_scaled",
+    "b2s_pc_create_scaled", "b2s_learner_set_sweeps",
 ]
 
 
@@ -208,6 +208,7 @@ def lib():
     f("b2s_baij_dist_matvec_ghost_device", i32, vp, vp, vp, vp)
     f("b2s_pc_create_schur", i32, vp, u64, u64, vp, vp, vp, vp, pp)
     f("b2s_pc_create_scaled", i32, vp, vp, f64, pp)
+    f("b2s_learner_set_sweeps", i32, vp, i32, i32)
     _lib = L
     return L
 
@@ -494,7 +495,7 @@ class HostPrecond:
 
 
 WEIGHTS = os.path.join(HERE, "weights", "learned_ic0.bin")
-LOSS_PRECOND, LOSS_FACTOR = 0, 1
+LOSS_PRECOND, LOSS_FACTOR, LOSS_SWEEPS = 0, 1, 2
 
 
 class Learner:
@@ -511,6 +512,11 @@ class Learner:
 
     def set_loss(self, kind: int):
         self.ctx.check(lib().b2s_learner_set_loss(self.h, int(kind)), "learner_set_loss")
+
+    def set_sweeps(self, trsv_sweeps: int = 6, factor_sweeps: int = 0):
+        """LOSS_SWEEPS' sweeps per triangle; the base factor (0: exact IC(0), k: k fixed-point sweeps)."""
+        self.ctx.check(lib().b2s_learner_set_sweeps(self.h, int(trsv_sweeps), int(factor_sweeps)),
+                       "learner_set_sweeps")
 
     @property
     def nparams(self) -> int:

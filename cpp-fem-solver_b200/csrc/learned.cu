@@ -30,6 +30,15 @@
 //     whose gradient needs only products with L~ and L~^T:
 //     dloss/dL~_ij = 2 (v_i u_j + w_i q_j) / ||Aw||^2,  u = L~^T w,
 //     v = L~ u - A w,  q = L~^T v.
+//   preconditioned residual through the deployed sweep apply
+//   (B2S_LOSS_SWEEPS): the same loss with M^-1 = F^T F, F = k Jacobi sweeps
+//   of L~ (y_0 = D^-1 r, y_s = D^-1 (r - N y_{s-1}); D, N the diagonal and
+//   strict part of L~) and F^T the k sweeps of L~^T -- the operator the
+//   B2S_TRSV_JACOBI preconditioner applies.  Its gradient runs the adjoint
+//   recursions back through both sweep sequences (every sweep state kept):
+//   with h = D^-1 gbar_s, dL~_ii -= h_i y_s[i], dN_ij -= h_i y_{s-1}[j] and
+//   gbar_{s-1} = -N^T h (lower) or -N h (upper), the upper sweeps' h summed
+//   into the adjoint of their right-hand side.
 // All parameter gradients are reduced in a fixed order (per-CTA partials,
 // then one ordered sum), so training is deterministic.
 #include <cuda_bf16.h>
@@ -665,6 +674,94 @@ __global__ void k_dL_pc(uint32_t n, const uint32_t* __restrict__ Lrp, const uint
         }
 }
 
+// ---- the sweep apply and its adjoint (B2S_LOSS_SWEEPS), FP64
+// L~ rows hold the strict entries in column order, then the diagonal.
+
+// lower sweep: yout_i = (r_i - sum_{j<i} L_ij yin_j) / L_ii (pass 0: yin null)
+__global__ void k_sw_lo(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lci,
+                        const double* __restrict__ Lv, const double* __restrict__ r, const double* __restrict__ yin,
+                        double* __restrict__ yout)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const uint32_t d = Lrp[i + 1] - 1;
+        double t = r[i];
+        if (yin)
+            for (uint32_t q = Lrp[i]; q < d; ++q) t -= Lv[q] * yin[Lci[q]];
+        yout[i] = t / Lv[d];
+    }
+}
+
+// upper sweep over L~^T rows (Trp / Tci / Tpos): zout_i = (u_i - sum_{j>i} L_ji zin_j) / L_ii
+__global__ void k_sw_up(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Trp,
+                        const uint32_t* __restrict__ Tci, const uint32_t* __restrict__ Tpos,
+                        const double* __restrict__ Lv, const double* __restrict__ u, const double* __restrict__ zin,
+                        double* __restrict__ zout)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        double t = u[i];
+        if (zin)
+            for (uint32_t q = Trp[i]; q < Trp[i + 1]; ++q) t -= Lv[Tpos[q]] * zin[Tci[q]];
+        zout[i] = t / Lv[Lrp[i + 1] - 1];
+    }
+}
+
+// adjoint step, diagonal part: h = gbar / L_ii; dL_ii -= h_i state_i; acc += h (when acc is given)
+__global__ void k_sw_h(uint32_t n, const uint32_t* __restrict__ Lrp, const double* __restrict__ Lv,
+                       const double* __restrict__ gbar, const double* __restrict__ state, double* __restrict__ h,
+                       double* __restrict__ acc, double* __restrict__ dL)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const uint32_t d = Lrp[i + 1] - 1;
+        const double hi = gbar[i] / Lv[d];
+        h[i] = hi;
+        if (acc) acc[i] += hi;
+        dL[d] -= hi * state[i];
+    }
+}
+
+// upper adjoint, strict part (rows j of L~): dL_ji -= h_i zprev_j; gnext_j = -sum_{i<j} L_ji h_i
+__global__ void k_sw_up_adj(uint32_t n, const uint32_t* __restrict__ Lrp, const uint32_t* __restrict__ Lci,
+                            const double* __restrict__ Lv, const double* __restrict__ h,
+                            const double* __restrict__ zprev, double* __restrict__ gnext, double* __restrict__ dL)
+{
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        double g = 0.0;
+        const double zj = zprev[j];
+        for (uint32_t q = Lrp[j]; q < Lrp[j + 1] - 1; ++q)
+        {
+            const double hi = h[Lci[q]];
+            g -= Lv[q] * hi;
+            dL[q] -= hi * zj;
+        }
+        gnext[j] = g;
+    }
+}
+
+// lower adjoint, strict part (rows j of L~^T): dL_ij -= h_i yprev_j; gnext_j = -sum_{i>j} L_ij h_i
+__global__ void k_sw_lo_adj(uint32_t n, const uint32_t* __restrict__ Trp, const uint32_t* __restrict__ Tci,
+                            const uint32_t* __restrict__ Tpos, const double* __restrict__ Lv,
+                            const double* __restrict__ h, const double* __restrict__ yprev,
+                            double* __restrict__ gnext, double* __restrict__ dL)
+{
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        double g = 0.0;
+        const double yj = yprev[j];
+        for (uint32_t t = Trp[j]; t < Trp[j + 1]; ++t)
+        {
+            const uint32_t q = Tpos[t];
+            const double hi = h[Tci[t]];
+            g -= Lv[q] * hi;
+            dL[q] -= hi * yj;
+        }
+        gnext[j] = g;
+    }
+}
+
 // diag[i] = L_ii, the last entry of row i of L (columns ascending, j <= i)
 __global__ void k_diag_from_rows(uint32_t n, const uint32_t* __restrict__ Lrp, const double* __restrict__ Lv,
                                  double* __restrict__ diag)
@@ -987,6 +1084,8 @@ struct b2s_learner
     b2s_ctx* ctx = nullptr;
     b2s::Gnn net;
     int loss = B2S_LOSS_PRECOND;
+    int trsv_sweeps = 6;    // B2S_LOSS_SWEEPS: sweeps per triangle
+    int factor_sweeps = 0;  // base factor: 0 exact IC(0), k > 0 k fixed-point sweeps
 };
 
 namespace b2s {
@@ -1083,13 +1182,16 @@ struct TrainBuffers
 };
 
 static void train_step(b2s_ctx* ctx, Gnn& net, const CsrDev& A, int nprobes, uint64_t seed, const double* host_probes,
-                       double lr, bool update, double* loss_out, float* grad_out, int loss_kind)
+                       double lr, bool update, double* loss_out, float* grad_out, int loss_kind, int ksweeps,
+                       int fsweeps)
 {
     need(nprobes > 0 && nprobes <= 64, B2S_INVALID_ARG, "nprobes must be 1..64");
     const uint32_t n = A.n;
-    // base IC(0) factor (FP64), its L^T structure
+    // base IC(0) factor (FP64; exact, or fsweeps fixed-point sweeps as deployed), its L^T structure
     b2s_pc_opts o;
     b2s_pc_opts_default(&o);
+    o.factor_sweeps = fsweeps;
+    if (fsweeps > 0) o.trsv = B2S_TRSV_JACOBI;  // the fixed-point factor comes with the sweep schedule
     auto base = make_pc_ic0(ctx, A, o);
     uint64_t sz[3];
     base->export_data(ctx, "ic0.L", sz, nullptr, nullptr, nullptr);
@@ -1136,6 +1238,22 @@ static void train_step(b2s_ctx* ctx, Gnn& net, const CsrDev& A, int nprobes, uin
         ya.alloc(n);
         yb.alloc(n);
     }
+    // sweep loss: the k + 1 states of each sweep sequence and the adjoint work vectors
+    std::vector<DBuf<double>> ys, zs;
+    DBuf<double> hb, gb, gb2, ub;
+    if (loss_kind == B2S_LOSS_SWEEPS)
+    {
+        need(ksweeps >= 0 && ksweeps <= 64, B2S_INVALID_ARG, "sweep loss: 0..64 sweeps");
+        for (int s = 0; s <= ksweeps; ++s)
+        {
+            ys.emplace_back(n);
+            zs.emplace_back(n);
+        }
+        hb.alloc(n);
+        gb.alloc(n);
+        gb2.alloc(n);
+        ub.alloc(n);
+    }
     B2S_CUDA(cudaMemsetAsync(T.scal.p, 0, T.scal.bytes(), ctx->stream));
     const unsigned gn = stream_grid(ctx, n);
     reserve_reduction(ctx, gn);
@@ -1154,6 +1272,41 @@ static void train_step(b2s_ctx* ctx, Gnn& net, const CsrDev& A, int nprobes, uin
                 }
         }
         spmv(ctx, A, T.w.p, T.Aw.p);
+        if (loss_kind == B2S_LOSS_SWEEPS)
+        {
+            const int K = ksweeps;
+            // y = F Aw (k sweeps of L~), z = F^T y (k sweeps of L~^T), e = w - z
+            for (int s = 0; s <= K; ++s)
+                B2S_LAUNCH(ctx, k_sw_lo, gn, kThreads, 0, n, Lrp.p, Lci.p, Lv.p, T.Aw.p,
+                           s ? ys[s - 1].p : (const double*)nullptr, ys[s].p);
+            for (int s = 0; s <= K; ++s)
+                B2S_LAUNCH(ctx, k_sw_up, gn, kThreads, 0, n, Lrp.p, Trp.p, Tci.p, Tpos.p, Lv.p, ys[K].p,
+                           s ? zs[s - 1].p : (const double*)nullptr, zs[s].p);
+            B2S_LAUNCH(ctx, k_sub, gn, kThreads, 0, n, T.w.p, zs[K].p, T.vres.p);
+            dot_dev(ctx, n, T.vres.p, T.vres.p, T.scal.p);
+            dot_dev(ctx, n, T.w.p, T.w.p, T.scal.p + 1);
+            B2S_LAUNCH(ctx, k_loss_scale, 1, 1, 0, T.scal.p, T.scal.p + 1, nprobes, T.scal.p + 2, T.scal.p + 3);
+            // adjoint of z_K: g = -scale e; back through the upper sweeps (ub collects the rhs adjoint)
+            B2S_LAUNCH(ctx, k_neg_scale, gn, kThreads, 0, n, T.vres.p, T.scal.p + 2, gb.p);
+            B2S_CUDA(cudaMemsetAsync(ub.p, 0, ub.bytes(), ctx->stream));
+            for (int s = K; s >= 0; --s)
+            {
+                B2S_LAUNCH(ctx, k_sw_h, gn, kThreads, 0, n, Lrp.p, Lv.p, gb.p, zs[s].p, hb.p, ub.p, dL.p);
+                if (s == 0) break;
+                B2S_LAUNCH(ctx, k_sw_up_adj, gn, kThreads, 0, n, Lrp.p, Lci.p, Lv.p, hb.p, zs[s - 1].p, gb2.p, dL.p);
+                std::swap(gb, gb2);
+            }
+            // back through the lower sweeps from y_K's adjoint ub (Aw is a constant)
+            for (int s = K; s >= 0; --s)
+            {
+                B2S_LAUNCH(ctx, k_sw_h, gn, kThreads, 0, n, Lrp.p, Lv.p, ub.p, ys[s].p, hb.p, (double*)nullptr, dL.p);
+                if (s == 0) break;
+                B2S_LAUNCH(ctx, k_sw_lo_adj, gn, kThreads, 0, n, Trp.p, Tci.p, Tpos.p, Lv.p, hb.p, ys[s - 1].p,
+                           gb2.p, dL.p);
+                std::swap(ub, gb2);
+            }
+            continue;
+        }
         if (loss_kind == B2S_LOSS_PRECOND)
         {
             // y = L~^-1 Aw (u), z = L~^-T y (qv), e = w - z (vres)
@@ -1303,15 +1456,26 @@ b2s_status b2s_learner_step(b2s_ctx* ctx, b2s_learner* L, const b2s_csr* A, int 
     if (!ctx || !L || !A) return B2S_INVALID_ARG;
     return guarded(ctx, [&] {
         need(A->d.n == A->d.m, B2S_SHAPE, "learned IC(0) needs a square matrix");
-        train_step(ctx, L->net, A->d, nprobes, seed, probes, lr, update != 0, loss, grad, L->loss);
+        train_step(ctx, L->net, A->d, nprobes, seed, probes, lr, update != 0, loss, grad, L->loss, L->trsv_sweeps,
+                   L->factor_sweeps);
         check_device_error(ctx, "a triangular-solve wait gave up during the training step");
     });
 }
 
 b2s_status b2s_learner_set_loss(b2s_learner* L, int kind)
 {
-    if (!L || (kind != B2S_LOSS_PRECOND && kind != B2S_LOSS_FACTOR)) return B2S_INVALID_ARG;
+    if (!L || (kind != B2S_LOSS_PRECOND && kind != B2S_LOSS_FACTOR && kind != B2S_LOSS_SWEEPS))
+        return B2S_INVALID_ARG;
     L->loss = kind;
+    return B2S_OK;
+}
+
+b2s_status b2s_learner_set_sweeps(b2s_learner* L, int trsv_sweeps, int factor_sweeps)
+{
+    if (!L || trsv_sweeps < 0 || trsv_sweeps > 64 || factor_sweeps < 0 || factor_sweeps > 1024)
+        return B2S_INVALID_ARG;
+    L->trsv_sweeps = trsv_sweeps;
+    L->factor_sweeps = factor_sweeps;
     return B2S_OK;
 }
 

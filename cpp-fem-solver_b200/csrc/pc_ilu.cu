@@ -28,6 +28,8 @@
 #include "pcg_band.cuh"
 #include "pcg_tile.cuh"
 
+#include <cstdlib>
+#include <cstring>
 #include <exception>
 #include <thread>
 
@@ -663,6 +665,8 @@ struct HostAnalysis
     ChunkPlan lo_plan, up_plan;
     BandPlan lo_band, up_band;
     TilePlan tiles;  // the tiled persistent PCG kernel's plan (sweep schedule, FP32)
+    bool tiles_grid5 = false;        // a 5-point grid: the index blobs are built on the device
+    std::vector<TileGeom> tile_geom;
     bool chunked = false;
     std::exception_ptr error;
     std::thread th;
@@ -776,20 +780,37 @@ struct PcIC0 final : PcImpl
     DBuf<uint8_t> tile_idx, tile_vals;
     DBuf<unsigned long long> tile_slots;
 
-    // uploads the plan and packs the value blobs from A and the band arrays
-    void load_tiles(b2s_ctx* ctx, const CsrDev& A, const TilePlan& P)
+    // uploads the plan (a 5-point grid's index blobs are built on the device)
+    // and packs the value blobs from A and the band arrays
+    void load_tiles(b2s_ctx* ctx, const CsrDev& A, const TilePlan& P, const std::vector<TileGeom>* grid5)
     {
         tiles_ready = false;
         if (!P.ok || A.n != n) return;
         tile_desc = upload(ctx, P.desc);
-        tile_idx = upload(ctx, P.idx.data(), P.idx.size());
+        DBuf<int> bad(1);
+        DBuf<TileGeom> geom;  // (held until the set-up's sync)
+        B2S_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream));
+        if (grid5)
+        {
+            const uint32_t B = P.B, ny = n / P.B;
+            uint32_t scratch = 0;
+            for (const TileGeom& g : *grid5) scratch = std::max(scratch, grid5_scratch(g, B, ny, (int)P.k));
+            tile_idx.alloc(P.ibytes ? P.ibytes : 16);
+            geom = upload(ctx, *grid5);
+            const size_t smem = 2ull * scratch * sizeof(uint16_t);
+            if (smem > 48 * 1024)
+                B2S_CUDA(cudaFuncSetAttribute(k_tile_build_grid5, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem));
+            B2S_LAUNCH(ctx, k_tile_build_grid5, P.ntiles, 32, smem, tile_desc.p, geom.p, tile_idx.p, B, ny, (int)P.k,
+                       scratch, bad.p);
+        }
+        else
+            tile_idx = upload(ctx, P.idx.data(), P.idx.size());
         tile_vals.alloc(P.vbytes ? P.vbytes : 16);
         tile_slots.alloc(6ull * P.ntiles);
-        DBuf<int> bad(1);
-        B2S_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), ctx->stream));
-        B2S_LAUNCH(ctx, k_tile_pack, P.ntiles, kThreads, 0, tile_desc.p, tile_idx.p, tile_vals.p, n, A.rp.p, A.ci.p,
-                   A.v.p, fwd.band_off.p, fwd.band_val.p, fwd.band_dinv.p, bwd.band_off.p, bwd.band_val.p,
-                   bwd.band_dinv.p, bad.p);
+        B2S_LAUNCH(ctx, k_tile_pack, P.ntiles, kThreads, 0, tile_desc.p, tile_idx.p, tile_vals.p, n, (int)P.k,
+                   A.rp.p, A.ci.p, A.v.p, fwd.band_off.p, fwd.band_val.p, fwd.band_dinv.p, bwd.band_off.p,
+                   bwd.band_val.p, bwd.band_dinv.p, bad.p);
         int hb = 0;
         d2h(ctx, &hb, bad.p, sizeof(int));
         sync(ctx);
@@ -975,6 +996,15 @@ struct PcIC0 final : PcImpl
             sizes[2] = tiles_ready ? tile_smem : 0;
             return;
         }
+        if (what == "pcg.tiles.idx")  // the tiles' index blobs as 32-bit words (ci)
+        {
+            sizes[0] = 0;
+            sizes[1] = tiles_ready ? tile_idx.n / 4 : 0;
+            sizes[2] = 0;
+            if (ci && sizes[1]) d2h(ctx, ci, tile_idx.p, sizes[1] * 4);
+            sync(ctx);
+            return;
+        }
         PcImpl::export_data(ctx, what, sizes, rp, ci, v);
     }
 };
@@ -1092,15 +1122,27 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
                         else
                             ha.up_band = plan_band_transposed(n, hrp.data(), hci.data(), nsweeps, sm_count, seg);
                     });
-                // the tiled persistent PCG kernel: plain Jacobi, two strict entries per row
+                // the tiled persistent PCG kernel: plain Jacobi, two strict entries per row.
+                // A 5-point grid is laid out from closed forms (its blobs are built on the
+                // device); other patterns take the breadth-first planner while it is cheap.
                 if (fp32 && seg == 1 && ha.lo_band.T && ha.up_band.T && ha.lo_band.W == 2 && ha.up_band.W == 2 &&
                     nsweeps <= kTileMaxSweeps)
                 {
-                    std::vector<uint32_t> lrp, lci, urp, uci;
-                    strict_lower(n, hrp.data(), hci.data(), lrp, lci);
-                    strict_transpose(n, hrp.data(), hci.data(), true, urp, uci);
-                    ha.tiles = plan_tiles(n, lrp.data(), lci.data(), urp.data(), uci.data(), nsweeps, sm_count,
-                                          tile_smem, 8);
+                    const char* planner = std::getenv("B2S_TILE_PLANNER");  // "bfs": the general planner
+                    const bool bfs = planner && std::strcmp(planner, "bfs") == 0;
+                    if (!bfs && is_grid5(n, hrp.data(), hci.data(), ha.lo_band.B, true))
+                    {
+                        ha.tiles = plan_tiles_grid5(n, ha.lo_band.B, nsweeps, sm_count, tile_smem, ha.tile_geom);
+                        ha.tiles_grid5 = true;
+                    }
+                    else if (n <= kTilePlanHostMaxRows)
+                    {
+                        std::vector<uint32_t> lrp, lci, urp, uci;
+                        strict_lower(n, hrp.data(), hci.data(), lrp, lci);
+                        strict_transpose(n, hrp.data(), hci.data(), true, urp, uci);
+                        ha.tiles = plan_tiles(n, lrp.data(), lci.data(), urp.data(), uci.data(), nsweeps, sm_count,
+                                              tile_smem, 8);
+                    }
                 }
                 return;
             }
@@ -1165,7 +1207,8 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     {
         pc->fwd.pack<float>(ctx, pc->L.v32.p, pc->diag32.p);
         pc->bwd.pack<float>(ctx, pc->LT.v32.p, pc->diag32.p);
-        if (sweeps && ha.tiles.ok && pc->fwd.band.T && pc->bwd.band.T) pc->load_tiles(ctx, A, ha.tiles);
+        if (sweeps && ha.tiles.ok && pc->fwd.band.T && pc->bwd.band.T)
+            pc->load_tiles(ctx, A, ha.tiles, ha.tiles_grid5 ? &ha.tile_geom : nullptr);
     }
     else
     {

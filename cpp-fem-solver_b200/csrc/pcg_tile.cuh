@@ -22,12 +22,13 @@
 // tiles are other row sets).
 //
 // A phase ends with an all-reduce that is also the grid barrier: thread 0
-// publishes the tile's partial as two 64-bit words {epoch, 32 value bits}
-// with release stores, and warp 0 of every CTA polls all tiles' words with
-// acquire loads (every lane its tiles at once) until they carry the phase's
-// epoch, then sums them in tile order -- one L2 round trip where a barrier
-// and a separate read of the partials took two.  Every CTA gets the same bits
-// and takes the same scalar step.  Each wait is bounded (kGridBarrierPolls
+// fences (gpu scope, after the CTA's barrier) and publishes the tile's
+// partial as two 64-bit words {epoch, 32 value bits}; warp 0 of every CTA
+// polls all tiles' words with relaxed loads, every lane its tiles at once,
+// until they carry the phase's epoch, then fences and sums them in tile order
+// -- one L2 round trip per poll where a barrier and a separate read of the
+// partials took two (acquire loads would serialise a lane's ten loads).
+// Every CTA gets the same bits and takes the same scalar step.  Each wait is bounded (kGridBarrierPolls
 // polls); a CTA that gives up records B2S_TIMEOUT and leaves, and the others
 // give up at their next all-reduce, so the launch always ends.
 #pragma once
@@ -58,17 +59,19 @@ struct PcgTileArgs
     int stall_window;
 };
 
-__device__ __forceinline__ void st_release_gpu_u64(unsigned long long* p, unsigned long long v)
+__device__ __forceinline__ void st_relaxed_gpu_u64(unsigned long long* p, unsigned long long v)
 {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-__device__ __forceinline__ unsigned long long ld_acquire_gpu_u64(const unsigned long long* p)
+__device__ __forceinline__ unsigned long long ld_relaxed_gpu_u64(const unsigned long long* p)
 {
     unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
+
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 // Thread 0 holds this tile's partial `part`.  Publishes it for `epoch`, waits
 // for every tile's, and leaves their sum (tile order; the same bits in every
@@ -78,10 +81,13 @@ __device__ __forceinline__ bool tile_allreduce(unsigned long long* slots, uint32
 {
     if (threadIdx.x == 0)
     {
+        // the CTA's writes (ordered before this thread by the barrier inside
+        // block_reduce) become visible before the words that announce them
+        fence_acq_rel_gpu();
         const unsigned long long e = (unsigned long long)epoch << 32;
         const unsigned long long b = (unsigned long long)__double_as_longlong(part);
-        st_release_gpu_u64(&slots[2 * tile], e | (b & 0xffffffffull));
-        st_release_gpu_u64(&slots[2 * tile + 1], e | (b >> 32));
+        st_relaxed_gpu_u64(&slots[2 * tile], e | (b & 0xffffffffull));
+        st_relaxed_gpu_u64(&slots[2 * tile + 1], e | (b >> 32));
     }
     if (threadIdx.x < 32)
     {
@@ -98,8 +104,8 @@ __device__ __forceinline__ bool tile_allreduce(unsigned long long* slots, uint32
                 v[j] = 0.0;
                 if (b < ntiles)
                 {
-                    const unsigned long long w0 = ld_acquire_gpu_u64(&slots[2 * b]);
-                    const unsigned long long w1 = ld_acquire_gpu_u64(&slots[2 * b + 1]);
+                    const unsigned long long w0 = ld_relaxed_gpu_u64(&slots[2 * b]);
+                    const unsigned long long w1 = ld_relaxed_gpu_u64(&slots[2 * b + 1]);
                     all &= (uint32_t)(w0 >> 32) == epoch && (uint32_t)(w1 >> 32) == epoch;
                     v[j] = __longlong_as_double((long long)(((w1 & 0xffffffffull) << 32) | (w0 & 0xffffffffull)));
                 }
@@ -110,6 +116,9 @@ __device__ __forceinline__ bool tile_allreduce(unsigned long long* slots, uint32
                 break;
             }
         }
+        // the words seen carry the other CTAs' fenced writes: this fence
+        // (then the block barrier below) orders the CTA's later reads after them
+        fence_acq_rel_gpu();
         double t = 0.0;
 #pragma unroll
         for (uint32_t j = 0; j < kTileMaxTilesPerLane; ++j)
@@ -354,13 +363,30 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
     if (tile == 0 && tid == 0) *a.st = sst;
 }
 
+// Builds the index blobs of a 5-point grid's tiles (tile_plan.hpp,
+// grid5_build_part): block t, threads 0..2 the three parts of tile t, the
+// lower and upper parts each with its box map in shared memory (scratch
+// entries).  *bad = 1 when a count disagrees with the descriptors.
+__global__ void k_tile_build_grid5(const TileDesc* __restrict__ desc, const TileGeom* __restrict__ geom,
+                                   uint8_t* __restrict__ idx, uint32_t B, uint32_t ny, int k, uint32_t scratch,
+                                   int* bad)
+{
+    extern __shared__ uint16_t loc[];  // 2 x scratch
+    const uint32_t t = blockIdx.x;
+    const int part = (int)threadIdx.x;
+    if (part >= 3) return;
+    const TileDesc D = desc[t];
+    const TileGeom G = geom[t];
+    if (!grid5_build_part(D, G, B, ny, k, part, idx + D.ibase, loc + (part == 1 ? scratch : 0u))) atomicExch(bad, 1);
+}
+
 // Fills the value blobs after factorisation: A's values for the owned rows
 // (checking that A's row holds exactly the planned columns), the triangles'
 // strict entries and reciprocals from the banded sweep arrays (slot e of row
 // g at e*n + g, checking the planned dependency's offset).  *bad = 1 when A's
 // pattern or the factor's differs from the plan.
 __global__ void k_tile_pack(const TileDesc* __restrict__ desc, const uint8_t* __restrict__ idx,
-                            uint8_t* __restrict__ vals, uint32_t n, const uint32_t* __restrict__ Arp,
+                            uint8_t* __restrict__ vals, uint32_t n, int k, const uint32_t* __restrict__ Arp,
                             const uint32_t* __restrict__ Aci, const double* __restrict__ Av,
                             const uint16_t* __restrict__ loff, const float* __restrict__ lval,
                             const float* __restrict__ ldinv, const uint16_t* __restrict__ uoff,
@@ -398,9 +424,11 @@ __global__ void k_tile_pack(const TileDesc* __restrict__ desc, const uint8_t* __
             aval[e0 + e] = Av[a0 + e];
         }
     }
-    // one triangle's extended rows: values and reciprocal from the band slots
-    auto tri = [&](uint32_t ne, const uint32_t* halo, const uint32_t* deps, const uint16_t* off, const float* val,
-                   const float* dinv, float2* outv, float* outd, bool lower) {
+    // one triangle's extended rows: values and reciprocal from the band slots;
+    // rows of layers below k (computed by the sweeps) must have every factor
+    // entry planned (a missing entry shows as a planned "none" over a band slot)
+    auto tri = [&](uint32_t ne, uint32_t below_k, const uint32_t* halo, const uint32_t* deps, const uint16_t* off,
+                   const float* val, const float* dinv, float2* outv, float* outd, bool lower) {
         auto glob = [&](uint32_t t) { return t < D.n_own ? owned[t] : halo[t - D.n_own]; };
         for (uint32_t t = threadIdx.x; t < ne; t += blockDim.x)
         {
@@ -416,13 +444,15 @@ __global__ void k_tile_pack(const TileDesc* __restrict__ desc, const uint8_t* __
                     const uint32_t j = glob(dp[e]);
                     if (o != (lower ? g - j : j - g)) atomicExch(bad, 1);
                 }
+                else if (o != 0 && t < below_k)
+                    atomicExch(bad, 1);
             }
             outv[t] = make_float2(v2[0], v2[1]);
             outd[t] = dinv[g];
         }
     };
-    tri(D.n_el, lhalo, ldeps, loff, lval, ldinv, lv, ld, true);
-    tri(D.n_eu, uhalo, udeps, uoff, uval, udinv, uv, ud, false);
+    tri(D.n_el, k > 0 ? D.lcnt[k - 1] : 0u, lhalo, ldeps, loff, lval, ldinv, lv, ld, true);
+    tri(D.n_eu, k > 0 ? D.ucnt[k - 1] : 0u, uhalo, udeps, uoff, uval, udinv, uv, ud, false);
 }
 
 }  // namespace b2s

@@ -36,6 +36,12 @@
 
 #include "trsv_plan.hpp"
 
+#ifdef __CUDACC__
+#define B2S_TILE_HD __host__ __device__
+#else
+#define B2S_TILE_HD
+#endif
+
 namespace b2s {
 
 constexpr int kTileMaxSweeps = 16;
@@ -43,6 +49,9 @@ constexpr uint32_t kTileThreads = 768;
 constexpr uint32_t kTileMaxQ = 4;  // extended rows per thread
 constexpr uint32_t kTileNoDep = 0xFFFFu;
 constexpr int kTileMaxTiles = 160;  // the kernel's all-reduce: 5 tiles per lane of one warp
+// the breadth-first planner runs on the host at set-up; above this many rows it
+// would cost more than it saves, and only 5-point grids (closed forms) are tiled
+constexpr uint32_t kTilePlanHostMaxRows = 1u << 16;
 
 struct TileDesc
 {
@@ -362,6 +371,290 @@ inline TilePlan plan_tiles_shape(uint32_t n, const uint32_t* lo_rp, const uint32
     P.ibytes = ibase;
     P.ok = true;
     return P;
+}
+
+// ------------------------------------------------------------------ 5-point grids
+//
+// A pattern whose strict lower entries are exactly, in column order,
+// {i - B if y > 0, i - 1 if x > 0} for x = i mod B, y = i div B, n = B * ny
+// (the natural-order 5-point stencil) has closed-form tile sets: for the
+// block [x0, x1) x [y0, y1) and k sweeps, the lower set holds the points of
+// the box [x0 - k, x1) x [y0 - k, y1) at distance dL = max(0, x0 - x) +
+// max(0, y0 - y) <= k, layer dL; the upper set mirrors it; the SpMV's columns
+// are the block and its one-wide ring.  plan_tiles_grid5 lays the blobs out
+// from these counts alone (no pass over the matrix), and grid5_build_part
+// writes a tile's index blob -- on the device at set-up, one thread per part
+// of a tile, and on the CPU in the tests, where it must equal plan_tiles'
+// output byte for byte.
+
+struct TileGeom
+{
+    uint32_t x0, x1, y0, y1;  // the block
+};
+
+// the pattern check (rp / ci: L with or without its diagonal last)
+inline bool is_grid5(uint32_t n, const uint32_t* rp, const uint32_t* ci, uint32_t B, bool diag_last)
+{
+    if (B == 0 || n % B) return false;
+    for (uint32_t i = 0; i < n; ++i)
+    {
+        const uint32_t x = i % B, y = i / B;
+        uint32_t e = rp[i];
+        const uint32_t e1 = rp[i + 1] - (diag_last ? 1u : 0u);
+        if (diag_last && (rp[i + 1] == rp[i] || ci[rp[i + 1] - 1] != i)) return false;
+        if (y > 0 && (e >= e1 || ci[e++] != i - B)) return false;
+        if (x > 0 && (e >= e1 || ci[e++] != i - 1)) return false;
+        if (e != e1) return false;
+    }
+    return true;
+}
+
+// points at distance d >= 1 from a block side: rows/columns clipped at ka / kb
+B2S_TILE_HD inline uint32_t grid5_layer(uint32_t d, uint32_t w, uint32_t h, uint32_t ka, uint32_t kb)
+{
+    uint32_t c = (d <= ka ? h : 0) + (d <= kb ? w : 0);
+    for (uint32_t a = 1; a <= ka && a < d; ++a)
+        if (d - a <= kb) ++c;
+    return c;
+}
+
+inline TilePlan plan_tiles_grid5(uint32_t n, uint32_t B, int k, int sm_count, uint32_t smem_limit,
+                                 std::vector<TileGeom>& geom)
+{
+    TilePlan P;
+    P.n = n;
+    P.k = (uint32_t)k;
+    if (!n || !B || n % B || k < 1 || k > kTileMaxSweeps || sm_count < 1) return P;
+    sm_count = std::min(sm_count, kTileMaxTiles);
+    const uint64_t ny = n / B;
+    uint64_t best = ~0ull, bx = 1, by = 1;
+    for (uint64_t tx = 1; tx <= std::min<uint64_t>(B, (uint64_t)sm_count); ++tx)
+    {
+        const uint64_t ty = std::min<uint64_t>((uint64_t)sm_count / tx, ny);
+        if (!ty) continue;
+        const uint64_t w = (B + tx - 1) / tx, h = (ny + ty - 1) / ty;
+        const uint64_t est = tx == 1 ? w * h + (uint64_t)k * B : (w + (uint64_t)k) * (h + (uint64_t)k);
+        if (est < best)
+        {
+            best = est;
+            bx = tx;
+            by = ty;
+        }
+    }
+    const uint64_t w = (B + bx - 1) / bx, h = (ny + by - 1) / by;
+    const uint32_t tiles_x = (uint32_t)((B + w - 1) / w), tiles_y = (uint32_t)((ny + h - 1) / h);
+    const uint32_t ntiles = tiles_x * tiles_y;
+    P.desc.resize(ntiles);
+    geom.resize(ntiles);
+    uint64_t vbase = 0, ibase = 0;
+    uint32_t max_pair = 0;
+    for (uint32_t t = 0; t < ntiles; ++t)
+    {
+        TileGeom& G = geom[t];
+        G.x0 = (uint32_t)((t % tiles_x) * w);
+        G.x1 = (uint32_t)std::min<uint64_t>(B, G.x0 + w);
+        G.y0 = (uint32_t)((t / tiles_x) * h);
+        G.y1 = (uint32_t)std::min<uint64_t>(ny, G.y0 + h);
+        const uint32_t tw = G.x1 - G.x0, th = G.y1 - G.y0, K = (uint32_t)k;
+        TileDesc& D = P.desc[t];
+        std::memset(&D, 0, sizeof(D));
+        D.n_own = tw * th;
+        // lower set: clipped at the grid's left / bottom edges
+        const uint32_t lka = std::min(K, G.x0), lkb = std::min(K, G.y0);
+        const uint32_t uka = std::min<uint32_t>(K, B - G.x1), ukb = std::min<uint32_t>(K, (uint32_t)ny - G.y1);
+        uint32_t cl = D.n_own, cu = D.n_own;
+        D.lcnt[0] = D.ucnt[0] = (uint16_t)D.n_own;
+        for (uint32_t d = 1; d <= K; ++d)
+        {
+            cl += grid5_layer(d, tw, th, lka, lkb);
+            cu += grid5_layer(d, tw, th, uka, ukb);
+            if (cl >= kTileNoDep || cu >= kTileNoDep) return P;
+            D.lcnt[d] = (uint16_t)cl;
+            D.ucnt[d] = (uint16_t)cu;
+        }
+        D.n_el = cl;
+        D.n_eu = cu;
+        D.n_ae = D.n_own + (G.x0 > 0 ? th : 0) + (G.x1 < B ? th : 0) + (G.y0 > 0 ? tw : 0) + (G.y1 < ny ? tw : 0);
+        D.nnz = D.n_own + th * (tw - (G.x0 == 0)) + th * (tw - (G.x1 == B)) + tw * (th - (G.y0 == 0)) +
+                tw * (th - (G.y1 == ny));
+        if (D.n_el > kTileThreads * kTileMaxQ || D.n_eu > kTileThreads * kTileMaxQ || D.n_ae >= kTileNoDep) return P;
+        uint32_t o = 0;
+        auto seg = [&o](uint64_t bytes) {
+            const uint32_t at = o;
+            o += tile_align16(bytes);
+            return at;
+        };
+        D.o_aval = seg(8ull * D.nnz);
+        D.o_lvals = seg(8ull * D.n_el);
+        D.o_uvals = seg(8ull * D.n_eu);
+        D.o_ldinv = seg(4ull * D.n_el);
+        D.o_udinv = seg(4ull * D.n_eu);
+        D.vbytes = o;
+        o = 0;
+        D.o_owned = seg(4ull * D.n_own);
+        D.o_lhalo = seg(4ull * (D.n_el - D.n_own));
+        D.o_ldeps = seg(4ull * D.n_el);
+        D.o_uhalo = seg(4ull * (D.n_eu - D.n_own));
+        D.o_udeps = seg(4ull * D.n_eu);
+        D.o_ahalo = seg(4ull * (D.n_ae - D.n_own));
+        D.o_arp = seg(4ull * (D.n_own + 1));
+        D.o_acol = seg(2ull * D.nnz);
+        D.ibytes = o;
+        D.vbase = vbase;
+        D.ibase = ibase;
+        vbase += D.vbytes;
+        ibase += D.ibytes;
+        max_pair = std::max(max_pair, D.vbytes + D.ibytes);
+        P.max_ext = std::max(P.max_ext, std::max(D.n_el, D.n_eu));
+        P.max_own = std::max(P.max_own, D.n_own);
+        P.max_ae = std::max(P.max_ae, D.n_ae);
+    }
+    P.work = max_pair;
+    P.smem = max_pair + tile_work_bytes(P.max_ext, P.max_ae);
+    P.Q = (P.max_ext + kTileThreads - 1) / kTileThreads;
+    if (P.smem > smem_limit || P.Q > kTileMaxQ) return P;
+    P.ntiles = ntiles;
+    P.tiles_x = tiles_x;
+    P.tiles_y = tiles_y;
+    P.B = B;
+    P.vbytes = vbase;
+    P.ibytes = ibase;
+    P.ok = true;
+    return P;
+}
+
+// Scratch (u16 entries) one part of one tile needs: a box of the set's points.
+inline uint32_t grid5_scratch(const TileGeom& G, uint32_t B, uint32_t ny, int k)
+{
+    const uint32_t K = (uint32_t)k;
+    const uint32_t lw = G.x1 - (G.x0 > K ? G.x0 - K : 0), lh = G.y1 - (G.y0 > K ? G.y0 - K : 0);
+    const uint32_t uw = std::min(B, G.x1 + K) - G.x0, uh = std::min(ny, G.y1 + K) - G.y0;
+    return std::max(lw * lh, uw * uh);
+}
+
+// Writes part `part` of a tile's index blob: 0 = owned rows and the lower
+// set (halo, dependencies), 1 = the upper set, 2 = the SpMV's ring, offsets
+// and columns.  The parts read nothing another part writes, so they can run
+// side by side.  loc: scratch of grid5_scratch entries.  Returns false when
+// a count disagrees with the descriptor (nothing is written past it).
+B2S_TILE_HD inline bool grid5_build_part(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, int k, int part,
+                                    uint8_t* ib, uint16_t* loc)
+{
+    const uint32_t K = (uint32_t)k, tw = G.x1 - G.x0, th = G.y1 - G.y0;
+    uint32_t* owned = reinterpret_cast<uint32_t*>(ib + D.o_owned);
+    auto own_local = [&](uint32_t x, uint32_t y) { return (y - G.y0) * tw + (x - G.x0); };
+    if (part == 0 || part == 1)
+    {
+        const bool lo = part == 0;
+        if (lo)
+            for (uint32_t y = G.y0, q = 0; y < G.y1; ++y)
+                for (uint32_t x = G.x0; x < G.x1; ++x) owned[q++] = y * B + x;
+        const uint32_t ne = lo ? D.n_el : D.n_eu;
+        const uint16_t* cnt = lo ? D.lcnt : D.ucnt;
+        uint32_t* halo = reinterpret_cast<uint32_t*>(ib + (lo ? D.o_lhalo : D.o_uhalo));
+        uint32_t* deps = reinterpret_cast<uint32_t*>(ib + (lo ? D.o_ldeps : D.o_udeps));
+        // the box of the set, row-major (= ascending global index)
+        const uint32_t bx0 = lo ? (G.x0 > K ? G.x0 - K : 0) : G.x0, by0 = lo ? (G.y0 > K ? G.y0 - K : 0) : G.y0;
+        const uint32_t bx1 = lo ? G.x1 : (B < G.x1 + K ? B : G.x1 + K);
+        const uint32_t by1 = lo ? G.y1 : (ny < G.y1 + K ? ny : G.y1 + K);
+        const uint32_t bw = bx1 - bx0;  // (the box holds (by1 - by0) * bw entries: grid5_scratch)
+        uint32_t next[kTileMaxSweeps + 1];
+        for (uint32_t d = 1; d <= K; ++d) next[d] = cnt[d - 1];
+        for (uint32_t y = by0, q = 0; y < by1; ++y)
+        {
+            const uint32_t db = lo ? (y < G.y0 ? G.y0 - y : 0) : (y >= G.y1 ? y - G.y1 + 1 : 0);
+            for (uint32_t x = bx0; x < bx1; ++x, ++q)
+            {
+                const uint32_t da = lo ? (x < G.x0 ? G.x0 - x : 0) : (x >= G.x1 ? x - G.x1 + 1 : 0);
+                const uint32_t d = da + db;
+                uint32_t l = kTileNoDep;
+                if (d == 0)
+                    l = own_local(x, y);
+                else if (d <= K)
+                {
+                    l = next[d]++;
+                    if (l >= cnt[d]) return false;
+                    halo[l - D.n_own] = y * B + x;
+                }
+                loc[q] = (uint16_t)l;
+            }
+        }
+        for (uint32_t d = 1; d <= K; ++d)
+            if (next[d] != cnt[d]) return false;
+        // dependencies in column order: lower (x, y-1) then (x-1, y); upper (x+1, y) then (x, y+1)
+        auto at = [&](uint32_t x, uint32_t y) -> uint32_t {
+            if (x < bx0 || x >= bx1 || y < by0 || y >= by1) return kTileNoDep;
+            return loc[(y - by0) * bw + (x - bx0)];
+        };
+        for (uint32_t t = 0; t < ne; ++t)
+        {
+            uint32_t x, y;
+            if (t < D.n_own)
+            {
+                x = G.x0 + t % tw;
+                y = G.y0 + t / tw;
+            }
+            else
+            {
+                const uint32_t g = halo[t - D.n_own];  // written by this part above
+                x = g % B;
+                y = g / B;
+            }
+            uint32_t s[2] = {kTileNoDep, kTileNoDep}, e = 0;
+            if (lo)
+            {
+                if (y > 0) s[e++] = at(x, y - 1);
+                if (x > 0) s[e++] = at(x - 1, y);
+            }
+            else
+            {
+                if (x + 1 < B) s[e++] = at(x + 1, y);
+                if (y + 1 < ny) s[e++] = at(x, y + 1);
+            }
+            deps[t] = s[0] | (s[1] << 16);
+        }
+        return true;
+    }
+    // part 2: the SpMV's columns -- ring order by global index: the row below
+    // the block, then left / right of each block row, then the row above
+    uint32_t* ahalo = reinterpret_cast<uint32_t*>(ib + D.o_ahalo);
+    uint32_t* arp = reinterpret_cast<uint32_t*>(ib + D.o_arp);
+    uint16_t* acol = reinterpret_cast<uint16_t*>(ib + D.o_acol);
+    const bool L = G.x0 > 0, R = G.x1 < B, Bo = G.y0 > 0, T = G.y1 < ny;
+    const uint32_t nb = Bo ? tw : 0, per_row = (L ? 1u : 0u) + (R ? 1u : 0u);
+    if (D.n_own + nb + th * per_row + (T ? tw : 0) != D.n_ae) return false;
+    uint32_t r = 0;
+    if (Bo)
+        for (uint32_t x = G.x0; x < G.x1; ++x) ahalo[r++] = (G.y0 - 1) * B + x;
+    for (uint32_t y = G.y0; y < G.y1; ++y)
+    {
+        if (L) ahalo[r++] = y * B + G.x0 - 1;
+        if (R) ahalo[r++] = y * B + G.x1;
+    }
+    if (T)
+        for (uint32_t x = G.x0; x < G.x1; ++x) ahalo[r++] = G.y1 * B + x;
+    if (D.n_own + r != D.n_ae) return false;
+    auto col = [&](uint32_t x, uint32_t y) -> uint32_t {
+        if (x >= G.x0 && x < G.x1 && y >= G.y0 && y < G.y1) return own_local(x, y);
+        if (y + 1 == G.y0) return D.n_own + (x - G.x0);
+        if (y == G.y1) return D.n_own + nb + th * per_row + (x - G.x0);
+        return D.n_own + nb + (y - G.y0) * per_row + (x + 1 == G.x0 ? 0u : (L ? 1u : 0u));
+    };
+    uint32_t e = 0;
+    arp[0] = 0;
+    for (uint32_t q = 0; q < D.n_own; ++q)
+    {
+        const uint32_t x = G.x0 + q % tw, y = G.y0 + q / tw;
+        const uint32_t c = 1u + (y > 0) + (x > 0) + (x + 1 < B) + (y + 1 < ny);
+        if (e + c > D.nnz) return false;
+        if (y > 0) acol[e++] = (uint16_t)col(x, y - 1);
+        if (x > 0) acol[e++] = (uint16_t)col(x - 1, y);
+        acol[e++] = (uint16_t)q;
+        if (x + 1 < B) acol[e++] = (uint16_t)col(x + 1, y);
+        if (y + 1 < ny) acol[e++] = (uint16_t)col(x, y + 1);
+        arp[q + 1] = e;
+    }
+    return e == D.nnz;
 }
 
 }  // namespace b2s

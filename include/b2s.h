@@ -279,6 +279,10 @@ b2s_status b2s_pc_apply_device(b2s_ctx* ctx, b2s_pc* pc, const double* d_r, doub
  *   "amg.N.A", "amg.N.P": level N operator / prolongation; "amg.N.agg": aggregates in ci
  *   "pcg.tiles": sizes = {tiles of the tiled persistent PCG kernel (0: none), rows per thread,
  *                shared memory per CTA}; no arrays
+ *   "pcg.tiles.idx": the tiles' index blobs as 32-bit words in ci.  A 5-point grid's blobs are
+ *                built on the device from closed forms; with the environment variable
+ *                B2S_TILE_PLANNER=bfs at set-up the general breadth-first planner (host) lays them
+ *                out instead, for grids up to 65536 rows (it gives the same bytes)
  * Query sizes with NULL arrays: sizes[0] = rows (+1 for rp), sizes[1] = nnz, sizes[2] = values. */
 b2s_status b2s_pc_export(b2s_ctx* ctx, b2s_pc* pc, const char* what, uint64_t* sizes, uint32_t* rp, uint32_t* ci,
                          double* v);
@@ -309,7 +313,13 @@ b2s_status b2s_learner_params(b2s_learner* L, float* params, uint64_t* count, in
 /* Training loss of b2s_learner_step, over probe vectors w: */
 #define B2S_LOSS_PRECOND 0 /* preconditioned residual mean_w ||w - (L~L~^T)^{-1} A w||^2 / ||w||^2 (default) */
 #define B2S_LOSS_FACTOR 1  /* factorisation residual mean_w ||(L~L~^T - A) w||^2 / ||A w||^2 */
+#define B2S_LOSS_SWEEPS 2  /* preconditioned residual with the deployed sweep apply: M^-1 = F^T F, F the
+                              trsv_sweeps Jacobi sweeps of L~ (B2S_TRSV_JACOBI's operator) */
 b2s_status b2s_learner_set_loss(b2s_learner* L, int kind);
+/* B2S_LOSS_SWEEPS: Jacobi sweeps per triangle (default 6); every loss: the base factor the network
+ * corrects, 0 = the exact IC(0) (default), k > 0 = k fixed-point sweeps (b2s_pc_opts.factor_sweeps),
+ * as the preconditioner that deploys the network is built. */
+b2s_status b2s_learner_set_sweeps(b2s_learner* L, int trsv_sweeps, int factor_sweeps);
 /* One training step on A (SPD, structurally symmetric) with the learner's
  * loss over nprobes probes (generated from seed, every second one
  * Jacobi-smoothed; or taken from `probes`, host, nprobes * n, when not NULL).

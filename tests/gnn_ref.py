@@ -57,13 +57,15 @@ def features(n, rp, ci, v):
             invdeg.astype(np.float32).astype(np.float64), diag)
 
 
-LOSS_PRECOND, LOSS_FACTOR = 0, 1
+LOSS_PRECOND, LOSS_FACTOR, LOSS_SWEEPS = 0, 1, 2
 
 
-def loss_and_grad(params, n, rp, ci, v, Lrp, Lci, L0, probes, loss_kind=LOSS_PRECOND):
+def loss_and_grad(params, n, rp, ci, v, Lrp, Lci, L0, probes, loss_kind=LOSS_PRECOND, sweeps=6):
     """params: FP32 master parameters (rounded to BF16 as the GPU forward does).
-    loss_kind: LOSS_PRECOND, mean_w ||w - (L~L~^T)^{-1} A w||^2 / ||w||^2, or
-    LOSS_FACTOR, mean_w ||(L~L~^T - A) w||^2 / ||A w||^2."""
+    loss_kind: LOSS_PRECOND, mean_w ||w - (L~L~^T)^{-1} A w||^2 / ||w||^2,
+    LOSS_FACTOR, mean_w ||(L~L~^T - A) w||^2 / ||A w||^2, or LOSS_SWEEPS, the
+    first with (L~L~^T)^{-1} replaced by F^T F, F = `sweeps` Jacobi sweeps of
+    L~ (y_0 = D^-1 r, y_s = D^-1 (r - N y_{s-1})) and F^T those of L~^T."""
     P = bf16_round(params).requires_grad_(True)
     F, EF, invdeg, diag = features(n, rp, ci, v)
     F, EF, invdeg = map(torch.from_numpy, (F, EF, invdeg))
@@ -109,6 +111,17 @@ def loss_and_grad(params, n, rp, ci, v, Lrp, Lci, L0, probes, loss_kind=LOSS_PRE
     if loss_kind == LOSS_PRECOND:
         Y = torch.linalg.solve_triangular(Lmat, AW, upper=False)
         Z = torch.linalg.solve_triangular(Lmat.T, Y, upper=True)
+        E = W - Z
+        loss = ((E ** 2).sum(0) / (W ** 2).sum(0)).mean()
+    elif loss_kind == LOSS_SWEEPS:
+        D = torch.diagonal(Lmat)[:, None]
+        N = Lmat - torch.diag(torch.diagonal(Lmat))
+        Y = AW / D
+        for _ in range(sweeps):
+            Y = (AW - N @ Y) / D
+        Z = Y / D
+        for _ in range(sweeps):
+            Z = (Y - N.T @ Z) / D
         E = W - Z
         loss = ((E ** 2).sum(0) / (W ** 2).sum(0)).mean()
     else:

@@ -175,3 +175,23 @@ def stokes3d(N, alpha=0.1):
     K, A, B, Bt = split_saddle(N_vel, N_pres, R, Cc, V)
     Lp = (N_pres, N_pres) + coo_merge(N_pres, N_pres, LR, LC, LV)
     return K, A, B, Bt, Lp
+
+
+def diffusion2d(nx, ny, seed):
+    """-div(k grad u) on an nx x ny grid (x fastest), 5-point, face
+    coefficients k = exp(N(0,1)) per face, Dirichlet outside: SPD."""
+    rng = np.random.default_rng(seed)
+    kx = np.exp(rng.standard_normal((ny, nx + 1)))
+    ky = np.exp(rng.standard_normal((ny + 1, nx)))
+    R, Cc, V = [], [], []
+    for y in range(ny):
+        for x in range(nx):
+            i = y * nx + x
+            d = kx[y, x] + kx[y, x + 1] + ky[y, x] + ky[y + 1, x]
+            R.append(i); Cc.append(i); V.append(d)
+            if x > 0: R.append(i); Cc.append(i - 1); V.append(-kx[y, x])
+            if x + 1 < nx: R.append(i); Cc.append(i + 1); V.append(-kx[y, x + 1])
+            if y > 0: R.append(i); Cc.append(i - nx); V.append(-ky[y, x])
+            if y + 1 < ny: R.append(i); Cc.append(i + nx); V.append(-ky[y + 1, x])
+    rp, ci, v = coo_to_csr(nx * ny, nx * ny, R, Cc, V)
+    return nx * ny, rp, ci, v

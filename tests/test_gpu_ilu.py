@@ -493,3 +493,30 @@ def test_tiled_pcg_small_grid_and_repeat(b2s, ctx):
     x2, s2 = b2s.solve(ctx, A, b, b2s.PCG, M, tol=1e-10, maxit=5000)
     assert s1["status"] == 0 and s1["relres_true"] < 1e-10
     assert np.array_equal(x1, x2) and s1["iterations"] == s2["iterations"]
+
+
+@pytest.mark.parametrize("nx,ny,k", [(160, 120, 6), (90, 300, 4), (200, 200, 8)])
+def test_tiled_grid_blobs_match_general_planner(b2s, ctx, monkeypatch, nx, ny, k):
+    """A 5-point grid's tiles are laid out from closed forms and their index
+    blobs built on the device; the general breadth-first planner (host) must
+    give the same plan and the same blobs byte for byte, and the two
+    preconditioners the same PCG iterate bit for bit."""
+    from problems import diffusion2d
+    n, rp, ci, v = diffusion2d(nx, ny, seed=nx + ny + k)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    b = b2s.uniform(nx * ny, n)
+    opts = dict(precision=b2s.FP32, trsv=b2s.TRSV_JACOBI, trsv_sweeps=k)
+    monkeypatch.delenv("B2S_TILE_PLANNER", raising=False)
+    M_grid = b2s.Precond(ctx, A, b2s.PC_IC0, **opts)
+    monkeypatch.setenv("B2S_TILE_PLANNER", "bfs")
+    M_bfs = b2s.Precond(ctx, A, b2s.PC_IC0, **opts)
+    monkeypatch.delenv("B2S_TILE_PLANNER")
+    assert M_grid.sizes("pcg.tiles")[0] > 0
+    assert M_grid.sizes("pcg.tiles") == M_bfs.sizes("pcg.tiles")
+    _, blob_grid, _ = M_grid.export("pcg.tiles.idx")
+    _, blob_bfs, _ = M_bfs.export("pcg.tiles.idx")
+    assert blob_grid.size > 0 and np.array_equal(blob_grid, blob_bfs)
+    x1, s1 = b2s.solve(ctx, A, b, b2s.PCG, M_grid, tol=1e-8, maxit=5000)
+    x2, s2 = b2s.solve(ctx, A, b, b2s.PCG, M_bfs, tol=1e-8, maxit=5000)
+    assert s1["status"] == 0 and s1["relres_true"] < 1e-8
+    assert s1["iterations"] == s2["iterations"] and np.array_equal(x1, x2)

@@ -24,12 +24,15 @@ def test_untrained_is_ic0(b2s, ctx):
     assert np.array_equal(L.precond(A).apply(r), b2s.Precond(ctx, A, b2s.PC_IC0).apply(r))
 
 
-@pytest.mark.parametrize("loss_kind", [0, 1])
+@pytest.mark.parametrize("loss_kind", [0, 1, 2])
 def test_gradient_matches_autograd(b2s, ctx, orc, loss_kind):
+    """loss 2 (LOSS_SWEEPS, 4 sweeps here) runs the hand-written adjoint back
+    through both sweep sequences."""
     import gnn_ref
     n, rp, ci, v = system(b2s, N=20)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
     L = b2s.Learner(ctx, seed=7, loss=loss_kind)
+    L.set_sweeps(4, 0)
     p = L.params()
     rng = np.random.default_rng(0)
     # a non-zero head so every path carries gradient
@@ -39,7 +42,8 @@ def test_gradient_matches_autograd(b2s, ctx, orc, loss_kind):
     probes = rng.normal(size=(3, n))
     loss, grad = L.step(A, nprobes=3, probes=probes, update=False, want_grad=True)
     e = orc.ic0_export(orc.pc(orc.csr(n, n, rp, ci, v), "ic0"))
-    rloss, rgrad, _ = gnn_ref.loss_and_grad(p, n, rp, ci, v, e["Lrp"], e["Lci"], e["Lv"], probes, loss_kind)
+    rloss, rgrad, _ = gnn_ref.loss_and_grad(p, n, rp, ci, v, e["Lrp"], e["Lci"], e["Lv"], probes, loss_kind,
+                                            sweeps=4)
     assert abs(loss - rloss) <= 1e-4 * abs(rloss)
     scale = np.abs(rgrad).max()
     err = np.abs(grad - rgrad).max() / scale
@@ -51,7 +55,7 @@ def test_gradient_matches_autograd(b2s, ctx, orc, loss_kind):
         assert num / den < 5e-3, (a, b, num / den)
 
 
-@pytest.mark.parametrize("loss_kind", [1, 0])
+@pytest.mark.parametrize("loss_kind", [1, 0, 2])
 def test_training_reduces_loss_and_stays_spd(b2s, ctx, tmp_path, loss_kind):
     # Adam on a fixed probe set (seed 0): the objective itself must go down
     n, rp, ci, v = system(b2s, N=32, seed=11)

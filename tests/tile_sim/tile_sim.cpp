@@ -225,8 +225,47 @@ static void check_plan(const char* name, const Pattern& P, int k, int sms, uint3
     for (uint32_t i = 0; i < n; ++i) CHECK(seen[i] == 1, "%s: row %u owned %u times", name, i, seen[i]);
 }
 
+// the closed-form 5-point planner and builder against the breadth-first planner:
+// the same descriptors and the same index blobs, byte for byte
+static void check_grid5(const char* name, uint32_t N, uint32_t M, int k, int sms)
+{
+    const Pattern P = five_point(N, M);
+    const TilePlan T = plan_tiles(P.n, P.lrp.data(), P.lci.data(), P.urp.data(), P.uci.data(), k, sms, 228352, 4);
+    std::vector<TileGeom> geom;
+    const TilePlan G = plan_tiles_grid5(P.n, N, k, sms, 228352, geom);
+    std::printf("%-22s grid5 ok=%d (BFS ok=%d) tiles=%u\n", name, G.ok, T.ok, G.ntiles);
+    CHECK(is_grid5(P.n, P.lrp.data(), P.lci.data(), N, false), "%s: not recognised as a 5-point grid", name);
+    CHECK(G.ok == T.ok, "%s: grid5 ok %d vs %d", name, G.ok, T.ok);
+    if (!G.ok || !T.ok) return;
+    CHECK(G.ntiles == T.ntiles && G.smem == T.smem && G.work == T.work && G.Q == T.Q && G.ibytes == T.idx.size() &&
+              G.vbytes == T.vbytes, "%s: plan sizes differ", name);
+    std::vector<uint8_t> blob(G.ibytes, 0);
+    uint32_t scratch = 0;
+    for (const TileGeom& g : geom) scratch = std::max(scratch, grid5_scratch(g, N, M, k));
+    std::vector<uint16_t> loc(scratch);
+    for (uint32_t t = 0; t < G.ntiles; ++t)
+    {
+        CHECK(std::memcmp(&G.desc[t], &T.desc[t], sizeof(TileDesc)) == 0, "%s tile %u: descriptor differs", name, t);
+        for (int part = 0; part < 3; ++part)
+            CHECK(grid5_build_part(G.desc[t], geom[t], N, M, k, part, blob.data() + G.desc[t].ibase, loc.data()),
+                  "%s tile %u part %d: build failed", name, t, part);
+    }
+    CHECK(blob == T.idx, "%s: index blobs differ", name);
+    // a pattern that is not a 5-point grid is not taken for one
+    Pattern Q = P;
+    if (Q.lci.size() > 2) std::swap(Q.lci[Q.lrp[N + 1]], Q.lci[Q.lrp[N + 1] + 1]);
+    CHECK(!is_grid5(Q.n, Q.lrp.data(), Q.lci.data(), N, false), "%s: a perturbed pattern passed the check", name);
+}
+
 int main()
 {
+    check_grid5("grid5 512^2 k=6", 512, 512, 6, 148);
+    check_grid5("grid5 512^2 k=8", 512, 512, 8, 148);
+    check_grid5("grid5 600x200 k=6", 600, 200, 6, 148);
+    check_grid5("grid5 100x3000 k=6", 100, 3000, 6, 148);
+    check_grid5("grid5 64^2 k=3", 64, 64, 3, 148);
+    check_grid5("grid5 37^2 k=16", 37, 37, 16, 148);
+    check_grid5("grid5 512^2 132 SMs", 512, 512, 6, 132);
     check_plan("5-point 512^2, k=6", five_point(512), 6, 148, 228352, true);
     check_plan("5-point 512^2, k=8", five_point(512), 8, 148, 228352, true);
     check_plan("5-point 256^2, k=6", five_point(256), 6, 148, 228352, true);
