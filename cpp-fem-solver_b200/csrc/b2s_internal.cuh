@@ -445,13 +445,18 @@ __device__ __forceinline__ bool grid_reduce_last(double (&v)[NV], double* partia
     __syncthreads();
     if (!s_last) return false;
     __threadfence();
+    // every value's partials summed in block order as before, but the NV loads of
+    // one stride issued together (one L2 round trip per stride, not NV)
 #pragma unroll
-    for (int k = 0; k < NV; ++k)
+    for (int k = 0; k < NV; ++k) v[k] = 0.0;
+#pragma unroll 2
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
     {
-        double a = 0.0;
-        for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
-            a += __ldcg(&partial[(size_t)k * gridDim.x + b]);
-        v[k] = a;
+        double p[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) p[k] = __ldcg(&partial[(size_t)k * gridDim.x + b]);
+#pragma unroll
+        for (int k = 0; k < NV; ++k) v[k] += p[k];
     }
     block_reduce<NV, NT>(v);
     if (threadIdx.x == 0) *counter = 0u;

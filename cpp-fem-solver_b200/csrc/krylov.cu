@@ -103,7 +103,14 @@ __global__ void __launch_bounds__(kThreads) k_vec(uint64_t n, const int* done, B
 template <typename Body>
 void launch_vec(b2s_ctx* ctx, uint64_t n, const int* done, const Body& body)
 {
-    const unsigned g = stream_grid(ctx, n);
+    // one wave: no more CTAs than fit at once (bodies with many sums hold more registers)
+    static const int occ = [] {
+        int o = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_vec<Body>, kThreads, 0) != cudaSuccess) o = 0;
+        return o;
+    }();
+    unsigned g = stream_grid(ctx, n);
+    if (occ > 0) g = std::min(g, (unsigned)(occ * ctx->sm_count));
     if (Body::NV > 0) reserve_reduction(ctx, g);
     B2S_LAUNCH(ctx, k_vec<Body>, g, kThreads, 0, n, done, body, ctx->partial.p, ctx->counter.p);
 }

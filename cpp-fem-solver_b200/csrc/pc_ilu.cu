@@ -796,6 +796,7 @@ struct PcIC0 final : PcImpl
             uint32_t scratch = 0;
             for (const TileGeom& g : *grid5) scratch = std::max(scratch, grid5_scratch(g, B, ny, (int)P.k));
             tile_idx.alloc(P.ibytes ? P.ibytes : 16);
+            B2S_CUDA(cudaMemsetAsync(tile_idx.p, 0, tile_idx.bytes(), ctx->stream));  // the segments' padding
             geom = upload(ctx, *grid5);
             const size_t smem = 2ull * scratch * sizeof(uint16_t);
             if (smem > 48 * 1024)
@@ -807,7 +808,7 @@ struct PcIC0 final : PcImpl
         else
             tile_idx = upload(ctx, P.idx.data(), P.idx.size());
         tile_vals.alloc(P.vbytes ? P.vbytes : 16);
-        tile_slots.alloc(6ull * P.ntiles);
+        tile_slots.alloc(3ull * kTileSlotStride * P.ntiles);
         B2S_LAUNCH(ctx, k_tile_pack, P.ntiles, kThreads, 0, tile_desc.p, tile_idx.p, tile_vals.p, n, (int)P.k,
                    A.rp.p, A.ci.p, A.v.p, fwd.band_off.p, fwd.band_val.p, fwd.band_dinv.p, bwd.band_off.p,
                    bwd.band_val.p, bwd.band_dinv.p, bad.p);

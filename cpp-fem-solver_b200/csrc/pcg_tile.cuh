@@ -23,14 +23,14 @@
 //
 // A phase ends with an all-reduce that is also the grid barrier: thread 0
 // fences (gpu scope, after the CTA's barrier) and publishes the tile's
-// partial as two 64-bit words {epoch, 32 value bits}; warp 0 of every CTA
-// polls all tiles' words with relaxed loads, every lane its tiles at once,
-// until they carry the phase's epoch, then fences and sums them in tile order
-// -- one L2 round trip per poll where a barrier and a separate read of the
-// partials took two (acquire loads would serialise a lane's ten loads).
-// Every CTA gets the same bits and takes the same scalar step.  Each wait is bounded (kGridBarrierPolls
-// polls); a CTA that gives up records B2S_TIMEOUT and leaves, and the others
-// give up at their next all-reduce, so the launch always ends.
+// partial as two 64-bit words {epoch, 32 value bits} in a line of its own;
+// thread b of every CTA polls tile b's words with relaxed loads until they
+// carry the phase's epoch, fences, and leaves the value in shared memory;
+// after one block barrier warp 0 sums them in tile order.  Every CTA gets the
+// same bits and takes the same scalar step.  Each wait is bounded
+// (kGridBarrierPolls polls); a CTA that gives up records B2S_TIMEOUT and
+// leaves, and the others give up at their next all-reduce, so the launch
+// always ends.
 #pragma once
 
 #include "pcg_band.cuh"
@@ -39,7 +39,7 @@
 
 namespace b2s {
 
-constexpr uint32_t kTileMaxTilesPerLane = 5;  // all-reduce over at most 160 tiles
+constexpr uint32_t kTileSlotStride = 16;      // words between two tiles' all-reduce slots (128 bytes)
 
 struct PcgTileArgs
 {
@@ -53,7 +53,7 @@ struct PcgTileArgs
     double* p[2];
     double *z, *Ap;
     float* y32;
-    unsigned long long* slots;  // 3 phases x ntiles x 2 words, zero at launch
+    unsigned long long* slots;  // 3 phases x ntiles x kTileSlotStride words, zero at launch
     KState* st;
     int* err;
     int stall_window;
@@ -74,66 +74,59 @@ __device__ __forceinline__ unsigned long long ld_relaxed_gpu_u64(const unsigned 
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 // Thread 0 holds this tile's partial `part`.  Publishes it for `epoch`, waits
-// for every tile's, and leaves their sum (tile order; the same bits in every
-// CTA) in *out.  False, with B2S_TIMEOUT recorded, when a wait gives up.
+// for every tile's and returns their sum in thread 0 (tile order, the same
+// association in every CTA, so the same bits); false in every thread, with
+// B2S_TIMEOUT recorded, when a wait gives up.  Each tile's two words sit alone
+// in a 128-byte line (kTileSlotStride words apart), and thread b < ntiles
+// polls tile b's words only until they carry the epoch, so a tile that has
+// arrived is not read again and the polls of all CTAs spread over as many
+// lines as tiles.
 __device__ __forceinline__ bool tile_allreduce(unsigned long long* slots, uint32_t tile, uint32_t ntiles,
-                                               uint32_t epoch, double part, double* out, int* err, int* s_ok)
+                                               uint32_t epoch, double part, double& sum, int* err,
+                                               double* s_part, int* s_fail)
 {
-    if (threadIdx.x == 0)
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0)
     {
         // the CTA's writes (ordered before this thread by the barrier inside
         // block_reduce) become visible before the words that announce them
         fence_acq_rel_gpu();
         const unsigned long long e = (unsigned long long)epoch << 32;
         const unsigned long long b = (unsigned long long)__double_as_longlong(part);
-        st_relaxed_gpu_u64(&slots[2 * tile], e | (b & 0xffffffffull));
-        st_relaxed_gpu_u64(&slots[2 * tile + 1], e | (b >> 32));
+        st_relaxed_gpu_u64(&slots[(size_t)kTileSlotStride * tile], e | (b & 0xffffffffull));
+        st_relaxed_gpu_u64(&slots[(size_t)kTileSlotStride * tile + 1], e | (b >> 32));
     }
-    if (threadIdx.x < 32)
+    if (tid < ntiles)
     {
-        const uint32_t lane = threadIdx.x;
-        double v[kTileMaxTilesPerLane];
-        bool ok = false;
-        for (unsigned polls = 0; polls < kGridBarrierPolls; ++polls)
+        const unsigned long long* w = &slots[(size_t)kTileSlotStride * tid];
+        unsigned long long w0 = 0, w1 = 0;
+        bool seen = false;
+        for (unsigned polls = 0; polls < kGridBarrierPolls && !seen; ++polls)
         {
-            bool all = true;
-#pragma unroll
-            for (uint32_t j = 0; j < kTileMaxTilesPerLane; ++j)
-            {
-                const uint32_t b = lane + 32 * j;
-                v[j] = 0.0;
-                if (b < ntiles)
-                {
-                    const unsigned long long w0 = ld_relaxed_gpu_u64(&slots[2 * b]);
-                    const unsigned long long w1 = ld_relaxed_gpu_u64(&slots[2 * b + 1]);
-                    all &= (uint32_t)(w0 >> 32) == epoch && (uint32_t)(w1 >> 32) == epoch;
-                    v[j] = __longlong_as_double((long long)(((w1 & 0xffffffffull) << 32) | (w0 & 0xffffffffull)));
-                }
-            }
-            if (__all_sync(0xffffffffu, all))
-            {
-                ok = true;
-                break;
-            }
+            w0 = ld_relaxed_gpu_u64(w);
+            w1 = ld_relaxed_gpu_u64(w + 1);
+            seen = (uint32_t)(w0 >> 32) == epoch && (uint32_t)(w1 >> 32) == epoch;
         }
-        // the words seen carry the other CTAs' fenced writes: this fence
-        // (then the block barrier below) orders the CTA's later reads after them
+        if (!seen)
+        {
+            *s_fail = 1;
+            atomicExch(err, (int)B2S_TIMEOUT);
+        }
+        // the words seen carry the other CTAs' fenced writes: this fence (then
+        // the block barrier below) orders the CTA's later reads after them
         fence_acq_rel_gpu();
-        double t = 0.0;
-#pragma unroll
-        for (uint32_t j = 0; j < kTileMaxTilesPerLane; ++j)
-            if (lane + 32 * j < ntiles) t += v[j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-        if (lane == 0)
-        {
-            *out = t;
-            *s_ok = ok ? 1 : 0;
-            if (!ok) atomicExch(err, (int)B2S_TIMEOUT);
-        }
+        s_part[tid] = __longlong_as_double((long long)(((w1 & 0xffffffffull) << 32) | (w0 & 0xffffffffull)));
     }
     __syncthreads();
-    return *s_ok != 0;
+    if (tid < 32)
+    {
+        double t = 0.0;
+        for (uint32_t b = tid; b < ntiles; b += 32) t += s_part[b];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        sum = t;
+    }
+    return *s_fail == 0;
 }
 
 // k + 1 passes over the extended set; rows of layers 0..k-s at pass s.
@@ -176,8 +169,9 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
     constexpr uint32_t NT = kTileThreads;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ KState sst;
-    __shared__ int s_ok;
-    __shared__ double s_best, s_sum;
+    __shared__ int s_fail;
+    __shared__ double s_part[kTileMaxTiles];
+    __shared__ double s_best;
     __shared__ int s_best_at;
     const uint32_t tile = blockIdx.x, ntiles = a.ntiles, tid = threadIdx.x;
     const TileDesc& Dg = a.desc[tile];
@@ -201,6 +195,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
     if (tid == 0)
     {
         sst = *a.st;
+        s_fail = 0;
         s_best = HUGE_VAL;
         s_best_at = 0;
     }
@@ -225,9 +220,19 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
 
     uint32_t epoch = 0;
     int parity = 0;
-    double pv[Q], rd[Q];  // the owned rows' p and updated r (thread's rows t = tid + NT q)
+    // The owned rows' p and x live in registers (thread's rows t = tid + NT q);
+    // p is also stored each iteration (other tiles read it), x once at the end.
+    double pv[Q], xv[Q];
 #pragma unroll
-    for (uint32_t q = 0; q < Q; ++q) pv[q] = rd[q] = 0.0;
+    for (uint32_t q = 0; q < Q; ++q)
+    {
+        const uint32_t t = tid + NT * q;
+        const uint32_t g = t < n_own ? owned[t] : 0u;
+        const bool in = t < n_own;
+        pv[q] = in ? a.p[0][g] : 0.0;
+        xv[q] = in ? a.x[g] : 0.0;
+    }
+    const float* yf = y0;  // the forward sweeps' result (phase 2 -> phase 3)
     while (!sst.done)
     {
         const double* pold = a.p[parity];
@@ -237,9 +242,15 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
         // ---- 1. p = z + beta p_old at the SpMV's columns; Ap; p.Ap
         {
             const double beta = sst.beta;
-            for (uint32_t t = tid; t < n_ae; t += NT)
+#pragma unroll
+            for (uint32_t q = 0; q < Q; ++q)
             {
-                const uint32_t g = t < n_own ? owned[t] : ahalo[t - n_own];
+                const uint32_t t = tid + NT * q;
+                if (t < n_own) pe[t] = __ldcg(&a.z[owned[t]]) + beta * pv[q];
+            }
+            for (uint32_t t = n_own + tid; t < n_ae; t += NT)
+            {
+                const uint32_t g = ahalo[t - n_own];
                 pe[t] = __ldcg(&a.z[g]) + beta * __ldcg(&pold[g]);
             }
             __syncthreads();
@@ -261,8 +272,9 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
                 }
             }
             block_reduce<1, NT>(acc);
-            if (!tile_allreduce(a.slots, tile, ntiles, ++epoch, acc[0], &s_sum, a.err, &s_ok)) break;
-            if (tid == 0) pcg_alpha(&sst, s_sum);
+            double tot;
+            if (!tile_allreduce(a.slots, tile, ntiles, ++epoch, acc[0], tot, a.err, s_part, &s_fail)) break;
+            if (tid == 0) pcg_alpha(&sst, tot);
             __syncthreads();
             if (sst.done) break;
         }
@@ -272,6 +284,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
             uint32_t dep[Q];
             float2 val[Q];
             float di[Q], rr[Q];
+            double acc[1] = {0.0};
 #pragma unroll
             for (uint32_t q = 0; q < Q; ++q)
             {
@@ -283,29 +296,28 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
                 di[q] = in ? ldinv[t] : 0.f;
                 const double rv = in ? __ldcg(&rold[g]) - alpha * __ldcg(&a.Ap[g]) : 0.0;
                 rr[q] = (float)rv;
-                if (t < n_own) rd[q] = rv;
+                if (t < n_own)  // the owned rows' r, r.r and x now, before the sweeps
+                {
+                    rnew[g] = rv;
+                    acc[0] += rv * rv;
+                    xv[q] += alpha * pv[q];
+                }
             }
-            const float* yk = tile_sweeps<Q>(a.k, s_lcnt, dep, val, di, rr, y0, y1);
-            double acc[1] = {0.0};
+            yf = tile_sweeps<Q>(a.k, s_lcnt, dep, val, di, rr, y0, y1);
 #pragma unroll
             for (uint32_t q = 0; q < Q; ++q)
             {
                 const uint32_t t = tid + NT * q;
-                if (t < n_own)
-                {
-                    const uint32_t g = owned[t];
-                    a.y32[g] = yk[t];
-                    a.x[g] += alpha * pv[q];
-                    rnew[g] = rd[q];
-                    acc[0] += rd[q] * rd[q];
-                }
+                if (t < n_own) a.y32[owned[t]] = yf[t];
             }
             block_reduce<1, NT>(acc);
-            if (!tile_allreduce(a.slots + 2ull * ntiles, tile, ntiles, ++epoch, acc[0], &s_sum, a.err, &s_ok))
+            double tot;
+            if (!tile_allreduce(a.slots + (size_t)kTileSlotStride * ntiles, tile, ntiles, ++epoch, acc[0], tot, a.err,
+                                s_part, &s_fail))
                 break;
             if (tid == 0)
             {
-                if (!pcg_check_converged(&sst, s_sum) && a.stall_window > 0)
+                if (!pcg_check_converged(&sst, tot) && a.stall_window > 0)
                 {
                     if (sst.relres < 0.5 * s_best)
                     {
@@ -337,7 +349,8 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
                 dep[q] = in ? udeps[t] : 0xFFFFFFFFu;
                 val[q] = in ? uvals[t] : make_float2(0.f, 0.f);
                 di[q] = in ? udinv[t] : 0.f;
-                rr[q] = in ? __ldcg(&a.y32[g]) : 0.f;
+                // (owned rows: this thread's own forward results, read before its sweeps write)
+                rr[q] = t < n_own ? yf[t] : in ? __ldcg(&a.y32[g]) : 0.f;
             }
             const float* yk = tile_sweeps<Q>(a.k, s_ucnt, dep, val, di, rr, y0, y1);
             double acc[1] = {0.0};
@@ -347,18 +360,27 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
                 const uint32_t t = tid + NT * q;
                 if (t < n_own)
                 {
+                    const uint32_t g = owned[t];
                     const double zi = (double)yk[t];
-                    a.z[owned[t]] = zi;
-                    acc[0] += rd[q] * zi;
+                    a.z[g] = zi;
+                    acc[0] += rnew[g] * zi;  // (this thread's own store of phase 2)
                 }
             }
             block_reduce<1, NT>(acc);
-            if (!tile_allreduce(a.slots + 4ull * ntiles, tile, ntiles, ++epoch, acc[0], &s_sum, a.err, &s_ok))
+            double tot;
+            if (!tile_allreduce(a.slots + 2ull * kTileSlotStride * ntiles, tile, ntiles, ++epoch, acc[0], tot, a.err,
+                                s_part, &s_fail))
                 break;
-            if (tid == 0) pcg_next(&sst, s_sum);
+            if (tid == 0) pcg_next(&sst, tot);
             __syncthreads();
         }
         parity ^= 1;
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < Q; ++q)
+    {
+        const uint32_t t = tid + NT * q;
+        if (t < n_own) a.x[owned[t]] = xv[q];
     }
     if (tile == 0 && tid == 0) *a.st = sst;
 }
