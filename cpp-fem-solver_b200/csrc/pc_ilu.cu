@@ -681,6 +681,82 @@ struct HostAnalysis
     }
 };
 
+// What the sweep schedules need of a lower factor's pattern (diagonal last in
+// each row), computed on the device: the bandwidth B (largest i - j), the
+// widest row and the widest column of the strict part, and whether the pattern
+// is a 5-point grid's of row length B (is_grid5 in tile_plan.hpp).
+struct PatternStats
+{
+    uint32_t B = 0, w_row = 0, w_col = 0;
+    bool grid5 = false;
+};
+
+__global__ void k_pattern_stats(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                                uint32_t* __restrict__ colcnt, uint32_t* __restrict__ out)
+{
+    uint32_t B = 0, w = 0, wc = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        uint32_t c = 0;
+        for (uint32_t q = rp[i]; q < rp[i + 1]; ++q)
+        {
+            const uint32_t j = ci[q];
+            if (j < i)
+            {
+                ++c;
+                B = max(B, i - j);
+                wc = max(wc, atomicAdd(&colcnt[j], 1u) + 1u);
+            }
+        }
+        w = max(w, c);
+    }
+    if (B) atomicMax(&out[0], B);
+    if (w) atomicMax(&out[1], w);
+    if (wc) atomicMax(&out[2], wc);
+}
+
+__global__ void k_pattern_grid5(uint32_t n, const uint32_t* __restrict__ rp, const uint32_t* __restrict__ ci,
+                                uint32_t B, uint32_t* __restrict__ bad)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const uint32_t x = i % B, y = i / B;
+        const uint32_t e0 = rp[i], e1 = rp[i + 1];
+        const uint32_t want = (y > 0) + (x > 0) + 1u;
+        bool ok = e1 - e0 == want && ci[e1 - 1] == i;
+        uint32_t e = e0;
+        if (ok && y > 0) ok = ci[e++] == i - B;
+        if (ok && x > 0) ok = ci[e] == i - 1;
+        if (!ok) atomicExch(bad, 1u);
+    }
+}
+
+static PatternStats pattern_stats(b2s_ctx* ctx, const Csr32& L)
+{
+    PatternStats ps;
+    const uint32_t n = L.n;
+    if (!n) return ps;
+    DBuf<uint32_t> colcnt(n), out(4);
+    B2S_CUDA(cudaMemsetAsync(colcnt.p, 0, colcnt.bytes(), ctx->stream));
+    B2S_CUDA(cudaMemsetAsync(out.p, 0, out.bytes(), ctx->stream));
+    const unsigned g = stream_grid(ctx, n);
+    B2S_LAUNCH(ctx, k_pattern_stats, g, kThreads, 0, n, L.rp.p, L.ci.p, colcnt.p, out.p);
+    uint32_t h[4] = {0, 0, 0, 0};
+    d2h(ctx, h, out.p, 3 * sizeof(uint32_t));
+    sync(ctx);
+    ps.B = h[0];
+    ps.w_row = h[1];
+    ps.w_col = h[2];
+    if (ps.B && n % ps.B == 0)
+    {
+        B2S_LAUNCH(ctx, k_pattern_grid5, g, kThreads, 0, n, L.rp.p, L.ci.p, ps.B, out.p + 3);
+        d2h(ctx, h + 3, out.p + 3, sizeof(uint32_t));
+        sync(ctx);
+        ps.grid5 = h[3] == 0;
+    }
+    return ps;
+}
+
 static void copy_pattern(b2s_ctx* ctx, const Csr32& M, std::vector<uint32_t>& rp, std::vector<uint32_t>& ci)
 {
     rp.resize((size_t)M.n + 1);
@@ -793,17 +869,11 @@ struct PcIC0 final : PcImpl
         if (grid5)
         {
             const uint32_t B = P.B, ny = n / P.B;
-            uint32_t scratch = 0;
-            for (const TileGeom& g : *grid5) scratch = std::max(scratch, grid5_scratch(g, B, ny, (int)P.k));
             tile_idx.alloc(P.ibytes ? P.ibytes : 16);
             B2S_CUDA(cudaMemsetAsync(tile_idx.p, 0, tile_idx.bytes(), ctx->stream));  // the segments' padding
             geom = upload(ctx, *grid5);
-            const size_t smem = 2ull * scratch * sizeof(uint16_t);
-            if (smem > 48 * 1024)
-                B2S_CUDA(cudaFuncSetAttribute(k_tile_build_grid5, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)smem));
-            B2S_LAUNCH(ctx, k_tile_build_grid5, P.ntiles, 32, smem, tile_desc.p, geom.p, tile_idx.p, B, ny, (int)P.k,
-                       scratch, bad.p);
+            B2S_LAUNCH(ctx, k_tile_build_grid5, P.ntiles, kThreads, 0, tile_desc.p, geom.p, tile_idx.p, B, ny, P.k,
+                       bad.p);
         }
         else
             tile_idx = upload(ctx, P.idx.data(), P.idx.size());
@@ -1094,15 +1164,25 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     const int nsweeps = sweep_count(o);
     const uint32_t seg = sweep_segment(o);
     const int fsweeps = o.factor_sweeps;
+    // The host copy of L's pattern feeds the level schedules and the chunk and
+    // breadth-first tile planners.  The sweep schedule over a fixed-point factor
+    // needs none of them: its band plans and the 5-point grid test come from
+    // statistics reduced on the device (a few words back instead of the pattern).
     std::vector<uint32_t> hrp, hci;
-    copy_pattern(ctx, pc->L, hrp, hci);
+    bool have_pattern = false;
+    auto need_pattern = [&] {
+        if (!have_pattern) copy_pattern(ctx, pc->L, hrp, hci);
+        have_pattern = true;
+    };
     pc->fwd.init(pc->L, true, false);
     // the levels of L order the exact factorisation and the exact solves
     auto levels = [&] {
+        need_pattern();
         compute_levels(n, hrp.data(), hci.data(), true, pc->fwd.h_level);
         pc->fwd.ensure_sched(ctx);
     };
-    if (!(sweeps && fsweeps > 0)) levels();
+    const bool sweep_only = sweeps && fsweeps > 0;
+    if (!sweep_only) levels();
     HostAnalysis ha;
     ha.chunked = pc->mode == B2S_TRSV_CHUNK && n;
     const int sm_count = ctx->sm_count;
@@ -1110,30 +1190,37 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     int smem_optin = 0;
     B2S_CUDA(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
     const uint32_t tile_smem = smem_optin > 4096 ? (uint32_t)smem_optin - 4096u : 0u;  // static shared memory aside
-    ha.th = std::thread([&ha, &hrp, &hci, &pc, n, vs, sweeps, nsweeps, seg, sm_count, fp32, tile_smem] {
+    PatternStats ps;
+    bool bfs = false;
+    if (sweeps)
+    {
+        ps = pattern_stats(ctx, pc->L);
+        const char* planner = std::getenv("B2S_TILE_PLANNER");  // "bfs": the general planner
+        bfs = (planner && std::strcmp(planner, "bfs") == 0) || !ps.grid5;
+        if (fp32 && bfs && n <= kTilePlanHostMaxRows) need_pattern();
+    }
+    else
+        need_pattern();
+    ha.th = std::thread([&ha, &hrp, &hci, &pc, ps, bfs, n, vs, sweeps, nsweeps, seg, sm_count, fp32, tile_smem] {
         try
         {
             if (sweeps)
             {
-                // both band plans from L's pattern (L^T's is not needed on the host)
+                // both band plans from L's statistics (L^T's pattern is not needed on the host)
                 if (fp32)
-                    plan_parallel(2, 2, [&](uint32_t side, unsigned) {
-                        if (side == 0)
-                            ha.lo_band = plan_band(n, hrp.data(), hci.data(), true, nsweeps, sm_count, seg);
-                        else
-                            ha.up_band = plan_band_transposed(n, hrp.data(), hci.data(), nsweeps, sm_count, seg);
-                    });
+                {
+                    ha.lo_band = plan_band_from(n, ps.B, ps.w_row, nsweeps, sm_count, seg);
+                    ha.up_band = plan_band_from(n, ps.B, ps.w_col, nsweeps, sm_count, seg);
+                }
                 // the tiled persistent PCG kernel: plain Jacobi, two strict entries per row.
                 // A 5-point grid is laid out from closed forms (its blobs are built on the
                 // device); other patterns take the breadth-first planner while it is cheap.
                 if (fp32 && seg == 1 && ha.lo_band.T && ha.up_band.T && ha.lo_band.W == 2 && ha.up_band.W == 2 &&
                     nsweeps <= kTileMaxSweeps)
                 {
-                    const char* planner = std::getenv("B2S_TILE_PLANNER");  // "bfs": the general planner
-                    const bool bfs = planner && std::strcmp(planner, "bfs") == 0;
-                    if (!bfs && is_grid5(n, hrp.data(), hci.data(), ha.lo_band.B, true))
+                    if (!bfs)
                     {
-                        ha.tiles = plan_tiles_grid5(n, ha.lo_band.B, nsweeps, sm_count, tile_smem, ha.tile_geom);
+                        ha.tiles = plan_tiles_grid5(n, ps.B, nsweeps, sm_count, tile_smem, ha.tile_geom);
                         ha.tiles_grid5 = true;
                     }
                     else if (n <= kTilePlanHostMaxRows)

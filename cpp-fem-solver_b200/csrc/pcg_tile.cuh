@@ -386,20 +386,29 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
 }
 
 // Builds the index blobs of a 5-point grid's tiles (tile_plan.hpp,
-// grid5_build_part): block t, threads 0..2 the three parts of tile t, the
-// lower and upper parts each with its box map in shared memory (scratch
-// entries).  *bad = 1 when a count disagrees with the descriptors.
-__global__ void k_tile_build_grid5(const TileDesc* __restrict__ desc, const TileGeom* __restrict__ geom,
-                                   uint8_t* __restrict__ idx, uint32_t B, uint32_t ny, int k, uint32_t scratch,
-                                   int* bad)
+// grid5_build_elem / grid5_build_dep): block t builds tile t, one thread per
+// blob element, then one per extended row for the dependencies once the
+// halos are written.  *bad = 1 when an index falls outside its segment.
+__global__ void __launch_bounds__(kThreads) k_tile_build_grid5(const TileDesc* __restrict__ desc,
+                                                               const TileGeom* __restrict__ geom,
+                                                               uint8_t* __restrict__ idx, uint32_t B, uint32_t ny,
+                                                               uint32_t K, int* bad)
 {
-    extern __shared__ uint16_t loc[];  // 2 x scratch
-    const uint32_t t = blockIdx.x;
-    const int part = (int)threadIdx.x;
-    if (part >= 3) return;
-    const TileDesc D = desc[t];
-    const TileGeom G = geom[t];
-    if (!grid5_build_part(D, G, B, ny, k, part, idx + D.ibase, loc + (part == 1 ? scratch : 0u))) atomicExch(bad, 1);
+    __shared__ TileDesc D;
+    __shared__ TileGeom G;
+    if (threadIdx.x == 0)
+    {
+        D = desc[blockIdx.x];
+        G = geom[blockIdx.x];
+    }
+    __syncthreads();
+    uint8_t* ib = idx + D.ibase;
+    const uint32_t ne = grid5_elements(D, G, B, ny, K);
+    for (uint32_t e = threadIdx.x; e < ne; e += blockDim.x)
+        if (!grid5_build_elem(D, G, B, ny, K, e, ib)) atomicExch(bad, 1);
+    __syncthreads();  // the halos, read back below
+    for (uint32_t t = threadIdx.x; t < D.n_el; t += blockDim.x) grid5_build_dep(D, G, B, ny, K, true, t, ib);
+    for (uint32_t t = threadIdx.x; t < D.n_eu; t += blockDim.x) grid5_build_dep(D, G, B, ny, K, false, t, ib);
 }
 
 // Fills the value blobs after factorisation: A's values for the owned rows

@@ -657,4 +657,208 @@ B2S_TILE_HD inline bool grid5_build_part(const TileDesc& D, const TileGeom& G, u
     return e == D.nnz;
 }
 
+// ---- the same blob, one element at a time (the device builds it with one
+// thread per element; grid5_build_part is the sequential statement of it).
+//
+// A set's box (lower: the block grown by k down and left, upper: up and
+// right) is walked in row-major order; an entry at distance d >= 1 from the
+// block (d = da + db, the distances along x and y) takes the next local index
+// of layer d.  Its rank inside layer d has a closed form: rows of the box
+// before it hold, per row, the whole block width when d = db (da = 0) or the
+// one entry at da = d - db (when it lies inside the box), and in its own row
+// no earlier entry of layer d precedes it unless da = 0.
+struct Grid5Box
+{
+    uint32_t bx0, bx1, by0, by1;
+};
+
+B2S_TILE_HD inline Grid5Box grid5_box(const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K, bool lo)
+{
+    Grid5Box b;
+    b.bx0 = lo ? (G.x0 > K ? G.x0 - K : 0) : G.x0;
+    b.by0 = lo ? (G.y0 > K ? G.y0 - K : 0) : G.y0;
+    b.bx1 = lo ? G.x1 : (B < G.x1 + K ? B : G.x1 + K);
+    b.by1 = lo ? G.y1 : (ny < G.y1 + K ? ny : G.y1 + K);
+    return b;
+}
+
+B2S_TILE_HD inline uint32_t grid5_dx(const TileGeom& G, bool lo, uint32_t x)
+{
+    return lo ? (x < G.x0 ? G.x0 - x : 0u) : (x >= G.x1 ? x - G.x1 + 1u : 0u);
+}
+
+B2S_TILE_HD inline uint32_t grid5_dy(const TileGeom& G, bool lo, uint32_t y)
+{
+    return lo ? (y < G.y0 ? G.y0 - y : 0u) : (y >= G.y1 ? y - G.y1 + 1u : 0u);
+}
+
+// entries of layer d in box row y
+B2S_TILE_HD inline uint32_t grid5_row_count(const TileGeom& G, const Grid5Box& b, bool lo, uint32_t y, uint32_t d)
+{
+    const uint32_t db = grid5_dy(G, lo, y);
+    if (d < db) return 0;
+    const uint32_t e = d - db;
+    if (e == 0) return G.x1 - G.x0;
+    return lo ? (G.x0 >= b.bx0 + e ? 1u : 0u) : (G.x1 - 1u + e < b.bx1 ? 1u : 0u);
+}
+
+// the local index of grid point (x, y) in a tile's lower (lo) or upper set, or
+// kTileNoDep when the point is outside it
+B2S_TILE_HD inline uint32_t grid5_local(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K,
+                                        bool lo, uint32_t x, uint32_t y)
+{
+    const Grid5Box b = grid5_box(G, B, ny, K, lo);
+    if (x < b.bx0 || x >= b.bx1 || y < b.by0 || y >= b.by1) return kTileNoDep;
+    const uint32_t da = grid5_dx(G, lo, x), db = grid5_dy(G, lo, y), d = da + db;
+    if (d == 0) return (y - G.y0) * (G.x1 - G.x0) + (x - G.x0);
+    if (d > K) return kTileNoDep;
+    uint32_t rank = 0;
+    // rows of the box before y: those off the block (db >= 1) one by one,
+    // those beside the block (db = 0) hold one entry of layer d each
+    const uint32_t side0 = lo ? G.y0 : b.by0, side1 = lo ? b.by1 : G.y1;  // rows with db = 0
+    const uint32_t per_side = grid5_row_count(G, b, lo, side0 < side1 ? side0 : b.by0, d);
+    for (uint32_t yy = b.by0; yy < y; ++yy)
+    {
+        if (yy >= side0 && yy < side1)
+        {
+            const uint32_t last = y < side1 ? y : side1;
+            rank += (last - yy) * per_side;
+            yy = last - 1;
+            continue;
+        }
+        rank += grid5_row_count(G, b, lo, yy, d);
+    }
+    if (da == 0) rank += x - G.x0;
+    const uint16_t* cnt = lo ? D.lcnt : D.ucnt;
+    const uint32_t l = cnt[d - 1] + rank;
+    return l < cnt[d] ? l : kTileNoDep;
+}
+
+// Element `e` of a tile's index blob, for e < grid5_elements(D): the owned
+// rows, the two sets' halos, the SpMV ring and its rows (offsets and
+// columns) -- everything but the dependencies, which need the halos first
+// (grid5_build_deps).  False when an index falls outside its segment.
+B2S_TILE_HD inline uint32_t grid5_elements(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K)
+{
+    const Grid5Box lb = grid5_box(G, B, ny, K, true), ub = grid5_box(G, B, ny, K, false);
+    return D.n_own + (lb.bx1 - lb.bx0) * (lb.by1 - lb.by0) + (ub.bx1 - ub.bx0) * (ub.by1 - ub.by0) +
+           (D.n_ae - D.n_own) + D.n_own;
+}
+
+B2S_TILE_HD inline bool grid5_build_elem(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K,
+                                         uint32_t e, uint8_t* ib)
+{
+    const uint32_t tw = G.x1 - G.x0, th = G.y1 - G.y0;
+    if (e < D.n_own)
+    {
+        reinterpret_cast<uint32_t*>(ib + D.o_owned)[e] = (G.y0 + e / tw) * B + G.x0 + e % tw;
+        return true;
+    }
+    e -= D.n_own;
+    for (int side = 0; side < 2; ++side)
+    {
+        const bool lo = side == 0;
+        const Grid5Box b = grid5_box(G, B, ny, K, lo);
+        const uint32_t bw = b.bx1 - b.bx0, sz = bw * (b.by1 - b.by0);
+        if (e < sz)
+        {
+            const uint32_t x = b.bx0 + e % bw, y = b.by0 + e / bw;
+            const uint32_t d = grid5_dx(G, lo, x) + grid5_dy(G, lo, y);
+            if (d == 0 || d > K) return true;
+            const uint32_t l = grid5_local(D, G, B, ny, K, lo, x, y);
+            if (l == kTileNoDep || l < D.n_own) return false;
+            reinterpret_cast<uint32_t*>(ib + (lo ? D.o_lhalo : D.o_uhalo))[l - D.n_own] = y * B + x;
+            return true;
+        }
+        e -= sz;
+    }
+    const bool L = G.x0 > 0, R = G.x1 < B, Bo = G.y0 > 0, T = G.y1 < ny;
+    const uint32_t nb = Bo ? tw : 0, per_row = (L ? 1u : 0u) + (R ? 1u : 0u);
+    if (e < D.n_ae - D.n_own)
+    {
+        uint32_t g;
+        if (e < nb)
+            g = (G.y0 - 1) * B + G.x0 + e;
+        else if (e - nb < th * per_row)
+        {
+            const uint32_t r = e - nb, y = G.y0 + r / per_row;
+            g = (r % per_row == 0 && L) ? y * B + G.x0 - 1 : y * B + G.x1;
+        }
+        else
+        {
+            const uint32_t x = G.x0 + (e - nb - th * per_row);
+            if (!T || x >= G.x1) return false;
+            g = G.y1 * B + x;
+        }
+        reinterpret_cast<uint32_t*>(ib + D.o_ahalo)[e] = g;
+        return true;
+    }
+    e -= D.n_ae - D.n_own;
+    if (e >= D.n_own) return false;
+    // owned row q = e: its CSR offset (the entries of the block's earlier
+    // rows and of the row's earlier points) and its columns in local numbering
+    const uint32_t q = e, x = G.x0 + q % tw, y = G.y0 + q / tw;
+    auto cnt_row = [&](uint32_t yy, uint32_t xa, uint32_t xb) {  // entries of points [xa, xb) of row yy
+        const uint32_t w = xb - xa;
+        uint32_t c = w * (1u + (yy > 0) + (yy + 1 < ny));
+        c += w - (xa == 0 && w ? 1u : 0u);  // left neighbours
+        c += w - (xb == B && w ? 1u : 0u);  // right neighbours
+        return c;
+    };
+    uint32_t off = 0;
+    for (uint32_t yy = G.y0; yy < y; ++yy) off += cnt_row(yy, G.x0, G.x1);
+    off += cnt_row(y, G.x0, x);
+    const uint32_t c = 1u + (y > 0) + (x > 0) + (x + 1 < B) + (y + 1 < ny);
+    if (off + c > D.nnz) return false;
+    uint32_t* arp = reinterpret_cast<uint32_t*>(ib + D.o_arp);
+    uint16_t* acol = reinterpret_cast<uint16_t*>(ib + D.o_acol);
+    if (q == 0) arp[0] = 0;
+    arp[q + 1] = off + c;
+    auto col = [&](uint32_t xx, uint32_t yy) -> uint32_t {
+        if (xx >= G.x0 && xx < G.x1 && yy >= G.y0 && yy < G.y1) return (yy - G.y0) * tw + (xx - G.x0);
+        if (yy + 1 == G.y0) return D.n_own + (xx - G.x0);
+        if (yy == G.y1) return D.n_own + nb + th * per_row + (xx - G.x0);
+        return D.n_own + nb + (yy - G.y0) * per_row + (xx + 1 == G.x0 ? 0u : (L ? 1u : 0u));
+    };
+    uint32_t p = off;
+    if (y > 0) acol[p++] = (uint16_t)col(x, y - 1);
+    if (x > 0) acol[p++] = (uint16_t)col(x - 1, y);
+    acol[p++] = (uint16_t)q;
+    if (x + 1 < B) acol[p++] = (uint16_t)col(x + 1, y);
+    if (y + 1 < ny) acol[p++] = (uint16_t)col(x, y + 1);
+    return true;
+}
+
+// Dependencies of extended row t of the lower (lo) or upper set, after the
+// halos are written: {first, second} local indices in column order.
+B2S_TILE_HD inline void grid5_build_dep(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K,
+                                        bool lo, uint32_t t, uint8_t* ib)
+{
+    const uint32_t tw = G.x1 - G.x0;
+    uint32_t x, y;
+    if (t < D.n_own)
+    {
+        x = G.x0 + t % tw;
+        y = G.y0 + t / tw;
+    }
+    else
+    {
+        const uint32_t g = reinterpret_cast<const uint32_t*>(ib + (lo ? D.o_lhalo : D.o_uhalo))[t - D.n_own];
+        x = g % B;
+        y = g / B;
+    }
+    uint32_t s[2] = {kTileNoDep, kTileNoDep}, e = 0;
+    if (lo)
+    {
+        if (y > 0) s[e++] = grid5_local(D, G, B, ny, K, true, x, y - 1);
+        if (x > 0) s[e++] = grid5_local(D, G, B, ny, K, true, x - 1, y);
+    }
+    else
+    {
+        if (x + 1 < B) s[e++] = grid5_local(D, G, B, ny, K, false, x + 1, y);
+        if (y + 1 < ny) s[e++] = grid5_local(D, G, B, ny, K, false, x, y + 1);
+    }
+    reinterpret_cast<uint32_t*>(ib + (lo ? D.o_ldeps : D.o_udeps))[t] = s[0] | (s[1] << 16);
+}
+
 }  // namespace b2s

@@ -251,6 +251,21 @@ static void check_grid5(const char* name, uint32_t N, uint32_t M, int k, int sms
                   "%s tile %u part %d: build failed", name, t, part);
     }
     CHECK(blob == T.idx, "%s: index blobs differ", name);
+    // the element-at-a-time builder (one device thread per element, then the
+    // dependencies once the halos are in place) in reverse element order
+    std::vector<uint8_t> blob2(G.ibytes, 0);
+    for (uint32_t t = 0; t < G.ntiles; ++t)
+    {
+        const TileDesc& D = G.desc[t];
+        uint8_t* ib = blob2.data() + D.ibase;
+        const uint32_t ne = grid5_elements(D, geom[t], N, M, (uint32_t)k);
+        for (uint32_t e = ne; e-- > 0;)
+            CHECK(grid5_build_elem(D, geom[t], N, M, (uint32_t)k, e, ib), "%s tile %u element %u: build failed", name,
+                  t, e);
+        for (uint32_t r = D.n_el; r-- > 0;) grid5_build_dep(D, geom[t], N, M, (uint32_t)k, true, r, ib);
+        for (uint32_t r = D.n_eu; r-- > 0;) grid5_build_dep(D, geom[t], N, M, (uint32_t)k, false, r, ib);
+    }
+    CHECK(blob2 == T.idx, "%s: element-wise index blobs differ", name);
     // a pattern that is not a 5-point grid is not taken for one
     Pattern Q = P;
     if (Q.lci.size() > 2) std::swap(Q.lci[Q.lrp[N + 1]], Q.lci[Q.lrp[N + 1] + 1]);
