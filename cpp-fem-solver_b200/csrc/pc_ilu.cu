@@ -852,6 +852,7 @@ struct PcIC0 final : PcImpl
     // and A's pattern matched it
     bool tiles_ready = false;
     uint32_t tile_n = 0, tile_count = 0, tile_Q = 0, tile_smem = 0, tile_work = 0, tile_ystride = 0;
+    bool tile_fused = false;  // the forward set grown from the upper set: two all-reduces per iteration
     DBuf<TileDesc> tile_desc;
     DBuf<uint8_t> tile_idx, tile_vals;
     DBuf<unsigned long long> tile_slots;
@@ -873,7 +874,7 @@ struct PcIC0 final : PcImpl
             B2S_CUDA(cudaMemsetAsync(tile_idx.p, 0, tile_idx.bytes(), ctx->stream));  // the segments' padding
             geom = upload(ctx, *grid5);
             B2S_LAUNCH(ctx, k_tile_build_grid5, P.ntiles, kThreads, 0, tile_desc.p, geom.p, tile_idx.p, B, ny, P.k,
-                       bad.p);
+                       P.fused, bad.p);
         }
         else
             tile_idx = upload(ctx, P.idx.data(), P.idx.size());
@@ -891,16 +892,18 @@ struct PcIC0 final : PcImpl
         tile_Q = P.Q;
         tile_smem = P.smem;
         tile_work = P.work;
-        tile_ystride = tile_align16(4ull * P.max_ext) / 4;
+        tile_ystride = ::b2s::tile_ystride(P.max_ext);
+        tile_fused = P.fused;
         tiles_ready = true;
     }
 
-    template <uint32_t Q>
+    template <uint32_t Q, bool FUSED>
     bool launch_tiles(b2s_ctx* ctx, PcgTileArgs& a)
     {
-        B2S_CUDA(cudaFuncSetAttribute(k_pcg_tile<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tile_smem));
+        B2S_CUDA(cudaFuncSetAttribute(k_pcg_tile<Q, FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)tile_smem));
         void* params[] = {&a};
-        const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_tile<Q>, dim3(tile_count),
+        const cudaError_t e = cudaLaunchCooperativeKernel((const void*)k_pcg_tile<Q, FUSED>, dim3(tile_count),
                                                           dim3(kTileThreads), params, tile_smem, ctx->stream);
         if (e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported)
         {
@@ -942,12 +945,16 @@ struct PcIC0 final : PcImpl
         a.err = reinterpret_cast<int*>(pcg_ctl.p + 1);
         a.stall_window = stall_window;
         bool ok = false;
-        switch (tile_Q)
+        switch (tile_Q * 2 + (tile_fused ? 1 : 0))
         {
-            case 1: ok = launch_tiles<1>(ctx, a); break;
-            case 2: ok = launch_tiles<2>(ctx, a); break;
-            case 3: ok = launch_tiles<3>(ctx, a); break;
-            case 4: ok = launch_tiles<4>(ctx, a); break;
+            case 2: ok = launch_tiles<1, false>(ctx, a); break;
+            case 3: ok = launch_tiles<1, true>(ctx, a); break;
+            case 4: ok = launch_tiles<2, false>(ctx, a); break;
+            case 5: ok = launch_tiles<2, true>(ctx, a); break;
+            case 6: ok = launch_tiles<3, false>(ctx, a); break;
+            case 7: ok = launch_tiles<3, true>(ctx, a); break;
+            case 8: ok = launch_tiles<4, false>(ctx, a); break;
+            case 9: ok = launch_tiles<4, true>(ctx, a); break;
             default: return false;
         }
         if (!ok) return false;

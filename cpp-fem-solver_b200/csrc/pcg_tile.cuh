@@ -73,18 +73,20 @@ __device__ __forceinline__ unsigned long long ld_relaxed_gpu_u64(const unsigned 
 
 __device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
-// Thread 0 holds this tile's partial `part`.  Publishes it for `epoch`, waits
-// for every tile's and returns their sum in thread 0 (tile order, the same
-// association in every CTA, so the same bits); false in every thread, with
-// B2S_TIMEOUT recorded, when a wait gives up.  Each tile's two words sit alone
-// in a 128-byte line (kTileSlotStride words apart), and thread b < ntiles
-// polls tile b's words only until they carry the epoch, so a tile that has
-// arrived is not read again and the polls of all CTAs spread over as many
-// lines as tiles.
+// Thread 0 holds this tile's NV partials `part`.  Publishes them for `epoch`,
+// waits for every tile's and returns their sums in thread 0 (tile order, the
+// same association in every CTA, so the same bits); false in every thread,
+// with B2S_TIMEOUT recorded, when a wait gives up.  Each tile's 2 NV words
+// ({epoch, 32 value bits} per half) sit alone in a 128-byte line
+// (kTileSlotStride words apart), and thread b < ntiles polls tile b's words
+// only until they carry the epoch, so a tile that has arrived is not read
+// again and the polls of all CTAs spread over as many lines as tiles.
+template <int NV>
 __device__ __forceinline__ bool tile_allreduce(unsigned long long* slots, uint32_t tile, uint32_t ntiles,
-                                               uint32_t epoch, double part, double& sum, int* err,
-                                               double* s_part, int* s_fail)
+                                               uint32_t epoch, const double (&part)[NV], double (&sum)[NV], int* err,
+                                               double (*s_part)[kTileMaxTiles], int* s_fail)
 {
+    static_assert(2 * NV <= (int)kTileSlotStride, "slot line");
     const uint32_t tid = threadIdx.x;
     if (tid == 0)
     {
@@ -92,20 +94,28 @@ __device__ __forceinline__ bool tile_allreduce(unsigned long long* slots, uint32
         // block_reduce) become visible before the words that announce them
         fence_acq_rel_gpu();
         const unsigned long long e = (unsigned long long)epoch << 32;
-        const unsigned long long b = (unsigned long long)__double_as_longlong(part);
-        st_relaxed_gpu_u64(&slots[(size_t)kTileSlotStride * tile], e | (b & 0xffffffffull));
-        st_relaxed_gpu_u64(&slots[(size_t)kTileSlotStride * tile + 1], e | (b >> 32));
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+        {
+            const unsigned long long b = (unsigned long long)__double_as_longlong(part[v]);
+            st_relaxed_gpu_u64(&slots[(size_t)kTileSlotStride * tile + 2 * v], e | (b & 0xffffffffull));
+            st_relaxed_gpu_u64(&slots[(size_t)kTileSlotStride * tile + 2 * v + 1], e | (b >> 32));
+        }
     }
     if (tid < ntiles)
     {
         const unsigned long long* w = &slots[(size_t)kTileSlotStride * tid];
-        unsigned long long w0 = 0, w1 = 0;
+        unsigned long long wd[2 * NV];
         bool seen = false;
         for (unsigned polls = 0; polls < kGridBarrierPolls && !seen; ++polls)
         {
-            w0 = ld_relaxed_gpu_u64(w);
-            w1 = ld_relaxed_gpu_u64(w + 1);
-            seen = (uint32_t)(w0 >> 32) == epoch && (uint32_t)(w1 >> 32) == epoch;
+            seen = true;
+#pragma unroll
+            for (int q = 0; q < 2 * NV; ++q)
+            {
+                wd[q] = ld_relaxed_gpu_u64(w + q);
+                seen &= (uint32_t)(wd[q] >> 32) == epoch;
+            }
         }
         if (!seen)
         {
@@ -115,62 +125,100 @@ __device__ __forceinline__ bool tile_allreduce(unsigned long long* slots, uint32
         // the words seen carry the other CTAs' fenced writes: this fence (then
         // the block barrier below) orders the CTA's later reads after them
         fence_acq_rel_gpu();
-        s_part[tid] = __longlong_as_double((long long)(((w1 & 0xffffffffull) << 32) | (w0 & 0xffffffffull)));
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+            s_part[v][tid] =
+                __longlong_as_double((long long)(((wd[2 * v + 1] & 0xffffffffull) << 32) | (wd[2 * v] & 0xffffffffull)));
     }
     __syncthreads();
     if (tid < 32)
     {
-        double t = 0.0;
-        for (uint32_t b = tid; b < ntiles; b += 32) t += s_part[b];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-        sum = t;
+        for (int v = 0; v < NV; ++v)
+        {
+            double t = 0.0;
+            for (uint32_t b = tid; b < ntiles; b += 32) t += s_part[v][b];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            sum[v] = t;
+        }
     }
     return *s_fail == 0;
 }
 
 // k + 1 passes over the extended set; rows of layers 0..k-s at pass s.
-// Returns the buffer holding pass k.
+// Returns the buffer holding pass k.  Branch-free over the thread's Q rows:
+// every row is evaluated at every pass and only rows t < cnt[k - s] are
+// stored.  An absent dependency names the spare slot `dummy` past the set,
+// which holds +0 in both buffers, with a coefficient of +0, so that
+// sum - 0 * 0 leaves sum unchanged (its sign included) and the stored rows
+// equal the global sweep definition bit for bit.
 template <uint32_t Q>
 __device__ __forceinline__ const float* tile_sweeps(int k, const uint16_t* cnt, const uint32_t (&dep)[Q],
                                                     const float2 (&val)[Q], const float (&di)[Q],
-                                                    const float (&rr)[Q], float* y0, float* y1)
+                                                    const float (&rr)[Q], float* y0, float* y1, uint32_t dummy)
 {
     constexpr uint32_t NT = kTileThreads;
+    if (threadIdx.x == 0)
+    {
+        y0[dummy] = 0.f;
+        y1[dummy] = 0.f;
+    }
     for (int s = 0; s <= k; ++s)
     {
         const float* yin = (s & 1) ? y0 : y1;
         float* yout = (s & 1) ? y1 : y0;
         const uint32_t t1 = cnt[k - s];
+        float out[Q];
+        if (s == 0)
+        {
+#pragma unroll
+            for (uint32_t q = 0; q < Q; ++q) out[q] = rr[q] * di[q];
+        }
+        else
+        {
+            float a0[Q], a1[Q];
+#pragma unroll
+            for (uint32_t q = 0; q < Q; ++q)
+            {
+                a0[q] = yin[dep[q] & 0xFFFFu];
+                a1[q] = yin[dep[q] >> 16];
+            }
+#pragma unroll
+            for (uint32_t q = 0; q < Q; ++q)
+            {
+                float sum = rr[q];
+                sum -= val[q].x * a0[q];
+                sum -= val[q].y * a1[q];
+                out[q] = sum * di[q];
+            }
+        }
 #pragma unroll
         for (uint32_t q = 0; q < Q; ++q)
         {
             const uint32_t t = threadIdx.x + NT * q;
-            if (t < t1)
-            {
-                float sum = rr[q];
-                if (s > 0)
-                {
-                    const uint32_t d0 = dep[q] & 0xFFFFu, d1 = dep[q] >> 16;
-                    if (d0 != kTileNoDep) sum -= val[q].x * yin[d0];
-                    if (d1 != kTileNoDep) sum -= val[q].y * yin[d1];
-                }
-                yout[t] = sum * di[q];
-            }
+            if (t < t1) yout[t] = out[q];
         }
         __syncthreads();
     }
     return (k & 1) ? y1 : y0;
 }
 
-template <uint32_t Q>
+// a row's two dependencies with the absent ones (kTileNoDep) sent to the spare slot
+__device__ __forceinline__ uint32_t tile_dep_slots(uint32_t w, uint32_t dummy)
+{
+    const uint32_t d0 = w & 0xFFFFu, d1 = w >> 16;
+    return (d0 == kTileNoDep ? dummy : d0) | ((d1 == kTileNoDep ? dummy : d1) << 16);
+}
+
+template <uint32_t Q, bool FUSED>
 __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
 {
     constexpr uint32_t NT = kTileThreads;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ KState sst;
     __shared__ int s_fail;
-    __shared__ double s_part[kTileMaxTiles];
+    __shared__ double s_part[2][kTileMaxTiles];
     __shared__ double s_best;
     __shared__ int s_best_at;
     const uint32_t tile = blockIdx.x, ntiles = a.ntiles, tid = threadIdx.x;
@@ -217,6 +265,31 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
     float* const y0 = reinterpret_cast<float*>(smem + a.work);
     float* const y1 = y0 + a.ystride;
     double* const pe = reinterpret_cast<double*>(smem + a.work);  // phase 1 only (aliases y0 / y1)
+    const uint32_t lbase = s_lcnt[0];  // the lower set's layer 0: the owned rows, or (fused) the upper set
+    const uint32_t dummy = a.ystride - 1;  // the sweeps' spare slot (past every set)
+
+    // the slot regions of the iteration's all-reduces (each ntiles lines)
+    unsigned long long* const slot_alpha = a.slots;
+    unsigned long long* const slot_rr = a.slots + (size_t)kTileSlotStride * ntiles;
+    unsigned long long* const slot_rz = a.slots + (size_t)(FUSED ? 1 : 2) * kTileSlotStride * ntiles;
+
+    // convergence test on r.r (thread 0), with the learned solve's stall guard
+    auto converge = [&](double rr) {
+        if (!pcg_check_converged(&sst, rr) && a.stall_window > 0)
+        {
+            if (sst.relres < 0.5 * s_best)
+            {
+                s_best = sst.relres;
+                s_best_at = sst.it;
+            }
+            else if (sst.it - s_best_at >= a.stall_window)
+            {
+                sst.stalled = 1;
+                sst.iters = sst.it + 1;
+                finish(&sst, B2S_OK);
+            }
+        }
+    };
 
     uint32_t epoch = 0;
     int parity = 0;
@@ -272,26 +345,26 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
                 }
             }
             block_reduce<1, NT>(acc);
-            double tot;
-            if (!tile_allreduce(a.slots, tile, ntiles, ++epoch, acc[0], tot, a.err, s_part, &s_fail)) break;
-            if (tid == 0) pcg_alpha(&sst, tot);
+            double tot[1];
+            if (!tile_allreduce<1>(slot_alpha, tile, ntiles, ++epoch, acc, tot, a.err, s_part, &s_fail)) break;
+            if (tid == 0) pcg_alpha(&sst, tot[0]);
             __syncthreads();
             if (sst.done) break;
         }
         // ---- 2. forward sweeps on r = r_old - alpha Ap; x, r; r.r
+        double rr_acc = 0.0;
         {
             const double alpha = sst.alpha;
             uint32_t dep[Q];
             float2 val[Q];
             float di[Q], rr[Q];
-            double acc[1] = {0.0};
 #pragma unroll
             for (uint32_t q = 0; q < Q; ++q)
             {
                 const uint32_t t = tid + NT * q;
                 const bool in = t < n_el;
-                const uint32_t g = in ? (t < n_own ? owned[t] : lhalo[t - n_own]) : 0u;
-                dep[q] = in ? ldeps[t] : 0xFFFFFFFFu;
+                const uint32_t g = !in ? 0u : t < n_own ? owned[t] : t < lbase ? uhalo[t - n_own] : lhalo[t - lbase];
+                dep[q] = tile_dep_slots(in ? ldeps[t] : 0xFFFFFFFFu, dummy);
                 val[q] = in ? lvals[t] : make_float2(0.f, 0.f);
                 di[q] = in ? ldinv[t] : 0.f;
                 const double rv = in ? __ldcg(&rold[g]) - alpha * __ldcg(&a.Ap[g]) : 0.0;
@@ -299,43 +372,29 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
                 if (t < n_own)  // the owned rows' r, r.r and x now, before the sweeps
                 {
                     rnew[g] = rv;
-                    acc[0] += rv * rv;
+                    rr_acc += rv * rv;
                     xv[q] += alpha * pv[q];
                 }
             }
-            yf = tile_sweeps<Q>(a.k, s_lcnt, dep, val, di, rr, y0, y1);
+            yf = tile_sweeps<Q>(a.k, s_lcnt, dep, val, di, rr, y0, y1, dummy);
+            if constexpr (!FUSED)
+            {
+                // other tiles read y at this tile's rows after the grid-wide exchange
 #pragma unroll
-            for (uint32_t q = 0; q < Q; ++q)
-            {
-                const uint32_t t = tid + NT * q;
-                if (t < n_own) a.y32[owned[t]] = yf[t];
-            }
-            block_reduce<1, NT>(acc);
-            double tot;
-            if (!tile_allreduce(a.slots + (size_t)kTileSlotStride * ntiles, tile, ntiles, ++epoch, acc[0], tot, a.err,
-                                s_part, &s_fail))
-                break;
-            if (tid == 0)
-            {
-                if (!pcg_check_converged(&sst, tot) && a.stall_window > 0)
+                for (uint32_t q = 0; q < Q; ++q)
                 {
-                    if (sst.relres < 0.5 * s_best)
-                    {
-                        s_best = sst.relres;
-                        s_best_at = sst.it;
-                    }
-                    else if (sst.it - s_best_at >= a.stall_window)
-                    {
-                        sst.stalled = 1;
-                        sst.iters = sst.it + 1;
-                        finish(&sst, B2S_OK);
-                    }
+                    const uint32_t t = tid + NT * q;
+                    if (t < n_own) a.y32[owned[t]] = yf[t];
                 }
+                double acc[1] = {rr_acc}, tot[1];
+                block_reduce<1, NT>(acc);
+                if (!tile_allreduce<1>(slot_rr, tile, ntiles, ++epoch, acc, tot, a.err, s_part, &s_fail)) break;
+                if (tid == 0) converge(tot[0]);
+                __syncthreads();
+                if (sst.done) break;
             }
-            __syncthreads();
-            if (sst.done) break;
         }
-        // ---- 3. backward sweeps on y; z; r.z and beta
+        // ---- 3. backward sweeps on y; z; r.z and beta (fused: with r.r and the test)
         {
             uint32_t dep[Q];
             float2 val[Q];
@@ -345,15 +404,18 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
             {
                 const uint32_t t = tid + NT * q;
                 const bool in = t < n_eu;
-                const uint32_t g = in ? (t < n_own ? owned[t] : uhalo[t - n_own]) : 0u;
-                dep[q] = in ? udeps[t] : 0xFFFFFFFFu;
+                dep[q] = tile_dep_slots(in ? udeps[t] : 0xFFFFFFFFu, dummy);
                 val[q] = in ? uvals[t] : make_float2(0.f, 0.f);
                 di[q] = in ? udinv[t] : 0.f;
-                // (owned rows: this thread's own forward results, read before its sweeps write)
-                rr[q] = t < n_own ? yf[t] : in ? __ldcg(&a.y32[g]) : 0.f;
+                // this thread's own forward results (read before its sweeps write):
+                // every row of the upper set when fused, else the owned rows
+                if constexpr (FUSED)
+                    rr[q] = in ? yf[t] : 0.f;
+                else
+                    rr[q] = t < n_own ? yf[t] : in ? __ldcg(&a.y32[uhalo[t - n_own]]) : 0.f;
             }
-            const float* yk = tile_sweeps<Q>(a.k, s_ucnt, dep, val, di, rr, y0, y1);
-            double acc[1] = {0.0};
+            const float* yk = tile_sweeps<Q>(a.k, s_ucnt, dep, val, di, rr, y0, y1, dummy);
+            double acc[2] = {0.0, 0.0};
 #pragma unroll
             for (uint32_t q = 0; q < Q; ++q)
             {
@@ -363,15 +425,28 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
                     const uint32_t g = owned[t];
                     const double zi = (double)yk[t];
                     a.z[g] = zi;
-                    acc[0] += rnew[g] * zi;  // (this thread's own store of phase 2)
+                    acc[1] += rnew[g] * zi;  // (this thread's own store of phase 2)
                 }
             }
-            block_reduce<1, NT>(acc);
-            double tot;
-            if (!tile_allreduce(a.slots + 2ull * kTileSlotStride * ntiles, tile, ntiles, ++epoch, acc[0], tot, a.err,
-                                s_part, &s_fail))
-                break;
-            if (tid == 0) pcg_next(&sst, tot);
+            if constexpr (FUSED)
+            {
+                acc[0] = rr_acc;
+                double tot[2];
+                block_reduce<2, NT>(acc);
+                if (!tile_allreduce<2>(slot_rz, tile, ntiles, ++epoch, acc, tot, a.err, s_part, &s_fail)) break;
+                if (tid == 0)
+                {
+                    converge(tot[0]);
+                    if (!sst.done) pcg_next(&sst, tot[1]);
+                }
+            }
+            else
+            {
+                double one[1] = {acc[1]}, tot[1];
+                block_reduce<1, NT>(one);
+                if (!tile_allreduce<1>(slot_rz, tile, ntiles, ++epoch, one, tot, a.err, s_part, &s_fail)) break;
+                if (tid == 0) pcg_next(&sst, tot[0]);
+            }
             __syncthreads();
         }
         parity ^= 1;
@@ -392,7 +467,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pcg_tile(PcgTileArgs a)
 __global__ void __launch_bounds__(kThreads) k_tile_build_grid5(const TileDesc* __restrict__ desc,
                                                                const TileGeom* __restrict__ geom,
                                                                uint8_t* __restrict__ idx, uint32_t B, uint32_t ny,
-                                                               uint32_t K, int* bad)
+                                                               uint32_t K, bool fused, int* bad)
 {
     __shared__ TileDesc D;
     __shared__ TileGeom G;
@@ -403,12 +478,12 @@ __global__ void __launch_bounds__(kThreads) k_tile_build_grid5(const TileDesc* _
     }
     __syncthreads();
     uint8_t* ib = idx + D.ibase;
-    const uint32_t ne = grid5_elements(D, G, B, ny, K);
+    const uint32_t ne = grid5_elements(D, G, B, ny, K, fused);
     for (uint32_t e = threadIdx.x; e < ne; e += blockDim.x)
-        if (!grid5_build_elem(D, G, B, ny, K, e, ib)) atomicExch(bad, 1);
+        if (!grid5_build_elem(D, G, B, ny, K, fused, e, ib)) atomicExch(bad, 1);
     __syncthreads();  // the halos, read back below
-    for (uint32_t t = threadIdx.x; t < D.n_el; t += blockDim.x) grid5_build_dep(D, G, B, ny, K, true, t, ib);
-    for (uint32_t t = threadIdx.x; t < D.n_eu; t += blockDim.x) grid5_build_dep(D, G, B, ny, K, false, t, ib);
+    for (uint32_t t = threadIdx.x; t < D.n_el; t += blockDim.x) grid5_build_dep(D, G, B, ny, K, true, fused, t, ib);
+    for (uint32_t t = threadIdx.x; t < D.n_eu; t += blockDim.x) grid5_build_dep(D, G, B, ny, K, false, fused, t, ib);
 }
 
 // Fills the value blobs after factorisation: A's values for the owned rows
@@ -458,9 +533,12 @@ __global__ void k_tile_pack(const TileDesc* __restrict__ desc, const uint8_t* __
     // one triangle's extended rows: values and reciprocal from the band slots;
     // rows of layers below k (computed by the sweeps) must have every factor
     // entry planned (a missing entry shows as a planned "none" over a band slot)
-    auto tri = [&](uint32_t ne, uint32_t below_k, const uint32_t* halo, const uint32_t* deps, const uint16_t* off,
-                   const float* val, const float* dinv, float2* outv, float* outd, bool lower) {
-        auto glob = [&](uint32_t t) { return t < D.n_own ? owned[t] : halo[t - D.n_own]; };
+    // (a fused plan's lower set: the upper set's rows first, then its own halo from base on)
+    auto tri = [&](uint32_t ne, uint32_t below_k, uint32_t base, const uint32_t* halo, const uint32_t* deps,
+                   const uint16_t* off, const float* val, const float* dinv, float2* outv, float* outd, bool lower) {
+        auto glob = [&](uint32_t t) {
+            return t < D.n_own ? owned[t] : t < base ? uhalo[t - D.n_own] : halo[t - base];
+        };
         for (uint32_t t = threadIdx.x; t < ne; t += blockDim.x)
         {
             const uint32_t g = glob(t);
@@ -475,15 +553,18 @@ __global__ void k_tile_pack(const TileDesc* __restrict__ desc, const uint8_t* __
                     const uint32_t j = glob(dp[e]);
                     if (o != (lower ? g - j : j - g)) atomicExch(bad, 1);
                 }
-                else if (o != 0 && t < below_k)
-                    atomicExch(bad, 1);
+                else
+                {
+                    if (o != 0 && t < below_k) atomicExch(bad, 1);
+                    v2[e] = 0.f;  // (read against the sweeps' +0 spare slot; layer-k rows never read it)
+                }
             }
             outv[t] = make_float2(v2[0], v2[1]);
             outd[t] = dinv[g];
         }
     };
-    tri(D.n_el, k > 0 ? D.lcnt[k - 1] : 0u, lhalo, ldeps, loff, lval, ldinv, lv, ld, true);
-    tri(D.n_eu, k > 0 ? D.ucnt[k - 1] : 0u, uhalo, udeps, uoff, uval, udinv, uv, ud, false);
+    tri(D.n_el, k > 0 ? D.lcnt[k - 1] : 0u, D.lcnt[0], lhalo, ldeps, loff, lval, ldinv, lv, ld, true);
+    tri(D.n_eu, k > 0 ? D.ucnt[k - 1] : 0u, D.n_own, uhalo, udeps, uoff, uval, udinv, uv, ud, false);
 }
 
 }  // namespace b2s

@@ -63,13 +63,20 @@ struct TileDesc
     uint32_t o_aval, o_lvals, o_uvals, o_ldinv, o_udinv;
     // index blob: owned rows, halos (global rows), dependencies (2 x u16 per row), A's offsets and columns
     uint32_t o_owned, o_lhalo, o_ldeps, o_uhalo, o_udeps, o_ahalo, o_arp, o_acol;
-    uint16_t lcnt[kTileMaxSweeps + 1];  // rows of layers 0..d of the lower triangle's set
+    // rows of layers 0..d of the lower triangle's set; layer 0 is the owned
+    // rows, or the whole upper set in a fused plan (rows n_own..lcnt[0]-1 are
+    // then the upper halo, and o_lhalo lists the rows past lcnt[0])
+    uint16_t lcnt[kTileMaxSweeps + 1];
     uint16_t ucnt[kTileMaxSweeps + 1];
 };
 
 struct TilePlan
 {
     bool ok = false;
+    // fused: the forward (lower) set is grown from the upper set instead of the
+    // owned rows, so the backward sweeps find all their right-hand sides in the
+    // CTA and one grid-wide exchange per iteration goes away
+    bool fused = false;
     uint32_t n = 0, ntiles = 0, k = 0, Q = 0;
     uint32_t tiles_x = 0, tiles_y = 0, B = 0;
     uint32_t max_ext = 0, max_own = 0, max_ae = 0;
@@ -98,9 +105,11 @@ inline void strict_lower(uint32_t n, const uint32_t* rp, const uint32_t* ci, std
 }
 
 // work buffers after the blobs: two FP32 sweep vectors, or the staged FP64 p
+// (each sweep vector holds the set and one spare slot: tile_ystride)
+inline uint32_t tile_ystride(uint32_t max_ext) { return tile_align16(4ull * (max_ext + 1)) / 4; }
 inline uint32_t tile_work_bytes(uint32_t max_ext, uint32_t max_ae)
 {
-    return std::max<uint32_t>(2 * tile_align16(4ull * max_ext), tile_align16(8ull * max_ae));
+    return std::max<uint32_t>(8 * tile_ystride(max_ext), tile_align16(8ull * max_ae));
 }
 
 struct TileBuild
@@ -180,10 +189,13 @@ inline bool tile_extend(const std::vector<uint32_t>& own, const uint32_t* rp, co
 // per CTA; workers host threads.
 inline TilePlan plan_tiles_shape(uint32_t n, const uint32_t* lo_rp, const uint32_t* lo_ci, const uint32_t* up_rp,
                                  const uint32_t* up_ci, int k, uint64_t B, uint64_t bx, uint64_t by,
-                                 uint32_t smem_limit, unsigned workers);
+                                 uint32_t smem_limit, unsigned workers, bool fused);
 
+// The fused layout is tried first (fused_first), then the separate one, for
+// the best 2-D block shape; strips (separate sets) are the last resort.
 inline TilePlan plan_tiles(uint32_t n, const uint32_t* lo_rp, const uint32_t* lo_ci, const uint32_t* up_rp,
-                           const uint32_t* up_ci, int k, int sm_count, uint32_t smem_limit, unsigned workers)
+                           const uint32_t* up_ci, int k, int sm_count, uint32_t smem_limit, unsigned workers,
+                           bool fused_first = true)
 {
     TilePlan P;
     P.n = n;
@@ -209,11 +221,15 @@ inline TilePlan plan_tiles(uint32_t n, const uint32_t* lo_rp, const uint32_t* lo
             by = ty;
         }
     }
-    P = plan_tiles_shape(n, lo_rp, lo_ci, up_rp, up_ci, k, B, bx, by, smem_limit, workers);
-    if (!P.ok && bx != 1)  // the blocks' halos outgrew a CTA (dependencies that cross block columns): strips
+    for (int f = fused_first ? 1 : 0; f >= 0; --f)
+    {
+        P = plan_tiles_shape(n, lo_rp, lo_ci, up_rp, up_ci, k, B, bx, by, smem_limit, workers, f != 0);
+        if (P.ok) return P;
+    }
+    if (bx != 1)  // the blocks' halos outgrew a CTA (dependencies that cross block columns): strips
     {
         const uint64_t B1 = std::max<uint64_t>(1, (n + (uint64_t)sm_count - 1) / (uint64_t)sm_count);
-        P = plan_tiles_shape(n, lo_rp, lo_ci, up_rp, up_ci, k, B1, 1, (n + B1 - 1) / B1, smem_limit, workers);
+        P = plan_tiles_shape(n, lo_rp, lo_ci, up_rp, up_ci, k, B1, 1, (n + B1 - 1) / B1, smem_limit, workers, false);
     }
     return P;
 }
@@ -222,11 +238,12 @@ inline TilePlan plan_tiles(uint32_t n, const uint32_t* lo_rp, const uint32_t* lo
 // grid rows, row i at (i mod B, i div B).
 inline TilePlan plan_tiles_shape(uint32_t n, const uint32_t* lo_rp, const uint32_t* lo_ci, const uint32_t* up_rp,
                                  const uint32_t* up_ci, int k, uint64_t B, uint64_t bx, uint64_t by,
-                                 uint32_t smem_limit, unsigned workers)
+                                 uint32_t smem_limit, unsigned workers, bool fused)
 {
     TilePlan P;
     P.n = n;
     P.k = (uint32_t)k;
+    P.fused = fused;
     const uint64_t ny = (n + B - 1) / B;
     const uint64_t w = (B + bx - 1) / bx, h = (ny + by - 1) / by;
     const uint32_t tiles_x = (uint32_t)((B + w - 1) / w), tiles_y = (uint32_t)((ny + h - 1) / h);
@@ -248,8 +265,8 @@ inline TilePlan plan_tiles_shape(uint32_t n, const uint32_t* lo_rp, const uint32
             lc.assign(n, 0);
         }
         TileBuild& T = tb[t];
-        if (!tile_extend(T.own, lo_rp, lo_ci, k, 3 * t, mk, lc, T.el, T.ldeps, T.lcnt)) return;
         if (!tile_extend(T.own, up_rp, up_ci, k, 3 * t + 1, mk, lc, T.eu, T.udeps, T.ucnt)) return;
+        if (!tile_extend(fused ? T.eu : T.own, lo_rp, lo_ci, k, 3 * t, mk, lc, T.el, T.ldeps, T.lcnt)) return;
         // the SpMV's columns: owned rows' [lower strict, diagonal, upper strict]
         const uint32_t stamp = 3 * t + 2;
         T.ae = T.own;
@@ -319,7 +336,7 @@ inline TilePlan plan_tiles_shape(uint32_t n, const uint32_t* lo_rp, const uint32
         D.vbytes = o;
         o = 0;
         D.o_owned = seg(4ull * D.n_own);
-        D.o_lhalo = seg(4ull * (D.n_el - D.n_own));
+        D.o_lhalo = seg(4ull * (D.n_el - T.lcnt[0]));  // rows of the lower set past its layer 0
         D.o_ldeps = seg(4ull * D.n_el);
         D.o_uhalo = seg(4ull * (D.n_eu - D.n_own));
         D.o_udeps = seg(4ull * D.n_eu);
@@ -355,7 +372,7 @@ inline TilePlan plan_tiles_shape(uint32_t n, const uint32_t* lo_rp, const uint32
             if (bytes) std::memcpy(b + off, src, bytes);
         };
         put(D.o_owned, T.own.data(), 4 * T.own.size());
-        put(D.o_lhalo, T.el.data() + D.n_own, 4 * (size_t)(D.n_el - D.n_own));
+        put(D.o_lhalo, T.el.data() + D.lcnt[0], 4 * (size_t)(D.n_el - D.lcnt[0]));
         put(D.o_ldeps, T.ldeps.data(), 4 * T.ldeps.size());
         put(D.o_uhalo, T.eu.data() + D.n_own, 4 * (size_t)(D.n_eu - D.n_own));
         put(D.o_udeps, T.udeps.data(), 4 * T.udeps.size());
@@ -382,10 +399,10 @@ inline TilePlan plan_tiles_shape(uint32_t n, const uint32_t* lo_rp, const uint32
 // the box [x0 - k, x1) x [y0 - k, y1) at distance dL = max(0, x0 - x) +
 // max(0, y0 - y) <= k, layer dL; the upper set mirrors it; the SpMV's columns
 // are the block and its one-wide ring.  plan_tiles_grid5 lays the blobs out
-// from these counts alone (no pass over the matrix), and grid5_build_part
-// writes a tile's index blob -- on the device at set-up, one thread per part
-// of a tile, and on the CPU in the tests, where it must equal plan_tiles'
-// output byte for byte.
+// from these counts alone (no pass over the matrix), and grid5_build_elem /
+// grid5_build_dep write a tile's index blob one element at a time -- on the
+// device at set-up, and on the CPU in the tests, where it must equal
+// plan_tiles' output byte for byte.
 
 struct TileGeom
 {
@@ -418,12 +435,42 @@ B2S_TILE_HD inline uint32_t grid5_layer(uint32_t d, uint32_t w, uint32_t h, uint
     return c;
 }
 
+inline TilePlan plan_tiles_grid5_mode(uint32_t n, uint32_t B, int k, int sm_count, uint32_t smem_limit,
+                                      std::vector<TileGeom>& geom, bool fused);
+
+// the fused layout first, then the separate one (as plan_tiles)
 inline TilePlan plan_tiles_grid5(uint32_t n, uint32_t B, int k, int sm_count, uint32_t smem_limit,
-                                 std::vector<TileGeom>& geom)
+                                 std::vector<TileGeom>& geom, bool fused_first = true)
+{
+    TilePlan P;
+    for (int f = fused_first ? 1 : 0; f >= 0; --f)
+    {
+        P = plan_tiles_grid5_mode(n, B, k, sm_count, smem_limit, geom, f != 0);
+        if (P.ok) return P;
+    }
+    return P;
+}
+
+// the block grown by k up and right (clipped): a fused plan's lower set is
+// this block's lower set with the upper set (its staircase) as layer 0
+B2S_TILE_HD inline TileGeom grid5_fwd_block(const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K, bool fused)
+{
+    TileGeom F = G;
+    if (fused)
+    {
+        F.x1 = B < G.x1 + K ? B : G.x1 + K;
+        F.y1 = ny < G.y1 + K ? ny : G.y1 + K;
+    }
+    return F;
+}
+
+inline TilePlan plan_tiles_grid5_mode(uint32_t n, uint32_t B, int k, int sm_count, uint32_t smem_limit,
+                                      std::vector<TileGeom>& geom, bool fused)
 {
     TilePlan P;
     P.n = n;
     P.k = (uint32_t)k;
+    P.fused = fused;
     if (!n || !B || n % B || k < 1 || k > kTileMaxSweeps || sm_count < 1) return P;
     sm_count = std::min(sm_count, kTileMaxTiles);
     const uint64_t ny = n / B;
@@ -462,15 +509,22 @@ inline TilePlan plan_tiles_grid5(uint32_t n, uint32_t B, int k, int sm_count, ui
         // lower set: clipped at the grid's left / bottom edges
         const uint32_t lka = std::min(K, G.x0), lkb = std::min(K, G.y0);
         const uint32_t uka = std::min<uint32_t>(K, B - G.x1), ukb = std::min<uint32_t>(K, (uint32_t)ny - G.y1);
-        uint32_t cl = D.n_own, cu = D.n_own;
-        D.lcnt[0] = D.ucnt[0] = (uint16_t)D.n_own;
+        uint32_t cu = D.n_own;
+        D.ucnt[0] = (uint16_t)D.n_own;
         for (uint32_t d = 1; d <= K; ++d)
         {
-            cl += grid5_layer(d, tw, th, lka, lkb);
             cu += grid5_layer(d, tw, th, uka, ukb);
-            if (cl >= kTileNoDep || cu >= kTileNoDep) return P;
-            D.lcnt[d] = (uint16_t)cl;
+            if (cu >= kTileNoDep) return P;
             D.ucnt[d] = (uint16_t)cu;
+        }
+        const TileGeom F = grid5_fwd_block(G, B, (uint32_t)ny, K, fused);
+        uint32_t cl = fused ? cu : D.n_own;
+        D.lcnt[0] = (uint16_t)cl;
+        for (uint32_t d = 1; d <= K; ++d)
+        {
+            cl += grid5_layer(d, F.x1 - F.x0, F.y1 - F.y0, lka, lkb);
+            if (cl >= kTileNoDep) return P;
+            D.lcnt[d] = (uint16_t)cl;
         }
         D.n_el = cl;
         D.n_eu = cu;
@@ -492,7 +546,7 @@ inline TilePlan plan_tiles_grid5(uint32_t n, uint32_t B, int k, int sm_count, ui
         D.vbytes = o;
         o = 0;
         D.o_owned = seg(4ull * D.n_own);
-        D.o_lhalo = seg(4ull * (D.n_el - D.n_own));
+        D.o_lhalo = seg(4ull * (D.n_el - D.lcnt[0]));  // rows of the lower set past its layer 0
         D.o_ldeps = seg(4ull * D.n_el);
         D.o_uhalo = seg(4ull * (D.n_eu - D.n_own));
         D.o_udeps = seg(4ull * D.n_eu);
@@ -523,142 +577,8 @@ inline TilePlan plan_tiles_grid5(uint32_t n, uint32_t B, int k, int sm_count, ui
     return P;
 }
 
-// Scratch (u16 entries) one part of one tile needs: a box of the set's points.
-inline uint32_t grid5_scratch(const TileGeom& G, uint32_t B, uint32_t ny, int k)
-{
-    const uint32_t K = (uint32_t)k;
-    const uint32_t lw = G.x1 - (G.x0 > K ? G.x0 - K : 0), lh = G.y1 - (G.y0 > K ? G.y0 - K : 0);
-    const uint32_t uw = std::min(B, G.x1 + K) - G.x0, uh = std::min(ny, G.y1 + K) - G.y0;
-    return std::max(lw * lh, uw * uh);
-}
-
-// Writes part `part` of a tile's index blob: 0 = owned rows and the lower
-// set (halo, dependencies), 1 = the upper set, 2 = the SpMV's ring, offsets
-// and columns.  The parts read nothing another part writes, so they can run
-// side by side.  loc: scratch of grid5_scratch entries.  Returns false when
-// a count disagrees with the descriptor (nothing is written past it).
-B2S_TILE_HD inline bool grid5_build_part(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, int k, int part,
-                                    uint8_t* ib, uint16_t* loc)
-{
-    const uint32_t K = (uint32_t)k, tw = G.x1 - G.x0, th = G.y1 - G.y0;
-    uint32_t* owned = reinterpret_cast<uint32_t*>(ib + D.o_owned);
-    auto own_local = [&](uint32_t x, uint32_t y) { return (y - G.y0) * tw + (x - G.x0); };
-    if (part == 0 || part == 1)
-    {
-        const bool lo = part == 0;
-        if (lo)
-            for (uint32_t y = G.y0, q = 0; y < G.y1; ++y)
-                for (uint32_t x = G.x0; x < G.x1; ++x) owned[q++] = y * B + x;
-        const uint32_t ne = lo ? D.n_el : D.n_eu;
-        const uint16_t* cnt = lo ? D.lcnt : D.ucnt;
-        uint32_t* halo = reinterpret_cast<uint32_t*>(ib + (lo ? D.o_lhalo : D.o_uhalo));
-        uint32_t* deps = reinterpret_cast<uint32_t*>(ib + (lo ? D.o_ldeps : D.o_udeps));
-        // the box of the set, row-major (= ascending global index)
-        const uint32_t bx0 = lo ? (G.x0 > K ? G.x0 - K : 0) : G.x0, by0 = lo ? (G.y0 > K ? G.y0 - K : 0) : G.y0;
-        const uint32_t bx1 = lo ? G.x1 : (B < G.x1 + K ? B : G.x1 + K);
-        const uint32_t by1 = lo ? G.y1 : (ny < G.y1 + K ? ny : G.y1 + K);
-        const uint32_t bw = bx1 - bx0;  // (the box holds (by1 - by0) * bw entries: grid5_scratch)
-        uint32_t next[kTileMaxSweeps + 1];
-        for (uint32_t d = 1; d <= K; ++d) next[d] = cnt[d - 1];
-        for (uint32_t y = by0, q = 0; y < by1; ++y)
-        {
-            const uint32_t db = lo ? (y < G.y0 ? G.y0 - y : 0) : (y >= G.y1 ? y - G.y1 + 1 : 0);
-            for (uint32_t x = bx0; x < bx1; ++x, ++q)
-            {
-                const uint32_t da = lo ? (x < G.x0 ? G.x0 - x : 0) : (x >= G.x1 ? x - G.x1 + 1 : 0);
-                const uint32_t d = da + db;
-                uint32_t l = kTileNoDep;
-                if (d == 0)
-                    l = own_local(x, y);
-                else if (d <= K)
-                {
-                    l = next[d]++;
-                    if (l >= cnt[d]) return false;
-                    halo[l - D.n_own] = y * B + x;
-                }
-                loc[q] = (uint16_t)l;
-            }
-        }
-        for (uint32_t d = 1; d <= K; ++d)
-            if (next[d] != cnt[d]) return false;
-        // dependencies in column order: lower (x, y-1) then (x-1, y); upper (x+1, y) then (x, y+1)
-        auto at = [&](uint32_t x, uint32_t y) -> uint32_t {
-            if (x < bx0 || x >= bx1 || y < by0 || y >= by1) return kTileNoDep;
-            return loc[(y - by0) * bw + (x - bx0)];
-        };
-        for (uint32_t t = 0; t < ne; ++t)
-        {
-            uint32_t x, y;
-            if (t < D.n_own)
-            {
-                x = G.x0 + t % tw;
-                y = G.y0 + t / tw;
-            }
-            else
-            {
-                const uint32_t g = halo[t - D.n_own];  // written by this part above
-                x = g % B;
-                y = g / B;
-            }
-            uint32_t s[2] = {kTileNoDep, kTileNoDep}, e = 0;
-            if (lo)
-            {
-                if (y > 0) s[e++] = at(x, y - 1);
-                if (x > 0) s[e++] = at(x - 1, y);
-            }
-            else
-            {
-                if (x + 1 < B) s[e++] = at(x + 1, y);
-                if (y + 1 < ny) s[e++] = at(x, y + 1);
-            }
-            deps[t] = s[0] | (s[1] << 16);
-        }
-        return true;
-    }
-    // part 2: the SpMV's columns -- ring order by global index: the row below
-    // the block, then left / right of each block row, then the row above
-    uint32_t* ahalo = reinterpret_cast<uint32_t*>(ib + D.o_ahalo);
-    uint32_t* arp = reinterpret_cast<uint32_t*>(ib + D.o_arp);
-    uint16_t* acol = reinterpret_cast<uint16_t*>(ib + D.o_acol);
-    const bool L = G.x0 > 0, R = G.x1 < B, Bo = G.y0 > 0, T = G.y1 < ny;
-    const uint32_t nb = Bo ? tw : 0, per_row = (L ? 1u : 0u) + (R ? 1u : 0u);
-    if (D.n_own + nb + th * per_row + (T ? tw : 0) != D.n_ae) return false;
-    uint32_t r = 0;
-    if (Bo)
-        for (uint32_t x = G.x0; x < G.x1; ++x) ahalo[r++] = (G.y0 - 1) * B + x;
-    for (uint32_t y = G.y0; y < G.y1; ++y)
-    {
-        if (L) ahalo[r++] = y * B + G.x0 - 1;
-        if (R) ahalo[r++] = y * B + G.x1;
-    }
-    if (T)
-        for (uint32_t x = G.x0; x < G.x1; ++x) ahalo[r++] = G.y1 * B + x;
-    if (D.n_own + r != D.n_ae) return false;
-    auto col = [&](uint32_t x, uint32_t y) -> uint32_t {
-        if (x >= G.x0 && x < G.x1 && y >= G.y0 && y < G.y1) return own_local(x, y);
-        if (y + 1 == G.y0) return D.n_own + (x - G.x0);
-        if (y == G.y1) return D.n_own + nb + th * per_row + (x - G.x0);
-        return D.n_own + nb + (y - G.y0) * per_row + (x + 1 == G.x0 ? 0u : (L ? 1u : 0u));
-    };
-    uint32_t e = 0;
-    arp[0] = 0;
-    for (uint32_t q = 0; q < D.n_own; ++q)
-    {
-        const uint32_t x = G.x0 + q % tw, y = G.y0 + q / tw;
-        const uint32_t c = 1u + (y > 0) + (x > 0) + (x + 1 < B) + (y + 1 < ny);
-        if (e + c > D.nnz) return false;
-        if (y > 0) acol[e++] = (uint16_t)col(x, y - 1);
-        if (x > 0) acol[e++] = (uint16_t)col(x - 1, y);
-        acol[e++] = (uint16_t)q;
-        if (x + 1 < B) acol[e++] = (uint16_t)col(x + 1, y);
-        if (y + 1 < ny) acol[e++] = (uint16_t)col(x, y + 1);
-        arp[q + 1] = e;
-    }
-    return e == D.nnz;
-}
-
-// ---- the same blob, one element at a time (the device builds it with one
-// thread per element; grid5_build_part is the sequential statement of it).
+// ---- a tile's index blob, one element at a time (the device builds it with
+// one thread per element; the tests check it against plan_tiles byte for byte).
 //
 // A set's box (lower: the block grown by k down and left, upper: up and
 // right) is walked in row-major order; an entry at distance d >= 1 from the
@@ -666,7 +586,9 @@ B2S_TILE_HD inline bool grid5_build_part(const TileDesc& D, const TileGeom& G, u
 // of layer d.  Its rank inside layer d has a closed form: rows of the box
 // before it hold, per row, the whole block width when d = db (da = 0) or the
 // one entry at da = d - db (when it lies inside the box), and in its own row
-// no earlier entry of layer d precedes it unless da = 0.
+// no earlier entry of layer d precedes it unless da = 0.  In a fused plan the
+// lower set is that of the block grown up and right (grid5_fwd_block), with
+// the upper set as its layer 0.
 struct Grid5Box
 {
     uint32_t bx0, bx1, by0, by1;
@@ -702,16 +624,11 @@ B2S_TILE_HD inline uint32_t grid5_row_count(const TileGeom& G, const Grid5Box& b
     return lo ? (G.x0 >= b.bx0 + e ? 1u : 0u) : (G.x1 - 1u + e < b.bx1 ? 1u : 0u);
 }
 
-// the local index of grid point (x, y) in a tile's lower (lo) or upper set, or
-// kTileNoDep when the point is outside it
-B2S_TILE_HD inline uint32_t grid5_local(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K,
-                                        bool lo, uint32_t x, uint32_t y)
+// local index of box point (x, y) at distance d in [1, K] from block G:
+// cnt[d-1] plus its rank in layer d, or kTileNoDep past cnt[d]
+B2S_TILE_HD inline uint32_t grid5_layer_index(const uint16_t* cnt, const TileGeom& G, const Grid5Box& b, bool lo,
+                                              uint32_t x, uint32_t y, uint32_t d)
 {
-    const Grid5Box b = grid5_box(G, B, ny, K, lo);
-    if (x < b.bx0 || x >= b.bx1 || y < b.by0 || y >= b.by1) return kTileNoDep;
-    const uint32_t da = grid5_dx(G, lo, x), db = grid5_dy(G, lo, y), d = da + db;
-    if (d == 0) return (y - G.y0) * (G.x1 - G.x0) + (x - G.x0);
-    if (d > K) return kTileNoDep;
     uint32_t rank = 0;
     // rows of the box before y: those off the block (db >= 1) one by one,
     // those beside the block (db = 0) hold one entry of layer d each
@@ -728,25 +645,45 @@ B2S_TILE_HD inline uint32_t grid5_local(const TileDesc& D, const TileGeom& G, ui
         }
         rank += grid5_row_count(G, b, lo, yy, d);
     }
-    if (da == 0) rank += x - G.x0;
-    const uint16_t* cnt = lo ? D.lcnt : D.ucnt;
+    if (grid5_dx(G, lo, x) == 0) rank += x - G.x0;
     const uint32_t l = cnt[d - 1] + rank;
     return l < cnt[d] ? l : kTileNoDep;
 }
 
-// Element `e` of a tile's index blob, for e < grid5_elements(D): the owned
-// rows, the two sets' halos, the SpMV ring and its rows (offsets and
-// columns) -- everything but the dependencies, which need the halos first
-// (grid5_build_deps).  False when an index falls outside its segment.
-B2S_TILE_HD inline uint32_t grid5_elements(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K)
+// the local index of grid point (x, y) in a tile's lower (lo) or upper set, or
+// kTileNoDep when the point is outside it
+B2S_TILE_HD inline uint32_t grid5_local(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K,
+                                        bool lo, bool fused, uint32_t x, uint32_t y)
 {
-    const Grid5Box lb = grid5_box(G, B, ny, K, true), ub = grid5_box(G, B, ny, K, false);
+    const TileGeom F = lo ? grid5_fwd_block(G, B, ny, K, fused) : G;
+    const Grid5Box b = grid5_box(F, B, ny, K, lo);
+    if (x < b.bx0 || x >= b.bx1 || y < b.by0 || y >= b.by1) return kTileNoDep;
+    const uint32_t d = grid5_dx(F, lo, x) + grid5_dy(F, lo, y);
+    if (d == 0)
+    {
+        if (lo && fused) return grid5_local(D, G, B, ny, K, false, false, x, y);  // the upper set (layer 0)
+        return (y - G.y0) * (G.x1 - G.x0) + (x - G.x0);
+    }
+    if (d > K) return kTileNoDep;
+    return grid5_layer_index(lo ? D.lcnt : D.ucnt, F, b, lo, x, y, d);
+}
+
+// Elements of a tile's index blob other than the dependencies: the owned
+// rows, the two sets' box points, the SpMV ring and the owned rows' entries.
+B2S_TILE_HD inline uint32_t grid5_elements(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K,
+                                           bool fused)
+{
+    const Grid5Box lb = grid5_box(grid5_fwd_block(G, B, ny, K, fused), B, ny, K, true);
+    const Grid5Box ub = grid5_box(G, B, ny, K, false);
     return D.n_own + (lb.bx1 - lb.bx0) * (lb.by1 - lb.by0) + (ub.bx1 - ub.bx0) * (ub.by1 - ub.by0) +
            (D.n_ae - D.n_own) + D.n_own;
 }
 
+// Writes element e (< grid5_elements) of a tile's index blob; false when an
+// index falls outside its segment.  The dependencies follow once the halos
+// are in place (grid5_build_dep).
 B2S_TILE_HD inline bool grid5_build_elem(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K,
-                                         uint32_t e, uint8_t* ib)
+                                         bool fused, uint32_t e, uint8_t* ib)
 {
     const uint32_t tw = G.x1 - G.x0, th = G.y1 - G.y0;
     if (e < D.n_own)
@@ -758,16 +695,18 @@ B2S_TILE_HD inline bool grid5_build_elem(const TileDesc& D, const TileGeom& G, u
     for (int side = 0; side < 2; ++side)
     {
         const bool lo = side == 0;
-        const Grid5Box b = grid5_box(G, B, ny, K, lo);
+        const TileGeom F = lo ? grid5_fwd_block(G, B, ny, K, fused) : G;
+        const Grid5Box b = grid5_box(F, B, ny, K, lo);
         const uint32_t bw = b.bx1 - b.bx0, sz = bw * (b.by1 - b.by0);
         if (e < sz)
         {
             const uint32_t x = b.bx0 + e % bw, y = b.by0 + e / bw;
-            const uint32_t d = grid5_dx(G, lo, x) + grid5_dy(G, lo, y);
+            const uint32_t d = grid5_dx(F, lo, x) + grid5_dy(F, lo, y);
             if (d == 0 || d > K) return true;
-            const uint32_t l = grid5_local(D, G, B, ny, K, lo, x, y);
-            if (l == kTileNoDep || l < D.n_own) return false;
-            reinterpret_cast<uint32_t*>(ib + (lo ? D.o_lhalo : D.o_uhalo))[l - D.n_own] = y * B + x;
+            const uint32_t l = grid5_layer_index(lo ? D.lcnt : D.ucnt, F, b, lo, x, y, d);
+            const uint32_t base = lo ? D.lcnt[0] : D.n_own;
+            if (l == kTileNoDep || l < base) return false;
+            reinterpret_cast<uint32_t*>(ib + (lo ? D.o_lhalo : D.o_uhalo))[l - base] = y * B + x;
             return true;
         }
         e -= sz;
@@ -829,10 +768,10 @@ B2S_TILE_HD inline bool grid5_build_elem(const TileDesc& D, const TileGeom& G, u
     return true;
 }
 
-// Dependencies of extended row t of the lower (lo) or upper set, after the
-// halos are written: {first, second} local indices in column order.
+// Dependencies of row t of the lower (lo) or upper set, after the halos are
+// written: {first, second} local indices in column order.
 B2S_TILE_HD inline void grid5_build_dep(const TileDesc& D, const TileGeom& G, uint32_t B, uint32_t ny, uint32_t K,
-                                        bool lo, uint32_t t, uint8_t* ib)
+                                        bool lo, bool fused, uint32_t t, uint8_t* ib)
 {
     const uint32_t tw = G.x1 - G.x0;
     uint32_t x, y;
@@ -843,20 +782,22 @@ B2S_TILE_HD inline void grid5_build_dep(const TileDesc& D, const TileGeom& G, ui
     }
     else
     {
-        const uint32_t g = reinterpret_cast<const uint32_t*>(ib + (lo ? D.o_lhalo : D.o_uhalo))[t - D.n_own];
+        const uint32_t base = lo ? D.lcnt[0] : D.n_own;  // (fused lower set: the upper halo before base)
+        const uint32_t g = t < base ? reinterpret_cast<const uint32_t*>(ib + D.o_uhalo)[t - D.n_own]
+                                    : reinterpret_cast<const uint32_t*>(ib + (lo ? D.o_lhalo : D.o_uhalo))[t - base];
         x = g % B;
         y = g / B;
     }
     uint32_t s[2] = {kTileNoDep, kTileNoDep}, e = 0;
     if (lo)
     {
-        if (y > 0) s[e++] = grid5_local(D, G, B, ny, K, true, x, y - 1);
-        if (x > 0) s[e++] = grid5_local(D, G, B, ny, K, true, x - 1, y);
+        if (y > 0) s[e++] = grid5_local(D, G, B, ny, K, true, fused, x, y - 1);
+        if (x > 0) s[e++] = grid5_local(D, G, B, ny, K, true, fused, x - 1, y);
     }
     else
     {
-        if (x + 1 < B) s[e++] = grid5_local(D, G, B, ny, K, false, x + 1, y);
-        if (y + 1 < ny) s[e++] = grid5_local(D, G, B, ny, K, false, x, y + 1);
+        if (x + 1 < B) s[e++] = grid5_local(D, G, B, ny, K, false, false, x + 1, y);
+        if (y + 1 < ny) s[e++] = grid5_local(D, G, B, ny, K, false, false, x, y + 1);
     }
     reinterpret_cast<uint32_t*>(ib + (lo ? D.o_ldeps : D.o_udeps))[t] = s[0] | (s[1] << 16);
 }

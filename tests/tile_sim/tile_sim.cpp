@@ -100,8 +100,8 @@ static void check_plan(const char* name, const Pattern& P, int k, int sms, uint3
 {
     const uint32_t n = P.n;
     TilePlan T = plan_tiles(n, P.lrp.data(), P.lci.data(), P.urp.data(), P.uci.data(), k, sms, smem_limit, 4);
-    std::printf("%-22s n=%u k=%d: ok=%d tiles=%u (%ux%u) B=%u Q=%u max_ext=%u smem=%u\n", name, n, k, T.ok, T.ntiles,
-                T.tiles_x, T.tiles_y, T.B, T.Q, T.max_ext, T.smem);
+    std::printf("%-22s n=%u k=%d: ok=%d fused=%d tiles=%u (%ux%u) B=%u Q=%u max_ext=%u smem=%u\n", name, n, k, T.ok,
+                T.fused, T.ntiles, T.tiles_x, T.tiles_y, T.B, T.Q, T.max_ext, T.smem);
     CHECK(T.ok == expect_ok, "%s: plan ok=%d, expected %d", name, T.ok, expect_ok);
     if (!T.ok) return;
     CHECK(T.ntiles <= (uint32_t)sms && T.ntiles <= (uint32_t)kTileMaxTiles, "%s: too many tiles", name);
@@ -124,7 +124,8 @@ static void check_plan(const char* name, const Pattern& P, int k, int sms, uint3
     std::vector<double> pg(n);
     for (auto& x : pg) x = (double)U(g);
     std::vector<uint32_t> seen(n, 0);
-    const uint32_t ystride = tile_align16(4ull * T.max_ext) / 4;
+    const uint32_t ystride = tile_ystride(T.max_ext);
+    CHECK(ystride > T.max_ext, "%s: no spare sweep slot", name);
     for (uint32_t t = 0; t < T.ntiles; ++t)
     {
         const TileDesc& D = T.desc[t];
@@ -147,12 +148,18 @@ static void check_plan(const char* name, const Pattern& P, int k, int sms, uint3
             return (uint32_t)v;
         };
         for (uint32_t q = 0; q < D.n_own; ++q) seen[u32(D.o_owned, q)]++;
-        // one triangle's sweeps as the kernel runs them (local buffers, prefix per pass)
+        // one triangle's sweeps as the kernel runs them (local buffers, prefix per
+        // pass); local_rhs: the right-hand side of rows t < its size taken from
+        // the CTA (a fused plan's backward sweeps), not from the global vector
         auto replay = [&](bool lower, uint32_t ne, const uint16_t* cnt, uint32_t o_halo, uint32_t o_deps,
                           const std::vector<uint32_t>& rp, const std::vector<uint32_t>& ci, const std::vector<float>& v,
-                          const std::vector<float>& dinv, const std::vector<float>& rhs, const std::vector<float>& want) {
-            CHECK(cnt[0] == D.n_own && cnt[k] == ne, "%s: layer counts", name);
-            auto glob = [&](uint32_t tl) { return tl < D.n_own ? u32(D.o_owned, tl) : u32(o_halo, tl - D.n_own); };
+                          const std::vector<float>& dinv, const std::vector<float>& rhs, const std::vector<float>& want,
+                          uint32_t check_rows, const std::vector<float>* local_rhs) {
+            const uint32_t base = lower ? cnt[0] : D.n_own;  // rows of the layer-0 set
+            CHECK(cnt[0] == (lower && T.fused ? D.n_eu : D.n_own) && cnt[k] == ne, "%s: layer counts", name);
+            auto glob = [&](uint32_t tl) {
+                return tl < D.n_own ? u32(D.o_owned, tl) : tl < base ? u32(D.o_uhalo, tl - D.n_own) : u32(o_halo, tl - base);
+            };
             std::vector<float> y0(ystride, NAN), y1(ystride, NAN);
             for (int s = 0; s <= k; ++s)
             {
@@ -162,7 +169,7 @@ static void check_plan(const char* name, const Pattern& P, int k, int sms, uint3
                 for (uint32_t tl = 0; tl < t1; ++tl)
                 {
                     const uint32_t gr = glob(tl);
-                    float sum = rhs[gr];
+                    float sum = local_rhs && tl < local_rhs->size() ? (*local_rhs)[tl] : rhs[gr];
                     const uint32_t w = u32(o_deps, tl);
                     const uint32_t d[2] = {w & 0xFFFFu, w >> 16};
                     // the planned dependencies are the row's strict entries in column order
@@ -188,15 +195,20 @@ static void check_plan(const char* name, const Pattern& P, int k, int sms, uint3
                 }
             }
             const std::vector<float>& yk = (k & 1) ? y1 : y0;
-            for (uint32_t tl = 0; tl < D.n_own; ++tl)
+            for (uint32_t tl = 0; tl < check_rows; ++tl)
             {
                 const uint32_t gr = glob(tl);
                 CHECK(std::memcmp(&yk[tl], &want[gr], 4) == 0, "%s tile %u row %u (%s): %g vs %g", name, t, gr,
                       lower ? "lower" : "upper", yk[tl], want[gr]);
             }
+            return std::vector<float>(yk.begin(), yk.begin() + check_rows);
         };
-        replay(true, D.n_el, D.lcnt, D.o_lhalo, D.o_ldeps, P.lrp, P.lci, lv, ld, r, yl);
-        replay(false, D.n_eu, D.ucnt, D.o_uhalo, D.o_udeps, P.urp, P.uci, uv, ud, yl, yu);
+        // fused: the forward sweeps must give every row of the upper set, which
+        // the backward sweeps then take from the CTA
+        const std::vector<float> yloc = replay(true, D.n_el, D.lcnt, D.o_lhalo, D.o_ldeps, P.lrp, P.lci, lv, ld, r, yl,
+                                               T.fused ? D.n_eu : D.n_own, nullptr);
+        replay(false, D.n_eu, D.ucnt, D.o_uhalo, D.o_udeps, P.urp, P.uci, uv, ud, yl, yu, D.n_own,
+               T.fused ? &yloc : nullptr);
         // SpMV over local columns against the CSR rows [lower | diag | upper]
         std::vector<double> pe(D.n_ae);
         for (uint32_t c = 0; c < D.n_ae; ++c) pe[c] = pg[c < D.n_own ? u32(D.o_owned, c) : u32(D.o_ahalo, c - D.n_own)];
@@ -226,46 +238,43 @@ static void check_plan(const char* name, const Pattern& P, int k, int sms, uint3
 }
 
 // the closed-form 5-point planner and builder against the breadth-first planner:
-// the same descriptors and the same index blobs, byte for byte
+// the same descriptors and the same index blobs, byte for byte, for the fused
+// layout (tried first) and the separate one
 static void check_grid5(const char* name, uint32_t N, uint32_t M, int k, int sms)
 {
     const Pattern P = five_point(N, M);
-    const TilePlan T = plan_tiles(P.n, P.lrp.data(), P.lci.data(), P.urp.data(), P.uci.data(), k, sms, 228352, 4);
-    std::vector<TileGeom> geom;
-    const TilePlan G = plan_tiles_grid5(P.n, N, k, sms, 228352, geom);
-    std::printf("%-22s grid5 ok=%d (BFS ok=%d) tiles=%u\n", name, G.ok, T.ok, G.ntiles);
-    CHECK(is_grid5(P.n, P.lrp.data(), P.lci.data(), N, false), "%s: not recognised as a 5-point grid", name);
-    CHECK(G.ok == T.ok, "%s: grid5 ok %d vs %d", name, G.ok, T.ok);
-    if (!G.ok || !T.ok) return;
-    CHECK(G.ntiles == T.ntiles && G.smem == T.smem && G.work == T.work && G.Q == T.Q && G.ibytes == T.idx.size() &&
-              G.vbytes == T.vbytes, "%s: plan sizes differ", name);
-    std::vector<uint8_t> blob(G.ibytes, 0);
-    uint32_t scratch = 0;
-    for (const TileGeom& g : geom) scratch = std::max(scratch, grid5_scratch(g, N, M, k));
-    std::vector<uint16_t> loc(scratch);
-    for (uint32_t t = 0; t < G.ntiles; ++t)
+    for (int fused_first = 1; fused_first >= 0; --fused_first)
     {
-        CHECK(std::memcmp(&G.desc[t], &T.desc[t], sizeof(TileDesc)) == 0, "%s tile %u: descriptor differs", name, t);
-        for (int part = 0; part < 3; ++part)
-            CHECK(grid5_build_part(G.desc[t], geom[t], N, M, k, part, blob.data() + G.desc[t].ibase, loc.data()),
-                  "%s tile %u part %d: build failed", name, t, part);
+        const TilePlan T = plan_tiles(P.n, P.lrp.data(), P.lci.data(), P.urp.data(), P.uci.data(), k, sms, 228352, 4,
+                                      fused_first != 0);
+        std::vector<TileGeom> geom;
+        const TilePlan G = plan_tiles_grid5(P.n, N, k, sms, 228352, geom, fused_first != 0);
+        std::printf("%-22s grid5 ok=%d fused=%d (BFS ok=%d fused=%d) tiles=%u Q=%u smem=%u\n", name, G.ok, G.fused, T.ok,
+                    T.fused, G.ntiles, G.Q, G.smem);
+        CHECK(is_grid5(P.n, P.lrp.data(), P.lci.data(), N, false), "%s: not recognised as a 5-point grid", name);
+        CHECK(G.ok == T.ok, "%s: grid5 ok %d vs %d", name, G.ok, T.ok);
+        if (!G.ok || !T.ok) continue;
+        CHECK(G.fused == T.fused, "%s: fused %d vs %d", name, G.fused, T.fused);
+        CHECK(G.ntiles == T.ntiles && G.smem == T.smem && G.work == T.work && G.Q == T.Q &&
+                  G.ibytes == T.idx.size() && G.vbytes == T.vbytes,
+              "%s: plan sizes differ", name);
+        // the element-at-a-time builder (one device thread per element, then the
+        // dependencies once the halos are in place), in reverse element order
+        std::vector<uint8_t> blob(G.ibytes, 0);
+        for (uint32_t t = 0; t < G.ntiles; ++t)
+        {
+            const TileDesc& D = G.desc[t];
+            CHECK(std::memcmp(&D, &T.desc[t], sizeof(TileDesc)) == 0, "%s tile %u: descriptor differs", name, t);
+            uint8_t* ib = blob.data() + D.ibase;
+            const uint32_t ne = grid5_elements(D, geom[t], N, M, (uint32_t)k, G.fused);
+            for (uint32_t e = ne; e-- > 0;)
+                CHECK(grid5_build_elem(D, geom[t], N, M, (uint32_t)k, G.fused, e, ib),
+                      "%s tile %u element %u: build failed", name, t, e);
+            for (uint32_t r = D.n_el; r-- > 0;) grid5_build_dep(D, geom[t], N, M, (uint32_t)k, true, G.fused, r, ib);
+            for (uint32_t r = D.n_eu; r-- > 0;) grid5_build_dep(D, geom[t], N, M, (uint32_t)k, false, G.fused, r, ib);
+        }
+        CHECK(blob == T.idx, "%s: index blobs differ", name);
     }
-    CHECK(blob == T.idx, "%s: index blobs differ", name);
-    // the element-at-a-time builder (one device thread per element, then the
-    // dependencies once the halos are in place) in reverse element order
-    std::vector<uint8_t> blob2(G.ibytes, 0);
-    for (uint32_t t = 0; t < G.ntiles; ++t)
-    {
-        const TileDesc& D = G.desc[t];
-        uint8_t* ib = blob2.data() + D.ibase;
-        const uint32_t ne = grid5_elements(D, geom[t], N, M, (uint32_t)k);
-        for (uint32_t e = ne; e-- > 0;)
-            CHECK(grid5_build_elem(D, geom[t], N, M, (uint32_t)k, e, ib), "%s tile %u element %u: build failed", name,
-                  t, e);
-        for (uint32_t r = D.n_el; r-- > 0;) grid5_build_dep(D, geom[t], N, M, (uint32_t)k, true, r, ib);
-        for (uint32_t r = D.n_eu; r-- > 0;) grid5_build_dep(D, geom[t], N, M, (uint32_t)k, false, r, ib);
-    }
-    CHECK(blob2 == T.idx, "%s: element-wise index blobs differ", name);
     // a pattern that is not a 5-point grid is not taken for one
     Pattern Q = P;
     if (Q.lci.size() > 2) std::swap(Q.lci[Q.lrp[N + 1]], Q.lci[Q.lrp[N + 1] + 1]);
