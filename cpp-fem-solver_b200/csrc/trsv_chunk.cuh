@@ -17,7 +17,8 @@
 //      trips, a divide and a barrier.
 //   3. publishes each row that another chunk reads, right after computing
 //      it, into the exchange array: one 64-bit word per 32-bit half of each
-//      value, {epoch, bits}, written with a relaxed store.  A 64-bit access
+//      value, {epoch, bits}, written with a relaxed store (every row reaches
+//      x only after the traversal, copied from shared memory).  A 64-bit access
 //      is single-copy atomic, so a reader that sees the epoch in a word also
 //      sees that word's value bits: one L2 round trip per slot and no fence
 //      on the publishing side.
@@ -223,7 +224,7 @@ __device__ __forceinline__ void compute_barrier()
 template <int NW>
 constexpr int chunk_block() { return (NW + 1) * 32 > 256 ? (NW + 1) * 32 : 256; }
 
-template <bool LOWER, bool UNIT, int NW, typename VT, typename XT, typename RT>
+template <bool LOWER, bool UNIT, int NW, typename VT, typename XT, typename RT, int MAXQ>
 __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, const RT* __restrict__ rhs,
                                                                    XT* __restrict__ x, double* __restrict__ out64,
                                                                    const int* done)
@@ -250,6 +251,7 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
         for (uint32_t k = tid; k < D.nr; k += blockDim.x) cp_async_elem<sizeof(RT)>(sr + k, rhs + D.lo + k);
         uint32_t* xr = reinterpret_cast<uint32_t*>(smem + L.xr);
         for (uint32_t s = tid; s < D.ns; s += blockDim.x) xr[s] = 0u;
+        if (tid == 0) reinterpret_cast<XT*>(smem + L.sx)[D.nr] = XT(0);  // the zero of absent entries
         cp_async_wait_all();
     }
     __syncthreads();
@@ -279,43 +281,60 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
     const uint16_t* slv = reinterpret_cast<const uint16_t*>(smem + L.meta + L.m.slv);
     XT* sx = reinterpret_cast<XT*>(smem + L.sx);
     const RT* sr = reinterpret_cast<const RT*>(smem + L.sr);
+    // A row with at most MAXQ entries is solved with straight-line code: its
+    // absent entries read the zero at sx[nr] with a zero coefficient (sum -
+    // 0 * 0 leaves sum, its sign included, unchanged), and the record's slot
+    // mask says which entries are values of other chunks.  Longer rows loop.
+    const uint32_t zero_pos = D.nr;
     struct Ops
     {
-        uint32_t pr = 0, e0 = 0, e1 = 0;
-        uint32_t m[4] = {0u, 0u, 0u, 0u};
-        VT vv[4] = {VT(0), VT(0), VT(0), VT(0)};
+        uint32_t pr = 0, e0 = 0, e1 = 0, smask = 0;
+        uint32_t m[MAXQ];
+        VT vv[MAXQ];
         XT rhs = XT(0), dv = XT(1);
     };
     unsigned slept = 0;  // this thread's sleeping polls in slot waits (bounded per launch)
-    auto fetch = [&](uint32_t t, uint32_t tend, Ops& o) {
-        if (t >= tend) return;
-        const uint2 rw = rec[t];
+    // a position's record (zero past the level's end), then everything else it
+    // needs, read through that record: the two steps run a level apart
+    auto rec_at = [&](uint32_t t, uint32_t tend) { return t < tend ? rec[t] : make_uint2(0u, 0u); };
+    auto fetch_ops = [&](uint2 rw, bool valid, uint32_t t, Ops& o) {
         o.pr = rec_perm(rw.x);
         o.e0 = rec_e0(rw.x);
         o.e1 = rec_e1(rw.y);
-        o.rhs = (XT)sr[o.pr & 0x7fffu];
-        if (!UNIT) o.dv = (XT)sd[t];
+        o.smask = rw.y >> 16;
+        o.rhs = valid ? (XT)sr[o.pr & 0x7fffu] : XT(0);
+        if (!UNIT) o.dv = valid ? (XT)sd[t] : XT(1);
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
+        for (int q = 0; q < MAXQ; ++q)
         {
             const bool on = o.e0 + q < o.e1;
-            o.m[q] = on ? slc[o.e0 + q] : 0u;
+            o.m[q] = on ? (uint32_t)slc[o.e0 + q] : zero_pos;
             o.vv[q] = on ? sv[o.e0 + q] : VT(0);
         }
     };
-    auto solve_row = [&](uint32_t t, const Ops& o) {
+    auto fetch = [&](uint32_t t, uint32_t tend, Ops& o) { fetch_ops(rec_at(t, tend), t < tend, t, o); };
+    auto solve_row = [&](uint32_t t, const Ops& o) -> XT {
         XT sum = o.rhs;
-        if (o.e1 - o.e0 <= 4)
+        if (o.e1 - o.e0 <= MAXQ)
         {
+            XT xj[MAXQ];
+            if (o.smask == 0)
+            {
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (o.e0 + q < o.e1 && (o.m[q] & 0x8000u)) slot_wait(xr, o.m[q] & 0x7fffu, a, slept);
-            XT xj[4];
+                for (int q = 0; q < MAXQ; ++q) xj[q] = sx[o.m[q]];
+            }
+            else
+            {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) xj[q] = (o.m[q] & 0x8000u) ? xv[o.m[q] & 0x7fffu] : sx[o.m[q]];
+                for (int q = 0; q < MAXQ; ++q)
+                {
+                    const bool slot = (o.smask >> q) & 1u;
+                    if (slot) slot_wait(xr, o.m[q] & 0x7fffu, a, slept);
+                    xj[q] = (slot ? xv : sx)[o.m[q] & 0x7fffu];
+                }
+            }
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                if (o.e0 + q < o.e1) sum -= (XT)o.vv[q] * xj[q];
+            for (int q = 0; q < MAXQ; ++q) sum -= (XT)o.vv[q] * xj[q];
         }
         else
         {
@@ -337,19 +356,25 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
         // FP64 divides, as the reference; FP32 multiplies by the packed reciprocal
         const XT r = UNIT ? sum : (sizeof(XT) == 4 ? sum * o.dv : sum / o.dv);
         sx[t] = r;
-        const uint32_t row = D.lo + (o.pr & 0x7fffu);
-        x[row] = r;
-        if (out64) out64[row] = (double)r;
-        if (o.pr & 0x8000u) xch_put<XT>(a.xch + (size_t)row * 2, r, epoch);
+        // rows other chunks read are published now; every row reaches x after the traversal
+        if (o.pr & 0x8000u) xch_put<XT>(a.xch + (size_t)(D.lo + (o.pr & 0x7fffu)) * 2, r, epoch);
+        return r;
     };
+    // Software-pipelined over levels: while level l is solved, the operands'
+    // metadata of level l + 1 (read through records loaded one level earlier)
+    // and the records of level l + 2 are in flight; none of them is consumed
+    // before the next iteration.
     uint32_t t0 = 0, t1 = slv[1];
+    uint32_t t2 = D.nl >= 2 ? slv[2] : t1;
     Ops cur;
     fetch(tid, t1, cur);
+    uint2 rnext = rec_at(t1 + tid, t2);
     for (uint32_t l = 0; l < D.nl; ++l)
     {
-        const uint32_t tn = l + 2 <= D.nl ? slv[l + 2] : t1;  // the next level's end
+        const uint32_t t3 = l + 3 <= D.nl ? slv[l + 3] : t2;  // the end of level l + 2
+        const uint2 rnn = rec_at(t2 + tid, t3);
         Ops nxt;
-        fetch(t1 + tid, tn, nxt);  // the next level's first pass, read ahead
+        fetch_ops(rnext, t1 + tid < t2, t1 + tid, nxt);
         if (t0 + tid < t1) solve_row(t0 + tid, cur);
         for (uint32_t t = t0 + tid + NW * 32; t < t1; t += NW * 32)
         {
@@ -359,8 +384,18 @@ __global__ void __launch_bounds__(chunk_block<NW>()) k_trsv_chunk(ChunkArgs a, c
         }
         compute_barrier<NW>();
         cur = nxt;
+        rnext = rnn;
         t0 = t1;
-        t1 = tn;
+        t1 = t2;
+        t2 = t3;
+    }
+    // the chunk's values, from shared memory to x (and out64) in position order
+    for (uint32_t t = tid; t < D.nr; t += NW * 32)
+    {
+        const uint32_t row = D.lo + (rec_perm(rec[t].x) & 0x7fffu);
+        const XT r = sx[t];
+        x[row] = r;
+        if (out64) out64[row] = (double)r;
     }
 
     // ---- 3. the last CTA to finish resets the tickets and advances the epoch
@@ -574,6 +609,7 @@ struct ChunkSchedule
     bool lower = true;
     uint32_t bs = 1, dv = 1;  // block size; divisor values per row (0: unit)
     int nw = 1;
+    int maxq = 4;          // scalar rows: straight-line entries per row (2, 3 or 4; longer rows loop)
     uint32_t plan_vs = 8;  // value size the chunks were sized for
     DBuf<ChunkDesc> desc;
     DBuf<uint4> meta, vals;
@@ -607,6 +643,7 @@ struct ChunkSchedule
         // one compute warp while a level needs at most two passes of it
         const uint32_t per_warp = 32 / bs;
         nw = P.max_level_rows <= 2 * per_warp ? 1 : 8;
+        maxq = P.max_row_deps <= 2 ? 2 : P.max_row_deps == 3 ? 3 : 4;
         h_desc = P.desc;
         desc = upload(ctx, P.desc);
         meta = upload(ctx, reinterpret_cast<const uint4*>(P.meta.data()), P.meta.size() / 16);
@@ -677,10 +714,14 @@ struct ChunkSchedule
         if (!n) return;
         if (packed_v != v || packed_d != d || packed_vs != sizeof(VT)) pack<VT>(ctx, v, d);
         const size_t smem = smem_bytes<VT, XT, RT>();
-        if (nw == 1)
-            go(ctx, k_trsv_chunk<LOWER, UNIT, 1, VT, XT, RT>, chunk_block<1>(), smem, rhs, x, out64, done);
+        if (nw == 1 && maxq == 2)
+            go(ctx, k_trsv_chunk<LOWER, UNIT, 1, VT, XT, RT, 2>, chunk_block<1>(), smem, rhs, x, out64, done);
+        else if (nw == 1 && maxq == 3)
+            go(ctx, k_trsv_chunk<LOWER, UNIT, 1, VT, XT, RT, 3>, chunk_block<1>(), smem, rhs, x, out64, done);
+        else if (nw == 1)
+            go(ctx, k_trsv_chunk<LOWER, UNIT, 1, VT, XT, RT, 4>, chunk_block<1>(), smem, rhs, x, out64, done);
         else
-            go(ctx, k_trsv_chunk<LOWER, UNIT, 8, VT, XT, RT>, chunk_block<8>(), smem, rhs, x, out64, done);
+            go(ctx, k_trsv_chunk<LOWER, UNIT, 8, VT, XT, RT, 4>, chunk_block<8>(), smem, rhs, x, out64, done);
     }
 
     // block rows: unit lower, or upper times the cached inverse blocks (d)

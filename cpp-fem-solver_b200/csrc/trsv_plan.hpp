@@ -28,7 +28,8 @@
 //     slc  u16[nd]    dependency entries: position, or 0x8000 | slot
 //     rec  u16x4[nr]  per position: local row (row - lo) | 0x8000 when rows
 //                     of another chunk depend on it (it publishes), then the
-//                     position's range [e0, e1) in slc, then 0
+//                     position's range [e0, e1) in slc, then the mask of its
+//                     entries (the first 16) that are slots
 //     slv  u16[nl+1]  level boundaries (positions)
 // and a value blob per precision (written on the device by k_chunk_pack):
 //     sv   VT[nd*bs*bs]  dependency values (blocks row-major), same order as slc
@@ -127,7 +128,7 @@ B2S_HD SmemLayout smem_layout(uint32_t nr, uint32_t nd, uint32_t nl, uint32_t ns
     L.m = meta_layout(nr, nd, nl);
     o += L.m.bytes;
     L.sx = o;
-    o += al16((uint64_t)nr * bs * xs);
+    o += al16(((uint64_t)nr * bs + 1) * xs);  // (+1: a zero the scalar solve reads for absent entries)
     L.sr = o;
     o += al16((uint64_t)nr * bs * rs);
     L.xv = o;
@@ -149,6 +150,7 @@ struct ChunkPlan
     std::vector<uint32_t> src;       // per dependency entry: index into the factor's values
     uint64_t v64_units = 0, v32_units = 0;
     uint32_t max_level_rows = 0;
+    uint32_t max_row_deps = 0;  // most dependency entries of one row
     bool ok = false;  // false when some row alone does not fit a chunk
 
     // largest shared-memory footprint of a chunk for the given element sizes
@@ -420,6 +422,7 @@ inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci,
         ~Scratch() { std::free(slot_of); }
     };
     std::vector<Scratch> scratch(std::max(1u, std::min(max_workers, 64u)));
+    std::vector<uint32_t> chunk_max_deps(nchunks, 0);
     plan_parallel(nchunks, (unsigned)scratch.size(), [&](uint32_t c, unsigned w) {
         const ChunkSpan& S = span[c];
         const ChunkDesc& D = P.desc[c];
@@ -439,6 +442,8 @@ inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci,
             put16(M.rec, 4 * t, r - D.lo);
             put16(M.rec, 4 * t + 1, e);
             rec_at[r] = (uint64_t)D.meta * 16 + M.rec + 8ull * t;
+            const uint32_t e_row = e;
+            uint32_t smask = 0;  // entries (of the first 16) that are slots
             for (uint32_t p = rp[r]; p < rp[r + 1]; ++p)
             {
                 const uint32_t j = ci[p];
@@ -456,6 +461,7 @@ inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci,
                         ++s;
                     }
                     m = 0x8000u | (slot_of[j] - 1);
+                    if (e - e_row < 16) smask |= 1u << (e - e_row);
                 }
                 if (e >= D.nd) throw std::logic_error("plan_chunks: dependency count");
                 put16(M.slc, e, m);
@@ -463,11 +469,14 @@ inline ChunkPlan plan_chunks(uint32_t n, const uint32_t* rp, const uint32_t* ci,
                 ++e;
             }
             put16(M.rec, 4 * t + 2, e);
+            put16(M.rec, 4 * t + 3, smask);
+            chunk_max_deps[c] = std::max(chunk_max_deps[c], e - e_row);
         }
         put16(M.slv, D.nl, D.nr);
         for (uint32_t q = 0; q < s; ++q) slot_of[P.slot_row[D.slot + q]] = 0;
         if (e != D.nd || s != D.ns) throw std::logic_error("plan_chunks: chunk counts");
     });
+    for (uint32_t c = 0; c < nchunks; ++c) P.max_row_deps = std::max(P.max_row_deps, chunk_max_deps[c]);
     // rows read by another chunk publish a ready flag (bit 15 of the record's local-row field)
     for (uint32_t j : P.slot_row)
     {

@@ -285,7 +285,11 @@ static void run_case(const char* name, Tri T, bool lower, uint32_t dv, uint32_t 
             {
                 const uint32_t pr = S.at<uint16_t>(mrec, mslv, 4 * t), k = pr & 0x7fffu;
                 const uint32_t e0 = S.at<uint16_t>(mrec, mslv, 4 * t + 1), e1 = S.at<uint16_t>(mrec, mslv, 4 * t + 2);
-                CHECK(S.at<uint16_t>(mrec, mslv, 4 * t + 3) == 0);
+                // the record's slot mask names exactly the row's slot entries (of the first 16)
+                uint32_t want_mask = 0;
+                for (uint32_t e = e0; e < e1 && e - e0 < 16; ++e)
+                    if (S.at<uint16_t>(mslc, mrec, e) & 0x8000u) want_mask |= 1u << (e - e0);
+                CHECK(S.at<uint16_t>(mrec, mslv, 4 * t + 3) == want_mask);
                 CHECK(k < D.nr);
                 // one lane per component (a single lane for scalar rows)
                 XT tr[BS];
