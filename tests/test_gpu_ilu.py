@@ -45,6 +45,27 @@ def test_ic0_bit_exact(b2s, ctx, orc, mat, trsv):
     assert np.array_equal(M.apply(r), po.apply(r))
 
 
+@pytest.mark.parametrize("spread,rhs_lo", [(60, -40), (500, -700)])
+def test_fp64_chunk_division_bit_exact(b2s, ctx, orc, spread, rhs_lo):
+    """FP64 chunked solves across the binary64 range: every quotient and
+    every partial sum must equal the restatement's.  D A D with D = 2^k, k
+    uniform in [0, spread] (the factorisations' absolute pivot test rules out
+    tiny pivots), and right-hand sides whose entries span 2^rhs_lo .. 2^40, put
+    the row sums and pivots from subnormal-adjacent to 2^500.  The IC(0) and
+    ILU(0) applies must equal the restatement bit for bit."""
+    n, rp, ci, v = P.random_spd(3000, 0.003, 11)
+    rng = np.random.default_rng(spread)
+    d = np.exp2(rng.integers(0, spread + 1, n).astype(np.float64))
+    rows = np.repeat(np.arange(n), np.diff(rp.astype(np.int64)))
+    vs = v * d[rows] * d[ci]
+    A = b2s.CSR(ctx, n, n, rp, ci, vs)
+    r = b2s.uniform(31, n) * np.exp2(rng.integers(rhs_lo, 41, n).astype(np.float64))
+    for kind in ("ic0", "ilu0"):
+        M = b2s.Precond(ctx, A, b2s.PC_NAMES[kind])
+        po = orc.pc(orc.csr(n, n, rp, ci, vs), kind)
+        assert np.array_equal(M.apply(r), po.apply(r)), kind
+
+
 @pytest.mark.parametrize("mat", ["poisson2d", "random", "poisson3d"])
 @pytest.mark.parametrize("trsv", [1, 2, 3])
 def test_ilu0_bit_exact(b2s, ctx, orc, mat, trsv):
