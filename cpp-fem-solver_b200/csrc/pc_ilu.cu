@@ -27,6 +27,7 @@
 #include "trsv_band.cuh"
 #include "pcg_band.cuh"
 #include "pcg_tile.cuh"
+#include "trsv_grid5.cuh"
 
 #include <cstdlib>
 #include <cstring>
@@ -506,6 +507,7 @@ struct Tri
     LevelSchedule sched;
     SyncFree sf;
     ChunkSchedule cs;
+    Grid5Tri g5;  // 5-point grid factors: the exact solve with a lane per grid line
     bool has_chunks = false, sched_ready = false;
     std::vector<uint32_t> h_level;  // host copy of the rows' levels (compute_levels), when known
     int sweeps = 8;                 // B2S_TRSV_JACOBI: sweeps after pass 0
@@ -593,6 +595,8 @@ struct Tri
     {
         if (mode == B2S_TRSV_JACOBI)
             run_sweeps<LOWER, UNIT, VT, XT, RT>(ctx, v, d, rhs, x, out64, done);
+        else if (mode == B2S_TRSV_CHUNK && g5.usable<VT, XT>() && g5.packed_v == (const void*)v)
+            g5.run<LOWER, UNIT, VT, XT, RT>(ctx, rhs, x, out64, done);
         else if (mode == B2S_TRSV_CHUNK && has_chunks && cs.usable<VT, XT, RT>())
             cs.run<LOWER, UNIT, VT, XT, RT>(ctx, v, d, rhs, x, out64, done);
         else
@@ -646,6 +650,7 @@ struct Tri
     void pack(b2s_ctx* ctx, const VT* v, const VT* d)
     {
         if (has_chunks && sizeof(VT) <= cs.plan_vs) cs.pack<VT>(ctx, v, d);
+        g5.pack<VT>(ctx, m->rp.p, m->ci.p, v, d, lower, unit);
         if constexpr (sizeof(VT) == 4)
         {
             if (band.T && n)
@@ -755,6 +760,25 @@ static PatternStats pattern_stats(b2s_ctx* ctx, const Csr32& L)
         ps.grid5 = h[3] == 0;
     }
     return ps;
+}
+
+// "trsv.grid5": sizes = {grid row length B (0: the grid schedule is off), lines, 1 when
+// both triangles' coefficients are packed}
+static void export_grid5(const Tri& fwd, const Tri& bwd, uint64_t* sizes)
+{
+    const bool on = fwd.g5.on && bwd.g5.on;
+    sizes[0] = on ? fwd.g5.B : 0;
+    sizes[1] = on ? fwd.g5.ny : 0;
+    sizes[2] = on && fwd.g5.packed_v && bwd.g5.packed_v ? 1 : 0;
+}
+
+// the grid row length B of a lower triangle that is a 5-point grid's, else 0
+static uint32_t grid5_lower_b(uint32_t n, const std::vector<uint32_t>& rp, const std::vector<uint32_t>& ci)
+{
+    uint32_t B = 0;
+    for (uint32_t i = 0; i < n; ++i)
+        if (rp[i + 1] > rp[i] && ci[rp[i]] < i) B = std::max(B, i - ci[rp[i]]);
+    return B && grid5_triangle(n, rp.data(), ci.data(), B, true) ? B : 0u;
 }
 
 static void copy_pattern(b2s_ctx* ctx, const Csr32& M, std::vector<uint32_t>& rp, std::vector<uint32_t>& ci)
@@ -1067,6 +1091,7 @@ struct PcIC0 final : PcImpl
         }
         if (what == "levels.L") return export_levels(ctx, fwd, sizes, ci);
         if (what == "levels.U") return export_levels(ctx, bwd, sizes, ci);
+        if (what == "trsv.grid5") return export_grid5(fwd, bwd, sizes);
         if (what == "pcg.tiles")  // the tiled persistent PCG kernel: tiles (0: not planned), rows per thread, smem
         {
             sizes[0] = tiles_ready ? tile_count : 0;
@@ -1293,6 +1318,12 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     pc->bwd.h_level = std::move(ha.up_level);
     pc->fwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.lo_plan : nullptr, vs);
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
+    if (pc->mode == B2S_TRSV_CHUNK && have_pattern && n)
+        if (const uint32_t B = grid5_lower_b(n, hrp, hci))  // L^T of a grid's L is the grid's upper triangle
+        {
+            pc->fwd.g5.enable(B, n / B);
+            pc->bwd.g5.enable(B, n / B);
+        }
     if (sweeps)
     {
         pc->fwd.prepare_sweeps(ctx, nsweeps, seg, pc->fp32, &ha.lo_band);
@@ -1353,6 +1384,7 @@ struct PcILU0 final : PcImpl
     {
         if (what == "ilu0.L") return export_csr(ctx, L, sizes, rp, ci, v);
         if (what == "ilu0.U") return export_csr(ctx, U, sizes, rp, ci, v);
+        if (what == "trsv.grid5") return export_grid5(fwd, bwd, sizes);
         if (what == "levels.L") return export_levels(ctx, fwd, sizes, ci);
         if (what == "levels.U") return export_levels(ctx, bwd, sizes, ci);
         PcImpl::export_data(ctx, what, sizes, rp, ci, v);
@@ -1439,6 +1471,13 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     pc->bwd.h_level = std::move(ha.up_level);
     pc->fwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.lo_plan : nullptr, vs);
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
+    if (pc->mode == B2S_TRSV_CHUNK && n)
+        if (const uint32_t B = grid5_lower_b(n, lrp, lci))
+            if (grid5_triangle(n, urp.data(), uci.data(), B, false))
+            {
+                pc->fwd.g5.enable(B, n / B);
+                pc->bwd.g5.enable(B, n / B);
+            }
     if (pc->mode == B2S_TRSV_JACOBI)
     {
         const int k = sweep_count(o);

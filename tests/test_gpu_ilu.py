@@ -66,6 +66,83 @@ def test_fp64_chunk_division_bit_exact(b2s, ctx, orc, spread, rhs_lo):
         assert np.array_equal(M.apply(r), po.apply(r)), kind
 
 
+def _f32_apply(L, U, r, lower_unit):
+    """The FP32 factor's apply as the GPU schedules compute it: FP32 values,
+    each row summed in column order in FP32, times the divisor's reciprocal
+    rounded once from FP64 (numpy float32 scalars: IEEE, no contraction)."""
+    f32 = np.float32
+    (lrp, lci, lv), (urp, uci, uv) = L, U
+    n = len(lrp) - 1
+    y = np.zeros(n, np.float32)
+    for i in range(n):
+        acc, dd = f32(r[i]), None
+        for e in range(lrp[i], lrp[i + 1]):
+            if lci[e] == i:
+                dd = f32(lv[e])
+            else:
+                acc = f32(acc - f32(f32(lv[e]) * y[lci[e]]))
+        y[i] = acc if lower_unit else f32(acc * f32(1.0 / np.float64(dd)))
+    z = np.zeros(n, np.float32)
+    for i in range(n - 1, -1, -1):
+        acc, dd = f32(y[i]), None
+        for e in range(urp[i], urp[i + 1]):
+            if uci[e] == i:
+                dd = f32(uv[e])
+            else:
+                acc = f32(acc - f32(f32(uv[e]) * z[uci[e]]))
+        z[i] = f32(acc * f32(1.0 / np.float64(dd)))
+    return z.astype(np.float64)
+
+
+@pytest.mark.parametrize("nx,ny", [(40, 40), (33, 70), (200, 31), (7, 512), (64, 33), (16, 1500)])
+def test_grid5_exact_solves(b2s, ctx, orc, nx, ny):
+    """5-point grid factors take the lane-per-grid-line schedule (exported as
+    "trsv.grid5"): one single-warp CTA per 32 lines, the boundary lines handed
+    between CTAs as epoch-tagged words.  Shapes with one and up to 47 CTAs, a
+    partial last warp and lines shorter than a warp; the IC(0) and ILU(0)
+    applies (FP64) equal the restatement bit for bit (applied twice, so the
+    second launch runs on the advanced epoch), and the FP32 factors' applies
+    equal an FP32 emulation of the schedules' arithmetic bit for bit."""
+    n, rp, ci, v = P.diffusion2d(nx, ny, seed=nx * ny)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    r = b2s.uniform(nx + ny, n)
+    for kind in ("ic0", "ilu0"):
+        M = b2s.Precond(ctx, A, b2s.PC_NAMES[kind])
+        assert M.sizes("trsv.grid5") == (nx, ny, 1), kind
+        po = orc.pc(orc.csr(n, n, rp, ci, v), kind)
+        want = po.apply(r)
+        assert np.array_equal(M.apply(r), want), kind
+        assert np.array_equal(M.apply(r), want), kind
+    for kind in ("ic0", "ilu0"):
+        M32 = b2s.Precond(ctx, A, b2s.PC_NAMES[kind], precision=b2s.FP32)
+        assert M32.sizes("trsv.grid5") == (nx, ny, 1), kind
+        if kind == "ic0":
+            L, U = M32.export("ic0.L"), M32.export("ic0.LT")
+            # L^T is stored strict: put the diagonal back from L (rows of L end with it)
+            lrp, lci, lv = L
+            d = lv[lrp[1:] - 1]
+            urp, uci, uv = U
+            rows = [(list(uci[urp[i]:urp[i + 1]]), list(uv[urp[i]:urp[i + 1]])) for i in range(n)]
+            urp2, uci2, uv2 = [0], [], []
+            for i, (c, vv) in enumerate(rows):
+                uci2 += [i] + c
+                uv2 += [d[i]] + vv
+                urp2.append(len(uci2))
+            U = (np.array(urp2), np.array(uci2), np.array(uv2))
+            want = _f32_apply(L, U, r, False)
+        else:
+            want = _f32_apply(M32.export("ilu0.L"), M32.export("ilu0.U"), r, True)
+        assert np.array_equal(M32.apply(r), want), kind
+
+
+def test_grid5_not_taken_elsewhere(b2s, ctx):
+    """Patterns that are not a 5-point grid's (7-point 3-D, random) and grids
+    with more than 4096 lines keep the chunked schedule."""
+    for n, rp, ci, v in (b2s.gen_poisson3d(12), P.random_spd(1500, 0.004, 3), P.diffusion2d(3, 4200, seed=3)):
+        A = b2s.CSR(ctx, n, n, rp, ci, v)
+        assert b2s.Precond(ctx, A, b2s.PC_IC0).sizes("trsv.grid5")[0] == 0
+
+
 @pytest.mark.parametrize("mat", ["poisson2d", "random", "poisson3d"])
 @pytest.mark.parametrize("trsv", [1, 2, 3])
 def test_ilu0_bit_exact(b2s, ctx, orc, mat, trsv):
