@@ -135,6 +135,27 @@ def test_grid5_exact_solves(b2s, ctx, orc, nx, ny):
         assert np.array_equal(M32.apply(r), want), kind
 
 
+@pytest.mark.parametrize("spread,rhs_lo", [(60, -40), (500, -700)])
+def test_grid5_division_bit_exact(b2s, ctx, orc, spread, rhs_lo):
+    """The grid schedule in FP64 across the binary64 range: a scaled 5-point
+    system D A D (D = 2^k, k in [0, spread]) with right-hand sides from
+    2^rhs_lo to 2^40; the IC(0) and ILU(0) applies must equal the restatement
+    bit for bit."""
+    nx, ny = 48, 70
+    n, rp, ci, v = P.diffusion2d(nx, ny, seed=spread)
+    rng = np.random.default_rng(spread + 1)
+    d = np.exp2(rng.integers(0, spread + 1, n).astype(np.float64))
+    rows = np.repeat(np.arange(n), np.diff(rp.astype(np.int64)))
+    vs = v * d[rows] * d[ci]
+    A = b2s.CSR(ctx, n, n, rp, ci, vs)
+    r = b2s.uniform(37, n) * np.exp2(rng.integers(rhs_lo, 41, n).astype(np.float64))
+    for kind in ("ic0", "ilu0"):
+        M = b2s.Precond(ctx, A, b2s.PC_NAMES[kind])
+        assert M.sizes("trsv.grid5") == (nx, ny, 1), kind
+        po = orc.pc(orc.csr(n, n, rp, ci, vs), kind)
+        assert np.array_equal(M.apply(r), po.apply(r)), kind
+
+
 def test_grid5_not_taken_elsewhere(b2s, ctx):
     """Patterns that are not a 5-point grid's (7-point 3-D, random) and grids
     with more than 4096 lines keep the chunked schedule."""
