@@ -13,7 +13,7 @@
 // an issue slot.  Lane 0 takes the neighbouring line from warp w - 1's lane 31
 // through epoch-tagged 64-bit words in global memory ({epoch, 32 value bits}:
 // one store publishes a value, no fence), published at the end of each group
-// of kGrid5Group steps, read a group ahead and checked when the group starts.
+// of kGrid5Group steps, read (half) a group ahead and checked when the group starts.
 // A level (anti-diagonal) costs one step: a shuffle, two products, two
 // differences and the divisor -- no shared-memory round trip and no barrier.
 //
@@ -168,6 +168,9 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid5(uint32_t B, uint32_t ny, u
     constexpr int G = kGrid5Group;
     constexpr int WPV = sizeof(XT) == 8 ? 2 : 1;  // exchange words per value
     constexpr bool MARK = sizeof(XT) == 8 && !UNIT;
+    // FP64 reads warp w - 1's words of the next group half way through a group,
+    // FP32 right after the check (each the faster on 512^2, measured)
+    constexpr bool NB_LATE = sizeof(XT) == 8;
     extern __shared__ __align__(16) unsigned long long g5_sm[];  // two groups of results
     XT* const stg = reinterpret_cast<XT*>(g5_sm);
     const uint32_t lane = threadIdx.x, nw = gridDim.x;
@@ -215,7 +218,7 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid5(uint32_t B, uint32_t ny, u
     double* o64 = out64 ? out64 : reinterpret_cast<double*>(x);
     const bool w64 = out64 != nullptr;
     auto write_back = [&](int pass, uint32_t sg, const XT* buf) {
-        const uint32_t l = (uint32_t)pass * 4u + (lane >> 3), u = lane & 7u;
+        const uint32_t l = (uint32_t)pass * (32u / G) + lane / G, u = lane % G;
         const uint32_t k = sg + u - l, ln = w * 32u + l;
         const bool p = ln < ny && k < B;
         const uint32_t i = ln * B + k, ii = LOWER ? i : n - 1u - i;
@@ -294,7 +297,7 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid5(uint32_t B, uint32_t ny, u
                 failed = true;
                 break;
             }
-            load_nb(s0 + G);  // the next group's words, checked when it starts
+            if constexpr (!NB_LATE) load_nb(s0 + G);  // the next group's words, checked when it starts
         }
         __syncwarp();  // the previous group's results are in stg for every lane
         XT* cur = stg + (g & 1u) * (G * 32);
@@ -323,6 +326,8 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid5(uint32_t B, uint32_t ny, u
             prev = active ? r : prev;  // inactive lanes compute garbage and keep prev
             cur[u * 32 + lane] = r;
             write_back(u, s0 - G, old);  // the previous group (none before the first: k falls off)
+            if constexpr (NB_LATE)
+                if (u == G / 2 - 1) load_nb(s0 + G);
         }
         if constexpr (MARK)
         {

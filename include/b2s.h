@@ -283,6 +283,9 @@ b2s_status b2s_pc_apply_device(b2s_ctx* ctx, b2s_pc* pc, const double* d_r, doub
  *                built on the device from closed forms; with the environment variable
  *                B2S_TILE_PLANNER=bfs at set-up the general breadth-first planner (host) lays them
  *                out instead, for grids up to 65536 rows (it gives the same bytes)
+ *   "trsv.grid5": sizes = {points per grid line B (0: the exact solves do not take the 5-point
+ *                grid schedule), grid lines, 1 if the factor's values are packed for it}; no
+ *                arrays (IC(0) and ILU(0) with the chunk schedule)
  * Query sizes with NULL arrays: sizes[0] = rows (+1 for rp), sizes[1] = nnz, sizes[2] = values. */
 b2s_status b2s_pc_export(b2s_ctx* ctx, b2s_pc* pc, const char* what, uint64_t* sizes, uint32_t* rp, uint32_t* ci,
                          double* v);
