@@ -203,10 +203,14 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid5(uint32_t B, uint32_t ny, u
         ++lk;
         ++li;
     };
-    // lane 0's words of warp w - 1 for the group starting at s0
+    // warp w - 1's words for the group starting at s0.  FP64 reads them in
+    // every lane (one broadcast request per word) and checks them with
+    // warp-uniform branches; FP32 in lane 0 alone (each the faster on 512^2,
+    // measured)
+    constexpr bool UNIFORM = sizeof(XT) == 8;
     unsigned long long nbw[G * WPV];
     auto load_nb = [&](uint32_t s0) {
-        if (lane == 0 && has_pred)
+        if ((UNIFORM || lane == 0) && has_pred)
 #pragma unroll
             for (int u = 0; u < G; ++u)
 #pragma unroll
@@ -253,49 +257,79 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid5(uint32_t B, uint32_t ny, u
     bool failed = false;
     for (; s0 < S; s0 += G, ++g)
     {
-        // lane 0: every word of this group must carry the epoch; re-read the others
+        // every word of this group must carry the epoch; the stale ones are read again
         XT nbv[G];
 #pragma unroll
         for (int u = 0; u < G; ++u) nbv[u] = XT(0);
         if (has_pred)
         {
-            int fail = 0;
-            if (lane == 0)
-            {
-                for (unsigned polls = 0;; ++polls)
-                {
-                    bool all = true;
-#pragma unroll
-                    for (int u = 0; u < G; ++u)
-#pragma unroll
-                        for (int c = 0; c < WPV; ++c)
-                            if (s0 + u < B && (uint32_t)(nbw[u * WPV + c] >> 32) != epoch)
-                            {
-                                all = false;
-                                nbw[u * WPV + c] = g5_ld(nbg + (size_t)(s0 + u) * WPV + c);
-                            }
-                    if (all) break;
-                    if (polls >= kGrid5Polls || ld_err(err) != 0)
-                    {
-                        fail = 1;
-                        atomicCAS(err, 0, (int)B2S_TIMEOUT);
-                        break;
-                    }
-                }
+            auto fresh = [&]() {
+                bool all = true;
 #pragma unroll
                 for (int u = 0; u < G; ++u)
-                {
-                    if constexpr (WPV == 1)
-                        nbv[u] = (XT)__uint_as_float((uint32_t)nbw[u]);
-                    else
-                        nbv[u] = (XT)__longlong_as_double(
-                            (long long)(((nbw[2 * u + 1] & 0xffffffffull) << 32) | (nbw[2 * u] & 0xffffffffull)));
-                }
-            }
-            if (__shfl_sync(0xffffffffu, fail, 0))
+#pragma unroll
+                    for (int c = 0; c < WPV; ++c)
+                        all &= s0 + u >= B || (uint32_t)(nbw[u * WPV + c] >> 32) == epoch;
+                return all;
+            };
+            auto reread = [&]() {
+#pragma unroll
+                for (int u = 0; u < G; ++u)
+#pragma unroll
+                    for (int c = 0; c < WPV; ++c)
+                        if (s0 + u < B && (uint32_t)(nbw[u * WPV + c] >> 32) != epoch)
+                            nbw[u * WPV + c] = g5_ld(nbg + (size_t)(s0 + u) * WPV + c);
+            };
+            if constexpr (UNIFORM)
             {
-                failed = true;
-                break;
+                if (!__all_sync(0xffffffffu, fresh()))
+                    for (unsigned polls = 0;; ++polls)
+                    {
+                        reread();
+                        if (__all_sync(0xffffffffu, fresh())) break;
+                        if (__any_sync(0xffffffffu, polls >= kGrid5Polls || ld_err(err) != 0))
+                        {
+                            if (lane == 0) atomicCAS(err, 0, (int)B2S_TIMEOUT);
+                            failed = true;
+                            break;
+                        }
+                    }
+            }
+            else
+            {
+                int fail = 0;
+                if (lane == 0)
+                    for (unsigned polls = 0;; ++polls)
+                    {
+                        bool all = true;
+#pragma unroll
+                        for (int u = 0; u < G; ++u)
+#pragma unroll
+                            for (int c = 0; c < WPV; ++c)
+                                if (s0 + u < B && (uint32_t)(nbw[u * WPV + c] >> 32) != epoch)
+                                {
+                                    all = false;
+                                    nbw[u * WPV + c] = g5_ld(nbg + (size_t)(s0 + u) * WPV + c);
+                                }
+                        if (all) break;
+                        if (polls >= kGrid5Polls || ld_err(err) != 0)
+                        {
+                            fail = 1;
+                            atomicCAS(err, 0, (int)B2S_TIMEOUT);
+                            break;
+                        }
+                    }
+                failed = __shfl_sync(0xffffffffu, fail, 0) != 0;
+            }
+            if (failed) break;
+#pragma unroll
+            for (int u = 0; u < G; ++u)
+            {
+                if constexpr (WPV == 1)
+                    nbv[u] = (XT)__uint_as_float((uint32_t)nbw[u]);
+                else
+                    nbv[u] = (XT)__longlong_as_double(
+                        (long long)(((nbw[2 * u + 1] & 0xffffffffull) << 32) | (nbw[2 * u] & 0xffffffffull)));
             }
             if constexpr (!NB_LATE) load_nb(s0 + G);  // the next group's words, checked when it starts
         }
