@@ -153,7 +153,7 @@ KERNELS = {
     "trsv_c5": "k_trsv_grid5: FP32 IC(0) exact apply (L then L^T, 5-point grid schedule) on a 512^2 GRF system (C5)",
     "trsv_c5_fp64": "k_trsv_grid5: FP64 IC(0) exact apply (5-point grid schedule) on a 512^2 GRF system (C5)",
     "trsv_c5_j8": "k_trsv_band: FP32 IC(0) apply with 8 Jacobi sweeps per triangle on a 512^2 GRF system (C5)",
-    "trsv_c2": "k_trsv_chunk: FP64 ILU(0) apply on the 128^3 Poisson matrix (C2)",
+    "trsv_c2": "k_trsv_grid7: FP64 ILU(0) exact apply (7-point grid schedule) on the 128^3 Poisson matrix (C2)",
     "btrsv_c4": "k_btrsv_chunk: FP64 block ILU(0) apply on the Q1 elasticity matrix (C4, 64^3 elements)",
     "vcycle_c2": "SA-AMG V-cycle (k_jacobi, BAIJ matvecs, k_dense_solve) on C2",
     "vcycle_c4": "block SA-AMG V-cycle on the Q1 elasticity matrix (C4, 64^3 elements, 3x3 blocks)",

@@ -28,6 +28,7 @@
 #include "pcg_band.cuh"
 #include "pcg_tile.cuh"
 #include "trsv_grid5.cuh"
+#include "trsv_grid7.cuh"
 
 #include <cstdlib>
 #include <cstring>
@@ -508,6 +509,7 @@ struct Tri
     SyncFree sf;
     ChunkSchedule cs;
     Grid5Tri g5;  // 5-point grid factors: the exact solve with a lane per grid line
+    Grid7Tri g7;  // 7-point grid factors: the same with planes handed on
     bool has_chunks = false, sched_ready = false;
     std::vector<uint32_t> h_level;  // host copy of the rows' levels (compute_levels), when known
     int sweeps = 8;                 // B2S_TRSV_JACOBI: sweeps after pass 0
@@ -597,6 +599,8 @@ struct Tri
             run_sweeps<LOWER, UNIT, VT, XT, RT>(ctx, v, d, rhs, x, out64, done);
         else if (mode == B2S_TRSV_CHUNK && g5.usable<VT, XT>() && g5.packed_v == (const void*)v)
             g5.run<LOWER, UNIT, VT, XT, RT>(ctx, rhs, x, out64, done);
+        else if (mode == B2S_TRSV_CHUNK && g7.usable<VT, XT>() && g7.packed_v == (const void*)v)
+            g7.run<LOWER, UNIT, VT, XT, RT>(ctx, rhs, x, out64, done);
         else if (mode == B2S_TRSV_CHUNK && has_chunks && cs.usable<VT, XT, RT>())
             cs.run<LOWER, UNIT, VT, XT, RT>(ctx, v, d, rhs, x, out64, done);
         else
@@ -651,6 +655,7 @@ struct Tri
     {
         if (has_chunks && sizeof(VT) <= cs.plan_vs) cs.pack<VT>(ctx, v, d);
         g5.pack<VT>(ctx, m->rp.p, m->ci.p, v, d, lower, unit);
+        g7.pack<VT>(ctx, m->rp.p, m->ci.p, v, d, lower, unit);
         if constexpr (sizeof(VT) == 4)
         {
             if (band.T && n)
@@ -770,6 +775,16 @@ static void export_grid5(const Tri& fwd, const Tri& bwd, uint64_t* sizes)
     sizes[0] = on ? fwd.g5.B : 0;
     sizes[1] = on ? fwd.g5.ny : 0;
     sizes[2] = on && fwd.g5.packed_v && bwd.g5.packed_v ? 1 : 0;
+}
+
+// "trsv.grid7": sizes = {B, ny, nz} of the 7-point grid schedule when both
+// triangles take it (packed), else zeros
+static void export_grid7(const Tri& fwd, const Tri& bwd, uint64_t* sizes)
+{
+    const bool on = fwd.g7.on && bwd.g7.on && fwd.g7.packed_v && bwd.g7.packed_v;
+    sizes[0] = on ? fwd.g7.B : 0;
+    sizes[1] = on ? fwd.g7.ny : 0;
+    sizes[2] = on ? fwd.g7.nz : 0;
 }
 
 // the grid row length B of a lower triangle that is a 5-point grid's, else 0
@@ -1092,6 +1107,7 @@ struct PcIC0 final : PcImpl
         if (what == "levels.L") return export_levels(ctx, fwd, sizes, ci);
         if (what == "levels.U") return export_levels(ctx, bwd, sizes, ci);
         if (what == "trsv.grid5") return export_grid5(fwd, bwd, sizes);
+        if (what == "trsv.grid7") return export_grid7(fwd, bwd, sizes);
         if (what == "pcg.tiles")  // the tiled persistent PCG kernel: tiles (0: not planned), rows per thread, smem
         {
             sizes[0] = tiles_ready ? tile_count : 0;
@@ -1319,11 +1335,24 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     pc->fwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.lo_plan : nullptr, vs);
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
     if (pc->mode == B2S_TRSV_CHUNK && have_pattern && n)
-        if (const uint32_t B = grid5_lower_b(n, hrp, hci))  // L^T of a grid's L is the grid's upper triangle
+    {
+        // L^T of a grid's L is the grid's upper triangle
+        if (const uint32_t B = grid5_lower_b(n, hrp, hci))
         {
             pc->fwd.g5.enable(B, n / B);
             pc->bwd.g5.enable(B, n / B);
         }
+        else
+        {
+            uint32_t dims[3];
+            grid7_dims(n, hrp.data(), hci.data(), dims);
+            if (dims[0])
+            {
+                pc->fwd.g7.enable(dims[0], dims[1], dims[2]);
+                pc->bwd.g7.enable(dims[0], dims[1], dims[2]);
+            }
+        }
+    }
     if (sweeps)
     {
         pc->fwd.prepare_sweeps(ctx, nsweeps, seg, pc->fp32, &ha.lo_band);
@@ -1385,6 +1414,7 @@ struct PcILU0 final : PcImpl
         if (what == "ilu0.L") return export_csr(ctx, L, sizes, rp, ci, v);
         if (what == "ilu0.U") return export_csr(ctx, U, sizes, rp, ci, v);
         if (what == "trsv.grid5") return export_grid5(fwd, bwd, sizes);
+        if (what == "trsv.grid7") return export_grid7(fwd, bwd, sizes);
         if (what == "levels.L") return export_levels(ctx, fwd, sizes, ci);
         if (what == "levels.U") return export_levels(ctx, bwd, sizes, ci);
         PcImpl::export_data(ctx, what, sizes, rp, ci, v);
@@ -1472,12 +1502,26 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     pc->fwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.lo_plan : nullptr, vs);
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
     if (pc->mode == B2S_TRSV_CHUNK && n)
+    {
         if (const uint32_t B = grid5_lower_b(n, lrp, lci))
+        {
             if (grid5_triangle(n, urp.data(), uci.data(), B, false))
             {
                 pc->fwd.g5.enable(B, n / B);
                 pc->bwd.g5.enable(B, n / B);
             }
+        }
+        else
+        {
+            uint32_t dims[3];
+            grid7_dims(n, lrp.data(), lci.data(), dims);
+            if (dims[0] && grid7_triangle(n, urp.data(), uci.data(), dims[0], dims[1], false))
+            {
+                pc->fwd.g7.enable(dims[0], dims[1], dims[2]);
+                pc->bwd.g7.enable(dims[0], dims[1], dims[2]);
+            }
+        }
+    }
     if (pc->mode == B2S_TRSV_JACOBI)
     {
         const int k = sweep_count(o);

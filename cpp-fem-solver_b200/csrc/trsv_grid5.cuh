@@ -42,7 +42,15 @@ namespace b2s {
 constexpr int kGrid5Group = 8;                   // steps between a warp's hand-overs and checks
 constexpr uint32_t kGrid5MaxLines = 4096;        // 128 CTAs
 constexpr uint32_t kGrid5MinSmem = 120u << 10;   // one CTA per SM
-constexpr unsigned kGrid5Polls = 1u << 20;       // polls of a group's words before giving up
+
+// polls of one group's hand-over words before a grid schedule's warp gives
+// up (B2S_TIMEOUT): the context's wait bounds (b2s_ctx_set_wait_limits), spin
+// and sleep budgets together, as the grid schedules never sleep
+inline unsigned grid_polls(const b2s_ctx* ctx)
+{
+    const uint64_t p = (uint64_t)ctx->wait_fast_polls + ctx->wait_slow_polls;
+    return (unsigned)std::min<uint64_t>(std::max<uint64_t>(p, 1), 0xffffffffu);
+}
 
 // one packed slot: the point's two coefficients, its divisor (d; the
 // reciprocal rounded once from FP64 for an FP32 factor; 1 for a unit
@@ -162,7 +170,8 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid5(uint32_t B, uint32_t ny, u
                                                       const G5Slot<VT>* __restrict__ slot,
                                                       const RT* __restrict__ rhs, XT* __restrict__ x,
                                                       double* __restrict__ out64, const int* done,
-                                                      unsigned long long* ew, uint32_t* ctl, int* err)
+                                                      unsigned long long* ew, uint32_t* ctl, int* err,
+                                                      unsigned polls_max)
 {
     if (done && *done) return;
     constexpr int G = kGrid5Group;
@@ -287,7 +296,7 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid5(uint32_t B, uint32_t ny, u
                     {
                         reread();
                         if (__all_sync(0xffffffffu, fresh())) break;
-                        if (__any_sync(0xffffffffu, polls >= kGrid5Polls || ld_err(err) != 0))
+                        if (__any_sync(0xffffffffu, polls >= polls_max || ld_err(err) != 0))
                         {
                             if (lane == 0) atomicCAS(err, 0, (int)B2S_TIMEOUT);
                             failed = true;
@@ -312,7 +321,7 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid5(uint32_t B, uint32_t ny, u
                                     nbw[u * WPV + c] = g5_ld(nbg + (size_t)(s0 + u) * WPV + c);
                                 }
                         if (all) break;
-                        if (polls >= kGrid5Polls || ld_err(err) != 0)
+                        if (polls >= polls_max || ld_err(err) != 0)
                         {
                             fail = 1;
                             atomicCAS(err, 0, (int)B2S_TIMEOUT);
@@ -489,7 +498,7 @@ struct Grid5Tri
             attr = true;
         }
         B2S_LAUNCH(ctx, kern, nw, 32, kGrid5MinSmem, B, ny, grid5_steps(B), c, rhs, x, out64, done, ew.p, ctl.p,
-                   ctx->errword());
+                   ctx->errword(), grid_polls(ctx));
     }
 };
 

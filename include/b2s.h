@@ -75,9 +75,11 @@ uint64_t b2s_ctx_kernel_launches(const b2s_ctx* ctx);
 /* Bounds of the device-side waits of the chunked triangular solves on ctx
  * (IC(0) / ILU(0) / block ILU(0) with B2S_TRSV_CHUNK, the default): a wait
  * polls spin_polls times without sleeping, then sleeps 1 us per poll, drawing
- * on a budget of sleep_polls per thread for the whole launch.  A wait that
- * runs out, and every later wait of the same launch, gives up at once and the
- * call reports B2S_TIMEOUT (the synchronous calls at their end, the _device
+ * on a budget of sleep_polls per thread for the whole launch.  The 5- and
+ * 7-point grid schedules of the same solves poll a group's hand-over words
+ * up to spin_polls + sleep_polls times (at least once) without sleeping.  A
+ * wait that runs out, and every later wait of the same launch, gives up at
+ * once and the call reports B2S_TIMEOUT (the synchronous calls at their end, the _device
  * ones at the next b2s_ctx_synchronize or solve).  (0, 0) restores the
  * defaults (2^20 and 2^20, about one second).  No counterpart in the
  * reference (its solves are sequential). */

@@ -195,3 +195,28 @@ def diffusion2d(nx, ny, seed):
             if y + 1 < ny: R.append(i); Cc.append(i + nx); V.append(-ky[y + 1, x])
     rp, ci, v = coo_to_csr(nx * ny, nx * ny, R, Cc, V)
     return nx * ny, rp, ci, v
+
+
+def diffusion3d(nx, ny, nz, seed):
+    """-div(k grad u) on an nx x ny x nz grid (x fastest, then y), 7-point,
+    face coefficients k = exp(N(0,1)) per face, Dirichlet outside: SPD."""
+    rng = np.random.default_rng(seed)
+    kx = np.exp(rng.standard_normal((nz, ny, nx + 1)))
+    ky = np.exp(rng.standard_normal((nz, ny + 1, nx)))
+    kz = np.exp(rng.standard_normal((nz + 1, ny, nx)))
+    R, Cc, V = [], [], []
+    for z in range(nz):
+        for y in range(ny):
+            for x in range(nx):
+                i = (z * ny + y) * nx + x
+                d = kx[z, y, x] + kx[z, y, x + 1] + ky[z, y, x] + ky[z, y + 1, x] + kz[z, y, x] + kz[z + 1, y, x]
+                R.append(i); Cc.append(i); V.append(d)
+                if x > 0: R.append(i); Cc.append(i - 1); V.append(-kx[z, y, x])
+                if x + 1 < nx: R.append(i); Cc.append(i + 1); V.append(-kx[z, y, x + 1])
+                if y > 0: R.append(i); Cc.append(i - nx); V.append(-ky[z, y, x])
+                if y + 1 < ny: R.append(i); Cc.append(i + nx); V.append(-ky[z, y + 1, x])
+                if z > 0: R.append(i); Cc.append(i - nx * ny); V.append(-kz[z, y, x])
+                if z + 1 < nz: R.append(i); Cc.append(i + nx * ny); V.append(-kz[z + 1, y, x])
+    n = nx * ny * nz
+    rp, ci, v = coo_to_csr(n, n, R, Cc, V)
+    return n, rp, ci, v

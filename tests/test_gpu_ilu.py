@@ -116,23 +116,28 @@ def test_grid5_exact_solves(b2s, ctx, orc, nx, ny):
     for kind in ("ic0", "ilu0"):
         M32 = b2s.Precond(ctx, A, b2s.PC_NAMES[kind], precision=b2s.FP32)
         assert M32.sizes("trsv.grid5") == (nx, ny, 1), kind
-        if kind == "ic0":
-            L, U = M32.export("ic0.L"), M32.export("ic0.LT")
-            # L^T is stored strict: put the diagonal back from L (rows of L end with it)
-            lrp, lci, lv = L
-            d = lv[lrp[1:] - 1]
-            urp, uci, uv = U
-            rows = [(list(uci[urp[i]:urp[i + 1]]), list(uv[urp[i]:urp[i + 1]])) for i in range(n)]
-            urp2, uci2, uv2 = [0], [], []
-            for i, (c, vv) in enumerate(rows):
-                uci2 += [i] + c
-                uv2 += [d[i]] + vv
-                urp2.append(len(uci2))
-            U = (np.array(urp2), np.array(uci2), np.array(uv2))
-            want = _f32_apply(L, U, r, False)
-        else:
-            want = _f32_apply(M32.export("ilu0.L"), M32.export("ilu0.U"), r, True)
-        assert np.array_equal(M32.apply(r), want), kind
+        assert np.array_equal(M32.apply(r), _f32_want(M32, kind, r)), kind
+
+
+def _f32_want(M32, kind, r):
+    """The FP32 emulation (_f32_apply) of an FP32 factor's exact apply, from
+    the factor the preconditioner exports."""
+    n = len(r)
+    if kind == "ic0":
+        L, U = M32.export("ic0.L"), M32.export("ic0.LT")
+        # L^T is stored strict: put the diagonal back from L (rows of L end with it)
+        lrp, lci, lv = L
+        d = lv[lrp[1:] - 1]
+        urp, uci, uv = U
+        rows = [(list(uci[urp[i]:urp[i + 1]]), list(uv[urp[i]:urp[i + 1]])) for i in range(n)]
+        urp2, uci2, uv2 = [0], [], []
+        for i, (c, vv) in enumerate(rows):
+            uci2 += [i] + c
+            uv2 += [d[i]] + vv
+            urp2.append(len(uci2))
+        U = (np.array(urp2), np.array(uci2), np.array(uv2))
+        return _f32_apply(L, U, r, False)
+    return _f32_apply(M32.export("ilu0.L"), M32.export("ilu0.U"), r, True)
 
 
 @pytest.mark.parametrize("spread,rhs_lo", [(60, -40), (500, -700)])
@@ -156,12 +161,63 @@ def test_grid5_division_bit_exact(b2s, ctx, orc, spread, rhs_lo):
         assert np.array_equal(M.apply(r), po.apply(r)), kind
 
 
+@pytest.mark.parametrize("nx,ny,nz", [(9, 40, 5), (33, 33, 3), (4, 70, 6), (64, 16, 9), (17, 96, 4), (12, 12, 12)])
+def test_grid7_exact_solves(b2s, ctx, orc, nx, ny, nz):
+    """7-point grid factors take the plane-by-plane grid schedule (exported as
+    "trsv.grid7"): one warp per 32 lines of a plane, the plane's last line
+    handed to the next block and every value to the next plane as
+    epoch-tagged words.  Shapes with partial warps, up to 3 blocks per plane,
+    lines shorter than a warp and up to 12 planes; the IC(0) and ILU(0)
+    applies (FP64) equal the restatement bit for bit (applied twice: the
+    second launch runs on the advanced epoch), and the FP32 factors' applies
+    equal the FP32 emulation bit for bit."""
+    n, rp, ci, v = P.diffusion3d(nx, ny, nz, seed=nx * ny + nz)
+    A = b2s.CSR(ctx, n, n, rp, ci, v)
+    r = b2s.uniform(nx + ny + nz, n)
+    for kind in ("ic0", "ilu0"):
+        M = b2s.Precond(ctx, A, b2s.PC_NAMES[kind])
+        assert M.sizes("trsv.grid7") == (nx, ny, nz), kind
+        assert M.sizes("trsv.grid5")[0] == 0, kind
+        po = orc.pc(orc.csr(n, n, rp, ci, v), kind)
+        want = po.apply(r)
+        assert np.array_equal(M.apply(r), want), kind
+        assert np.array_equal(M.apply(r), want), kind
+    for kind in ("ic0", "ilu0"):
+        M32 = b2s.Precond(ctx, A, b2s.PC_NAMES[kind], precision=b2s.FP32)
+        assert M32.sizes("trsv.grid7") == (nx, ny, nz), kind
+        assert np.array_equal(M32.apply(r), _f32_want(M32, kind, r)), kind
+
+
+def test_grid7_division_bit_exact(b2s, ctx, orc):
+    """The 7-point grid schedule in FP64 across the binary64 range (scaled
+    system D A D, D = 2^k with k in [0, 500], right-hand sides from 2^-700
+    to 2^40: quotients reach the subnormal range, so groups are redone with
+    the division); IC(0) and ILU(0) applies equal the restatement bit for bit."""
+    nx, ny, nz = 20, 36, 5
+    n, rp, ci, v = P.diffusion3d(nx, ny, nz, seed=5)
+    rng = np.random.default_rng(6)
+    d = np.exp2(rng.integers(0, 501, n).astype(np.float64))
+    rows = np.repeat(np.arange(n), np.diff(rp.astype(np.int64)))
+    vs = v * d[rows] * d[ci]
+    A = b2s.CSR(ctx, n, n, rp, ci, vs)
+    r = b2s.uniform(41, n) * np.exp2(rng.integers(-700, 41, n).astype(np.float64))
+    for kind in ("ic0", "ilu0"):
+        M = b2s.Precond(ctx, A, b2s.PC_NAMES[kind])
+        assert M.sizes("trsv.grid7") == (nx, ny, nz), kind
+        po = orc.pc(orc.csr(n, n, rp, ci, vs), kind)
+        assert np.array_equal(M.apply(r), po.apply(r)), kind
+
+
 def test_grid5_not_taken_elsewhere(b2s, ctx):
     """Patterns that are not a 5-point grid's (7-point 3-D, random) and grids
     with more than 4096 lines keep the chunked schedule."""
     for n, rp, ci, v in (b2s.gen_poisson3d(12), P.random_spd(1500, 0.004, 3), P.diffusion2d(3, 4200, seed=3)):
         A = b2s.CSR(ctx, n, n, rp, ci, v)
         assert b2s.Precond(ctx, A, b2s.PC_IC0).sizes("trsv.grid5")[0] == 0
+    # nor the 7-point schedule: random, 2-D, and a 3-D grid with one point per line
+    for n, rp, ci, v in (P.random_spd(1500, 0.004, 3), P.diffusion2d(40, 40, seed=4), P.diffusion3d(1, 30, 20, seed=4)):
+        A = b2s.CSR(ctx, n, n, rp, ci, v)
+        assert b2s.Precond(ctx, A, b2s.PC_IC0).sizes("trsv.grid7")[0] == 0
 
 
 @pytest.mark.parametrize("mat", ["poisson2d", "random", "poisson3d"])
@@ -249,17 +305,34 @@ def test_grf_ic0_pcg_parity(b2s, ctx, orc):
     assert rel(x, xo) < 100 * 2.2e-15, rel(x, xo)
 
 
-def test_chunk_wait_timeout_reported(b2s, ctx):
-    """The chunked solve's waits are bounded per launch.  With the bounds cut
-    to one poll and no sleeps, the ILU(0) apply on the 128^3 Poisson matrix
-    (hundreds of chunks, each needing rows that the chunk before it is still
-    computing) gives up: the call reports B2S_TIMEOUT and returns at once,
-    every later wait of the launch skipped.  The context stays usable: with
-    the default bounds the same apply gives the exact result again."""
+@pytest.mark.parametrize("schedule", ["chunk", "grid7"])
+def test_chunk_wait_timeout_reported(b2s, ctx, schedule):
+    """The exact solves' waits are bounded per launch.  With the bounds cut to
+    one poll and no sleeps, the ILU(0) apply on the 128^3 Poisson matrix
+    gives up: on the 7-point grid schedule (512 warps, each waiting on the
+    warps of the block and plane before it), and on the chunked schedule
+    (hundreds of chunks, each needing rows the chunk before it is still
+    computing; one symmetric pair of entries added at rows 0 and 2 keeps the
+    pattern off the grid schedule).  The call reports B2S_TIMEOUT and
+    returns at once, every later wait of the launch skipped.  The context
+    stays usable: with the default bounds the same apply gives the exact
+    result again."""
     import time
     n, rp, ci, v = b2s.gen_poisson3d(128)
+    if schedule == "chunk":
+        rp = rp.astype(np.int64)
+        # row 0 gets (0, 2) after its entry (0, 1); row 2 gets (2, 0) first
+        p0 = int(np.searchsorted(ci[rp[0]:rp[1]], 2)) + rp[0]
+        ci = np.insert(ci, p0, 2)
+        v = np.insert(v, p0, -0.01)
+        rp[1:] += 1
+        ci = np.insert(ci, rp[2], 0)
+        v = np.insert(v, rp[2], -0.01)
+        rp[3:] += 1
+        rp = rp.astype(np.uint32)
     A = b2s.CSR(ctx, n, n, rp, ci, v)
     M = b2s.Precond(ctx, A, b2s.PC_ILU0)
+    assert (M.sizes("trsv.grid7")[0] > 0) == (schedule == "grid7")
     r = b2s.uniform(21, n)
     z0 = M.apply(r)
     ctx.set_wait_limits(1, 0)
