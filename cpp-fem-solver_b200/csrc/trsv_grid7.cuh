@@ -127,6 +127,9 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid7(uint32_t B, uint32_t ny, u
     constexpr int G = kGrid5Group;
     constexpr int WPV = sizeof(XT) == 8 ? 2 : 1;  // exchange words per value
     constexpr bool MARK = sizeof(XT) == 8 && !UNIT;
+    // FP32 reads the next group's words half way through a group, FP64 right
+    // after the check (each the faster on 128^3, measured)
+    constexpr bool NB_LATE = sizeof(XT) == 4;
     extern __shared__ __align__(16) unsigned long long g7_sm[];  // two groups of results
     XT* const stg = reinterpret_cast<XT*>(g7_sm);
     const uint32_t lane = threadIdx.x, nw = gridDim.x;
@@ -269,8 +272,8 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid7(uint32_t B, uint32_t ny, u
             nbv[u] = has_y ? word_value(&nbw[u * WPV]) : XT(0);
             zbv[u] = has_z ? word_value(&zbw[u * WPV]) : XT(0);
         }
-        load_nb(s0 + G);  // the next group's words, checked when it starts
-        __syncwarp();     // the previous group's results are in stg for every lane
+        if constexpr (!NB_LATE) load_nb(s0 + G);  // the next group's words, checked when it starts
+        __syncwarp();  // the previous group's results are in stg for every lane
         XT* cur = stg + (g & 1u) * (G * 32);
         const XT* old = stg + ((g & 1u) ^ 1u) * (G * 32);
         const uint32_t kg = k0 + s0;
@@ -296,6 +299,8 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid7(uint32_t B, uint32_t ny, u
             prev = active ? r : prev;
             cur[u * 32 + lane] = r;
             write_back(u, s0 - G, old);
+            if constexpr (NB_LATE)
+                if (u == G / 2 - 1) load_nb(s0 + G);
             if constexpr (!MARK)
             {
                 // this step's value to the next plane's warp ([step][lane])
