@@ -796,6 +796,45 @@ static uint32_t grid5_lower_b(uint32_t n, const std::vector<uint32_t>& rp, const
     return B && grid5_triangle(n, rp.data(), ci.data(), B, true) ? B : 0u;
 }
 
+// The grid schedule that the exact solves of a factor take, found from L's
+// pattern before any planning (a factor that takes one needs no chunk plans);
+// ILU(0) passes U's pattern to be checked too (IC(0)'s L^T is the grid's).
+struct GridShape
+{
+    uint32_t b5 = 0, d7[3] = {0, 0, 0};
+    bool any() const { return b5 || d7[0]; }
+};
+static GridShape grid_shape(uint32_t n, const std::vector<uint32_t>& lrp, const std::vector<uint32_t>& lci,
+                            const std::vector<uint32_t>* urp, const std::vector<uint32_t>* uci)
+{
+    GridShape g;
+    if (!n) return g;
+    if (const uint32_t B = grid5_lower_b(n, lrp, lci))
+    {
+        if (Grid5Tri::fits(B, n / B) && (!urp || grid5_triangle(n, urp->data(), uci->data(), B, false))) g.b5 = B;
+        return g;
+    }
+    uint32_t d[3];
+    grid7_dims(n, lrp.data(), lci.data(), d);
+    if (d[0] && Grid7Tri::fits(d[0], d[1], d[2]) &&
+        (!urp || grid7_triangle(n, urp->data(), uci->data(), d[0], d[1], false)))
+        std::copy(d, d + 3, g.d7);
+    return g;
+}
+static void enable_grid(Tri& fwd, Tri& bwd, const GridShape& g, uint32_t n)
+{
+    if (g.b5)
+    {
+        fwd.g5.enable(g.b5, n / g.b5);
+        bwd.g5.enable(g.b5, n / g.b5);
+    }
+    else if (g.d7[0])
+    {
+        fwd.g7.enable(g.d7[0], g.d7[1], g.d7[2]);
+        bwd.g7.enable(g.d7[0], g.d7[1], g.d7[2]);
+    }
+}
+
 static void copy_pattern(b2s_ctx* ctx, const Csr32& M, std::vector<uint32_t>& rp, std::vector<uint32_t>& ci)
 {
     rp.resize((size_t)M.n + 1);
@@ -1249,6 +1288,12 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     }
     else
         need_pattern();
+    GridShape gs;
+    if (ha.chunked && have_pattern)
+    {
+        gs = grid_shape(n, hrp, hci, nullptr, nullptr);
+        if (gs.any()) ha.chunked = false;  // the grid schedule takes the exact solves
+    }
     ha.th = std::thread([&ha, &hrp, &hci, &pc, ps, bfs, n, vs, sweeps, nsweeps, seg, sm_count, fp32, tile_smem] {
         try
         {
@@ -1334,25 +1379,7 @@ std::unique_ptr<PcImpl> make_pc_ic0_ex(b2s_ctx* ctx, const CsrDev& A, const b2s_
     pc->bwd.h_level = std::move(ha.up_level);
     pc->fwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.lo_plan : nullptr, vs);
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
-    if (pc->mode == B2S_TRSV_CHUNK && have_pattern && n)
-    {
-        // L^T of a grid's L is the grid's upper triangle
-        if (const uint32_t B = grid5_lower_b(n, hrp, hci))
-        {
-            pc->fwd.g5.enable(B, n / B);
-            pc->bwd.g5.enable(B, n / B);
-        }
-        else
-        {
-            uint32_t dims[3];
-            grid7_dims(n, hrp.data(), hci.data(), dims);
-            if (dims[0])
-            {
-                pc->fwd.g7.enable(dims[0], dims[1], dims[2]);
-                pc->bwd.g7.enable(dims[0], dims[1], dims[2]);
-            }
-        }
-    }
+    enable_grid(pc->fwd, pc->bwd, gs, n);
     if (sweeps)
     {
         pc->fwd.prepare_sweeps(ctx, nsweeps, seg, pc->fp32, &ha.lo_band);
@@ -1454,6 +1481,12 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     pc->fwd.ensure_sched(ctx);
     HostAnalysis ha;
     ha.chunked = pc->mode == B2S_TRSV_CHUNK && n;
+    GridShape gs;
+    if (ha.chunked)
+    {
+        gs = grid_shape(n, lrp, lci, &urp, &uci);
+        if (gs.any()) ha.chunked = false;  // the grid schedule takes the exact solves
+    }
     ha.th = std::thread([&ha, &lrp, &lci, &urp, &uci, &pc, n, vs] {
         try
         {
@@ -1501,27 +1534,7 @@ std::unique_ptr<PcImpl> make_pc_ilu0(b2s_ctx* ctx, const CsrDev& A, const b2s_pc
     pc->bwd.h_level = std::move(ha.up_level);
     pc->fwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.lo_plan : nullptr, vs);
     pc->bwd.load_chunks(ctx, pc->mode, ha.chunked ? &ha.up_plan : nullptr, vs);
-    if (pc->mode == B2S_TRSV_CHUNK && n)
-    {
-        if (const uint32_t B = grid5_lower_b(n, lrp, lci))
-        {
-            if (grid5_triangle(n, urp.data(), uci.data(), B, false))
-            {
-                pc->fwd.g5.enable(B, n / B);
-                pc->bwd.g5.enable(B, n / B);
-            }
-        }
-        else
-        {
-            uint32_t dims[3];
-            grid7_dims(n, lrp.data(), lci.data(), dims);
-            if (dims[0] && grid7_triangle(n, urp.data(), uci.data(), dims[0], dims[1], false))
-            {
-                pc->fwd.g7.enable(dims[0], dims[1], dims[2]);
-                pc->bwd.g7.enable(dims[0], dims[1], dims[2]);
-            }
-        }
-    }
+    enable_grid(pc->fwd, pc->bwd, gs, n);
     if (pc->mode == B2S_TRSV_JACOBI)
     {
         const int k = sweep_count(o);

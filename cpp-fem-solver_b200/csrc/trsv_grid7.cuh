@@ -391,12 +391,16 @@ struct Grid7Tri
     DBuf<uint32_t> ctl;
 
     uint32_t warps() const { return (ny + 31) / 32 * nz; }
+    static bool fits(uint32_t b, uint32_t y, uint32_t z)
+    {
+        return b >= 2 && y >= 2 && z >= 2 && (uint64_t)(y + 31) / 32 * z <= kGrid7MaxWarps;
+    }
     void enable(uint32_t b, uint32_t y, uint32_t z)
     {
         B = b;
         ny = y;
         nz = z;
-        on = B >= 2 && ny >= 2 && nz >= 2 && warps() <= kGrid7MaxWarps;
+        on = fits(B, ny, nz);
     }
     template <typename VT, typename XT>
     bool usable() const
