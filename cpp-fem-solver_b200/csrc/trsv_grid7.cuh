@@ -301,16 +301,18 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid7(uint32_t B, uint32_t ny, u
             write_back(u, s0 - G, old);
             if constexpr (NB_LATE)
                 if (u == G / 2 - 1) load_nb(s0 + G);
-            if constexpr (!MARK)
+            // this step's value to the next plane's warp ([step][lane]); with the
+            // FP64 quotient only while no lane of the group has needed the
+            // division yet (a redo keeps the earlier steps' values: both
+            // roundings are correct), the rest after the group
+            bool pz = pub_z;
+            if constexpr (MARK) pz = pz && !__any_sync(0xffffffffu, bad);
+            if constexpr (WPV == 1)
+                g5_st_if(pz, zo + (size_t)(s0 + u) * 32u, etag | __float_as_uint((float)r));
+            else
             {
-                // this step's value to the next plane's warp ([step][lane])
-                if constexpr (WPV == 1)
-                    g5_st_if(pub_z, zo + (size_t)(s0 + u) * 32u, etag | __float_as_uint((float)r));
-                else
-                {
-                    const unsigned long long bits = (unsigned long long)__double_as_longlong((double)r);
-                    g7_st2_if(pub_z, zo + (size_t)(s0 + u) * 64u, etag | (bits & 0xffffffffull), etag | (bits >> 32));
-                }
+                const unsigned long long bits = (unsigned long long)__double_as_longlong((double)r);
+                g7_st2_if(pz, zo + (size_t)(s0 + u) * 64u, etag | (bits & 0xffffffffull), etag | (bits >> 32));
             }
         }
         if constexpr (MARK)
@@ -332,13 +334,15 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid7(uint32_t B, uint32_t ny, u
                     prev = active ? r : prev;
                     cur[u * 32 + lane] = r;
                 }
-            }
-            // the group's values to the next plane's warp, after any redo
+                // the group's values to the next plane's warp (the steps already
+                // handed over get the same values again)
 #pragma unroll
-            for (int u = 0; u < G; ++u)
-            {
-                const unsigned long long bits = (unsigned long long)__double_as_longlong((double)cur[u * 32 + lane]);
-                g7_st2_if(pub_z, zo + (size_t)(s0 + u) * 64u, etag | (bits & 0xffffffffull), etag | (bits >> 32));
+                for (int u = 0; u < G; ++u)
+                {
+                    const unsigned long long bits =
+                        (unsigned long long)__double_as_longlong((double)cur[u * 32 + lane]);
+                    g7_st2_if(pub_z, zo + (size_t)(s0 + u) * 64u, etag | (bits & 0xffffffffull), etag | (bits >> 32));
+                }
             }
         }
         // lane 31: the group's values of the last line to warp w + 1
