@@ -33,6 +33,14 @@
 namespace b2s {
 
 constexpr uint32_t kGrid7MaxWarps = 1u << 16;  // ny / 32 * nz line warps
+constexpr uint32_t kGrid7Ring = 32;            // steps of operands in flight (shared-memory ring)
+
+// packed steps per warp: B + 31 steps, rounded up to whole groups, plus the
+// steps the operand ring copies ahead of the last one
+inline uint32_t grid7_steps(uint32_t B)
+{
+    return (B + 31u + kGrid5Group - 1u) / kGrid5Group * kGrid5Group + kGrid7Ring;
+}
 
 template <typename VT>
 struct G7Slot;
@@ -67,6 +75,23 @@ __device__ __forceinline__ void g7_st2_if(bool q, unsigned long long* p, unsigne
 __device__ __forceinline__ void g7_ld2(const unsigned long long* p, unsigned long long& a, unsigned long long& b)
 {
     asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p));
+}
+__device__ __forceinline__ void g7_cp16(uint32_t dst, const void* src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+// BYTES (4 or 8) of src, zero-filled where src_bytes is 0
+template <int BYTES>
+__device__ __forceinline__ void g7_cp_small(uint32_t dst, const void* src, uint32_t src_bytes)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(BYTES), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void g7_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void g7_cp_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 template <typename VT>
@@ -130,7 +155,7 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid7(uint32_t B, uint32_t ny, u
     // FP32 reads the next group's words half way through a group, FP64 right
     // after the check (each the faster on 128^3, measured)
     constexpr bool NB_LATE = sizeof(XT) == 4;
-    extern __shared__ __align__(16) unsigned long long g7_sm[];  // two groups of results
+    extern __shared__ __align__(16) unsigned long long g7_sm[];  // two groups of results (4 KB), the operand ring
     XT* const stg = reinterpret_cast<XT*>(g7_sm);
     const uint32_t lane = threadIdx.x, nw = gridDim.x;
     uint32_t w = 0;
@@ -156,13 +181,42 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid7(uint32_t B, uint32_t ny, u
         RT r;
     };
     const G7Slot<VT>* ps = slot + (size_t)w * SP * 32u + lane;
-    uint32_t lk = k0, li = L * B - lane;
+    uint32_t lk = k0, li = L * B - lane, lq = 0;  // k, solve-order index and ring entry of the step being fetched
+    // registers, a group ahead (FP64 with a divisor: its long steps hide the
+    // latency) ...
     auto load_next = [&](Op& o) {
         o.c = g7_slot(ps);
         o.r = lk < B ? __ldg(&rhs[LOWER ? li : n - 1u - li]) : RT(0);
         ps += 32;
         ++lk;
         ++li;
+    };
+    // ... or a shared-memory ring of kGrid7Ring steps copied asynchronously
+    // kGrid7Ring - 1 steps ahead (FP32 and unit triangles, whose short steps
+    // would wait on operands that 128^3 streams from DRAM): step s reads entry
+    // s % kGrid7Ring, and its copy for step s + kGrid7Ring - 1 refills the
+    // entry that step s - 1 read
+    constexpr bool RING = sizeof(VT) == 4 || UNIT;
+    constexpr uint32_t D = kGrid7Ring;
+    const uint32_t ring_c = (uint32_t)__cvta_generic_to_shared(g7_sm) + 4096u;
+    const uint32_t ring_r = ring_c + D * 32u * (uint32_t)sizeof(G7Slot<VT>);
+    const G7Slot<VT>* ring_cp =
+        reinterpret_cast<const G7Slot<VT>*>(reinterpret_cast<const unsigned char*>(g7_sm) + 4096);
+    const RT* ring_rp = reinterpret_cast<const RT*>(ring_cp + D * 32u);
+    auto copy_next = [&]() {
+        const uint32_t e = lq * 32u + lane;
+#pragma unroll
+        for (uint32_t c = 0; c < sizeof(G7Slot<VT>) / 16; ++c)
+            g7_cp16(ring_c + e * (uint32_t)sizeof(G7Slot<VT>) + 16u * c,
+                    reinterpret_cast<const unsigned char*>(ps) + 16u * c);
+        const bool on = lk < B;
+        g7_cp_small<sizeof(RT)>(ring_r + e * (uint32_t)sizeof(RT), on ? &rhs[LOWER ? li : n - 1u - li] : rhs,
+                                on ? (uint32_t)sizeof(RT) : 0u);
+        g7_cp_commit();
+        ps += 32;
+        ++lk;
+        ++li;
+        lq = lq + 1u == D ? 0u : lq + 1u;
     };
     // warp w - 1's last-line words (every lane reads them) and warp w - nyb's
     // words of this lane, for the group starting at s0
@@ -220,9 +274,12 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid7(uint32_t B, uint32_t ny, u
             return (XT)__longlong_as_double(
                 (long long)(((wd[1] & 0xffffffffull) << 32) | (wd[0] & 0xffffffffull)));
     };
-    Op ops[G];
+    Op ops[RING ? 1 : G];
+    if constexpr (RING)
+        for (uint32_t q = 0; q + 1 < D; ++q) copy_next();
+    else
 #pragma unroll
-    for (int u = 0; u < G; ++u) load_next(ops[u]);
+        for (int u = 0; u < G; ++u) load_next(ops[u]);
     load_nb(0);
     XT prev = XT(0);
     uint32_t s0 = 0, g = 0;
@@ -286,8 +343,20 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid7(uint32_t B, uint32_t ny, u
             const bool active = k < B;
             XT nb = __shfl_up_sync(0xffffffffu, prev, 1);
             if (lane == 0) nb = nbv[u];
-            const Op o = ops[u];
-            load_next(ops[u]);
+            Op o;
+            if constexpr (RING)
+            {
+                g7_cp_wait<D - 2>();  // this step's copies have landed
+                const uint32_t e = ((s0 % D) + (uint32_t)u) * 32u + lane;
+                o.c = ring_cp[e];
+                o.r = ring_rp[e];
+                copy_next();
+            }
+            else
+            {
+                o = ops[u];
+                load_next(ops[u]);
+            }
             const XT sum = row_sum(o.r, o.c, zbv[u], nb, prev);
             XT r;
             if constexpr (UNIT)
@@ -368,6 +437,7 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid7(uint32_t B, uint32_t ny, u
 #pragma unroll
         for (int pass = 0; pass < G; ++pass) write_back(pass, s0 - G, stg + ((g - 1u) & 1u) * (G * 32));
     }
+    if constexpr (RING) g7_cp_wait<0>();  // no copy into shared memory outlives the CTA
     if (lane == 0)
     {
         __threadfence();
@@ -415,7 +485,7 @@ struct Grid7Tri
     void pack(b2s_ctx* ctx, const uint32_t* rp, const uint32_t* ci, const VT* v, const VT* d, bool lower, bool unit)
     {
         if (!on) return;
-        const uint32_t nw = warps(), SP = grid5_steps(B);
+        const uint32_t nw = warps(), SP = grid7_steps(B);
         const size_t slots = (size_t)nw * SP * 32;
         DBuf<G7Slot<VT>>* c;
         if constexpr (sizeof(VT) == 8)
@@ -452,7 +522,7 @@ struct Grid7Tri
             B2S_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGrid5MinSmem));
             attr = true;
         }
-        B2S_LAUNCH(ctx, kern, warps(), 32, kGrid5MinSmem, B, ny, nz, grid5_steps(B), c, rhs, x, out64, done, ew.p,
+        B2S_LAUNCH(ctx, kern, warps(), 32, kGrid5MinSmem, B, ny, nz, grid7_steps(B), c, rhs, x, out64, done, ew.p,
                    zw.p, ctl.p, ctx->errword(), grid_polls(ctx));
     }
 };
