@@ -608,7 +608,9 @@ struct Tri
                          TrsvOp<LOWER, UNIT, VT, XT, RT>{m->rp.p, m->ci.p, v, d, rhs, x, out64}, done);
     }
 
-    // x = T^-1 rhs; precision per the type parameters
+    // x = T^-1 rhs; precision per the type parameters.  With out64 the results
+    // also go there in FP64, and the grid schedules then leave x unwritten
+    // (an FP32 x is scratch for every caller that passes out64)
     template <typename VT, typename XT, typename RT>
     void solve(b2s_ctx* ctx, int mode, const VT* v, const VT* d, const RT* rhs, XT* x, double* out64, const int* done)
     {

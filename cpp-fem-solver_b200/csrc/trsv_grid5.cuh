@@ -236,7 +236,12 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid5(uint32_t B, uint32_t ny, u
         const bool p = ln < ny && k < B;
         const uint32_t i = ln * B + k, ii = LOWER ? i : n - 1u - i;
         const XT r = buf[u * 32u + l];
-        g5_stx_if(p, x + ii, r);
+        // FP32 given out64: the FP64 copy is the result and x is not written
+        // (FP64 keeps the unconditional store, the faster code there, measured)
+        if constexpr (sizeof(XT) == 4)
+            g5_stx_if(p && !w64, x + ii, r);
+        else
+            g5_stx_if(p, x + ii, r);
         g5_stx_if(p && w64, o64 + ii, (double)r);
     };
     // The row's entries in column order: lower (x, y-1) then (x-1, y), upper

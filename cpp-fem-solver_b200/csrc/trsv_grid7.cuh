@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(32, 1) k_trsv_grid7(uint32_t B, uint32_t ny, u
         const bool p = yl < ny && k < B;
         const uint32_t i = (zs * ny + yl) * B + k, ii = LOWER ? i : n - 1u - i;
         const XT r = buf[u * 32u + l];
-        g5_stx_if(p, x + ii, r);
+        g5_stx_if(p && !w64, x + ii, r);  // given out64, the FP64 copy is the result and x is not written
         g5_stx_if(p && w64, o64 + ii, (double)r);
     };
     // the row's entries in column order: lower (z-1), (y-1), (x-1); upper
