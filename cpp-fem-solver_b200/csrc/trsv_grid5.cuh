@@ -13,9 +13,10 @@
 // an issue slot.  Lane 0 takes the neighbouring line from warp w - 1's lane 31
 // through epoch-tagged 64-bit words in global memory ({epoch, 32 value bits}:
 // one store publishes a value, no fence), published at the end of each group
-// of kGrid5Group steps, read (half) a group ahead and checked when the group starts.
-// A level (anti-diagonal) costs one step: a shuffle, two products, two
-// differences and the divisor -- no shared-memory round trip and no barrier.
+// of kGrid5Group steps, read a group (FP32) or half a group (FP64) ahead and
+// checked when the group starts.  A level (anti-diagonal) costs one step: a
+// shuffle, two products, two differences and the divisor -- no shared-memory
+// round trip and no barrier.
 //
 // Each row is summed in its column order with the reference's arithmetic
 // (FP32 multiplies by a reciprocal rounded once from FP64, as the chunked
@@ -23,8 +24,8 @@
 // rounded reciprocal, g5_quotient, and divides where that is not exact), so
 // the result equals the other schedules bit for bit.  The step body is
 // branch-free: the write-back of the previous group's results (runs of eight
-// consecutive points, through shared memory) and the hand-over are predicated
-// stores interleaved with the steps.
+// consecutive points, through shared memory) is predicated stores interleaved
+// with the steps, and the hand-over predicated stores after them.
 //
 // The coefficients are packed at set-up in the order the warps consume them:
 // slot (w, s, j) holds lane j's point of step s as {c_y, c_x, divisor, 1 / d}
